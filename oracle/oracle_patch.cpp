@@ -1,0 +1,726 @@
+// ORACLE -- test infrastructure only (see oracle_patch.hpp).
+//
+// Every routine below restates one reference routine; the citation is given
+// above each.  Expression association follows the Fortran source (left to
+// right for * and /, as gfortran evaluates it) and the build uses
+// -ffp-contract=off so that no fused multiply-add changes a rounding.
+#include "oracle_patch.hpp"
+
+#include <algorithm>
+#include <stdexcept>
+
+namespace orc {
+
+namespace {
+
+// One 1-D slice array with Fortran index range [1-mbc, maxm+mbc].
+struct Slice {
+    int L, mbc;
+    Slice(int maxm, int mbc_) : L(maxm + 2 * mbc_), mbc(mbc_) {}
+    inline int at(int i) const { return i + mbc - 1; }
+};
+
+// ---------------------------------------------------------------------------
+// Riemann solvers.  Arrays are slice-major: a(i, m) -> a[m*L + at(i)],
+// wave(i, m, mw) -> wave[(mw*meqn + m)*L + at(i)], s(i, mw) -> s[mw*L + at(i)].
+// ---------------------------------------------------------------------------
+struct RiemannState {
+    // Fortran COMMON /comroe/ equivalents (Roe averages per interface).
+    std::vector<double> u, v, a, h, u2v2, enth, g1a2, euv;
+    void resize(int L) {
+        u.assign(L, 0); v.assign(L, 0); a.assign(L, 0); h.assign(L, 0);
+        u2v2.assign(L, 0); enth.assign(L, 0); g1a2.assign(L, 0); euv.assign(L, 0);
+    }
+};
+
+// applications/clawpack/advection/2d/all/clawpack46_rpn2adv.f:1-61
+void rpn2_adv(const Slice& S, int ixy, int meqn, int mwaves, int mx, const double* q,
+              const double* auxl, double* wave, double* s, double* amdq, double* apdq) {
+    const int L = S.L, mbc = S.mbc;
+    const int iface = ixy;  // aux component 1 = x velocity, 2 = y velocity
+    double delta[10];
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int ii = S.at(i);
+        for (int mq = 0; mq < meqn; ++mq)
+            for (int mw = 0; mw < mwaves; ++mw) wave[(mw * meqn + mq) * L + ii] = 0.0;
+        for (int mq = 0; mq < meqn; ++mq) {
+            delta[mq] = q[mq * L + ii] - q[mq * L + ii - 1];
+            for (int mw = 0; mw < mwaves; ++mw) wave[(mw * meqn + mq) * L + ii] = delta[mq];
+        }
+        for (int mw = 0; mw < mwaves; ++mw) s[mw * L + ii] = auxl[(iface - 1) * L + ii];
+        for (int mq = 0; mq < meqn; ++mq) {
+            amdq[mq * L + ii] = 0.0;
+            apdq[mq * L + ii] = 0.0;
+            for (int mw = 0; mw < mwaves; ++mw) {
+                const double sw = s[mw * L + ii];
+                const double w = wave[(mw * meqn + mq) * L + ii];
+                amdq[mq * L + ii] = amdq[mq * L + ii] + dmin(sw, 0.0) * w;
+                apdq[mq * L + ii] = apdq[mq * L + ii] + dmax(sw, 0.0) * w;
+            }
+        }
+    }
+}
+
+// applications/clawpack/advection/2d/all/clawpack46_rpt2adv.f:62-89
+void rpt2_adv(const Slice& S, int ixy, int meqn, int mx, const double* aux2, const double* aux3,
+              int imp, const double* asdq, double* bmasdq, double* bpasdq) {
+    const int L = S.L, mbc = S.mbc;
+    const int kv = 3 - ixy;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int ii = S.at(i);
+        const int i1 = S.at(i - 2 + imp);
+        for (int mq = 0; mq < meqn; ++mq) {
+            bmasdq[mq * L + ii] = dmin(aux2[(kv - 1) * L + i1], 0.0) * asdq[mq * L + ii];
+            bpasdq[mq * L + ii] = dmax(aux3[(kv - 1) * L + i1], 0.0) * asdq[mq * L + ii];
+        }
+    }
+}
+
+// applications/clawpack/shallow/2d/rp/clawpack46_rpn2.f:1-247 (entropy fix on)
+void rpn2_swe(const Slice& S, RiemannState& R, double grav, int ixy, int meqn, int mwaves, int mx,
+              const double* q, double* wave, double* s, double* amdq, double* apdq) {
+    const int L = S.L, mbc = S.mbc;
+    const int mu = (ixy == 1) ? 1 : 2;  // 0-based component of normal momentum
+    const int mv = (ixy == 1) ? 2 : 1;
+    auto Q = [&](int i, int m) { return q[m * L + S.at(i)]; };
+    auto W = [&](int i, int m, int mw) -> double& { return wave[(mw * meqn + m) * L + S.at(i)]; };
+    auto Sp = [&](int i, int mw) -> double& { return s[mw * L + S.at(i)]; };
+    auto AM = [&](int i, int m) -> double& { return amdq[m * L + S.at(i)]; };
+    auto AP = [&](int i, int m) -> double& { return apdq[m * L + S.at(i)]; };
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int ii = S.at(i);
+        R.h[ii] = (Q(i - 1, 0) + Q(i, 0)) / 2.0;
+        const double hsqrtl = std::sqrt(Q(i - 1, 0));
+        const double hsqrtr = std::sqrt(Q(i, 0));
+        const double hsq2 = hsqrtl + hsqrtr;
+        R.u[ii] = (Q(i - 1, mu) / hsqrtl + Q(i, mu) / hsqrtr) / hsq2;
+        R.v[ii] = (Q(i - 1, mv) / hsqrtl + Q(i, mv) / hsqrtr) / hsq2;
+        R.a[ii] = std::sqrt(grav * R.h[ii]);
+    }
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int ii = S.at(i);
+        const double u = R.u[ii], v = R.v[ii], a = R.a[ii];
+        const double d1 = Q(i, 0) - Q(i - 1, 0);
+        const double d2 = Q(i, mu) - Q(i - 1, mu);
+        const double d3 = Q(i, mv) - Q(i - 1, mv);
+        const double a1 = ((u + a) * d1 - d2) / (2.0 * a);
+        const double a2 = -(v * d1) + d3;
+        const double a3 = (-((u - a) * d1) + d2) / (2.0 * a);
+        W(i, 0, 0) = a1; W(i, mu, 0) = a1 * (u - a); W(i, mv, 0) = a1 * v; Sp(i, 0) = u - a;
+        W(i, 0, 1) = 0.0; W(i, mu, 1) = 0.0; W(i, mv, 1) = a2; Sp(i, 1) = u;
+        W(i, 0, 2) = a3; W(i, mu, 2) = a3 * (u + a); W(i, mv, 2) = a3 * v; Sp(i, 2) = u + a;
+    }
+    // entropy fix (label 110)
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const double him1 = Q(i - 1, 0);
+        const double s0 = Q(i - 1, mu) / him1 - std::sqrt(grav * him1);
+        double sfract;
+        if (s0 > 0.0 && Sp(i, 0) > 0.0) {
+            for (int m = 0; m < 3; ++m) AM(i, m) = 0.0;
+            goto done;
+        }
+        {
+            const double h1 = Q(i - 1, 0) + W(i, 0, 0);
+            const double hu1 = Q(i - 1, mu) + W(i, mu, 0);
+            const double s1 = hu1 / h1 - std::sqrt(grav * h1);
+            if (s0 < 0.0 && s1 > 0.0) sfract = s0 * ((s1 - Sp(i, 0)) / (s1 - s0));
+            else if (Sp(i, 0) < 0.0) sfract = Sp(i, 0);
+            else sfract = 0.0;
+            for (int m = 0; m < 3; ++m) AM(i, m) = sfract * W(i, m, 0);
+        }
+        if (Sp(i, 1) > 0.0) goto done;
+        for (int m = 0; m < 3; ++m) AM(i, m) = AM(i, m) + Sp(i, 1) * W(i, m, 1);
+        {
+            const double hi = Q(i, 0);
+            const double s03 = Q(i, mu) / hi + std::sqrt(grav * hi);
+            const double h3 = Q(i, 0) - W(i, 0, 2);
+            const double hu3 = Q(i, mu) - W(i, mu, 2);
+            const double s3 = hu3 / h3 + std::sqrt(grav * h3);
+            if (s3 < 0.0 && s03 > 0.0) sfract = s3 * ((s03 - Sp(i, 2)) / (s03 - s3));
+            else if (Sp(i, 2) < 0.0) sfract = Sp(i, 2);
+            else goto done;
+            for (int m = 0; m < 3; ++m) AM(i, m) = AM(i, m) + sfract * W(i, m, 2);
+        }
+    done:;
+    }
+    for (int m = 0; m < 3; ++m)
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            double df = 0.0;
+            for (int mw = 0; mw < mwaves; ++mw) df = df + Sp(i, mw) * W(i, m, mw);
+            AP(i, m) = df - AM(i, m);
+        }
+}
+
+// applications/clawpack/shallow/2d/rp/clawpack46_rpt2.f:1-74
+void rpt2_swe(const Slice& S, const RiemannState& R, int ixy, int meqn, int mwaves, int mx,
+              const double* asdq, double* bmasdq, double* bpasdq) {
+    const int L = S.L, mbc = S.mbc;
+    const int mu = (ixy == 1) ? 1 : 2;
+    const int mv = (ixy == 1) ? 2 : 1;
+    double waveb[3][3], sb[3];
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int ii = S.at(i);
+        const double u = R.u[ii], v = R.v[ii], a = R.a[ii];
+        const double q1 = asdq[0 * L + ii], qmu = asdq[mu * L + ii], qmv = asdq[mv * L + ii];
+        const double a1 = ((v + a) * q1 - qmv) / (2 * a);
+        const double a2 = qmu - u * q1;
+        const double a3 = (-((v - a) * q1) + qmv) / (2 * a);
+        waveb[0][0] = a1; waveb[mu][0] = a1 * u; waveb[mv][0] = a1 * (v - a); sb[0] = v - a;
+        waveb[0][1] = 0.0; waveb[mu][1] = a2; waveb[mv][1] = 0.0; sb[1] = v;
+        waveb[0][2] = a3; waveb[mu][2] = a3 * u; waveb[mv][2] = a3 * (v + a); sb[2] = v + a;
+        for (int m = 0; m < meqn; ++m) {
+            double bm = 0.0, bp = 0.0;
+            for (int mw = 0; mw < mwaves; ++mw) {
+                bm = bm + dmin(sb[mw], 0.0) * waveb[m][mw];
+                bp = bp + dmax(sb[mw], 0.0) * waveb[m][mw];
+            }
+            bmasdq[m * L + ii] = bm;
+            bpasdq[m * L + ii] = bp;
+        }
+    }
+}
+
+// applications/clawpack/euler/2d/rp/clawpack46_rpn2_euler4.f:1-289 (entropy fix on)
+void rpn2_euler4(const Slice& S, RiemannState& R, double gamma, double gamma1, int ixy, int meqn,
+                 int mwaves, int mx, const double* q, double* wave, double* s, double* amdq,
+                 double* apdq) {
+    const int L = S.L, mbc = S.mbc;
+    const int mu = (ixy == 1) ? 1 : 2;
+    const int mv = (ixy == 1) ? 2 : 1;
+    auto Q = [&](int i, int m) { return q[m * L + S.at(i)]; };
+    auto W = [&](int i, int m, int mw) -> double& { return wave[(mw * meqn + m) * L + S.at(i)]; };
+    auto Sp = [&](int i, int mw) -> double& { return s[mw * L + S.at(i)]; };
+    auto AM = [&](int i, int m) -> double& { return amdq[m * L + S.at(i)]; };
+    auto AP = [&](int i, int m) -> double& { return apdq[m * L + S.at(i)]; };
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int ii = S.at(i);
+        const double rhsqrtl = std::sqrt(Q(i - 1, 0));
+        const double rhsqrtr = std::sqrt(Q(i, 0));
+        const double pl = gamma1 * (Q(i - 1, 3) - 0.5 * (Q(i - 1, 1) * Q(i - 1, 1) +
+                                                          Q(i - 1, 2) * Q(i - 1, 2)) / Q(i - 1, 0));
+        const double pr = gamma1 * (Q(i, 3) - 0.5 * (Q(i, 1) * Q(i, 1) + Q(i, 2) * Q(i, 2)) / Q(i, 0));
+        const double rhsq2 = rhsqrtl + rhsqrtr;
+        R.u[ii] = (Q(i - 1, mu) / rhsqrtl + Q(i, mu) / rhsqrtr) / rhsq2;
+        R.v[ii] = (Q(i - 1, mv) / rhsqrtl + Q(i, mv) / rhsqrtr) / rhsq2;
+        R.enth[ii] = (((Q(i - 1, 3) + pl) / rhsqrtl + (Q(i, 3) + pr) / rhsqrtr)) / rhsq2;
+        R.u2v2[ii] = R.u[ii] * R.u[ii] + R.v[ii] * R.v[ii];
+        const double a2 = gamma1 * (R.enth[ii] - 0.5 * R.u2v2[ii]);
+        R.a[ii] = std::sqrt(a2);
+        R.g1a2[ii] = gamma1 / a2;
+        R.euv[ii] = R.enth[ii] - R.u2v2[ii];
+    }
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int ii = S.at(i);
+        const double u = R.u[ii], v = R.v[ii], a = R.a[ii], enth = R.enth[ii];
+        const double d1 = Q(i, 0) - Q(i - 1, 0);
+        const double d2 = Q(i, mu) - Q(i - 1, mu);
+        const double d3 = Q(i, mv) - Q(i - 1, mv);
+        const double d4 = Q(i, 3) - Q(i - 1, 3);
+        const double a3 = R.g1a2[ii] * (R.euv[ii] * d1 + u * d2 + v * d3 - d4);
+        const double a2 = d3 - v * d1;
+        const double a4 = (d2 + (a - u) * d1 - a * a3) / (2.0 * a);
+        const double a1 = d1 - a3 - a4;
+        W(i, 0, 0) = a1; W(i, mu, 0) = a1 * (u - a); W(i, mv, 0) = a1 * v;
+        W(i, 3, 0) = a1 * (enth - u * a); Sp(i, 0) = u - a;
+        W(i, 0, 1) = 0.0; W(i, mu, 1) = 0.0; W(i, mv, 1) = a2; W(i, 3, 1) = a2 * v; Sp(i, 1) = u;
+        W(i, 0, 2) = a3; W(i, mu, 2) = a3 * u; W(i, mv, 2) = a3 * v;
+        W(i, 3, 2) = a3 * 0.5 * R.u2v2[ii]; Sp(i, 2) = u;
+        W(i, 0, 3) = a4; W(i, mu, 3) = a4 * (u + a); W(i, mv, 3) = a4 * v;
+        W(i, 3, 3) = a4 * (enth + u * a); Sp(i, 3) = u + a;
+    }
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const double rhoim1 = Q(i - 1, 0);
+        const double pim1 = gamma1 * (Q(i - 1, 3) - 0.5 * (Q(i - 1, mu) * Q(i - 1, mu) +
+                                                           Q(i - 1, mv) * Q(i - 1, mv)) / rhoim1);
+        const double cim1 = std::sqrt(gamma * pim1 / rhoim1);
+        const double s0 = Q(i - 1, mu) / rhoim1 - cim1;
+        double sfract;
+        if (s0 >= 0.0 && Sp(i, 0) > 0.0) {
+            for (int m = 0; m < meqn; ++m) AM(i, m) = 0.0;
+            goto done;
+        }
+        {
+            const double rho1 = Q(i - 1, 0) + W(i, 0, 0);
+            const double rhou1 = Q(i - 1, mu) + W(i, mu, 0);
+            const double rhov1 = Q(i - 1, mv) + W(i, mv, 0);
+            const double en1 = Q(i - 1, 3) + W(i, 3, 0);
+            const double p1 = gamma1 * (en1 - 0.5 * (rhou1 * rhou1 + rhov1 * rhov1) / rho1);
+            const double c1 = std::sqrt(gamma * p1 / rho1);
+            const double s1 = rhou1 / rho1 - c1;
+            if (s0 < 0.0 && s1 > 0.0) sfract = s0 * (s1 - Sp(i, 0)) / (s1 - s0);
+            else if (Sp(i, 0) < 0.0) sfract = Sp(i, 0);
+            else sfract = 0.0;
+            for (int m = 0; m < meqn; ++m) AM(i, m) = sfract * W(i, m, 0);
+        }
+        if (Sp(i, 1) >= 0.0) goto done;
+        for (int m = 0; m < meqn; ++m) {
+            AM(i, m) = AM(i, m) + Sp(i, 1) * W(i, m, 1);
+            AM(i, m) = AM(i, m) + Sp(i, 2) * W(i, m, 2);
+        }
+        {
+            const double rhoi = Q(i, 0);
+            const double pi = gamma1 * (Q(i, 3) - 0.5 * (Q(i, mu) * Q(i, mu) +
+                                                         Q(i, mv) * Q(i, mv)) / rhoi);
+            const double ci = std::sqrt(gamma * pi / rhoi);
+            const double s3 = Q(i, mu) / rhoi + ci;
+            const double rho2 = Q(i, 0) - W(i, 0, 3);
+            const double rhou2 = Q(i, mu) - W(i, mu, 3);
+            const double rhov2 = Q(i, mv) - W(i, mv, 3);
+            const double en2 = Q(i, 3) - W(i, 3, 3);
+            const double p2 = gamma1 * (en2 - 0.5 * (rhou2 * rhou2 + rhov2 * rhov2) / rho2);
+            const double c2 = std::sqrt(gamma * p2 / rho2);
+            const double s2 = rhou2 / rho2 + c2;
+            if (s2 < 0.0 && s3 > 0.0) sfract = s2 * (s3 - Sp(i, 3)) / (s3 - s2);
+            else if (Sp(i, 3) < 0.0) sfract = Sp(i, 3);
+            else goto done;
+            for (int m = 0; m < meqn; ++m) AM(i, m) = AM(i, m) + sfract * W(i, m, 3);
+        }
+    done:;
+    }
+    for (int m = 0; m < meqn; ++m)
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            double df = 0.0;
+            for (int mw = 0; mw < mwaves; ++mw) df = df + Sp(i, mw) * W(i, m, mw);
+            AP(i, m) = df - AM(i, m);
+        }
+}
+
+// applications/clawpack/euler/2d/rp/clawpack46_rpt2_euler4.f:290-386
+void rpt2_euler4(const Slice& S, const RiemannState& R, int ixy, int meqn, int mx,
+                 const double* asdq, double* bmasdq, double* bpasdq) {
+    const int L = S.L, mbc = S.mbc;
+    const int mu = (ixy == 1) ? 1 : 2;
+    const int mv = (ixy == 1) ? 2 : 1;
+    double waveb[4][3], sb[3];
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int ii = S.at(i);
+        const double u = R.u[ii], v = R.v[ii], a = R.a[ii], enth = R.enth[ii];
+        const double q1 = asdq[0 * L + ii], qmu = asdq[mu * L + ii], qmv = asdq[mv * L + ii],
+                     q4 = asdq[3 * L + ii];
+        const double a3 = R.g1a2[ii] * (R.euv[ii] * q1 + u * qmu + v * qmv - q4);
+        const double a2 = qmu - u * q1;
+        const double a4 = (qmv + (a - v) * q1 - a * a3) / (2.0 * a);
+        const double a1 = q1 - a3 - a4;
+        waveb[0][0] = a1; waveb[mu][0] = a1 * u; waveb[mv][0] = a1 * (v - a);
+        waveb[3][0] = a1 * (enth - v * a); sb[0] = v - a;
+        waveb[0][1] = a3; waveb[mu][1] = a3 * u + a2; waveb[mv][1] = a3 * v;
+        waveb[3][1] = a3 * 0.5 * R.u2v2[ii] + a2 * u; sb[1] = v;
+        waveb[0][2] = a4; waveb[mu][2] = a4 * u; waveb[mv][2] = a4 * (v + a);
+        waveb[3][2] = a4 * (enth + v * a); sb[2] = v + a;
+        for (int m = 0; m < meqn; ++m) {
+            double bm = 0.0, bp = 0.0;
+            for (int mw = 0; mw < 3; ++mw) {
+                bm = bm + dmin(sb[mw], 0.0) * waveb[m][mw];
+                bp = bp + dmax(sb[mw], 0.0) * waveb[m][mw];
+            }
+            bmasdq[m * L + ii] = bm;
+            bpasdq[m * L + ii] = bp;
+        }
+    }
+}
+
+// src/solvers/fc2d_clawpack4.6/fortran_source/clawpack46_inlinelimiter.f:4-118
+void inlinelimiter(const Slice& S, int meqn, int mwaves, int mx, double* wave, const double* s,
+                   const int* mthlim) {
+    const int L = S.L;
+    auto W = [&](int i, int m, int mw) -> double& { return wave[(mw * meqn + m) * L + S.at(i)]; };
+    for (int mw = 0; mw < mwaves; ++mw) {
+        if (mthlim[mw] == 0) continue;
+        double dotr = 0.0;
+        for (int i = 0; i <= mx + 1; ++i) {
+            double wnorm2 = 0.0;
+            const double dotl = dotr;
+            dotr = 0.0;
+            for (int m = 0; m < meqn; ++m) {
+                wnorm2 = wnorm2 + W(i, m, mw) * W(i, m, mw);
+                dotr = dotr + W(i, m, mw) * W(i + 1, m, mw);
+            }
+            if (i == 0) continue;
+            if (wnorm2 == 0.0) continue;
+            const double r = (s[mw * L + S.at(i)] > 0.0) ? dotl / wnorm2 : dotr / wnorm2;
+            double wlimitr;
+            switch (mthlim[mw]) {
+                case 2: wlimitr = dmax(dmax(0.0, dmin(1.0, 2.0 * r)), dmin(2.0, r)); break;
+                case 3: wlimitr = (r + std::fabs(r)) / (1.0 + std::fabs(r)); break;
+                case 4: {
+                    const double c = (1.0 + r) / 2.0;
+                    wlimitr = dmax(0.0, dmin(dmin(c, 2.0), 2.0 * r));
+                    break;
+                }
+                case 5: wlimitr = r; break;
+                case 6: {
+                    const double th = (double)1.3f;  // REAL*4 literal assigned to a double
+                    wlimitr = dmax(0.0, dmin(dmin(th * r, (1 + r) / 2.0), th));
+                    break;
+                }
+                default:  // 1 and out-of-range values fall to label 10 (minmod)
+                    wlimitr = dmax(0.0, dmin(1.0, r));
+                    break;
+            }
+            for (int m = 0; m < meqn; ++m) W(i, m, mw) = wlimitr * W(i, m, mw);
+        }
+    }
+}
+
+struct Work {
+    Slice S;
+    int meqn, maux, mwaves;
+    std::vector<double> q1d, dtdx1d, dtdy1d, aux1, aux2, aux3, faddm, faddp, gaddm, gaddp;
+    std::vector<double> wave, s, amdq, apdq, cqxx, bmasdq, bpasdq;
+    RiemannState R;
+    Work(int maxm, int mbc, int meqn_, int maux_, int mwaves_)
+        : S(maxm, mbc), meqn(meqn_), maux(maux_), mwaves(mwaves_) {
+        const int L = S.L;
+        q1d.assign((size_t)L * meqn, 0); dtdx1d.assign(L, 0); dtdy1d.assign(L, 0);
+        aux1.assign((size_t)L * std::max(maux, 1), 0); aux2 = aux1; aux3 = aux1;
+        faddm.assign((size_t)L * meqn, 0); faddp = faddm;
+        gaddm.assign((size_t)L * meqn * 2, 0); gaddp = gaddm;
+        wave.assign((size_t)L * meqn * mwaves, 0); s.assign((size_t)L * mwaves, 0);
+        amdq.assign((size_t)L * meqn, 0); apdq = amdq; cqxx = amdq; bmasdq = amdq; bpasdq = amdq;
+        R.resize(L);
+    }
+};
+
+void call_rpn2(const SolverParams& sp, Work& w, int ixy, int mx) {
+    switch (sp.kind) {
+        case SOLVER_ADVECTION:
+            rpn2_adv(w.S, ixy, w.meqn, w.mwaves, mx, w.q1d.data(), w.aux2.data(), w.wave.data(),
+                     w.s.data(), w.amdq.data(), w.apdq.data());
+            break;
+        case SOLVER_SWE_ROE:
+            rpn2_swe(w.S, w.R, sp.grav, ixy, w.meqn, w.mwaves, mx, w.q1d.data(), w.wave.data(),
+                     w.s.data(), w.amdq.data(), w.apdq.data());
+            break;
+        case SOLVER_EULER4_ROE:
+            rpn2_euler4(w.S, w.R, sp.gamma, sp.gamma1, ixy, w.meqn, w.mwaves, mx, w.q1d.data(),
+                        w.wave.data(), w.s.data(), w.amdq.data(), w.apdq.data());
+            break;
+        default: throw std::runtime_error("unknown solver kind");
+    }
+}
+
+void call_rpt2(const SolverParams& sp, Work& w, int ixy, int mx, int imp, const double* asdq) {
+    switch (sp.kind) {
+        case SOLVER_ADVECTION:
+            rpt2_adv(w.S, ixy, w.meqn, mx, w.aux2.data(), w.aux3.data(), imp, asdq,
+                     w.bmasdq.data(), w.bpasdq.data());
+            break;
+        case SOLVER_SWE_ROE:
+            rpt2_swe(w.S, w.R, ixy, w.meqn, w.mwaves, mx, asdq, w.bmasdq.data(), w.bpasdq.data());
+            break;
+        case SOLVER_EULER4_ROE:
+            rpt2_euler4(w.S, w.R, ixy, w.meqn, mx, asdq, w.bmasdq.data(), w.bpasdq.data());
+            break;
+        default: throw std::runtime_error("unknown solver kind");
+    }
+}
+
+// src/solvers/fc2d_clawpack4.6/fortran_source/clawpack46_flux2.f:4-228
+double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, int mx,
+             const double* dtdx1d) {
+    const Slice& S = w.S;
+    const int L = S.L, mbc = S.mbc, meqn = w.meqn, mwaves = w.mwaves;
+    bool limit = false;
+    for (int mw = 0; mw < mwaves; ++mw)
+        if (mp.mthlim[mw] > 0) limit = true;
+    for (int side = 0; side < 2; ++side)
+        for (int m = 0; m < meqn; ++m)
+            for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+                w.faddm[m * L + S.at(i)] = 0.0;
+                w.faddp[m * L + S.at(i)] = 0.0;
+                w.gaddm[(side * meqn + m) * L + S.at(i)] = 0.0;
+                w.gaddp[(side * meqn + m) * L + S.at(i)] = 0.0;
+            }
+    call_rpn2(sp, w, ixy, mx);
+    for (int i = 2 - mbc; i <= mx + mbc - 1; ++i)
+        for (int m = 0; m < meqn; ++m) {
+            const int k = m * L + S.at(i);
+            w.faddp[k] = w.faddp[k] - w.apdq[k];
+            w.faddm[k] = w.faddm[k] + w.amdq[k];
+        }
+    double cfl1d = 0.0;
+    for (int mw = 0; mw < mwaves; ++mw)
+        for (int i = 1; i <= mx + 1; ++i) {
+            const double sw = w.s[mw * L + S.at(i)];
+            cfl1d = dmax(dmax(cfl1d, dtdx1d[S.at(i)] * sw), -dtdx1d[S.at(i - 1)] * sw);
+        }
+    if (mp.order0 == 2) {
+        if (limit) inlinelimiter(S, meqn, mwaves, mx, w.wave.data(), w.s.data(), mp.mthlim);
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            const double dtdxave = 0.5 * (dtdx1d[S.at(i - 1)] + dtdx1d[S.at(i)]);
+            for (int m = 0; m < meqn; ++m) {
+                const int k = m * L + S.at(i);
+                w.cqxx[k] = 0.0;
+                for (int mw = 0; mw < mwaves; ++mw) {
+                    const double as = std::fabs(w.s[mw * L + S.at(i)]);
+                    w.cqxx[k] = w.cqxx[k] + as * (1.0 - as * dtdxave) *
+                                                w.wave[(mw * meqn + m) * L + S.at(i)];
+                }
+                w.faddm[k] = w.faddm[k] + 0.5 * w.cqxx[k];
+                w.faddp[k] = w.faddp[k] + 0.5 * w.cqxx[k];
+            }
+        }
+    }
+    if (mp.order1 > 0) {
+        if (mp.order0 > 1 && mp.order1 == 2)
+            for (int i = 2 - mbc; i <= mx + mbc - 1; ++i)
+                for (int m = 0; m < meqn; ++m) {
+                    const int k = m * L + S.at(i);
+                    w.amdq[k] = w.amdq[k] + w.cqxx[k];
+                    w.apdq[k] = w.apdq[k] - w.cqxx[k];
+                }
+        call_rpt2(sp, w, ixy, mx, 1, w.amdq.data());
+        for (int m = 0; m < meqn; ++m)
+            for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+                const int k = m * L + S.at(i);
+                const int k1 = (0 * meqn + m) * L + S.at(i - 1);
+                const int k2 = (1 * meqn + m) * L + S.at(i - 1);
+                double gupdate = 0.5 * dtdx1d[S.at(i - 1)] * w.bmasdq[k];
+                w.gaddm[k1] = w.gaddm[k1] - gupdate;
+                w.gaddp[k1] = w.gaddp[k1] - gupdate;
+                gupdate = 0.5 * dtdx1d[S.at(i - 1)] * w.bpasdq[k];
+                w.gaddm[k2] = w.gaddm[k2] - gupdate;
+                w.gaddp[k2] = w.gaddp[k2] - gupdate;
+            }
+        call_rpt2(sp, w, ixy, mx, 2, w.apdq.data());
+        for (int m = 0; m < meqn; ++m)
+            for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+                const int k = m * L + S.at(i);
+                const int k1 = (0 * meqn + m) * L + S.at(i);
+                const int k2 = (1 * meqn + m) * L + S.at(i);
+                double gupdate = 0.5 * dtdx1d[S.at(i)] * w.bmasdq[k];
+                w.gaddm[k1] = w.gaddm[k1] - gupdate;
+                w.gaddp[k1] = w.gaddp[k1] - gupdate;
+                gupdate = 0.5 * dtdx1d[S.at(i)] * w.bpasdq[k];
+                w.gaddm[k2] = w.gaddm[k2] - gupdate;
+                w.gaddp[k2] = w.gaddp[k2] - gupdate;
+            }
+    }
+    return cfl1d;
+}
+
+}  // namespace
+
+double step2(const SolverParams& sp, const MethodParams& mp, int mx, int my, int mbc, int meqn,
+             int maux, double* q, const double* aux, double dx, double dy, double dt) {
+    const PatchIdx P(mx, my, mbc);
+    const int maxm = std::max(mx, my);
+    const int mwaves = mp.mwaves;
+    const bool capa = mp.mcapa > 0;
+    Work w(maxm, mbc, meqn, maux, mwaves);
+    const Slice& S = w.S;
+    const int L = S.L;
+    const size_t n = (size_t)P.size(meqn);
+    std::vector<double> fm(n, 0.0), fp(n, 0.0), gm(n, 0.0), gp(n, 0.0);
+
+    double cflgrid = 0.0;
+    const double dtdx = dt / dx, dtdy = dt / dy;
+    if (!capa)
+        for (int i = 1 - mbc; i <= maxm + mbc; ++i) {
+            w.dtdx1d[S.at(i)] = dtdx;
+            w.dtdy1d[S.at(i)] = dtdy;
+        }
+
+    // x-sweeps (clawpack46_step2.f:113-167)
+    for (int j = 2 - mbc; j <= my + mbc - 1; ++j) {
+        for (int m = 0; m < meqn; ++m)
+            for (int i = 1 - mbc; i <= mx + mbc; ++i) w.q1d[m * L + S.at(i)] = q[P(i, j, m)];
+        if (capa)
+            for (int i = 1 - mbc; i <= mx + mbc; ++i)
+                w.dtdx1d[S.at(i)] = dtdx / aux[P(i, j, mp.mcapa - 1)];
+        if (maux > 0)
+            for (int ma = 0; ma < maux; ++ma)
+                for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+                    w.aux1[ma * L + S.at(i)] = aux[P(i, j - 1, ma)];
+                    w.aux2[ma * L + S.at(i)] = aux[P(i, j, ma)];
+                    w.aux3[ma * L + S.at(i)] = aux[P(i, j + 1, ma)];
+                }
+        const double cfl1d = flux2(sp, mp, w, 1, mx, w.dtdx1d.data());
+        cflgrid = dmax(cflgrid, cfl1d);
+        for (int m = 0; m < meqn; ++m)
+            for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+                const int k = m * L + S.at(i);
+                fm[P(i, j, m)] = fm[P(i, j, m)] + w.faddm[k];
+                fp[P(i, j, m)] = fp[P(i, j, m)] + w.faddp[k];
+                gm[P(i, j, m)] = gm[P(i, j, m)] + w.gaddm[(0 * meqn + m) * L + S.at(i)];
+                gp[P(i, j, m)] = gp[P(i, j, m)] + w.gaddp[(0 * meqn + m) * L + S.at(i)];
+                gm[P(i, j + 1, m)] = gm[P(i, j + 1, m)] + w.gaddm[(1 * meqn + m) * L + S.at(i)];
+                gp[P(i, j + 1, m)] = gp[P(i, j + 1, m)] + w.gaddp[(1 * meqn + m) * L + S.at(i)];
+            }
+    }
+    // y-sweeps (clawpack46_step2.f:182-236)
+    for (int i = 2 - mbc; i <= mx + mbc - 1; ++i) {
+        for (int m = 0; m < meqn; ++m)
+            for (int j = 1 - mbc; j <= my + mbc; ++j) w.q1d[m * L + S.at(j)] = q[P(i, j, m)];
+        if (capa)
+            for (int j = 1 - mbc; j <= my + mbc; ++j)
+                w.dtdy1d[S.at(j)] = dtdy / aux[P(i, j, mp.mcapa - 1)];
+        if (maux > 0)
+            for (int ma = 0; ma < maux; ++ma)
+                for (int j = 1 - mbc; j <= my + mbc; ++j) {
+                    w.aux1[ma * L + S.at(j)] = aux[P(i - 1, j, ma)];
+                    w.aux2[ma * L + S.at(j)] = aux[P(i, j, ma)];
+                    w.aux3[ma * L + S.at(j)] = aux[P(i + 1, j, ma)];
+                }
+        const double cfl1d = flux2(sp, mp, w, 2, my, w.dtdy1d.data());
+        cflgrid = dmax(cflgrid, cfl1d);
+        for (int m = 0; m < meqn; ++m)
+            for (int j = 2 - mbc; j <= my + mbc; ++j) {
+                const int k = m * L + S.at(j);
+                gm[P(i, j, m)] = gm[P(i, j, m)] + w.faddm[k];
+                gp[P(i, j, m)] = gp[P(i, j, m)] + w.faddp[k];
+                fm[P(i, j, m)] = fm[P(i, j, m)] + w.gaddm[(0 * meqn + m) * L + S.at(j)];
+                fp[P(i, j, m)] = fp[P(i, j, m)] + w.gaddp[(0 * meqn + m) * L + S.at(j)];
+                fm[P(i + 1, j, m)] = fm[P(i + 1, j, m)] + w.gaddm[(1 * meqn + m) * L + S.at(j)];
+                fp[P(i + 1, j, m)] = fp[P(i + 1, j, m)] + w.gaddp[(1 * meqn + m) * L + S.at(j)];
+            }
+    }
+    // conservative update (clawpack46_step2_wrap.f:106-125)
+    for (int m = 0; m < meqn; ++m)
+        for (int i = 1 - mbc; i <= mx + mbc - 1; ++i)
+            for (int j = 1 - mbc; j <= my + mbc - 1; ++j) {
+                const double df = fm[P(i + 1, j, m)] - fp[P(i, j, m)];
+                const double dg = gm[P(i, j + 1, m)] - gp[P(i, j, m)];
+                if (!capa)
+                    q[P(i, j, m)] = q[P(i, j, m)] - dtdx * df - dtdy * dg;
+                else
+                    q[P(i, j, m)] = q[P(i, j, m)] - (dtdx * df + dtdy * dg) / aux[P(i, j, mp.mcapa - 1)];
+            }
+    return cflgrid;
+}
+
+void b4step2_swirl(int mx, int my, int mbc, int maux, double xlower, double ylower, double dx,
+                   double dy, double t, double dt, double tperiod, double* aux) {
+    (void)maux;
+    const PatchIdx P(mx, my, mbc);
+    if (tperiod == 0.0) return;
+    const double pi = 4.0 * std::atan(1.0);
+    const double pi2 = 2.0 * pi;
+    // swirl/psi.f
+    auto psi = [&](double xp, double yp) {
+        const double sx = std::sin(pi * xp), sy = std::sin(pi * yp);
+        return ((sx * sx) * (sy * sy)) / pi;
+    };
+    const double vt = std::cos(pi2 * (t + dt / 2.0) / tperiod);
+    const double vty = vt / dy;
+    const double vtx = vt / dx;
+    for (int j = 1 - mbc; j <= my + mbc; ++j) {
+        const double yll = ylower + (j - 1) * dy;
+        for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+            const double xll = xlower + (i - 1) * dx;
+            const double pij = psi(xll, yll);
+            aux[P(i, j, 0)] = vty * (psi(xll, yll + dy) - pij);
+            aux[P(i, j, 1)] = -vtx * (psi(xll + dx, yll) - pij);
+        }
+    }
+}
+
+void qinit_swirl(int mx, int my, int mbc, int meqn, double xlower, double ylower, double dx,
+                 double dy, double* q) {
+    (void)ylower; (void)dy;
+    const PatchIdx P(mx, my, mbc);
+    for (int mq = 0; mq < meqn; ++mq)
+        for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+            const double xc = xlower + (i - 0.5) * dx;
+            for (int j = 1 - mbc; j <= my + mbc; ++j) q[P(i, j, mq)] = (xc < 0.5) ? 1.0 : 0.0;
+        }
+}
+
+void qinit_radialdam(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy,
+                     double x0, double y0, double r0, double hin, double hout, double* q) {
+    const PatchIdx P(mx, my, mbc);
+    for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+        const double xc = xlower + (i - 0.5) * dx;
+        for (int j = 1 - mbc; j <= my + mbc; ++j) {
+            const double yc = ylower + (j - 0.5) * dy;
+            const double r = std::sqrt((xc - x0) * (xc - x0) + (yc - y0) * (yc - y0));
+            q[P(i, j, 0)] = (r < r0) ? hin : hout;
+            q[P(i, j, 1)] = 0.0;
+            q[P(i, j, 2)] = 0.0;
+        }
+    }
+}
+
+void qinit_quadrants(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy,
+                     double gamma1, const double* rpr, const double* rpu, const double* rpv,
+                     const double* rpp, double xs, double ys, double* q) {
+    const PatchIdx P(mx, my, mbc);
+    for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+        const double xcell = xlower + (i - 0.5) * dx;
+        for (int j = 1 - mbc; j <= my + mbc; ++j) {
+            const double ycell = ylower + (j - 0.5) * dy;
+            int iq = 0;
+            if (xcell >= xs && ycell >= ys) iq = 0;
+            if (xcell < xs && ycell >= ys) iq = 1;
+            if (xcell < xs && ycell < ys) iq = 2;
+            if (xcell >= xs && ycell < ys) iq = 3;
+            q[P(i, j, 0)] = rpr[iq];
+            q[P(i, j, 1)] = rpr[iq] * rpu[iq];
+            q[P(i, j, 2)] = rpr[iq] * rpv[iq];
+            q[P(i, j, 3)] = rpp[iq] / gamma1 + 0.5 * rpr[iq] * (rpu[iq] * rpu[iq] + rpv[iq] * rpv[iq]);
+        }
+    }
+}
+
+void bc2_default(int mx, int my, int mbc, int meqn, double* q, const int mthbc[4]) {
+    const PatchIdx P(mx, my, mbc);
+    auto bad = [](int k) {
+        return k == 0 || k == 2;  // user BC without a routine, or periodic: an error in bc2
+    };
+    for (int k = 0; k < 4; ++k)
+        if (bad(mthbc[k])) throw std::runtime_error("bc2_default: mthbc 0 or 2 not supported");
+    // left
+    if (mthbc[0] == 1) {
+        for (int m = 0; m < meqn; ++m)
+            for (int ibc = 1; ibc <= mbc; ++ibc)
+                for (int j = 1 - mbc; j <= my + mbc; ++j) q[P(1 - ibc, j, m)] = q[P(1, j, m)];
+    } else if (mthbc[0] == 3) {
+        for (int m = 0; m < meqn; ++m)
+            for (int ibc = 1; ibc <= mbc; ++ibc)
+                for (int j = 1 - mbc; j <= my + mbc; ++j) q[P(1 - ibc, j, m)] = q[P(ibc, j, m)];
+        for (int ibc = 1; ibc <= mbc; ++ibc)
+            for (int j = 1 - mbc; j <= my + mbc; ++j) q[P(1 - ibc, j, 1)] = -q[P(ibc, j, 1)];
+    }
+    // right
+    if (mthbc[1] == 1) {
+        for (int m = 0; m < meqn; ++m)
+            for (int ibc = 1; ibc <= mbc; ++ibc)
+                for (int j = 1 - mbc; j <= my + mbc; ++j) q[P(mx + ibc, j, m)] = q[P(mx, j, m)];
+    } else if (mthbc[1] == 3) {
+        for (int m = 0; m < meqn; ++m)
+            for (int ibc = 1; ibc <= mbc; ++ibc)
+                for (int j = 1 - mbc; j <= my + mbc; ++j)
+                    q[P(mx + ibc, j, m)] = q[P(mx + 1 - ibc, j, m)];
+        for (int ibc = 1; ibc <= mbc; ++ibc)
+            for (int j = 1 - mbc; j <= my + mbc; ++j)
+                q[P(mx + ibc, j, 1)] = -q[P(mx + 1 - ibc, j, 1)];
+    }
+    // bottom
+    if (mthbc[2] == 1) {
+        for (int m = 0; m < meqn; ++m)
+            for (int jbc = 1; jbc <= mbc; ++jbc)
+                for (int i = 1 - mbc; i <= mx + mbc; ++i) q[P(i, 1 - jbc, m)] = q[P(i, 1, m)];
+    } else if (mthbc[2] == 3) {
+        for (int m = 0; m < meqn; ++m)
+            for (int jbc = 1; jbc <= mbc; ++jbc)
+                for (int i = 1 - mbc; i <= mx + mbc; ++i) q[P(i, 1 - jbc, m)] = q[P(i, jbc, m)];
+        for (int jbc = 1; jbc <= mbc; ++jbc)
+            for (int i = 1 - mbc; i <= mx + mbc; ++i) q[P(i, 1 - jbc, 2)] = -q[P(i, jbc, 2)];
+    }
+    // top
+    if (mthbc[3] == 1) {
+        for (int m = 0; m < meqn; ++m)
+            for (int jbc = 1; jbc <= mbc; ++jbc)
+                for (int i = 1 - mbc; i <= mx + mbc; ++i) q[P(i, my + jbc, m)] = q[P(i, my, m)];
+    } else if (mthbc[3] == 3) {
+        for (int m = 0; m < meqn; ++m)
+            for (int jbc = 1; jbc <= mbc; ++jbc)
+                for (int i = 1 - mbc; i <= mx + mbc; ++i)
+                    q[P(i, my + jbc, m)] = q[P(i, my + 1 - jbc, m)];
+        for (int jbc = 1; jbc <= mbc; ++jbc)
+            for (int i = 1 - mbc; i <= mx + mbc; ++i)
+                q[P(i, my + jbc, 2)] = -q[P(i, my + 1 - jbc, 2)];
+    }
+}
+
+}  // namespace orc

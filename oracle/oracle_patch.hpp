@@ -1,0 +1,79 @@
+// ORACLE -- test infrastructure only.
+//
+// CPU restatement of ForestClaw's Clawpack 4.6 patch arithmetic, written
+// loop-for-loop after the reference Fortran so that loop bounds, accumulation
+// order and ghost-region updates are the same.  It exists to check the CUDA
+// path: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg
+// may load it.  The product library never links it.
+//
+// Storage convention (the reference "46" layout): q(i,j,m) with Fortran
+// indices i in [1-mbc, mx+mbc], j in [1-mbc, my+mbc], i fastest, then j, then m.
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+namespace orc {
+
+enum SolverKind {
+    SOLVER_ADVECTION = 0,   // clawpack46_rpn2adv / rpt2adv (swirl aux velocities)
+    SOLVER_SWE_ROE = 1,     // shallow/2d/rp/clawpack46_rpn2.f / rpt2.f
+    SOLVER_EULER4_ROE = 2,  // euler/2d/rp/clawpack46_rpn2_euler4.f / rpt2_euler4.f
+};
+
+struct SolverParams {
+    int kind = SOLVER_ADVECTION;
+    double grav = 1.0;      // /cparam/ grav (SWE)
+    double gamma = 1.4;     // /cparam/ gamma (Euler)
+    double gamma1 = 0.4;    // /cparam/ gamma1 = gamma - 1
+};
+
+struct MethodParams {
+    int order0 = 2;         // method(2): 1 = Godunov only, 2 = second-order corrections
+    int order1 = 2;         // method(3): 0 none, 1 transverse increments, 2 + corrections
+    int mcapa = 0;          // capacity index (0 = none)
+    int mwaves = 1;
+    int mthlim[8] = {4, 4, 4, 4, 4, 4, 4, 4};
+};
+
+// Index helper for one patch array with Fortran bounds.
+struct PatchIdx {
+    int mx, my, mbc, nx, ny;
+    PatchIdx(int mx_, int my_, int mbc_) : mx(mx_), my(my_), mbc(mbc_),
+        nx(mx_ + 2 * mbc_), ny(my_ + 2 * mbc_) {}
+    inline int64_t operator()(int i, int j, int m) const {
+        return ((int64_t)m * ny + (j + mbc - 1)) * nx + (i + mbc - 1);
+    }
+    inline int64_t size(int meqn) const { return (int64_t)meqn * nx * ny; }
+};
+
+// Fortran DMAX1/DMIN1 on non-NaN operands.
+inline double dmax(double a, double b) { return a > b ? a : b; }
+inline double dmin(double a, double b) { return a < b ? a : b; }
+
+// clawpack46_step2_wrap.f:1-127 + clawpack46_step2.f:5-239 + clawpack46_flux2.f:4-228.
+// Updates q in place over i,j = 1-mbc..mx+mbc-1 and returns cflgrid.
+double step2(const SolverParams& sp, const MethodParams& mp,
+             int mx, int my, int mbc, int meqn, int maux,
+             double* q, const double* aux, double dx, double dy, double dt);
+
+// swirl/user_4.6/b4step2.f (+ swirl/psi.f): time-dependent edge velocities.
+void b4step2_swirl(int mx, int my, int mbc, int maux, double xlower, double ylower,
+                   double dx, double dy, double t, double dt, double tperiod, double* aux);
+
+// swirl/user_4.6/qinit.f
+void qinit_swirl(int mx, int my, int mbc, int meqn, double xlower, double ylower,
+                 double dx, double dy, double* q);
+// Radial dam break (cell-centre test), hu = hv = 0.
+void qinit_radialdam(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy,
+                     double x0, double y0, double r0, double hin, double hout, double* q);
+// euler/2d/quadrants/user_4.6/qinit.f with the quadrant states as parameters
+// (rho, u, v, p for quadrants 1..4) and the split point (xs, ys).
+void qinit_quadrants(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy,
+                     double gamma1, const double* rpr, const double* rpu, const double* rpv,
+                     const double* rpp, double xs, double ys, double* q);
+
+// clawpack46_bc2_default.f: mthbc per side (left,right,bottom,top); -1 = skip.
+void bc2_default(int mx, int my, int mbc, int meqn, double* q, const int mthbc[4]);
+
+}  // namespace orc

@@ -1,0 +1,294 @@
+"""ctypes access to the CPU oracle (oracle/liboracle.so).
+
+Test infrastructure only: the oracle is the checker for the CUDA path and is
+never the thing measured or shipped.  The option arrays follow the layout
+fixed in oracle/oracle_capi.cpp.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE_DIR = ROOT / "oracle"
+
+# Solver kinds (oracle/oracle_patch.hpp SolverKind)
+ADVECTION, SWE_ROE, EULER4_ROE = 0, 1, 2
+# Problems (oracle/oracle_amr.hpp Problem)
+SWIRL, RADIALDAM, QUADRANTS = 0, 1, 2
+# Tagging criteria (oracle/oracle_clawpatch.hpp TagCriteria)
+VALUE, MINMAX, DIFFERENCE, GRADIENT = 0, 1, 2, 3
+
+_I_FIELDS = (["mx", "my", "mbc", "meqn", "maux", "order0", "order1", "mcapa", "mwaves"]
+             + [f"mthlim{k}" for k in range(8)] + [f"mthbc{k}" for k in range(4)]
+             + ["minlevel", "maxlevel", "subcycle", "regrid_interval", "smooth_refine",
+                "smooth_level", "criteria", "ivar", "use_fixed_dt", "nout", "init_ghostcell",
+                "reduce_cfl", "solver", "problem"])
+_D_FIELDS = (["refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
+              "desired_cfl", "grav", "gamma", "gamma1"] + [f"p{k}" for k in range(32)])
+
+
+@dataclass
+class Config:
+    """Options of one solve (names follow the reference's ini sections)."""
+    mx: int = 16
+    my: int = 16
+    mbc: int = 2
+    meqn: int = 1
+    maux: int = 2
+    order: tuple = (2, 2)
+    mcapa: int = 0
+    mwaves: int = 1
+    mthlim: tuple = (4,)
+    mthbc: tuple = (1, 1, 1, 1)
+    minlevel: int = 4
+    maxlevel: int = 4
+    subcycle: int = 1
+    regrid_interval: int = 1
+    smooth_refine: int = 0
+    smooth_level: int = 0
+    criteria: int = MINMAX
+    ivar: int = 0
+    use_fixed_dt: int = 0
+    nout: int = 1
+    init_ghostcell: int = 0
+    reduce_cfl: int = 1
+    solver: int = ADVECTION
+    problem: int = SWIRL
+    refine_threshold: float = 0.5
+    coarsen_threshold: float = 0.1
+    tfinal: float = 1.0
+    initial_dt: float = 0.01
+    max_cfl: float = 1.0
+    desired_cfl: float = 0.9
+    grav: float = 1.0
+    gamma: float = 1.4
+    pparams: tuple = field(default_factory=tuple)
+
+    @property
+    def gamma1(self) -> float:
+        return self.gamma - 1.0
+
+    def arrays(self):
+        iv = {
+            "mx": self.mx, "my": self.my, "mbc": self.mbc, "meqn": self.meqn, "maux": self.maux,
+            "order0": self.order[0], "order1": self.order[1], "mcapa": self.mcapa,
+            "mwaves": self.mwaves, "minlevel": self.minlevel, "maxlevel": self.maxlevel,
+            "subcycle": self.subcycle, "regrid_interval": self.regrid_interval,
+            "smooth_refine": self.smooth_refine, "smooth_level": self.smooth_level,
+            "criteria": self.criteria, "ivar": self.ivar, "use_fixed_dt": self.use_fixed_dt,
+            "nout": self.nout, "init_ghostcell": self.init_ghostcell,
+            "reduce_cfl": self.reduce_cfl, "solver": self.solver, "problem": self.problem,
+        }
+        for k in range(8):
+            iv[f"mthlim{k}"] = self.mthlim[k] if k < len(self.mthlim) else 0
+        for k in range(4):
+            iv[f"mthbc{k}"] = self.mthbc[k]
+        dv = {
+            "refine_threshold": self.refine_threshold, "coarsen_threshold": self.coarsen_threshold,
+            "tfinal": self.tfinal, "initial_dt": self.initial_dt, "max_cfl": self.max_cfl,
+            "desired_cfl": self.desired_cfl, "grav": self.grav, "gamma": self.gamma,
+            "gamma1": self.gamma1,
+        }
+        for k in range(32):
+            dv[f"p{k}"] = float(self.pparams[k]) if k < len(self.pparams) else 0.0
+        ia = (ctypes.c_int * len(_I_FIELDS))(*[int(iv[n]) for n in _I_FIELDS])
+        da = (ctypes.c_double * len(_D_FIELDS))(*[float(dv[n]) for n in _D_FIELDS])
+        return ia, da
+
+    @property
+    def nx(self) -> int:
+        return self.mx + 2 * self.mbc
+
+    @property
+    def ny(self) -> int:
+        return self.my + 2 * self.mbc
+
+
+_lib = None
+
+
+def lib():
+    """Load (building on first use if needed) the oracle shared library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    so = ORACLE_DIR / "liboracle.so"
+    srcs = list(ORACLE_DIR.glob("*.cpp")) + list(ORACLE_DIR.glob("*.hpp"))
+    if not so.exists() or any(s.stat().st_mtime > so.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-s", "liboracle.so"], cwd=ORACLE_DIR, check=True)
+    L = ctypes.CDLL(str(so))
+    assert L.orc_iopt_count() == len(_I_FIELDS), "oracle option layout changed"
+    assert L.orc_dopt_count() == len(_D_FIELDS), "oracle option layout changed"
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.orc_last_error.restype = ctypes.c_char_p
+    L.orc_solver_new.restype = ctypes.c_void_p
+    L.orc_solver_new.argtypes = [ip, dp]
+    for name in ["orc_solver_free", "orc_initialize", "orc_run", "orc_regrid", "orc_num_patches"]:
+        getattr(L, name).argtypes = [ctypes.c_void_p]
+    L.orc_advance.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, dp]
+    L.orc_update_single_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp]
+    L.orc_timeinterp_level.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+    L.orc_ghost_update.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+    L.orc_patch_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ip, ip, ip]
+    L.orc_get_q.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+    L.orc_set_q.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+    L.orc_get_qinterp.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+    L.orc_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]
+    L.orc_conservation.argtypes = [ctypes.c_void_p, dp]
+    L.orc_neighbors.argtypes = [ctypes.c_void_p, ctypes.c_int, ip]
+    L.orc_step2.argtypes = [ip, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp]
+    _lib = L
+    return L
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+
+
+class OracleSolver:
+    """One CPU solve: forest + patch data + counters."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        ia, da = cfg.arrays()
+        self._h = lib().orc_solver_new(ia, da)
+        if not self._h:
+            raise RuntimeError(lib().orc_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_solver_free(self._h)
+            self._h = None
+
+    def initialize(self):
+        _check(lib().orc_initialize(self._h))
+
+    def run(self):
+        _check(lib().orc_run(self._h))
+
+    def advance(self, t: float, dt: float) -> float:
+        c = ctypes.c_double()
+        _check(lib().orc_advance(self._h, t, dt, ctypes.byref(c)))
+        return c.value
+
+    def update_single_step(self, level: int, t: float, dt: float) -> float:
+        c = ctypes.c_double()
+        _check(lib().orc_update_single_step(self._h, level, t, dt, ctypes.byref(c)))
+        return c.value
+
+    def timeinterp(self, level: int, alpha: float):
+        _check(lib().orc_timeinterp_level(self._h, level, alpha))
+
+    def ghost_update(self, minlevel: int, maxlevel: int, t: float = 0.0, time_interp: int = 0):
+        _check(lib().orc_ghost_update(self._h, minlevel, maxlevel, t, time_interp))
+
+    def regrid(self):
+        _check(lib().orc_regrid(self._h))
+
+    @property
+    def num_patches(self) -> int:
+        return lib().orc_num_patches(self._h)
+
+    def patch_info(self, p: int):
+        lv, x, y = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lib().orc_patch_info(self._h, p, ctypes.byref(lv), ctypes.byref(x), ctypes.byref(y))
+        return lv.value, x.value, y.value
+
+    def leaves(self):
+        return [self.patch_info(p) for p in range(self.num_patches)]
+
+    def q(self, p: int) -> np.ndarray:
+        c = self.cfg
+        out = np.empty((c.meqn, c.ny, c.nx), dtype=np.float64)
+        lib().orc_get_q(self._h, p, _dptr(out))
+        return out
+
+    def qinterp(self, p: int) -> np.ndarray:
+        c = self.cfg
+        out = np.empty((c.meqn, c.ny, c.nx), dtype=np.float64)
+        lib().orc_get_qinterp(self._h, p, _dptr(out))
+        return out
+
+    def all_q(self) -> np.ndarray:
+        return np.stack([self.q(p) for p in range(self.num_patches)])
+
+    def set_q(self, p: int, q: np.ndarray):
+        a = np.ascontiguousarray(q, dtype=np.float64)
+        lib().orc_set_q(self._h, p, _dptr(a))
+
+    def counters(self):
+        a = (ctypes.c_longlong * 4)()
+        lib().orc_counters(self._h, a)
+        return {"count_amr_advance": a[0], "count_amr_new_domain": a[1],
+                "count_amr_regrid": a[2], "count_single_step": a[3]}
+
+    def conservation(self) -> np.ndarray:
+        out = np.zeros(self.cfg.meqn)
+        lib().orc_conservation(self._h, _dptr(out))
+        return out
+
+    def neighbors(self, p: int):
+        a = (ctypes.c_int * 22)()
+        lib().orc_neighbors(self._h, p, a)
+        return list(a)
+
+
+def step2(cfg: Config, q: np.ndarray, aux, dx: float, dy: float, dt: float) -> float:
+    """One clawpack46 patch update in place; returns the patch CFL number."""
+    ia, da = cfg.arrays()
+    c = ctypes.c_double()
+    auxp = _dptr(aux) if aux is not None else ctypes.POINTER(ctypes.c_double)()
+    _check(lib().orc_step2(ia, da, _dptr(q), auxp, dx, dy, dt, ctypes.byref(c)))
+    return c.value
+
+
+# ---- configurations of the reference regression tests -----------------------
+def swirl_regression(claw_version: int = 4) -> Config:
+    """applications/clawpack/advection/2d/swirl/regression.ini"""
+    return Config(mx=8, my=8, mbc=2, meqn=1, maux=3, order=(2, 2), mwaves=1, mthlim=(3,),
+                  mthbc=(1, 1, 1, 1), minlevel=2, maxlevel=6, regrid_interval=1,
+                  refine_threshold=0.25, coarsen_threshold=0.05, smooth_refine=1,
+                  tfinal=0.1, initial_dt=0.005, max_cfl=1.0, desired_cfl=0.9, nout=1,
+                  subcycle=1, solver=ADVECTION, problem=SWIRL, criteria=MINMAX,
+                  pparams=(4.0,))
+
+
+QUADRANT_STATES = (
+    # rho, u, v, p for quadrants 1..4 (euler/2d/quadrants/user_4.6/qinit.f)
+    (1.5, 0.0, 0.0, 1.5),
+    (0.532258064516129, 1.206045378311055, 0.0, 0.3),
+    (0.137992831541219, 1.206045378311055, 1.206045378311055, 0.029032258064516),
+    (0.532258064516129, 0.0, 1.206045378311055, 0.3),
+)
+
+
+def quadrants_params(states=QUADRANT_STATES, xs=0.8, ys=0.8):
+    rho = [s[0] for s in states]
+    u = [s[1] for s in states]
+    v = [s[2] for s in states]
+    p = [s[3] for s in states]
+    return tuple(rho + u + v + p + [xs, ys])
+
+
+def quadrants_regression() -> Config:
+    """applications/clawpack/euler/2d/quadrants/regression.ini on top of that directory's
+    fclaw_options.ini, which the application reads first from its working directory
+    (fclaw_base.c:758-786); that file sets refinement-criteria = difference."""
+    return Config(mx=8, my=8, mbc=2, meqn=4, maux=0, order=(2, 2), mwaves=4, mthlim=(4, 4, 4, 4),
+                  mthbc=(1, 1, 1, 1), minlevel=0, maxlevel=5, regrid_interval=1,
+                  refine_threshold=0.25, coarsen_threshold=0.025, smooth_refine=1, smooth_level=5,
+                  tfinal=0.1, initial_dt=0.05, max_cfl=1.0, desired_cfl=0.9, nout=1,
+                  subcycle=1, solver=EULER4_ROE, problem=QUADRANTS, criteria=DIFFERENCE, gamma=1.4,
+                  pparams=quadrants_params())
