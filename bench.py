@@ -1,0 +1,350 @@
+"""Benchmark of the patch hot path on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload uniform_swirl] [--level L] [--mx MX]
+
+One "step" is one fclaw2d_advance_all_levels call (every patch updated once by
+the clawpack 4.6 wave-propagation step, then the ghost-cell fill) on the
+uniform swirl advection case: meqn = 1, MC limiter, order (2,2), extrapolation
+boundaries, swirl velocities with T = 1, q0 = 1 for x < 0.5, FP64.  The mesh is
+uniform at `level` with mx = my = 16 (level 8: 65,536 patches, 16.8 M cells).
+The patch arrays (q, its pre-step copy, the time-interpolated copy and the
+CFL-retry copy) take more than the 126 MB L2, so no flush is needed between
+steps.
+
+Prints ONE JSON line.  With torchrun (N > 1) each rank advances its own
+replica (independent solves, weak scaling, no data-path collective); the time
+is the max over ranks and the value the cell updates of all ranks over it.
+
+--impl reference times the CPU restatement of the reference's Fortran/C
+(oracle/, compiled -O3 -march=native with OpenMP over the patches of a level)
+on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="uniform_swirl", choices=["uniform_swirl"])
+    p.add_argument("--level", type=int, default=8)
+    p.add_argument("--mx", type=int, default=16)
+    p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        smax = max((float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 5 + k and s[5 + k].lower().startswith("active")})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def peaks():
+    if PEAKS_FILE.exists():
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# ----------------------------------------------------------------------------
+# CPU restatement (oracle) timing: cpu_baseline and the reference arm
+# ----------------------------------------------------------------------------
+def native_oracle():
+    """Compile the OpenMP timing build of the oracle for this host's CPU."""
+    so = ROOT / "oracle" / "liboracle_native.so"
+    stamp = ROOT / "oracle" / "liboracle_native.host"
+    host = open("/proc/cpuinfo").read().split("model name")[1].split("\n")[0] if Path("/proc/cpuinfo").exists() else "?"
+    if not so.exists() or not stamp.exists() or stamp.read_text() != host:
+        srcs = [str(ROOT / "oracle" / f) for f in
+                ("oracle_patch.cpp", "oracle_clawpatch.cpp", "oracle_amr.cpp", "oracle_capi.cpp")]
+        cxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
+        subprocess.run([cxx, "-O3", "-march=native", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fopenmp",
+                        "-DORC_OPENMP", "-shared", "-o", str(so), *srcs], check=True)
+        stamp.write_text(host)
+    return so
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def time_oracle(cfg, dt, steps, warmup):
+    """Advance the oracle `warmup` + `steps` steps; returns (seconds for `steps`, cell updates)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle as O
+
+    O.use_library(native_oracle())
+    s = O.OracleSolver(cfg)
+    s.initialize()
+    t = 0.0
+    for _ in range(warmup):
+        s.advance(t, dt)
+        t += dt
+    c0 = s.counters()["count_single_step"]
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.advance(t, dt)
+        t += dt
+    el = time.perf_counter() - t0
+    cells = (s.counters()["count_single_step"] - c0) * cfg.mx * cfg.my
+    return el, cells
+
+
+def cpu_sample(args, budget_s):
+    import cases
+
+    cfg = cases.swirl_uniform(level=args.level, mx=args.mx)
+    dt = cases.swirl_dt(level=args.level, mx=args.mx)
+    el1, _ = time_oracle(cfg, dt, 1, 0)
+    steps = max(1, int(budget_s / max(el1, 1e-3)))
+    el, cells = time_oracle(cfg, dt, steps, 1)
+    return {"value": cells / el, "unit": "cell-updates/s", "cores": cpu_threads(), "kind": "port",
+            "sample": f"uniform swirl level {args.level}, mx={args.mx}: {steps} steps "
+                      f"({cells} cell updates, {el:.2f} s) of the C++ restatement of the reference "
+                      f"Fortran (reference binary not buildable: no Fortran compiler, MPI or p4est), "
+                      f"OpenMP over the patches of the level"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import cases
+
+    cfg = cases.swirl_uniform(level=args.level, mx=args.mx)
+    dt = cases.swirl_dt(level=args.level, mx=args.mx)
+    el, cells = time_oracle(cfg, dt, args.steps, args.warmup)
+    v = cells / el
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"uniform swirl advection, level {args.level}, mx=my={args.mx}, FP64",
+                   "patches": 4 ** args.level, "cells": 4 ** args.level * args.mx * args.mx},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cpu_threads(), "kind": "port",
+                         "sample": f"full workload, {args.steps} timed steps after {args.warmup} warm-up"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import forestclaw_b200 as fcb
+    from forestclaw_b200 import workloads
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.current_stream()
+    opts = workloads.uniform_swirl(args.level, args.mx)
+    dt = workloads.swirl_dt(args.level, args.mx)
+    s = fcb.Solver(opts, stream=stream.cuda_stream)
+    s.initialize()
+    npatch = s.num_patches
+    cells_per_step = npatch * args.mx * args.mx
+    t = 0.0
+    for _ in range(args.warmup):
+        s.advance_all_levels(t, dt)
+        t += dt
+    dist = world > 1
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    c0 = s.counters()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        if dist:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.advance_all_levels(t, dt)
+            t += dt
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            torch.distributed.barrier()
+    ms = e0.elapsed_time(e1)
+    c1 = s.counters()
+    launches = c1["count_kernel_launches"] - c0["count_kernel_launches"]
+    cells = (c1["count_single_step"] - c0["count_single_step"]) * args.mx * args.mx
+    ms_t = torch.tensor([ms], device="cuda")
+    if dist:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    total_cells = cells * world
+
+    # --- step-kernel alone: K launches of the level update between events ---
+    nk = max(5, args.steps)
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    k0.record(stream)
+    for _ in range(nk):
+        s.update_single_step_async(args.level, t, dt)
+    k1.record(stream)
+    torch.cuda.synchronize()
+    step_ms = k0.elapsed_time(k1) / nk
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(nk):
+        s.ghost_update(args.level, args.level, t, 0)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    ghost_ms = g0.elapsed_time(g1) / nk
+
+    # --- end to end through the C ABI with host buffers: upload the state from
+    # pinned host memory, advance K steps (host dt in, CFL out each step),
+    # download the result ---
+    psize = opts.meqn * opts.nx * opts.ny
+    host = torch.empty(npatch * psize, dtype=torch.float64, pin_memory=True)
+    hv = host.numpy().reshape(npatch, opts.meqn, opts.ny, opts.nx)
+    hv[...] = s.get_q()
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    t_e2e0 = time.perf_counter()
+    x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    s.set_q(hv)
+    for _ in range(args.steps):
+        s.advance_all_levels(t, dt)
+        t += dt
+    hv[...] = s.get_q()
+    x1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = x0.elapsed_time(x1)
+    e2e_t = torch.tensor([e2e_ms], device="cuda")
+    if dist:
+        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = float(e2e_t.item())
+    state_bytes = npatch * psize * 8
+
+    if rank != 0:
+        return None
+    hbm, src = peaks()
+    nx = opts.nx
+    bytes_per_cell = 8.0 * opts.meqn * (1.0 + nx * nx / (args.mx * args.mx))
+    achieved = cells_per_step * bytes_per_cell / (step_ms * 1e-3) / 1e9
+    line = {
+        "metric": "cell-updates/s", "value": total_cells / (ms_max * 1e-3), "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"uniform swirl advection, level {args.level}, mx=my={args.mx}, FP64 plain",
+                   "patches": npatch, "cells": cells_per_step, "l2_flush": "inputs larger than L2",
+                   "parallelism": f"{world} independent replicas" if world > 1 else "single GPU",
+                   "step_kernel_ms": step_ms, "ghost_fill_ms": ghost_ms},
+        "clocks": clk.summary(),
+        "e2e": {"value": total_cells / (e2e_ms * 1e-3),
+                "unit": "cell-updates/s",
+                "h2d_bytes_per_step": state_bytes / args.steps + 16,
+                "d2h_bytes_per_step": state_bytes / args.steps + 8},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback",
+                     "bytes_per_cell": bytes_per_cell, "kernel": "step_kernel"},
+    }
+    if world == 1:
+        sys.path.insert(0, str(ROOT / "tests"))
+        line["cpu_baseline"] = cpu_sample(args, args.cpu_seconds)
+    s.close()
+    return line
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        sys.path.insert(0, str(ROOT / "tests"))
+        line = run_reference(args, rank, world)
+        if line:
+            print(json.dumps(line), flush=True)
+        return
+    import torch
+
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        line = run_ours(args, rank, world, local_rank)
+        if line:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

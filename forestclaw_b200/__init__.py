@@ -1,0 +1,314 @@
+"""forestclaw_b200: the ForestClaw patch hot path on NVIDIA B200 (sm_100a).
+
+Python binding of the C ABI in include/fclaw_b200.h.  The names follow the
+reference's time-stepping core (fclaw2d_initialize, fclaw2d_run,
+fclaw2d_advance_all_levels, fclaw2d_update_single_step, fclaw2d_ghost_update,
+fclaw2d_timeinterp, fclaw2d_regrid) and its option sections ([clawpatch],
+[clawpack46], [Options]).
+
+The CUDA library is required: loading fails loudly if libfclaw_b200.so is
+missing, and there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+__all__ = ["Options", "Solver", "lib", "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
+           "SOLVER_EULER4_ROE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM", "PROBLEM_QUADRANTS",
+           "TAG_VALUE", "TAG_MINMAX", "TAG_DIFFERENCE", "TAG_GRADIENT", "EXPORTED_SYMBOLS"]
+
+PKG = Path(__file__).resolve().parent
+LIBPATH = PKG / "libfclaw_b200.so"
+
+SOLVER_ADVECTION, SOLVER_SWE_ROE, SOLVER_EULER4_ROE = 0, 1, 2
+PROBLEM_SWIRL, PROBLEM_RADIALDAM, PROBLEM_QUADRANTS = 0, 1, 2
+TAG_VALUE, TAG_MINMAX, TAG_DIFFERENCE, TAG_GRADIENT = 0, 1, 2, 3
+
+EXPORTED_SYMBOLS = (
+    "fcb_abi_version", "fcb_advance_all_levels", "fcb_conservation_check", "fcb_context_create",
+    "fcb_context_destroy", "fcb_counters", "fcb_curr_time", "fcb_get_q", "fcb_get_qinterp",
+    "fcb_ghost_update", "fcb_initialize", "fcb_last_error", "fcb_num_patches", "fcb_patch_info",
+    "fcb_patch_neighbors", "fcb_patch_size", "fcb_physical_set_bc", "fcb_regrid", "fcb_run",
+    "fcb_set_q", "fcb_single_step_update", "fcb_synchronize", "fcb_timeinterp",
+    "fcb_update_single_step", "fcb_update_single_step_async",
+)
+
+
+class _Options(ctypes.Structure):
+    """Mirror of fcb_options_t."""
+    _fields_ = [
+        ("mx", ctypes.c_int), ("my", ctypes.c_int), ("mbc", ctypes.c_int), ("meqn", ctypes.c_int),
+        ("maux", ctypes.c_int), ("refinement_criteria", ctypes.c_int),
+        ("threshold_variable", ctypes.c_int),
+        ("order", ctypes.c_int * 2), ("mcapa", ctypes.c_int), ("mwaves", ctypes.c_int),
+        ("mthlim", ctypes.c_int * 8), ("mthbc", ctypes.c_int * 4),
+        ("minlevel", ctypes.c_int), ("maxlevel", ctypes.c_int), ("subcycle", ctypes.c_int),
+        ("regrid_interval", ctypes.c_int), ("smooth_refine", ctypes.c_int),
+        ("smooth_level", ctypes.c_int), ("use_fixed_dt", ctypes.c_int), ("nout", ctypes.c_int),
+        ("init_ghostcell", ctypes.c_int), ("reduce_cfl", ctypes.c_int),
+        ("refine_threshold", ctypes.c_double), ("coarsen_threshold", ctypes.c_double),
+        ("tfinal", ctypes.c_double), ("initial_dt", ctypes.c_double), ("max_cfl", ctypes.c_double),
+        ("desired_cfl", ctypes.c_double),
+        ("solver_kind", ctypes.c_int), ("problem", ctypes.c_int),
+        ("grav", ctypes.c_double), ("gamma", ctypes.c_double),
+        ("problem_params", ctypes.c_double * 32),
+    ]
+
+
+class _Counters(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_longlong) for n in (
+        "count_amr_advance", "count_amr_new_domain", "count_amr_regrid", "count_single_step",
+        "count_ghost_waves", "count_kernel_launches")]
+
+
+@dataclass
+class Options:
+    """Options of one solve, named as in the reference's ini sections."""
+    # [clawpatch]
+    mx: int = 16
+    my: int = 16
+    mbc: int = 2
+    meqn: int = 1
+    maux: int = 2
+    refinement_criteria: int = TAG_MINMAX
+    threshold_variable: int = 1
+    # [clawpack46]
+    order: Sequence[int] = (2, 2)
+    mcapa: int = 0
+    mwaves: int = 1
+    mthlim: Sequence[int] = (4,)
+    mthbc: Sequence[int] = (1, 1, 1, 1)
+    # [Options]
+    minlevel: int = 4
+    maxlevel: int = 4
+    subcycle: int = 1
+    regrid_interval: int = 1
+    smooth_refine: int = 0
+    smooth_level: int = 0
+    use_fixed_dt: int = 0
+    nout: int = 1
+    init_ghostcell: int = 0
+    reduce_cfl: int = 1
+    refine_threshold: float = 0.5
+    coarsen_threshold: float = 0.1
+    tfinal: float = 1.0
+    initial_dt: float = 0.01
+    max_cfl: float = 1.0
+    desired_cfl: float = 0.9
+    # solver / problem
+    solver_kind: int = SOLVER_ADVECTION
+    problem: int = PROBLEM_SWIRL
+    grav: float = 1.0
+    gamma: float = 1.4
+    problem_params: Sequence[float] = field(default_factory=tuple)
+
+    def to_c(self) -> _Options:
+        o = _Options()
+        for name in ("mx", "my", "mbc", "meqn", "maux", "refinement_criteria", "threshold_variable",
+                     "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
+                     "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
+                     "reduce_cfl", "solver_kind", "problem"):
+            setattr(o, name, int(getattr(self, name)))
+        for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
+                     "desired_cfl", "grav", "gamma"):
+            setattr(o, name, float(getattr(self, name)))
+        o.order[0], o.order[1] = int(self.order[0]), int(self.order[1])
+        for k in range(8):
+            o.mthlim[k] = int(self.mthlim[k]) if k < len(self.mthlim) else 0
+        for k in range(4):
+            o.mthbc[k] = int(self.mthbc[k])
+        for k in range(32):
+            o.problem_params[k] = float(self.problem_params[k]) if k < len(self.problem_params) else 0.0
+        return o
+
+    @property
+    def nx(self) -> int:
+        return self.mx + 2 * self.mbc
+
+    @property
+    def ny(self) -> int:
+        return self.my + 2 * self.mbc
+
+
+class FcbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"fcb error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libfclaw_b200.so; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("FCB_LIBRARY", LIBPATH))
+    if not path.exists():
+        raise ImportError(f"{path} not found: build it with `python -m forestclaw_b200.build`")
+    L = ctypes.CDLL(str(path))
+    vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    sz = ctypes.c_size_t
+    L.fcb_last_error.restype = ctypes.c_char_p
+    L.fcb_context_create.argtypes = [ctypes.POINTER(_Options), vp, ctypes.POINTER(vp)]
+    L.fcb_context_destroy.argtypes = [vp]
+    for n in ("fcb_initialize", "fcb_run", "fcb_synchronize"):
+        getattr(L, n).argtypes = [vp]
+    L.fcb_advance_all_levels.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp]
+    L.fcb_update_single_step.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp]
+    L.fcb_update_single_step_async.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+    L.fcb_single_step_update.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_int, ctypes.c_int, dp]
+    L.fcb_ghost_update.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+    L.fcb_timeinterp.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.fcb_regrid.argtypes = [vp, ip]
+    L.fcb_physical_set_bc.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.fcb_num_patches.argtypes = [vp, ip]
+    L.fcb_patch_info.argtypes = [vp, ctypes.c_int, ip, ip, ip]
+    L.fcb_patch_neighbors.argtypes = [vp, ctypes.c_int, ip]
+    L.fcb_patch_size.argtypes = [vp, ctypes.POINTER(sz)]
+    L.fcb_get_q.argtypes = [vp, dp, sz]
+    L.fcb_set_q.argtypes = [vp, dp, sz]
+    L.fcb_get_qinterp.argtypes = [vp, dp, sz]
+    L.fcb_counters.argtypes = [vp, ctypes.POINTER(_Counters)]
+    L.fcb_conservation_check.argtypes = [vp, dp]
+    L.fcb_curr_time.argtypes = [vp, dp]
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise FcbError(rc, lib().fcb_last_error().decode())
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Solver:
+    """One solve on one GPU (a context of the C ABI)."""
+
+    def __init__(self, options: Options, stream: Optional[int] = None):
+        self.options = options
+        self._copt = options.to_c()
+        h = ctypes.c_void_p()
+        _check(lib().fcb_context_create(ctypes.byref(self._copt), ctypes.c_void_p(stream or 0),
+                                        ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().fcb_context_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- time stepping core -------------------------------------------------
+    def initialize(self):
+        _check(lib().fcb_initialize(self._h))
+
+    def run(self):
+        _check(lib().fcb_run(self._h))
+
+    def advance_all_levels(self, t: float, dt: float) -> float:
+        c = ctypes.c_double()
+        _check(lib().fcb_advance_all_levels(self._h, t, dt, ctypes.byref(c)))
+        return c.value
+
+    def update_single_step(self, level: int, t: float, dt: float) -> float:
+        c = ctypes.c_double()
+        _check(lib().fcb_update_single_step(self._h, level, t, dt, ctypes.byref(c)))
+        return c.value
+
+    def update_single_step_async(self, level: int, t: float, dt: float):
+        _check(lib().fcb_update_single_step_async(self._h, level, t, dt))
+
+    def single_step_update(self, patchno: int, t: float, dt: float, iter: int, total_count: int) -> float:
+        c = ctypes.c_double()
+        _check(lib().fcb_single_step_update(self._h, patchno, t, dt, iter, total_count, ctypes.byref(c)))
+        return c.value
+
+    def ghost_update(self, minlevel: int, maxlevel: int, sync_time: float = 0.0, time_interp: int = 0):
+        _check(lib().fcb_ghost_update(self._h, minlevel, maxlevel, sync_time, time_interp))
+
+    def timeinterp(self, level: int, alpha: float):
+        _check(lib().fcb_timeinterp(self._h, level, alpha))
+
+    def regrid(self) -> bool:
+        c = ctypes.c_int()
+        _check(lib().fcb_regrid(self._h, ctypes.byref(c)))
+        return bool(c.value)
+
+    def physical_set_bc(self, level: int, time_interp: int = 0):
+        _check(lib().fcb_physical_set_bc(self._h, level, time_interp))
+
+    def synchronize(self):
+        _check(lib().fcb_synchronize(self._h))
+
+    # --- queries -----------------------------------------------------------
+    @property
+    def num_patches(self) -> int:
+        n = ctypes.c_int()
+        _check(lib().fcb_num_patches(self._h, ctypes.byref(n)))
+        return n.value
+
+    def patch_info(self, p: int):
+        lv, x, y = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().fcb_patch_info(self._h, p, ctypes.byref(lv), ctypes.byref(x), ctypes.byref(y)))
+        return lv.value, x.value, y.value
+
+    def leaves(self):
+        return [self.patch_info(p) for p in range(self.num_patches)]
+
+    def neighbors(self, p: int):
+        a = (ctypes.c_int * 22)()
+        _check(lib().fcb_patch_neighbors(self._h, p, a))
+        return list(a)
+
+    def _shape(self):
+        o = self.options
+        return (self.num_patches, o.meqn, o.ny, o.nx)
+
+    def get_q(self) -> np.ndarray:
+        out = np.empty(self._shape(), dtype=np.float64)
+        _check(lib().fcb_get_q(self._h, _dp(out), out.size))
+        return out
+
+    def get_qinterp(self) -> np.ndarray:
+        out = np.empty(self._shape(), dtype=np.float64)
+        _check(lib().fcb_get_qinterp(self._h, _dp(out), out.size))
+        return out
+
+    def set_q(self, q: np.ndarray):
+        a = np.ascontiguousarray(q, dtype=np.float64)
+        if a.shape != self._shape():
+            raise ValueError(f"expected shape {self._shape()}, got {a.shape}")
+        _check(lib().fcb_set_q(self._h, _dp(a), a.size))
+
+    def counters(self) -> dict:
+        c = _Counters()
+        _check(lib().fcb_counters(self._h, ctypes.byref(c)))
+        return {n: getattr(c, n) for n, _ in _Counters._fields_}
+
+    def conservation_check(self) -> np.ndarray:
+        out = np.zeros(self.options.meqn)
+        _check(lib().fcb_conservation_check(self._h, _dp(out)))
+        return out
+
+    @property
+    def curr_time(self) -> float:
+        t = ctypes.c_double()
+        _check(lib().fcb_curr_time(self._h, ctypes.byref(t)))
+        return t.value

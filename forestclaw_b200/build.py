@@ -1,0 +1,73 @@
+"""Build libfclaw_b200.so (sm_100a) in-tree with nvcc.
+
+Usage: python -m forestclaw_b200.build [--force]
+
+The step kernel is compiled with -fmad=false: every multiply and add is
+rounded separately, as the reference Fortran is on x86-64 without FMA, so the
+FP64 results match the reference's arithmetic operation by operation.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "libfclaw_b200.so"
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+          "-I", str(PKG.parent / "include")]
+
+# per-source extra flags
+SOURCES = {
+    "fcb_step.cu": ["-fmad=false"],
+    "fcb_ghost.cu": ["-fmad=false"],
+    "fcb_amr.cu": ["-fmad=false"],
+    "fcb_runtime.cu": [],
+    "fcb_capi.cu": ["-Xcompiler", "-fvisibility=default"],
+}
+HEADERS = ["fcb_device.h", "fcb_solvers.cuh", "fcb_forest.hpp", "fcb_runtime.hpp"]
+
+
+def _stale(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    hdrs = [CSRC / h for h in HEADERS] + [PKG.parent / "include" / "fclaw_b200.h", Path(__file__)]
+    objs = []
+    jobs = []
+    for src, flags in SOURCES.items():
+        obj = BUILD / (src + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [CSRC / src] + hdrs):
+            cmd = [NVCC, *ARCH, *COMMON, *flags, "-c", str(CSRC / src), "-o", str(obj)]
+            jobs.append(cmd)
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        return r
+
+    with ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
+        list(ex.map(run, jobs))
+    if force or jobs or _stale(LIB, objs):
+        run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), *map(str, objs)])
+    return LIB
+
+
+if __name__ == "__main__":
+    p = build(force="--force" in sys.argv, verbose=True)
+    print(p)

@@ -1,0 +1,277 @@
+// Initial conditions, refinement tags, regrid transfers and the mass sum.
+//
+// References:
+//   qinit:     applications/clawpack/advection/2d/swirl/user_4.6/qinit.f,
+//              applications/clawpack/euler/2d/quadrants/user_4.6/qinit.f,
+//              radial dam break (cell-centre test, as configured for this path)
+//   tagging:   src/patches/clawpatch/fort_4.6/fclaw2d_clawpatch46_tag4refinement.f,
+//              fclaw2d_clawpatch46_tag4coarsening.f, fort_user/*_exceeds_th.f90.
+//              Every criterion's verdict is order independent (a running
+//              max-min only grows; the others are "any cell exceeds"), so the
+//              device reduces per patch and the host combines families.
+//   regrid:    fort_4.6/fclaw2d_clawpatch46_interpolate.f:324-400 (interpolate2fine),
+//              fort_4.6/fclaw2d_clawpatch46_average.f:282-364 (average2coarse)
+//   mass:      fort_4.6/fclaw2d_clawpatch46_diagnostics.f:13-58 (Kahan per patch)
+#include <cuda_runtime.h>
+
+#include "fcb_device.h"
+
+namespace fcb {
+
+__global__ void qinit_kernel(const QinitArgs a) {
+    const int pi = blockIdx.x;
+    if (pi >= a.n) return;
+    const int slot = a.slots[pi];
+    const PatchMeta mt = a.meta[slot];
+    const int nx = a.mx + 2 * a.mbc, ny = a.my + 2 * a.mbc;
+    double* q = a.q + (int64_t)slot * a.stride;
+    for (int k = threadIdx.x; k < nx * ny; k += blockDim.x) {
+        const int r = k / nx, c = k - r * nx;
+        const int i = c - a.mbc + 1, j = r - a.mbc + 1;
+        const double xc = mt.xlower + (i - 0.5) * mt.dx;
+        const double yc = mt.ylower + (j - 0.5) * mt.dy;
+        if (a.problem == PROB_SWIRL) {
+            for (int m = 0; m < a.meqn; ++m) q[((int64_t)m * ny + r) * nx + c] = (xc < 0.5) ? 1.0 : 0.0;
+        } else if (a.problem == PROB_RADIALDAM) {
+            const double x0 = a.p[0], y0 = a.p[1], r0 = a.p[2];
+            const double rr = sqrt((xc - x0) * (xc - x0) + (yc - y0) * (yc - y0));
+            q[((int64_t)0 * ny + r) * nx + c] = (rr < r0) ? a.p[3] : a.p[4];
+            q[((int64_t)1 * ny + r) * nx + c] = 0.0;
+            q[((int64_t)2 * ny + r) * nx + c] = 0.0;
+        } else if (a.problem == PROB_QUADRANTS) {
+            const double xs = a.p[16], ys = a.p[17];
+            int iq = 0;
+            if (xc >= xs && yc >= ys) iq = 0;
+            if (xc < xs && yc >= ys) iq = 1;
+            if (xc < xs && yc < ys) iq = 2;
+            if (xc >= xs && yc < ys) iq = 3;
+            const double rho = a.p[iq], u = a.p[4 + iq], v = a.p[8 + iq], pr = a.p[12 + iq];
+            q[((int64_t)0 * ny + r) * nx + c] = rho;
+            q[((int64_t)1 * ny + r) * nx + c] = rho * u;
+            q[((int64_t)2 * ny + r) * nx + c] = rho * v;
+            q[((int64_t)3 * ny + r) * nx + c] = pr / a.gamma1 + 0.5 * rho * (u * u + v * v);
+        }
+    }
+}
+
+cudaError_t launch_qinit(const QinitArgs& a, cudaStream_t st) {
+    if (a.n <= 0) return cudaSuccess;
+    qinit_kernel<<<a.n, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Tagging: per patch, the min/max of component ivar over all cells (ghosts
+// included) and, for the "difference"/"gradient"/"value" criteria, whether any
+// cell exceeds the refine and the coarsen threshold.
+// out[4*p + 0] = qmin, [1] = qmax, [2] = refine-exceeds (0/1), [3] = coarsen-exceeds (0/1)
+// ---------------------------------------------------------------------------
+__global__ void tag_kernel(const TagArgs a) {
+    const int pi = blockIdx.x;
+    if (pi >= a.n) return;
+    const int slot = a.slots[pi];
+    const PatchMeta mt = a.meta[slot];
+    const int nx = a.mx + 2 * a.mbc, ny = a.my + 2 * a.mbc;
+    const double* q = a.q + (int64_t)slot * a.stride + (int64_t)a.ivar * nx * ny;
+    double qmin = q[(a.mbc) * nx + a.mbc], qmax = qmin;
+    int ex_r = 0, ex_c = 0;
+    for (int k = threadIdx.x; k < nx * ny; k += blockDim.x) {
+        const int r = k / nx, c = k - r * nx;
+        const double v = q[k];
+        qmin = v < qmin ? v : qmin;
+        qmax = v > qmax ? v : qmax;
+        const bool ghost = c < a.mbc || r < a.mbc || c >= a.mbc + a.mx || r >= a.mbc + a.my;
+        if (a.criteria == TAG_VALUE) {
+            ex_r |= (v > a.refine_th);
+            ex_c |= (v > a.coarsen_th);
+        } else if (!ghost && (a.criteria == TAG_DIFFERENCE || a.criteria == TAG_GRADIENT)) {
+            const double e = q[k + 1], w = q[k - 1], n_ = q[k + nx], s = q[k - nx];
+            if (a.criteria == TAG_DIFFERENCE) {
+                const double dqx = fabs(e - w), dqy = fabs(n_ - s);
+                const double dq = dqx > dqy ? dqx : dqy;
+                ex_r |= (dq > a.refine_th);
+                ex_c |= (dq > a.coarsen_th);
+            } else {
+                const double dx2 = 2 * mt.dx, dy2 = 2 * mt.dy;
+                const double dqx = (e - w) / dx2, dqy = (n_ - s) / dy2;
+                const double g3 = 0;
+                const double ds = sqrt(dqx * dqx + dqy * dqy + g3 * g3);
+                ex_r |= (ds > a.refine_th);
+                ex_c |= (ds > a.coarsen_th);
+            }
+        }
+    }
+    __shared__ double smin[32], smax[32];
+    __shared__ int sr[32], sc[32];
+    for (int off = 16; off > 0; off >>= 1) {
+        const double a1 = __shfl_xor_sync(0xffffffffu, qmin, off);
+        const double a2 = __shfl_xor_sync(0xffffffffu, qmax, off);
+        qmin = a1 < qmin ? a1 : qmin;
+        qmax = a2 > qmax ? a2 : qmax;
+        ex_r |= __shfl_xor_sync(0xffffffffu, ex_r, off);
+        ex_c |= __shfl_xor_sync(0xffffffffu, ex_c, off);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { smin[w] = qmin; smax[w] = qmax; sr[w] = ex_r; sc[w] = ex_c; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int k = 1; k < nw; ++k) {
+            qmin = smin[k] < qmin ? smin[k] : qmin;
+            qmax = smax[k] > qmax ? smax[k] : qmax;
+            ex_r |= sr[k];
+            ex_c |= sc[k];
+        }
+        a.out[4 * pi + 0] = qmin;
+        a.out[4 * pi + 1] = qmax;
+        a.out[4 * pi + 2] = ex_r;
+        a.out[4 * pi + 3] = ex_c;
+    }
+}
+
+cudaError_t launch_tag(const TagArgs& a, cudaStream_t st) {
+    if (a.n <= 0) return cudaSuccess;
+    tag_kernel<<<a.n, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Regrid transfers.  ops[3*k] = kind (0 = interpolate2fine, 1 = average2coarse),
+// ops[3*k+1] = coarse slot, ops[3*k+2] = first of four consecutive entries in
+// `fine` (the four children in z-order).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double slope5b(double sl, double sr) {
+    const double sc = (sl + sr) / 2.0;
+    double m = 2 * fabs(sl);
+    const double b = 2 * fabs(sr), cc = fabs(sc);
+    if (b < m) m = b;
+    if (cc < m) m = cc;
+    const double s0 = copysign(1.0, sl * sr);
+    return m * (s0 > 0.0 ? s0 : 0.0) * copysign(1.0, sc);
+}
+
+__global__ void regrid_kernel(double* q, int64_t stride, const int32_t* ops, const int32_t* fine,
+                              int nops, int mx, int my, int mbc, int meqn) {
+    const int k = blockIdx.x >> 2;  // four CTAs per record: one per child
+    const int igrid = blockIdx.x & 3;
+    if (k >= nops) return;
+    const int kind = ops[3 * k], cslot = ops[3 * k + 1];
+    const int fslot = fine[ops[3 * k + 2] + igrid];
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    double* qc = q + (int64_t)cslot * stride;
+    double* qf = q + (int64_t)fslot * stride;
+    auto C = [&](int i, int j, int m) -> double& { return qc[((int64_t)m * ny + j + mbc - 1) * nx + i + mbc - 1]; };
+    auto F = [&](int i, int j, int m) -> double& { return qf[((int64_t)m * ny + j + mbc - 1) * nx + i + mbc - 1]; };
+    const int ig = igrid % 2, jg = igrid / 2;
+    if (kind == 0) {
+        const int i1 = 1 - ig, i2 = mx / 2 + (1 - ig), ic_add = ig * mx / 2;
+        const int j1 = 1 - jg, j2 = my / 2 + (1 - jg), jc_add = jg * my / 2;
+        const int wi = i2 - i1 + 1, wj = j2 - j1 + 1;
+        for (int t = threadIdx.x; t < meqn * wi * wj; t += blockDim.x) {
+            const int m = t / (wi * wj), rem = t - m * wi * wj;
+            const int j = j1 + rem / wi, i = i1 + rem % wi;
+            const int ic = i + ic_add, jc = j + jc_add;
+            const double qcv = C(ic, jc, m);
+            double sl = (qcv - C(ic - 1, jc, m));
+            double sr = (C(ic + 1, jc, m) - qcv);
+            const double gradx = slope5b(sl, sr);
+            sl = (qcv - C(ic, jc - 1, m));
+            sr = (C(ic, jc + 1, m) - qcv);
+            const double grady = slope5b(sl, sr);
+            for (int ii = 1; ii <= 2; ++ii)
+                for (int jj = 1; jj <= 2; ++jj) {
+                    const double shiftx = (ii - 2 / 2.0 - 0.5) / 2;
+                    const double shifty = (jj - 2 / 2.0 - 0.5) / 2;
+                    F((i - 1) * 2 + ii, (j - 1) * 2 + jj, m) = qcv + shiftx * gradx + shifty * grady;
+                }
+        }
+    } else {
+        const int ic_add = ig * mx / 2, jc_add = jg * mx / 2;  // the reference uses mx for both
+        const int wi = mx / 2, wj = my / 2;
+        for (int t = threadIdx.x; t < meqn * wi * wj; t += blockDim.x) {
+            const int m = t / (wi * wj), rem = t - m * wi * wj;
+            const int j = 1 + rem / wi, i = 1 + rem % wi;
+            double sum = 0;
+            sum = sum + F((i - 1) * 2 + 1, (j - 1) * 2 + 1, m);
+            sum = sum + F((i - 1) * 2 + 2, (j - 1) * 2 + 1, m);
+            sum = sum + F((i - 1) * 2 + 1, (j - 1) * 2 + 2, m);
+            sum = sum + F((i - 1) * 2 + 2, (j - 1) * 2 + 2, m);
+            C(i + ic_add, j + jc_add, m) = sum / 4;
+        }
+    }
+}
+
+cudaError_t launch_regrid(double* q, int64_t stride, const int32_t* ops, const int32_t* fine, int nops,
+                          int mx, int my, int mbc, int meqn, cudaStream_t st) {
+    if (nops <= 0) return cudaSuccess;
+    regrid_kernel<<<nops * 4, 128, 0, st>>>(q, stride, ops, fine, nops, mx, my, mbc, meqn);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Mass: Kahan-compensated sum of q*dx*dy over the interior of each patch, in
+// the reference's loop order (m, j, i); out[p*meqn + m].
+// ---------------------------------------------------------------------------
+__global__ void mass_kernel(const double* q, int64_t stride, const int32_t* slots, const PatchMeta* meta,
+                            int n, int mx, int my, int mbc, int meqn, double* out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int slot = slots[p];
+    const double area = meta[slot].dx * meta[slot].dy;
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    const double* qp = q + (int64_t)slot * stride;
+    for (int m = 0; m < meqn; ++m) {
+        double sum = 0.0, ck = 0.0;
+        for (int j = 1; j <= my; ++j)
+            for (int i = 1; i <= mx; ++i) {
+                const double y = qp[((int64_t)m * ny + j + mbc - 1) * nx + i + mbc - 1] * area - ck;
+                const double t = sum + y;
+                ck = (t - sum) - y;
+                sum = t;
+            }
+        out[(int64_t)p * meqn + m] = sum;
+    }
+}
+
+cudaError_t launch_mass(const double* q, int64_t stride, const int32_t* slots, const PatchMeta* meta, int n,
+                        int mx, int my, int mbc, int meqn, double* out, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    mass_kernel<<<(n + 127) / 128, 128, 0, st>>>(q, stride, slots, meta, n, mx, my, mbc, meqn, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Gather / scatter of whole patches between the slot arena and a contiguous
+// buffer (leaf order), so that host transfers are one copy each way.
+// ---------------------------------------------------------------------------
+__global__ void gather_kernel(const double* __restrict__ src, int64_t stride, const int32_t* slots, int n,
+                              int64_t psize, double* __restrict__ dst) {
+    const int p = blockIdx.y;
+    if (p >= n) return;
+    const double* s = src + (int64_t)slots[p] * stride;
+    double* d = dst + (int64_t)p * psize;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < psize; k += (int64_t)gridDim.x * blockDim.x)
+        d[k] = s[k];
+}
+
+__global__ void scatter_kernel(double* __restrict__ dst, int64_t stride, const int32_t* slots, int n,
+                               int64_t psize, const double* __restrict__ src) {
+    const int p = blockIdx.y;
+    if (p >= n) return;
+    double* d = dst + (int64_t)slots[p] * stride;
+    const double* s = src + (int64_t)p * psize;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < psize; k += (int64_t)gridDim.x * blockDim.x)
+        d[k] = s[k];
+}
+
+cudaError_t launch_gather(const double* src, int64_t stride, const int32_t* slots, int n, int64_t psize,
+                          double* dst, bool scatter, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int bx = (int)((psize + 255) / 256 < 8 ? (psize + 255) / 256 : 8);
+    dim3 grid(bx, n);
+    if (scatter) scatter_kernel<<<grid, 256, 0, st>>>(const_cast<double*>(src), stride, slots, n, psize, dst);
+    else gather_kernel<<<grid, 256, 0, st>>>(src, stride, slots, n, psize, dst);
+    return cudaGetLastError();
+}
+
+}  // namespace fcb

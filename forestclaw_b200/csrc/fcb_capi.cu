@@ -1,0 +1,204 @@
+// extern "C" entry points declared in include/fclaw_b200.h.  Every call
+// catches exceptions and CUDA errors and turns them into status codes; the
+// library never terminates the process.
+#include <cmath>
+#include <new>
+#include <string>
+
+#include "fcb_runtime.hpp"
+
+struct fcb_context {
+    fcb::Context* impl;
+};
+
+namespace {
+thread_local std::string g_error;
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        return FCB_OK;
+    } catch (const fcb::Error& e) {
+        g_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_error = "out of host memory";
+        return FCB_ERR_INTERNAL;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return FCB_ERR_INTERNAL;
+    }
+}
+
+int need(const void* p, const char* what) {
+    if (!p) throw fcb::Error(FCB_ERR_INVALID, std::string("null argument: ") + what);
+    return 0;
+}
+}  // namespace
+
+extern "C" {
+
+const char* fcb_last_error(void) { return g_error.c_str(); }
+int fcb_abi_version(void) { return FCB_ABI_VERSION; }
+
+int fcb_context_create(const fcb_options_t* opt, void* cuda_stream, fcb_context_t** out) {
+    return guard([&] {
+        need(opt, "opt");
+        need(out, "out");
+        *out = nullptr;
+        auto* c = new fcb_context{nullptr};
+        try {
+            c->impl = new fcb::Context(*opt, (cudaStream_t)cuda_stream);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int fcb_context_destroy(fcb_context_t* ctx) {
+    return guard([&] {
+        if (!ctx) return;
+        delete ctx->impl;
+        delete ctx;
+    });
+}
+
+#define CTX()                 \
+    need(ctx, "ctx");         \
+    fcb::Context& C = *ctx->impl
+
+int fcb_initialize(fcb_context_t* ctx) { return guard([&] { CTX(); C.initialize(); }); }
+int fcb_run(fcb_context_t* ctx) { return guard([&] { CTX(); C.run(); }); }
+
+int fcb_advance_all_levels(fcb_context_t* ctx, double t, double dt, double* maxcfl) {
+    return guard([&] {
+        CTX();
+        need(maxcfl, "maxcfl");
+        *maxcfl = C.advance_all_levels(t, dt);
+        if (std::isnan(*maxcfl)) throw fcb::Error(FCB_ERR_NUMERIC, "NaN in the CFL number");
+    });
+}
+
+int fcb_update_single_step(fcb_context_t* ctx, int level, double t, double dt, double* maxcfl) {
+    return guard([&] {
+        CTX();
+        need(maxcfl, "maxcfl");
+        *maxcfl = C.update_single_step(level, t, dt);
+        if (std::isnan(*maxcfl)) throw fcb::Error(FCB_ERR_NUMERIC, "NaN in the CFL number");
+    });
+}
+
+int fcb_update_single_step_async(fcb_context_t* ctx, int level, double t, double dt) {
+    return guard([&] { CTX(); C.update_single_step_async(level, t, dt); });
+}
+
+int fcb_single_step_update(fcb_context_t* ctx, int patchno, double t, double dt, int iter, int total_count,
+                           double* cfl) {
+    return guard([&] {
+        CTX();
+        need(cfl, "cfl");
+        if (iter < 0 || total_count <= 0 || iter >= total_count) throw fcb::Error(FCB_ERR_INVALID, "bad iter/total_count");
+        *cfl = C.single_step_update(patchno, t, dt, iter, total_count);
+    });
+}
+
+int fcb_ghost_update(fcb_context_t* ctx, int minlevel, int maxlevel, double sync_time, int time_interp) {
+    return guard([&] {
+        CTX();
+        C.ghost_update(minlevel, maxlevel, sync_time, time_interp);
+    });
+}
+
+int fcb_timeinterp(fcb_context_t* ctx, int level, double alpha) {
+    return guard([&] { CTX(); C.timeinterp(level, alpha); });
+}
+
+int fcb_regrid(fcb_context_t* ctx, int* changed) {
+    return guard([&] {
+        CTX();
+        const bool ch = C.regrid();
+        if (changed) *changed = ch ? 1 : 0;
+    });
+}
+
+int fcb_physical_set_bc(fcb_context_t* ctx, int level, int time_interp) {
+    return guard([&] { CTX(); C.physical_set_bc(level, time_interp); });
+}
+
+int fcb_num_patches(fcb_context_t* ctx, int* n) {
+    return guard([&] {
+        CTX();
+        need(n, "n");
+        *n = C.num_patches();
+    });
+}
+
+int fcb_patch_info(fcb_context_t* ctx, int p, int* level, int* x, int* y) {
+    return guard([&] {
+        CTX();
+        if (p < 0 || p >= C.num_patches()) throw fcb::Error(FCB_ERR_INVALID, "bad patch number");
+        const fcb::Leaf& l = C.leaf(p);
+        if (level) *level = l.level;
+        if (x) *x = l.x;
+        if (y) *y = l.y;
+    });
+}
+
+int fcb_patch_neighbors(fcb_context_t* ctx, int p, int* out) {
+    return guard([&] {
+        CTX();
+        need(out, "out");
+        if (p < 0 || p >= C.num_patches()) throw fcb::Error(FCB_ERR_INVALID, "bad patch number");
+        const fcb::Neighbors& n = C.nbrs(p);
+        for (int f = 0; f < 4; ++f) {
+            out[f] = n.face_rel[f];
+            out[4 + 2 * f] = n.face_nbr[f][0];
+            out[5 + 2 * f] = n.face_nbr[f][1];
+            out[12 + f] = n.corner_rel[f];
+            out[16 + f] = n.corner_nbr[f];
+        }
+        out[20] = n.has_fine;
+        out[21] = n.on_cf;
+    });
+}
+
+int fcb_patch_size(fcb_context_t* ctx, size_t* n) {
+    return guard([&] {
+        CTX();
+        need(n, "n");
+        *n = C.patch_size();
+    });
+}
+
+int fcb_get_q(fcb_context_t* ctx, double* host, size_t n) {
+    return guard([&] { CTX(); need(host, "host"); C.get_q(host, n, false); });
+}
+int fcb_set_q(fcb_context_t* ctx, const double* host, size_t n) {
+    return guard([&] { CTX(); need(host, "host"); C.set_q(host, n); });
+}
+int fcb_get_qinterp(fcb_context_t* ctx, double* host, size_t n) {
+    return guard([&] { CTX(); need(host, "host"); C.get_q(host, n, true); });
+}
+
+int fcb_counters(fcb_context_t* ctx, fcb_counters_t* out) {
+    return guard([&] {
+        CTX();
+        need(out, "out");
+        *out = C.counters();
+    });
+}
+
+int fcb_conservation_check(fcb_context_t* ctx, double* sums) {
+    return guard([&] { CTX(); need(sums, "sums"); C.conservation(sums); });
+}
+
+int fcb_curr_time(fcb_context_t* ctx, double* t) {
+    return guard([&] { CTX(); need(t, "t"); *t = C.curr_time(); });
+}
+
+int fcb_synchronize(fcb_context_t* ctx) { return guard([&] { CTX(); C.synchronize(); }); }
+
+}  // extern "C"

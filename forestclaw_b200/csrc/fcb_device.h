@@ -1,0 +1,94 @@
+// Plain-old-data structures shared by the host runtime and the CUDA kernels.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace fcb {
+
+// Per-slot patch geometry, uploaded after each regrid.
+struct PatchMeta {
+    double xlower, ylower, dx, dy;
+    int32_t level;
+    int32_t flags;  // PATCH_SAVE_LAST: write q into qlast before stepping
+};
+enum : int32_t { PATCH_SAVE_LAST = 1 };
+
+enum SolverKind : int32_t { SOLVER_ADVECTION = 0, SOLVER_SWE_ROE = 1, SOLVER_EULER4_ROE = 2 };
+enum AuxKind : int32_t { AUX_NONE = 0, AUX_SWIRL = 1, AUX_STORED = 2 };
+
+// Arguments of one batched step launch (all patches of one level).
+struct StepArgs {
+    double* q;             // arena base
+    double* qlast;         // arena base
+    const double* aux;     // stored-aux arena base (AUX_STORED), else null
+    const int32_t* slots;  // patch list
+    const PatchMeta* meta; // indexed by slot
+    int64_t q_stride;      // doubles per slot in q / qlast
+    int64_t aux_stride;    // doubles per slot in aux
+    int32_t npatches;
+    int32_t maux;
+    int32_t order0, order1;
+    int32_t mthlim[8];
+    double dt;
+    double vt;             // swirl: cos(2 pi (t + dt/2) / tperiod)
+    double grav, gamma, gamma1;
+    unsigned long long* cfl_out;  // atomicMax on the bits of a non-negative double
+};
+
+// Ghost-cell operations, one record per reference kernel call.
+enum GhostOpType : int32_t {
+    OP_COPY_FACE = 0,
+    OP_COPY_CORNER = 1,
+    OP_AVERAGE_FACE = 2,
+    OP_AVERAGE_CORNER = 3,
+    OP_INTERP_FACE = 4,
+    OP_INTERP_CORNER = 5,
+    OP_PHYSBC = 6,
+};
+struct GhostOp {
+    int32_t type;
+    int32_t dst;       // slot written (this patch / coarse patch for average / fine patch for interp)
+    int32_t src;       // slot read
+    int32_t face;      // iface / icorner (relative to the coarse patch for average/interp)
+    int32_t dx, dy;    // index shift (copy) or fine-index offset D (average/interp)
+    int32_t dst_ti;    // 1: dst uses the time-interpolated array
+    int32_t src_ti;    // 1: src uses the time-interpolated array
+    int32_t mthbc[4];  // physbc: per side, -1 = not a physical boundary
+};
+
+// Arguments of one ghost-fill wave launch.
+struct GhostArgs {
+    double* q;        // arena of current solutions
+    double* qti;      // arena of time-interpolated solutions
+    int64_t stride;
+    int mx, my, mbc, meqn;
+    const GhostOp* ops;
+    int nops;
+};
+
+enum Problem : int32_t { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2 };
+
+struct QinitArgs {
+    double* q;
+    int64_t stride;
+    const int32_t* slots;
+    const PatchMeta* meta;
+    int n, mx, my, mbc, meqn, problem;
+    double gamma1;
+    double p[32];
+};
+
+enum TagCriteria : int32_t { TAG_VALUE = 0, TAG_MINMAX = 1, TAG_DIFFERENCE = 2, TAG_GRADIENT = 3 };
+
+// out[4*p + 0] = qmin, [1] = qmax, [2] = refine-exceeds (0/1), [3] = coarsen-exceeds (0/1)
+struct TagArgs {
+    const double* q;
+    int64_t stride;
+    const int32_t* slots;
+    const PatchMeta* meta;
+    int n, mx, my, mbc, ivar, criteria;
+    double refine_th, coarsen_th;
+    double* out;
+};
+
+}  // namespace fcb

@@ -1,0 +1,258 @@
+// Ghost-cell fill kernels (copy / average / interpolate across faces and
+// corners, physical boundary conditions) and time interpolation.
+//
+// One warp executes one GhostOp record; a launch executes one "wave" of
+// records that the host has proven independent (no record in a wave reads or
+// writes cells another record of the same wave writes), so the result equals
+// the reference's sequential order.
+//
+// References (clawpack 4.6 layout, same-block transforms):
+//   copy:        src/patches/clawpatch/fort_4.6/fclaw2d_clawpatch46_copy.f:17-133
+//   average:     fort_4.6/fclaw2d_clawpatch46_average.f:16-272
+//   interpolate: fort_4.6/fclaw2d_clawpatch46_interpolate.f:30-314 (+ slopes,
+//                fclaw2d_clawpatch_utils.f:11-66 with mth = 5)
+//   physical BC: src/solvers/fc2d_clawpack4.6/fortran_source/clawpack46_bc2_default.f
+//   time interp: fort_4.6/fclaw2d_clawpatch46_timeinterp.f:11-78
+// Index transforms: src/forestclaw2d.c same-block branches; a copy maps
+// (i,j) -> (i+dx, j+dy); a half-size map sends coarse (ic,jc) to the fine
+// cells (2ic+dx+kx, 2jc+dy+ky), kx,ky in {0,1}.
+#include <cuda_runtime.h>
+
+#include "fcb_device.h"
+
+namespace fcb {
+
+namespace {
+
+struct PatchView {
+    double* p;
+    int mx, my, mbc, nx, ny;
+    __device__ __forceinline__ double& at(int i, int j, int m) const {
+        return p[((int64_t)m * ny + (j + mbc - 1)) * nx + (i + mbc - 1)];
+    }
+};
+
+// fclaw2d_clawpatch_compute_slopes, mth = 5 (SIGN(1,x) follows the sign bit).
+__device__ __forceinline__ double slope5(double sl, double sr) {
+    const double sc = (sl + sr) / 2.0;
+    double m = 2 * fabs(sl);
+    const double b = 2 * fabs(sr), cc = fabs(sc);
+    if (b < m) m = b;
+    if (cc < m) m = cc;
+    const double s0 = copysign(1.0, sl * sr);
+    return m * (s0 > 0.0 ? s0 : 0.0) * copysign(1.0, sc);
+}
+
+__device__ __forceinline__ void interp_cell(const PatchView& C, const PatchView& F, int m, int ic, int jc,
+                                            int i20, int j20) {
+    const double qc = C.at(ic, jc, m);
+    double sl = (qc - C.at(ic - 1, jc, m));
+    double sr = (C.at(ic + 1, jc, m) - qc);
+    const double gradx = slope5(sl, sr);
+    sl = (qc - C.at(ic, jc - 1, m));
+    sr = (C.at(ic, jc + 1, m) - qc);
+    const double grady = slope5(sl, sr);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int ii = k & 1, jj = k >> 1;
+        const double shiftx = (ii - 0.5) / 2.0;
+        const double shifty = (jj - 0.5) / 2.0;
+        F.at(i20 + ii, j20 + jj, m) = qc + gradx * shiftx + grady * shifty;
+    }
+}
+
+}  // namespace
+
+__global__ void ghost_wave_kernel(const GhostArgs a) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= a.nops) return;
+    const GhostOp op = a.ops[warp];
+    const int mx = a.mx, my = a.my, mbc = a.mbc, meqn = a.meqn;
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    PatchView D{(op.dst_ti ? a.qti : a.q) + (int64_t)op.dst * a.stride, mx, my, mbc, nx, ny};
+    PatchView S{(op.src_ti ? a.qti : a.q) + (int64_t)op.src * a.stride, mx, my, mbc, nx, ny};
+
+    switch (op.type) {
+        case OP_COPY_FACE: {
+            int i0, i1, j0, j1;
+            if (op.face == 0) { i0 = 1 - mbc; i1 = 0; j0 = 1; j1 = my; }
+            else if (op.face == 1) { i0 = mx + 1; i1 = mx + mbc; j0 = 1; j1 = my; }
+            else if (op.face == 2) { i0 = 1; i1 = mx; j0 = 1 - mbc; j1 = 0; }
+            else { i0 = 1; i1 = mx; j0 = my + 1; j1 = my + mbc; }
+            const int w = i1 - i0 + 1, h = j1 - j0 + 1, n = w * h * meqn;
+            for (int k = lane; k < n; k += 32) {
+                const int m = k / (w * h), rem = k - m * w * h, jj = rem / w, ii = rem - jj * w;
+                const int i = i0 + ii, j = j0 + jj;
+                D.at(i, j, m) = S.at(i + op.dx, j + op.dy, m);
+            }
+            break;
+        }
+        case OP_COPY_CORNER: {
+            const int n = mbc * mbc * meqn;
+            for (int k = lane; k < n; k += 32) {
+                const int m = k / (mbc * mbc), rem = k - m * mbc * mbc;
+                const int ibc = rem / mbc + 1, jbc = rem % mbc + 1;
+                int i1, j1;
+                if (op.face == 0) { i1 = 1 - ibc; j1 = 1 - jbc; }
+                else if (op.face == 1) { i1 = mx + ibc; j1 = 1 - jbc; }
+                else if (op.face == 2) { i1 = 1 - ibc; j1 = my + jbc; }
+                else { i1 = mx + ibc; j1 = my + jbc; }
+                D.at(i1, j1, m) = S.at(i1 + op.dx, j1 + op.dy, m);
+            }
+            break;
+        }
+        case OP_AVERAGE_FACE: {
+            // dst = coarse patch, src = fine patch; face is the coarse face.
+            const int idir = op.face / 2;
+            const int along = idir == 0 ? my : mx;
+            const int n = along * mbc * meqn;
+            for (int k = lane; k < n; k += 32) {
+                const int m = k / (along * mbc), rem = k - m * along * mbc;
+                const int t = rem / mbc + 1, bc = rem % mbc + 1;
+                int ic, jc;
+                if (idir == 0) { jc = t; ic = (op.face == 0) ? 1 - bc : mx + bc; }
+                else { ic = t; jc = (op.face == 2) ? 1 - bc : my + bc; }
+                const int fi = 2 * ic + op.dx, fj = 2 * jc + op.dy;
+                if (fi < 1 || fi + 1 > mx || fj < 1 || fj + 1 > my) continue;  // is_valid_average
+                double sum = 0;
+                sum = sum + S.at(fi, fj, m);
+                sum = sum + S.at(fi + 1, fj, m);
+                sum = sum + S.at(fi, fj + 1, m);
+                sum = sum + S.at(fi + 1, fj + 1, m);
+                D.at(ic, jc, m) = sum / 4.0;
+            }
+            break;
+        }
+        case OP_AVERAGE_CORNER: {
+            const int n = mbc * mbc * meqn;
+            for (int k = lane; k < n; k += 32) {
+                const int m = k / (mbc * mbc), rem = k - m * mbc * mbc;
+                const int ibc = rem / mbc + 1, jbc = rem % mbc + 1;
+                int i1, j1;
+                if (op.face == 0) { i1 = 1 - ibc; j1 = 1 - jbc; }
+                else if (op.face == 1) { i1 = mx + ibc; j1 = 1 - jbc; }
+                else if (op.face == 2) { i1 = 1 - ibc; j1 = my + jbc; }
+                else { i1 = mx + ibc; j1 = my + jbc; }
+                const int fi = 2 * i1 + op.dx, fj = 2 * j1 + op.dy;
+                double sum = 0;
+                sum = sum + S.at(fi, fj, m);
+                sum = sum + S.at(fi + 1, fj, m);
+                sum = sum + S.at(fi, fj + 1, m);
+                sum = sum + S.at(fi + 1, fj + 1, m);
+                D.at(i1, j1, m) = sum / 4.0;
+            }
+            break;
+        }
+        case OP_INTERP_FACE: {
+            // src = coarse patch (q or time-interpolated), dst = fine patch (q).
+            const int idir = op.face / 2;
+            const int nb = mbc / 2;
+            const int along = idir == 0 ? mx : mx;  // the reference loops jc = 1..mx for idir = 0
+            const int n = along * nb * meqn;
+            for (int k = lane; k < n; k += 32) {
+                const int m = k / (along * nb), rem = k - m * along * nb;
+                const int t = rem / nb + 1, b = rem % nb + 1;
+                int ic, jc;
+                if (idir == 0) { jc = t; ic = (op.face == 0) ? b : mx - b + 1; }
+                else { ic = t; jc = (op.face == 2) ? b : my - b + 1; }
+                const int fi = 2 * ic + op.dx, fj = 2 * jc + op.dy;
+                if (fi < 1 - mbc || fi + 1 > mx + mbc || fj < 1 - mbc || fj + 1 > my + mbc) continue;
+                interp_cell(S, D, m, ic, jc, fi, fj);
+            }
+            break;
+        }
+        case OP_INTERP_CORNER: {
+            const int nb = mbc / 2;
+            const int n = nb * nb * meqn;
+            for (int k = lane; k < n; k += 32) {
+                const int m = k / (nb * nb), rem = k - m * nb * nb;
+                const int ibc = rem / nb + 1, jbc = rem % nb + 1;
+                int ic, jc;
+                if (op.face == 0) { ic = ibc; jc = jbc; }
+                else if (op.face == 1) { ic = mx - ibc + 1; jc = jbc; }
+                else if (op.face == 2) { ic = ibc; jc = my - jbc + 1; }
+                else { ic = mx - ibc + 1; jc = my - jbc + 1; }
+                interp_cell(S, D, m, ic, jc, 2 * ic + op.dx, 2 * jc + op.dy);
+            }
+            break;
+        }
+        case OP_PHYSBC: {
+            // Sides in the reference order; each side reads cells the previous side may write.
+            const int nyg = my + 2 * mbc, nxg = mx + 2 * mbc;
+            for (int side = 0; side < 4; ++side) {
+                const int mth = op.mthbc[side];
+                if (mth == 1 || mth == 3) {
+                    const bool xside = side < 2;
+                    const int len = xside ? nyg : nxg;
+                    const int n = meqn * mbc * len;
+                    for (int k = lane; k < n; k += 32) {
+                        const int m = k / (mbc * len), rem = k - m * mbc * len;
+                        const int bc = rem / len + 1, t = rem % len + (1 - mbc);
+                        if (side == 0) {
+                            double v = (mth == 1) ? D.at(1, t, m) : D.at(bc, t, m);
+                            if (mth == 3 && m == 1) v = -v;
+                            D.at(1 - bc, t, m) = v;
+                        } else if (side == 1) {
+                            double v = (mth == 1) ? D.at(mx, t, m) : D.at(mx + 1 - bc, t, m);
+                            if (mth == 3 && m == 1) v = -v;
+                            D.at(mx + bc, t, m) = v;
+                        } else if (side == 2) {
+                            double v = (mth == 1) ? D.at(t, 1, m) : D.at(t, bc, m);
+                            if (mth == 3 && m == 2) v = -v;
+                            D.at(t, 1 - bc, m) = v;
+                        } else {
+                            double v = (mth == 1) ? D.at(t, my, m) : D.at(t, my + 1 - bc, m);
+                            if (mth == 3 && m == 2) v = -v;
+                            D.at(t, my + bc, m) = v;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            break;
+        }
+        default: break;
+    }
+}
+
+cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st) {
+    if (a.nops <= 0) return cudaSuccess;
+    const int tpb = 256;
+    const int blocks = (a.nops * 32 + tpb - 1) / tpb;
+    ghost_wave_kernel<<<blocks, tpb, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Time interpolation on the interior band of width mbc (the four strips in the
+// reference's order; every strip cell is written once, so order is free).
+// ---------------------------------------------------------------------------
+__global__ void timeinterp_kernel(double* q, const double* qlast, double* qti, int64_t stride,
+                                  const int32_t* slots, int n, int mx, int my, int mbc, int meqn,
+                                  double alpha) {
+    const int p = blockIdx.x;
+    if (p >= n) return;
+    const int64_t base = (int64_t)slots[p] * stride;
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    const int mint = mbc;
+    const int total = meqn * mx * my;
+    for (int k = threadIdx.x; k < total; k += blockDim.x) {
+        const int m = k / (mx * my), rem = k - m * mx * my;
+        const int j = rem / mx + 1, i = rem % mx + 1;
+        const bool in_band = (i <= mint) || (i > mx - mint) || (j <= mint) || (j > my - mint);
+        if (!in_band) continue;
+        const int64_t idx = base + ((int64_t)m * ny + (j + mbc - 1)) * nx + (i + mbc - 1);
+        qti[idx] = qlast[idx] + alpha * (q[idx] - qlast[idx]);
+    }
+}
+
+cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64_t stride,
+                              const int32_t* slots, int n, int mx, int my, int mbc, int meqn,
+                              double alpha, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    timeinterp_kernel<<<n, 128, 0, st>>>(q, qlast, qti, stride, slots, n, mx, my, mbc, meqn, alpha);
+    return cudaGetLastError();
+}
+
+}  // namespace fcb

@@ -1,0 +1,960 @@
+// Host runtime: forest management, slot arena, ghost plans and the level
+// schedule of ForestClaw's time-stepping core on one GPU.
+#include "fcb_runtime.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <unordered_map>
+
+namespace fcb {
+
+template <class T>
+void DevBuf<T>::reserve(size_t n) {
+    if (n <= cap) return;
+    size_t nc = std::max(n, cap + cap / 2);
+    T* np = nullptr;
+    if (cudaMalloc(&np, nc * sizeof(T)) != cudaSuccess) throw Error(FCB_ERR_CUDA, "cudaMalloc failed (DevBuf)");
+    if (p) {
+        cudaDeviceSynchronize();
+        cudaFree(p);
+    }
+    p = np;
+    cap = nc;
+}
+template <class T>
+void DevBuf<T>::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+template struct DevBuf<int32_t>;
+template struct DevBuf<GhostOp>;
+
+void Context::check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Error(FCB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static int solver_meqn(int kind) {
+    switch (kind) {
+        case FCB_SOLVER_ADVECTION: return 1;
+        case FCB_SOLVER_SWE_ROE: return 3;
+        case FCB_SOLVER_EULER4_ROE: return 4;
+        default: return -1;
+    }
+}
+
+Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
+    auto bad = [](const std::string& m) { throw Error(FCB_ERR_INVALID, m); };
+    if (opt_.mx != opt_.my) bad("mx must equal my");
+    if (opt_.mbc != 2) bad("mbc must be 2");
+    if (opt_.mx != 8 && opt_.mx != 16 && opt_.mx != 32 && opt_.mx != 64) bad("mx must be 8, 16, 32 or 64");
+    if (opt_.mcapa > 0) bad("capacity (mcapa > 0) is not supported on this path");
+    if (solver_meqn(opt_.solver_kind) < 0) bad("unknown solver kind");
+    if (opt_.meqn != solver_meqn(opt_.solver_kind)) bad("meqn does not match the solver");
+    if (opt_.mwaves != opt_.meqn) bad("mwaves must equal meqn for the configured solvers");
+    for (int k = 0; k < 4; ++k)
+        if (opt_.mthbc[k] != 1 && opt_.mthbc[k] != 3) bad("mthbc must be 1 (extrapolation) or 3 (wall)");
+    if (opt_.minlevel < 0 || opt_.maxlevel < opt_.minlevel || opt_.maxlevel > 20) bad("bad minlevel/maxlevel");
+    if (opt_.threshold_variable < 1 || opt_.threshold_variable > opt_.meqn) bad("bad threshold_variable");
+    if (opt_.problem == FCB_PROBLEM_SWIRL && opt_.solver_kind != FCB_SOLVER_ADVECTION) bad("swirl needs advection");
+    if (opt_.solver_kind == FCB_SOLVER_ADVECTION && opt_.problem != FCB_PROBLEM_SWIRL)
+        bad("the advection solver takes its velocities from the swirl stream function");
+    if (opt_.problem == FCB_PROBLEM_RADIALDAM && opt_.solver_kind != FCB_SOLVER_SWE_ROE) bad("radialdam needs SWE");
+    if (opt_.problem == FCB_PROBLEM_QUADRANTS && opt_.solver_kind != FCB_SOLVER_EULER4_ROE) bad("quadrants needs Euler");
+    aux_kind_ = (opt_.solver_kind == FCB_SOLVER_ADVECTION) ? AUX_SWIRL : AUX_NONE;
+    nx_ = opt_.mx + 2 * opt_.mbc;
+    ny_ = opt_.my + 2 * opt_.mbc;
+    const int64_t ps = (int64_t)opt_.meqn * nx_ * ny_;
+    stride_ = (ps + 31) / 32 * 32;  // 256-byte aligned slots
+    check(cudaMalloc(&d_cfl_, 4 * sizeof(unsigned long long)), "cudaMalloc cfl");
+}
+
+Context::~Context() {
+    cudaStreamSynchronize(st_);
+    cudaFree(d_q_);
+    cudaFree(d_qlast_);
+    cudaFree(d_qti_);
+    cudaFree(d_qsave_);
+    cudaFree(d_meta_);
+    cudaFree(d_cfl_);
+    cudaFree(d_scratch_);
+    cudaFree(d_stage_);
+}
+
+void Context::synchronize() { check(cudaStreamSynchronize(st_), "cudaStreamSynchronize"); }
+
+void Context::ensure_capacity(int n) {
+    if (n <= capacity_) return;
+    const int nc = std::max({n, capacity_ + capacity_ / 2, 64});
+    const size_t bytes = (size_t)nc * stride_ * sizeof(double);
+    auto grow = [&](double*& p) {
+        double* np = nullptr;
+        check(cudaMalloc(&np, bytes), "cudaMalloc arena");
+        check(cudaMemsetAsync(np, 0, bytes, st_), "cudaMemset arena");
+        if (p) {
+            check(cudaMemcpyAsync(np, p, (size_t)capacity_ * stride_ * sizeof(double), cudaMemcpyDeviceToDevice, st_),
+                  "arena copy");
+            check(cudaStreamSynchronize(st_), "sync");
+            cudaFree(p);
+        }
+        p = np;
+    };
+    grow(d_q_);
+    grow(d_qlast_);
+    grow(d_qti_);
+    if (!opt_.use_fixed_dt) grow(d_qsave_);
+    PatchMeta* nm = nullptr;
+    check(cudaMalloc(&nm, (size_t)nc * sizeof(PatchMeta)), "cudaMalloc meta");
+    if (d_meta_) {
+        check(cudaMemcpyAsync(nm, d_meta_, (size_t)capacity_ * sizeof(PatchMeta), cudaMemcpyDeviceToDevice, st_), "meta");
+        check(cudaStreamSynchronize(st_), "sync");
+        cudaFree(d_meta_);
+    }
+    d_meta_ = nm;
+    capacity_ = nc;
+}
+
+int Context::alloc_slot() {
+    if (!free_slots_.empty()) {
+        const int s = free_slots_.back();
+        free_slots_.pop_back();
+        return s;
+    }
+    return nslots_used_++;
+}
+
+PatchMeta Context::meta_of(const Leaf& l) const {
+    // fclaw2d_clawpatch.cpp clawpatch_define: xlower = ax + (bx-ax)*patch->xlower, dx = (xupper-xlower)/mx
+    const double R = (double)QuadForest::kRoot;
+    const double xl = (double)l.x / R, yl = (double)l.y / R;
+    const double xu = (double)(l.x + QuadForest::width(l.level)) / R;
+    const double yu = (double)(l.y + QuadForest::width(l.level)) / R;
+    const double ax = 0.0, bx = 1.0, ay = 0.0, by = 1.0;
+    PatchMeta m;
+    m.xlower = ax + (bx - ax) * xl;
+    m.ylower = ay + (by - ay) * yl;
+    m.dx = ((ax + (bx - ax) * xu) - m.xlower) / opt_.mx;
+    m.dy = ((ay + (by - ay) * yu) - m.ylower) / opt_.my;
+    m.level = l.level;
+    m.flags = 0;
+    return m;
+}
+
+void Context::mesh_changed() {
+    const int n = num_patches();
+    nbrs_.resize(n);
+    for (int p = 0; p < n; ++p) nbrs_[p] = forest_.neighbors(p);
+    // slot metadata
+    std::vector<PatchMeta> hm((size_t)capacity_);
+    check(cudaStreamSynchronize(st_), "sync");
+    for (int p = 0; p < n; ++p) {
+        PatchMeta m = meta_of(forest_.leaves[p]);
+        if (nbrs_[p].has_fine) m.flags |= PATCH_SAVE_LAST;
+        hm[slot_of_[p]] = m;
+    }
+    check(cudaMemcpy(d_meta_, hm.data(), (size_t)capacity_ * sizeof(PatchMeta), cudaMemcpyHostToDevice), "meta upload");
+    // level lists in Morton order
+    const int L = QuadForest::kMaxLevel + 2;
+    level_begin_.assign(L + 1, 0);
+    ti_begin_.assign(L + 1, 0);
+    std::vector<std::vector<int32_t>> by(L), tby(L);
+    for (int p = 0; p < n; ++p) {
+        by[forest_.leaves[p].level].push_back(slot_of_[p]);
+        if (nbrs_[p].has_fine) tby[forest_.leaves[p].level].push_back(slot_of_[p]);
+    }
+    h_level_slots_.clear();
+    std::vector<int32_t> tis;
+    for (int l = 0; l < L; ++l) {
+        level_begin_[l] = (int)h_level_slots_.size();
+        h_level_slots_.insert(h_level_slots_.end(), by[l].begin(), by[l].end());
+        ti_begin_[l] = (int)tis.size();
+        tis.insert(tis.end(), tby[l].begin(), tby[l].end());
+    }
+    level_begin_[L] = (int)h_level_slots_.size();
+    ti_begin_[L] = (int)tis.size();
+    d_level_slots_.reserve(std::max<size_t>(1, h_level_slots_.size()));
+    d_ti_slots_.reserve(std::max<size_t>(1, tis.size()));
+    d_all_slots_.reserve(std::max(1, n));
+    check(cudaMemcpy(d_level_slots_.p, h_level_slots_.data(), h_level_slots_.size() * 4, cudaMemcpyHostToDevice), "levels");
+    if (!tis.empty()) check(cudaMemcpy(d_ti_slots_.p, tis.data(), tis.size() * 4, cudaMemcpyHostToDevice), "ti");
+    std::vector<int32_t> all(slot_of_.begin(), slot_of_.end());
+    check(cudaMemcpy(d_all_slots_.p, all.data(), all.size() * 4, cudaMemcpyHostToDevice), "all slots");
+    plans_.clear();
+    h_ops_.clear();
+    ops_dirty_ = true;
+}
+
+// ---------------------------------------------------------------------------
+// Ghost plans
+// ---------------------------------------------------------------------------
+namespace {
+struct Rect {
+    int i0, i1, j0, j1;
+    bool hits(const Rect& o) const { return i0 <= o.i1 && o.i0 <= i1 && j0 <= o.j1 && o.j0 <= j1; }
+};
+struct Touch {
+    int64_t key;  // slot * 2 + time-interp array
+    Rect r;
+    bool write;
+};
+}  // namespace
+
+// fclaw2d_ghost_update_async (src/fclaw2d_ghost_fill.c:611-831) on one rank:
+// the records are emitted in the order the reference's callbacks run.
+void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>& ops) {
+    const int mx = opt_.mx, my = opt_.my;
+    const int n = num_patches();
+    std::vector<std::vector<int>> at((size_t)QuadForest::kMaxLevel + 1);
+    for (int p = 0; p < n; ++p) at[forest_.leaves[p].level].push_back(p);
+    auto level_list = [&](int l) -> const std::vector<int>& {
+        static const std::vector<int> empty;
+        return (l < 0 || l > QuadForest::kMaxLevel) ? empty : at[l];
+    };
+    auto xl = [&](int p) { return (double)forest_.leaves[p].x / (double)QuadForest::kRoot; };
+    auto yl = [&](int p) { return (double)forest_.leaves[p].y / (double)QuadForest::kRoot; };
+    auto base = [&](int type, int dst, int src, int face, int dti, int sti) {
+        GhostOp o{};
+        o.type = type; o.dst = dst; o.src = src; o.face = face; o.dst_ti = dti; o.src_ti = sti;
+        for (int k = 0; k < 4; ++k) o.mthbc[k] = -1;
+        return o;
+    };
+    // copy2ghost (fclaw2d_ghost_fill.c:145-168)
+    auto copy2ghost = [&](int level, int t) {
+        const double iw = (double)(1 << level);
+        for (int p : level_list(level))
+            for (int f = 0; f < 4; ++f) {
+                if (nbrs_[p].face_rel[f] != REL_SAMESIZE) continue;
+                const int q = nbrs_[p].face_nbr[f][0];
+                GhostOp o = base(OP_COPY_FACE, slot_of_[p], slot_of_[q], f, t, t);
+                o.dx = (int)((xl(p) - xl(q)) * iw * (double)mx);
+                o.dy = (int)((yl(p) - yl(q)) * iw * (double)my);
+                ops.push_back(o);
+            }
+        for (int p : level_list(level))
+            for (int c = 0; c < 4; ++c) {
+                if (nbrs_[p].corner_rel[c] != REL_SAMESIZE) continue;
+                const int q = nbrs_[p].corner_nbr[c];
+                GhostOp o = base(OP_COPY_CORNER, slot_of_[p], slot_of_[q], c, t, t);
+                o.dx = (int)((xl(p) - xl(q) + 0.) * (iw * (double)mx));
+                o.dy = (int)((yl(p) - yl(q) + 0.) * (iw * (double)my));
+                ops.push_back(o);
+            }
+    };
+    // half-size transform offset D: fine index = 2*coarse + D
+    auto half = [&](int c, int f, int& Dx, int& Dy) {
+        const double ow = (double)(1 << forest_.leaves[f].level);
+        Dx = (int)((xl(c) - xl(f)) * ow * (double)mx) - 1;
+        Dy = (int)((yl(c) - yl(f)) * ow * (double)my) - 1;
+    };
+    // average2ghost (fclaw2d_ghost_fill.c:171-226), interpolate2ghost (:228-287)
+    auto coarse_fine = [&](int level, int t, bool average) {
+        for (int p : level_list(level)) {
+            if (!nbrs_[p].on_cf) continue;
+            for (int f = 0; f < 4; ++f) {
+                if (nbrs_[p].face_rel[f] != REL_HALFSIZE) continue;
+                for (int ig = 0; ig < 2; ++ig) {
+                    const int q = nbrs_[p].face_nbr[f][ig];
+                    GhostOp o = average ? base(OP_AVERAGE_FACE, slot_of_[p], slot_of_[q], f, t, 0)
+                                        : base(OP_INTERP_FACE, slot_of_[q], slot_of_[p], f, 0, t);
+                    half(p, q, o.dx, o.dy);
+                    ops.push_back(o);
+                }
+            }
+        }
+        for (int p : level_list(level)) {
+            if (!nbrs_[p].on_cf) continue;
+            for (int c = 0; c < 4; ++c) {
+                if (nbrs_[p].corner_rel[c] != REL_HALFSIZE) continue;
+                const int q = nbrs_[p].corner_nbr[c];
+                GhostOp o = average ? base(OP_AVERAGE_CORNER, slot_of_[p], slot_of_[q], c, t, 0)
+                                    : base(OP_INTERP_CORNER, slot_of_[q], slot_of_[p], c, 0, t);
+                half(p, q, o.dx, o.dy);
+                ops.push_back(o);
+            }
+        }
+    };
+    // setphysical (fclaw2d_ghost_fill.c:290-308) -> clawpack46_bc2
+    auto setphysical = [&](int level, int t) {
+        for (int p : level_list(level)) {
+            GhostOp o = base(OP_PHYSBC, slot_of_[p], slot_of_[p], 0, t, t);
+            bool any = false;
+            for (int f = 0; f < 4; ++f)
+                if (nbrs_[p].face_rel[f] == REL_BOUNDARY) { o.mthbc[f] = opt_.mthbc[f]; any = true; }
+            if (any) ops.push_back(o);
+        }
+    };
+    const int mincoarse = minlevel, maxcoarse = maxlevel - 1;
+    for (int l = maxcoarse; l >= mincoarse; --l) coarse_fine(l, 0, true);
+    if (ti) coarse_fine(mincoarse - 1, 1, true);
+    for (int l = maxlevel; l >= minlevel; --l) copy2ghost(l, 0);
+    if (ti) copy2ghost(minlevel - 1, 1);
+    for (int l = maxcoarse; l >= mincoarse; --l) setphysical(l, 0);
+    if (ti) setphysical(mincoarse - 1, 1);
+    for (int l = maxcoarse; l >= mincoarse; --l) coarse_fine(l, 0, false);
+    if (ti) coarse_fine(mincoarse - 1, 1, false);
+    const int minfine = mincoarse + 1, maxfine = maxlevel;
+    for (int l = maxfine; l >= minfine; --l) setphysical(l, 0);
+    if (ti) setphysical(minfine - 1, 1);
+    for (int l = maxlevel; l >= minlevel; --l) setphysical(l, 0);
+    if (ti) setphysical(minlevel - 1, 1);
+}
+
+const GhostPlan& Context::plan(int minlevel, int maxlevel, int ti) {
+    auto key = std::make_tuple(minlevel, maxlevel, ti);
+    auto it = plans_.find(key);
+    if (it != plans_.end()) return it->second;
+    std::vector<GhostOp> ops;
+    build_ops(minlevel, maxlevel, ti, ops);
+    // Wave of each record: one more than the latest earlier record it
+    // conflicts with (read-after-write, write-after-read, write-after-write).
+    const int mx = opt_.mx, my = opt_.my, mbc = opt_.mbc;
+    const Rect whole{1 - mbc, mx + mbc, 1 - mbc, my + mbc};
+    const Rect interior{1, mx, 1, my};
+    std::vector<int> wave(ops.size(), 0);
+    std::unordered_map<int64_t, std::vector<std::pair<Touch, int>>> seen;
+    auto band = [&](int face) -> Rect {
+        if (face == 0) return {1 - mbc, 0, 1, my};
+        if (face == 1) return {mx + 1, mx + mbc, 1, my};
+        if (face == 2) return {1, mx, 1 - mbc, 0};
+        return {1, mx, my + 1, my + mbc};
+    };
+    auto corner = [&](int c) -> Rect {
+        const int i0 = (c & 1) ? mx + 1 : 1 - mbc, j0 = (c & 2) ? my + 1 : 1 - mbc;
+        return {i0, i0 + mbc - 1, j0, j0 + mbc - 1};
+    };
+    auto shift = [](Rect r, int dx, int dy) { return Rect{r.i0 + dx, r.i1 + dx, r.j0 + dy, r.j1 + dy}; };
+    auto clip = [&](Rect r) {
+        return Rect{std::max(r.i0, whole.i0), std::min(r.i1, whole.i1), std::max(r.j0, whole.j0), std::min(r.j1, whole.j1)};
+    };
+    for (size_t k = 0; k < ops.size(); ++k) {
+        const GhostOp& o = ops[k];
+        std::vector<Touch> t;
+        const int64_t kd = (int64_t)o.dst * 2 + o.dst_ti, ks = (int64_t)o.src * 2 + o.src_ti;
+        switch (o.type) {
+            case OP_COPY_FACE:
+                t.push_back({kd, band(o.face), true});
+                t.push_back({ks, shift(band(o.face), o.dx, o.dy), false});
+                break;
+            case OP_COPY_CORNER:
+                t.push_back({kd, corner(o.face), true});
+                t.push_back({ks, shift(corner(o.face), o.dx, o.dy), false});
+                break;
+            case OP_AVERAGE_FACE:
+            case OP_AVERAGE_CORNER:
+                t.push_back({kd, o.type == OP_AVERAGE_FACE ? band(o.face) : corner(o.face), true});
+                t.push_back({ks, interior, false});
+                break;
+            case OP_INTERP_FACE:
+            case OP_INTERP_CORNER: {
+                // coarse cells read: the coarse band (one cell deep) grown by one
+                Rect cb;
+                if (o.type == OP_INTERP_FACE) {
+                    if (o.face == 0) cb = {1, mbc / 2, 1, mx};
+                    else if (o.face == 1) cb = {mx - mbc / 2 + 1, mx, 1, mx};
+                    else if (o.face == 2) cb = {1, mx, 1, mbc / 2};
+                    else cb = {1, mx, my - mbc / 2 + 1, my};
+                } else {
+                    const int i0 = (o.face & 1) ? mx - mbc / 2 + 1 : 1, j0 = (o.face & 2) ? my - mbc / 2 + 1 : 1;
+                    cb = {i0, i0 + mbc / 2 - 1, j0, j0 + mbc / 2 - 1};
+                }
+                t.push_back({ks, Rect{cb.i0 - 1, cb.i1 + 1, cb.j0 - 1, cb.j1 + 1}, false});
+                t.push_back({kd, clip(Rect{2 * cb.i0 + o.dx, 2 * cb.i1 + o.dx + 1, 2 * cb.j0 + o.dy, 2 * cb.j1 + o.dy + 1}), true});
+                break;
+            }
+            case OP_PHYSBC:
+                t.push_back({kd, whole, true});
+                t.push_back({kd, whole, false});
+                break;
+        }
+        int w = 0;
+        for (const Touch& a : t) {
+            auto f = seen.find(a.key);
+            if (f == seen.end()) continue;
+            for (const auto& pr : f->second) {
+                const Touch& b = pr.first;
+                if ((a.write || b.write) && a.r.hits(b.r)) w = std::max(w, pr.second + 1);
+            }
+        }
+        wave[k] = w;
+        for (const Touch& a : t) seen[a.key].push_back({a, w});
+    }
+    const int nw = ops.empty() ? 0 : *std::max_element(wave.begin(), wave.end()) + 1;
+    GhostPlan g;
+    g.first = h_ops_.size();
+    g.wave_begin.assign(nw + 1, 0);
+    std::vector<int> count(nw, 0);
+    for (int w : wave) ++count[w];
+    for (int w = 0; w < nw; ++w) g.wave_begin[w + 1] = g.wave_begin[w] + count[w];
+    std::vector<GhostOp> sorted(ops.size());
+    std::vector<int> pos(g.wave_begin.begin(), g.wave_begin.end() - (nw ? 1 : 0));
+    for (size_t k = 0; k < ops.size(); ++k) sorted[pos[wave[k]]++] = ops[k];
+    h_ops_.insert(h_ops_.end(), sorted.begin(), sorted.end());
+    ops_dirty_ = true;
+    return plans_.emplace(key, std::move(g)).first->second;
+}
+
+void Context::run_plan(const GhostPlan& g) {
+    if (ops_dirty_) {
+        d_ops_.reserve(std::max<size_t>(1, h_ops_.size()));
+        check(cudaStreamSynchronize(st_), "sync");
+        if (!h_ops_.empty())
+            check(cudaMemcpy(d_ops_.p, h_ops_.data(), h_ops_.size() * sizeof(GhostOp), cudaMemcpyHostToDevice), "ops");
+        ops_dirty_ = false;
+    }
+    const int nw = (int)g.wave_begin.size() - 1;
+    for (int w = 0; w < nw; ++w) {
+        GhostArgs a;
+        a.q = d_q_;
+        a.qti = d_qti_;
+        a.stride = stride_;
+        a.mx = opt_.mx; a.my = opt_.my; a.mbc = opt_.mbc; a.meqn = opt_.meqn;
+        a.ops = d_ops_.p + g.first + g.wave_begin[w];
+        a.nops = g.wave_begin[w + 1] - g.wave_begin[w];
+        check(launch_ghost_wave(a, st_), "ghost wave");
+        ++cnt_.count_ghost_waves;
+        ++cnt_.count_kernel_launches;
+    }
+}
+
+void Context::ghost_update(int minlevel, int maxlevel, double, int time_interp) {
+    if (!d_q_) throw Error(FCB_ERR_STATE, "ghost_update before initialize");
+    run_plan(plan(minlevel, maxlevel, time_interp));
+}
+
+void Context::physical_set_bc(int level, int time_interp) {
+    std::vector<GhostOp> ops;
+    for (int p = 0; p < num_patches(); ++p) {
+        if (forest_.leaves[p].level != level) continue;
+        GhostOp o{};
+        o.type = OP_PHYSBC; o.dst = o.src = slot_of_[p]; o.dst_ti = o.src_ti = time_interp;
+        bool any = false;
+        for (int f = 0; f < 4; ++f) {
+            o.mthbc[f] = -1;
+            if (nbrs_[p].face_rel[f] == REL_BOUNDARY) { o.mthbc[f] = opt_.mthbc[f]; any = true; }
+        }
+        if (any) ops.push_back(o);
+    }
+    if (ops.empty()) return;
+    GhostPlan g;
+    g.first = h_ops_.size();
+    g.wave_begin = {0, (int)ops.size()};
+    h_ops_.insert(h_ops_.end(), ops.begin(), ops.end());
+    ops_dirty_ = true;
+    run_plan(g);
+}
+
+// ---------------------------------------------------------------------------
+// Stepping
+// ---------------------------------------------------------------------------
+void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, double dt,
+                                      unsigned long long* cfl_slot) {
+    if (n <= 0) return;
+    StepArgs a{};
+    a.q = d_q_;
+    a.qlast = d_qlast_;
+    a.aux = nullptr;
+    a.slots = d_slots;
+    a.meta = d_meta_;
+    a.q_stride = stride_;
+    a.aux_stride = 0;
+    a.npatches = n;
+    a.maux = 0;
+    a.order0 = opt_.order[0];
+    a.order1 = opt_.order[1];
+    for (int k = 0; k < 8; ++k) a.mthlim[k] = opt_.mthlim[k];
+    a.dt = dt;
+    if (aux_kind_ == AUX_SWIRL) {
+        // swirl b4step2.f: vt = cos(pi2*(time+dt/2)/tperiod), pi2 = 2*(4*atan(1))
+        const double pi = 4.0 * std::atan(1.0);
+        const double pi2 = 2.0 * pi;
+        const double tperiod = opt_.problem_params[0];
+        a.vt = (tperiod == 0.0) ? 0.0 : std::cos(pi2 * (t + dt / 2.0) / tperiod);
+    }
+    a.grav = opt_.grav;
+    a.gamma = opt_.gamma;
+    a.gamma1 = opt_.gamma - 1.0;
+    a.cfl_out = cfl_slot;
+    check(launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_), "step");
+    cnt_.count_single_step += n;
+    ++cnt_.count_kernel_launches;
+}
+
+double Context::launch_level_step(int level, double t, double dt, unsigned long long* cfl_slot) {
+    if (level < 0 || level > QuadForest::kMaxLevel) return 0.0;
+    const int b = level_begin_[level], e = level_begin_[level + 1];
+    launch_level_step_slots(d_level_slots_.p + b, e - b, t, dt, cfl_slot);
+    return 0.0;
+}
+
+static double cfl_from_bits(unsigned long long b) {
+    double v;
+    std::memcpy(&v, &b, sizeof v);
+    return v;
+}
+
+double Context::update_single_step(int level, double t, double dt) {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "update_single_step before initialize");
+    check(cudaMemsetAsync(d_cfl_ + 1, 0, sizeof(unsigned long long), st_), "memset");
+    launch_level_step(level, t, dt, d_cfl_ + 1);
+    unsigned long long b = 0;
+    check(cudaMemcpyAsync(&b, d_cfl_ + 1, sizeof b, cudaMemcpyDeviceToHost, st_), "cfl");
+    synchronize();
+    return cfl_from_bits(b);
+}
+
+void Context::update_single_step_async(int level, double t, double dt) {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "update_single_step before initialize");
+    launch_level_step(level, t, dt, d_cfl_);
+}
+
+double Context::single_step_update(int patchno, double t, double dt, int iter, int total) {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "single_step_update before initialize");
+    if (patchno < 0 || patchno >= num_patches()) throw Error(FCB_ERR_INVALID, "bad patch number");
+    if (iter == 0) pending_.clear();
+    pending_.push_back(slot_of_[patchno]);
+    if (iter + 1 < total) return 0.0;
+    d_pending_.reserve(pending_.size());
+    check(cudaMemcpyAsync(d_pending_.p, pending_.data(), pending_.size() * 4, cudaMemcpyHostToDevice, st_), "pending");
+    check(cudaMemsetAsync(d_cfl_ + 1, 0, sizeof(unsigned long long), st_), "memset");
+    launch_level_step_slots(d_pending_.p, (int)pending_.size(), t, dt, d_cfl_ + 1);
+    unsigned long long b = 0;
+    check(cudaMemcpyAsync(&b, d_cfl_ + 1, sizeof b, cudaMemcpyDeviceToHost, st_), "cfl");
+    synchronize();
+    pending_.clear();
+    return cfl_from_bits(b);
+}
+
+void Context::timeinterp(int level, double alpha) {
+    if (level < 0 || level > QuadForest::kMaxLevel) return;
+    const int b = ti_begin_[level], e = ti_begin_[level + 1];
+    if (e == b) return;
+    check(launch_timeinterp(d_q_, d_qlast_, d_qti_, stride_, d_ti_slots_.p + b, e - b, opt_.mx, opt_.my, opt_.mbc,
+                            opt_.meqn, alpha, st_),
+          "timeinterp");
+    ++cnt_.count_kernel_launches;
+}
+
+// fclaw2d_advance_all_levels (src/fclaw2d_advance.c:247-357)
+double Context::advance_all_levels(double t_curr, double dt) {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "advance before initialize");
+    const int gmin = forest_.min_level(), gmax = forest_.max_level();
+    struct Counter { int last_step, step_inc, total_steps; double current_time, dt_step; };
+    std::vector<Counter> ts(opt_.maxlevel + 1);
+    for (int l = opt_.minlevel; l <= opt_.maxlevel; ++l) { ts[l].last_step = 0; ts[l].current_time = t_curr; }
+    if (opt_.subcycle) {
+        double dt_level = dt;
+        int steps_inc = 1 << (gmax - opt_.minlevel);
+        int total_steps = 1;
+        for (int l = opt_.minlevel; l <= opt_.maxlevel; ++l) {
+            ts[l].dt_step = dt_level; ts[l].total_steps = total_steps; ts[l].step_inc = steps_inc;
+            dt_level /= 2; steps_inc /= 2; total_steps *= 2;
+        }
+    } else {
+        const int rf = 1 << (opt_.maxlevel - opt_.minlevel);
+        for (int l = opt_.minlevel; l <= opt_.maxlevel; ++l) {
+            ts[l].step_inc = 1; ts[l].dt_step = dt / rf; ts[l].total_steps = rf;
+        }
+    }
+    check(cudaMemsetAsync(d_cfl_, 0, sizeof(unsigned long long), st_), "memset");
+    std::function<void(int, int)> advance_level = [&](int level, int curr_fine_step) {
+        launch_level_step(level, ts[level].current_time, ts[level].dt_step, d_cfl_);
+        ts[level].last_step += ts[level].step_inc;
+        ts[level].current_time += ts[level].dt_step;
+        if (level > gmin) {
+            const int last_coarse_step = ts[level - 1].last_step;
+            if (last_coarse_step == curr_fine_step) {
+                advance_level(level - 1, last_coarse_step);
+                if (opt_.subcycle) {
+                    const int coarse_inc = ts[level - 1].step_inc;
+                    const double alpha = ((double)(ts[level].last_step % coarse_inc)) / coarse_inc;
+                    timeinterp(level - 1, alpha);
+                }
+            }
+        }
+    };
+    const int n_fine = ts[gmax].total_steps;
+    for (int nf = 0; nf < n_fine; ++nf) {
+        advance_level(gmax, nf);
+        const int last_step = ts[gmax].last_step;
+        if (last_step < ts[gmax].total_steps) {
+            const double sync_time = ts[gmax].current_time;
+            if (opt_.subcycle) {
+                int ti_level = gmax - 1;
+                while (last_step % ts[ti_level].step_inc == 0) --ti_level;
+                ghost_update(ti_level + 1, gmax, sync_time, 1);
+            } else {
+                ghost_update(gmin, gmax, sync_time, 0);
+            }
+        }
+    }
+    ghost_update(gmin, gmax, ts[gmax].current_time, 0);
+    ++cnt_.count_amr_advance;
+    unsigned long long b = 0;
+    check(cudaMemcpyAsync(&b, d_cfl_, sizeof b, cudaMemcpyDeviceToHost, st_), "cfl");
+    synchronize();
+    return cfl_from_bits(b);
+}
+
+// ---------------------------------------------------------------------------
+// Regrid
+// ---------------------------------------------------------------------------
+void Context::tag(bool domain_init, std::vector<int>& target) {
+    const int n = num_patches();
+    const size_t need = (size_t)4 * n;
+    if (need > scratch_cap_) {
+        cudaFree(d_scratch_);
+        check(cudaMalloc(&d_scratch_, need * sizeof(double)), "cudaMalloc scratch");
+        scratch_cap_ = need;
+    }
+    TagArgs a{};
+    a.q = d_q_; a.stride = stride_; a.slots = d_all_slots_.p; a.meta = d_meta_;
+    a.n = n; a.mx = opt_.mx; a.my = opt_.my; a.mbc = opt_.mbc; a.ivar = opt_.threshold_variable - 1;
+    a.criteria = opt_.refinement_criteria;
+    a.refine_th = opt_.refine_threshold; a.coarsen_th = opt_.coarsen_threshold;
+    a.out = d_scratch_;
+    check(launch_tag(a, st_), "tag");
+    ++cnt_.count_kernel_launches;
+    std::vector<double> h(need);
+    check(cudaMemcpyAsync(h.data(), d_scratch_, need * sizeof(double), cudaMemcpyDeviceToHost, st_), "tags");
+    synchronize();
+    target.resize(n);
+    for (int p = 0; p < n; ++p) target[p] = forest_.leaves[p].level;
+    const bool minmax = opt_.refinement_criteria == FCB_TAG_MINMAX;
+    // cb_regrid_tag4coarsening over families (fclaw2d_regrid.c:70-97,
+    // clawpatch_tag4coarsening fclaw2d_clawpatch.cpp:860-914)
+    for (int p = 0; p < n; ++p) {
+        if (!forest_.is_first_sibling(p)) continue;
+        const int level = forest_.leaves[p].level;
+        if (level > opt_.minlevel && opt_.coarsen_threshold > 0 && !domain_init) {
+            bool keep;
+            if (minmax) {
+                double lo = h[4 * p], hi = h[4 * p + 1];
+                for (int k = 1; k < 4; ++k) { lo = std::min(lo, h[4 * (p + k)]); hi = std::max(hi, h[4 * (p + k) + 1]); }
+                keep = (hi - lo > opt_.coarsen_threshold);
+            } else {
+                keep = false;
+                for (int k = 0; k < 4; ++k) keep = keep || h[4 * (p + k) + 3] != 0.0;
+            }
+            if (!keep)
+                for (int k = 0; k < 4; ++k) target[p + k] = std::max(forest_.leaves[p + k].level - 1, 0);
+        }
+        p += 3;
+    }
+    // cb_fclaw2d_regrid_tag4refinement (fclaw2d_regrid.c:45-67)
+    for (int p = 0; p < n; ++p) {
+        const int level = forest_.leaves[p].level;
+        if (level >= opt_.maxlevel) continue;
+        bool refine;
+        if (opt_.refine_threshold < 0) refine = true;
+        else if (minmax) refine = (h[4 * p + 1] - h[4 * p] > opt_.refine_threshold);
+        else refine = h[4 * p + 2] != 0.0;
+        if (refine) target[p] = level + 1;
+    }
+}
+
+// fclaw2d_domain_adapt (fclaw2d_convenience.c:498-680) + p4est_wrap_adapt:
+// refine marked leaves once, coarsen complete marked families, balance.
+bool Context::adapt(const std::vector<int>& target, std::vector<Leaf>& out) {
+    const int n = num_patches();
+    enum { REFINE = 1, COARSEN = 2 };
+    std::vector<int> flag(n, 0);
+    auto refine = [&](int p) { flag[p] = REFINE; };
+    auto coarsen = [&](int p) { flag[p] = forest_.leaves[p].level > 0 ? COARSEN : 0; };
+    for (int p = 0; p < n; ++p) {
+        const int level = forest_.leaves[p].level;
+        int t = target[p];
+        if (opt_.smooth_refine) {
+            const Neighbors& nb = nbrs_[p];
+            auto consider = [&](int q) {
+                if (forest_.leaves[q].level >= opt_.smooth_level) t = std::max(t, target[q]);
+            };
+            for (int f = 0; t <= level && f < 4; ++f) {
+                if (nb.face_rel[f] == REL_SAMESIZE || nb.face_rel[f] == REL_DOUBLESIZE) consider(nb.face_nbr[f][0]);
+                else if (nb.face_rel[f] == REL_HALFSIZE) { consider(nb.face_nbr[f][0]); consider(nb.face_nbr[f][1]); }
+            }
+            for (int c = 0; t <= level && c < 4; ++c)
+                if (nb.corner_rel[c] != 0) consider(nb.corner_nbr[c]);
+        }
+        if (t > level) refine(p);
+        else if (t < level) coarsen(p);
+    }
+    bool changed = false;
+    std::vector<Leaf> r;
+    std::vector<int> rf;
+    r.reserve(n);
+    for (int p = 0; p < n; ++p) {
+        const Leaf& l = forest_.leaves[p];
+        if (flag[p] == REFINE) {
+            changed = true;
+            const int32_t hh = QuadForest::width(l.level + 1);
+            for (int k = 0; k < 4; ++k) {
+                r.push_back(QuadForest::make(l.level + 1, l.x + (k & 1) * hh, l.y + (k >> 1) * hh));
+                rf.push_back(0);
+            }
+        } else {
+            r.push_back(l);
+            rf.push_back(flag[p]);
+        }
+    }
+    QuadForest tmp;
+    tmp.leaves = r;
+    std::vector<Leaf> c;
+    c.reserve(r.size());
+    for (size_t p = 0; p < r.size();) {
+        if (tmp.is_first_sibling((int)p) && rf[p] == COARSEN && rf[p + 1] == COARSEN && rf[p + 2] == COARSEN &&
+            rf[p + 3] == COARSEN) {
+            c.push_back(QuadForest::make(r[p].level - 1, r[p].x, r[p].y));
+            changed = true;
+            p += 4;
+        } else {
+            c.push_back(r[p]);
+            ++p;
+        }
+    }
+    if (!changed) return false;
+    QuadForest f;
+    f.leaves = c;
+    f.balance();
+    out = f.leaves;
+    return true;
+}
+
+void Context::qinit_slots(const std::vector<int32_t>& slots) {
+    if (slots.empty()) return;
+    DevBuf<int32_t> d;
+    d.reserve(slots.size());
+    check(cudaMemcpy(d.p, slots.data(), slots.size() * 4, cudaMemcpyHostToDevice), "qinit slots");
+    QinitArgs a{};
+    a.q = d_q_; a.stride = stride_; a.slots = d.p; a.meta = d_meta_;
+    a.n = (int)slots.size(); a.mx = opt_.mx; a.my = opt_.my; a.mbc = opt_.mbc; a.meqn = opt_.meqn;
+    a.problem = opt_.problem; a.gamma1 = opt_.gamma - 1.0;
+    for (int k = 0; k < 32; ++k) a.p[k] = opt_.problem_params[k];
+    check(launch_qinit(a, st_), "qinit");
+    ++cnt_.count_kernel_launches;
+    synchronize();
+}
+
+// fclaw2d_domain_iterate_adapted + cb_fclaw2d_regrid_repopulate (fclaw2d_regrid.c:114-230)
+void Context::repopulate(const std::vector<Leaf>& old_leaves, const std::vector<int>& old_slots,
+                         bool domain_init) {
+    const int nn = num_patches();
+    std::vector<int> ns(nn, -1);
+    std::vector<int32_t> transfer, fine, fresh, freed;
+    int oj = 0, nj = 0;
+    // pass 1: assign slots (new slots never reuse a slot freed in this regrid)
+    std::vector<std::tuple<int, int, int>> events;  // kind, oj, nj
+    while (oj < (int)old_leaves.size()) {
+        const Leaf& o = old_leaves[oj];
+        const Leaf& w = forest_.leaves[nj];
+        if (o.level < w.level) { events.emplace_back(0, oj, nj); oj += 1; nj += 4; }
+        else if (o.level > w.level) { events.emplace_back(1, oj, nj); oj += 4; nj += 1; }
+        else { ns[nj] = old_slots[oj]; oj += 1; nj += 1; }
+    }
+    if (nj != nn) throw Error(FCB_ERR_INTERNAL, "iterate_adapted: leaf count mismatch");
+    int need = nslots_used_;
+    for (auto& e : events) need += (std::get<0>(e) == 0) ? 4 : 1;
+    ensure_capacity(need);
+    std::vector<int> saved_free = free_slots_;
+    free_slots_.clear();  // allocate only fresh slots in this pass
+    for (auto& e : events) {
+        const int kind = std::get<0>(e), o = std::get<1>(e), w = std::get<2>(e);
+        if (kind == 0) {
+            const int f0 = (int)fine.size();
+            for (int k = 0; k < 4; ++k) { ns[w + k] = alloc_slot(); fine.push_back(ns[w + k]); fresh.push_back(ns[w + k]); }
+            transfer.insert(transfer.end(), {0, old_slots[o], f0});
+            freed.push_back(old_slots[o]);
+        } else {
+            ns[w] = alloc_slot();
+            fresh.push_back(ns[w]);
+            const int f0 = (int)fine.size();
+            for (int k = 0; k < 4; ++k) { fine.push_back(old_slots[o + k]); freed.push_back(old_slots[o + k]); }
+            transfer.insert(transfer.end(), {1, ns[w], f0});
+        }
+    }
+    slot_of_ = ns;
+    // metadata of the new mesh is needed by qinit; transfers only need slots
+    if (domain_init) {
+        mesh_changed();
+        qinit_slots(fresh);
+    } else if (!transfer.empty()) {
+        DevBuf<int32_t> dt, df;
+        dt.reserve(transfer.size());
+        df.reserve(fine.size());
+        check(cudaMemcpy(dt.p, transfer.data(), transfer.size() * 4, cudaMemcpyHostToDevice), "transfer");
+        check(cudaMemcpy(df.p, fine.data(), fine.size() * 4, cudaMemcpyHostToDevice), "fine");
+        check(launch_regrid(d_q_, stride_, dt.p, df.p, (int)transfer.size() / 3, opt_.mx, opt_.my, opt_.mbc,
+                            opt_.meqn, st_),
+              "regrid transfer");
+        ++cnt_.count_kernel_launches;
+        synchronize();
+    }
+    free_slots_ = saved_free;
+    free_slots_.insert(free_slots_.end(), freed.begin(), freed.end());
+}
+
+bool Context::regrid() {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "regrid before initialize");
+    std::vector<int> target;
+    tag(false, target);
+    std::vector<Leaf> nl;
+    const bool changed = adapt(target, nl);
+    if (changed) {
+        const std::vector<Leaf> old = forest_.leaves;
+        const std::vector<int> old_slots = slot_of_;
+        forest_.leaves = nl;
+        repopulate(old, old_slots, false);
+        mesh_changed();
+        ghost_update(forest_.min_level(), forest_.max_level(), curr_time_, 0);
+        ++cnt_.count_amr_new_domain;
+    }
+    ++cnt_.count_amr_regrid;
+    return changed;
+}
+
+// fclaw2d_initialize (src/fclaw2d_initialize.c:75-248)
+void Context::initialize() {
+    forest_.uniform(opt_.minlevel);
+    const int n = num_patches();
+    free_slots_.clear();
+    nslots_used_ = 0;
+    ensure_capacity(n);
+    slot_of_.resize(n);
+    for (int p = 0; p < n; ++p) slot_of_[p] = alloc_slot();
+    mesh_changed();
+    qinit_slots(std::vector<int32_t>(slot_of_.begin(), slot_of_.end()));
+    initialized_ = true;
+    if (opt_.init_ghostcell) ghost_update(forest_.min_level(), forest_.max_level(), 0.0, 0);
+    if (opt_.minlevel < opt_.maxlevel) {
+        for (int level = opt_.minlevel; level <= opt_.maxlevel; ++level) {
+            std::vector<int> target;
+            tag(true, target);
+            std::vector<Leaf> nl;
+            if (!adapt(target, nl)) break;
+            const std::vector<Leaf> old = forest_.leaves;
+            const std::vector<int> old_slots = slot_of_;
+            forest_.leaves = nl;
+            repopulate(old, old_slots, true);
+            mesh_changed();
+        }
+    }
+    if (opt_.init_ghostcell) ghost_update(forest_.min_level(), forest_.max_level(), 0.0, 0);
+    synchronize();
+}
+
+// outstyle_1 (src/fclaw2d_run.c:120-290)
+void Context::run() {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "run before initialize");
+    const double final_time = opt_.tfinal;
+    const int nout = opt_.nout;
+    double dt_minlevel = opt_.initial_dt;
+    const double t0 = 0;
+    const double dt_outer = (final_time - t0) / ((double)nout);
+    double t_curr = t0;
+    int n_inner = 0;
+    const size_t arena_bytes = (size_t)capacity_ * stride_ * sizeof(double);
+    for (int n = 0; n < nout; ++n) {
+        const double tstart = t_curr;
+        curr_time_ = t_curr;
+        const double tend = tstart + dt_outer;
+        while (t_curr < tend) {
+            const size_t bytes = (size_t)capacity_ * stride_ * sizeof(double);
+            (void)arena_bytes;
+            if (!opt_.use_fixed_dt)
+                check(cudaMemcpyAsync(d_qsave_, d_q_, bytes, cudaMemcpyDeviceToDevice, st_), "save_time_step");
+            double dt_step = dt_minlevel;
+            const double tol = 1e-2 * dt_step;
+            int took_small_step = 0;
+            if (!opt_.use_fixed_dt) {
+                const double small_step = tend - (t_curr + dt_step);
+                if (small_step < tol) {
+                    dt_step = tend - t_curr;
+                    if (small_step < 0) took_small_step = 1;
+                }
+            }
+            const double maxcfl_step = advance_all_levels(t_curr, dt_step);
+            if (std::isnan(maxcfl_step)) throw Error(FCB_ERR_NUMERIC, "NaN in the CFL number");
+            if ((maxcfl_step > opt_.max_cfl) && opt_.reduce_cfl) {
+                if (!opt_.use_fixed_dt) {
+                    check(cudaMemcpyAsync(d_q_, d_qsave_, bytes, cudaMemcpyDeviceToDevice, st_), "restore_time_step");
+                    dt_minlevel = dt_minlevel * opt_.desired_cfl / maxcfl_step;
+                    continue;
+                }
+            }
+            ++n_inner;
+            t_curr += dt_step;
+            if (!opt_.use_fixed_dt) {
+                const double dt_new = dt_minlevel * opt_.desired_cfl / maxcfl_step;
+                if (!took_small_step) dt_minlevel = dt_new;
+            }
+            curr_time_ = t_curr;
+            if (opt_.regrid_interval > 0 && n_inner % opt_.regrid_interval == 0) regrid();
+        }
+        curr_time_ = t_curr;
+    }
+    synchronize();
+}
+
+// ---------------------------------------------------------------------------
+// Data movement and diagnostics
+// ---------------------------------------------------------------------------
+void Context::get_q(double* host, size_t n, bool qinterp) {
+    const size_t ps = patch_size();
+    const size_t total = ps * num_patches();
+    if (n < total) throw Error(FCB_ERR_INVALID, "host buffer too small");
+    if (total > stage_cap_) {
+        cudaFree(d_stage_);
+        check(cudaMalloc(&d_stage_, total * sizeof(double)), "cudaMalloc stage");
+        stage_cap_ = total;
+    }
+    check(launch_gather(qinterp ? d_qti_ : d_q_, stride_, d_all_slots_.p, num_patches(), (int64_t)ps, d_stage_,
+                        false, st_),
+          "gather");
+    ++cnt_.count_kernel_launches;
+    check(cudaMemcpyAsync(host, d_stage_, total * sizeof(double), cudaMemcpyDeviceToHost, st_), "get_q");
+    synchronize();
+}
+
+void Context::set_q(const double* host, size_t n) {
+    const size_t ps = patch_size();
+    const size_t total = ps * num_patches();
+    if (n < total) throw Error(FCB_ERR_INVALID, "host buffer too small");
+    if (total > stage_cap_) {
+        cudaFree(d_stage_);
+        check(cudaMalloc(&d_stage_, total * sizeof(double)), "cudaMalloc stage");
+        stage_cap_ = total;
+    }
+    check(cudaMemcpyAsync(d_stage_, host, total * sizeof(double), cudaMemcpyHostToDevice, st_), "set_q");
+    check(launch_gather(d_q_, stride_, d_all_slots_.p, num_patches(), (int64_t)ps, d_stage_, true, st_), "scatter");
+    ++cnt_.count_kernel_launches;
+    synchronize();
+}
+
+void Context::conservation(double* sums) {
+    const int n = num_patches();
+    const size_t need = (size_t)n * opt_.meqn;
+    if (need > scratch_cap_) {
+        cudaFree(d_scratch_);
+        check(cudaMalloc(&d_scratch_, need * sizeof(double)), "cudaMalloc scratch");
+        scratch_cap_ = need;
+    }
+    check(launch_mass(d_q_, stride_, d_all_slots_.p, d_meta_, n, opt_.mx, opt_.my, opt_.mbc, opt_.meqn, d_scratch_, st_),
+          "mass");
+    ++cnt_.count_kernel_launches;
+    std::vector<double> h(need);
+    check(cudaMemcpyAsync(h.data(), d_scratch_, need * sizeof(double), cudaMemcpyDeviceToHost, st_), "mass");
+    synchronize();
+    for (int m = 0; m < opt_.meqn; ++m) {
+        double s = 0.0, c = 0.0;
+        for (int p = 0; p < n; ++p) {
+            const double y = h[(size_t)p * opt_.meqn + m] - c;
+            const double t = s + y;
+            c = (t - s) - y;
+            s = t;
+        }
+        sums[m] = s;
+    }
+}
+
+}  // namespace fcb

@@ -1,0 +1,151 @@
+// Host runtime of one solve: options, forest, device arena, ghost-operation
+// lists and the level schedule.  All device work is enqueued on one stream.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/fclaw_b200.h"
+#include "fcb_device.h"
+#include "fcb_forest.hpp"
+
+namespace fcb {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// Kernel launchers (fcb_step.cu, fcb_ghost.cu, fcb_amr.cu)
+cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
+                        cudaStream_t st);
+struct GhostArgs;
+cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st);
+cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64_t stride,
+                              const int32_t* slots, int n, int mx, int my, int mbc, int meqn,
+                              double alpha, cudaStream_t st);
+struct QinitArgs;
+cudaError_t launch_qinit(const QinitArgs& a, cudaStream_t st);
+struct TagArgs;
+cudaError_t launch_tag(const TagArgs& a, cudaStream_t st);
+cudaError_t launch_regrid(double* q, int64_t stride, const int32_t* ops, const int32_t* fine, int nops,
+                          int mx, int my, int mbc, int meqn, cudaStream_t st);
+// scatter == false: dst[p] = src[slots[p]]; scatter == true: src[slots[p]] = dst[p]
+cudaError_t launch_gather(const double* src, int64_t stride, const int32_t* slots, int n, int64_t psize,
+                          double* dst, bool scatter, cudaStream_t st);
+cudaError_t launch_mass(const double* q, int64_t stride, const int32_t* slots, const PatchMeta* meta, int n,
+                        int mx, int my, int mbc, int meqn, double* out, cudaStream_t st);
+
+// A device buffer that only grows.
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    void reserve(size_t n);
+    void release();
+    ~DevBuf() { release(); }
+};
+
+struct GhostPlan {
+    std::vector<int> wave_begin;  // op offsets of each wave, size nwaves+1
+    size_t first = 0;             // first op of the plan in the context's op buffer
+};
+
+class Context {
+  public:
+    Context(const fcb_options_t& o, cudaStream_t st);
+    ~Context();
+
+    void initialize();
+    void run();
+    double advance_all_levels(double t, double dt);
+    double update_single_step(int level, double t, double dt);
+    void update_single_step_async(int level, double t, double dt);
+    double single_step_update(int patchno, double t, double dt, int iter, int total);
+    void ghost_update(int minlevel, int maxlevel, double sync_time, int time_interp);
+    void timeinterp(int level, double alpha);
+    bool regrid();
+    void physical_set_bc(int level, int time_interp);
+
+    int num_patches() const { return (int)forest_.leaves.size(); }
+    const Leaf& leaf(int p) const { return forest_.leaves[p]; }
+    const Neighbors& nbrs(int p) const { return nbrs_[p]; }
+    size_t patch_size() const { return (size_t)opt_.meqn * nx_ * ny_; }
+    void get_q(double* host, size_t n, bool qinterp);
+    void set_q(const double* host, size_t n);
+    void conservation(double* sums);
+    void synchronize();
+    fcb_counters_t counters() const { return cnt_; }
+    double curr_time() const { return curr_time_; }
+
+  private:
+    // --- setup ---
+    void check(cudaError_t e, const char* what);
+    void ensure_capacity(int nslots);
+    int alloc_slot();
+    void mesh_changed();  // rebuild neighbour tables, level lists, metadata; drop ghost plans
+    PatchMeta meta_of(const Leaf& l) const;
+    // --- ghost plans ---
+    const GhostPlan& plan(int minlevel, int maxlevel, int time_interp);
+    void build_ops(int minlevel, int maxlevel, int time_interp, std::vector<GhostOp>& ops);
+    void run_plan(const GhostPlan& g);
+    // --- regrid helpers ---
+    void tag(bool domain_init, std::vector<int>& target);
+    bool adapt(const std::vector<int>& target, std::vector<Leaf>& out);
+    void repopulate(const std::vector<Leaf>& old_leaves, const std::vector<int>& old_slots,
+                    bool domain_init);
+    void qinit_slots(const std::vector<int32_t>& slots);
+    double launch_level_step(int level, double t, double dt, unsigned long long* cfl_slot);
+    void launch_level_step_slots(const int32_t* d_slots, int n, double t, double dt, unsigned long long* cfl_slot);
+
+    fcb_options_t opt_;
+    cudaStream_t st_;
+    int nx_, ny_;
+    int64_t stride_;      // doubles per slot
+    int aux_kind_;
+    QuadForest forest_;
+    std::vector<int> slot_of_;        // per leaf
+    std::vector<Neighbors> nbrs_;     // per leaf
+    std::vector<int> free_slots_;
+    int nslots_used_ = 0;
+    int capacity_ = 0;
+    // device arena
+    double* d_q_ = nullptr;
+    double* d_qlast_ = nullptr;
+    double* d_qti_ = nullptr;
+    double* d_qsave_ = nullptr;
+    PatchMeta* d_meta_ = nullptr;
+    // level lists (device), grouped by level
+    DevBuf<int32_t> d_level_slots_;
+    std::vector<int> level_begin_;    // size maxlevel+2
+    std::vector<int32_t> h_level_slots_;
+    DevBuf<int32_t> d_ti_slots_;      // per level: slots with fine-grid neighbours
+    std::vector<int> ti_begin_;
+    DevBuf<int32_t> d_all_slots_;     // all leaves in Morton order
+    // ghost plans
+    std::map<std::tuple<int, int, int>, GhostPlan> plans_;
+    std::vector<GhostOp> h_ops_;
+    DevBuf<GhostOp> d_ops_;
+    bool ops_dirty_ = true;
+    // scalars
+    unsigned long long* d_cfl_ = nullptr;  // [0]: advance accumulator, [1]: level / batch
+    double* d_scratch_ = nullptr;          // tagging / mass output
+    size_t scratch_cap_ = 0;
+    // per-patch single_step_update batching
+    std::vector<int32_t> pending_;
+    DevBuf<int32_t> d_pending_;
+    // contiguous staging buffer for host transfers
+    double* d_stage_ = nullptr;
+    size_t stage_cap_ = 0;
+    // state
+    bool initialized_ = false;
+    double curr_time_ = 0.0;
+    fcb_counters_t cnt_{};
+};
+
+}  // namespace fcb

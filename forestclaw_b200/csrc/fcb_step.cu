@@ -1,0 +1,518 @@
+// Batched Clawpack 4.6 patch update (step2 + flux2 + conservative update) for
+// sm_100a.  One thread per patch column, several patches per CTA; the patch
+// rows stream through a two-row pipeline so that q is read once and written
+// once per step with no global flux scratch.
+//
+// Reference: src/solvers/fc2d_clawpack4.6/fortran_source/clawpack46_step2_wrap.f
+// (conservative update over i,j = 1-mbc..mx+mbc-1), clawpack46_step2.f (x- and
+// y-sweeps, fm/fp/gm/gp accumulation), clawpack46_flux2.f (Godunov, CFL,
+// limiter, second-order and transverse corrections).
+//
+// Index map: cell (c, r) with c, r in [0, NX) holds Fortran cell
+// (i, j) = (c - mbc + 1, r - mbc + 1).  x-interface c sits between cells c-1
+// and c, y-interface r between rows r-1 and r.  With the reference's loop
+// bounds this gives: x-sweep rows r in [1, NY-2], x-interfaces c in [1, NX-1],
+// Godunov part for c <= NX-2, CFL and limiting for c in [mbc, mbc+mx];
+// y-sweep columns c in [1, NX-2], interfaces r in [1, NY-1]; updated cells
+// c in [0, NX-2], r in [0, NY-2].
+//
+// The flux accumulators are formed in the reference's order:
+//   fm(i,j) = (FXm + GYu[col i-1]) + GYd[col i],   gm(i,j) = (GXu[row j-1] + GXd[row j]) + FYm
+// (absent terms are +0, which leaves every sum unchanged), and
+//   q = q - dtdx*(fm(i+1,j) - fp(i,j)) - dtdy*(gm(i,j+1) - gp(i,j)).
+// This file is compiled without FMA contraction, so each result is rounded
+// exactly as the reference's, operation by operation.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "fcb_device.h"
+#include "fcb_solvers.cuh"
+
+namespace fcb {
+
+namespace {
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double v) {
+    // Non-negative doubles order like their bit patterns; NaN (large bits) wins
+    // and is reported to the host.
+    atomicMax(p, (unsigned long long)__double_as_longlong(v));
+}
+
+template <int NX, int NY, int PPB, int M, int W, int NAUX>
+struct StepSmem {
+    static constexpr int QROW = 0;
+    static constexpr int XW = QROW + PPB * NX * M;
+    static constexpr int XS = XW + PPB * NX * W * M;
+    static constexpr int GL = XS + PPB * NX * W;
+    static constexpr int FX = GL + PPB * NX * 2 * M;
+    static constexpr int GY = FX + 3 * PPB * NX * 2 * M;
+    static constexpr int AUX = GY + PPB * NX * 2 * M;
+    static constexpr int TAB = AUX + PPB * NAUX * NY * NX;
+    static constexpr int TOTAL = TAB + PPB * 4 * NX;
+};
+
+}  // namespace
+
+// AUXK: AUX_NONE, AUX_SWIRL (velocities computed from the swirl stream function),
+// AUX_STORED (aux arena, NAUX components).
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB>
+__global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
+    constexpr int M = SOL::M;
+    constexpr int W = SOL::W;
+    constexpr int NX = MX + 2 * MBC;
+    constexpr int NY = NX;
+    constexpr int PPB = TPB / NX;
+    using L = StepSmem<NX, NY, PPB, M, W, NAUX>;
+    extern __shared__ double smem[];
+    double* s_qrow = smem + L::QROW;  // [PPB][NX][M]
+    double* s_xw = smem + L::XW;      // [PPB][NX][W][M]
+    double* s_xs = smem + L::XS;      // [PPB][NX][W]
+    double* s_gl = smem + L::GL;      // [PPB][NX][2][M]
+    double* s_fx = smem + L::FX;      // [3][PPB][NX][2][M]
+    double* s_gy = smem + L::GY;      // [PPB][NX][2][M]
+    double* s_aux = smem + L::AUX;    // [PPB][NAUX][NY][NX]
+    double* s_tab = smem + L::TAB;    // [PPB][4][NX]
+
+    const int t = threadIdx.x;
+    const int pl = t / NX;
+    const int c = t - pl * NX;
+    const int pg = blockIdx.x * PPB + pl;
+    const bool active = (pl < PPB) && (pg < a.npatches);
+    const int slot = active ? a.slots[pg] : 0;
+    const PatchMeta meta = active ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0};
+    double* __restrict__ q = a.q + (int64_t)slot * a.q_stride;
+    double* __restrict__ qlast = a.qlast + (int64_t)slot * a.q_stride;
+    const bool save_last = active && (meta.flags & PATCH_SAVE_LAST);
+    const double dtdx = a.dt / meta.dx;
+    const double dtdy = a.dt / meta.dy;
+    const double dtdxave = 0.5 * (dtdx + dtdx);  // 0.5*(dtdx1d(i-1)+dtdx1d(i)), no capacity
+    const double dtdyave = 0.5 * (dtdy + dtdy);
+    SOL sol{a.grav, a.gamma, a.gamma1};
+
+    // ---- aux tile ---------------------------------------------------------
+    if constexpr (AUXK == AUX_SWIRL) {
+        // swirl/user_4.6/b4step2.f with swirl/psi.f:
+        //   u(i,j) = vty*(psi(xll,yll+dy) - psi(xll,yll)),  v(i,j) = -vtx*(psi(xll+dx,yll) - psi(xll,yll))
+        //   psi(x,y) = (sin(pi x)**2 * sin(pi y)**2)/pi
+        constexpr double pi = 3.141592653589793;  // 4*atan(1) in double precision
+        double* tab = s_tab + pl * 4 * NX;
+        if (active) {
+            const double xll = meta.xlower + (double)(c - MBC) * meta.dx;
+            const double yll = meta.ylower + (double)(c - MBC) * meta.dy;  // row c of the table
+            const double sxa = sin(pi * xll), sxb = sin(pi * (xll + meta.dx));
+            const double sya = sin(pi * yll), syb = sin(pi * (yll + meta.dy));
+            tab[0 * NX + c] = sxa * sxa;
+            tab[1 * NX + c] = sxb * sxb;
+            tab[2 * NX + c] = sya * sya;
+            tab[3 * NX + c] = syb * syb;
+        }
+        __syncthreads();
+        if (active) {
+            const double vty = a.vt / meta.dy;
+            const double vtx = a.vt / meta.dx;
+            const double sx2a = tab[0 * NX + c], sx2b = tab[1 * NX + c];
+            double* au = s_aux + (pl * NAUX + 0) * NY * NX;
+            double* av = s_aux + (pl * NAUX + 1) * NY * NX;
+            for (int r = 0; r < NY; ++r) {
+                const double sy2a = tab[2 * NX + r], sy2b = tab[3 * NX + r];
+                const double pij = (sx2a * sy2a) / pi;
+                au[r * NX + c] = vty * ((sx2a * sy2b) / pi - pij);
+                av[r * NX + c] = -vtx * ((sx2b * sy2a) / pi - pij);
+            }
+        }
+    } else if constexpr (AUXK == AUX_STORED) {
+        if (active) {
+            const double* ag = a.aux + (int64_t)slot * a.aux_stride;
+            for (int k = 0; k < NAUX; ++k)
+                for (int r = 0; r < NY; ++r)
+                    s_aux[((pl * NAUX + k) * NY + r) * NX + c] = ag[(k * NY + r) * NX + c];
+        }
+    }
+    __syncthreads();
+    auto AUXV = [&](int k, int cc, int rr) -> double {
+        if constexpr (NAUX > 0) return s_aux[((pl * NAUX + k) * NY + rr) * NX + cc];
+        else return 0.0;
+    };
+
+    const bool ycol = active && c >= 1 && c <= NX - 2;
+    double cfl = 0.0;
+
+    // q rows s-2, s-1, s of this column
+    double q_m2[M], q_m1[M], q_n[M];
+    // y window: finalizing interface f = s-1 uses its raw waves (yw_f) and the
+    // dot products with interfaces f-1 (ydotl) and f+1 (ydotr).
+    double yw_f[W][M], ys_f[W], yam_f[M], yap_f[M], ydotl[W];
+    typename SOL::Roe yR_f{};
+    double yw_n[W][M], ys_n[W], yam_n[M], yap_n[M], ydotr[W];
+    typename SOL::Roe yR_n{};
+    double gRm_prev[M], gRp_prev[M];  // y transverse parts from interface f-1 into cell f-1
+    double FYp_prev[M];               // faddp of interface s-2
+    double GXu_prev[M];               // x-row s-1 "up" transverse part
+    double GXs_m2[M], GXs_m1[M];      // GXu(row-1) + GXd(row) for rows s-2, s-1
+    double GYd_r[M], GYu_r[M];        // y transverse parts for cell row s-2
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        q_m2[m] = q_m1[m] = q_n[m] = 0.0;
+        yam_f[m] = yap_f[m] = yam_n[m] = yap_n[m] = 0.0;
+        gRm_prev[m] = gRp_prev[m] = FYp_prev[m] = GXu_prev[m] = 0.0;
+        GXs_m2[m] = GXs_m1[m] = GYd_r[m] = GYu_r[m] = 0.0;
+    }
+#pragma unroll
+    for (int mw = 0; mw < W; ++mw) {
+        ys_f[mw] = ys_n[mw] = ydotl[mw] = ydotr[mw] = 0.0;
+#pragma unroll
+        for (int m = 0; m < M; ++m) yw_f[mw][m] = yw_n[mw][m] = 0.0;
+    }
+
+    double* qrow = s_qrow + pl * NX * M;
+    double* xw = s_xw + pl * NX * W * M;
+    double* xs = s_xs + pl * NX * W;
+    double* gl = s_gl + pl * NX * 2 * M;
+    double* gy = s_gy + pl * NX * 2 * M;
+
+    for (int s = 0; s <= NY; ++s) {
+        // ---------------- phase 1: load row s; raw y-interface s ----------------
+        if (s < NY && active) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const int64_t k = ((int64_t)m * NY + s) * NX + c;
+                q_n[m] = q[k];
+                if (save_last) qlast[k] = q_n[m];
+                qrow[c * M + m] = q_n[m];
+            }
+            if (ycol && s >= 1) {
+                sol.rpn2(2, q_m1, q_n, AUXV(1, c, s), yw_n, ys_n, yam_n, yap_n, yR_n);
+#pragma unroll
+                for (int mw = 0; mw < W; ++mw) {
+                    double d = 0.0;
+#pragma unroll
+                    for (int m = 0; m < M; ++m) d = d + yw_f[mw][m] * yw_n[mw][m];
+                    ydotr[mw] = d;  // dot(w(s-1), w(s))
+                }
+            }
+        }
+        __syncthreads();  // A
+
+        // ---------------- phase 2: raw x-interface (c, s) ----------------
+        const bool xrow = active && s >= 1 && s <= NY - 2;
+        const bool xint = xrow && c >= 1;
+        double xwl[W][M], xsl[W], xam[M], xap[M];
+        typename SOL::Roe xR{};
+        if (xint) {
+            double qL[M];
+#pragma unroll
+            for (int m = 0; m < M; ++m) qL[m] = qrow[(c - 1) * M + m];
+            sol.rpn2(1, qL, q_n, AUXV(0, c, s), xwl, xsl, xam, xap, xR);
+#pragma unroll
+            for (int mw = 0; mw < W; ++mw) {
+                xs[c * W + mw] = xsl[mw];
+#pragma unroll
+                for (int m = 0; m < M; ++m) xw[(c * W + mw) * M + m] = xwl[mw][m];
+                if (c >= MBC && c <= MBC + MX) cfl = dmax(dmax(cfl, dtdx * xsl[mw]), -dtdx * xsl[mw]);
+            }
+        }
+
+        // ---------------- y: finalize interface f = s-1 (own column) ----------------
+        double FYm_cur[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) { FYm_cur[m] = 0.0; GYd_r[m] = 0.0; GYu_r[m] = 0.0; }
+        const int f = s - 1;
+        if (ycol && f >= 1) {
+            double w[W][M];
+#pragma unroll
+            for (int mw = 0; mw < W; ++mw)
+#pragma unroll
+                for (int m = 0; m < M; ++m) w[mw][m] = yw_f[mw][m];
+            if (f >= MBC && f <= MBC + MX) {
+#pragma unroll
+                for (int mw = 0; mw < W; ++mw) cfl = dmax(dmax(cfl, dtdy * ys_f[mw]), -dtdy * ys_f[mw]);
+            }
+            double cq[M];
+#pragma unroll
+            for (int m = 0; m < M; ++m) cq[m] = 0.0;
+            if (a.order0 == 2) {
+                if (f >= MBC && f <= MBC + MX) {
+#pragma unroll
+                    for (int mw = 0; mw < W; ++mw) {
+                        if (a.mthlim[mw] == 0) continue;
+                        double wn2 = 0.0;
+#pragma unroll
+                        for (int m = 0; m < M; ++m) wn2 = wn2 + yw_f[mw][m] * yw_f[mw][m];
+                        if (wn2 == 0.0) continue;
+                        const double r = (ys_f[mw] > 0.0) ? ydotl[mw] / wn2 : ydotr[mw] / wn2;
+                        const double phi = limiter_phi(a.mthlim[mw], r);
+#pragma unroll
+                        for (int m = 0; m < M; ++m) w[mw][m] = phi * w[mw][m];
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < M; ++m) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int mw = 0; mw < W; ++mw) {
+                        const double as = fabs(ys_f[mw]);
+                        acc = acc + as * (1.0 - as * dtdyave) * w[mw][m];
+                    }
+                    cq[m] = acc;
+                }
+            }
+            double fm_[M], fp_[M], am[M], ap[M];
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                double fmv = 0.0, fpv = 0.0;
+                if (f <= NY - 2) { fmv = fmv + yam_f[m]; fpv = fpv - yap_f[m]; }
+                if (a.order0 == 2) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
+                fm_[m] = fmv; fp_[m] = fpv;
+                am[m] = yam_f[m]; ap[m] = yap_f[m];
+                if (a.order0 > 1 && a.order1 == 2 && f <= NY - 2) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
+                FYm_cur[m] = fmv;
+            }
+            double gLm[M], gLp[M], gRm[M], gRp[M];
+            if (a.order1 > 0) {
+                double bm[M], bp[M];
+                // imp = 1: aux2(j-1, kv=1), aux3(j-1, kv=1) = u at columns c, c+1, row f-1
+                sol.rpt2(2, am, yR_f, AUXV(0, c, f - 1), AUXV(0, c + 1, f - 1), bm, bp);
+#pragma unroll
+                for (int m = 0; m < M; ++m) { gLm[m] = 0.5 * dtdy * bm[m]; gLp[m] = 0.5 * dtdy * bp[m]; }
+                sol.rpt2(2, ap, yR_f, AUXV(0, c, f), AUXV(0, c + 1, f), bm, bp);
+#pragma unroll
+                for (int m = 0; m < M; ++m) { gRm[m] = 0.5 * dtdy * bm[m]; gRp[m] = 0.5 * dtdy * bp[m]; }
+            } else {
+#pragma unroll
+                for (int m = 0; m < M; ++m) gLm[m] = gLp[m] = gRm[m] = gRp[m] = 0.0;
+            }
+            // cell row k = f-1 is now complete: gadd(k,.,1) = (0 - gL(k+1)) - gR(k)
+            if (f - 1 >= 1) {
+#pragma unroll
+                for (int m = 0; m < M; ++m) {
+                    GYd_r[m] = (0.0 - gLm[m]) - gRm_prev[m];
+                    GYu_r[m] = (0.0 - gLp[m]) - gRp_prev[m];
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < M; ++m) { gRm_prev[m] = gRm[m]; gRp_prev[m] = gRp[m]; }
+            // FYp of interface f is needed when updating cell row f (two steps on)
+#pragma unroll
+            for (int m = 0; m < M; ++m) { FYm_cur[m] = fm_[m]; }
+            // rotate FYp below, after the update of row s-2 has used FYp(s-2)
+#pragma unroll
+            for (int m = 0; m < M; ++m) yap_f[m] = fp_[m];  // reuse slot: holds FYp(f) until rotation
+        }
+        // shift the y window: raw interface s becomes the one to finalize next
+#pragma unroll
+        for (int mw = 0; mw < W; ++mw) {
+            ydotl[mw] = ydotr[mw];
+            ys_f[mw] = ys_n[mw];
+#pragma unroll
+            for (int m = 0; m < M; ++m) yw_f[mw][m] = yw_n[mw][m];
+        }
+        double FYp_cur[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            FYp_cur[m] = (ycol && f >= 1) ? yap_f[m] : 0.0;
+            yam_f[m] = yam_n[m];
+            yap_f[m] = yap_n[m];
+        }
+        yR_f = yR_n;
+        __syncthreads();  // B
+
+        // ---------------- phase 3: x limiter, corrections, transverse ----------------
+        double* fxs = s_fx + ((s % 3) * PPB + pl) * NX * 2 * M;
+        double gRmx[M], gRpx[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) gRmx[m] = gRpx[m] = 0.0;
+        if (xint) {
+            double cq[M];
+#pragma unroll
+            for (int m = 0; m < M; ++m) cq[m] = 0.0;
+            if (a.order0 == 2) {
+                if (c >= MBC && c <= MBC + MX) {
+#pragma unroll
+                    for (int mw = 0; mw < W; ++mw) {
+                        if (a.mthlim[mw] == 0) continue;
+                        double wn2 = 0.0, dl = 0.0, dr = 0.0;
+#pragma unroll
+                        for (int m = 0; m < M; ++m) {
+                            const double wc = xwl[mw][m];
+                            wn2 = wn2 + wc * wc;
+                            dl = dl + xw[((c - 1) * W + mw) * M + m] * wc;
+                            dr = dr + wc * xw[((c + 1) * W + mw) * M + m];
+                        }
+                        if (wn2 == 0.0) continue;
+                        const double r = (xsl[mw] > 0.0) ? dl / wn2 : dr / wn2;
+                        const double phi = limiter_phi(a.mthlim[mw], r);
+#pragma unroll
+                        for (int m = 0; m < M; ++m) xwl[mw][m] = phi * xwl[mw][m];
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < M; ++m) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int mw = 0; mw < W; ++mw) {
+                        const double as = fabs(xsl[mw]);
+                        acc = acc + as * (1.0 - as * dtdxave) * xwl[mw][m];
+                    }
+                    cq[m] = acc;
+                }
+            }
+            double am[M], ap[M];
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                double fmv = 0.0, fpv = 0.0;
+                if (c <= NX - 2) { fmv = fmv + xam[m]; fpv = fpv - xap[m]; }
+                if (a.order0 == 2) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
+                fxs[(c * 2 + 0) * M + m] = fmv;
+                fxs[(c * 2 + 1) * M + m] = fpv;
+                am[m] = xam[m]; ap[m] = xap[m];
+                if (a.order0 > 1 && a.order1 == 2 && c <= NX - 2) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
+            }
+            if (a.order1 > 0) {
+                double bm[M], bp[M];
+                // imp = 1: aux2(i-1, kv=2), aux3(i-1, kv=2) = v at column c-1, rows s, s+1
+                sol.rpt2(1, am, xR, AUXV(1, c - 1, s), AUXV(1, c - 1, s + 1), bm, bp);
+#pragma unroll
+                for (int m = 0; m < M; ++m) {
+                    gl[(c * 2 + 0) * M + m] = 0.5 * dtdx * bm[m];
+                    gl[(c * 2 + 1) * M + m] = 0.5 * dtdx * bp[m];
+                }
+                sol.rpt2(1, ap, xR, AUXV(1, c, s), AUXV(1, c, s + 1), bm, bp);
+#pragma unroll
+                for (int m = 0; m < M; ++m) { gRmx[m] = 0.5 * dtdx * bm[m]; gRpx[m] = 0.5 * dtdx * bp[m]; }
+            } else {
+#pragma unroll
+                for (int m = 0; m < M; ++m) { gl[(c * 2 + 0) * M + m] = 0.0; gl[(c * 2 + 1) * M + m] = 0.0; }
+            }
+        } else if (active) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                fxs[(c * 2 + 0) * M + m] = 0.0;
+                fxs[(c * 2 + 1) * M + m] = 0.0;
+                gl[(c * 2 + 0) * M + m] = 0.0;
+                gl[(c * 2 + 1) * M + m] = 0.0;
+            }
+        }
+        __syncthreads();  // C
+
+        // ---------------- phase 4: complete GX(c, s); publish GY(c, s-2) ----------------
+        double GXs_n[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            double gxd = 0.0, gxu = 0.0;
+            if (xint) {
+                if (c + 1 <= NX - 1) {
+                    gxd = gxd - gl[((c + 1) * 2 + 0) * M + m];
+                    gxu = gxu - gl[((c + 1) * 2 + 1) * M + m];
+                }
+                gxd = gxd - gRmx[m];
+                gxu = gxu - gRpx[m];
+            }
+            GXs_n[m] = GXu_prev[m] + gxd;
+            GXu_prev[m] = gxu;
+        }
+        if (active) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                gy[(c * 2 + 0) * M + m] = GYd_r[m];
+                gy[(c * 2 + 1) * M + m] = GYu_r[m];
+            }
+        }
+        __syncthreads();  // D
+
+        // ---------------- phase 5: update cell row r = s-2 ----------------
+        const int r = s - 2;
+        if (active && r >= 0 && r <= NY - 2 && c <= NX - 2) {
+            const double* fxr = s_fx + ((r % 3) * PPB + pl) * NX * 2 * M;
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const double fxm1 = fxr[((c + 1) * 2 + 0) * M + m];
+                const double fxp0 = fxr[(c * 2 + 1) * M + m];
+                const double gyu_l = (c >= 1) ? gy[((c - 1) * 2 + 1) * M + m] : 0.0;
+                const double gyd_r = gy[((c + 1) * 2 + 0) * M + m];
+                const double fmv = (fxm1 + GYu_r[m]) + gyd_r;       // fm(i+1, j)
+                const double fpv = (fxp0 + gyu_l) + GYd_r[m];       // fp(i, j)
+                const double gmv = GXs_m1[m] + FYm_cur[m];          // gm(i, j+1)
+                const double gpv = GXs_m2[m] + FYp_prev[m];         // gp(i, j)
+                const double qv = q_m2[m] - dtdx * (fmv - fpv) - dtdy * (gmv - gpv);
+                q[((int64_t)m * NY + r) * NX + c] = qv;
+            }
+        }
+        // rotate per-row registers
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            q_m2[m] = q_m1[m];
+            q_m1[m] = q_n[m];
+            GXs_m2[m] = GXs_m1[m];
+            GXs_m1[m] = GXs_n[m];
+            FYp_prev[m] = FYp_cur[m];
+        }
+    }
+
+    // ---- CFL: warp max, one atomic per warp ----
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+    if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg(a.cfl_out, cfl);
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launcher: dispatch on (solver, mx, aux kind).
+// ---------------------------------------------------------------------------
+namespace {
+
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB>
+cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
+    constexpr int NX = MX + 2 * MBC;
+    constexpr int PPB = TPB / NX;
+    static_assert(PPB >= 1, "patch wider than the CTA");
+    using L = StepSmem<NX, NX, PPB, SOL::M, SOL::W, NAUX>;
+    const size_t bytes = (size_t)L::TOTAL * sizeof(double);
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    const int blocks = (a.npatches + PPB - 1) / PPB;
+    if (blocks == 0) return cudaSuccess;
+    step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB><<<blocks, TPB, bytes, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <class SOL, int AUXK, int NAUX>
+cudaError_t launch_mx(int mx, int mbc, const StepArgs& a, cudaStream_t st) {
+    if (mbc != 2) return cudaErrorInvalidValue;
+    switch (mx) {
+        case 8: return launch_one<SOL, 8, 2, AUXK, NAUX, 128>(a, st);
+        case 16: return launch_one<SOL, 16, 2, AUXK, NAUX, 128>(a, st);
+        case 32: return launch_one<SOL, 32, 2, AUXK, NAUX, 128>(a, st);
+        case 64: return launch_one<SOL, 64, 2, AUXK, NAUX, 128>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+// Returns cudaErrorInvalidValue for an unsupported (solver, mx, mbc, aux) combination.
+cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
+                        const StepArgs& a, cudaStream_t st) {
+    if (mx != my) return cudaErrorInvalidValue;
+    switch (solver) {
+        case SOLVER_ADVECTION:
+            if (mwaves != 1) return cudaErrorInvalidValue;
+            if (aux_kind == AUX_SWIRL) return launch_mx<AdvectionSolver<1>, AUX_SWIRL, 2>(mx, mbc, a, st);
+            if (aux_kind == AUX_STORED && a.maux == 2)
+                return launch_mx<AdvectionSolver<1>, AUX_STORED, 2>(mx, mbc, a, st);
+            return cudaErrorInvalidValue;
+        case SOLVER_SWE_ROE:
+            if (mwaves != 3 || aux_kind != AUX_NONE) return cudaErrorInvalidValue;
+            return launch_mx<SweRoeSolver, AUX_NONE, 0>(mx, mbc, a, st);
+        case SOLVER_EULER4_ROE:
+            if (mwaves != 4 || aux_kind != AUX_NONE) return cudaErrorInvalidValue;
+            return launch_mx<Euler4RoeSolver, AUX_NONE, 0>(mx, mbc, a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace fcb

@@ -1,0 +1,173 @@
+/*
+ * forestclaw-b200: C ABI of the B200 (sm_100a) patch hot path.
+ *
+ * One context holds one solve: the quadtree forest (single unit-square block,
+ * p4est leaf-order semantics) on the host, and every patch array (q, the
+ * pre-step copy used for time interpolation, the time-interpolated copy, the
+ * CFL-retry copy, aux) resident in a pooled device arena indexed by slot.
+ * Neighbour tables and ghost-fill operation lists are rebuilt on the host and
+ * uploaded only after a regrid.
+ *
+ * Every entry point returns FCB_OK (0) or an error code and never exits the
+ * process; fcb_last_error() returns the message of the last failure on the
+ * calling thread.  Host buffers are plain pointers; patch arrays use the
+ * reference's clawpack 4.6 layout q(i,j,m) with i fastest and Fortran ranges
+ * i in [1-mbc, mx+mbc], j in [1-mbc, my+mbc].
+ *
+ * A context is used from one host thread at a time.  Work is enqueued on the
+ * CUDA stream given at creation (or the legacy default stream for NULL).
+ */
+#ifndef FCLAW_B200_H
+#define FCLAW_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FCB_ABI_VERSION 1
+
+enum fcb_status {
+    FCB_OK = 0,
+    FCB_ERR_INVALID = 1,     /* bad argument or unsupported option combination */
+    FCB_ERR_CUDA = 2,        /* a CUDA call failed */
+    FCB_ERR_STATE = 3,       /* call out of order (e.g. step before initialize) */
+    FCB_ERR_NUMERIC = 4,     /* NaN/Inf in the CFL number */
+    FCB_ERR_INTERNAL = 5
+};
+
+/* Riemann solver families (fc2d_clawpack46_vtable_t rpn2/rpt2 pairs). */
+enum fcb_solver_kind {
+    FCB_SOLVER_ADVECTION = 0,  /* clawpack46_rpn2adv / rpt2adv (edge velocities in aux) */
+    FCB_SOLVER_SWE_ROE = 1,    /* shallow water Roe with entropy fix (clawpack46_rpn2/rpt2) */
+    FCB_SOLVER_EULER4_ROE = 2  /* Euler Roe with entropy fix (clawpack46_rpn2_euler4/rpt2_euler4) */
+};
+
+/* Initial conditions / b4step2 hooks of the configured applications. */
+enum fcb_problem {
+    FCB_PROBLEM_SWIRL = 0,      /* advection/2d/swirl: qinit.f, b4step2.f velocities; p[0] = tperiod */
+    FCB_PROBLEM_RADIALDAM = 1,  /* dam break: p = {x0, y0, r0, h_in, h_out} */
+    FCB_PROBLEM_QUADRANTS = 2   /* euler/2d/quadrants qinit.f: p = rho[4], u[4], v[4], p[4], xs, ys */
+};
+
+/* Refinement criteria (fclaw2d_clawpatch_options "refinement-criteria"). */
+enum fcb_criteria { FCB_TAG_VALUE = 0, FCB_TAG_MINMAX = 1, FCB_TAG_DIFFERENCE = 2, FCB_TAG_GRADIENT = 3 };
+
+/*
+ * The fields of fclaw_options_t, fclaw2d_clawpatch_options_t and
+ * fc2d_clawpack46_options_t that the patch hot path reads (names as in the
+ * reference's ini sections).  The domain is the unit square (ax=0,bx=1,ay=0,by=1).
+ */
+typedef struct fcb_options {
+    /* [clawpatch] */
+    int mx, my, mbc, meqn, maux;
+    int refinement_criteria;   /* enum fcb_criteria */
+    int threshold_variable;    /* 1-based component used for tagging */
+    /* [clawpack46] */
+    int order[2];              /* method(2:3) */
+    int mcapa;                 /* must be 0: capacity is not part of this path */
+    int mwaves;
+    int mthlim[8];
+    int mthbc[4];              /* left, right, bottom, top: 1 extrapolation, 3 wall */
+    /* [Options] */
+    int minlevel, maxlevel;
+    int subcycle;
+    int regrid_interval;
+    int smooth_refine, smooth_level;
+    int use_fixed_dt;
+    int nout;
+    int init_ghostcell;
+    int reduce_cfl;
+    double refine_threshold, coarsen_threshold;
+    double tfinal, initial_dt, max_cfl, desired_cfl;
+    /* solver and problem */
+    int solver_kind;           /* enum fcb_solver_kind */
+    int problem;               /* enum fcb_problem */
+    double grav;               /* SWE /cparam/ grav */
+    double gamma;              /* Euler /cparam/ gamma; gamma1 = gamma - 1 */
+    double problem_params[32];
+} fcb_options_t;
+
+typedef struct fcb_counters {
+    long long count_amr_advance;     /* fclaw2d_global_t counters of the same names */
+    long long count_amr_new_domain;
+    long long count_amr_regrid;
+    long long count_single_step;     /* patch updates; x mx*my = cell updates */
+    long long count_ghost_waves;     /* ghost-fill kernel launches */
+    long long count_kernel_launches; /* all kernels launched by the library */
+} fcb_counters_t;
+
+typedef struct fcb_context fcb_context_t;
+
+/* ---- context ---------------------------------------------------------------- */
+/* Replaces the solver/patch setup of fc2d_clawpack46_solver_initialize
+ * (src/solvers/fc2d_clawpack4.6/fc2d_clawpack46.cpp:483-537) and
+ * fclaw2d_domain_new_unitsquare (src/fclaw2d_convenience.c:326). */
+int fcb_context_create(const fcb_options_t* opt, void* cuda_stream, fcb_context_t** out);
+int fcb_context_destroy(fcb_context_t* ctx);
+const char* fcb_last_error(void);
+int fcb_abi_version(void);
+
+/* ---- time stepping core ---------------------------------------------------- */
+/* fclaw2d_initialize (src/fclaw2d_initialize.c:75): uniform minlevel, qinit,
+ * initial refinement up to maxlevel. */
+int fcb_initialize(fcb_context_t* ctx);
+/* fclaw2d_run outstyle 1 (src/fclaw2d_run.c:120-290): advance to tfinal with
+ * adaptive dt, CFL rejection and regridding. */
+int fcb_run(fcb_context_t* ctx);
+/* fclaw2d_advance_all_levels (src/fclaw2d_advance.c:247): one subcycled
+ * macro-step from t with coarse step dt; returns the max CFL over all updates. */
+int fcb_advance_all_levels(fcb_context_t* ctx, double t, double dt, double* maxcfl);
+/* fclaw2d_update_single_step (src/fclaw2d_update_single_step.c:73): every patch
+ * of `level` advanced by dt in one batched launch; returns the level max CFL. */
+int fcb_update_single_step(fcb_context_t* ctx, int level, double t, double dt, double* maxcfl);
+/* The batched level update of fcb_update_single_step without the CFL
+ * read-back: the launch is only enqueued on the context's stream, and the
+ * level max CFL is folded into the value fcb_advance_all_levels reports next.
+ * For callers that pipeline several levels before synchronising. */
+int fcb_update_single_step_async(fcb_context_t* ctx, int level, double t, double dt);
+/* patch_vt->single_step_update (src/fclaw2d_patch.h:937-943, set at
+ * fc2d_clawpack46.cpp:512) with the buffer_data protocol of
+ * fclaw2d_update_single_step.h:47-71: calls with iter = 0..total_count-1 are
+ * recorded; the call with iter == total_count-1 launches the batch and returns
+ * the batch CFL in *cfl (the other calls return 0). */
+int fcb_single_step_update(fcb_context_t* ctx, int patchno, double t, double dt, int iter,
+                           int total_count, double* cfl);
+/* fclaw2d_ghost_update (src/fclaw2d_ghost_fill.c:838), one rank. */
+int fcb_ghost_update(fcb_context_t* ctx, int minlevel, int maxlevel, double sync_time, int time_interp);
+/* fclaw2d_timeinterp (src/fclaw2d_timeinterp.c:51). */
+int fcb_timeinterp(fcb_context_t* ctx, int level, double alpha);
+/* fclaw2d_regrid (src/fclaw2d_regrid.c:234); *changed = 1 if the mesh changed. */
+int fcb_regrid(fcb_context_t* ctx, int* changed);
+/* fclaw2d_physical_set_bc (src/fclaw2d_physical_bc.c) for every patch of a level. */
+int fcb_physical_set_bc(fcb_context_t* ctx, int level, int time_interp);
+
+/* ---- queries and data movement ------------------------------------------------ */
+int fcb_num_patches(fcb_context_t* ctx, int* n);
+/* Leaf p in Morton order: level and lower-left corner in units of 2^-28. */
+int fcb_patch_info(fcb_context_t* ctx, int p, int* level, int* x, int* y);
+/* Neighbour relations of leaf p (layout: face_rel[4], face_nbr[4][2],
+ * corner_rel[4] (0 = no corner neighbour), corner_nbr[4], has_fine, on_cf):
+ * relation codes 0 boundary, 1 half size, 2 same size, 3 double size. */
+int fcb_patch_neighbors(fcb_context_t* ctx, int p, int* out22);
+/* Size in doubles of one patch array: meqn*(mx+2mbc)*(my+2mbc). */
+int fcb_patch_size(fcb_context_t* ctx, size_t* n);
+/* Copy all leaves' q (Morton order, patch after patch) to/from host memory. */
+int fcb_get_q(fcb_context_t* ctx, double* host, size_t n);
+int fcb_set_q(fcb_context_t* ctx, const double* host, size_t n);
+/* Time-interpolated arrays of all leaves (same layout). */
+int fcb_get_qinterp(fcb_context_t* ctx, double* host, size_t n);
+int fcb_counters(fcb_context_t* ctx, fcb_counters_t* out);
+/* Mass diagnostic (fclaw2d_clawpatch46_diagnostics.f:13-58): Kahan sum of
+ * q*dx*dy per component over all leaves; sums has meqn entries. */
+int fcb_conservation_check(fcb_context_t* ctx, double* sums);
+/* Current time of the run loop. */
+int fcb_curr_time(fcb_context_t* ctx, double* t);
+/* Wait for all work of the context. */
+int fcb_synchronize(fcb_context_t* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FCLAW_B200_H */

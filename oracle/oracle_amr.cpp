@@ -217,11 +217,19 @@ double Solver::single_step_patch(int p, double t, double dt) {
 
 double Solver::update_single_step(int level, double t, double dt) {
     double maxcfl = 0;
-    for (int p : patches_at_level(level)) {
+    const std::vector<int> ps = patches_at_level(level);
+#ifdef ORC_OPENMP
+    // timing build: patches of one level are independent (max is order-free)
+#pragma omp parallel for schedule(dynamic, 4) reduction(max : maxcfl)
+    for (int k = 0; k < (int)ps.size(); ++k) maxcfl = std::fmax(single_step_patch(ps[k], t, dt), maxcfl);
+    count_single_step += (long long)ps.size();
+#else
+    for (int p : ps) {
         const double cfl = single_step_patch(p, t, dt);
         ++count_single_step;
         maxcfl = std::fmax(cfl, maxcfl);
     }
+#endif
     return maxcfl;
 }
 

@@ -1,0 +1,73 @@
+"""Shared configurations: one Config (oracle) <-> Options (CUDA path) per case."""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+import oracle as O
+
+
+def to_options(cfg: O.Config):
+    import forestclaw_b200 as fcb
+
+    return fcb.Options(
+        mx=cfg.mx, my=cfg.my, mbc=cfg.mbc, meqn=cfg.meqn, maux=cfg.maux,
+        refinement_criteria=cfg.criteria, threshold_variable=cfg.ivar + 1,
+        order=cfg.order, mcapa=cfg.mcapa, mwaves=cfg.mwaves, mthlim=cfg.mthlim, mthbc=cfg.mthbc,
+        minlevel=cfg.minlevel, maxlevel=cfg.maxlevel, subcycle=cfg.subcycle,
+        regrid_interval=cfg.regrid_interval, smooth_refine=cfg.smooth_refine,
+        smooth_level=cfg.smooth_level, use_fixed_dt=cfg.use_fixed_dt, nout=cfg.nout,
+        init_ghostcell=cfg.init_ghostcell, reduce_cfl=cfg.reduce_cfl,
+        refine_threshold=cfg.refine_threshold, coarsen_threshold=cfg.coarsen_threshold,
+        tfinal=cfg.tfinal, initial_dt=cfg.initial_dt, max_cfl=cfg.max_cfl,
+        desired_cfl=cfg.desired_cfl, solver_kind=cfg.solver, problem=cfg.problem,
+        grav=cfg.grav, gamma=cfg.gamma, problem_params=cfg.pparams,
+    )
+
+
+def swirl_uniform(level=4, mx=16, tperiod=2.0) -> O.Config:
+    """Plain-method advection case: uniform level, MC limiter, order (2,2), swirl
+    velocities with T = tperiod/2 (cos(pi t/T) at mid-step), q0 = 1 for x < 0.5."""
+    return O.Config(mx=mx, my=mx, mbc=2, meqn=1, maux=2, order=(2, 2), mwaves=1, mthlim=(4,),
+                    mthbc=(1, 1, 1, 1), minlevel=level, maxlevel=level, subcycle=1,
+                    regrid_interval=0, use_fixed_dt=1, solver=O.ADVECTION, problem=O.SWIRL,
+                    pparams=(tperiod,))
+
+
+def swirl_dt(level=4, mx=16, cfl=0.9) -> float:
+    """dt = cfl * dx / max|u| with max|u| = 1 on the unit square."""
+    return cfl / (mx * (1 << level))
+
+
+def radialdam_uniform(level=3, mx=16, r0=0.25, hin=2.0, hout=1.0) -> O.Config:
+    return O.Config(mx=mx, my=mx, mbc=2, meqn=3, maux=0, order=(2, 2), mwaves=3, mthlim=(4, 4, 4),
+                    mthbc=(1, 1, 1, 1), minlevel=level, maxlevel=level, regrid_interval=0,
+                    use_fixed_dt=1, solver=O.SWE_ROE, problem=O.RADIALDAM, grav=1.0,
+                    pparams=(0.5, 0.5, r0, hin, hout))
+
+
+def quadrants_uniform(level=3, mx=16) -> O.Config:
+    return O.Config(mx=mx, my=mx, mbc=2, meqn=4, maux=0, order=(2, 2), mwaves=4, mthlim=(4, 4, 4, 4),
+                    mthbc=(1, 1, 1, 1), minlevel=level, maxlevel=level, regrid_interval=0,
+                    use_fixed_dt=1, solver=O.EULER4_ROE, problem=O.QUADRANTS, gamma=1.4,
+                    pparams=O.quadrants_params())
+
+
+def radialdam_amr(seed=0, minlevel=3, maxlevel=6, mx=32, tfinal=0.5) -> O.Config:
+    """AMR shallow water: Roe rpn2/rpt2, g = 1, subcycling, gradient tagging on h
+    (refine > 0.05, coarsen < 0.01), regrid every step, smooth refinement,
+    h = 2 inside r < r0 = 0.25 + 0.05*U(-1,1) (seeded), h = 1 outside."""
+    rng = np.random.default_rng(seed)
+    r0 = 0.25 + 0.05 * rng.uniform(-1.0, 1.0)
+    return O.Config(mx=mx, my=mx, mbc=2, meqn=3, maux=0, order=(2, 2), mwaves=3, mthlim=(4, 4, 4),
+                    mthbc=(1, 1, 1, 1), minlevel=minlevel, maxlevel=maxlevel, subcycle=1,
+                    regrid_interval=1, smooth_refine=1, criteria=O.GRADIENT,
+                    refine_threshold=0.05, coarsen_threshold=0.01, tfinal=tfinal,
+                    initial_dt=0.9 / (mx * (1 << minlevel)) / 1.5, max_cfl=1.0, desired_cfl=0.9,
+                    solver=O.SWE_ROE, problem=O.RADIALDAM, grav=1.0,
+                    pparams=(0.5, 0.5, r0, 2.0, 1.0))
+
+
+def replace(cfg, **kw):
+    return dataclasses.replace(cfg, **kw)

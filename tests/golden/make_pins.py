@@ -1,0 +1,43 @@
+"""Regenerate tests/golden/regression_pins.json from the reference tree.
+
+The reference's regression tests pin three counters per run
+(src/fclaw2d_finalize.c:140-197): count_amr_advance, global_num_patches and
+count_amr_new_domain.  This script copies those numbers for the runs whose
+configuration lies on this path (swirl and quadrants, clawpack 4.6), so the
+tests can check the oracle and the CUDA path without the reference tree.
+
+Usage: python tests/golden/make_pins.py /path/to/reference
+"""
+import csv
+import json
+import sys
+from pathlib import Path
+
+
+def read_csv(p: Path) -> dict:
+    out = {}
+    with open(p) as f:
+        for row in csv.reader(f):
+            if len(row) == 2:
+                out[row[0]] = int(row[1])
+    return out
+
+
+def main(ref: Path):
+    pins = {
+        "swirl": {
+            "source": "applications/clawpack/advection/2d/swirl/regression_values_0.csv",
+            "values": read_csv(ref / "applications/clawpack/advection/2d/swirl/regression_values_0.csv"),
+        },
+        "quadrants": {
+            "source": "applications/clawpack/euler/2d/quadrants/regression_values_0.csv",
+            "values": read_csv(ref / "applications/clawpack/euler/2d/quadrants/regression_values_0.csv"),
+        },
+    }
+    out = Path(__file__).with_name("regression_pins.json")
+    out.write_text(json.dumps(pins, indent=1) + "\n")
+    print(out)
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))

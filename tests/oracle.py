@@ -111,6 +111,14 @@ class Config:
 
 
 _lib = None
+_lib_path = None
+
+
+def use_library(path):
+    """Select another build of the oracle (e.g. the OpenMP timing build) before first use."""
+    global _lib_path, _lib
+    _lib_path = Path(path)
+    _lib = None
 
 
 def lib():
@@ -118,10 +126,13 @@ def lib():
     global _lib
     if _lib is not None:
         return _lib
-    so = ORACLE_DIR / "liboracle.so"
-    srcs = list(ORACLE_DIR.glob("*.cpp")) + list(ORACLE_DIR.glob("*.hpp"))
-    if not so.exists() or any(s.stat().st_mtime > so.stat().st_mtime for s in srcs):
-        subprocess.run(["make", "-s", "liboracle.so"], cwd=ORACLE_DIR, check=True)
+    if _lib_path is not None:
+        so = _lib_path
+    else:
+        so = ORACLE_DIR / "liboracle.so"
+        srcs = list(ORACLE_DIR.glob("*.cpp")) + list(ORACLE_DIR.glob("*.hpp"))
+        if not so.exists() or any(s.stat().st_mtime > so.stat().st_mtime for s in srcs):
+            subprocess.run(["make", "-s", "liboracle.so"], cwd=ORACLE_DIR, check=True)
     L = ctypes.CDLL(str(so))
     assert L.orc_iopt_count() == len(_I_FIELDS), "oracle option layout changed"
     assert L.orc_dopt_count() == len(_D_FIELDS), "oracle option layout changed"

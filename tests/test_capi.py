@@ -1,0 +1,71 @@
+"""The C ABI library loads, exports every entry point the header declares,
+and its options struct has the header's layout.  No GPU is needed."""
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "fclaw_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(fcb_\w+)\s*\(", text, flags=re.M)))
+
+
+@pytest.fixture(scope="module")
+def built():
+    from forestclaw_b200 import build
+
+    build.build()
+    import forestclaw_b200 as fcb
+
+    return fcb
+
+
+def test_library_exports_every_declared_symbol(built):
+    lib = built.lib()
+    names = declared_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(built.EXPORTED_SYMBOLS)
+    assert lib.fcb_abi_version() == 1
+
+
+def test_options_layout_matches_header(built, tmp_path):
+    src = tmp_path / "sz.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "fclaw_b200.h"\n'
+        "int main(void){printf(\"%zu %zu %zu %zu\\n\", sizeof(fcb_options_t),"
+        " offsetof(fcb_options_t, refine_threshold), offsetof(fcb_options_t, problem_params),"
+        " sizeof(fcb_counters_t)); return 0;}\n")
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    from forestclaw_b200 import _Counters, _Options
+
+    assert int(out[0]) == ctypes.sizeof(_Options)
+    assert int(out[1]) == _Options.refine_threshold.offset
+    assert int(out[2]) == _Options.problem_params.offset
+    assert int(out[3]) == ctypes.sizeof(_Counters)
+
+
+def test_invalid_options_rejected_before_any_device_call(built):
+    o = built.Options(mx=12, my=12)
+    with pytest.raises(built.FcbError) as e:
+        built.Solver(o)
+    assert e.value.code == 1  # FCB_ERR_INVALID
+    o = built.Options(mthbc=(0, 1, 1, 1))
+    with pytest.raises(built.FcbError) as e:
+        built.Solver(o)
+    assert e.value.code == 1
+
+
+def test_null_arguments_are_errors(built):
+    lib = built.lib()
+    assert lib.fcb_context_create(None, None, None) == 1
+    assert b"null" in lib.fcb_last_error()

@@ -1,0 +1,153 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances: the step, ghost and regrid kernels are compiled without FMA
+contraction and follow the reference's operation order, so square roots and
+divisions (correctly rounded on both sides) give identical bits; the swirl
+velocities use sin(), whose last bit may differ between CUDA and glibc, so the
+advection cases allow 1e-12 relative max-norm per step (the contract's bound).
+"""
+import numpy as np
+import pytest
+
+import cases
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-12
+
+
+def _pair(cfg):
+    import forestclaw_b200 as fcb
+
+    o = O.OracleSolver(cfg)
+    d = fcb.Solver(cases.to_options(cfg))
+    o.initialize()
+    d.initialize()
+    return o, d
+
+
+def _rel_err(a, b):
+    scale = max(1.0, float(np.max(np.abs(b))))
+    return float(np.max(np.abs(a - b))) / scale
+
+
+def _assert_same_mesh(o, d):
+    assert d.leaves() == o.leaves()
+
+
+@pytest.mark.parametrize("mx", [8, 16, 32])
+def test_uniform_swirl_steps(gpu_lib, mx):
+    cfg = cases.swirl_uniform(level=3, mx=mx)
+    dt = cases.swirl_dt(level=3, mx=mx)
+    o, d = _pair(cfg)
+    _assert_same_mesh(o, d)
+    assert np.array_equal(d.get_q(), o.all_q()), "qinit differs"
+    t = 0.0
+    for step in range(12):
+        c_o = o.advance(t, dt)
+        c_d = d.advance_all_levels(t, dt)
+        t += dt
+        err = _rel_err(d.get_q(), o.all_q())
+        assert err <= REL_TOL, f"step {step}: rel err {err:.3e}"
+        assert abs(c_d - c_o) <= 1e-12 * max(1.0, c_o), (c_d, c_o)
+
+
+@pytest.mark.parametrize("mx", [16, 32])
+def test_uniform_radialdam_bit_exact(gpu_lib, mx):
+    cfg = cases.radialdam_uniform(level=2, mx=mx)
+    dt = 0.4 / (mx * 4) / 1.5
+    o, d = _pair(cfg)
+    assert np.array_equal(d.get_q(), o.all_q())
+    t = 0.0
+    for step in range(10):
+        c_o = o.advance(t, dt)
+        c_d = d.advance_all_levels(t, dt)
+        t += dt
+        qd, qo = d.get_q(), o.all_q()
+        assert np.array_equal(qd, qo), f"step {step}: max diff {np.max(np.abs(qd - qo)):.3e}"
+        assert c_d == c_o
+
+
+@pytest.mark.parametrize("mx", [8, 16])
+def test_uniform_quadrants_bit_exact(gpu_lib, mx):
+    cfg = cases.quadrants_uniform(level=2, mx=mx)
+    dt = 0.3 / (mx * 4) / 2.0
+    o, d = _pair(cfg)
+    assert np.array_equal(d.get_q(), o.all_q())
+    t = 0.0
+    for step in range(8):
+        c_o = o.advance(t, dt)
+        c_d = d.advance_all_levels(t, dt)
+        t += dt
+        qd, qo = d.get_q(), o.all_q()
+        assert np.array_equal(qd, qo), f"step {step}: max diff {np.max(np.abs(qd - qo)):.3e}"
+        assert c_d == c_o
+
+
+def test_single_step_update_protocol(gpu_lib):
+    """patch_vt->single_step_update semantics: the batch runs on the last call."""
+    cfg = cases.radialdam_uniform(level=2, mx=16)
+    dt = 0.005
+    o, d = _pair(cfg)
+    n = d.num_patches
+    cfls = [d.single_step_update(p, 0.0, dt, p, n) for p in range(n)]
+    assert all(c == 0.0 for c in cfls[:-1])
+    c_o = o.update_single_step(2, 0.0, dt)
+    assert cfls[-1] == c_o
+    assert np.array_equal(d.get_q(), o.all_q())
+
+
+@pytest.mark.parametrize("name", ["swirl", "quadrants"])
+def test_regression_pins_on_gpu(gpu_lib, name):
+    """The reference's own regression counters, reproduced by the CUDA path, with
+    the final fields equal to the oracle's."""
+    import json
+    from pathlib import Path
+
+    pins = json.loads((Path(__file__).parent / "golden" / "regression_pins.json").read_text())[name]["values"]
+    cfg = O.swirl_regression() if name == "swirl" else O.quadrants_regression()
+    o, d = _pair(cfg)
+    _assert_same_mesh(o, d)
+    assert np.array_equal(d.get_q(), o.all_q())
+    o.run()
+    d.run()
+    c = d.counters()
+    assert c["count_amr_advance"] == pins["count_amr_advance"]
+    assert d.num_patches == pins["global_num_patches"]
+    assert c["count_amr_new_domain"] == pins["count_amr_new_domain"]
+    _assert_same_mesh(o, d)
+    err = _rel_err(d.get_q(), o.all_q())
+    tol = 1e-11 if name == "swirl" else 0.0
+    assert err <= tol, f"rel err {err:.3e}"
+
+
+def test_amr_radialdam_macro_steps(gpu_lib):
+    """AMR shallow water with subcycling and time interpolation: advance + regrid
+    step by step, comparing mesh and every patch array."""
+    cfg = cases.radialdam_amr(seed=0, minlevel=2, maxlevel=4, mx=16, tfinal=0.05)
+    o, d = _pair(cfg)
+    _assert_same_mesh(o, d)
+    assert np.array_equal(d.get_q(), o.all_q())
+    t, dt = 0.0, 0.9 / (16 * 4) / 1.5
+    for k in range(4):
+        c_o = o.advance(t, dt)
+        c_d = d.advance_all_levels(t, dt)
+        assert c_d == c_o
+        qd, qo = d.get_q(), o.all_q()
+        assert np.array_equal(qd, qo), f"macro step {k}: max diff {np.max(np.abs(qd - qo)):.3e}"
+        t += dt
+        o.regrid()
+        d.regrid()
+        _assert_same_mesh(o, d)
+        assert np.array_equal(d.get_q(), o.all_q()), f"after regrid {k}"
+
+
+def test_mass_conservation_matches_oracle(gpu_lib):
+    cfg = cases.radialdam_uniform(level=2, mx=16)
+    o, d = _pair(cfg)
+    for k in range(5):
+        o.advance(k * 0.002, 0.002)
+        d.advance_all_levels(k * 0.002, 0.002)
+    m_o, m_d = o.conservation(), d.conservation_check()
+    assert np.allclose(m_d, m_o, rtol=1e-13, atol=1e-15)
