@@ -245,32 +245,21 @@ cudaError_t launch_mass(const double* q, int64_t stride, const int32_t* slots, c
 // buffer (leaf order), so that host transfers are one copy each way.
 // ---------------------------------------------------------------------------
 __global__ void gather_kernel(const double* __restrict__ src, int64_t stride, const int32_t* slots, int n,
-                              int64_t psize, double* __restrict__ dst) {
-    const int p = blockIdx.y;
-    if (p >= n) return;
-    const double* s = src + (int64_t)slots[p] * stride;
-    double* d = dst + (int64_t)p * psize;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < psize; k += (int64_t)gridDim.x * blockDim.x)
-        d[k] = s[k];
-}
-
-__global__ void scatter_kernel(double* __restrict__ dst, int64_t stride, const int32_t* slots, int n,
-                               int64_t psize, const double* __restrict__ src) {
-    const int p = blockIdx.y;
-    if (p >= n) return;
-    double* d = dst + (int64_t)slots[p] * stride;
-    const double* s = src + (int64_t)p * psize;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < psize; k += (int64_t)gridDim.x * blockDim.x)
-        d[k] = s[k];
+                              int64_t psize, double* __restrict__ dst, int scatter) {
+    for (int p = blockIdx.x; p < n; p += gridDim.x) {
+        const int64_t a = (int64_t)slots[p] * stride, b = (int64_t)p * psize;
+        for (int64_t k = threadIdx.x; k < psize; k += blockDim.x) {
+            if (scatter) const_cast<double*>(src)[a + k] = dst[b + k];
+            else dst[b + k] = src[a + k];
+        }
+    }
 }
 
 cudaError_t launch_gather(const double* src, int64_t stride, const int32_t* slots, int n, int64_t psize,
                           double* dst, bool scatter, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    const int bx = (int)((psize + 255) / 256 < 8 ? (psize + 255) / 256 : 8);
-    dim3 grid(bx, n);
-    if (scatter) scatter_kernel<<<grid, 256, 0, st>>>(const_cast<double*>(src), stride, slots, n, psize, dst);
-    else gather_kernel<<<grid, 256, 0, st>>>(src, stride, slots, n, psize, dst);
+    const int blocks = n < 148 * 16 ? n : 148 * 16;
+    gather_kernel<<<blocks, 256, 0, st>>>(src, stride, slots, n, psize, dst, scatter ? 1 : 0);
     return cudaGetLastError();
 }
 
