@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = (
     "fcb_ghost_update", "fcb_initialize", "fcb_last_error", "fcb_num_patches", "fcb_patch_info",
     "fcb_patch_neighbors", "fcb_patch_size", "fcb_physical_set_bc", "fcb_regrid", "fcb_run",
     "fcb_set_q", "fcb_single_step_update", "fcb_synchronize", "fcb_timeinterp",
-    "fcb_update_single_step", "fcb_update_single_step_async",
+    "fcb_update_single_step", "fcb_update_single_step_async", "fcb_conservation_sum_noalloc",
 )
 
 
@@ -180,6 +180,8 @@ def lib():
     L.fcb_counters.argtypes = [vp, ctypes.POINTER(_Counters)]
     L.fcb_conservation_check.argtypes = [vp, dp]
     L.fcb_curr_time.argtypes = [vp, dp]
+    L.fcb_conservation_sum_noalloc.argtypes = [vp, sz, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, vp, vp, vp]
     _lib = L
     return L
 

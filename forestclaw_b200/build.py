@@ -30,6 +30,7 @@ SOURCES = {
     "fcb_amr.cu": ["-fmad=false"],
     "fcb_runtime.cu": [],
     "fcb_capi.cu": ["-Xcompiler", "-fvisibility=default"],
+    "fcb_noalloc.cu": ["-fmad=false"],
 }
 HEADERS = ["fcb_device.h", "fcb_solvers.cuh", "fcb_forest.hpp", "fcb_runtime.hpp"]
 

@@ -37,6 +37,10 @@ int need(const void* p, const char* what) {
 }
 }  // namespace
 
+namespace fcb {
+__attribute__((visibility("hidden"))) void set_last_error(const std::string& msg) { g_error = msg; }
+}  // namespace fcb
+
 extern "C" {
 
 const char* fcb_last_error(void) { return g_error.c_str(); }

@@ -162,6 +162,23 @@ int fcb_counters(fcb_context_t* ctx, fcb_counters_t* out);
 /* Mass diagnostic (fclaw2d_clawpatch46_diagnostics.f:13-58): Kahan sum of
  * q*dx*dy per component over all leaves; sums has meqn entries. */
 int fcb_conservation_check(fcb_context_t* ctx, double* sums);
+/* Mass sums that allocate no device memory.  No counterpart in the reference:
+ * it exists for callers that must not allocate while they run (a serving loop
+ * whose HBM is fully committed to admitted solves, code that must not let a
+ * cudaMalloc/cudaFree synchronise the device, hosts that own all device memory).
+ * Inputs are the caller's device arrays: npatches patch arrays of
+ * meqn*(mx+2mbc)*(my+2mbc) doubles in the layout above, patch_stride doubles
+ * apart, and one cell area (dx*dy) per patch; d_sums receives meqn doubles
+ * (Kahan over each patch's interior, then over the patches in order, the same
+ * sequence as fcb_conservation_check).  Work is enqueued on cuda_stream.
+ * Per-patch partial sums live in a fixed array of 262,144 doubles (2 MiB)
+ * inside the library, held by every GPU that loads it; npatches*meqn above
+ * that is rejected with FCB_ERR_INVALID.  The first call on each device looks
+ * up that array's address, so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller. */
+int fcb_conservation_sum_noalloc(const double* d_q, size_t patch_stride, int npatches, int mx, int my, int mbc,
+                                 int meqn, const double* d_area, double* d_sums, void* cuda_stream);
 /* Current time of the run loop. */
 int fcb_curr_time(fcb_context_t* ctx, double* t);
 /* Wait for all work of the context. */
