@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--mx", type=int, default=16)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
+    p.add_argument("--step-variant", type=int, default=0, help="0 library's choice, 1 CTA rows, 2 warp")
     return p.parse_args()
 
 
@@ -203,6 +204,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     stream = torch.cuda.current_stream()
     opts = workloads.uniform_swirl(args.level, args.mx)
+    opts.step_variant = args.step_variant
     dt = workloads.swirl_dt(args.level, args.mx)
     s = fcb.Solver(opts, stream=stream.cuda_stream)
     s.initialize()

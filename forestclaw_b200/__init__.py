@@ -58,6 +58,7 @@ class _Options(ctypes.Structure):
         ("solver_kind", ctypes.c_int), ("problem", ctypes.c_int),
         ("grav", ctypes.c_double), ("gamma", ctypes.c_double),
         ("problem_params", ctypes.c_double * 32),
+        ("step_variant", ctypes.c_int),
     ]
 
 
@@ -107,13 +108,15 @@ class Options:
     grav: float = 1.0
     gamma: float = 1.4
     problem_params: Sequence[float] = field(default_factory=tuple)
+    # step kernel form: 0 = library's choice, 1 = CTA rows, 2 = warp-synchronous
+    step_variant: int = 0
 
     def to_c(self) -> _Options:
         o = _Options()
         for name in ("mx", "my", "mbc", "meqn", "maux", "refinement_criteria", "threshold_variable",
                      "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
                      "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
-                     "reduce_cfl", "solver_kind", "problem"):
+                     "reduce_cfl", "solver_kind", "problem", "step_variant"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
                      "desired_cfl", "grav", "gamma"):

@@ -26,6 +26,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # per-source extra flags
 SOURCES = {
     "fcb_step.cu": ["-fmad=false"],
+    "fcb_step_warp.cu": ["-fmad=false"],
     "fcb_ghost.cu": ["-fmad=false"],
     "fcb_amr.cu": ["-fmad=false"],
     "fcb_runtime.cu": [],

@@ -62,8 +62,9 @@ struct GhostArgs {
     double* qti;      // arena of time-interpolated solutions
     int64_t stride;
     int mx, my, mbc, meqn;
-    const GhostOp* ops;
-    int nops;
+    const GhostOp* ops;    // records of the wave, sorted by destination patch
+    const int32_t* groups; // group k = records [groups[k], groups[k+1]) (absolute indices into ops)
+    int ngroups;
 };
 
 enum Problem : int32_t { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2 };

@@ -1,7 +1,7 @@
 // Ghost-cell fill kernels (copy / average / interpolate across faces and
 // corners, physical boundary conditions) and time interpolation.
 //
-// One warp executes one GhostOp record; a launch executes one "wave" of
+// A warp executes the records of one destination patch; a launch executes one "wave" of
 // records that the host has proven independent (no record in a wave reads or
 // writes cells another record of the same wave writes), so the result equals
 // the reference's sequential order.
@@ -63,11 +63,8 @@ __device__ __forceinline__ void interp_cell(const PatchView& C, const PatchView&
 
 }  // namespace
 
-__global__ void ghost_wave_kernel(const GhostArgs a) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= a.nops) return;
-    const GhostOp op = a.ops[warp];
+// One record executed by the 32 lanes of a warp.
+__device__ __forceinline__ void ghost_op(const GhostArgs& a, const GhostOp& op, int lane) {
     const int mx = a.mx, my = a.my, mbc = a.mbc, meqn = a.meqn;
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
     PatchView D{(op.dst_ti ? a.qti : a.q) + (int64_t)op.dst * a.stride, mx, my, mbc, nx, ny};
@@ -216,11 +213,183 @@ __global__ void ghost_wave_kernel(const GhostArgs a) {
     }
 }
 
+// Number of cells one lane-level work item of a record covers (0 for the
+// physical-boundary record, which keeps its whole-warp form: its sides read
+// cells that the previous side writes).
+__device__ __forceinline__ int op_cells(const GhostArgs& a, const GhostOp& op) {
+    const int mx = a.mx, my = a.my, mbc = a.mbc, meqn = a.meqn;
+    switch (op.type) {
+        case OP_COPY_FACE: return (op.face < 2 ? mbc * my : mx * mbc) * meqn;
+        case OP_COPY_CORNER:
+        case OP_AVERAGE_CORNER: return mbc * mbc * meqn;
+        case OP_AVERAGE_FACE: return (op.face < 2 ? my : mx) * mbc * meqn;
+        case OP_INTERP_FACE: return mx * (mbc / 2) * meqn;
+        case OP_INTERP_CORNER: return (mbc / 2) * (mbc / 2) * meqn;
+        default: return 0;
+    }
+}
+
+// Work item k of a record (the same decomposition as ghost_op's loops).  Copy
+// and average items return their value and destination so the caller can
+// issue several loads before the stores; interpolation items store their four
+// fine cells themselves and return nullptr.
+__device__ __forceinline__ double* op_cell(const GhostArgs& a, const GhostOp& op, int k, double& v) {
+    const int mx = a.mx, my = a.my, mbc = a.mbc;
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    PatchView D{(op.dst_ti ? a.qti : a.q) + (int64_t)op.dst * a.stride, mx, my, mbc, nx, ny};
+    PatchView S{(op.src_ti ? a.qti : a.q) + (int64_t)op.src * a.stride, mx, my, mbc, nx, ny};
+    switch (op.type) {
+        case OP_COPY_FACE: {
+            int i0, j0, w, h;
+            if (op.face == 0) { i0 = 1 - mbc; j0 = 1; w = mbc; h = my; }
+            else if (op.face == 1) { i0 = mx + 1; j0 = 1; w = mbc; h = my; }
+            else if (op.face == 2) { i0 = 1; j0 = 1 - mbc; w = mx; h = mbc; }
+            else { i0 = 1; j0 = my + 1; w = mx; h = mbc; }
+            const int m = k / (w * h), rem = k - m * w * h, jj = rem / w, ii = rem - jj * w;
+            const int i = i0 + ii, j = j0 + jj;
+            v = S.at(i + op.dx, j + op.dy, m);
+            return &D.at(i, j, m);
+        }
+        case OP_COPY_CORNER:
+        case OP_AVERAGE_CORNER: {
+            const int m = k / (mbc * mbc), rem = k - m * mbc * mbc;
+            const int ibc = rem / mbc + 1, jbc = rem % mbc + 1;
+            int i1, j1;
+            if (op.face == 0) { i1 = 1 - ibc; j1 = 1 - jbc; }
+            else if (op.face == 1) { i1 = mx + ibc; j1 = 1 - jbc; }
+            else if (op.face == 2) { i1 = 1 - ibc; j1 = my + jbc; }
+            else { i1 = mx + ibc; j1 = my + jbc; }
+            if (op.type == OP_COPY_CORNER) {
+                v = S.at(i1 + op.dx, j1 + op.dy, m);
+            } else {
+                const int fi = 2 * i1 + op.dx, fj = 2 * j1 + op.dy;
+                double sum = 0;
+                sum = sum + S.at(fi, fj, m);
+                sum = sum + S.at(fi + 1, fj, m);
+                sum = sum + S.at(fi, fj + 1, m);
+                sum = sum + S.at(fi + 1, fj + 1, m);
+                v = sum / 4.0;
+            }
+            return &D.at(i1, j1, m);
+        }
+        case OP_AVERAGE_FACE: {
+            const int idir = op.face / 2;
+            const int along = idir == 0 ? my : mx;
+            const int m = k / (along * mbc), rem = k - m * along * mbc;
+            const int t = rem / mbc + 1, bc = rem % mbc + 1;
+            int ic, jc;
+            if (idir == 0) { jc = t; ic = (op.face == 0) ? 1 - bc : mx + bc; }
+            else { ic = t; jc = (op.face == 2) ? 1 - bc : my + bc; }
+            const int fi = 2 * ic + op.dx, fj = 2 * jc + op.dy;
+            if (fi < 1 || fi + 1 > mx || fj < 1 || fj + 1 > my) return nullptr;  // is_valid_average
+            double sum = 0;
+            sum = sum + S.at(fi, fj, m);
+            sum = sum + S.at(fi + 1, fj, m);
+            sum = sum + S.at(fi, fj + 1, m);
+            sum = sum + S.at(fi + 1, fj + 1, m);
+            v = sum / 4.0;
+            return &D.at(ic, jc, m);
+        }
+        case OP_INTERP_FACE: {
+            const int idir = op.face / 2;
+            const int nb = mbc / 2;
+            const int along = mx;  // the reference loops jc = 1..mx for idir = 0 as well
+            const int m = k / (along * nb), rem = k - m * along * nb;
+            const int t = rem / nb + 1, b = rem % nb + 1;
+            int ic, jc;
+            if (idir == 0) { jc = t; ic = (op.face == 0) ? b : mx - b + 1; }
+            else { ic = t; jc = (op.face == 2) ? b : my - b + 1; }
+            const int fi = 2 * ic + op.dx, fj = 2 * jc + op.dy;
+            if (fi < 1 - mbc || fi + 1 > mx + mbc || fj < 1 - mbc || fj + 1 > my + mbc) return nullptr;
+            interp_cell(S, D, m, ic, jc, fi, fj);
+            return nullptr;
+        }
+        case OP_INTERP_CORNER: {
+            const int nb = mbc / 2;
+            const int m = k / (nb * nb), rem = k - m * nb * nb;
+            const int ibc = rem / nb + 1, jbc = rem % nb + 1;
+            int ic, jc;
+            if (op.face == 0) { ic = ibc; jc = jbc; }
+            else if (op.face == 1) { ic = mx - ibc + 1; jc = jbc; }
+            else if (op.face == 2) { ic = ibc; jc = my - jbc + 1; }
+            else { ic = mx - ibc + 1; jc = my - jbc + 1; }
+            interp_cell(S, D, m, ic, jc, 2 * ic + op.dx, 2 * jc + op.dy);
+            return nullptr;
+        }
+        default: return nullptr;
+    }
+}
+
+// One warp per group.  The records of a group share their destination patch;
+// the host proved every record of a wave independent of the others (none reads
+// or writes a cell another writes), so their work items may run in any order:
+// the warp lays the items of up to 32 records out in one flat index range
+// (prefix sum of op_cells over the lanes) and each lane takes items lane,
+// lane+32, ...  UNROLL items per lane issue their loads before any store.
+constexpr int GHOST_TPB = 256;
+constexpr int GHOST_UNROLL = 4;
+
+__global__ void __launch_bounds__(GHOST_TPB) ghost_wave_kernel(const GhostArgs a) {
+    __shared__ GhostOp s_ops[GHOST_TPB / 32][32];
+    __shared__ int s_end[GHOST_TPB / 32][32];
+    const int wl = threadIdx.x >> 5;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= a.ngroups) return;
+    const int b = a.groups[warp], e = a.groups[warp + 1];
+    for (int base = b; base < e; base += 32) {
+        const int cnt = min(32, e - base);
+        int n = 0;
+        bool phys = false;
+        if (lane < cnt) {
+            const GhostOp op = a.ops[base + lane];
+            s_ops[wl][lane] = op;
+            phys = op.type == OP_PHYSBC;
+            n = op_cells(a, op);
+        }
+        int incl = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        s_end[wl][lane] = incl;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();
+        int r = 0;  // record of the current item; items are visited in increasing order
+        for (int f0 = lane; f0 < total; f0 += 32 * GHOST_UNROLL) {
+            double v[GHOST_UNROLL];
+            double* dst[GHOST_UNROLL];
+#pragma unroll
+            for (int u = 0; u < GHOST_UNROLL; ++u) {
+                const int f = f0 + 32 * u;
+                dst[u] = nullptr;
+                v[u] = 0.0;
+                if (f < total) {
+                    while (f >= s_end[wl][r]) ++r;
+                    const int first = r > 0 ? s_end[wl][r - 1] : 0;
+                    dst[u] = op_cell(a, s_ops[wl][r], f - first, v[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < GHOST_UNROLL; ++u)
+                if (dst[u]) *dst[u] = v[u];
+        }
+        // physical-boundary records (independent of the items above)
+        unsigned pm = __ballot_sync(0xffffffffu, phys);
+        while (pm) {
+            const int l = __ffs(pm) - 1;
+            pm &= pm - 1;
+            ghost_op(a, s_ops[wl][l], lane);
+        }
+        __syncwarp();
+    }
+}
+
 cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st) {
-    if (a.nops <= 0) return cudaSuccess;
-    const int tpb = 256;
-    const int blocks = (a.nops * 32 + tpb - 1) / tpb;
-    ghost_wave_kernel<<<blocks, tpb, 0, st>>>(a);
+    if (a.ngroups <= 0) return cudaSuccess;
+    const int blocks = (int)(((int64_t)a.ngroups * 32 + GHOST_TPB - 1) / GHOST_TPB);
+    ghost_wave_kernel<<<blocks, GHOST_TPB, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -64,6 +64,8 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
     if (opt_.problem == FCB_PROBLEM_RADIALDAM && opt_.solver_kind != FCB_SOLVER_SWE_ROE) bad("radialdam needs SWE");
     if (opt_.problem == FCB_PROBLEM_QUADRANTS && opt_.solver_kind != FCB_SOLVER_EULER4_ROE) bad("quadrants needs Euler");
     aux_kind_ = (opt_.solver_kind == FCB_SOLVER_ADVECTION) ? AUX_SWIRL : AUX_NONE;
+    if (opt_.step_variant < 0 || opt_.step_variant > 2) bad("step_variant must be 0, 1 or 2");
+    if ((opt_.mx & (opt_.mx - 1)) != 0) bad("mx must be a power of two");
     nx_ = opt_.mx + 2 * opt_.mbc;
     ny_ = opt_.my + 2 * opt_.mbc;
     const int64_t ps = (int64_t)opt_.meqn * nx_ * ny_;
@@ -183,6 +185,7 @@ void Context::mesh_changed() {
     check(cudaMemcpy(d_all_slots_.p, all.data(), all.size() * 4, cudaMemcpyHostToDevice), "all slots");
     plans_.clear();
     h_ops_.clear();
+    h_groups_.clear();
     ops_dirty_ = true;
 }
 
@@ -390,6 +393,19 @@ const GhostPlan& Context::plan(int minlevel, int maxlevel, int ti) {
     std::vector<GhostOp> sorted(ops.size());
     std::vector<int> pos(g.wave_begin.begin(), g.wave_begin.end() - (nw ? 1 : 0));
     for (size_t k = 0; k < ops.size(); ++k) sorted[pos[wave[k]]++] = ops[k];
+    // within a wave, records with the same destination patch form one group
+    g.first_group = h_groups_.size();
+    g.group_begin.assign(nw + 1, 0);
+    for (int w = 0; w < nw; ++w) {
+        auto b = sorted.begin() + g.wave_begin[w], e = sorted.begin() + g.wave_begin[w + 1];
+        std::stable_sort(b, e, [](const GhostOp& x, const GhostOp& y) { return x.dst < y.dst; });
+        g.group_begin[w] = (int)(h_groups_.size() - g.first_group);
+        for (int k = g.wave_begin[w]; k < g.wave_begin[w + 1]; ++k)
+            if (k == g.wave_begin[w] || sorted[k].dst != sorted[k - 1].dst)
+                h_groups_.push_back((int32_t)(g.first + k));
+        h_groups_.push_back((int32_t)(g.first + g.wave_begin[w + 1]));  // end marker of the wave
+    }
+    g.group_begin[nw] = (int)(h_groups_.size() - g.first_group);
     h_ops_.insert(h_ops_.end(), sorted.begin(), sorted.end());
     ops_dirty_ = true;
     return plans_.emplace(key, std::move(g)).first->second;
@@ -398,9 +414,13 @@ const GhostPlan& Context::plan(int minlevel, int maxlevel, int ti) {
 void Context::run_plan(const GhostPlan& g) {
     if (ops_dirty_) {
         d_ops_.reserve(std::max<size_t>(1, h_ops_.size()));
+        d_groups_.reserve(std::max<size_t>(1, h_groups_.size()));
         check(cudaStreamSynchronize(st_), "sync");
         if (!h_ops_.empty())
             check(cudaMemcpy(d_ops_.p, h_ops_.data(), h_ops_.size() * sizeof(GhostOp), cudaMemcpyHostToDevice), "ops");
+        if (!h_groups_.empty())
+            check(cudaMemcpy(d_groups_.p, h_groups_.data(), h_groups_.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+                  "groups");
         ops_dirty_ = false;
     }
     const int nw = (int)g.wave_begin.size() - 1;
@@ -410,8 +430,9 @@ void Context::run_plan(const GhostPlan& g) {
         a.qti = d_qti_;
         a.stride = stride_;
         a.mx = opt_.mx; a.my = opt_.my; a.mbc = opt_.mbc; a.meqn = opt_.meqn;
-        a.ops = d_ops_.p + g.first + g.wave_begin[w];
-        a.nops = g.wave_begin[w + 1] - g.wave_begin[w];
+        a.ops = d_ops_.p;
+        a.groups = d_groups_.p + g.first_group + g.group_begin[w];  // group starts, then an end marker
+        a.ngroups = g.group_begin[w + 1] - g.group_begin[w] - 1;
         check(launch_ghost_wave(a, st_), "ghost wave");
         ++cnt_.count_ghost_waves;
         ++cnt_.count_kernel_launches;
@@ -440,6 +461,10 @@ void Context::physical_set_bc(int level, int time_interp) {
     GhostPlan g;
     g.first = h_ops_.size();
     g.wave_begin = {0, (int)ops.size()};
+    g.first_group = h_groups_.size();
+    for (size_t k = 0; k < ops.size(); ++k) h_groups_.push_back((int32_t)(g.first + k));
+    h_groups_.push_back((int32_t)(g.first + ops.size()));
+    g.group_begin = {0, (int)ops.size() + 1};
     h_ops_.insert(h_ops_.end(), ops.begin(), ops.end());
     ops_dirty_ = true;
     run_plan(g);
@@ -476,7 +501,16 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     a.gamma = opt_.gamma;
     a.gamma1 = opt_.gamma - 1.0;
     a.cfl_out = cfl_slot;
-    check(launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_), "step");
+    // The warp form computes each swirl velocity node once, which equals the
+    // reference's per-cell evaluations because the unit-square mesh with mx a
+    // power of two is dyadic (xll + dx == next xll exactly); checked at creation.
+    cudaError_t e = cudaErrorNotSupported;
+    if (aux_kind_ == AUX_SWIRL && opt_.step_variant == 2) e = launch_step_warp_swirl(opt_.mx, opt_.mbc, a, st_);
+    if (e == cudaErrorNotSupported) {
+        if (opt_.step_variant == 2) throw Error(FCB_ERR_INVALID, "no warp-synchronous step for this case");
+        e = launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_);
+    }
+    check(e, "step");
     cnt_.count_single_step += n;
     ++cnt_.count_kernel_launches;
 }

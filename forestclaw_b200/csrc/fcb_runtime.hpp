@@ -24,6 +24,7 @@ struct Error : std::runtime_error {
 // Kernel launchers (fcb_step.cu, fcb_ghost.cu, fcb_amr.cu)
 cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
                         cudaStream_t st);
+cudaError_t launch_step_warp_swirl(int mx, int mbc, const StepArgs& a, cudaStream_t st);
 struct GhostArgs;
 cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st);
 cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64_t stride,
@@ -52,8 +53,10 @@ struct DevBuf {
 };
 
 struct GhostPlan {
-    std::vector<int> wave_begin;  // op offsets of each wave, size nwaves+1
-    size_t first = 0;             // first op of the plan in the context's op buffer
+    std::vector<int> wave_begin;   // op offsets of each wave, size nwaves+1
+    size_t first = 0;              // first op of the plan in the context's op buffer
+    std::vector<int> group_begin;  // per wave: first group, size nwaves+1
+    size_t first_group = 0;        // first group of the plan in the context's group buffer
 };
 
 class Context {
@@ -131,6 +134,8 @@ class Context {
     std::map<std::tuple<int, int, int>, GhostPlan> plans_;
     std::vector<GhostOp> h_ops_;
     DevBuf<GhostOp> d_ops_;
+    std::vector<int32_t> h_groups_;  // absolute op indices; one extra end marker per plan wave
+    DevBuf<int32_t> d_groups_;
     bool ops_dirty_ = true;
     // scalars
     unsigned long long* d_cfl_ = nullptr;  // [0]: advance accumulator, [1]: level / batch

@@ -34,9 +34,12 @@ struct AdvectionSolver {
             wave[mw][0] = delta;
             s[mw] = speed;
         }
-        double am = 0.0, ap = 0.0;
+        // the reference starts both sums at 0; starting at the first term differs
+        // only in the sign of a zero result
+        double am = dmin(s[0], 0.0) * wave[0][0];
+        double ap = dmax(s[0], 0.0) * wave[0][0];
 #pragma unroll
-        for (int mw = 0; mw < W; ++mw) {
+        for (int mw = 1; mw < W; ++mw) {
             am = am + dmin(s[mw], 0.0) * wave[mw][0];
             ap = ap + dmax(s[mw], 0.0) * wave[mw][0];
         }
@@ -121,9 +124,9 @@ struct SweRoeSolver {
     done:
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            double df = 0.0;
+            double df = s[0] * wave[0][m];
 #pragma unroll
-            for (int mw = 0; mw < W; ++mw) df = df + s[mw] * wave[mw][m];
+            for (int mw = 1; mw < W; ++mw) df = df + s[mw] * wave[mw][m];
             amdq[m] = am[m];
             apdq[m] = df - am[m];
         }
@@ -142,9 +145,9 @@ struct SweRoeSolver {
         waveb[0][2] = a3; waveb[mu][2] = a3 * u; waveb[mv][2] = a3 * (v + a); sb[2] = v + a;
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            double m1 = 0.0, p1 = 0.0;
+            double m1 = dmin(sb[0], 0.0) * waveb[m][0], p1 = dmax(sb[0], 0.0) * waveb[m][0];
 #pragma unroll
-            for (int mw = 0; mw < 3; ++mw) {
+            for (int mw = 1; mw < 3; ++mw) {
                 m1 = m1 + dmin(sb[mw], 0.0) * waveb[m][mw];
                 p1 = p1 + dmax(sb[mw], 0.0) * waveb[m][mw];
             }
@@ -250,9 +253,9 @@ struct Euler4RoeSolver {
     done:
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            double df = 0.0;
+            double df = s[0] * wave[0][m];
 #pragma unroll
-            for (int mw = 0; mw < W; ++mw) df = df + s[mw] * wave[mw][m];
+            for (int mw = 1; mw < W; ++mw) df = df + s[mw] * wave[mw][m];
             amdq[m] = am[m];
             apdq[m] = df - am[m];
         }
@@ -275,9 +278,9 @@ struct Euler4RoeSolver {
         sb[2] = v + a;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            double m1 = 0.0, p1 = 0.0;
+            double m1 = dmin(sb[0], 0.0) * waveb[m][0], p1 = dmax(sb[0], 0.0) * waveb[m][0];
 #pragma unroll
-            for (int mw = 0; mw < 3; ++mw) {
+            for (int mw = 1; mw < 3; ++mw) {
                 m1 = m1 + dmin(sb[mw], 0.0) * waveb[m][mw];
                 p1 = p1 + dmax(sb[mw], 0.0) * waveb[m][mw];
             }

@@ -39,7 +39,7 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double 
     atomicMax(p, (unsigned long long)__double_as_longlong(v));
 }
 
-template <int NX, int NY, int PPB, int M, int W, int NAUX>
+template <int NX, int NY, int PPB, int M, int W, int NAUX, bool PSI>
 struct StepSmem {
     static constexpr int QROW = 0;
     static constexpr int XW = QROW + PPB * NX * M;
@@ -49,7 +49,8 @@ struct StepSmem {
     static constexpr int GY = FX + 3 * PPB * NX * 2 * M;
     static constexpr int AUX = GY + PPB * NX * 2 * M;
     static constexpr int TAB = AUX + PPB * NAUX * NY * NX;
-    static constexpr int TOTAL = TAB + PPB * 4 * NX;
+    static constexpr int PSIT = TAB + (PSI ? PPB * 2 * (NX + 1) : 0);
+    static constexpr int TOTAL = PSIT + (PSI ? PPB * (NY + 1) * (NX + 1) : 0);
 };
 
 }  // namespace
@@ -63,7 +64,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     constexpr int NX = MX + 2 * MBC;
     constexpr int NY = NX;
     constexpr int PPB = TPB / NX;
-    using L = StepSmem<NX, NY, PPB, M, W, NAUX>;
+    using L = StepSmem<NX, NY, PPB, M, W, NAUX, AUXK == AUX_SWIRL>;
     extern __shared__ double smem[];
     double* s_qrow = smem + L::QROW;  // [PPB][NX][M]
     double* s_xw = smem + L::XW;      // [PPB][NX][W][M]
@@ -72,7 +73,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     double* s_fx = smem + L::FX;      // [3][PPB][NX][2][M]
     double* s_gy = smem + L::GY;      // [PPB][NX][2][M]
     double* s_aux = smem + L::AUX;    // [PPB][NAUX][NY][NX]
-    double* s_tab = smem + L::TAB;    // [PPB][4][NX]
+    double* s_tab = smem + L::TAB;    // [PPB][2][NX+1] (swirl)
+    double* s_psi = smem + L::PSIT;   // [PPB][NY+1][NX+1] (swirl)
 
     const int t = threadIdx.x;
     const int pl = t / NX;
@@ -95,30 +97,39 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         // swirl/user_4.6/b4step2.f with swirl/psi.f:
         //   u(i,j) = vty*(psi(xll,yll+dy) - psi(xll,yll)),  v(i,j) = -vtx*(psi(xll+dx,yll) - psi(xll,yll))
         //   psi(x,y) = (sin(pi x)**2 * sin(pi y)**2)/pi
+        // On the dyadic unit-square mesh (mx a power of two) xll + dx is the next
+        // node's xll exactly, so psi is evaluated once per node: P(c,r) at the
+        // lower-left corner of cell (c,r), c in [0,NX], r in [0,NY].
         constexpr double pi = 3.141592653589793;  // 4*atan(1) in double precision
-        double* tab = s_tab + pl * 4 * NX;
+        double* tx = s_tab + pl * 2 * (NX + 1);
+        double* ty = tx + (NX + 1);
+        double* P = s_psi + pl * (NY + 1) * (NX + 1);
         if (active) {
-            const double xll = meta.xlower + (double)(c - MBC) * meta.dx;
-            const double yll = meta.ylower + (double)(c - MBC) * meta.dy;  // row c of the table
-            const double sxa = sin(pi * xll), sxb = sin(pi * (xll + meta.dx));
-            const double sya = sin(pi * yll), syb = sin(pi * (yll + meta.dy));
-            tab[0 * NX + c] = sxa * sxa;
-            tab[1 * NX + c] = sxb * sxb;
-            tab[2 * NX + c] = sya * sya;
-            tab[3 * NX + c] = syb * syb;
+            for (int n = c; n <= NX; n += NX) {
+                const double x = meta.xlower + (double)(n - MBC) * meta.dx;
+                const double y = meta.ylower + (double)(n - MBC) * meta.dy;
+                const double sx = sin(pi * x), sy = sin(pi * y);
+                tx[n] = sx * sx;
+                ty[n] = sy * sy;
+            }
+        }
+        __syncthreads();
+        if (active) {
+            for (int n = c; n <= NX; n += NX) {
+                const double sx2 = tx[n];
+                for (int r = 0; r <= NY; ++r) P[r * (NX + 1) + n] = (sx2 * ty[r]) / pi;
+            }
         }
         __syncthreads();
         if (active) {
             const double vty = a.vt / meta.dy;
             const double vtx = a.vt / meta.dx;
-            const double sx2a = tab[0 * NX + c], sx2b = tab[1 * NX + c];
             double* au = s_aux + (pl * NAUX + 0) * NY * NX;
             double* av = s_aux + (pl * NAUX + 1) * NY * NX;
             for (int r = 0; r < NY; ++r) {
-                const double sy2a = tab[2 * NX + r], sy2b = tab[3 * NX + r];
-                const double pij = (sx2a * sy2a) / pi;
-                au[r * NX + c] = vty * ((sx2a * sy2b) / pi - pij);
-                av[r * NX + c] = -vtx * ((sx2b * sy2a) / pi - pij);
+                const double pij = P[r * (NX + 1) + c];
+                au[r * NX + c] = vty * (P[(r + 1) * (NX + 1) + c] - pij);
+                av[r * NX + c] = -vtx * (P[r * (NX + 1) + c + 1] - pij);
             }
         }
     } else if constexpr (AUXK == AUX_STORED) {
@@ -185,9 +196,9 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 sol.rpn2(2, q_m1, q_n, AUXV(1, c, s), yw_n, ys_n, yam_n, yap_n, yR_n);
 #pragma unroll
                 for (int mw = 0; mw < W; ++mw) {
-                    double d = 0.0;
+                    double d = yw_f[mw][0] * yw_n[mw][0];
 #pragma unroll
-                    for (int m = 0; m < M; ++m) d = d + yw_f[mw][m] * yw_n[mw][m];
+                    for (int m = 1; m < M; ++m) d = d + yw_f[mw][m] * yw_n[mw][m];
                     ydotr[mw] = d;  // dot(w(s-1), w(s))
                 }
             }
@@ -236,9 +247,9 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
 #pragma unroll
                     for (int mw = 0; mw < W; ++mw) {
                         if (a.mthlim[mw] == 0) continue;
-                        double wn2 = 0.0;
+                        double wn2 = yw_f[mw][0] * yw_f[mw][0];
 #pragma unroll
-                        for (int m = 0; m < M; ++m) wn2 = wn2 + yw_f[mw][m] * yw_f[mw][m];
+                        for (int m = 1; m < M; ++m) wn2 = wn2 + yw_f[mw][m] * yw_f[mw][m];
                         if (wn2 == 0.0) continue;
                         const double r = (ys_f[mw] > 0.0) ? ydotl[mw] / wn2 : ydotr[mw] / wn2;
                         const double phi = limiter_phi(a.mthlim[mw], r);
@@ -248,9 +259,13 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 }
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
-                    double acc = 0.0;
+                    double acc;
+                    {
+                        const double as = fabs(ys_f[0]);
+                        acc = as * (1.0 - as * dtdyave) * w[0][m];
+                    }
 #pragma unroll
-                    for (int mw = 0; mw < W; ++mw) {
+                    for (int mw = 1; mw < W; ++mw) {
                         const double as = fabs(ys_f[mw]);
                         acc = acc + as * (1.0 - as * dtdyave) * w[mw][m];
                     }
@@ -260,8 +275,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             double fm_[M], fp_[M], am[M], ap[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) {
-                double fmv = 0.0, fpv = 0.0;
-                if (f <= NY - 2) { fmv = fmv + yam_f[m]; fpv = fpv - yap_f[m]; }
+                double fmv = (f <= NY - 2) ? yam_f[m] : 0.0;
+                double fpv = (f <= NY - 2) ? -yap_f[m] : 0.0;
                 if (a.order0 == 2) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
                 fm_[m] = fmv; fp_[m] = fpv;
                 am[m] = yam_f[m]; ap[m] = yap_f[m];
@@ -286,8 +301,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             if (f - 1 >= 1) {
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
-                    GYd_r[m] = (0.0 - gLm[m]) - gRm_prev[m];
-                    GYu_r[m] = (0.0 - gLp[m]) - gRp_prev[m];
+                    GYd_r[m] = -gLm[m] - gRm_prev[m];
+                    GYu_r[m] = -gLp[m] - gRp_prev[m];
                 }
             }
 #pragma unroll
@@ -331,9 +346,11 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
 #pragma unroll
                     for (int mw = 0; mw < W; ++mw) {
                         if (a.mthlim[mw] == 0) continue;
-                        double wn2 = 0.0, dl = 0.0, dr = 0.0;
+                        double wn2 = xwl[mw][0] * xwl[mw][0];
+                        double dl = xw[((c - 1) * W + mw) * M + 0] * xwl[mw][0];
+                        double dr = xwl[mw][0] * xw[((c + 1) * W + mw) * M + 0];
 #pragma unroll
-                        for (int m = 0; m < M; ++m) {
+                        for (int m = 1; m < M; ++m) {
                             const double wc = xwl[mw][m];
                             wn2 = wn2 + wc * wc;
                             dl = dl + xw[((c - 1) * W + mw) * M + m] * wc;
@@ -348,9 +365,13 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 }
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
-                    double acc = 0.0;
+                    double acc;
+                    {
+                        const double as = fabs(xsl[0]);
+                        acc = as * (1.0 - as * dtdxave) * xwl[0][m];
+                    }
 #pragma unroll
-                    for (int mw = 0; mw < W; ++mw) {
+                    for (int mw = 1; mw < W; ++mw) {
                         const double as = fabs(xsl[mw]);
                         acc = acc + as * (1.0 - as * dtdxave) * xwl[mw][m];
                     }
@@ -360,8 +381,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             double am[M], ap[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) {
-                double fmv = 0.0, fpv = 0.0;
-                if (c <= NX - 2) { fmv = fmv + xam[m]; fpv = fpv - xap[m]; }
+                double fmv = (c <= NX - 2) ? xam[m] : 0.0;
+                double fpv = (c <= NX - 2) ? -xap[m] : 0.0;
                 if (a.order0 == 2) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
                 fxs[(c * 2 + 0) * M + m] = fmv;
                 fxs[(c * 2 + 1) * M + m] = fpv;
@@ -402,11 +423,12 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             double gxd = 0.0, gxu = 0.0;
             if (xint) {
                 if (c + 1 <= NX - 1) {
-                    gxd = gxd - gl[((c + 1) * 2 + 0) * M + m];
-                    gxu = gxu - gl[((c + 1) * 2 + 1) * M + m];
+                    gxd = -gl[((c + 1) * 2 + 0) * M + m] - gRmx[m];
+                    gxu = -gl[((c + 1) * 2 + 1) * M + m] - gRpx[m];
+                } else {
+                    gxd = -gRmx[m];
+                    gxu = -gRpx[m];
                 }
-                gxd = gxd - gRmx[m];
-                gxu = gxu - gRpx[m];
             }
             GXs_n[m] = GXu_prev[m] + gxd;
             GXu_prev[m] = gxu;
@@ -465,7 +487,7 @@ cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
     constexpr int NX = MX + 2 * MBC;
     constexpr int PPB = TPB / NX;
     static_assert(PPB >= 1, "patch wider than the CTA");
-    using L = StepSmem<NX, NX, PPB, SOL::M, SOL::W, NAUX>;
+    using L = StepSmem<NX, NX, PPB, SOL::M, SOL::W, NAUX, AUXK == AUX_SWIRL>;
     const size_t bytes = (size_t)L::TOTAL * sizeof(double);
     static bool configured = false;
     if (!configured) {

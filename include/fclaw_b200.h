@@ -87,6 +87,10 @@ typedef struct fcb_options {
     double grav;               /* SWE /cparam/ grav */
     double gamma;              /* Euler /cparam/ gamma; gamma1 = gamma - 1 */
     double problem_params[32];
+    /* step kernel form: 0 = chosen by the library, 1 = one CTA per patch group
+     * (rows through shared memory), 2 = warp-synchronous (swirl advection,
+     * mx = 8, 16, 32); both give identical results */
+    int step_variant;
 } fcb_options_t;
 
 typedef struct fcb_counters {

@@ -36,11 +36,25 @@ def _assert_same_mesh(o, d):
     assert d.leaves() == o.leaves()
 
 
+def _pair_variant(cfg, variant):
+    import forestclaw_b200 as fcb
+
+    opts = cases.to_options(cfg)
+    opts.step_variant = variant
+    o = O.OracleSolver(cfg)
+    d = fcb.Solver(opts)
+    o.initialize()
+    d.initialize()
+    return o, d
+
+
+@pytest.mark.parametrize("variant", [1, 2])
 @pytest.mark.parametrize("mx", [8, 16, 32])
-def test_uniform_swirl_steps(gpu_lib, mx):
+def test_uniform_swirl_steps(gpu_lib, mx, variant):
+    """Both step-kernel forms (CTA rows, warp-synchronous) against the oracle."""
     cfg = cases.swirl_uniform(level=3, mx=mx)
     dt = cases.swirl_dt(level=3, mx=mx)
-    o, d = _pair(cfg)
+    o, d = _pair_variant(cfg, variant)
     _assert_same_mesh(o, d)
     assert np.array_equal(d.get_q(), o.all_q()), "qinit differs"
     t = 0.0
