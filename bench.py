@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--mx", type=int, default=16)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
-    p.add_argument("--step-variant", type=int, default=0, help="0 library's choice, 1 CTA rows, 2 warp")
+    p.add_argument("--step-variant", type=int, default=0, help="0 library's choice, 1 CTA rows, 2 warp, 3 pipelined CTA")
     return p.parse_args()
 
 

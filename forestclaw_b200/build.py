@@ -27,6 +27,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 SOURCES = {
     "fcb_step.cu": ["-fmad=false"],
     "fcb_step_warp.cu": ["-fmad=false"],
+    "fcb_step_pipe.cu": ["-fmad=false"],
     "fcb_ghost.cu": ["-fmad=false"],
     "fcb_amr.cu": ["-fmad=false"],
     "fcb_runtime.cu": [],

@@ -64,7 +64,7 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
     if (opt_.problem == FCB_PROBLEM_RADIALDAM && opt_.solver_kind != FCB_SOLVER_SWE_ROE) bad("radialdam needs SWE");
     if (opt_.problem == FCB_PROBLEM_QUADRANTS && opt_.solver_kind != FCB_SOLVER_EULER4_ROE) bad("quadrants needs Euler");
     aux_kind_ = (opt_.solver_kind == FCB_SOLVER_ADVECTION) ? AUX_SWIRL : AUX_NONE;
-    if (opt_.step_variant < 0 || opt_.step_variant > 2) bad("step_variant must be 0, 1 or 2");
+    if (opt_.step_variant < 0 || opt_.step_variant > 3) bad("step_variant must be 0, 1, 2 or 3");
     if ((opt_.mx & (opt_.mx - 1)) != 0) bad("mx must be a power of two");
     nx_ = opt_.mx + 2 * opt_.mbc;
     ny_ = opt_.my + 2 * opt_.mbc;
@@ -505,11 +505,18 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     // reference's per-cell evaluations because the unit-square mesh with mx a
     // power of two is dyadic (xll + dx == next xll exactly); checked at creation.
     cudaError_t e = cudaErrorNotSupported;
-    if (aux_kind_ == AUX_SWIRL && opt_.step_variant == 2) e = launch_step_warp_swirl(opt_.mx, opt_.mbc, a, st_);
-    if (e == cudaErrorNotSupported) {
-        if (opt_.step_variant == 2) throw Error(FCB_ERR_INVALID, "no warp-synchronous step for this case");
-        e = launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_);
+    const int v = opt_.step_variant;
+    if (v == 2) {
+        if (aux_kind_ == AUX_SWIRL) e = launch_step_warp_swirl(opt_.mx, opt_.mbc, a, st_);
+        if (e == cudaErrorNotSupported) throw Error(FCB_ERR_INVALID, "no warp-synchronous step for this case");
+    } else if (v == 3 || (v == 0 && opt_.solver_kind == SOLVER_ADVECTION)) {
+        // default: the pipelined form for scalar advection; the Roe solvers keep
+        // the four-barrier form, whose smaller register footprint suits them
+        e = launch_step_pipe(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_);
+        if (e == cudaErrorNotSupported && v == 3) throw Error(FCB_ERR_INVALID, "no pipelined step for this case");
     }
+    if (e == cudaErrorNotSupported)
+        e = launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_);
     check(e, "step");
     cnt_.count_single_step += n;
     ++cnt_.count_kernel_launches;

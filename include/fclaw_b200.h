@@ -88,8 +88,9 @@ typedef struct fcb_options {
     double gamma;              /* Euler /cparam/ gamma; gamma1 = gamma - 1 */
     double problem_params[32];
     /* step kernel form: 0 = chosen by the library, 1 = one CTA per patch group
-     * (rows through shared memory), 2 = warp-synchronous (swirl advection,
-     * mx = 8, 16, 32); both give identical results */
+     * (rows through shared memory, four barriers per row), 2 = warp-synchronous
+     * (swirl advection, mx = 8, 16, 32), 3 = software-pipelined CTA form (one
+     * barrier per row; mx = 8, 16, 32); all give identical results */
     int step_variant;
 } fcb_options_t;
 

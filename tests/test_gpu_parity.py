@@ -48,10 +48,10 @@ def _pair_variant(cfg, variant):
     return o, d
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 @pytest.mark.parametrize("mx", [8, 16, 32])
 def test_uniform_swirl_steps(gpu_lib, mx, variant):
-    """Both step-kernel forms (CTA rows, warp-synchronous) against the oracle."""
+    """Every step-kernel form (CTA rows, warp-synchronous, pipelined CTA) against the oracle."""
     cfg = cases.swirl_uniform(level=3, mx=mx)
     dt = cases.swirl_dt(level=3, mx=mx)
     o, d = _pair_variant(cfg, variant)
@@ -67,11 +67,12 @@ def test_uniform_swirl_steps(gpu_lib, mx, variant):
         assert abs(c_d - c_o) <= 1e-12 * max(1.0, c_o), (c_d, c_o)
 
 
+@pytest.mark.parametrize("variant", [1, 3])
 @pytest.mark.parametrize("mx", [16, 32])
-def test_uniform_radialdam_bit_exact(gpu_lib, mx):
+def test_uniform_radialdam_bit_exact(gpu_lib, mx, variant):
     cfg = cases.radialdam_uniform(level=2, mx=mx)
     dt = 0.4 / (mx * 4) / 1.5
-    o, d = _pair(cfg)
+    o, d = _pair_variant(cfg, variant)
     assert np.array_equal(d.get_q(), o.all_q())
     t = 0.0
     for step in range(10):
@@ -83,11 +84,12 @@ def test_uniform_radialdam_bit_exact(gpu_lib, mx):
         assert c_d == c_o
 
 
+@pytest.mark.parametrize("variant", [1, 3])
 @pytest.mark.parametrize("mx", [8, 16])
-def test_uniform_quadrants_bit_exact(gpu_lib, mx):
+def test_uniform_quadrants_bit_exact(gpu_lib, mx, variant):
     cfg = cases.quadrants_uniform(level=2, mx=mx)
     dt = 0.3 / (mx * 4) / 2.0
-    o, d = _pair(cfg)
+    o, d = _pair_variant(cfg, variant)
     assert np.array_equal(d.get_q(), o.all_q())
     t = 0.0
     for step in range(8):
