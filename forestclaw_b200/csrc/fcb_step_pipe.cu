@@ -52,22 +52,20 @@ struct Method {
 
 template <int NX, int PPB, int M, int W, int NAUX, bool SWIRL>
 struct PipeSmem {
-    // one ring slot holds one row of every patch of the CTA
-    static constexpr int QS = PPB * M * NX;
-    static constexpr int XWS = PPB * W * M * NX;
-    static constexpr int GLS = PPB * 2 * M * NX;
-    static constexpr int FXS = PPB * 2 * M * NX;
-    static constexpr int GYS = PPB * 2 * M * NX;
-    static constexpr int AXS = PPB * NAUX * NX;
+    // Every ring is [slot][component][patch][column]: one thread's element of
+    // any ring sits at (pl * NX + c) + a compile-time offset.
+    static constexpr int PNX = PPB * NX;
+    static constexpr int Q = 0;                                 // 2 slots x M
+    static constexpr int XW = Q + 2 * M * PNX;                  // 2 slots x W*M
+    static constexpr int GL = XW + 2 * W * M * PNX;             // 2 slots x 2M
+    static constexpr int FX = GL + 2 * 2 * M * PNX;             // 4 slots x 2M
+    static constexpr int GY = FX + 4 * 2 * M * PNX;             // 4 slots x 2M
+    static constexpr int AX = GY + 4 * 2 * M * PNX;             // 4 slots x NAUX
+    static constexpr int RINGS = AX + 4 * NAUX * PNX;
+    // swirl: sin^2 table of the node rows [patch][NX+1], psi node rows [2 slots][patch][NX+1]
     static constexpr int NDS = PPB * (NX + 1);
-    static constexpr int Q = 0;                                   // 2 slots: [PPB][M][NX]
-    static constexpr int XW = Q + 2 * QS;                         // 2 slots: [PPB][W][M][NX]
-    static constexpr int GL = XW + 2 * XWS;                       // 2 slots: [PPB][2][M][NX]
-    static constexpr int FX = GL + 2 * GLS;                       // 4 slots: [PPB][2][M][NX]
-    static constexpr int GY = FX + 4 * FXS;                       // 4 slots: [PPB][2][M][NX]
-    static constexpr int AX = GY + 4 * GYS;                       // 4 slots: [PPB][NAUX][NX]
-    static constexpr int TY = AX + 4 * AXS;                       // [PPB][NX+1]           (swirl)
-    static constexpr int ND = TY + (SWIRL ? PPB * (NX + 1) : 0);  // 2 slots: [PPB][NX+1]  (swirl)
+    static constexpr int TY = RINGS;
+    static constexpr int ND = TY + (SWIRL ? NDS : 0);
     static constexpr int TOTAL = ND + (SWIRL ? 2 * NDS : 0);
 };
 
@@ -89,22 +87,17 @@ struct PipeState {
     double cfl;
 };
 
-// Per-thread constants: column, flags and this thread's column in every ring.
+// Per-thread constants: column, flags and this thread's element of the rings.
 struct PipeThread {
     double* q;        // q of the patch, offset to column c
     double* qlast;    // qlast of the patch, offset to column c
     const double* aux;
-    double* Qb;
-    double* XWb;
-    double* GLb;
-    double* FXb;
-    double* GYb;
-    double* AXb;
-    double* NDb;
-    const double* TYb;
-    double dtdx, dtdy, dtdxave, dtdyave, vty, vtx, tx, txr;
+    double* sb;       // smem + pl * NX + c: this thread's element of every ring
+    double* nb;       // swirl: this thread's node in the psi node rows
+    const double* ty; // swirl: sin^2 table of the patch's node rows
+    double dtdx, dtdy, hdtdx, hdtdy, vty, vtx, tx;
     int c;
-    bool active, save_last, ycol;
+    bool active, save_last, ycol, node;
 };
 
 // ring slot of row s - d when s == J (mod D) is known at compile time
@@ -129,7 +122,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
     auto s4 = [&](int d) -> int { return J >= 0 ? cslot(J, d, 4) : ((s - d) & 3); };
     // aux component k of row s-d, column c+dc
     auto AUXV = [&](int k, int dc, int d) -> double {
-        if constexpr (NAUX > 0) return T.AXb[s4(d) * L::AXS + k * NX + dc];
+        if constexpr (NAUX > 0) return T.sb[L::AX + (s4(d) * NAUX + k) * L::PNX + dc];
         else return 0.0;
     };
 
@@ -146,14 +139,14 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
     {
         const int k = s - 3;
         const bool xint = T.active && (STEADY || (k >= 1 && k <= NY - 2)) && c >= 1;
-        const double* gl = T.GLb + s2(3) * L::GLS;
+        const double* gl = T.sb + L::GL + s2(3) * (2 * M * L::PNX);
 #pragma unroll
         for (int m = 0; m < M; ++m) {
             double gxd = 0.0, gxu = 0.0;
             if (xint) {
                 if (c + 1 <= NX - 1) {
-                    gxd = -gl[(0 * M + m) * NX + 1] - S.gRmx[m];
-                    gxu = -gl[(1 * M + m) * NX + 1] - S.gRpx[m];
+                    gxd = -gl[(0 * M + m) * L::PNX + 1] - S.gRmx[m];
+                    gxu = -gl[(1 * M + m) * L::PNX + 1] - S.gRpx[m];
                 } else {
                     gxd = -S.gRmx[m];
                     gxu = -S.gRpx[m];
@@ -168,18 +161,18 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
     {
         const int r = s - 4;
         if (T.active && (STEADY || (r >= 0 && r <= NY - 2)) && c <= NX - 2) {
-            const double* fx = T.FXb + s4(4) * L::FXS;
-            const double* gy = T.GYb + s4(4) * L::GYS;
+            const double* fx = T.sb + L::FX + s4(4) * (2 * M * L::PNX);
+            const double* gy = T.sb + L::GY + s4(4) * (2 * M * L::PNX);
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 double* qp = T.q + ((int64_t)m * NY + r) * NX;
                 const double qold = *qp;
-                const double fxm1 = fx[(0 * M + m) * NX + 1];
-                const double fxp0 = fx[(1 * M + m) * NX];
-                const double gyu_l = (c >= 1) ? gy[(1 * M + m) * NX - 1] : 0.0;
-                const double gyd_r = gy[(0 * M + m) * NX + 1];
-                const double gyd = gy[(0 * M + m) * NX];
-                const double gyu = gy[(1 * M + m) * NX];
+                const double fxm1 = fx[(0 * M + m) * L::PNX + 1];
+                const double fxp0 = fx[(1 * M + m) * L::PNX];
+                const double gyu_l = (c >= 1) ? gy[(1 * M + m) * L::PNX - 1] : 0.0;
+                const double gyd_r = gy[(0 * M + m) * L::PNX + 1];
+                const double gyd = gy[(0 * M + m) * L::PNX];
+                const double gyu = gy[(1 * M + m) * L::PNX];
                 const double fmv = (fxm1 + gyu) + gyd_r;   // fm(i+1, j)
                 const double fpv = (fxp0 + gyu_l) + gyd;   // fp(i, j)
                 const double gmv = GXs_new[m] + S.FYm2[m];   // gm(i, j+1)
@@ -195,10 +188,10 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
     {
         const int k = s - 2;
         if (T.active && (STEADY || (k >= 0 && k <= NY - 2))) {
-            double* fx = T.FXb + s4(2) * L::FXS;
+            double* fx = T.sb + L::FX + s4(2) * (2 * M * L::PNX);
             const bool xint = (STEADY || k >= 1) && c >= 1;
             if (xint) {
-                const double* xw = T.XWb + s2(2) * L::XWS;
+                const double* xw = T.sb + L::XW + s2(2) * (W * M * L::PNX);
                 double cq[M];
 #pragma unroll
                 for (int m = 0; m < M; ++m) cq[m] = 0.0;
@@ -209,14 +202,14 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
                             const int mth = meth.lim(mw);
                             if (mth == 0) continue;
                             double wn2 = S.xwl[mw][0] * S.xwl[mw][0];
-                            double dl = xw[(mw * M + 0) * NX - 1] * S.xwl[mw][0];
-                            double dr = S.xwl[mw][0] * xw[(mw * M + 0) * NX + 1];
+                            double dl = xw[(mw * M + 0) * L::PNX - 1] * S.xwl[mw][0];
+                            double dr = S.xwl[mw][0] * xw[(mw * M + 0) * L::PNX + 1];
 #pragma unroll
                             for (int m = 1; m < M; ++m) {
                                 const double wc = S.xwl[mw][m];
                                 wn2 = wn2 + wc * wc;
-                                dl = dl + xw[(mw * M + m) * NX - 1] * wc;
-                                dr = dr + wc * xw[(mw * M + m) * NX + 1];
+                                dl = dl + xw[(mw * M + m) * L::PNX - 1] * wc;
+                                dr = dr + wc * xw[(mw * M + m) * L::PNX + 1];
                             }
                             if (wn2 == 0.0) continue;
                             const double rr = (S.xsl[mw] > 0.0) ? dl / wn2 : dr / wn2;
@@ -230,12 +223,12 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
                         double acc;
                         {
                             const double as = fabs(S.xsl[0]);
-                            acc = as * (1.0 - as * T.dtdxave) * S.xwl[0][m];
+                            acc = as * (1.0 - as * T.dtdx) * S.xwl[0][m];
                         }
 #pragma unroll
                         for (int mw = 1; mw < W; ++mw) {
                             const double as = fabs(S.xsl[mw]);
-                            acc = acc + as * (1.0 - as * T.dtdxave) * S.xwl[mw][m];
+                            acc = acc + as * (1.0 - as * T.dtdx) * S.xwl[mw][m];
                         }
                         cq[m] = acc;
                     }
@@ -246,41 +239,41 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
                     double fmv = (c <= NX - 2) ? S.xam[m] : 0.0;
                     double fpv = (c <= NX - 2) ? -S.xap[m] : 0.0;
                     if (meth.second_order()) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
-                    fx[(0 * M + m) * NX] = fmv;
-                    fx[(1 * M + m) * NX] = fpv;
+                    fx[(0 * M + m) * L::PNX] = fmv;
+                    fx[(1 * M + m) * L::PNX] = fpv;
                     am[m] = S.xam[m];
                     ap[m] = S.xap[m];
                     if (meth.transverse2() && c <= NX - 2) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
                 }
-                double* gl = T.GLb + s2(2) * L::GLS;
+                double* gl = T.sb + L::GL + s2(2) * (2 * M * L::PNX);
                 if (meth.transverse()) {
                     double bm[M], bp[M];
                     // imp = 1: aux2(i-1, kv=2), aux3(i-1, kv=2) = v at column c-1, rows k, k+1
                     sol.rpt2(1, am, S.xR, AUXV(1, -1, 2), AUXV(1, -1, 1), bm, bp);
 #pragma unroll
                     for (int m = 0; m < M; ++m) {
-                        gl[(0 * M + m) * NX] = 0.5 * T.dtdx * bm[m];
-                        gl[(1 * M + m) * NX] = 0.5 * T.dtdx * bp[m];
+                        gl[(0 * M + m) * L::PNX] = T.hdtdx * bm[m];
+                        gl[(1 * M + m) * L::PNX] = T.hdtdx * bp[m];
                     }
                     sol.rpt2(1, ap, S.xR, AUXV(1, 0, 2), AUXV(1, 0, 1), bm, bp);
 #pragma unroll
                     for (int m = 0; m < M; ++m) {
-                        S.gRmx[m] = 0.5 * T.dtdx * bm[m];
-                        S.gRpx[m] = 0.5 * T.dtdx * bp[m];
+                        S.gRmx[m] = T.hdtdx * bm[m];
+                        S.gRpx[m] = T.hdtdx * bp[m];
                     }
                 } else {
 #pragma unroll
                     for (int m = 0; m < M; ++m) {
-                        gl[(0 * M + m) * NX] = 0.0;
-                        gl[(1 * M + m) * NX] = 0.0;
+                        gl[(0 * M + m) * L::PNX] = 0.0;
+                        gl[(1 * M + m) * L::PNX] = 0.0;
                         S.gRmx[m] = S.gRpx[m] = 0.0;
                     }
                 }
             } else {
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
-                    fx[(0 * M + m) * NX] = 0.0;
-                    fx[(1 * M + m) * NX] = 0.0;
+                    fx[(0 * M + m) * L::PNX] = 0.0;
+                    fx[(1 * M + m) * L::PNX] = 0.0;
                 }
             }
         }
@@ -290,16 +283,16 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
     {
         const int k = s - 1;
         if (T.active && (STEADY || (k >= 1 && k <= NY - 2)) && c >= 1) {
-            const double* qr = T.Qb + s2(1) * L::QS;
+            const double* qr = T.sb + L::Q + s2(1) * (M * L::PNX);
             double qL[M];
 #pragma unroll
-            for (int m = 0; m < M; ++m) qL[m] = qr[m * NX - 1];
+            for (int m = 0; m < M; ++m) qL[m] = qr[m * L::PNX - 1];
             sol.rpn2(1, qL, S.q_m1, AUXV(0, 0, 1), S.xwl, S.xsl, S.xam, S.xap, S.xR);
-            double* xw = T.XWb + s2(1) * L::XWS;
+            double* xw = T.sb + L::XW + s2(1) * (W * M * L::PNX);
 #pragma unroll
             for (int mw = 0; mw < W; ++mw) {
 #pragma unroll
-                for (int m = 0; m < M; ++m) xw[(mw * M + m) * NX] = S.xwl[mw][m];
+                for (int m = 0; m < M; ++m) xw[(mw * M + m) * L::PNX] = S.xwl[mw][m];
                 if (c >= MBC && c <= MBC + MX) S.cfl = dmax(dmax(S.cfl, T.dtdx * S.xsl[mw]), -T.dtdx * S.xsl[mw]);
             }
         }
@@ -318,11 +311,11 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
 #pragma unroll
         for (int m = 0; m < M; ++m) yam_n[m] = yap_n[m] = 0.0;
         if (T.active && (STEADY || s < NY)) {
-            double* qr = T.Qb + s2(0) * L::QS;
+            double* qr = T.sb + L::Q + s2(0) * (M * L::PNX);
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 if (T.save_last) T.qlast[((int64_t)m * NY + s) * NX] = S.qcur[m];
-                qr[m * NX] = S.qcur[m];
+                qr[m * L::PNX] = S.qcur[m];
             }
             // raw y-interface s (between rows s-1 and s)
             if (T.ycol && (STEADY || s >= 1)) {
@@ -378,12 +371,12 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
                     double acc;
                     {
                         const double as = fabs(S.ys_f[0]);
-                        acc = as * (1.0 - as * T.dtdyave) * w[0][m];
+                        acc = as * (1.0 - as * T.dtdy) * w[0][m];
                     }
 #pragma unroll
                     for (int mw = 1; mw < W; ++mw) {
                         const double as = fabs(S.ys_f[mw]);
-                        acc = acc + as * (1.0 - as * T.dtdyave) * w[mw][m];
+                        acc = acc + as * (1.0 - as * T.dtdy) * w[mw][m];
                     }
                     cq[m] = acc;
                 }
@@ -406,10 +399,10 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
                 // imp = 1: aux2(j-1, kv=1), aux3(j-1, kv=1) = u at columns c, c+1, row f-1
                 sol.rpt2(2, am, S.yR_f, AUXV(0, 0, 2), AUXV(0, 1, 2), bm, bp);
 #pragma unroll
-                for (int m = 0; m < M; ++m) { gLm[m] = 0.5 * T.dtdy * bm[m]; gLp[m] = 0.5 * T.dtdy * bp[m]; }
+                for (int m = 0; m < M; ++m) { gLm[m] = T.hdtdy * bm[m]; gLp[m] = T.hdtdy * bp[m]; }
                 sol.rpt2(2, ap, S.yR_f, AUXV(0, 0, 1), AUXV(0, 1, 1), bm, bp);
 #pragma unroll
-                for (int m = 0; m < M; ++m) { gRm[m] = 0.5 * T.dtdy * bm[m]; gRp[m] = 0.5 * T.dtdy * bp[m]; }
+                for (int m = 0; m < M; ++m) { gRm[m] = T.hdtdy * bm[m]; gRp[m] = T.hdtdy * bp[m]; }
             } else {
 #pragma unroll
                 for (int m = 0; m < M; ++m) gLm[m] = gLp[m] = gRm[m] = gRp[m] = 0.0;
@@ -427,11 +420,11 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
         }
         // GY of cell row s-2 (zero outside the y-columns and for row 0)
         if (T.active && (STEADY || (s >= 2 && s - 2 <= NY - 2))) {
-            double* gy = T.GYb + s4(2) * L::GYS;
+            double* gy = T.sb + L::GY + s4(2) * (2 * M * L::PNX);
 #pragma unroll
             for (int m = 0; m < M; ++m) {
-                gy[(0 * M + m) * NX] = GYd[m];
-                gy[(1 * M + m) * NX] = GYu[m];
+                gy[(0 * M + m) * L::PNX] = GYd[m];
+                gy[(1 * M + m) * L::PNX] = GYu[m];
             }
         }
         // delay lines: FYm(f) serves row f-1 two iterations on, FYp(f) row f three on
@@ -463,29 +456,29 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, con
         // aux row s+1
         if (STEADY || s + 1 <= NY - 1) {
             if constexpr (SWIRL) {
-                double* Nn = T.NDb + s2(-2) * L::NDS;        // node row s+2
-                const double* Nc = T.NDb + s2(-1) * L::NDS;  // node row s+1
-                const double ty = T.TYb[s + 2];
-                const double pn = (T.tx * ty) / pi;
+                // node thread c (c in [0, NX]) computes psi at node (c, s+2)
+                const double pn = (T.tx * T.ty[s + 2]) / pi;
+                if (T.node) T.nb[s2(-2) * L::NDS] = pn;
                 if (T.active) {
-                    double* ax = T.AXb + s4(-1) * L::AXS;
-                    ax[0 * NX] = T.vty * (pn - S.pcur);
-                    ax[1 * NX] = -T.vtx * (Nc[1] - S.pcur);
-                    Nn[0] = pn;
-                    if (c == NX - 1) Nn[1] = (T.txr * ty) / pi;
+                    double* ax = T.sb + L::AX + s4(-1) * (NAUX * L::PNX);
+                    ax[0 * L::PNX] = T.vty * (pn - S.pcur);
+                    ax[1 * L::PNX] = -T.vtx * (T.nb[s2(-1) * L::NDS + 1] - S.pcur);
                 }
                 S.pcur = pn;
             } else if constexpr (AUXK == AUX_STORED) {
                 if (T.active) {
-                    double* ax = T.AXb + s4(-1) * L::AXS;
+                    double* ax = T.sb + L::AX + s4(-1) * (NAUX * L::PNX);
 #pragma unroll
-                    for (int kk = 0; kk < NAUX; ++kk) ax[kk * NX] = T.aux[(kk * NY + s + 1) * NX];
+                    for (int kk = 0; kk < NAUX; ++kk) ax[kk * L::PNX] = T.aux[(kk * NY + s + 1) * NX];
                 }
             }
         }
     }
     __syncthreads();
 }
+
+template <int NX, bool SWIRL>
+__host__ __device__ constexpr int pipe_threads_per_patch() { return SWIRL ? NX + 1 : NX; }
 
 }  // namespace
 
@@ -495,44 +488,47 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     constexpr int W = SOL::W;
     constexpr int NX = MX + 2 * MBC;
     constexpr int NY = NX;
-    constexpr int PPB = TPB / NX;
     constexpr bool SWIRL = AUXK == AUX_SWIRL;
+    constexpr int TPP = pipe_threads_per_patch<NX, SWIRL>();
+    constexpr int PPB = TPB / TPP;
     using L = PipeSmem<NX, PPB, M, W, NAUX, SWIRL>;
     extern __shared__ double smem[];
 
+    // Threads (pl, c): c in [0, NX) owns column c of patch pl; with the swirl
+    // velocities one more thread per patch (c == NX) computes the last node
+    // column of the stream function.
     const int t = threadIdx.x;
-    const int pl = t / NX;
-    const int c = t - pl * NX;
+    const int pl = t / TPP;
+    const int c = t - pl * TPP;
     const int pg = blockIdx.x * PPB + pl;
-    const bool active = (pl < PPB) && (pg < a.npatches);
-    const int pls = active ? pl : 0;  // idle threads of a partial CTA read (never write) patch 0's rows
-    const int slot = active ? a.slots[pg] : 0;
-    const PatchMeta meta = active ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0};
+    const bool patch_ok = (pl < PPB) && (pg < a.npatches);
+    const bool active = patch_ok && c < NX;
+    const int pls = patch_ok ? pl : 0;  // threads without a patch read (never write) patch 0's rows
+    const int cc = c < NX ? c : NX - 1;
+    const int slot = patch_ok ? a.slots[pg] : 0;
+    const PatchMeta meta = patch_ok ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0};
     const SOL sol{a.grav, a.gamma, a.gamma1};
 
     PipeThread T;
-    T.c = c;
+    T.c = cc;
     T.active = active;
+    T.node = SWIRL && patch_ok;
     T.save_last = active && (meta.flags & PATCH_SAVE_LAST);
     T.ycol = active && c >= 1 && c <= NX - 2;
-    T.q = a.q + (int64_t)slot * a.q_stride + c;
-    T.qlast = a.qlast + (int64_t)slot * a.q_stride + c;
-    T.aux = (AUXK == AUX_STORED && active) ? a.aux + (int64_t)slot * a.aux_stride + c : nullptr;
-    T.Qb = smem + L::Q + pls * M * NX + c;
-    T.XWb = smem + L::XW + pls * W * M * NX + c;
-    T.GLb = smem + L::GL + pls * 2 * M * NX + c;
-    T.FXb = smem + L::FX + pls * 2 * M * NX + c;
-    T.GYb = smem + L::GY + pls * 2 * M * NX + c;
-    T.AXb = smem + L::AX + pls * NAUX * NX + c;
-    T.NDb = smem + L::ND + pls * (NX + 1) + c;
-    T.TYb = smem + L::TY + pls * (NX + 1);
+    T.q = a.q + (int64_t)slot * a.q_stride + cc;
+    T.qlast = a.qlast + (int64_t)slot * a.q_stride + cc;
+    T.aux = (AUXK == AUX_STORED && active) ? a.aux + (int64_t)slot * a.aux_stride + cc : nullptr;
+    T.sb = smem + pls * NX + cc;
+    T.nb = smem + L::ND + pls * (NX + 1) + c;
+    T.ty = smem + L::TY + pls * (NX + 1);
+    // dtdx1d is uniform without capacity, so 0.5*(dtdx1d(i-1)+dtdx1d(i)) == dtdx exactly
     T.dtdx = a.dt / meta.dx;
     T.dtdy = a.dt / meta.dy;
-    T.dtdxave = 0.5 * (T.dtdx + T.dtdx);  // 0.5*(dtdx1d(i-1)+dtdx1d(i)), no capacity
-    T.dtdyave = 0.5 * (T.dtdy + T.dtdy);
+    T.hdtdx = 0.5 * T.dtdx;  // the reference's 0.5d0*dtdx*b, evaluated left to right
+    T.hdtdy = 0.5 * T.dtdy;
     T.vty = a.vt / meta.dy;
     T.vtx = a.vt / meta.dx;
-    T.tx = T.txr = 0.0;
+    T.tx = 0.0;
 
     PipeState<SOL> S;
 #pragma unroll
@@ -566,43 +562,29 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
         // next node's xll exactly; checked on the host), so psi is evaluated
         // once per node: P(c,n) at the lower-left corner of cell (c,n).
         constexpr double pi = 3.141592653589793;
-        double* TY = smem + L::TY + pls * (NX + 1);
         {
             const double x = meta.xlower + (double)(c - MBC) * meta.dx;
             const double y = meta.ylower + (double)(c - MBC) * meta.dy;
             const double sx = sin(pi * x), sy = sin(pi * y);
             T.tx = sx * sx;
-            if (active) TY[c] = sy * sy;
-            if (c == NX - 1) {
-                const double xr = meta.xlower + (double)(NX - MBC) * meta.dx;
-                const double yr = meta.ylower + (double)(NX - MBC) * meta.dy;
-                const double sxr = sin(pi * xr), syr = sin(pi * yr);
-                T.txr = sxr * sxr;
-                if (active) TY[NX] = syr * syr;
-            }
+            if (T.node) smem[L::TY + pls * (NX + 1) + c] = sy * sy;
         }
         __syncthreads();
-        double* N0 = T.NDb;              // node row 0
-        double* N1 = T.NDb + L::NDS;     // node row 1
-        const double p0 = (T.tx * TY[0]) / pi, p1 = (T.tx * TY[1]) / pi;
-        if (active) {
-            N0[0] = p0;
-            N1[0] = p1;
-            if (c == NX - 1) {
-                N0[1] = (T.txr * TY[0]) / pi;
-                N1[1] = (T.txr * TY[1]) / pi;
-            }
+        const double p0 = (T.tx * T.ty[0]) / pi, p1 = (T.tx * T.ty[1]) / pi;
+        if (T.node) {
+            T.nb[0] = p0;          // node row 0
+            T.nb[L::NDS] = p1;     // node row 1
         }
         __syncthreads();
         if (active) {
-            T.AXb[0 * NX] = T.vty * (p1 - p0);
-            T.AXb[1 * NX] = -T.vtx * (N0[1] - p0);
+            T.sb[L::AX + 0 * L::PNX] = T.vty * (p1 - p0);
+            T.sb[L::AX + 1 * L::PNX] = -T.vtx * (T.nb[1] - p0);
         }
         S.pcur = p1;
     } else if constexpr (AUXK == AUX_STORED) {
         if (active) {
 #pragma unroll
-            for (int k = 0; k < NAUX; ++k) T.AXb[k * NX] = T.aux[(k * NY + 0) * NX];
+            for (int k = 0; k < NAUX; ++k) T.sb[L::AX + k * L::PNX] = T.aux[(k * NY + 0) * NX];
         }
     }
     __syncthreads();
@@ -634,7 +616,7 @@ namespace {
 template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
 cudaError_t launch_pipe_one(const StepArgs& a, cudaStream_t st) {
     constexpr int NX = MX + 2 * MBC;
-    constexpr int PPB = TPB / NX;
+    constexpr int PPB = TPB / pipe_threads_per_patch<NX, AUXK == AUX_SWIRL>();
     static_assert(PPB >= 1, "patch wider than the CTA");
     using L = PipeSmem<NX, PPB, SOL::M, SOL::W, NAUX, AUXK == AUX_SWIRL>;
     const size_t bytes = (size_t)L::TOTAL * sizeof(double);
