@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--mx", type=int, default=16)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                   help="fp64: the reference's arithmetic; mixed: FP32 solves, FP64 sums and state")
     p.add_argument("--step-variant", type=int, default=0, help="0 library's choice, 1 CTA rows, 2 warp, 3 pipelined CTA")
     return p.parse_args()
 
@@ -205,6 +207,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     opts = workloads.uniform_swirl(args.level, args.mx)
     opts.step_variant = args.step_variant
+    opts.precision = fcb.PRECISION_MIXED if args.precision == "mixed" else fcb.PRECISION_FP64
     dt = workloads.swirl_dt(args.level, args.mx)
     s = fcb.Solver(opts, stream=stream.cuda_stream)
     s.initialize()
@@ -277,7 +280,7 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.steps):
         s.advance_all_levels(t, dt)
         t += dt
-    hv[...] = s.get_q()
+    s.get_q(out=hv)
     x1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = x0.elapsed_time(x1)
@@ -296,9 +299,11 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": "cell-updates/s", "value": total_cells / (ms_max * 1e-3), "unit": "cell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32/f64",
         "data": "synthetic",
-        "config": {"workload": f"uniform swirl advection, level {args.level}, mx=my={args.mx}, FP64 plain",
+        "config": {"workload": f"uniform swirl advection, level {args.level}, mx=my={args.mx}, "
+                               + ("FP64 plain" if args.precision == "fp64" else "mixed FP32/FP64"),
                    "patches": npatch, "cells": cells_per_step, "l2_flush": "inputs larger than L2",
                    "parallelism": f"{world} independent replicas" if world > 1 else "single GPU",
                    "step_kernel_ms": step_ms, "ghost_fill_ms": ghost_ms},

@@ -21,6 +21,7 @@ import numpy as np
 
 __all__ = ["Options", "Solver", "lib", "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
            "SOLVER_EULER4_ROE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM", "PROBLEM_QUADRANTS",
+           "PRECISION_FP64", "PRECISION_MIXED",
            "TAG_VALUE", "TAG_MINMAX", "TAG_DIFFERENCE", "TAG_GRADIENT", "EXPORTED_SYMBOLS"]
 
 PKG = Path(__file__).resolve().parent
@@ -28,6 +29,7 @@ LIBPATH = PKG / "libfclaw_b200.so"
 
 SOLVER_ADVECTION, SOLVER_SWE_ROE, SOLVER_EULER4_ROE = 0, 1, 2
 PROBLEM_SWIRL, PROBLEM_RADIALDAM, PROBLEM_QUADRANTS = 0, 1, 2
+PRECISION_FP64, PRECISION_MIXED = 0, 1
 TAG_VALUE, TAG_MINMAX, TAG_DIFFERENCE, TAG_GRADIENT = 0, 1, 2, 3
 
 EXPORTED_SYMBOLS = (
@@ -59,6 +61,7 @@ class _Options(ctypes.Structure):
         ("grav", ctypes.c_double), ("gamma", ctypes.c_double),
         ("problem_params", ctypes.c_double * 32),
         ("step_variant", ctypes.c_int),
+        ("precision", ctypes.c_int),
     ]
 
 
@@ -108,15 +111,17 @@ class Options:
     grav: float = 1.0
     gamma: float = 1.4
     problem_params: Sequence[float] = field(default_factory=tuple)
-    # step kernel form: 0 = library's choice, 1 = CTA rows, 2 = warp-synchronous
+    # step kernel form: 0 = library's choice, 1 = CTA rows, 2 = warp-synchronous, 3 = pipelined
     step_variant: int = 0
+    # 0 = FP64 throughout, 1 = mixed FP32 solves / FP64 accumulation
+    precision: int = PRECISION_FP64
 
     def to_c(self) -> _Options:
         o = _Options()
         for name in ("mx", "my", "mbc", "meqn", "maux", "refinement_criteria", "threshold_variable",
                      "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
                      "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
-                     "reduce_cfl", "solver_kind", "problem", "step_variant"):
+                     "reduce_cfl", "solver_kind", "problem", "step_variant", "precision"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
                      "desired_cfl", "grav", "gamma"):
@@ -286,8 +291,13 @@ class Solver:
         o = self.options
         return (self.num_patches, o.meqn, o.ny, o.nx)
 
-    def get_q(self) -> np.ndarray:
-        out = np.empty(self._shape(), dtype=np.float64)
+    def get_q(self, out: np.ndarray | None = None) -> np.ndarray:
+        """All patch arrays, (patches, meqn, ny, nx) in leaf order; `out` (for
+        instance a view of pinned host memory) is filled in place if given."""
+        if out is None:
+            out = np.empty(self._shape(), dtype=np.float64)
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size < int(np.prod(self._shape())):
+            raise ValueError("out must be a C-contiguous float64 array of at least the state's size")
         _check(lib().fcb_get_q(self._h, _dp(out), out.size))
         return out
 

@@ -2,9 +2,11 @@
 
 Usage: python -m forestclaw_b200.build [--force]
 
-The step kernel is compiled with -fmad=false: every multiply and add is
+The FP64 kernels are compiled with -fmad=false: every multiply and add is
 rounded separately, as the reference Fortran is on x86-64 without FMA, so the
-FP64 results match the reference's arithmetic operation by operation.
+FP64 results match the reference's arithmetic operation by operation.  The
+mixed-precision step (fcb_step_mixed.cu) is compiled with --use_fast_math:
+its FP32 solves use the fast division and square root.
 """
 from __future__ import annotations
 
@@ -28,13 +30,14 @@ SOURCES = {
     "fcb_step.cu": ["-fmad=false"],
     "fcb_step_warp.cu": ["-fmad=false"],
     "fcb_step_pipe.cu": ["-fmad=false"],
+    "fcb_step_mixed.cu": ["--use_fast_math"],
     "fcb_ghost.cu": ["-fmad=false"],
     "fcb_amr.cu": ["-fmad=false"],
     "fcb_runtime.cu": [],
     "fcb_capi.cu": ["-Xcompiler", "-fvisibility=default"],
     "fcb_noalloc.cu": ["-fmad=false"],
 }
-HEADERS = ["fcb_device.h", "fcb_solvers.cuh", "fcb_forest.hpp", "fcb_runtime.hpp"]
+HEADERS = ["fcb_device.h", "fcb_solvers.cuh", "fcb_step_pipe.cuh", "fcb_forest.hpp", "fcb_runtime.hpp"]
 
 
 def _stale(target: Path, deps) -> bool:

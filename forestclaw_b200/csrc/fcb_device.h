@@ -65,6 +65,7 @@ struct GhostArgs {
     const GhostOp* ops;    // records of the wave, sorted by destination patch
     const int32_t* groups; // group k = records [groups[k], groups[k+1]) (absolute indices into ops)
     int ngroups;
+    int interp_fp32;       // mixed precision: coarse-to-fine interpolation in FP32
 };
 
 enum Problem : int32_t { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2 };

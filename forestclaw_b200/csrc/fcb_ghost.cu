@@ -33,32 +33,41 @@ struct PatchView {
 };
 
 // fclaw2d_clawpatch_compute_slopes, mth = 5 (SIGN(1,x) follows the sign bit).
-__device__ __forceinline__ double slope5(double sl, double sr) {
-    const double sc = (sl + sr) / 2.0;
-    double m = 2 * fabs(sl);
-    const double b = 2 * fabs(sr), cc = fabs(sc);
+template <typename R>
+__device__ __forceinline__ R slope5(R sl, R sr) {
+    const R sc = (sl + sr) / R(2);
+    R m = 2 * fabs(sl);
+    const R b = 2 * fabs(sr), cc = fabs(sc);
     if (b < m) m = b;
     if (cc < m) m = cc;
-    const double s0 = copysign(1.0, sl * sr);
-    return m * (s0 > 0.0 ? s0 : 0.0) * copysign(1.0, sc);
+    const R s0 = copysign(R(1), sl * sr);
+    return m * (s0 > R(0) ? s0 : R(0)) * copysign(R(1), sc);
 }
 
-__device__ __forceinline__ void interp_cell(const PatchView& C, const PatchView& F, int m, int ic, int jc,
-                                            int i20, int j20) {
-    const double qc = C.at(ic, jc, m);
-    double sl = (qc - C.at(ic - 1, jc, m));
-    double sr = (C.at(ic + 1, jc, m) - qc);
-    const double gradx = slope5(sl, sr);
-    sl = (qc - C.at(ic, jc - 1, m));
-    sr = (C.at(ic, jc + 1, m) - qc);
-    const double grady = slope5(sl, sr);
+// R = double: the reference's arithmetic; R = float: the mixed-precision form.
+template <typename R>
+__device__ __forceinline__ void interp_cell_t(const PatchView& C, const PatchView& F, int m, int ic, int jc,
+                                              int i20, int j20) {
+    const R qc = R(C.at(ic, jc, m));
+    R sl = (qc - R(C.at(ic - 1, jc, m)));
+    R sr = (R(C.at(ic + 1, jc, m)) - qc);
+    const R gradx = slope5(sl, sr);
+    sl = (qc - R(C.at(ic, jc - 1, m)));
+    sr = (R(C.at(ic, jc + 1, m)) - qc);
+    const R grady = slope5(sl, sr);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int ii = k & 1, jj = k >> 1;
-        const double shiftx = (ii - 0.5) / 2.0;
-        const double shifty = (jj - 0.5) / 2.0;
-        F.at(i20 + ii, j20 + jj, m) = qc + gradx * shiftx + grady * shifty;
+        const R shiftx = (ii - R(0.5)) / R(2);
+        const R shifty = (jj - R(0.5)) / R(2);
+        F.at(i20 + ii, j20 + jj, m) = double(qc + gradx * shiftx + grady * shifty);
     }
+}
+
+__device__ __forceinline__ void interp_cell(bool fp32, const PatchView& C, const PatchView& F, int m, int ic,
+                                            int jc, int i20, int j20) {
+    if (fp32) interp_cell_t<float>(C, F, m, ic, jc, i20, j20);
+    else interp_cell_t<double>(C, F, m, ic, jc, i20, j20);
 }
 
 }  // namespace
@@ -155,7 +164,7 @@ __device__ __forceinline__ void ghost_op(const GhostArgs& a, const GhostOp& op, 
                 else { ic = t; jc = (op.face == 2) ? b : my - b + 1; }
                 const int fi = 2 * ic + op.dx, fj = 2 * jc + op.dy;
                 if (fi < 1 - mbc || fi + 1 > mx + mbc || fj < 1 - mbc || fj + 1 > my + mbc) continue;
-                interp_cell(S, D, m, ic, jc, fi, fj);
+                interp_cell(a.interp_fp32 != 0, S, D, m, ic, jc, fi, fj);
             }
             break;
         }
@@ -170,7 +179,7 @@ __device__ __forceinline__ void ghost_op(const GhostArgs& a, const GhostOp& op, 
                 else if (op.face == 1) { ic = mx - ibc + 1; jc = jbc; }
                 else if (op.face == 2) { ic = ibc; jc = my - jbc + 1; }
                 else { ic = mx - ibc + 1; jc = my - jbc + 1; }
-                interp_cell(S, D, m, ic, jc, 2 * ic + op.dx, 2 * jc + op.dy);
+                interp_cell(a.interp_fp32 != 0, S, D, m, ic, jc, 2 * ic + op.dx, 2 * jc + op.dy);
             }
             break;
         }
@@ -301,7 +310,7 @@ __device__ __forceinline__ double* op_cell(const GhostArgs& a, const GhostOp& op
             else { ic = t; jc = (op.face == 2) ? b : my - b + 1; }
             const int fi = 2 * ic + op.dx, fj = 2 * jc + op.dy;
             if (fi < 1 - mbc || fi + 1 > mx + mbc || fj < 1 - mbc || fj + 1 > my + mbc) return nullptr;
-            interp_cell(S, D, m, ic, jc, fi, fj);
+            interp_cell(a.interp_fp32 != 0, S, D, m, ic, jc, fi, fj);
             return nullptr;
         }
         case OP_INTERP_CORNER: {
@@ -313,7 +322,7 @@ __device__ __forceinline__ double* op_cell(const GhostArgs& a, const GhostOp& op
             else if (op.face == 1) { ic = mx - ibc + 1; jc = jbc; }
             else if (op.face == 2) { ic = ibc; jc = my - jbc + 1; }
             else { ic = mx - ibc + 1; jc = my - jbc + 1; }
-            interp_cell(S, D, m, ic, jc, 2 * ic + op.dx, 2 * jc + op.dy);
+            interp_cell(a.interp_fp32 != 0, S, D, m, ic, jc, 2 * ic + op.dx, 2 * jc + op.dy);
             return nullptr;
         }
         default: return nullptr;

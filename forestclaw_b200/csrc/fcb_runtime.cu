@@ -65,6 +65,9 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
     if (opt_.problem == FCB_PROBLEM_QUADRANTS && opt_.solver_kind != FCB_SOLVER_EULER4_ROE) bad("quadrants needs Euler");
     aux_kind_ = (opt_.solver_kind == FCB_SOLVER_ADVECTION) ? AUX_SWIRL : AUX_NONE;
     if (opt_.step_variant < 0 || opt_.step_variant > 3) bad("step_variant must be 0, 1, 2 or 3");
+    if (opt_.precision != 0 && opt_.precision != 1) bad("precision must be 0 (FP64) or 1 (mixed)");
+    if (opt_.precision == 1 && (opt_.step_variant == 1 || opt_.step_variant == 2))
+        bad("the mixed-precision update exists in the pipelined step form only");
     if ((opt_.mx & (opt_.mx - 1)) != 0) bad("mx must be a power of two");
     nx_ = opt_.mx + 2 * opt_.mbc;
     ny_ = opt_.my + 2 * opt_.mbc;
@@ -433,6 +436,7 @@ void Context::run_plan(const GhostPlan& g) {
         a.ops = d_ops_.p;
         a.groups = d_groups_.p + g.first_group + g.group_begin[w];  // group starts, then an end marker
         a.ngroups = g.group_begin[w + 1] - g.group_begin[w] - 1;
+        a.interp_fp32 = opt_.precision == 1;
         check(launch_ghost_wave(a, st_), "ghost wave");
         ++cnt_.count_ghost_waves;
         ++cnt_.count_kernel_launches;
@@ -506,7 +510,10 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     // power of two is dyadic (xll + dx == next xll exactly); checked at creation.
     cudaError_t e = cudaErrorNotSupported;
     const int v = opt_.step_variant;
-    if (v == 2) {
+    if (opt_.precision == 1) {
+        e = launch_step_pipe_mixed(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_);
+        if (e == cudaErrorNotSupported) throw Error(FCB_ERR_INVALID, "no mixed-precision step for this case");
+    } else if (v == 2) {
         if (aux_kind_ == AUX_SWIRL) e = launch_step_warp_swirl(opt_.mx, opt_.mbc, a, st_);
         if (e == cudaErrorNotSupported) throw Error(FCB_ERR_INVALID, "no warp-synchronous step for this case");
     } else if (v == 3 || (v == 0 && opt_.solver_kind == SOLVER_ADVECTION)) {

@@ -27,6 +27,8 @@ cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, in
 cudaError_t launch_step_warp_swirl(int mx, int mbc, const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_pipe(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
                              cudaStream_t st);
+cudaError_t launch_step_pipe_mixed(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
+                                   const StepArgs& a, cudaStream_t st);
 struct GhostArgs;
 cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st);
 cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64_t stride,

@@ -1,689 +1,12 @@
-// Software-pipelined form of the batched Clawpack 4.6 patch update (step2 +
-// flux2 + conservative update): one thread per patch column, several patches
-// per CTA, the patch rows streamed top to bottom.  The arithmetic, operation
-// order and loop bounds are those of fcb_step.cu (and of the reference:
-// src/solvers/fc2d_clawpack4.6/fortran_source/clawpack46_step2.f,
-// clawpack46_flux2.f, clawpack46_step2_wrap.f); only the schedule differs.
-//
-// Every exchange between neighbouring columns goes through a small ring of
-// rows in shared memory (2 or 4 slots), and every consumer runs at least one
-// row-iteration after its producer, so one CTA barrier per row separates all
-// producer/consumer pairs.  In the steady state the row loop is unrolled by the
-// ring period, which turns every ring slot into a compile-time offset.
-// Iteration s runs, in this order (k = row index of the stage):
-//   S4  x-row s-3: transverse parts from the right neighbour (ring GL) -> GX(c, s-3)
-//   S5  cell row s-4: conservative update (rings FX, GY; own GX, FY)
-//   S3  x-row s-2: limiter with the neighbours' waves (ring XW), second-order
-//       and transverse corrections -> rings FX, GL
-//   S2  x-row s-1: Riemann problem with the left neighbour's state (ring Q) -> ring XW
-//   S1  row s: y-interface s (raw) and y-interface s-1 (final, own column);
-//       y transverse parts -> ring GY; aux row s+1 -> ring AX
-// with q(c, s+1) prefetched at the top of iteration s.  Stages that carry
-// values to the next iteration run before their producers, so the carries
-// need no register copies.
-//
-// Accumulation order (identical to fcb_step.cu):
-//   fm(i,j) = (FXm + GYu[col i-1]) + GYd[col i],   gm(i,j) = (GXu[row j-1] + GXd[row j]) + FYm
-//   q = q - dtdx*(fm(i+1,j) - fp(i,j)) - dtdy*(gm(i,j+1) - gp(i,j)).
-// Compiled without FMA contraction.
-#include <cuda_runtime.h>
-
-#include "fcb_device.h"
-#include "fcb_solvers.cuh"
+// FP64 form of the pipelined step kernel (fcb_step_pipe.cuh), compiled with
+// -fmad=false so that every product and sum is rounded as in the reference.
+#include "fcb_step_pipe.cuh"
 
 namespace fcb {
 
-namespace {
-
-__device__ __forceinline__ void atomic_max_nonneg_p(unsigned long long* p, double v) {
-    atomicMax(p, (unsigned long long)__double_as_longlong(v));
-}
-
-// LIM > 0: order (2, 2) and limiter LIM on every wave, fixed at compile time;
-// LIM == 0: order and limiters read from the launch arguments.
-template <int LIM>
-struct Method {
-    const StepArgs& a;
-    __device__ __forceinline__ bool second_order() const { return LIM > 0 || a.order0 == 2; }
-    __device__ __forceinline__ bool transverse() const { return LIM > 0 || a.order1 > 0; }
-    __device__ __forceinline__ bool transverse2() const { return LIM > 0 || (a.order0 > 1 && a.order1 == 2); }
-    __device__ __forceinline__ int lim(int mw) const { return LIM > 0 ? LIM : a.mthlim[mw]; }
-};
-
-template <int NX, int PPB, int M, int W, int NAUX, bool SWIRL>
-struct PipeSmem {
-    // Every ring is [slot][component][patch][column]: one thread's element of
-    // any ring sits at (pl * NX + c) + a compile-time offset.
-    static constexpr int PNX = PPB * NX;
-    static constexpr int Q = 0;                                 // 2 slots x M
-    static constexpr int XW = Q + 2 * M * PNX;                  // 2 slots x W*M
-    static constexpr int GL = XW + 2 * W * M * PNX;             // 2 slots x 2M
-    static constexpr int FX = GL + 2 * 2 * M * PNX;             // 4 slots x 2M
-    static constexpr int GY = FX + 4 * 2 * M * PNX;             // 4 slots x 2M
-    static constexpr int AX = GY + 4 * 2 * M * PNX;             // 4 slots x NAUX
-    static constexpr int RINGS = AX + 4 * NAUX * PNX;
-    // swirl: sin^2 table of the node rows [patch][NX+1], psi node rows [2 slots][patch][NX+1]
-    static constexpr int NDS = PPB * (NX + 1);
-    static constexpr int TY = RINGS;
-    static constexpr int ND = TY + (SWIRL ? NDS : 0);
-    static constexpr int TOTAL = ND + (SWIRL ? 2 * NDS : 0);
-};
-
-// Values a thread carries from one row-iteration to the next.
-template <class SOL>
-struct PipeState {
-    static constexpr int M = SOL::M;
-    static constexpr int W = SOL::W;
-    double qcur[M], q_m1[M];                                   // q(c, s), q(c, s-1)
-    double yw_f[W][M], ys_f[W], yam_f[M], yap_f[M], ydotl[W];  // raw y-interface s-1
-    typename SOL::Roe yR_f;
-    double gRm_prev[M], gRp_prev[M];                           // y transverse parts into row s-2
-    double xwl[W][M], xsl[W], xam[M], xap[M];                  // S2 -> S3
-    typename SOL::Roe xR;
-    double gRmx[M], gRpx[M];                                   // S3 -> S4
-    double GXu_prev[M], GXs_prev[M];                           // S4 -> S4, S4 -> S5
-    double FYm1[M], FYm2[M], FYp1[M], FYp2[M], FYp3[M];        // y fluxes of the own column, delayed
-    double pcur;                                               // swirl: psi at node (c, s+1)
-    double cfl;
-};
-
-// Per-thread constants: column, flags and this thread's element of the rings.
-struct PipeThread {
-    double* q;        // q of the patch, offset to column c
-    double* qlast;    // qlast of the patch, offset to column c
-    const double* aux;
-    double* sb;       // smem + pl * NX + c: this thread's element of every ring
-    double* nb;       // swirl: this thread's node in the psi node rows
-    const double* ty; // swirl: sin^2 table of the patch's node rows
-    double dtdx, dtdy, hdtdx, hdtdy, vty, vtx, tx;
-    int c;
-    bool active, save_last, ycol, node;
-};
-
-// ring slot of row s - d when s == J (mod D) is known at compile time
-__host__ __device__ constexpr int cslot(int J, int d, int D) { return ((J - d) % D + D) % D; }
-
-// One row-iteration.  J >= 0: s == J (mod 4) at compile time, so every ring
-// slot is a constant; STEADY: s in [4, NY-2], where every stage is active for
-// every row and the row-range tests vanish.
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int PPB, int LIM, int J, bool STEADY>
-__device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol, const PipeThread& T,
-                                          PipeState<SOL>& S, int s) {
-    constexpr int M = SOL::M;
-    constexpr int W = SOL::W;
-    constexpr int NX = MX + 2 * MBC;
-    constexpr int NY = NX;
-    constexpr bool SWIRL = AUXK == AUX_SWIRL;
-    using L = PipeSmem<NX, PPB, M, W, NAUX, SWIRL>;
-    constexpr double pi = 3.141592653589793;  // 4*atan(1) in double precision
-    const Method<LIM> meth{a};
-    const int c = T.c;
-    auto s2 = [&](int d) -> int { return J >= 0 ? cslot(J, d, 2) : ((s - d) & 1); };
-    auto s4 = [&](int d) -> int { return J >= 0 ? cslot(J, d, 4) : ((s - d) & 3); };
-    // aux component k of row s-d, column c+dc
-    auto AUXV = [&](int k, int dc, int d) -> double {
-        if constexpr (NAUX > 0) return T.sb[L::AX + (s4(d) * NAUX + k) * L::PNX + dc];
-        else return 0.0;
-    };
-
-    // prefetch q(c, s+1)
-    double qnext[M];
-    {
-        const bool on = T.active && (STEADY || s + 1 < NY);
-#pragma unroll
-        for (int m = 0; m < M; ++m) qnext[m] = on ? T.q[((int64_t)m * NY + s + 1) * NX] : 0.0;
-    }
-
-    // ---------------- S4: GX(c, k), k = s-3 ----------------
-    double GXs_new[M];
-    {
-        const int k = s - 3;
-        const bool xint = T.active && (STEADY || (k >= 1 && k <= NY - 2)) && c >= 1;
-        const double* gl = T.sb + L::GL + s2(3) * (2 * M * L::PNX);
-#pragma unroll
-        for (int m = 0; m < M; ++m) {
-            double gxd = 0.0, gxu = 0.0;
-            if (xint) {
-                if (c + 1 <= NX - 1) {
-                    gxd = -gl[(0 * M + m) * L::PNX + 1] - S.gRmx[m];
-                    gxu = -gl[(1 * M + m) * L::PNX + 1] - S.gRpx[m];
-                } else {
-                    gxd = -S.gRmx[m];
-                    gxu = -S.gRpx[m];
-                }
-            }
-            GXs_new[m] = S.GXu_prev[m] + gxd;  // GX(c, k) = GXu(row k-1) + GXd(row k)
-            S.GXu_prev[m] = gxu;
-        }
-    }
-
-    // ---------------- S5: update cell row r = s-4 ----------------
-    {
-        const int r = s - 4;
-        if (T.active && (STEADY || (r >= 0 && r <= NY - 2)) && c <= NX - 2) {
-            const double* fx = T.sb + L::FX + s4(4) * (2 * M * L::PNX);
-            const double* gy = T.sb + L::GY + s4(4) * (2 * M * L::PNX);
-#pragma unroll
-            for (int m = 0; m < M; ++m) {
-                double* qp = T.q + ((int64_t)m * NY + r) * NX;
-                const double qold = *qp;
-                const double fxm1 = fx[(0 * M + m) * L::PNX + 1];
-                const double fxp0 = fx[(1 * M + m) * L::PNX];
-                const double gyu_l = (c >= 1) ? gy[(1 * M + m) * L::PNX - 1] : 0.0;
-                const double gyd_r = gy[(0 * M + m) * L::PNX + 1];
-                const double gyd = gy[(0 * M + m) * L::PNX];
-                const double gyu = gy[(1 * M + m) * L::PNX];
-                const double fmv = (fxm1 + gyu) + gyd_r;   // fm(i+1, j)
-                const double fpv = (fxp0 + gyu_l) + gyd;   // fp(i, j)
-                const double gmv = GXs_new[m] + S.FYm2[m];   // gm(i, j+1)
-                const double gpv = S.GXs_prev[m] + S.FYp3[m];  // gp(i, j)
-                *qp = qold - T.dtdx * (fmv - fpv) - T.dtdy * (gmv - gpv);
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < M; ++m) S.GXs_prev[m] = GXs_new[m];
-    }
-
-    // ---------------- S3: x-row k = s-2: limiter, corrections, transverse ----------------
-    {
-        const int k = s - 2;
-        if (T.active && (STEADY || (k >= 0 && k <= NY - 2))) {
-            double* fx = T.sb + L::FX + s4(2) * (2 * M * L::PNX);
-            const bool xint = (STEADY || k >= 1) && c >= 1;
-            if (xint) {
-                const double* xw = T.sb + L::XW + s2(2) * (W * M * L::PNX);
-                double cq[M];
-#pragma unroll
-                for (int m = 0; m < M; ++m) cq[m] = 0.0;
-                if (meth.second_order()) {
-                    if (c >= MBC && c <= MBC + MX) {
-#pragma unroll
-                        for (int mw = 0; mw < W; ++mw) {
-                            const int mth = meth.lim(mw);
-                            if (mth == 0) continue;
-                            double wn2 = S.xwl[mw][0] * S.xwl[mw][0];
-                            double dl = xw[(mw * M + 0) * L::PNX - 1] * S.xwl[mw][0];
-                            double dr = S.xwl[mw][0] * xw[(mw * M + 0) * L::PNX + 1];
-#pragma unroll
-                            for (int m = 1; m < M; ++m) {
-                                const double wc = S.xwl[mw][m];
-                                wn2 = wn2 + wc * wc;
-                                dl = dl + xw[(mw * M + m) * L::PNX - 1] * wc;
-                                dr = dr + wc * xw[(mw * M + m) * L::PNX + 1];
-                            }
-                            if (wn2 == 0.0) continue;
-                            const double rr = (S.xsl[mw] > 0.0) ? dl / wn2 : dr / wn2;
-                            const double phi = limiter_phi(mth, rr);
-#pragma unroll
-                            for (int m = 0; m < M; ++m) S.xwl[mw][m] = phi * S.xwl[mw][m];
-                        }
-                    }
-#pragma unroll
-                    for (int m = 0; m < M; ++m) {
-                        double acc;
-                        {
-                            const double as = fabs(S.xsl[0]);
-                            acc = as * (1.0 - as * T.dtdx) * S.xwl[0][m];
-                        }
-#pragma unroll
-                        for (int mw = 1; mw < W; ++mw) {
-                            const double as = fabs(S.xsl[mw]);
-                            acc = acc + as * (1.0 - as * T.dtdx) * S.xwl[mw][m];
-                        }
-                        cq[m] = acc;
-                    }
-                }
-                double am[M], ap[M];
-#pragma unroll
-                for (int m = 0; m < M; ++m) {
-                    double fmv = (c <= NX - 2) ? S.xam[m] : 0.0;
-                    double fpv = (c <= NX - 2) ? -S.xap[m] : 0.0;
-                    if (meth.second_order()) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
-                    fx[(0 * M + m) * L::PNX] = fmv;
-                    fx[(1 * M + m) * L::PNX] = fpv;
-                    am[m] = S.xam[m];
-                    ap[m] = S.xap[m];
-                    if (meth.transverse2() && c <= NX - 2) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
-                }
-                double* gl = T.sb + L::GL + s2(2) * (2 * M * L::PNX);
-                if (meth.transverse()) {
-                    double bm[M], bp[M];
-                    // imp = 1: aux2(i-1, kv=2), aux3(i-1, kv=2) = v at column c-1, rows k, k+1
-                    sol.rpt2(1, am, S.xR, AUXV(1, -1, 2), AUXV(1, -1, 1), bm, bp);
-#pragma unroll
-                    for (int m = 0; m < M; ++m) {
-                        gl[(0 * M + m) * L::PNX] = T.hdtdx * bm[m];
-                        gl[(1 * M + m) * L::PNX] = T.hdtdx * bp[m];
-                    }
-                    sol.rpt2(1, ap, S.xR, AUXV(1, 0, 2), AUXV(1, 0, 1), bm, bp);
-#pragma unroll
-                    for (int m = 0; m < M; ++m) {
-                        S.gRmx[m] = T.hdtdx * bm[m];
-                        S.gRpx[m] = T.hdtdx * bp[m];
-                    }
-                } else {
-#pragma unroll
-                    for (int m = 0; m < M; ++m) {
-                        gl[(0 * M + m) * L::PNX] = 0.0;
-                        gl[(1 * M + m) * L::PNX] = 0.0;
-                        S.gRmx[m] = S.gRpx[m] = 0.0;
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int m = 0; m < M; ++m) {
-                    fx[(0 * M + m) * L::PNX] = 0.0;
-                    fx[(1 * M + m) * L::PNX] = 0.0;
-                }
-            }
-        }
-    }
-
-    // ---------------- S2: x-row k = s-1: Riemann problem at x-interface c ----------------
-    {
-        const int k = s - 1;
-        if (T.active && (STEADY || (k >= 1 && k <= NY - 2)) && c >= 1) {
-            const double* qr = T.sb + L::Q + s2(1) * (M * L::PNX);
-            double qL[M];
-#pragma unroll
-            for (int m = 0; m < M; ++m) qL[m] = qr[m * L::PNX - 1];
-            sol.rpn2(1, qL, S.q_m1, AUXV(0, 0, 1), S.xwl, S.xsl, S.xam, S.xap, S.xR);
-            double* xw = T.sb + L::XW + s2(1) * (W * M * L::PNX);
-#pragma unroll
-            for (int mw = 0; mw < W; ++mw) {
-#pragma unroll
-                for (int m = 0; m < M; ++m) xw[(mw * M + m) * L::PNX] = S.xwl[mw][m];
-                if (c >= MBC && c <= MBC + MX) S.cfl = dmax(dmax(S.cfl, T.dtdx * S.xsl[mw]), -T.dtdx * S.xsl[mw]);
-            }
-        }
-    }
-
-    // ---------------- S1: row s ----------------
-    {
-        double yw_n[W][M], ys_n[W], yam_n[M], yap_n[M], ydotr[W];
-        typename SOL::Roe yR_n{};
-#pragma unroll
-        for (int mw = 0; mw < W; ++mw) {
-            ys_n[mw] = ydotr[mw] = 0.0;
-#pragma unroll
-            for (int m = 0; m < M; ++m) yw_n[mw][m] = 0.0;
-        }
-#pragma unroll
-        for (int m = 0; m < M; ++m) yam_n[m] = yap_n[m] = 0.0;
-        if (T.active && (STEADY || s < NY)) {
-            double* qr = T.sb + L::Q + s2(0) * (M * L::PNX);
-#pragma unroll
-            for (int m = 0; m < M; ++m) {
-                if (T.save_last) T.qlast[((int64_t)m * NY + s) * NX] = S.qcur[m];
-                qr[m * L::PNX] = S.qcur[m];
-            }
-            // raw y-interface s (between rows s-1 and s)
-            if (T.ycol && (STEADY || s >= 1)) {
-                sol.rpn2(2, S.q_m1, S.qcur, AUXV(1, 0, 0), yw_n, ys_n, yam_n, yap_n, yR_n);
-#pragma unroll
-                for (int mw = 0; mw < W; ++mw) {
-                    double d = S.yw_f[mw][0] * yw_n[mw][0];
-#pragma unroll
-                    for (int m = 1; m < M; ++m) d = d + S.yw_f[mw][m] * yw_n[mw][m];
-                    ydotr[mw] = d;  // dot(w(s-1), w(s))
-                }
-            }
-        }
-
-        // finalize y-interface f = s-1 (own column)
-        const int f = s - 1;
-        double FYm_new[M], FYp_new[M], GYd[M], GYu[M];
-#pragma unroll
-        for (int m = 0; m < M; ++m) FYm_new[m] = FYp_new[m] = GYd[m] = GYu[m] = 0.0;
-        if (T.ycol && (STEADY || (f >= 1 && f <= NY - 1))) {
-            const bool inner = STEADY || (f >= MBC && f <= MBC + MX);
-            const bool god = STEADY || f <= NY - 2;
-            double w[W][M];
-#pragma unroll
-            for (int mw = 0; mw < W; ++mw)
-#pragma unroll
-                for (int m = 0; m < M; ++m) w[mw][m] = S.yw_f[mw][m];
-            if (inner) {
-#pragma unroll
-                for (int mw = 0; mw < W; ++mw) S.cfl = dmax(dmax(S.cfl, T.dtdy * S.ys_f[mw]), -T.dtdy * S.ys_f[mw]);
-            }
-            double cq[M];
-#pragma unroll
-            for (int m = 0; m < M; ++m) cq[m] = 0.0;
-            if (meth.second_order()) {
-                if (inner) {
-#pragma unroll
-                    for (int mw = 0; mw < W; ++mw) {
-                        const int mth = meth.lim(mw);
-                        if (mth == 0) continue;
-                        double wn2 = S.yw_f[mw][0] * S.yw_f[mw][0];
-#pragma unroll
-                        for (int m = 1; m < M; ++m) wn2 = wn2 + S.yw_f[mw][m] * S.yw_f[mw][m];
-                        if (wn2 == 0.0) continue;
-                        const double rr = (S.ys_f[mw] > 0.0) ? S.ydotl[mw] / wn2 : ydotr[mw] / wn2;
-                        const double phi = limiter_phi(mth, rr);
-#pragma unroll
-                        for (int m = 0; m < M; ++m) w[mw][m] = phi * w[mw][m];
-                    }
-                }
-#pragma unroll
-                for (int m = 0; m < M; ++m) {
-                    double acc;
-                    {
-                        const double as = fabs(S.ys_f[0]);
-                        acc = as * (1.0 - as * T.dtdy) * w[0][m];
-                    }
-#pragma unroll
-                    for (int mw = 1; mw < W; ++mw) {
-                        const double as = fabs(S.ys_f[mw]);
-                        acc = acc + as * (1.0 - as * T.dtdy) * w[mw][m];
-                    }
-                    cq[m] = acc;
-                }
-            }
-            double am[M], ap[M];
-#pragma unroll
-            for (int m = 0; m < M; ++m) {
-                double fmv = god ? S.yam_f[m] : 0.0;
-                double fpv = god ? -S.yap_f[m] : 0.0;
-                if (meth.second_order()) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
-                FYm_new[m] = fmv;
-                FYp_new[m] = fpv;
-                am[m] = S.yam_f[m];
-                ap[m] = S.yap_f[m];
-                if (meth.transverse2() && god) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
-            }
-            double gLm[M], gLp[M], gRm[M], gRp[M];
-            if (meth.transverse()) {
-                double bm[M], bp[M];
-                // imp = 1: aux2(j-1, kv=1), aux3(j-1, kv=1) = u at columns c, c+1, row f-1
-                sol.rpt2(2, am, S.yR_f, AUXV(0, 0, 2), AUXV(0, 1, 2), bm, bp);
-#pragma unroll
-                for (int m = 0; m < M; ++m) { gLm[m] = T.hdtdy * bm[m]; gLp[m] = T.hdtdy * bp[m]; }
-                sol.rpt2(2, ap, S.yR_f, AUXV(0, 0, 1), AUXV(0, 1, 1), bm, bp);
-#pragma unroll
-                for (int m = 0; m < M; ++m) { gRm[m] = T.hdtdy * bm[m]; gRp[m] = T.hdtdy * bp[m]; }
-            } else {
-#pragma unroll
-                for (int m = 0; m < M; ++m) gLm[m] = gLp[m] = gRm[m] = gRp[m] = 0.0;
-            }
-            // cell row f-1 is complete: gadd(f-1,.,1) = (0 - gL(f)) - gR(f-1)
-            if (STEADY || f - 1 >= 1) {
-#pragma unroll
-                for (int m = 0; m < M; ++m) {
-                    GYd[m] = -gLm[m] - S.gRm_prev[m];
-                    GYu[m] = -gLp[m] - S.gRp_prev[m];
-                }
-            }
-#pragma unroll
-            for (int m = 0; m < M; ++m) { S.gRm_prev[m] = gRm[m]; S.gRp_prev[m] = gRp[m]; }
-        }
-        // GY of cell row s-2 (zero outside the y-columns and for row 0)
-        if (T.active && (STEADY || (s >= 2 && s - 2 <= NY - 2))) {
-            double* gy = T.sb + L::GY + s4(2) * (2 * M * L::PNX);
-#pragma unroll
-            for (int m = 0; m < M; ++m) {
-                gy[(0 * M + m) * L::PNX] = GYd[m];
-                gy[(1 * M + m) * L::PNX] = GYu[m];
-            }
-        }
-        // delay lines: FYm(f) serves row f-1 two iterations on, FYp(f) row f three on
-#pragma unroll
-        for (int m = 0; m < M; ++m) {
-            S.FYm2[m] = S.FYm1[m];
-            S.FYm1[m] = FYm_new[m];
-            S.FYp3[m] = S.FYp2[m];
-            S.FYp2[m] = S.FYp1[m];
-            S.FYp1[m] = FYp_new[m];
-        }
-        // shift the y window
-#pragma unroll
-        for (int mw = 0; mw < W; ++mw) {
-            S.ydotl[mw] = ydotr[mw];
-            S.ys_f[mw] = ys_n[mw];
-#pragma unroll
-            for (int m = 0; m < M; ++m) S.yw_f[mw][m] = yw_n[mw][m];
-        }
-#pragma unroll
-        for (int m = 0; m < M; ++m) {
-            S.yam_f[m] = yam_n[m];
-            S.yap_f[m] = yap_n[m];
-            S.q_m1[m] = S.qcur[m];
-            S.qcur[m] = qnext[m];
-        }
-        S.yR_f = yR_n;
-
-        // aux row s+1
-        if (STEADY || s + 1 <= NY - 1) {
-            if constexpr (SWIRL) {
-                // node thread c (c in [0, NX]) computes psi at node (c, s+2)
-                const double pn = (T.tx * T.ty[s + 2]) / pi;
-                if (T.node) T.nb[s2(-2) * L::NDS] = pn;
-                if (T.active) {
-                    double* ax = T.sb + L::AX + s4(-1) * (NAUX * L::PNX);
-                    ax[0 * L::PNX] = T.vty * (pn - S.pcur);
-                    ax[1 * L::PNX] = -T.vtx * (T.nb[s2(-1) * L::NDS + 1] - S.pcur);
-                }
-                S.pcur = pn;
-            } else if constexpr (AUXK == AUX_STORED) {
-                if (T.active) {
-                    double* ax = T.sb + L::AX + s4(-1) * (NAUX * L::PNX);
-#pragma unroll
-                    for (int kk = 0; kk < NAUX; ++kk) ax[kk * L::PNX] = T.aux[(kk * NY + s + 1) * NX];
-                }
-            }
-        }
-    }
-    __syncthreads();
-}
-
-template <int NX, bool SWIRL>
-__host__ __device__ constexpr int pipe_threads_per_patch() { return SWIRL ? NX + 1 : NX; }
-
-}  // namespace
-
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
-__global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
-    constexpr int M = SOL::M;
-    constexpr int W = SOL::W;
-    constexpr int NX = MX + 2 * MBC;
-    constexpr int NY = NX;
-    constexpr bool SWIRL = AUXK == AUX_SWIRL;
-    constexpr int TPP = pipe_threads_per_patch<NX, SWIRL>();
-    constexpr int PPB = TPB / TPP;
-    using L = PipeSmem<NX, PPB, M, W, NAUX, SWIRL>;
-    extern __shared__ double smem[];
-
-    // Threads (pl, c): c in [0, NX) owns column c of patch pl; with the swirl
-    // velocities one more thread per patch (c == NX) computes the last node
-    // column of the stream function.
-    const int t = threadIdx.x;
-    const int pl = t / TPP;
-    const int c = t - pl * TPP;
-    const int pg = blockIdx.x * PPB + pl;
-    const bool patch_ok = (pl < PPB) && (pg < a.npatches);
-    const bool active = patch_ok && c < NX;
-    const int pls = patch_ok ? pl : 0;  // threads without a patch read (never write) patch 0's rows
-    const int cc = c < NX ? c : NX - 1;
-    const int slot = patch_ok ? a.slots[pg] : 0;
-    const PatchMeta meta = patch_ok ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0};
-    const SOL sol{a.grav, a.gamma, a.gamma1};
-
-    PipeThread T;
-    T.c = cc;
-    T.active = active;
-    T.node = SWIRL && patch_ok;
-    T.save_last = active && (meta.flags & PATCH_SAVE_LAST);
-    T.ycol = active && c >= 1 && c <= NX - 2;
-    T.q = a.q + (int64_t)slot * a.q_stride + cc;
-    T.qlast = a.qlast + (int64_t)slot * a.q_stride + cc;
-    T.aux = (AUXK == AUX_STORED && active) ? a.aux + (int64_t)slot * a.aux_stride + cc : nullptr;
-    T.sb = smem + pls * NX + cc;
-    T.nb = smem + L::ND + pls * (NX + 1) + c;
-    T.ty = smem + L::TY + pls * (NX + 1);
-    // dtdx1d is uniform without capacity, so 0.5*(dtdx1d(i-1)+dtdx1d(i)) == dtdx exactly
-    T.dtdx = a.dt / meta.dx;
-    T.dtdy = a.dt / meta.dy;
-    T.hdtdx = 0.5 * T.dtdx;  // the reference's 0.5d0*dtdx*b, evaluated left to right
-    T.hdtdy = 0.5 * T.dtdy;
-    T.vty = a.vt / meta.dy;
-    T.vtx = a.vt / meta.dx;
-    T.tx = 0.0;
-
-    PipeState<SOL> S;
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-        S.qcur[m] = active ? T.q[(int64_t)m * NY * NX] : 0.0;
-        S.q_m1[m] = 0.0;
-        S.yam_f[m] = S.yap_f[m] = 0.0;
-        S.gRm_prev[m] = S.gRp_prev[m] = 0.0;
-        S.xam[m] = S.xap[m] = 0.0;
-        S.gRmx[m] = S.gRpx[m] = 0.0;
-        S.GXu_prev[m] = S.GXs_prev[m] = 0.0;
-        S.FYm1[m] = S.FYm2[m] = S.FYp1[m] = S.FYp2[m] = S.FYp3[m] = 0.0;
-    }
-#pragma unroll
-    for (int mw = 0; mw < W; ++mw) {
-        S.ys_f[mw] = S.ydotl[mw] = S.xsl[mw] = 0.0;
-#pragma unroll
-        for (int m = 0; m < M; ++m) S.yw_f[mw][m] = S.xwl[mw][m] = 0.0;
-    }
-    S.yR_f = typename SOL::Roe{};
-    S.xR = typename SOL::Roe{};
-    S.pcur = 0.0;
-    S.cfl = 0.0;
-
-    // ---- prologue: aux row 0 ----
-    if constexpr (SWIRL) {
-        // swirl/user_4.6/b4step2.f with swirl/psi.f:
-        //   u(i,j) = vty*(psi(xll,yll+dy) - psi(xll,yll)),  v(i,j) = -vtx*(psi(xll+dx,yll) - psi(xll,yll)),
-        //   psi(x,y) = (sin(pi x)**2 * sin(pi y)**2)/pi.
-        // The unit-square mesh with mx a power of two is dyadic (xll + dx is the
-        // next node's xll exactly; checked on the host), so psi is evaluated
-        // once per node: P(c,n) at the lower-left corner of cell (c,n).
-        constexpr double pi = 3.141592653589793;
-        {
-            const double x = meta.xlower + (double)(c - MBC) * meta.dx;
-            const double y = meta.ylower + (double)(c - MBC) * meta.dy;
-            const double sx = sin(pi * x), sy = sin(pi * y);
-            T.tx = sx * sx;
-            if (T.node) smem[L::TY + pls * (NX + 1) + c] = sy * sy;
-        }
-        __syncthreads();
-        const double p0 = (T.tx * T.ty[0]) / pi, p1 = (T.tx * T.ty[1]) / pi;
-        if (T.node) {
-            T.nb[0] = p0;          // node row 0
-            T.nb[L::NDS] = p1;     // node row 1
-        }
-        __syncthreads();
-        if (active) {
-            T.sb[L::AX + 0 * L::PNX] = T.vty * (p1 - p0);
-            T.sb[L::AX + 1 * L::PNX] = -T.vtx * (T.nb[1] - p0);
-        }
-        S.pcur = p1;
-    } else if constexpr (AUXK == AUX_STORED) {
-        if (active) {
-#pragma unroll
-            for (int k = 0; k < NAUX; ++k) T.sb[L::AX + k * L::PNX] = T.aux[(k * NY + 0) * NX];
-        }
-    }
-    __syncthreads();
-
-    // ---- rows: ramp-up, steady state (unrolled by the ring period 4), ramp-down ----
-    int s = 0;
-    for (; s < 4; ++s) pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, -1, false>(a, sol, T, S, s);
-    constexpr int NSTEADY = NY - 5;  // s = 4 .. NY-2
-    for (int rnd = 0; rnd < NSTEADY / 4; ++rnd, s += 4) {
-        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 0, true>(a, sol, T, S, s);
-        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 1, true>(a, sol, T, S, s + 1);
-        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 2, true>(a, sol, T, S, s + 2);
-        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 3, true>(a, sol, T, S, s + 3);
-    }
-    for (; s <= NY + 2; ++s) pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, -1, false>(a, sol, T, S, s);
-
-    // ---- CFL: warp max, one atomic per warp ----
-    double cfl = S.cfl;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
-    if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg_p(a.cfl_out, cfl);
-}
-
-// ---------------------------------------------------------------------------
-// Host-side launcher
-// ---------------------------------------------------------------------------
-namespace {
-
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
-cudaError_t launch_pipe_one(const StepArgs& a, cudaStream_t st) {
-    constexpr int NX = MX + 2 * MBC;
-    constexpr int PPB = TPB / pipe_threads_per_patch<NX, AUXK == AUX_SWIRL>();
-    static_assert(PPB >= 1, "patch wider than the CTA");
-    using L = PipeSmem<NX, PPB, SOL::M, SOL::W, NAUX, AUXK == AUX_SWIRL>;
-    const size_t bytes = (size_t)L::TOTAL * sizeof(double);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(step_kernel_pipe<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    const int blocks = (a.npatches + PPB - 1) / PPB;
-    if (blocks == 0) return cudaSuccess;
-    step_kernel_pipe<SOL, MX, MBC, AUXK, NAUX, TPB, LIM><<<blocks, TPB, bytes, st>>>(a);
-    return cudaGetLastError();
-}
-
-// Limiter specialisation: every wave limited with the same code and order (2, 2).
-template <class SOL>
-int fixed_limiter(const StepArgs& a) {
-    if (a.order0 != 2 || a.order1 != 2) return 0;
-    const int l = a.mthlim[0];
-    for (int mw = 1; mw < SOL::W; ++mw)
-        if (a.mthlim[mw] != l) return 0;
-    return (l == 3 || l == 4) ? l : 0;
-}
-
-template <class SOL, int MX, int AUXK, int NAUX>
-cudaError_t launch_pipe_lim(const StepArgs& a, cudaStream_t st) {
-    switch (fixed_limiter<SOL>(a)) {
-        case 3: return launch_pipe_one<SOL, MX, 2, AUXK, NAUX, 128, 3>(a, st);
-        case 4: return launch_pipe_one<SOL, MX, 2, AUXK, NAUX, 128, 4>(a, st);
-        default: return launch_pipe_one<SOL, MX, 2, AUXK, NAUX, 128, 0>(a, st);
-    }
-}
-
-template <class SOL, int AUXK, int NAUX>
-cudaError_t launch_pipe_mx(int mx, int mbc, const StepArgs& a, cudaStream_t st) {
-    if (mbc != 2) return cudaErrorNotSupported;
-    switch (mx) {
-        case 8: return launch_pipe_lim<SOL, 8, AUXK, NAUX>(a, st);
-        case 16: return launch_pipe_lim<SOL, 16, AUXK, NAUX>(a, st);
-        case 32: return launch_pipe_lim<SOL, 32, AUXK, NAUX>(a, st);
-        default: return cudaErrorNotSupported;
-    }
-}
-
-}  // namespace
-
-// cudaErrorNotSupported: no pipelined form for this (solver, mx, mbc, aux).
 cudaError_t launch_step_pipe(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
                              cudaStream_t st) {
-    if (mx != my) return cudaErrorNotSupported;
-    switch (solver) {
-        case SOLVER_ADVECTION:
-            if (mwaves != 1) return cudaErrorNotSupported;
-            if (aux_kind == AUX_SWIRL) return launch_pipe_mx<AdvectionSolver<1>, AUX_SWIRL, 2>(mx, mbc, a, st);
-            if (aux_kind == AUX_STORED && a.maux == 2)
-                return launch_pipe_mx<AdvectionSolver<1>, AUX_STORED, 2>(mx, mbc, a, st);
-            return cudaErrorNotSupported;
-        case SOLVER_SWE_ROE:
-            if (mwaves != 3 || aux_kind != AUX_NONE) return cudaErrorNotSupported;
-            return launch_pipe_mx<SweRoeSolver, AUX_NONE, 0>(mx, mbc, a, st);
-        case SOLVER_EULER4_ROE:
-            if (mwaves != 4 || aux_kind != AUX_NONE) return cudaErrorNotSupported;
-            return launch_pipe_mx<Euler4RoeSolver, AUX_NONE, 0>(mx, mbc, a, st);
-        default: return cudaErrorNotSupported;
-    }
+    return launch_step_pipe_t<double>(solver, aux_kind, mwaves, mx, my, mbc, a, st);
 }
 
 }  // namespace fcb

@@ -45,6 +45,11 @@ enum fcb_solver_kind {
 };
 
 /* Initial conditions / b4step2 hooks of the configured applications. */
+enum fcb_precision {
+    FCB_PRECISION_FP64 = 0,  /* the reference's FP64 arithmetic */
+    FCB_PRECISION_MIXED = 1  /* FP32 solves / limiters / ghost interpolation, FP64 sums and state */
+};
+
 enum fcb_problem {
     FCB_PROBLEM_SWIRL = 0,      /* advection/2d/swirl: qinit.f, b4step2.f velocities; p[0] = tperiod */
     FCB_PROBLEM_RADIALDAM = 1,  /* dam break: p = {x0, y0, r0, h_in, h_out} */
@@ -92,6 +97,11 @@ typedef struct fcb_options {
      * (swirl advection, mx = 8, 16, 32), 3 = software-pipelined CTA form (one
      * barrier per row; mx = 8, 16, 32); all give identical results */
     int step_variant;
+    /* arithmetic of the patch update: 0 = FP64 throughout (the reference's
+     * arithmetic), 1 = mixed: Riemann solves, limiters, transverse parts and
+     * ghost interpolation in FP32, flux sums, cell update, state and mass sums
+     * in FP64 (pipelined step form only); enum fcb_precision */
+    int precision;
 } fcb_options_t;
 
 typedef struct fcb_counters {

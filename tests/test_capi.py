@@ -42,7 +42,8 @@ def test_options_layout_matches_header(built, tmp_path):
         '#include <stdio.h>\n#include <stddef.h>\n#include "fclaw_b200.h"\n'
         "int main(void){printf(\"%zu %zu %zu %zu\\n\", sizeof(fcb_options_t),"
         " offsetof(fcb_options_t, refine_threshold), offsetof(fcb_options_t, problem_params),"
-        " sizeof(fcb_counters_t)); return 0;}\n")
+        " sizeof(fcb_counters_t)); printf(\"%zu %zu\\n\", offsetof(fcb_options_t, step_variant),"
+        " offsetof(fcb_options_t, precision)); return 0;}\n")
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
@@ -52,6 +53,8 @@ def test_options_layout_matches_header(built, tmp_path):
     assert int(out[1]) == _Options.refine_threshold.offset
     assert int(out[2]) == _Options.problem_params.offset
     assert int(out[3]) == ctypes.sizeof(_Counters)
+    assert int(out[4]) == _Options.step_variant.offset
+    assert int(out[5]) == _Options.precision.offset
 
 
 def test_invalid_options_rejected_before_any_device_call(built):
@@ -62,6 +65,15 @@ def test_invalid_options_rejected_before_any_device_call(built):
     o = built.Options(mthbc=(0, 1, 1, 1))
     with pytest.raises(built.FcbError) as e:
         built.Solver(o)
+    assert e.value.code == 1
+    # the mixed-precision update exists in the pipelined step form only
+    for variant in (1, 2):
+        o = built.Options(precision=built.PRECISION_MIXED, step_variant=variant)
+        with pytest.raises(built.FcbError) as e:
+            built.Solver(o)
+        assert e.value.code == 1
+    with pytest.raises(built.FcbError) as e:
+        built.Solver(built.Options(precision=2))
     assert e.value.code == 1
 
 
