@@ -104,7 +104,7 @@ struct PipeState {
     double GXu_prev[M], GXs_prev[M];                     // S4 -> S4, S4 -> S5
     R FYm1[M], FYm2[M], FYp1[M], FYp2[M], FYp3[M];       // y fluxes of the own column, delayed
     double pcur;                                         // swirl: psi at node (c, s+1)
-    R cfl;
+    R smax_x, smax_y;  // largest |s| over the CFL interfaces of each direction
 };
 
 // Per-thread constants: column, flags and this thread's element of the rings.
@@ -149,12 +149,16 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
         else return R(0);
     };
 
-    // prefetch q(c, s+1)
-    double qnext[M];
+    // prefetch q(c, s+1); load q(c, s-4) for this iteration's update early
+    double qnext[M], qold[M];
+    const bool upd = T.active && (STEADY || (s - 4 >= 0 && s - 4 <= NY - 2)) && c <= NX - 2;
     {
         const bool on = T.active && (STEADY || s + 1 < NY);
 #pragma unroll
-        for (int m = 0; m < M; ++m) qnext[m] = on ? T.q[((int64_t)m * NY + s + 1) * NX] : 0.0;
+        for (int m = 0; m < M; ++m) {
+            qnext[m] = on ? T.q[((int64_t)m * NY + s + 1) * NX] : 0.0;
+            qold[m] = upd ? T.q[((int64_t)m * NY + s - 4) * NX] : 0.0;
+        }
     }
 
     // ---------------- S4: GX(c, k), k = s-3 ----------------
@@ -183,13 +187,12 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
     // ---------------- S5: update cell row r = s-4 ----------------
     {
         const int r = s - 4;
-        if (T.active && (STEADY || (r >= 0 && r <= NY - 2)) && c <= NX - 2) {
+        if (upd) {
             const R* fx = T.rb + L::FX + s4(4) * (2 * M * L::PNX);
             const double* gy = T.db + L::GY + s4(4) * (2 * M * L::PNX);
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 double* qp = T.q + ((int64_t)m * NY + r) * NX;
-                const double qold = *qp;
                 const double fxm1 = fx[(0 * M + m) * L::PNX + 1];  // FP32 flux parts widen exactly
                 const double fxp0 = fx[(1 * M + m) * L::PNX];
                 const double gyu_l = (c >= 1) ? gy[(1 * M + m) * L::PNX - 1] : 0.0;
@@ -200,7 +203,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 const double fpv = (fxp0 + gyu_l) + gyd;   // fp(i, j)
                 const double gmv = GXs_new[m] + (double)S.FYm2[m];    // gm(i, j+1)
                 const double gpv = S.GXs_prev[m] + (double)S.FYp3[m];  // gp(i, j)
-                *qp = qold - T.dtdx * (fmv - fpv) - T.dtdy * (gmv - gpv);
+                *qp = qold[m] - T.dtdx * (fmv - fpv) - T.dtdy * (gmv - gpv);
             }
         }
 #pragma unroll
@@ -319,7 +322,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
             for (int mw = 0; mw < W; ++mw) {
 #pragma unroll
                 for (int m = 0; m < M; ++m) xw[(mw * M + m) * L::PNX] = S.xwl[mw][m];
-                if (c >= MBC && c <= MBC + MX) S.cfl = dmax(dmax(S.cfl, T.rdtdx * S.xsl[mw]), -T.rdtdx * S.xsl[mw]);
+                if (c >= MBC && c <= MBC + MX) S.smax_x = dmax(S.smax_x, fabs(S.xsl[mw]));
             }
         }
     }
@@ -381,7 +384,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 for (int m = 0; m < M; ++m) w[mw][m] = S.yw_f[mw][m];
             if (inner) {
 #pragma unroll
-                for (int mw = 0; mw < W; ++mw) S.cfl = dmax(dmax(S.cfl, T.rdtdy * S.ys_f[mw]), -T.rdtdy * S.ys_f[mw]);
+                for (int mw = 0; mw < W; ++mw) S.smax_y = dmax(S.smax_y, fabs(S.ys_f[mw]));
             }
             R cq[M];
 #pragma unroll
@@ -593,7 +596,7 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     S.yR_f = typename SOL::Roe{};
     S.xR = typename SOL::Roe{};
     S.pcur = 0.0;
-    S.cfl = R(0);
+    S.smax_x = S.smax_y = R(0);
 
     // ---- prologue: aux row 0 ----
     if constexpr (SWIRL) {
@@ -644,7 +647,10 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     for (; s <= NY + 2; ++s) pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, -1, false>(a, sol, T, S, s);
 
     // ---- CFL: warp max, one atomic per warp ----
-    double cfl = (double)S.cfl;
+    // flux2: cfl = max(cfl, dtdx*s, -dtdx*s) over the interfaces.  Rounding is
+    // monotone, so max_i fl(dtdx*|s_i|) == fl(dtdx * max_i |s_i|): one product
+    // per direction gives the reference's value exactly.
+    double cfl = (double)dmax(T.rdtdx * S.smax_x, T.rdtdy * S.smax_y);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
     if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg_p(a.cfl_out, cfl);
