@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                    help="fp64: the reference's arithmetic; mixed: FP32 solves, FP64 sums and state")
+    p.add_argument("--macro-graph", type=int, default=2, choices=[0, 1, 2],
+                   help="1: replay each macro step from a captured CUDA graph; 0: host launches; 2: automatic")
     p.add_argument("--step-variant", type=int, default=0, help="0 library's choice, 1 CTA rows, 2 warp, 3 pipelined CTA")
     return p.parse_args()
 
@@ -208,6 +210,7 @@ def run_ours(args, rank, world, local_rank):
     opts = workloads.uniform_swirl(args.level, args.mx)
     opts.step_variant = args.step_variant
     opts.precision = fcb.PRECISION_MIXED if args.precision == "mixed" else fcb.PRECISION_FP64
+    opts.macro_graph = args.macro_graph
     dt = workloads.swirl_dt(args.level, args.mx)
     s = fcb.Solver(opts, stream=stream.cuda_stream)
     s.initialize()

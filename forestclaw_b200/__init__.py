@@ -62,13 +62,14 @@ class _Options(ctypes.Structure):
         ("problem_params", ctypes.c_double * 32),
         ("step_variant", ctypes.c_int),
         ("precision", ctypes.c_int),
+        ("macro_graph", ctypes.c_int),
     ]
 
 
 class _Counters(ctypes.Structure):
     _fields_ = [(n, ctypes.c_longlong) for n in (
         "count_amr_advance", "count_amr_new_domain", "count_amr_regrid", "count_single_step",
-        "count_ghost_waves", "count_kernel_launches")]
+        "count_ghost_waves", "count_kernel_launches", "count_graph_replays")]
 
 
 @dataclass
@@ -115,13 +116,16 @@ class Options:
     step_variant: int = 0
     # 0 = FP64 throughout, 1 = mixed FP32 solves / FP64 accumulation
     precision: int = PRECISION_FP64
+    # 1: advance_all_levels replays the macro-step as one CUDA graph; 0: host
+    # launches; 2: graph once a macro step updates three or more level batches
+    macro_graph: int = 2
 
     def to_c(self) -> _Options:
         o = _Options()
         for name in ("mx", "my", "mbc", "meqn", "maux", "refinement_criteria", "threshold_variable",
                      "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
                      "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
-                     "reduce_cfl", "solver_kind", "problem", "step_variant", "precision"):
+                     "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
                      "desired_cfl", "grav", "gamma"):

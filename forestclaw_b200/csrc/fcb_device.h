@@ -31,9 +31,14 @@ struct StepArgs {
     int32_t mthlim[8];
     double dt;
     double vt;             // swirl: cos(2 pi (t + dt/2) / tperiod)
+    const double* dyn;     // non-null: {dt, vt} read from device memory (one macro-step graph serves every step)
     double grav, gamma, gamma1;
     unsigned long long* cfl_out;  // atomicMax on the bits of a non-negative double
 };
+#ifdef __CUDACC__
+__device__ __forceinline__ double step_dt(const StepArgs& a) { return a.dyn ? a.dyn[0] : a.dt; }
+__device__ __forceinline__ double step_vt(const StepArgs& a) { return a.dyn ? a.dyn[1] : a.vt; }
+#endif
 
 // Ghost-cell operations, one record per reference kernel call.
 enum GhostOpType : int32_t {

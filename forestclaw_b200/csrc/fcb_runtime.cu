@@ -69,21 +69,39 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
     if (opt_.precision == 1 && (opt_.step_variant == 1 || opt_.step_variant == 2))
         bad("the mixed-precision update exists in the pipelined step form only");
     if ((opt_.mx & (opt_.mx - 1)) != 0) bad("mx must be a power of two");
+    if (opt_.macro_graph < 0 || opt_.macro_graph > 2) bad("macro_graph must be 0, 1 or 2");
     nx_ = opt_.mx + 2 * opt_.mbc;
     ny_ = opt_.my + 2 * opt_.mbc;
     const int64_t ps = (int64_t)opt_.meqn * nx_ * ny_;
     stride_ = (ps + 31) / 32 * 32;  // 256-byte aligned slots
     check(cudaMalloc(&d_cfl_, 4 * sizeof(unsigned long long)), "cudaMalloc cfl");
+    check(cudaHostAlloc(&h_cfl_, sizeof(unsigned long long), cudaHostAllocDefault), "cudaHostAlloc cfl");
+}
+
+static double cfl_from_bits(unsigned long long b) {
+    double v;
+    std::memcpy(&v, &b, sizeof v);
+    return v;
+}
+
+double Context::read_cfl(const unsigned long long* d) {
+    check(cudaMemcpyAsync(h_cfl_, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st_), "cfl");
+    synchronize();
+    return cfl_from_bits(*h_cfl_);
 }
 
 Context::~Context() {
     cudaStreamSynchronize(st_);
+    drop_macro_graph();
+    if (cap_st_) cudaStreamDestroy(cap_st_);
+    cudaFreeHost(h_dyn_);
     cudaFree(d_q_);
     cudaFree(d_qlast_);
     cudaFree(d_qti_);
     cudaFree(d_qsave_);
     cudaFree(d_meta_);
     cudaFree(d_cfl_);
+    cudaFreeHost(h_cfl_);
     cudaFree(d_scratch_);
     cudaFree(d_stage_);
 }
@@ -148,6 +166,8 @@ PatchMeta Context::meta_of(const Leaf& l) const {
 }
 
 void Context::mesh_changed() {
+    ++mesh_version_;
+    drop_macro_graph();
     const int n = num_patches();
     nbrs_.resize(n);
     for (int p = 0; p < n; ++p) nbrs_[p] = forest_.neighbors(p);
@@ -445,6 +465,7 @@ void Context::run_plan(const GhostPlan& g) {
 
 void Context::ghost_update(int minlevel, int maxlevel, double, int time_interp) {
     if (!d_q_) throw Error(FCB_ERR_STATE, "ghost_update before initialize");
+    if (dry_) return;
     run_plan(plan(minlevel, maxlevel, time_interp));
 }
 
@@ -505,6 +526,31 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     a.gamma = opt_.gamma;
     a.gamma1 = opt_.gamma - 1.0;
     a.cfl_out = cfl_slot;
+    if (use_dyn_) {
+        // {dt, vt} of launch dyn_n_ of the macro step: written to the table by
+        // the dry pass, read from the device table by the launch itself
+        if (dry_) {
+            if (dyn_n_ >= (int)dyn_cap_) {
+                const size_t nc = std::max<size_t>(64, 2 * dyn_cap_);
+                double* np = nullptr;
+                check(cudaHostAlloc(&np, nc * 2 * sizeof(double), cudaHostAllocDefault), "cudaHostAlloc dyn");
+                if (h_dyn_) {
+                    std::copy(h_dyn_, h_dyn_ + 2 * dyn_cap_, np);
+                    cudaFreeHost(h_dyn_);
+                }
+                h_dyn_ = np;
+                dyn_cap_ = nc;
+            }
+            h_dyn_[2 * dyn_n_] = a.dt;
+            h_dyn_[2 * dyn_n_ + 1] = a.vt;
+            ++dyn_n_;
+            return;
+        }
+        if (!d_dyn_.p || 2 * (size_t)dyn_n_ + 2 > d_dyn_.cap)
+            throw Error(FCB_ERR_STATE, "step-parameter table not sized by the dry pass");
+        a.dyn = d_dyn_.p + 2 * dyn_n_;
+        ++dyn_n_;
+    }
     // The warp form computes each swirl velocity node once, which equals the
     // reference's per-cell evaluations because the unit-square mesh with mx a
     // power of two is dyadic (xll + dx == next xll exactly); checked at creation.
@@ -536,20 +582,11 @@ double Context::launch_level_step(int level, double t, double dt, unsigned long 
     return 0.0;
 }
 
-static double cfl_from_bits(unsigned long long b) {
-    double v;
-    std::memcpy(&v, &b, sizeof v);
-    return v;
-}
-
 double Context::update_single_step(int level, double t, double dt) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "update_single_step before initialize");
     check(cudaMemsetAsync(d_cfl_ + 1, 0, sizeof(unsigned long long), st_), "memset");
     launch_level_step(level, t, dt, d_cfl_ + 1);
-    unsigned long long b = 0;
-    check(cudaMemcpyAsync(&b, d_cfl_ + 1, sizeof b, cudaMemcpyDeviceToHost, st_), "cfl");
-    synchronize();
-    return cfl_from_bits(b);
+    return read_cfl(d_cfl_ + 1);
 }
 
 void Context::update_single_step_async(int level, double t, double dt) {
@@ -567,15 +604,12 @@ double Context::single_step_update(int patchno, double t, double dt, int iter, i
     check(cudaMemcpyAsync(d_pending_.p, pending_.data(), pending_.size() * 4, cudaMemcpyHostToDevice, st_), "pending");
     check(cudaMemsetAsync(d_cfl_ + 1, 0, sizeof(unsigned long long), st_), "memset");
     launch_level_step_slots(d_pending_.p, (int)pending_.size(), t, dt, d_cfl_ + 1);
-    unsigned long long b = 0;
-    check(cudaMemcpyAsync(&b, d_cfl_ + 1, sizeof b, cudaMemcpyDeviceToHost, st_), "cfl");
-    synchronize();
     pending_.clear();
-    return cfl_from_bits(b);
+    return read_cfl(d_cfl_ + 1);
 }
 
 void Context::timeinterp(int level, double alpha) {
-    if (level < 0 || level > QuadForest::kMaxLevel) return;
+    if (dry_ || level < 0 || level > QuadForest::kMaxLevel) return;
     const int b = ti_begin_[level], e = ti_begin_[level + 1];
     if (e == b) return;
     check(launch_timeinterp(d_q_, d_qlast_, d_qti_, stride_, d_ti_slots_.p + b, e - b, opt_.mx, opt_.my, opt_.mbc,
@@ -585,8 +619,7 @@ void Context::timeinterp(int level, double alpha) {
 }
 
 // fclaw2d_advance_all_levels (src/fclaw2d_advance.c:247-357)
-double Context::advance_all_levels(double t_curr, double dt) {
-    if (!initialized_) throw Error(FCB_ERR_STATE, "advance before initialize");
+void Context::run_schedule(double t_curr, double dt) {
     const int gmin = forest_.min_level(), gmax = forest_.max_level();
     struct Counter { int last_step, step_inc, total_steps; double current_time, dt_step; };
     std::vector<Counter> ts(opt_.maxlevel + 1);
@@ -605,7 +638,7 @@ double Context::advance_all_levels(double t_curr, double dt) {
             ts[l].step_inc = 1; ts[l].dt_step = dt / rf; ts[l].total_steps = rf;
         }
     }
-    check(cudaMemsetAsync(d_cfl_, 0, sizeof(unsigned long long), st_), "memset");
+    if (!dry_) check(cudaMemsetAsync(d_cfl_, 0, sizeof(unsigned long long), st_), "memset");
     std::function<void(int, int)> advance_level = [&](int level, int curr_fine_step) {
         launch_level_step(level, ts[level].current_time, ts[level].dt_step, d_cfl_);
         ts[level].last_step += ts[level].step_inc;
@@ -638,11 +671,105 @@ double Context::advance_all_levels(double t_curr, double dt) {
         }
     }
     ghost_update(gmin, gmax, ts[gmax].current_time, 0);
+}
+
+std::vector<uintptr_t> Context::macro_fingerprint() const {
+    return {(uintptr_t)d_q_, (uintptr_t)d_qlast_, (uintptr_t)d_qti_, (uintptr_t)d_meta_,
+            (uintptr_t)d_level_slots_.p, (uintptr_t)d_ti_slots_.p, (uintptr_t)d_ops_.p, (uintptr_t)d_groups_.p,
+            (uintptr_t)d_dyn_.p, (uintptr_t)d_cfl_, (uintptr_t)mesh_version_, (uintptr_t)plans_.size(),
+            (uintptr_t)dyn_n_, (uintptr_t)forest_.min_level(), (uintptr_t)forest_.max_level()};
+}
+
+void Context::drop_macro_graph() {
+    if (macro_exec_) cudaGraphExecDestroy(macro_exec_);
+    macro_exec_ = nullptr;
+    macro_key_.clear();
+    macro_seen_.clear();
+}
+
+// fclaw2d_advance_all_levels (src/fclaw2d_advance.c:247-346).  With
+// macro_graph on, the first call on a mesh runs eagerly (building and uploading
+// the ghost plans), the second captures the schedule into a CUDA graph, and
+// later calls replay it; every call first runs the schedule "dry" on the host
+// to fill the {dt, vt} table that the step launches read.
+double Context::advance_all_levels(double t_curr, double dt) {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "advance before initialize");
+    use_dyn_ = opt_.macro_graph != 0;
+    if (use_dyn_) {
+        dyn_n_ = 0;
+        dry_ = true;
+        try {
+            run_schedule(t_curr, dt);
+        } catch (...) {
+            dry_ = false;
+            throw;
+        }
+        dry_ = false;
+        // auto: a graph pays off once a macro step issues several level steps
+        // (subcycling); a single-level macro step is three launches
+        if (opt_.macro_graph == 2 && dyn_n_ < 3) use_dyn_ = false;
+    }
+    if (use_dyn_) {
+        d_dyn_.reserve(std::max<size_t>(2, 2 * (size_t)dyn_n_));
+        if (dyn_n_ > 0)
+            check(cudaMemcpyAsync(d_dyn_.p, h_dyn_, 2 * (size_t)dyn_n_ * sizeof(double), cudaMemcpyHostToDevice, st_),
+                  "step parameters");
+        const int n_launch = dyn_n_;
+        std::vector<uintptr_t> key = macro_fingerprint();
+        if (macro_exec_ && key == macro_key_) {
+            check(cudaGraphLaunch(macro_exec_, st_), "cudaGraphLaunch");
+            ++cnt_.count_graph_replays;
+            cnt_.count_single_step += macro_delta_.count_single_step;
+            cnt_.count_kernel_launches += macro_delta_.count_kernel_launches;
+            cnt_.count_ghost_waves += macro_delta_.count_ghost_waves;
+        } else if (key == macro_seen_ && !ops_dirty_) {
+            drop_macro_graph();
+            const fcb_counters_t c0 = cnt_;
+            dyn_n_ = 0;
+            cudaGraph_t graph = nullptr;
+            // capture on a private stream: the work is only recorded there, and the
+            // graph is launched on the caller's stream (which may be the legacy
+            // default stream, which cannot be captured)
+            if (!cap_st_) check(cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking), "cudaStreamCreate");
+            const cudaStream_t user_st = st_;
+            st_ = cap_st_;
+            cudaError_t be = cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal);
+            if (be != cudaSuccess) {
+                st_ = user_st;
+                check(be, "cudaStreamBeginCapture");
+            }
+            try {
+                run_schedule(t_curr, dt);
+            } catch (...) {
+                cudaStreamEndCapture(st_, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                st_ = user_st;
+                use_dyn_ = false;
+                throw;
+            }
+            cudaError_t ee = cudaStreamEndCapture(st_, &graph);
+            st_ = user_st;
+            check(ee, "cudaStreamEndCapture");
+            cudaError_t e = cudaGraphInstantiate(&macro_exec_, graph, 0);
+            cudaGraphDestroy(graph);
+            check(e, "cudaGraphInstantiate");
+            if (dyn_n_ != n_launch) throw Error(FCB_ERR_STATE, "macro-step schedule changed during capture");
+            macro_key_ = key;
+            macro_delta_.count_single_step = cnt_.count_single_step - c0.count_single_step;
+            macro_delta_.count_kernel_launches = cnt_.count_kernel_launches - c0.count_kernel_launches;
+            macro_delta_.count_ghost_waves = cnt_.count_ghost_waves - c0.count_ghost_waves;
+            check(cudaGraphLaunch(macro_exec_, st_), "cudaGraphLaunch");
+        } else {
+            dyn_n_ = 0;
+            run_schedule(t_curr, dt);
+            macro_seen_ = macro_fingerprint();
+        }
+    } else {
+        run_schedule(t_curr, dt);
+    }
+    use_dyn_ = false;
     ++cnt_.count_amr_advance;
-    unsigned long long b = 0;
-    check(cudaMemcpyAsync(&b, d_cfl_, sizeof b, cudaMemcpyDeviceToHost, st_), "cfl");
-    synchronize();
-    return cfl_from_bits(b);
+    return read_cfl(d_cfl_);
 }
 
 // ---------------------------------------------------------------------------

@@ -108,6 +108,10 @@ class Context {
                     bool domain_init);
     void qinit_slots(const std::vector<int32_t>& slots);
     double launch_level_step(int level, double t, double dt, unsigned long long* cfl_slot);
+    // --- macro step ---
+    void run_schedule(double t, double dt);  // the level schedule of one advance_all_levels
+    std::vector<uintptr_t> macro_fingerprint() const;
+    void drop_macro_graph();
     void launch_level_step_slots(const int32_t* d_slots, int n, double t, double dt, unsigned long long* cfl_slot);
 
     fcb_options_t opt_;
@@ -143,6 +147,8 @@ class Context {
     bool ops_dirty_ = true;
     // scalars
     unsigned long long* d_cfl_ = nullptr;  // [0]: advance accumulator, [1]: level / batch
+    unsigned long long* h_cfl_ = nullptr;  // pinned readback of one CFL word
+    double read_cfl(const unsigned long long* d);  // copy one CFL word back and synchronize
     double* d_scratch_ = nullptr;          // tagging / mass output
     size_t scratch_cap_ = 0;
     // per-patch single_step_update batching
@@ -151,6 +157,19 @@ class Context {
     // contiguous staging buffer for host transfers
     double* d_stage_ = nullptr;
     size_t stage_cap_ = 0;
+    // macro-step graph: per step launch {dt, vt} in a device table, so that one
+    // captured graph replays every macro step of a mesh
+    bool dry_ = false;               // schedule pass that only fills the table
+    bool use_dyn_ = false;           // step launches read {dt, vt} from the table
+    double* h_dyn_ = nullptr;        // pinned
+    size_t dyn_cap_ = 0;             // entries
+    int dyn_n_ = 0;
+    DevBuf<double> d_dyn_;
+    uint64_t mesh_version_ = 0;
+    cudaGraphExec_t macro_exec_ = nullptr;
+    cudaStream_t cap_st_ = nullptr;  // capture stream (the caller's stream may be the legacy one)
+    std::vector<uintptr_t> macro_key_, macro_seen_;
+    fcb_counters_t macro_delta_{};
     // state
     bool initialized_ = false;
     double curr_time_ = 0.0;

@@ -86,8 +86,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     double* __restrict__ q = a.q + (int64_t)slot * a.q_stride;
     double* __restrict__ qlast = a.qlast + (int64_t)slot * a.q_stride;
     const bool save_last = active && (meta.flags & PATCH_SAVE_LAST);
-    const double dtdx = a.dt / meta.dx;
-    const double dtdy = a.dt / meta.dy;
+    const double dtdx = step_dt(a) / meta.dx;
+    const double dtdy = step_dt(a) / meta.dy;
     const double dtdxave = 0.5 * (dtdx + dtdx);  // 0.5*(dtdx1d(i-1)+dtdx1d(i)), no capacity
     const double dtdyave = 0.5 * (dtdy + dtdy);
     SOL sol{a.grav, a.gamma, a.gamma1};
@@ -122,8 +122,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         }
         __syncthreads();
         if (active) {
-            const double vty = a.vt / meta.dy;
-            const double vtx = a.vt / meta.dx;
+            const double vty = step_vt(a) / meta.dy;
+            const double vtx = step_vt(a) / meta.dx;
             double* au = s_aux + (pl * NAUX + 0) * NY * NX;
             double* av = s_aux + (pl * NAUX + 1) * NY * NX;
             for (int r = 0; r < NY; ++r) {

@@ -565,14 +565,15 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     T.nb = dsm + L::ND + pls * (NX + 1) + c;
     T.ty = dsm + L::TY + pls * (NX + 1);
     // dtdx1d is uniform without capacity, so 0.5*(dtdx1d(i-1)+dtdx1d(i)) == dtdx exactly
-    T.dtdx = a.dt / meta.dx;
-    T.dtdy = a.dt / meta.dy;
+    const double dt = step_dt(a), vt = step_vt(a);
+    T.dtdx = dt / meta.dx;
+    T.dtdy = dt / meta.dy;
     T.rdtdx = R(T.dtdx);
     T.rdtdy = R(T.dtdy);
     T.rhdtdx = R(0.5 * T.dtdx);  // the reference's 0.5d0*dtdx*b, evaluated left to right
     T.rhdtdy = R(0.5 * T.dtdy);
-    T.vty = a.vt / meta.dy;
-    T.vtx = a.vt / meta.dx;
+    T.vty = vt / meta.dy;
+    T.vtx = vt / meta.dx;
     T.tx = 0.0;
 
     PipeState<SOL> S;

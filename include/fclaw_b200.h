@@ -102,6 +102,11 @@ typedef struct fcb_options {
      * ghost interpolation in FP32, flux sums, cell update, state and mass sums
      * in FP64 (pipelined step form only); enum fcb_precision */
     int precision;
+    /* 1: fcb_advance_all_levels replays the whole subcycled macro-step (level
+     * updates, time interpolation, ghost fills) as one CUDA graph, captured on
+     * the second call for a mesh; 0: every launch is issued from the host;
+     * 2: graph when a macro step updates three or more level batches */
+    int macro_graph;
 } fcb_options_t;
 
 typedef struct fcb_counters {
@@ -110,7 +115,8 @@ typedef struct fcb_counters {
     long long count_amr_regrid;
     long long count_single_step;     /* patch updates; x mx*my = cell updates */
     long long count_ghost_waves;     /* ghost-fill kernel launches */
-    long long count_kernel_launches; /* all kernels launched by the library */
+    long long count_kernel_launches; /* all kernels launched by the library (graph replays included) */
+    long long count_graph_replays;   /* macro steps replayed from a captured CUDA graph */
 } fcb_counters_t;
 
 typedef struct fcb_context fcb_context_t;

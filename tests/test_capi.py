@@ -42,8 +42,8 @@ def test_options_layout_matches_header(built, tmp_path):
         '#include <stdio.h>\n#include <stddef.h>\n#include "fclaw_b200.h"\n'
         "int main(void){printf(\"%zu %zu %zu %zu\\n\", sizeof(fcb_options_t),"
         " offsetof(fcb_options_t, refine_threshold), offsetof(fcb_options_t, problem_params),"
-        " sizeof(fcb_counters_t)); printf(\"%zu %zu\\n\", offsetof(fcb_options_t, step_variant),"
-        " offsetof(fcb_options_t, precision)); return 0;}\n")
+        " sizeof(fcb_counters_t)); printf(\"%zu %zu %zu\\n\", offsetof(fcb_options_t, step_variant),"
+        " offsetof(fcb_options_t, precision), offsetof(fcb_options_t, macro_graph)); return 0;}\n")
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
@@ -55,6 +55,7 @@ def test_options_layout_matches_header(built, tmp_path):
     assert int(out[3]) == ctypes.sizeof(_Counters)
     assert int(out[4]) == _Options.step_variant.offset
     assert int(out[5]) == _Options.precision.offset
+    assert int(out[6]) == _Options.macro_graph.offset
 
 
 def test_invalid_options_rejected_before_any_device_call(built):
