@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="uniform_swirl", choices=["uniform_swirl"])
+    p.add_argument("--workload", default="uniform_swirl", choices=["uniform_swirl", "amr_radialdam"])
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--mx", type=int, default=16)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
@@ -328,6 +328,114 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+# ----------------------------------------------------------------------------
+# AMR shallow water: dam break, Roe solver, levels 3..6, mx = 32, subcycling,
+# gradient tagging, regrid after every macro step, adaptive dt
+# ----------------------------------------------------------------------------
+def _amr_cfg(seed=0):
+    sys.path.insert(0, str(ROOT / "tests"))
+    import cases
+
+    return cases.radialdam_amr(seed=seed, minlevel=3, maxlevel=6, mx=32)
+
+
+def _next_dt(dt, cfl, cfg):
+    # fclaw2d_run: dt_new = dt * desired_cfl / cfl
+    return dt * cfg.desired_cfl / cfl if cfl > 0 else dt
+
+
+def run_amr(args, rank, world, local_rank):
+    import torch
+
+    import cases
+    import forestclaw_b200 as fcb
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.current_stream()
+    cfg = _amr_cfg()
+    opts = cases.to_options(cfg)
+    opts.precision = fcb.PRECISION_MIXED if args.precision == "mixed" else fcb.PRECISION_FP64
+    opts.macro_graph = args.macro_graph
+    s = fcb.Solver(opts, stream=stream.cuda_stream)
+    s.initialize()
+    t, dt = 0.0, cfg.initial_dt
+    for _ in range(args.warmup):
+        cfl = s.advance_all_levels(t, dt)
+        t += dt
+        s.regrid()
+        dt = _next_dt(dt, cfl, cfg)
+    torch.cuda.synchronize()
+    c0 = s.counters()
+    adv_ms, reg_s, patches = 0.0, 0.0, []
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            cfl = s.advance_all_levels(t, dt)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            adv_ms += e0.elapsed_time(e1)
+            t += dt
+            r0 = time.perf_counter()
+            s.regrid()
+            torch.cuda.synchronize()
+            reg_s += time.perf_counter() - r0
+            patches.append(s.num_patches)
+            dt = _next_dt(dt, cfl, cfg)
+    c1 = s.counters()
+    cells = (c1["count_single_step"] - c0["count_single_step"]) * cfg.mx * cfg.my
+    if rank != 0:
+        return None
+    hbm, src = peaks()
+    bytes_per_cell = 54.4  # meqn 3, mx 32, mbc 2: 8*3*(1 + 36*36/(32*32))
+    achieved = cells * bytes_per_cell / (adv_ms * 1e-3) / 1e9
+    line = {
+        "metric": "cell-updates/s", "value": cells / (adv_ms * 1e-3), "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": adv_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
+        "config": {"workload": "AMR shallow-water dam break, Roe, levels 3-6, mx=my=32, subcycled, "
+                               "regrid every macro step (advance phase timed; regrid reported apart)",
+                   "patches_min": min(patches), "patches_max": max(patches),
+                   "regrid_ms_per_step": reg_s * 1e3 / args.steps, "macro_graph": args.macro_graph,
+                   "graph_replays": c1["count_graph_replays"] - c0["count_graph_replays"],
+                   "launches_per_step": (c1["count_kernel_launches"] - c0["count_kernel_launches"]) / args.steps},
+        "clocks": clk.summary(),
+        "gpu_launches": c1["count_kernel_launches"] - c0["count_kernel_launches"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "bytes_per_cell": bytes_per_cell, "kernel": "advance phase (all kernels)",
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback"},
+    }
+    if world == 1:
+        line["cpu_baseline"] = amr_cpu_sample(args.cpu_seconds)
+    s.close()
+    return line
+
+
+def amr_cpu_sample(budget_s):
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle as O
+
+    O.use_library(native_oracle())
+    cfg = _amr_cfg()
+    o = O.OracleSolver(cfg)
+    o.initialize()
+    t, dt, el, cells, n = 0.0, cfg.initial_dt, 0.0, 0, 0
+    while el < budget_s and n < 50:
+        c0 = o.counters()["count_single_step"]
+        t0 = time.perf_counter()
+        cfl = o.advance(t, dt)
+        el += time.perf_counter() - t0
+        cells += (o.counters()["count_single_step"] - c0) * cfg.mx * cfg.my
+        t += dt
+        o.regrid()
+        dt = _next_dt(dt, cfl, cfg)
+        n += 1
+    return {"value": cells / el, "unit": "cell-updates/s", "cores": cpu_threads(), "kind": "port",
+            "sample": f"first {n} macro steps of the same AMR run (advance phase, {el:.2f} s), C++ restatement "
+                      f"of the reference, OpenMP over the patches of each level"}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -348,7 +456,9 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device("cuda", local_rank))
     try:
-        line = run_ours(args, rank, world, local_rank)
+        sys.path.insert(0, str(ROOT / "tests"))
+        run = run_amr if args.workload == "amr_radialdam" else run_ours
+        line = run(args, rank, world, local_rank)
         if line:
             print(json.dumps(line), flush=True)
     finally:
