@@ -63,6 +63,7 @@ class _Options(ctypes.Structure):
         ("step_variant", ctypes.c_int),
         ("precision", ctypes.c_int),
         ("macro_graph", ctypes.c_int),
+        ("claw_version", ctypes.c_int),
     ]
 
 
@@ -119,13 +120,15 @@ class Options:
     # 1: advance_all_levels replays the macro-step as one CUDA graph; 0: host
     # launches; 2: graph once a macro step updates three or more level batches
     macro_graph: int = 2
+    # 4: fc2d_clawpack46 update, 5: fc2d_clawpack5 update (arrays in q(m,i,j) order)
+    claw_version: int = 4
 
     def to_c(self) -> _Options:
         o = _Options()
         for name in ("mx", "my", "mbc", "meqn", "maux", "refinement_criteria", "threshold_variable",
                      "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
                      "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
-                     "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph"):
+                     "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph", "claw_version"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
                      "desired_cfl", "grav", "gamma"):
@@ -293,6 +296,8 @@ class Solver:
 
     def _shape(self):
         o = self.options
+        if o.claw_version == 5:  # q(m,i,j): component fastest
+            return (self.num_patches, o.ny, o.nx, o.meqn)
         return (self.num_patches, o.meqn, o.ny, o.nx)
 
     def get_q(self, out: np.ndarray | None = None) -> np.ndarray:

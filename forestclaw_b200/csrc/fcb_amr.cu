@@ -244,22 +244,30 @@ cudaError_t launch_mass(const double* q, int64_t stride, const int32_t* slots, c
 // Gather / scatter of whole patches between the slot arena and a contiguous
 // buffer (leaf order), so that host transfers are one copy each way.
 // ---------------------------------------------------------------------------
+// meqn5 > 0: the staging side holds each patch in the clawpack 5 order q(m,i,j)
+// (component fastest) while the arena keeps q(i,j,m).
 __global__ void gather_kernel(const double* __restrict__ src, int64_t stride, const int32_t* slots, int n,
-                              int64_t psize, double* __restrict__ dst, int scatter) {
+                              int64_t psize, double* __restrict__ dst, int scatter, int meqn5) {
+    const int64_t ncell = meqn5 > 0 ? psize / meqn5 : psize;
     for (int p = blockIdx.x; p < n; p += gridDim.x) {
         const int64_t a = (int64_t)slots[p] * stride, b = (int64_t)p * psize;
         for (int64_t k = threadIdx.x; k < psize; k += blockDim.x) {
-            if (scatter) const_cast<double*>(src)[a + k] = dst[b + k];
-            else dst[b + k] = src[a + k];
+            int64_t h = k;
+            if (meqn5 > 0) {
+                const int64_t m = k / ncell, cell = k - m * ncell;
+                h = cell * meqn5 + m;
+            }
+            if (scatter) const_cast<double*>(src)[a + k] = dst[b + h];
+            else dst[b + h] = src[a + k];
         }
     }
 }
 
 cudaError_t launch_gather(const double* src, int64_t stride, const int32_t* slots, int n, int64_t psize,
-                          double* dst, bool scatter, cudaStream_t st) {
+                          double* dst, bool scatter, int meqn5, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const int blocks = n < 148 * 16 ? n : 148 * 16;
-    gather_kernel<<<blocks, 256, 0, st>>>(src, stride, slots, n, psize, dst, scatter ? 1 : 0);
+    gather_kernel<<<blocks, 256, 0, st>>>(src, stride, slots, n, psize, dst, scatter ? 1 : 0, meqn5);
     return cudaGetLastError();
 }
 

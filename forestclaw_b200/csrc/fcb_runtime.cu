@@ -70,6 +70,10 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
         bad("the mixed-precision update exists in the pipelined step form only");
     if ((opt_.mx & (opt_.mx - 1)) != 0) bad("mx must be a power of two");
     if (opt_.macro_graph < 0 || opt_.macro_graph > 2) bad("macro_graph must be 0, 1 or 2");
+    if (opt_.claw_version == 0) opt_.claw_version = 4;
+    if (opt_.claw_version != 4 && opt_.claw_version != 5) bad("claw_version must be 4 (clawpack 4.6) or 5");
+    if (opt_.claw_version == 5 && (opt_.step_variant == 1 || opt_.step_variant == 2))
+        bad("the clawpack 5 update exists in the pipelined step form only");
     nx_ = opt_.mx + 2 * opt_.mbc;
     ny_ = opt_.my + 2 * opt_.mbc;
     const int64_t ps = (int64_t)opt_.meqn * nx_ * ny_;
@@ -557,15 +561,17 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     cudaError_t e = cudaErrorNotSupported;
     const int v = opt_.step_variant;
     if (opt_.precision == 1) {
-        e = launch_step_pipe_mixed(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_);
+        e = launch_step_pipe_mixed(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc,
+                                   opt_.claw_version, a, st_);
         if (e == cudaErrorNotSupported) throw Error(FCB_ERR_INVALID, "no mixed-precision step for this case");
     } else if (v == 2) {
         if (aux_kind_ == AUX_SWIRL) e = launch_step_warp_swirl(opt_.mx, opt_.mbc, a, st_);
         if (e == cudaErrorNotSupported) throw Error(FCB_ERR_INVALID, "no warp-synchronous step for this case");
-    } else if (v == 3 || (v == 0 && opt_.solver_kind == SOLVER_ADVECTION)) {
+    } else if (v == 3 || (v == 0 && (opt_.solver_kind == SOLVER_ADVECTION || opt_.claw_version == 5))) {
         // default: the pipelined form for scalar advection; the Roe solvers keep
         // the four-barrier form, whose smaller register footprint suits them
-        e = launch_step_pipe(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_);
+        e = launch_step_pipe(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, opt_.claw_version,
+                             a, st_);
         if (e == cudaErrorNotSupported && v == 3) throw Error(FCB_ERR_INVALID, "no pipelined step for this case");
     }
     if (e == cudaErrorNotSupported)
@@ -1084,7 +1090,7 @@ void Context::get_q(double* host, size_t n, bool qinterp) {
         stage_cap_ = total;
     }
     check(launch_gather(qinterp ? d_qti_ : d_q_, stride_, d_all_slots_.p, num_patches(), (int64_t)ps, d_stage_,
-                        false, st_),
+                        false, opt_.claw_version == 5 ? opt_.meqn : 0, st_),
           "gather");
     ++cnt_.count_kernel_launches;
     check(cudaMemcpyAsync(host, d_stage_, total * sizeof(double), cudaMemcpyDeviceToHost, st_), "get_q");
@@ -1101,7 +1107,9 @@ void Context::set_q(const double* host, size_t n) {
         stage_cap_ = total;
     }
     check(cudaMemcpyAsync(d_stage_, host, total * sizeof(double), cudaMemcpyHostToDevice, st_), "set_q");
-    check(launch_gather(d_q_, stride_, d_all_slots_.p, num_patches(), (int64_t)ps, d_stage_, true, st_), "scatter");
+    check(launch_gather(d_q_, stride_, d_all_slots_.p, num_patches(), (int64_t)ps, d_stage_, true,
+                        opt_.claw_version == 5 ? opt_.meqn : 0, st_),
+          "scatter");
     ++cnt_.count_kernel_launches;
     synchronize();
 }

@@ -25,10 +25,10 @@ struct Error : std::runtime_error {
 cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
                         cudaStream_t st);
 cudaError_t launch_step_warp_swirl(int mx, int mbc, const StepArgs& a, cudaStream_t st);
-cudaError_t launch_step_pipe(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
-                             cudaStream_t st);
+cudaError_t launch_step_pipe(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, int claw_version,
+                             const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_pipe_mixed(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
-                                   const StepArgs& a, cudaStream_t st);
+                                   int claw_version, const StepArgs& a, cudaStream_t st);
 struct GhostArgs;
 cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st);
 cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64_t stride,
@@ -40,9 +40,10 @@ struct TagArgs;
 cudaError_t launch_tag(const TagArgs& a, cudaStream_t st);
 cudaError_t launch_regrid(double* q, int64_t stride, const int32_t* ops, const int32_t* fine, int nops,
                           int mx, int my, int mbc, int meqn, cudaStream_t st);
-// scatter == false: dst[p] = src[slots[p]]; scatter == true: src[slots[p]] = dst[p]
+// scatter == false: dst[p] = src[slots[p]]; scatter == true: src[slots[p]] = dst[p];
+// meqn5 > 0: dst holds the patches in the clawpack 5 order q(m,i,j)
 cudaError_t launch_gather(const double* src, int64_t stride, const int32_t* slots, int n, int64_t psize,
-                          double* dst, bool scatter, cudaStream_t st);
+                          double* dst, bool scatter, int meqn5, cudaStream_t st);
 cudaError_t launch_mass(const double* q, int64_t stride, const int32_t* slots, const PatchMeta* meta, int n,
                         int mx, int my, int mbc, int meqn, double* out, cudaStream_t st);
 

@@ -1,6 +1,7 @@
 // Point-wise Riemann solvers and the wave limiter for the device step kernel.
 //
 // Each solver restates one reference Fortran routine for a single interface
+// (V5: the clawpack 5 twin of the routine where its arithmetic differs)
 // (the reference loops over a whole 1-D slice; the per-interface arithmetic is
 // the same).  The Roe averages that the reference passes from rpn2 to rpt2
 // through COMMON /comroe/ travel here in an explicit per-interface struct.
@@ -21,9 +22,11 @@ __device__ __forceinline__ T dmin(T a, T b) { return a < b ? a : b; }
 // clawpack46_rpt2adv.f.  The normal speed is the edge velocity aux(i,j,ixy);
 // the transverse splitting uses the two edge velocities of the cell pair.
 // ---------------------------------------------------------------------------
-template <int W_, typename R = double>
+// clawpack5_rpn2adv.f90 / clawpack5_rpt2adv.f90 have the same arithmetic.
+template <int W_, typename R = double, bool V5_ = false>
 struct AdvectionSolver {
     using Real = R;
+    static constexpr bool V5 = V5_;
     static constexpr int M = 1;
     static constexpr int W = W_;
     struct Roe {};
@@ -61,9 +64,12 @@ struct AdvectionSolver {
 // Shallow water, Roe with entropy fix:
 // applications/clawpack/shallow/2d/rp/clawpack46_rpn2.f:1-247, clawpack46_rpt2.f:1-74
 // ---------------------------------------------------------------------------
-template <typename R>
+// V5: clawpack5_rpn2.f90, clawpack5_rpt2.f90 (a1, a3 scaled by 0.5/a instead
+// of divided by 2a; the Roe averages clawpack5_rpt2 recomputes equal rpn2's).
+template <typename R, bool V5_ = false>
 struct SweRoeT {
     using Real = R;
+    static constexpr bool V5 = V5_;
     static constexpr int M = 3;
     static constexpr int W = 3;
     struct Roe { R u, v, a; };
@@ -84,9 +90,9 @@ struct SweRoeT {
         const R d1 = qR[0] - qL[0];
         const R d2 = qR[mu] - qL[mu];
         const R d3 = qR[mv] - qL[mv];
-        const R a1 = ((u + a) * d1 - d2) / (R(2.0) * a);
+        const R a1 = V5 ? ((u + a) * d1 - d2) * (R(0.5) / a) : ((u + a) * d1 - d2) / (R(2.0) * a);
         const R a2 = -(v * d1) + d3;
-        const R a3 = (-((u - a) * d1) + d2) / (R(2.0) * a);
+        const R a3 = V5 ? (-((u - a) * d1) + d2) * (R(0.5) / a) : (-((u - a) * d1) + d2) / (R(2.0) * a);
         wave[0][0] = a1; wave[0][mu] = a1 * (u - a); wave[0][mv] = a1 * v; s[0] = u - a;
         wave[1][0] = R(0.0); wave[1][mu] = R(0.0); wave[1][mv] = a2; s[1] = u;
         wave[2][0] = a3; wave[2][mu] = a3 * (u + a); wave[2][mv] = a3 * v; s[2] = u + a;
@@ -141,9 +147,9 @@ struct SweRoeT {
         const int mu = (ixy == 1) ? 1 : 2;
         const int mv = (ixy == 1) ? 2 : 1;
         const R u = rr.u, v = rr.v, a = rr.a;
-        const R a1 = ((v + a) * asdq[0] - asdq[mv]) / (2 * a);
+        const R a1 = V5 ? (R(0.5) / a) * ((v + a) * asdq[0] - asdq[mv]) : ((v + a) * asdq[0] - asdq[mv]) / (2 * a);
         const R a2 = asdq[mu] - u * asdq[0];
-        const R a3 = (-((v - a) * asdq[0]) + asdq[mv]) / (2 * a);
+        const R a3 = V5 ? (R(0.5) / a) * (-((v - a) * asdq[0]) + asdq[mv]) : (-((v - a) * asdq[0]) + asdq[mv]) / (2 * a);
         R waveb[3][3], sb[3];
         waveb[0][0] = a1; waveb[mu][0] = a1 * u; waveb[mv][0] = a1 * (v - a); sb[0] = v - a;
         waveb[0][1] = R(0.0); waveb[mu][1] = a2; waveb[mv][1] = R(0.0); sb[1] = v;
@@ -167,9 +173,11 @@ struct SweRoeT {
 // applications/clawpack/euler/2d/rp/clawpack46_rpn2_euler4.f:1-289,
 // clawpack46_rpt2_euler4.f:290-386
 // ---------------------------------------------------------------------------
-template <typename R>
+// clawpack5_rpn2_euler4.f90 / clawpack5_rpt2_euler4.f90 have the same arithmetic.
+template <typename R, bool V5_ = false>
 struct Euler4RoeT {
     using Real = R;
+    static constexpr bool V5 = V5_;
     static constexpr int M = 4;
     static constexpr int W = 4;
     struct Roe { R u, v, a, enth, u2v2, g1a2, euv; };
@@ -300,7 +308,8 @@ struct Euler4RoeT {
 using SweRoeSolver = SweRoeT<double>;
 using Euler4RoeSolver = Euler4RoeT<double>;
 
-// clawpack46_inlinelimiter.f:4-118: phi(r) for limiter code `mth`.
+// clawpack46_inlinelimiter.f:4-118: phi(r) for limiter code `mth`
+// (clawpack5_inlinelimiter.f:4-109 knows codes 1-5; callers map the others to 1).
 template <typename R>
 __device__ __forceinline__ R limiter_phi(int mth, R r) {
     switch (mth) {

@@ -140,6 +140,10 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
     constexpr bool SWIRL = AUXK == AUX_SWIRL;
     using L = PipeSmem<NX, PPB, M, W, NAUX, SWIRL, R>;
     const Method<LIM> meth{a};
+    // clawpack 5 (clawpack5_flux2.f, clawpack5_step2.f90, clawpack5_step2_wrap.f):
+    // fluxes at interfaces 1..mx+1 only, accumulated into cells 1..mx+1, and
+    // only the interior cells updated
+    constexpr bool V5 = SOL::V5;
     const int c = T.c;
     auto s2 = [&](int d) -> int { return J >= 0 ? cslot(J, d, 2) : ((s - d) & 1); };
     auto s4 = [&](int d) -> int { return J >= 0 ? cslot(J, d, 4) : ((s - d) & 3); };
@@ -151,7 +155,8 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
 
     // prefetch q(c, s+1); load q(c, s-4) for this iteration's update early
     double qnext[M], qold[M];
-    const bool upd = T.active && (STEADY || (s - 4 >= 0 && s - 4 <= NY - 2)) && c <= NX - 2;
+    const bool upd = T.active && (V5 ? (s - 4 >= MBC && s - 4 <= MBC + MX - 1 && c >= MBC && c <= MBC + MX - 1)
+                                     : ((STEADY || (s - 4 >= 0 && s - 4 <= NY - 2)) && c <= NX - 2));
     {
         const bool on = T.active && (STEADY || s + 1 < NY);
 #pragma unroll
@@ -165,7 +170,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
     double GXs_new[M];
     {
         const int k = s - 3;
-        const bool xint = T.active && (STEADY || (k >= 1 && k <= NY - 2)) && c >= 1;
+        const bool xint = T.active && (STEADY || (k >= 1 && k <= NY - 2)) && (V5 ? (c >= MBC && c <= MBC + MX) : c >= 1);
         const R* gl = T.rb + L::GL + s2(3) * (2 * M * L::PNX);
 #pragma unroll
         for (int m = 0; m < M; ++m) {
@@ -215,7 +220,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
         const int k = s - 2;
         if (T.active && (STEADY || (k >= 0 && k <= NY - 2))) {
             R* fx = T.rb + L::FX + s4(2) * (2 * M * L::PNX);
-            const bool xint = (STEADY || k >= 1) && c >= 1;
+            const bool xint = (STEADY || k >= 1) && (V5 ? (c >= MBC && c <= MBC + MX) : c >= 1);
             if (xint) {
                 const R* xw = T.rb + L::XW + s2(2) * (W * M * L::PNX);
                 R cq[M];
@@ -239,7 +244,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                             }
                             if (wn2 == R(0)) continue;
                             const R rr = (S.xsl[mw] > R(0)) ? dl / wn2 : dr / wn2;
-                            const R phi = limiter_phi(mth, rr);
+                            const R phi = limiter_phi((SOL::V5 && mth > 5) ? 1 : mth, rr);
 #pragma unroll
                             for (int m = 0; m < M; ++m) S.xwl[mw][m] = phi * S.xwl[mw][m];
                         }
@@ -300,6 +305,11 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 for (int m = 0; m < M; ++m) {
                     fx[(0 * M + m) * L::PNX] = R(0);
                     fx[(1 * M + m) * L::PNX] = R(0);
+                    if constexpr (V5) {  // read by the cell to the left (mx+1 at the right end)
+                        R* gl = T.rb + L::GL + s2(2) * (2 * M * L::PNX);
+                        gl[(0 * M + m) * L::PNX] = R(0);
+                        gl[(1 * M + m) * L::PNX] = R(0);
+                    }
                 }
             }
         }
@@ -374,9 +384,13 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
             FYm_new[m] = FYp_new[m] = R(0);
             GYd[m] = GYu[m] = 0.0;
         }
-        if (T.ycol && (STEADY || (f >= 1 && f <= NY - 1))) {
-            const bool inner = STEADY || (f >= MBC && f <= MBC + MX);
-            const bool god = STEADY || f <= NY - 2;
+        // clawpack 5: interfaces MBC..MBC+MX carry fluxes; f = MBC+MX+1 only
+        // closes the transverse sum of cell row MBC+MX
+        const bool yblk = T.ycol && (V5 ? (f >= MBC && f <= MBC + MX + 1) : (STEADY || (f >= 1 && f <= NY - 1)));
+        if (yblk) {
+            const bool fact = !V5 || f <= MBC + MX;
+            const bool inner = V5 ? fact : (STEADY || (f >= MBC && f <= MBC + MX));
+            const bool god = V5 ? fact : (STEADY || f <= NY - 2);
             R w[W][M];
 #pragma unroll
             for (int mw = 0; mw < W; ++mw)
@@ -389,7 +403,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
             R cq[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) cq[m] = R(0);
-            if (meth.second_order()) {
+            if (meth.second_order() && fact) {
                 if (inner) {
 #pragma unroll
                     for (int mw = 0; mw < W; ++mw) {
@@ -400,7 +414,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                         for (int m = 1; m < M; ++m) wn2 = wn2 + S.yw_f[mw][m] * S.yw_f[mw][m];
                         if (wn2 == R(0)) continue;
                         const R rr = (S.ys_f[mw] > R(0)) ? S.ydotl[mw] / wn2 : ydotr[mw] / wn2;
-                        const R phi = limiter_phi(mth, rr);
+                        const R phi = limiter_phi((SOL::V5 && mth > 5) ? 1 : mth, rr);
 #pragma unroll
                         for (int m = 0; m < M; ++m) w[mw][m] = phi * w[mw][m];
                     }
@@ -433,7 +447,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 if (meth.transverse2() && god) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
             }
             R gLm[M], gLp[M], gRm[M], gRp[M];
-            if (meth.transverse()) {
+            if (meth.transverse() && fact) {
                 R bm[M], bp[M];
                 // imp = 1: aux2(j-1, kv=1), aux3(j-1, kv=1) = u at columns c, c+1, row f-1
                 sol.rpt2(2, am, S.yR_f, AUXV(0, 0, 2), AUXV(0, 1, 2), bm, bp);
@@ -447,7 +461,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 for (int m = 0; m < M; ++m) gLm[m] = gLp[m] = gRm[m] = gRp[m] = R(0);
             }
             // cell row f-1 is complete: gadd(f-1,.,1) = (0 - gL(f)) - gR(f-1)
-            if (STEADY || f - 1 >= 1) {
+            if (V5 ? (f - 1 >= MBC && f - 1 <= MBC + MX) : (STEADY || f - 1 >= 1)) {
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
                     GYd[m] = -(double)gLm[m] - (double)S.gRm_prev[m];
@@ -715,26 +729,34 @@ cudaError_t launch_pipe_mx(int mx, int mbc, const StepArgs& a, cudaStream_t st) 
 }  // namespace
 
 // cudaErrorNotSupported: no pipelined form for this (solver, mx, mbc, aux).
-// R: compute type of the Riemann solves, limiters and transverse parts.
-template <typename R>
-cudaError_t launch_step_pipe_t(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
+// R: compute type of the Riemann solves, limiters and transverse parts;
+// V5: the clawpack 5 update (fc2d_clawpack5) instead of clawpack 4.6.
+template <typename R, bool V5>
+cudaError_t launch_step_pipe_v(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
                                cudaStream_t st) {
     if (mx != my) return cudaErrorNotSupported;
     switch (solver) {
         case SOLVER_ADVECTION:
             if (mwaves != 1) return cudaErrorNotSupported;
-            if (aux_kind == AUX_SWIRL) return launch_pipe_mx<AdvectionSolver<1, R>, AUX_SWIRL, 2>(mx, mbc, a, st);
+            if (aux_kind == AUX_SWIRL) return launch_pipe_mx<AdvectionSolver<1, R, V5>, AUX_SWIRL, 2>(mx, mbc, a, st);
             if (aux_kind == AUX_STORED && a.maux == 2)
-                return launch_pipe_mx<AdvectionSolver<1, R>, AUX_STORED, 2>(mx, mbc, a, st);
+                return launch_pipe_mx<AdvectionSolver<1, R, V5>, AUX_STORED, 2>(mx, mbc, a, st);
             return cudaErrorNotSupported;
         case SOLVER_SWE_ROE:
             if (mwaves != 3 || aux_kind != AUX_NONE) return cudaErrorNotSupported;
-            return launch_pipe_mx<SweRoeT<R>, AUX_NONE, 0>(mx, mbc, a, st);
+            return launch_pipe_mx<SweRoeT<R, V5>, AUX_NONE, 0>(mx, mbc, a, st);
         case SOLVER_EULER4_ROE:
             if (mwaves != 4 || aux_kind != AUX_NONE) return cudaErrorNotSupported;
-            return launch_pipe_mx<Euler4RoeT<R>, AUX_NONE, 0>(mx, mbc, a, st);
+            return launch_pipe_mx<Euler4RoeT<R, V5>, AUX_NONE, 0>(mx, mbc, a, st);
         default: return cudaErrorNotSupported;
     }
+}
+
+template <typename R>
+cudaError_t launch_step_pipe_t(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, int claw_version,
+                               const StepArgs& a, cudaStream_t st) {
+    if (claw_version == 5) return launch_step_pipe_v<R, true>(solver, aux_kind, mwaves, mx, my, mbc, a, st);
+    return launch_step_pipe_v<R, false>(solver, aux_kind, mwaves, mx, my, mbc, a, st);
 }
 
 }  // namespace fcb

@@ -107,6 +107,11 @@ typedef struct fcb_options {
      * the second call for a mesh; 0: every launch is issued from the host;
      * 2: graph when a macro step updates three or more level batches */
     int macro_graph;
+    /* 4 (or 0): the fc2d_clawpack46 update; 5: the fc2d_clawpack5 update
+     * (fluxes at interfaces 1..mx+1, interior cells updated, clawpack5 Riemann
+     * solver arithmetic); fcb_get_q / fcb_set_q then use the clawpack 5 array
+     * order q(m,i,j) for every patch (pipelined step form only) */
+    int claw_version;
 } fcb_options_t;
 
 typedef struct fcb_counters {

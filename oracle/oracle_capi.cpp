@@ -21,7 +21,7 @@ enum IOpt {
     I_MTHBC0, I_MTHBC3 = I_MTHBC0 + 3,
     I_MINLEVEL, I_MAXLEVEL, I_SUBCYCLE, I_REGRID_INTERVAL, I_SMOOTH_REFINE, I_SMOOTH_LEVEL,
     I_CRITERIA, I_IVAR, I_USE_FIXED_DT, I_NOUT, I_INIT_GHOSTCELL, I_REDUCE_CFL,
-    I_SOLVER, I_PROBLEM, I_COUNT
+    I_SOLVER, I_PROBLEM, I_CLAW_VERSION, I_COUNT
 };
 enum DOpt {
     D_REFINE_TH, D_COARSEN_TH, D_TFINAL, D_INITIAL_DT, D_MAX_CFL, D_DESIRED_CFL,
@@ -41,6 +41,7 @@ Options unpack(const int* io, const double* d) {
     o.use_fixed_dt = io[I_USE_FIXED_DT]; o.nout = io[I_NOUT]; o.init_ghostcell = io[I_INIT_GHOSTCELL];
     o.reduce_cfl = io[I_REDUCE_CFL];
     o.solver.kind = io[I_SOLVER]; o.problem = io[I_PROBLEM];
+    o.method.version = io[I_CLAW_VERSION];
     o.refine_threshold = d[D_REFINE_TH]; o.coarsen_threshold = d[D_COARSEN_TH];
     o.tfinal = d[D_TFINAL]; o.initial_dt = d[D_INITIAL_DT]; o.max_cfl = d[D_MAX_CFL];
     o.desired_cfl = d[D_DESIRED_CFL];

@@ -77,8 +77,10 @@ void rpt2_adv(const Slice& S, int ixy, int meqn, int mx, const double* aux2, con
 }
 
 // applications/clawpack/shallow/2d/rp/clawpack46_rpn2.f:1-247 (entropy fix on)
+// v5: applications/clawpack/shallow/2d/rp/clawpack5_rpn2.f90 (a1, a3 scaled by
+// (0.5/a) instead of divided by 2a)
 void rpn2_swe(const Slice& S, RiemannState& R, double grav, int ixy, int meqn, int mwaves, int mx,
-              const double* q, double* wave, double* s, double* amdq, double* apdq) {
+              const double* q, double* wave, double* s, double* amdq, double* apdq, bool v5) {
     const int L = S.L, mbc = S.mbc;
     const int mu = (ixy == 1) ? 1 : 2;  // 0-based component of normal momentum
     const int mv = (ixy == 1) ? 2 : 1;
@@ -103,9 +105,9 @@ void rpn2_swe(const Slice& S, RiemannState& R, double grav, int ixy, int meqn, i
         const double d1 = Q(i, 0) - Q(i - 1, 0);
         const double d2 = Q(i, mu) - Q(i - 1, mu);
         const double d3 = Q(i, mv) - Q(i - 1, mv);
-        const double a1 = ((u + a) * d1 - d2) / (2.0 * a);
+        const double a1 = v5 ? ((u + a) * d1 - d2) * (0.50 / a) : ((u + a) * d1 - d2) / (2.0 * a);
         const double a2 = -(v * d1) + d3;
-        const double a3 = (-((u - a) * d1) + d2) / (2.0 * a);
+        const double a3 = v5 ? (-((u - a) * d1) + d2) * (0.50 / a) : (-((u - a) * d1) + d2) / (2.0 * a);
         W(i, 0, 0) = a1; W(i, mu, 0) = a1 * (u - a); W(i, mv, 0) = a1 * v; Sp(i, 0) = u - a;
         W(i, 0, 1) = 0.0; W(i, mu, 1) = 0.0; W(i, mv, 1) = a2; Sp(i, 1) = u;
         W(i, 0, 2) = a3; W(i, mu, 2) = a3 * (u + a); W(i, mv, 2) = a3 * v; Sp(i, 2) = u + a;
@@ -152,8 +154,9 @@ void rpn2_swe(const Slice& S, RiemannState& R, double grav, int ixy, int meqn, i
 }
 
 // applications/clawpack/shallow/2d/rp/clawpack46_rpt2.f:1-74
+// v5: clawpack5_rpt2.f90 (the Roe averages it recomputes equal rpn2's)
 void rpt2_swe(const Slice& S, const RiemannState& R, int ixy, int meqn, int mwaves, int mx,
-              const double* asdq, double* bmasdq, double* bpasdq) {
+              const double* asdq, double* bmasdq, double* bpasdq, bool v5) {
     const int L = S.L, mbc = S.mbc;
     const int mu = (ixy == 1) ? 1 : 2;
     const int mv = (ixy == 1) ? 2 : 1;
@@ -162,9 +165,9 @@ void rpt2_swe(const Slice& S, const RiemannState& R, int ixy, int meqn, int mwav
         const int ii = S.at(i);
         const double u = R.u[ii], v = R.v[ii], a = R.a[ii];
         const double q1 = asdq[0 * L + ii], qmu = asdq[mu * L + ii], qmv = asdq[mv * L + ii];
-        const double a1 = ((v + a) * q1 - qmv) / (2 * a);
+        const double a1 = v5 ? (0.50 / a) * ((v + a) * q1 - qmv) : ((v + a) * q1 - qmv) / (2 * a);
         const double a2 = qmu - u * q1;
-        const double a3 = (-((v - a) * q1) + qmv) / (2 * a);
+        const double a3 = v5 ? (0.50 / a) * (-((v - a) * q1) + qmv) : (-((v - a) * q1) + qmv) / (2 * a);
         waveb[0][0] = a1; waveb[mu][0] = a1 * u; waveb[mv][0] = a1 * (v - a); sb[0] = v - a;
         waveb[0][1] = 0.0; waveb[mu][1] = a2; waveb[mv][1] = 0.0; sb[1] = v;
         waveb[0][2] = a3; waveb[mu][2] = a3 * u; waveb[mv][2] = a3 * (v + a); sb[2] = v + a;
@@ -320,8 +323,9 @@ void rpt2_euler4(const Slice& S, const RiemannState& R, int ixy, int meqn, int m
 }
 
 // src/solvers/fc2d_clawpack4.6/fortran_source/clawpack46_inlinelimiter.f:4-118
+// v5: clawpack5_inlinelimiter.f:4-109 (codes 1-5; others fall to label 10)
 void inlinelimiter(const Slice& S, int meqn, int mwaves, int mx, double* wave, const double* s,
-                   const int* mthlim) {
+                   const int* mthlim, bool v5) {
     const int L = S.L;
     auto W = [&](int i, int m, int mw) -> double& { return wave[(mw * meqn + m) * L + S.at(i)]; };
     for (int mw = 0; mw < mwaves; ++mw) {
@@ -339,7 +343,7 @@ void inlinelimiter(const Slice& S, int meqn, int mwaves, int mx, double* wave, c
             if (wnorm2 == 0.0) continue;
             const double r = (s[mw * L + S.at(i)] > 0.0) ? dotl / wnorm2 : dotr / wnorm2;
             double wlimitr;
-            switch (mthlim[mw]) {
+            switch ((v5 && mthlim[mw] > 5) ? 1 : mthlim[mw]) {
                 case 2: wlimitr = dmax(dmax(0.0, dmin(1.0, 2.0 * r)), dmin(2.0, r)); break;
                 case 3: wlimitr = (r + std::fabs(r)) / (1.0 + std::fabs(r)); break;
                 case 4: {
@@ -365,6 +369,7 @@ void inlinelimiter(const Slice& S, int meqn, int mwaves, int mx, double* wave, c
 struct Work {
     Slice S;
     int meqn, maux, mwaves;
+    bool v5 = false;  // clawpack 5 solver arithmetic
     std::vector<double> q1d, dtdx1d, dtdy1d, aux1, aux2, aux3, faddm, faddp, gaddm, gaddp;
     std::vector<double> wave, s, amdq, apdq, cqxx, bmasdq, bpasdq;
     RiemannState R;
@@ -389,7 +394,7 @@ void call_rpn2(const SolverParams& sp, Work& w, int ixy, int mx) {
             break;
         case SOLVER_SWE_ROE:
             rpn2_swe(w.S, w.R, sp.grav, ixy, w.meqn, w.mwaves, mx, w.q1d.data(), w.wave.data(),
-                     w.s.data(), w.amdq.data(), w.apdq.data());
+                     w.s.data(), w.amdq.data(), w.apdq.data(), w.v5);
             break;
         case SOLVER_EULER4_ROE:
             rpn2_euler4(w.S, w.R, sp.gamma, sp.gamma1, ixy, w.meqn, w.mwaves, mx, w.q1d.data(),
@@ -406,7 +411,7 @@ void call_rpt2(const SolverParams& sp, Work& w, int ixy, int mx, int imp, const 
                      w.bmasdq.data(), w.bpasdq.data());
             break;
         case SOLVER_SWE_ROE:
-            rpt2_swe(w.S, w.R, ixy, w.meqn, w.mwaves, mx, asdq, w.bmasdq.data(), w.bpasdq.data());
+            rpt2_swe(w.S, w.R, ixy, w.meqn, w.mwaves, mx, asdq, w.bmasdq.data(), w.bpasdq.data(), w.v5);
             break;
         case SOLVER_EULER4_ROE:
             rpt2_euler4(w.S, w.R, ixy, w.meqn, mx, asdq, w.bmasdq.data(), w.bpasdq.data());
@@ -415,11 +420,16 @@ void call_rpt2(const SolverParams& sp, Work& w, int ixy, int mx, int imp, const 
     }
 }
 
-// src/solvers/fc2d_clawpack4.6/fortran_source/clawpack46_flux2.f:4-228
+// src/solvers/fc2d_clawpack4.6/fortran_source/clawpack46_flux2.f:4-228; with
+// mp.version == 5, fc2d_clawpack5/fortran_source/clawpack5_flux2.f:4-235, whose
+// Godunov, correction and transverse loops all run over i = 1..mx+1.
 double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, int mx,
              const double* dtdx1d) {
     const Slice& S = w.S;
     const int L = S.L, mbc = S.mbc, meqn = w.meqn, mwaves = w.mwaves;
+    const bool v5 = mp.version == 5;
+    const int god_lo = v5 ? 1 : 2 - mbc, god_hi = v5 ? mx + 1 : mx + mbc - 1;  // Godunov, amdq += cqxx
+    const int cq_lo = v5 ? 1 : 2 - mbc, cq_hi = v5 ? mx + 1 : mx + mbc;          // cqxx, gadd updates
     bool limit = false;
     for (int mw = 0; mw < mwaves; ++mw)
         if (mp.mthlim[mw] > 0) limit = true;
@@ -432,7 +442,7 @@ double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, i
                 w.gaddp[(side * meqn + m) * L + S.at(i)] = 0.0;
             }
     call_rpn2(sp, w, ixy, mx);
-    for (int i = 2 - mbc; i <= mx + mbc - 1; ++i)
+    for (int i = god_lo; i <= god_hi; ++i)
         for (int m = 0; m < meqn; ++m) {
             const int k = m * L + S.at(i);
             w.faddp[k] = w.faddp[k] - w.apdq[k];
@@ -445,8 +455,8 @@ double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, i
             cfl1d = dmax(dmax(cfl1d, dtdx1d[S.at(i)] * sw), -dtdx1d[S.at(i - 1)] * sw);
         }
     if (mp.order0 == 2) {
-        if (limit) inlinelimiter(S, meqn, mwaves, mx, w.wave.data(), w.s.data(), mp.mthlim);
-        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        if (limit) inlinelimiter(S, meqn, mwaves, mx, w.wave.data(), w.s.data(), mp.mthlim, w.v5);
+        for (int i = cq_lo; i <= cq_hi; ++i) {
             const double dtdxave = 0.5 * (dtdx1d[S.at(i - 1)] + dtdx1d[S.at(i)]);
             for (int m = 0; m < meqn; ++m) {
                 const int k = m * L + S.at(i);
@@ -463,7 +473,7 @@ double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, i
     }
     if (mp.order1 > 0) {
         if (mp.order0 > 1 && mp.order1 == 2)
-            for (int i = 2 - mbc; i <= mx + mbc - 1; ++i)
+            for (int i = god_lo; i <= god_hi; ++i)
                 for (int m = 0; m < meqn; ++m) {
                     const int k = m * L + S.at(i);
                     w.amdq[k] = w.amdq[k] + w.cqxx[k];
@@ -471,7 +481,7 @@ double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, i
                 }
         call_rpt2(sp, w, ixy, mx, 1, w.amdq.data());
         for (int m = 0; m < meqn; ++m)
-            for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            for (int i = cq_lo; i <= cq_hi; ++i) {
                 const int k = m * L + S.at(i);
                 const int k1 = (0 * meqn + m) * L + S.at(i - 1);
                 const int k2 = (1 * meqn + m) * L + S.at(i - 1);
@@ -484,7 +494,7 @@ double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, i
             }
         call_rpt2(sp, w, ixy, mx, 2, w.apdq.data());
         for (int m = 0; m < meqn; ++m)
-            for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            for (int i = cq_lo; i <= cq_hi; ++i) {
                 const int k = m * L + S.at(i);
                 const int k1 = (0 * meqn + m) * L + S.at(i);
                 const int k2 = (1 * meqn + m) * L + S.at(i);
@@ -508,6 +518,13 @@ double step2(const SolverParams& sp, const MethodParams& mp, int mx, int my, int
     const int mwaves = mp.mwaves;
     const bool capa = mp.mcapa > 0;
     Work w(maxm, mbc, meqn, maux, mwaves);
+    w.v5 = mp.version == 5;
+    // accumulation ranges of fm/fp/gm/gp (clawpack46_step2.f:240-294 / clawpack5_step2.f90:
+    // 1..mx+1) and of the update (clawpack46_step2_wrap.f:106-125 / clawpack5_step2_wrap.f:94-113)
+    const int acc_lo = w.v5 ? 1 : 2 - mbc;
+    const int accx_hi = w.v5 ? mx + 1 : mx + mbc, accy_hi = w.v5 ? my + 1 : my + mbc;
+    const int upd_lo = w.v5 ? 1 : 1 - mbc;
+    const int updx_hi = w.v5 ? mx : mx + mbc - 1, updy_hi = w.v5 ? my : my + mbc - 1;
     const Slice& S = w.S;
     const int L = S.L;
     const size_t n = (size_t)P.size(meqn);
@@ -538,7 +555,7 @@ double step2(const SolverParams& sp, const MethodParams& mp, int mx, int my, int
         const double cfl1d = flux2(sp, mp, w, 1, mx, w.dtdx1d.data());
         cflgrid = dmax(cflgrid, cfl1d);
         for (int m = 0; m < meqn; ++m)
-            for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            for (int i = acc_lo; i <= accx_hi; ++i) {
                 const int k = m * L + S.at(i);
                 fm[P(i, j, m)] = fm[P(i, j, m)] + w.faddm[k];
                 fp[P(i, j, m)] = fp[P(i, j, m)] + w.faddp[k];
@@ -565,7 +582,7 @@ double step2(const SolverParams& sp, const MethodParams& mp, int mx, int my, int
         const double cfl1d = flux2(sp, mp, w, 2, my, w.dtdy1d.data());
         cflgrid = dmax(cflgrid, cfl1d);
         for (int m = 0; m < meqn; ++m)
-            for (int j = 2 - mbc; j <= my + mbc; ++j) {
+            for (int j = acc_lo; j <= accy_hi; ++j) {
                 const int k = m * L + S.at(j);
                 gm[P(i, j, m)] = gm[P(i, j, m)] + w.faddm[k];
                 gp[P(i, j, m)] = gp[P(i, j, m)] + w.faddp[k];
@@ -577,8 +594,8 @@ double step2(const SolverParams& sp, const MethodParams& mp, int mx, int my, int
     }
     // conservative update (clawpack46_step2_wrap.f:106-125)
     for (int m = 0; m < meqn; ++m)
-        for (int i = 1 - mbc; i <= mx + mbc - 1; ++i)
-            for (int j = 1 - mbc; j <= my + mbc - 1; ++j) {
+        for (int i = upd_lo; i <= updx_hi; ++i)
+            for (int j = upd_lo; j <= updy_hi; ++j) {
                 const double df = fm[P(i + 1, j, m)] - fp[P(i, j, m)];
                 const double dg = gm[P(i, j + 1, m)] - gp[P(i, j, m)];
                 if (!capa)

@@ -34,6 +34,7 @@ struct MethodParams {
     int mcapa = 0;          // capacity index (0 = none)
     int mwaves = 1;
     int mthlim[8] = {4, 4, 4, 4, 4, 4, 4, 4};
+    int version = 4;        // 4: clawpack 4.6 (fc2d_clawpack46), 5: clawpack 5 (fc2d_clawpack5)
 };
 
 // Index helper for one patch array with Fortran bounds.
@@ -51,8 +52,11 @@ struct PatchIdx {
 inline double dmax(double a, double b) { return a > b ? a : b; }
 inline double dmin(double a, double b) { return a < b ? a : b; }
 
-// clawpack46_step2_wrap.f:1-127 + clawpack46_step2.f:5-239 + clawpack46_flux2.f:4-228.
-// Updates q in place over i,j = 1-mbc..mx+mbc-1 and returns cflgrid.
+// clawpack46_step2_wrap.f:1-127 + clawpack46_step2.f:5-239 + clawpack46_flux2.f:4-228:
+// updates q in place over i,j = 1-mbc..mx+mbc-1 and returns cflgrid.
+// With mp.version == 5: clawpack5_step2_wrap.f:1-115 + clawpack5_step2.f90:1-172 +
+// clawpack5_flux2.f:4-235 (interfaces 1..mx+1 only, interior update i,j = 1..mx,
+// clawpack5_rpn2.f90 / clawpack5_rpt2.f90 arithmetic for the shallow-water solver).
 double step2(const SolverParams& sp, const MethodParams& mp,
              int mx, int my, int mbc, int meqn, int maux,
              double* q, const double* aux, double dx, double dy, double dt);

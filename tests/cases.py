@@ -22,7 +22,7 @@ def to_options(cfg: O.Config):
         refine_threshold=cfg.refine_threshold, coarsen_threshold=cfg.coarsen_threshold,
         tfinal=cfg.tfinal, initial_dt=cfg.initial_dt, max_cfl=cfg.max_cfl,
         desired_cfl=cfg.desired_cfl, solver_kind=cfg.solver, problem=cfg.problem,
-        grav=cfg.grav, gamma=cfg.gamma, problem_params=cfg.pparams,
+        grav=cfg.grav, gamma=cfg.gamma, problem_params=cfg.pparams, claw_version=cfg.claw_version,
     )
 
 

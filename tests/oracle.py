@@ -28,7 +28,7 @@ _I_FIELDS = (["mx", "my", "mbc", "meqn", "maux", "order0", "order1", "mcapa", "m
              + [f"mthlim{k}" for k in range(8)] + [f"mthbc{k}" for k in range(4)]
              + ["minlevel", "maxlevel", "subcycle", "regrid_interval", "smooth_refine",
                 "smooth_level", "criteria", "ivar", "use_fixed_dt", "nout", "init_ghostcell",
-                "reduce_cfl", "solver", "problem"])
+                "reduce_cfl", "solver", "problem", "claw_version"])
 _D_FIELDS = (["refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
               "desired_cfl", "grav", "gamma", "gamma1"] + [f"p{k}" for k in range(32)])
 
@@ -69,6 +69,7 @@ class Config:
     grav: float = 1.0
     gamma: float = 1.4
     pparams: tuple = field(default_factory=tuple)
+    claw_version: int = 4   # 4: fc2d_clawpack46, 5: fc2d_clawpack5
 
     @property
     def gamma1(self) -> float:
@@ -84,6 +85,7 @@ class Config:
             "criteria": self.criteria, "ivar": self.ivar, "use_fixed_dt": self.use_fixed_dt,
             "nout": self.nout, "init_ghostcell": self.init_ghostcell,
             "reduce_cfl": self.reduce_cfl, "solver": self.solver, "problem": self.problem,
+            "claw_version": self.claw_version,
         }
         for k in range(8):
             iv[f"mthlim{k}"] = self.mthlim[k] if k < len(self.mthlim) else 0
@@ -273,7 +275,7 @@ def swirl_regression(claw_version: int = 4) -> Config:
                   refine_threshold=0.25, coarsen_threshold=0.05, smooth_refine=1,
                   tfinal=0.1, initial_dt=0.005, max_cfl=1.0, desired_cfl=0.9, nout=1,
                   subcycle=1, solver=ADVECTION, problem=SWIRL, criteria=MINMAX,
-                  pparams=(4.0,))
+                  pparams=(4.0,), claw_version=claw_version)
 
 
 QUADRANT_STATES = (

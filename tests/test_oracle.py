@@ -12,11 +12,13 @@ import oracle as O
 PINS = json.loads((Path(__file__).parent / "golden" / "regression_pins.json").read_text())
 
 
-@pytest.mark.parametrize("name", ["swirl", "quadrants"])
+@pytest.mark.parametrize("name", ["swirl", "swirl_claw5", "quadrants"])
 def test_regression_pins(name):
-    """applications/**/regression_values_0.csv: count_amr_advance,
-    global_num_patches and count_amr_new_domain of the clawpack 4.6 runs."""
-    cfg = O.swirl_regression() if name == "swirl" else O.quadrants_regression()
+    """applications/**/regression_values_{0,1}.csv: count_amr_advance,
+    global_num_patches and count_amr_new_domain of the clawpack 4.6 runs and of
+    the swirl run with --user:claw-version=5."""
+    cfg = {"swirl": O.swirl_regression, "swirl_claw5": lambda: O.swirl_regression(5),
+           "quadrants": O.quadrants_regression}[name]()
     s = O.OracleSolver(cfg)
     s.initialize()
     s.run()
@@ -79,3 +81,34 @@ def test_first_order_upwind_known_answer():
     O.step2(cfg, qn, aux, dx, dy, dt)
     expect = q[0, :, 1:-1] - dt / dx * 0.7 * (q[0, :, 1:-1] - q[0, :, :-2])
     assert np.allclose(qn[0, 1:-1, 1:-1], expect[1:-1, :], rtol=0, atol=1e-15)
+
+
+def test_claw5_step_updates_interior_cells_only():
+    """clawpack5_step2_wrap.f updates i,j = 1..mx only; clawpack46 also updates
+    the ghost band 1-mbc..mx+mbc-1."""
+    cfg4 = cases.radialdam_uniform(level=0, mx=8)
+    cfg5 = cases.replace(cfg4, claw_version=5)
+    s = O.OracleSolver(cfg4)
+    s.initialize()
+    rng = np.random.default_rng(0)
+    qin = s.all_q()[0] + 0.01 * rng.uniform(size=s.all_q()[0].shape)
+    qin[0] = np.abs(qin[0]) + 0.5
+    q4, q5 = qin.copy(), qin.copy()
+    O.step2(cfg4, q4, None, 1 / 8, 1 / 8, 0.01)
+    O.step2(cfg5, q5, None, 1 / 8, 1 / 8, 0.01)
+    mbc = cfg4.mbc
+    ghost = np.ones(qin.shape[1:], bool)
+    ghost[mbc:-mbc, mbc:-mbc] = False
+    assert np.array_equal(q5[:, ghost], qin[:, ghost])
+    assert not np.array_equal(q4[:, ghost], qin[:, ghost])
+    assert not np.array_equal(q5[:, ~ghost], qin[:, ~ghost])
+
+
+def test_claw5_interior_mass_conservation():
+    cfg = cases.replace(cases.radialdam_uniform(level=3, mx=16, r0=0.1), claw_version=5)
+    s = O.OracleSolver(cfg)
+    s.initialize()
+    m0 = s.conservation()[0]
+    for k in range(10):
+        s.advance(k * 0.002, 0.002)
+    assert abs(s.conservation()[0] - m0) <= 1e-13 * m0
