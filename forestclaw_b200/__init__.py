@@ -20,15 +20,16 @@ from typing import Optional, Sequence
 import numpy as np
 
 __all__ = ["Options", "Solver", "lib", "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
-           "SOLVER_EULER4_ROE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM", "PROBLEM_QUADRANTS",
+           "SOLVER_EULER4_ROE", "SOLVER_GEOCLAW_FWAVE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM",
+           "PROBLEM_QUADRANTS", "PROBLEM_BATHY",
            "PRECISION_FP64", "PRECISION_MIXED",
            "TAG_VALUE", "TAG_MINMAX", "TAG_DIFFERENCE", "TAG_GRADIENT", "EXPORTED_SYMBOLS"]
 
 PKG = Path(__file__).resolve().parent
 LIBPATH = PKG / "libfclaw_b200.so"
 
-SOLVER_ADVECTION, SOLVER_SWE_ROE, SOLVER_EULER4_ROE = 0, 1, 2
-PROBLEM_SWIRL, PROBLEM_RADIALDAM, PROBLEM_QUADRANTS = 0, 1, 2
+SOLVER_ADVECTION, SOLVER_SWE_ROE, SOLVER_EULER4_ROE, SOLVER_GEOCLAW_FWAVE = 0, 1, 2, 3
+PROBLEM_SWIRL, PROBLEM_RADIALDAM, PROBLEM_QUADRANTS, PROBLEM_BATHY = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 TAG_VALUE, TAG_MINMAX, TAG_DIFFERENCE, TAG_GRADIENT = 0, 1, 2, 3
 
@@ -64,6 +65,7 @@ class _Options(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("macro_graph", ctypes.c_int),
         ("claw_version", ctypes.c_int),
+        ("dry_tolerance", ctypes.c_double),
     ]
 
 
@@ -122,6 +124,8 @@ class Options:
     macro_graph: int = 2
     # 4: fc2d_clawpack46 update, 5: fc2d_clawpack5 update (arrays in q(m,i,j) order)
     claw_version: int = 4
+    # GeoClaw /common_swe/ dry_tolerance
+    dry_tolerance: float = 1e-3
 
     def to_c(self) -> _Options:
         o = _Options()
@@ -131,7 +135,7 @@ class Options:
                      "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph", "claw_version"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
-                     "desired_cfl", "grav", "gamma"):
+                     "desired_cfl", "grav", "gamma", "dry_tolerance"):
             setattr(o, name, float(getattr(self, name)))
         o.order[0], o.order[1] = int(self.order[0]), int(self.order[1])
         for k in range(8):

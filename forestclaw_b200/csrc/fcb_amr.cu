@@ -18,6 +18,11 @@
 
 namespace fcb {
 
+// Bathymetry of the lake-at-rest problem at a cell centre.
+__device__ __forceinline__ double bathy_b(double xc, double yc) {
+    return -1.0 + 0.8 * exp(-((xc - 0.5) * (xc - 0.5) + (yc - 0.5) * (yc - 0.5)) / 0.02);
+}
+
 __global__ void qinit_kernel(const QinitArgs a) {
     const int pi = blockIdx.x;
     if (pi >= a.n) return;
@@ -50,8 +55,40 @@ __global__ void qinit_kernel(const QinitArgs a) {
             q[((int64_t)1 * ny + r) * nx + c] = rho * u;
             q[((int64_t)2 * ny + r) * nx + c] = rho * v;
             q[((int64_t)3 * ny + r) * nx + c] = pr / a.gamma1 + 0.5 * rho * (u * u + v * v);
+        } else if (a.problem == PROB_BATHY) {
+            const double r2 = (xc - a.p[0]) * (xc - a.p[0]) + (yc - a.p[1]) * (yc - a.p[1]);
+            const double eta = a.p[2] * exp(-r2 / (a.p[3] * a.p[3]));
+            const double b = bathy_b(xc, yc);
+            q[((int64_t)0 * ny + r) * nx + c] = (eta - b > 0.0) ? eta - b : 0.0;  // max(0, eta - b)
+            q[((int64_t)1 * ny + r) * nx + c] = 0.0;
+            q[((int64_t)2 * ny + r) * nx + c] = 0.0;
         }
     }
+}
+
+// setaux of the lake-at-rest problem: aux(i,j,1) = b at the cell centres,
+// ghost cells included, for every listed slot.
+__global__ void setaux_kernel(double* aux, int64_t stride, const int32_t* slots, const PatchMeta* meta, int n,
+                              int mx, int my, int mbc) {
+    const int pi = blockIdx.x;
+    if (pi >= n) return;
+    const int slot = slots[pi];
+    const PatchMeta mt = meta[slot];
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    double* a = aux + (int64_t)slot * stride;
+    for (int k = threadIdx.x; k < nx * ny; k += blockDim.x) {
+        const int r = k / nx, c = k - r * nx;
+        const double xc = mt.xlower + (c - mbc + 1 - 0.5) * mt.dx;
+        const double yc = mt.ylower + (r - mbc + 1 - 0.5) * mt.dy;
+        a[k] = bathy_b(xc, yc);
+    }
+}
+
+cudaError_t launch_setaux(double* aux, int64_t stride, const int32_t* slots, const PatchMeta* meta, int n, int mx,
+                          int my, int mbc, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    setaux_kernel<<<n, 256, 0, st>>>(aux, stride, slots, meta, n, mx, my, mbc);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_qinit(const QinitArgs& a, cudaStream_t st) {

@@ -13,7 +13,7 @@ struct PatchMeta {
 };
 enum : int32_t { PATCH_SAVE_LAST = 1 };
 
-enum SolverKind : int32_t { SOLVER_ADVECTION = 0, SOLVER_SWE_ROE = 1, SOLVER_EULER4_ROE = 2 };
+enum SolverKind : int32_t { SOLVER_ADVECTION = 0, SOLVER_SWE_ROE = 1, SOLVER_EULER4_ROE = 2, SOLVER_GEOCLAW_FWAVE = 3 };
 enum AuxKind : int32_t { AUX_NONE = 0, AUX_SWIRL = 1, AUX_STORED = 2 };
 
 // Arguments of one batched step launch (all patches of one level).
@@ -33,6 +33,7 @@ struct StepArgs {
     double vt;             // swirl: cos(2 pi (t + dt/2) / tperiod)
     const double* dyn;     // non-null: {dt, vt} read from device memory (one macro-step graph serves every step)
     double grav, gamma, gamma1;
+    double drytol;         // GeoClaw dry tolerance
     unsigned long long* cfl_out;  // atomicMax on the bits of a non-negative double
 };
 #ifdef __CUDACC__
@@ -73,7 +74,7 @@ struct GhostArgs {
     int interp_fp32;       // mixed precision: coarse-to-fine interpolation in FP32
 };
 
-enum Problem : int32_t { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2 };
+enum Problem : int32_t { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2, PROB_BATHY = 3 };
 
 struct QinitArgs {
     double* q;

@@ -41,6 +41,7 @@ static int solver_meqn(int kind) {
         case FCB_SOLVER_ADVECTION: return 1;
         case FCB_SOLVER_SWE_ROE: return 3;
         case FCB_SOLVER_EULER4_ROE: return 4;
+        case FCB_SOLVER_GEOCLAW_FWAVE: return 3;
         default: return -1;
     }
 }
@@ -63,7 +64,19 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
         bad("the advection solver takes its velocities from the swirl stream function");
     if (opt_.problem == FCB_PROBLEM_RADIALDAM && opt_.solver_kind != FCB_SOLVER_SWE_ROE) bad("radialdam needs SWE");
     if (opt_.problem == FCB_PROBLEM_QUADRANTS && opt_.solver_kind != FCB_SOLVER_EULER4_ROE) bad("quadrants needs Euler");
-    aux_kind_ = (opt_.solver_kind == FCB_SOLVER_ADVECTION) ? AUX_SWIRL : AUX_NONE;
+    if ((opt_.problem == FCB_PROBLEM_BATHY) != (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE))
+        bad("the bathymetry problem and the GeoClaw f-wave solver go together");
+    aux_kind_ = (opt_.solver_kind == FCB_SOLVER_ADVECTION) ? AUX_SWIRL
+              : (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE) ? AUX_STORED : AUX_NONE;
+    if (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE) {
+        if (opt_.maux != 1) bad("the GeoClaw solver reads aux(1) = b: maux must be 1");
+        if (opt_.order[1] != 0) bad("rpt2_geoclaw stops in the reference: the GeoClaw solver needs order (., 0)");
+        if (opt_.precision != 0) bad("the GeoClaw solver is FP64 only");
+        if (opt_.claw_version == 5) bad("the GeoClaw solver is on the clawpack 4.6 path");
+        if (opt_.step_variant == 1 || opt_.step_variant == 2)
+            bad("the GeoClaw solver exists in the pipelined step form only");
+        if (!(opt_.dry_tolerance >= 0.0)) bad("dry_tolerance must be >= 0");
+    }
     if (opt_.step_variant < 0 || opt_.step_variant > 3) bad("step_variant must be 0, 1, 2 or 3");
     if (opt_.precision != 0 && opt_.precision != 1) bad("precision must be 0 (FP64) or 1 (mixed)");
     if (opt_.precision == 1 && (opt_.step_variant == 1 || opt_.step_variant == 2))
@@ -78,6 +91,7 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
     ny_ = opt_.my + 2 * opt_.mbc;
     const int64_t ps = (int64_t)opt_.meqn * nx_ * ny_;
     stride_ = (ps + 31) / 32 * 32;  // 256-byte aligned slots
+    aux_stride_ = aux_kind_ == AUX_STORED ? ((int64_t)opt_.maux * nx_ * ny_ + 31) / 32 * 32 : 0;
     check(cudaMalloc(&d_cfl_, 4 * sizeof(unsigned long long)), "cudaMalloc cfl");
     check(cudaHostAlloc(&h_cfl_, sizeof(unsigned long long), cudaHostAllocDefault), "cudaHostAlloc cfl");
 }
@@ -91,7 +105,11 @@ static double cfl_from_bits(unsigned long long b) {
 double Context::read_cfl(const unsigned long long* d) {
     check(cudaMemcpyAsync(h_cfl_, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st_), "cfl");
     synchronize();
-    return cfl_from_bits(*h_cfl_);
+    const double c = cfl_from_bits(*h_cfl_);
+    if (std::isnan(c))
+        throw Error(FCB_ERR_NUMERIC, "NaN CFL: non-finite state, or a Riemann problem the reference stops on "
+                                     "(negative depth, sonic state in riemann_aug_JCP)");
+    return c;
 }
 
 Context::~Context() {
@@ -103,6 +121,7 @@ Context::~Context() {
     cudaFree(d_qlast_);
     cudaFree(d_qti_);
     cudaFree(d_qsave_);
+    cudaFree(d_aux_);
     cudaFree(d_meta_);
     cudaFree(d_cfl_);
     cudaFreeHost(h_cfl_);
@@ -132,6 +151,12 @@ void Context::ensure_capacity(int n) {
     grow(d_qlast_);
     grow(d_qti_);
     if (!opt_.use_fixed_dt) grow(d_qsave_);
+    if (aux_kind_ == AUX_STORED) {  // recomputed for every patch by mesh_changed
+        check(cudaStreamSynchronize(st_), "sync");
+        cudaFree(d_aux_);
+        d_aux_ = nullptr;
+        check(cudaMalloc(&d_aux_, (size_t)nc * aux_stride_ * sizeof(double)), "cudaMalloc aux");
+    }
     PatchMeta* nm = nullptr;
     check(cudaMalloc(&nm, (size_t)nc * sizeof(PatchMeta)), "cudaMalloc meta");
     if (d_meta_) {
@@ -210,6 +235,11 @@ void Context::mesh_changed() {
     if (!tis.empty()) check(cudaMemcpy(d_ti_slots_.p, tis.data(), tis.size() * 4, cudaMemcpyHostToDevice), "ti");
     std::vector<int32_t> all(slot_of_.begin(), slot_of_.end());
     check(cudaMemcpy(d_all_slots_.p, all.data(), all.size() * 4, cudaMemcpyHostToDevice), "all slots");
+    if (opt_.problem == FCB_PROBLEM_BATHY) {
+        check(launch_setaux(d_aux_, aux_stride_, d_all_slots_.p, d_meta_, n, opt_.mx, opt_.my, opt_.mbc, st_),
+              "setaux");
+        ++cnt_.count_kernel_launches;
+    }
     plans_.clear();
     h_ops_.clear();
     h_groups_.clear();
@@ -508,13 +538,13 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     StepArgs a{};
     a.q = d_q_;
     a.qlast = d_qlast_;
-    a.aux = nullptr;
+    a.aux = aux_kind_ == AUX_STORED ? d_aux_ : nullptr;
     a.slots = d_slots;
     a.meta = d_meta_;
     a.q_stride = stride_;
-    a.aux_stride = 0;
+    a.aux_stride = aux_stride_;
     a.npatches = n;
-    a.maux = 0;
+    a.maux = aux_kind_ == AUX_STORED ? opt_.maux : 0;
     a.order0 = opt_.order[0];
     a.order1 = opt_.order[1];
     for (int k = 0; k < 8; ++k) a.mthlim[k] = opt_.mthlim[k];
@@ -529,6 +559,7 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     a.grav = opt_.grav;
     a.gamma = opt_.gamma;
     a.gamma1 = opt_.gamma - 1.0;
+    a.drytol = opt_.dry_tolerance;
     a.cfl_out = cfl_slot;
     if (use_dyn_) {
         // {dt, vt} of launch dyn_n_ of the macro step: written to the table by
@@ -567,7 +598,8 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     } else if (v == 2) {
         if (aux_kind_ == AUX_SWIRL) e = launch_step_warp_swirl(opt_.mx, opt_.mbc, a, st_);
         if (e == cudaErrorNotSupported) throw Error(FCB_ERR_INVALID, "no warp-synchronous step for this case");
-    } else if (v == 3 || (v == 0 && (opt_.solver_kind == SOLVER_ADVECTION || opt_.claw_version == 5))) {
+    } else if (v == 3 || (v == 0 && (opt_.solver_kind == SOLVER_ADVECTION || opt_.claw_version == 5 ||
+                                    opt_.solver_kind == SOLVER_GEOCLAW_FWAVE))) {
         // default: the pipelined form for scalar advection; the Roe solvers keep
         // the four-barrier form, whose smaller register footprint suits them
         e = launch_step_pipe(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, opt_.claw_version,

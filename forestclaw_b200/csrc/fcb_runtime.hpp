@@ -36,6 +36,8 @@ cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64
                               double alpha, cudaStream_t st);
 struct QinitArgs;
 cudaError_t launch_qinit(const QinitArgs& a, cudaStream_t st);
+cudaError_t launch_setaux(double* aux, int64_t stride, const int32_t* slots, const PatchMeta* meta, int n, int mx,
+                          int my, int mbc, cudaStream_t st);
 struct TagArgs;
 cudaError_t launch_tag(const TagArgs& a, cudaStream_t st);
 cudaError_t launch_regrid(double* q, int64_t stride, const int32_t* ops, const int32_t* fine, int nops,
@@ -131,6 +133,8 @@ class Context {
     double* d_qlast_ = nullptr;
     double* d_qti_ = nullptr;
     double* d_qsave_ = nullptr;
+    double* d_aux_ = nullptr;         // stored aux (bathymetry), recomputed after every mesh change
+    int64_t aux_stride_ = 0;
     PatchMeta* d_meta_ = nullptr;
     // level lists (device), grouped by level
     DevBuf<int32_t> d_level_slots_;

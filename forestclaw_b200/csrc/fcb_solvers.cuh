@@ -27,10 +27,11 @@ template <int W_, typename R = double, bool V5_ = false>
 struct AdvectionSolver {
     using Real = R;
     static constexpr bool V5 = V5_;
+    static constexpr bool FWAVE = false;
     static constexpr int M = 1;
     static constexpr int W = W_;
     struct Roe {};
-    R grav, gamma, gamma1;  // unused
+    R grav, gamma, gamma1, drytol;  // unused
     __device__ __forceinline__ void rpn2(int /*ixy*/, const R* qL, const R* qR, R speed,
                                          R (*wave)[M], R* s, R* amdq, R* apdq,
                                          Roe&) const {
@@ -70,10 +71,11 @@ template <typename R, bool V5_ = false>
 struct SweRoeT {
     using Real = R;
     static constexpr bool V5 = V5_;
+    static constexpr bool FWAVE = false;
     static constexpr int M = 3;
     static constexpr int W = 3;
     struct Roe { R u, v, a; };
-    R grav, gamma, gamma1;
+    R grav, gamma, gamma1, drytol;  // drytol: GeoClaw only
     __device__ __forceinline__ void rpn2(int ixy, const R* qL, const R* qR, R /*speed*/,
                                          R (*wave)[M], R* s, R* amdq, R* apdq,
                                          Roe& rr) const {
@@ -178,10 +180,11 @@ template <typename R, bool V5_ = false>
 struct Euler4RoeT {
     using Real = R;
     static constexpr bool V5 = V5_;
+    static constexpr bool FWAVE = false;
     static constexpr int M = 4;
     static constexpr int W = 4;
     struct Roe { R u, v, a, enth, u2v2, g1a2, euv; };
-    R grav, gamma, gamma1;
+    R grav, gamma, gamma1, drytol;  // drytol: GeoClaw only
     __device__ __forceinline__ void rpn2(int ixy, const R* qL, const R* qR, R,
                                          R (*wave)[M], R* s, R* amdq, R* apdq,
                                          Roe& rr) const {
@@ -307,6 +310,257 @@ struct Euler4RoeT {
 
 using SweRoeSolver = SweRoeT<double>;
 using Euler4RoeSolver = Euler4RoeT<double>;
+
+
+// ---------------------------------------------------------------------------
+// GeoClaw f-wave solver: applications/clawpack/shallow/2d/rp/rpn2_geoclaw.f90
+// with geoclaw_riemann_utils.f (riemanntype, riemann_aug_JCP, maxiter = 1).
+// FP64 only.  The reference stops on a negative depth or a sonic state; here
+// such an interface sets `bad`, which the kernel reports as a NaN CFL.  The
+// reference's rpt2_geoclaw stops on entry, so no transverse solver exists.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double fsignd(double a, double b) { return signbit(b) ? -fabs(a) : fabs(a); }
+
+__device__ __forceinline__ void geo_riemanntype(double hL, double hR, double uL, double uR, double& hm, double& s1m,
+                                                double& s2m, double drytol, double g) {
+    const double h_min = fmin(hR, hL), h_max = fmax(hR, hL);
+    const double delu = uR - uL;
+    if (h_min <= drytol) {
+        hm = 0.0;
+        s1m = uR + uL - 2.0 * sqrt(g * hR) + 2.0 * sqrt(g * hL);
+        s2m = s1m;
+    } else {
+        const double F_min = delu + 2.0 * (sqrt(g * h_min) - sqrt(g * h_max));
+        const double F_max = delu + (h_max - h_min) * (sqrt(.5 * g * (h_max + h_min) / (h_max * h_min)));
+        if (F_min > 0.0) {
+            const double t = dmax(0.0, -delu + 2.0 * (sqrt(g * hL) + sqrt(g * hR)));
+            hm = (1.0 / (16.0 * g)) * (t * t);
+            s1m = uL + 2.0 * sqrt(g * hL) - 3.0 * sqrt(g * hm);
+            s2m = uR - 2.0 * sqrt(g * hR) + 3.0 * sqrt(g * hm);
+        } else if (F_max <= 0.0) {
+            double h0 = h_max;
+            {
+                const double gL = sqrt(.5 * g * (1 / h0 + 1 / hL));
+                const double gR = sqrt(.5 * g * (1 / h0 + 1 / hR));
+                const double F0 = delu + (h0 - hL) * gL + (h0 - hR) * gR;
+                const double dfdh = gL - g * (h0 - hL) / (4.0 * (h0 * h0) * gL) + gR - g * (h0 - hR) / (4.0 * (h0 * h0) * gR);
+                const double slope = 2.0 * sqrt(h0) * dfdh;
+                const double t = sqrt(h0) - F0 / slope;
+                h0 = t * t;
+            }
+            hm = h0;
+            const double u1m = uL - (hm - hL) * sqrt((.5 * g) * (1 / hm + 1 / hL));
+            const double u2m = uR + (hm - hR) * sqrt((.5 * g) * (1 / hm + 1 / hR));
+            s1m = u1m - sqrt(g * hm);
+            s2m = u2m + sqrt(g * hm);
+        } else {
+            double h0 = h_min;
+            {
+                const double F0 = delu + 2.0 * (sqrt(g * h0) - sqrt(g * h_max)) +
+                                  (h0 - h_min) * sqrt(.5 * g * (1 / h0 + 1 / h_min));
+                const double slope = (F_max - F0) / (h_max - h_min);
+                h0 = h0 - F0 / slope;
+            }
+            hm = h0;
+            if (hL > hR) {
+                s1m = uL + 2.0 * sqrt(g * hL) - 3.0 * sqrt(g * hm);
+                s2m = uL + 2.0 * sqrt(g * hL) - sqrt(g * hm);
+            } else {
+                s2m = uR - 2.0 * sqrt(g * hR) + 3.0 * sqrt(g * hm);
+                s1m = uR - 2.0 * sqrt(g * hR) + sqrt(g * hm);
+            }
+        }
+    }
+}
+
+// riemann_aug_JCP with maxiter = 1 and rarecorrectortest = .false.; returns false on a sonic state
+__device__ __forceinline__ bool geo_riemann_aug(double hL, double hR, double huL, double huR, double bL, double bR,
+                                                double uL, double uR, double vL, double vR, double phiL, double phiR,
+                                                double sE1, double sE2, double drytol, double g, double sw[3],
+                                                double fw[3][3]) {
+    const double rho = -9999999.0, pL = 0.0, pR = 0.0;
+    const double delh = hR - hL, delhu = huR - huL, delphi = phiR - phiL, delb = bR - bL, delP = pR - pL;
+    double hm, s1m, s2m;
+    geo_riemanntype(hL, hR, uL, uR, hm, s1m, s2m, drytol, g);
+    double lambda[3];
+    lambda[0] = dmin(sE1, s2m);
+    lambda[2] = dmax(sE2, s1m);
+    sE1 = lambda[0];
+    sE2 = lambda[2];
+    const double hstarHLL = dmax((huL - huR + sE2 * hR - sE1 * hL) / (sE2 - sE1), 0.0);
+    double r[3][3];
+#pragma unroll
+    for (int mw = 0; mw < 3; ++mw) {
+        r[0][mw] = 1.0;
+        r[1][mw] = (mw == 1) ? 0.0 : lambda[mw];
+        r[2][mw] = (mw == 1) ? 0.0 : lambda[mw] * lambda[mw];
+    }
+    lambda[1] = 0.5 * (lambda[0] + lambda[2]);
+    r[0][1] = 0.0;
+    r[1][1] = 0.0;
+    r[2][1] = 1.0;
+    const double criticaltol = dmax(drytol * g, 1e-6);
+    const double criticaltol_2 = sqrt(criticaltol);
+    const double hbar = dmax(0.5 * (hL + hR), 0.0);
+    const double s1s2bar = 0.25 * ((uL + uR) * (uL + uR)) - g * hbar;
+    const double s1s2tilde = dmax(0.0, uL * uR) - g * hbar;
+    bool sonic = false;
+    if (fabs(s1s2bar) <= criticaltol) sonic = true;
+    else if (s1s2bar * s1s2tilde <= criticaltol * criticaltol) sonic = true;
+    else if (s1s2bar * sE1 * sE2 <= criticaltol * criticaltol) sonic = true;
+    else if (dmin(fabs(sE1), fabs(sE2)) < criticaltol_2) sonic = true;
+    else if (sE1 < criticaltol_2 && s1m > -criticaltol_2) sonic = true;
+    else if (sE2 > -criticaltol_2 && s2m < criticaltol_2) sonic = true;
+    else if ((uL + sqrt(g * hL)) * (uR + sqrt(g * hR)) < 0.0) sonic = true;
+    else if ((uL - sqrt(g * hL)) * (uR - sqrt(g * hR)) < 0.0) sonic = true;
+    double deldelh = delb * g * hbar / s1s2bar;
+    if (sE1 < -criticaltol && sE2 > criticaltol) {
+        deldelh = dmin(deldelh, hstarHLL * (sE2 - sE1) / sE2);
+        deldelh = dmax(deldelh, hstarHLL * (sE2 - sE1) / sE1);
+    } else if (sE1 >= criticaltol) {
+        deldelh = dmin(deldelh, hstarHLL * (sE2 - sE1) / sE1);
+        deldelh = dmax(deldelh, -hL);
+    } else if (sE2 <= -criticaltol) {
+        deldelh = dmin(deldelh, hR);
+        deldelh = dmax(deldelh, hstarHLL * (sE2 - sE1) / sE2);
+    }
+    deldelh = deldelh - delP / (rho * g);
+    double deldelphi = -(delb * g * hbar * s1s2tilde / s1s2bar);
+    deldelphi = dmin(deldelphi, g * dmax(-hL * delb, -hR * delb));
+    deldelphi = dmax(deldelphi, g * dmin(-hL * delb, -hR * delb));
+    deldelphi = deldelphi - hbar * delP / rho;
+    const double del[3] = {delh - deldelh, delhu, delphi - deldelphi};
+    double det1 = r[0][0] * (r[1][1] * r[2][2] - r[1][2] * r[2][1]);
+    double det2 = r[0][1] * (r[1][0] * r[2][2] - r[1][2] * r[2][0]);
+    double det3 = r[0][2] * (r[1][0] * r[2][1] - r[1][1] * r[2][0]);
+    const double determinant = det1 - det2 + det3;
+    double beta[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double A[3][3];
+#pragma unroll
+        for (int mw = 0; mw < 3; ++mw)
+#pragma unroll
+            for (int m = 0; m < 3; ++m) A[m][mw] = (mw == k) ? del[m] : r[m][mw];
+        det1 = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]);
+        det2 = A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]);
+        det3 = A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+        beta[k] = (det1 - det2 + det3) / determinant;
+    }
+#pragma unroll
+    for (int mw = 0; mw < 3; ++mw) {
+        sw[mw] = lambda[mw];
+        fw[0][mw] = beta[mw] * r[1][mw];
+        fw[1][mw] = beta[mw] * r[2][mw];
+        fw[2][mw] = beta[mw] * r[1][mw];
+    }
+    fw[2][0] = fw[2][0] * vL;
+    fw[2][2] = fw[2][2] * vR;
+    fw[2][1] = 0.0;
+    const double hustar_interface = huL + fw[0][0];
+    if (hustar_interface <= 0.0) fw[2][0] = fw[2][0] + (hR * uR * vR - hL * uL * vL - fw[2][0] - fw[2][2]);
+    else fw[2][2] = fw[2][2] + (hR * uR * vR - hL * uL * vL - fw[2][0] - fw[2][2]);
+    return !sonic;
+}
+
+template <typename R, bool V5_ = false>
+struct GeoclawFwaveT {
+    static_assert(sizeof(R) == sizeof(double), "the GeoClaw solver is FP64 only");
+    using Real = R;
+    static constexpr bool V5 = V5_;
+    static constexpr bool FWAVE = true;
+    static constexpr int M = 3;
+    static constexpr int W = 3;
+    struct Roe {};
+    R grav, gamma, gamma1, drytol;
+    // one interface of rpn2_geoclaw.f90; bL, bR: aux(1) of the two cells
+    __device__ __forceinline__ void rpn2b(int ixy, const double* qL, const double* qR, double bL, double bR,
+                                          double (*wave)[M], double* s, double* amdq, double* apdq,
+                                          bool& bad) const {
+        const int mu = (ixy == 1) ? 1 : 2;
+        const int mv = (ixy == 1) ? 2 : 1;
+        const double g = grav;
+#pragma unroll
+        for (int mw = 0; mw < 3; ++mw) {
+            s[mw] = 0.0;
+            wave[mw][0] = 0.0; wave[mw][1] = 0.0; wave[mw][2] = 0.0;
+        }
+        if (qL[0] < 0.0 || qR[0] < 0.0) bad = true;
+        if (!(qL[0] <= drytol && qR[0] <= drytol)) {
+            double hL = qL[0], hR = qR[0], huL = qL[mu], huR = qR[mu], hvL = qL[mv], hvR = qR[mv];
+            double uR, vR, phiR, uL, vL, phiL;
+            if (hR > drytol) {
+                uR = huR / hR; vR = hvR / hR;
+                phiR = 0.5 * grav * (hR * hR) + (huR * huR) / hR;
+            } else {
+                hR = 0.0; huR = 0.0; hvR = 0.0; uR = 0.0; vR = 0; phiR = 0.0;
+            }
+            if (hL > drytol) {
+                uL = huL / hL; vL = hvL / hL;
+                phiL = 0.5 * grav * (hL * hL) + (huL * huL) / hL;
+            } else {
+                hL = 0.0; huL = 0.0; hvL = 0.0; uL = 0.0; vL = 0.0; phiL = 0.0;
+            }
+            double wall[3] = {1.0, 1.0, 1.0};
+            double hstar, s1m, s2m;
+            if (hR <= drytol) {
+                geo_riemanntype(hL, hL, uL, -uL, hstar, s1m, s2m, drytol, grav);
+                const double hstartest = dmax(hL, hstar);
+                if (hstartest + bL < bR) {
+                    wall[1] = 0.0; wall[2] = 0.0;
+                    hR = hL; huR = -huL; bR = bL; phiR = phiL; uR = -uL; vL = vR;
+                } else if (hL + bL < bR) {
+                    bR = hL + bL;
+                }
+            } else if (hL <= drytol) {
+                geo_riemanntype(hR, hR, -uR, uR, hstar, s1m, s2m, drytol, grav);
+                const double hstartest = dmax(hR, hstar);
+                if (hstartest + bR < bL) {
+                    wall[0] = 0.0; wall[1] = 0.0;
+                    hL = hR; huL = -huR; bL = bR; phiL = phiR; uL = -uR; vR = vL;
+                } else if (hR + bR < bL) {
+                    bL = hR + bR;
+                }
+            }
+            const double sL = uL - sqrt(grav * hL);
+            const double sR = uR + sqrt(grav * hR);
+            const double uhat = (sqrt(grav * hL) * uL + sqrt(grav * hR) * uR) / (sqrt(grav * hR) + sqrt(grav * hL));
+            const double chat = sqrt(grav * 0.5 * (hR + hL));
+            const double sE1 = dmin(sL, uhat - chat), sE2 = dmax(sR, uhat + chat);
+            double sw[3], fw[3][3];
+            if (!geo_riemann_aug(hL, hR, huL, huR, bL, bR, uL, uR, vL, vR, phiL, phiR, sE1, sE2, drytol, g, sw, fw))
+                bad = true;
+#pragma unroll
+            for (int mw = 0; mw < 3; ++mw) {
+                s[mw] = sw[mw] * wall[mw];
+                wave[mw][0] = fw[0][mw] * wall[mw];
+                wave[mw][mu] = fw[1][mw] * wall[mw];
+                wave[mw][mv] = fw[2][mw] * wall[mw];
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            double am = 0.0, ap = 0.0;
+#pragma unroll
+            for (int mw = 0; mw < 3; ++mw) {
+                if (s[mw] < 0.0) am = am + wave[mw][m];
+                else if (s[mw] > 0.0) ap = ap + wave[mw][m];
+                else {
+                    am = am + 0.5 * wave[mw][m];
+                    ap = ap + 0.5 * wave[mw][m];
+                }
+            }
+            amdq[m] = am;
+            apdq[m] = ap;
+        }
+    }
+    // never called: order (2, 0) is enforced for this solver
+    __device__ __forceinline__ void rpt2(int, const R* asdq, const Roe&, R, R, R* bm, R* bp) const {
+#pragma unroll
+        for (int m = 0; m < M; ++m) bm[m] = bp[m] = R(0) * asdq[m];
+    }
+    __device__ __forceinline__ void rpn2(int, const R*, const R*, R, R (*)[M], R*, R*, R*, Roe&) const {}
+};
 
 // clawpack46_inlinelimiter.f:4-118: phi(r) for limiter code `mth`
 // (clawpack5_inlinelimiter.f:4-109 knows codes 1-5; callers map the others to 1).

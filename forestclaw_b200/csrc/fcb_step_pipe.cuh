@@ -105,6 +105,7 @@ struct PipeState {
     R FYm1[M], FYm2[M], FYp1[M], FYp2[M], FYp3[M];       // y fluxes of the own column, delayed
     double pcur;                                         // swirl: psi at node (c, s+1)
     R smax_x, smax_y;  // largest |s| over the CFL interfaces of each direction
+    bool bad;          // a Riemann problem the reference would stop on (reported as a NaN CFL)
 };
 
 // Per-thread constants: column, flags and this thread's element of the rings.
@@ -144,12 +145,20 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
     // fluxes at interfaces 1..mx+1 only, accumulated into cells 1..mx+1, and
     // only the interior cells updated
     constexpr bool V5 = SOL::V5;
+    // f-waves (clawpack46_flux2fw.f): Godunov and correction terms on interfaces
+    // 1..mx+1 only, corrections weighted by sign(s), no transverse part
+    constexpr bool FWAVE = SOL::FWAVE;
+    constexpr bool R15 = V5 || FWAVE;  // fluxes on interfaces MBC..MBC+MX only
+    auto abs_sign = [](R sv) -> R {
+        if constexpr (FWAVE) return copysign(R(1), sv);
+        else return fabs(sv);
+    };
     const int c = T.c;
     auto s2 = [&](int d) -> int { return J >= 0 ? cslot(J, d, 2) : ((s - d) & 1); };
     auto s4 = [&](int d) -> int { return J >= 0 ? cslot(J, d, 4) : ((s - d) & 3); };
     // aux component k of row s-d, column c+dc
     auto AUXV = [&](int k, int dc, int d) -> R {
-        if constexpr (NAUX > 0) return T.rb[L::AX + (s4(d) * NAUX + k) * L::PNX + dc];
+        if constexpr (NAUX > 0) return k < NAUX ? T.rb[L::AX + (s4(d) * NAUX + k) * L::PNX + dc] : R(0);
         else return R(0);
     };
 
@@ -220,7 +229,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
         const int k = s - 2;
         if (T.active && (STEADY || (k >= 0 && k <= NY - 2))) {
             R* fx = T.rb + L::FX + s4(2) * (2 * M * L::PNX);
-            const bool xint = (STEADY || k >= 1) && (V5 ? (c >= MBC && c <= MBC + MX) : c >= 1);
+            const bool xint = (STEADY || k >= 1) && (R15 ? (c >= MBC && c <= MBC + MX) : c >= 1);
             if (xint) {
                 const R* xw = T.rb + L::XW + s2(2) * (W * M * L::PNX);
                 R cq[M];
@@ -254,12 +263,12 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                         R acc;
                         {
                             const R as = fabs(S.xsl[0]);
-                            acc = as * (R(1) - as * T.rdtdx) * S.xwl[0][m];
+                            acc = abs_sign(S.xsl[0]) * (R(1) - as * T.rdtdx) * S.xwl[0][m];
                         }
 #pragma unroll
                         for (int mw = 1; mw < W; ++mw) {
                             const R as = fabs(S.xsl[mw]);
-                            acc = acc + as * (R(1) - as * T.rdtdx) * S.xwl[mw][m];
+                            acc = acc + abs_sign(S.xsl[mw]) * (R(1) - as * T.rdtdx) * S.xwl[mw][m];
                         }
                         cq[m] = acc;
                     }
@@ -305,7 +314,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 for (int m = 0; m < M; ++m) {
                     fx[(0 * M + m) * L::PNX] = R(0);
                     fx[(1 * M + m) * L::PNX] = R(0);
-                    if constexpr (V5) {  // read by the cell to the left (mx+1 at the right end)
+                    if constexpr (R15) {  // read by the cell to the left (mx+1 at the right end)
                         R* gl = T.rb + L::GL + s2(2) * (2 * M * L::PNX);
                         gl[(0 * M + m) * L::PNX] = R(0);
                         gl[(1 * M + m) * L::PNX] = R(0);
@@ -326,7 +335,13 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 qL[m] = qr[m * L::PNX - 1];
                 qR[m] = R(S.q_m1[m]);
             }
-            sol.rpn2(1, qL, qR, AUXV(0, 0, 1), S.xwl, S.xsl, S.xam, S.xap, S.xR);
+            if constexpr (FWAVE) {
+                bool bad = false;
+                sol.rpn2b(1, qL, qR, AUXV(0, -1, 1), AUXV(0, 0, 1), S.xwl, S.xsl, S.xam, S.xap, bad);
+                S.bad = S.bad || bad;
+            } else {
+                sol.rpn2(1, qL, qR, AUXV(0, 0, 1), S.xwl, S.xsl, S.xam, S.xap, S.xR);
+            }
             R* xw = T.rb + L::XW + s2(1) * (W * M * L::PNX);
 #pragma unroll
             for (int mw = 0; mw < W; ++mw) {
@@ -364,7 +379,13 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                     qD[m] = R(S.q_m1[m]);
                     qU[m] = R(S.qcur[m]);
                 }
-                sol.rpn2(2, qD, qU, AUXV(1, 0, 0), yw_n, ys_n, yam_n, yap_n, yR_n);
+                if constexpr (FWAVE) {
+                    bool bad = false;
+                    sol.rpn2b(2, qD, qU, AUXV(0, 0, 1), AUXV(0, 0, 0), yw_n, ys_n, yam_n, yap_n, bad);
+                    S.bad = S.bad || bad;
+                } else {
+                    sol.rpn2(2, qD, qU, AUXV(1, 0, 0), yw_n, ys_n, yam_n, yap_n, yR_n);
+                }
 #pragma unroll
                 for (int mw = 0; mw < W; ++mw) {
                     R d = S.yw_f[mw][0] * yw_n[mw][0];
@@ -386,11 +407,11 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
         }
         // clawpack 5: interfaces MBC..MBC+MX carry fluxes; f = MBC+MX+1 only
         // closes the transverse sum of cell row MBC+MX
-        const bool yblk = T.ycol && (V5 ? (f >= MBC && f <= MBC + MX + 1) : (STEADY || (f >= 1 && f <= NY - 1)));
+        const bool yblk = T.ycol && (R15 ? (f >= MBC && f <= MBC + MX + 1) : (STEADY || (f >= 1 && f <= NY - 1)));
         if (yblk) {
-            const bool fact = !V5 || f <= MBC + MX;
-            const bool inner = V5 ? fact : (STEADY || (f >= MBC && f <= MBC + MX));
-            const bool god = V5 ? fact : (STEADY || f <= NY - 2);
+            const bool fact = !R15 || f <= MBC + MX;
+            const bool inner = R15 ? fact : (STEADY || (f >= MBC && f <= MBC + MX));
+            const bool god = R15 ? fact : (STEADY || f <= NY - 2);
             R w[W][M];
 #pragma unroll
             for (int mw = 0; mw < W; ++mw)
@@ -424,12 +445,12 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                     R acc;
                     {
                         const R as = fabs(S.ys_f[0]);
-                        acc = as * (R(1) - as * T.rdtdy) * w[0][m];
+                        acc = abs_sign(S.ys_f[0]) * (R(1) - as * T.rdtdy) * w[0][m];
                     }
 #pragma unroll
                     for (int mw = 1; mw < W; ++mw) {
                         const R as = fabs(S.ys_f[mw]);
-                        acc = acc + as * (R(1) - as * T.rdtdy) * w[mw][m];
+                        acc = acc + abs_sign(S.ys_f[mw]) * (R(1) - as * T.rdtdy) * w[mw][m];
                     }
                     cq[m] = acc;
                 }
@@ -461,7 +482,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 for (int m = 0; m < M; ++m) gLm[m] = gLp[m] = gRm[m] = gRp[m] = R(0);
             }
             // cell row f-1 is complete: gadd(f-1,.,1) = (0 - gL(f)) - gR(f-1)
-            if (V5 ? (f - 1 >= MBC && f - 1 <= MBC + MX) : (STEADY || f - 1 >= 1)) {
+            if (R15 ? (f - 1 >= MBC && f - 1 <= MBC + MX) : (STEADY || f - 1 >= 1)) {
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
                     GYd[m] = -(double)gLm[m] - (double)S.gRm_prev[m];
@@ -563,7 +584,7 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     const int cc = c < NX ? c : NX - 1;
     const int slot = patch_ok ? a.slots[pg] : 0;
     const PatchMeta meta = patch_ok ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0};
-    const SOL sol{R(a.grav), R(a.gamma), R(a.gamma1)};
+    const SOL sol{R(a.grav), R(a.gamma), R(a.gamma1), R(a.drytol)};
 
     PipeThread<R> T;
     T.c = cc;
@@ -612,6 +633,7 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     S.xR = typename SOL::Roe{};
     S.pcur = 0.0;
     S.smax_x = S.smax_y = R(0);
+    S.bad = false;
 
     // ---- prologue: aux row 0 ----
     if constexpr (SWIRL) {
@@ -666,6 +688,7 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     // monotone, so max_i fl(dtdx*|s_i|) == fl(dtdx * max_i |s_i|): one product
     // per direction gives the reference's value exactly.
     double cfl = (double)dmax(T.rdtdx * S.smax_x, T.rdtdy * S.smax_y);
+    if (S.bad) cfl = __longlong_as_double(0x7ff8000000000000LL);  // NaN: wins the max, reported by the host
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
     if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg_p(a.cfl_out, cfl);
@@ -748,6 +771,12 @@ cudaError_t launch_step_pipe_v(int solver, int aux_kind, int mwaves, int mx, int
         case SOLVER_EULER4_ROE:
             if (mwaves != 4 || aux_kind != AUX_NONE) return cudaErrorNotSupported;
             return launch_pipe_mx<Euler4RoeT<R, V5>, AUX_NONE, 0>(mx, mbc, a, st);
+        case SOLVER_GEOCLAW_FWAVE:
+            if constexpr (sizeof(R) == sizeof(double) && !V5) {
+                if (mwaves != 3 || aux_kind != AUX_STORED || a.maux != 1) return cudaErrorNotSupported;
+                return launch_pipe_mx<GeoclawFwaveT<R>, AUX_STORED, 1>(mx, mbc, a, st);
+            }
+            return cudaErrorNotSupported;
         default: return cudaErrorNotSupported;
     }
 }

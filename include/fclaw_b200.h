@@ -41,7 +41,10 @@ enum fcb_status {
 enum fcb_solver_kind {
     FCB_SOLVER_ADVECTION = 0,  /* clawpack46_rpn2adv / rpt2adv (edge velocities in aux) */
     FCB_SOLVER_SWE_ROE = 1,    /* shallow water Roe with entropy fix (clawpack46_rpn2/rpt2) */
-    FCB_SOLVER_EULER4_ROE = 2  /* Euler Roe with entropy fix (clawpack46_rpn2_euler4/rpt2_euler4) */
+    FCB_SOLVER_EULER4_ROE = 2, /* Euler Roe with entropy fix (clawpack46_rpn2_euler4/rpt2_euler4) */
+    FCB_SOLVER_GEOCLAW_FWAVE = 3 /* shallow water over bathymetry aux(1) = b: rpn2_geoclaw f-waves
+                                  * with clawpack46_flux2fw; order (2, 0) only, because the
+                                  * reference's rpt2_geoclaw stops; FP64 only */
 };
 
 /* Initial conditions / b4step2 hooks of the configured applications. */
@@ -53,7 +56,9 @@ enum fcb_precision {
 enum fcb_problem {
     FCB_PROBLEM_SWIRL = 0,      /* advection/2d/swirl: qinit.f, b4step2.f velocities; p[0] = tperiod */
     FCB_PROBLEM_RADIALDAM = 1,  /* dam break: p = {x0, y0, r0, h_in, h_out} */
-    FCB_PROBLEM_QUADRANTS = 2   /* euler/2d/quadrants qinit.f: p = rho[4], u[4], v[4], p[4], xs, ys */
+    FCB_PROBLEM_QUADRANTS = 2,  /* euler/2d/quadrants qinit.f: p = rho[4], u[4], v[4], p[4], xs, ys */
+    FCB_PROBLEM_BATHY = 3       /* lake at rest over b = -1 + 0.8 exp(-((x-.5)^2+(y-.5)^2)/0.02)
+                                 * with a surface pulse p[2] exp(-((x-p[0])^2+(y-p[1])^2)/p[3]^2) */
 };
 
 /* Refinement criteria (fclaw2d_clawpatch_options "refinement-criteria"). */
@@ -112,6 +117,8 @@ typedef struct fcb_options {
      * solver arithmetic); fcb_get_q / fcb_set_q then use the clawpack 5 array
      * order q(m,i,j) for every patch (pipelined step form only) */
     int claw_version;
+    /* GeoClaw /common_swe/ dry_tolerance */
+    double dry_tolerance;
 } fcb_options_t;
 
 typedef struct fcb_counters {

@@ -198,11 +198,19 @@ void Solver::qinit_patch(int p) {
             qinit_quadrants(opt.mx, opt.my, opt.mbc, xlower(p), ylower(p), dx(p), dy(p),
                             opt.solver.gamma1, pp + 0, pp + 4, pp + 8, pp + 12, pp[16], pp[17], q);
             break;
+        case PROB_BATHY:
+            qinit_bathy(opt.mx, opt.my, opt.mbc, xlower(p), ylower(p), dx(p), dy(p), pp, q);
+            break;
         default: throw std::runtime_error("unknown problem");
     }
 }
 
-void Solver::setaux_patch(int) {}
+// setaux: the bathymetry depends on the cell centres only, so a new patch gets
+// it from the formula (no transfer from its parent or children).
+void Solver::setaux_patch(int p) {
+    if (opt.problem == PROB_BATHY)
+        setaux_bathy(opt.mx, opt.my, opt.mbc, xlower(p), ylower(p), dx(p), dy(p), data[p].aux.data());
+}
 
 // clawpack46_update (fc2d_clawpack46.cpp:403-444) for one patch.
 double Solver::single_step_patch(int p, double t, double dt) {

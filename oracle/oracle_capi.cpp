@@ -25,7 +25,7 @@ enum IOpt {
 };
 enum DOpt {
     D_REFINE_TH, D_COARSEN_TH, D_TFINAL, D_INITIAL_DT, D_MAX_CFL, D_DESIRED_CFL,
-    D_GRAV, D_GAMMA, D_GAMMA1, D_PPARAM0, D_COUNT = D_PPARAM0 + 32
+    D_GRAV, D_GAMMA, D_GAMMA1, D_DRYTOL, D_PPARAM0, D_COUNT = D_PPARAM0 + 32
 };
 
 Options unpack(const int* io, const double* d) {
@@ -46,6 +46,7 @@ Options unpack(const int* io, const double* d) {
     o.tfinal = d[D_TFINAL]; o.initial_dt = d[D_INITIAL_DT]; o.max_cfl = d[D_MAX_CFL];
     o.desired_cfl = d[D_DESIRED_CFL];
     o.solver.grav = d[D_GRAV]; o.solver.gamma = d[D_GAMMA]; o.solver.gamma1 = d[D_GAMMA1];
+    o.solver.drytol = d[D_DRYTOL];
     for (int k = 0; k < 32; ++k) o.pparams[k] = d[D_PPARAM0 + k];
     return o;
 }

@@ -33,6 +33,302 @@ struct RiemannState {
     }
 };
 
+// ---------------------------------------------------------------------------
+// GeoClaw f-wave solver (applications/clawpack/shallow/2d/rp/rpn2_geoclaw.f90
+// with geoclaw_riemann_utils.f: riemanntype, riemann_aug_JCP), called with
+// maxiter = 1 as the reference does.  The reference stops (Fortran STOP) on a
+// negative depth and on a sonic state; here those raise std::runtime_error.
+// ---------------------------------------------------------------------------
+inline double fsign(double a, double b) { return std::signbit(b) ? -std::fabs(a) : std::fabs(a); }
+
+// geoclaw_riemann_utils.f: riemanntype
+void riemanntype(double hL, double hR, double uL, double uR, double& hm, double& s1m, double& s2m,
+                 bool& rare1, bool& rare2, int maxiter, double drytol, double g) {
+    double um, u1m, u2m, h0, F0, slope, gL, gR, dfdh;
+    const double h_min = std::min(hR, hL), h_max = std::max(hR, hL);
+    const double delu = uR - uL;
+    if (h_min <= drytol) {
+        hm = 0.0;
+        um = 0.0;
+        s1m = uR + uL - 2.0 * std::sqrt(g * hR) + 2.0 * std::sqrt(g * hL);
+        s2m = uR + uL - 2.0 * std::sqrt(g * hR) + 2.0 * std::sqrt(g * hL);
+        if (hL <= 0.0) { rare2 = true; rare1 = false; }
+        else { rare1 = true; rare2 = false; }
+    } else {
+        const double F_min = delu + 2.0 * (std::sqrt(g * h_min) - std::sqrt(g * h_max));
+        const double F_max = delu + (h_max - h_min) * (std::sqrt(.5 * g * (h_max + h_min) / (h_max * h_min)));
+        if (F_min > 0.0) {  // 2-rarefactions
+            const double t = std::max(0.0, -delu + 2.0 * (std::sqrt(g * hL) + std::sqrt(g * hR)));
+            hm = (1.0 / (16.0 * g)) * (t * t);
+            um = fsign(1.0, hm) * (uL + 2.0 * (std::sqrt(g * hL) - std::sqrt(g * hm)));
+            s1m = uL + 2.0 * std::sqrt(g * hL) - 3.0 * std::sqrt(g * hm);
+            s2m = uR - 2.0 * std::sqrt(g * hR) + 3.0 * std::sqrt(g * hm);
+            rare1 = true;
+            rare2 = true;
+        } else if (F_max <= 0.0) {  // 2 shocks
+            h0 = h_max;
+            for (int iter = 1; iter <= maxiter; ++iter) {
+                gL = std::sqrt(.5 * g * (1 / h0 + 1 / hL));
+                gR = std::sqrt(.5 * g * (1 / h0 + 1 / hR));
+                F0 = delu + (h0 - hL) * gL + (h0 - hR) * gR;
+                dfdh = gL - g * (h0 - hL) / (4.0 * (h0 * h0) * gL) + gR - g * (h0 - hR) / (4.0 * (h0 * h0) * gR);
+                slope = 2.0 * std::sqrt(h0) * dfdh;
+                const double t = std::sqrt(h0) - F0 / slope;
+                h0 = t * t;
+            }
+            hm = h0;
+            u1m = uL - (hm - hL) * std::sqrt((.5 * g) * (1 / hm + 1 / hL));
+            u2m = uR + (hm - hR) * std::sqrt((.5 * g) * (1 / hm + 1 / hR));
+            um = .5 * (u1m + u2m);
+            s1m = u1m - std::sqrt(g * hm);
+            s2m = u2m + std::sqrt(g * hm);
+            rare1 = false;
+            rare2 = false;
+        } else {  // one shock one rarefaction
+            h0 = h_min;
+            for (int iter = 1; iter <= maxiter; ++iter) {
+                F0 = delu + 2.0 * (std::sqrt(g * h0) - std::sqrt(g * h_max)) +
+                     (h0 - h_min) * std::sqrt(.5 * g * (1 / h0 + 1 / h_min));
+                slope = (F_max - F0) / (h_max - h_min);
+                h0 = h0 - F0 / slope;
+            }
+            hm = h0;
+            if (hL > hR) {
+                um = uL + 2.0 * std::sqrt(g * hL) - 2.0 * std::sqrt(g * hm);
+                s1m = uL + 2.0 * std::sqrt(g * hL) - 3.0 * std::sqrt(g * hm);
+                s2m = uL + 2.0 * std::sqrt(g * hL) - std::sqrt(g * hm);
+                rare1 = true;
+                rare2 = false;
+            } else {
+                s2m = uR - 2.0 * std::sqrt(g * hR) + 3.0 * std::sqrt(g * hm);
+                s1m = uR - 2.0 * std::sqrt(g * hR) + std::sqrt(g * hm);
+                um = uR - 2.0 * std::sqrt(g * hR) + 2.0 * std::sqrt(g * hm);
+                rare2 = true;
+                rare1 = false;
+            }
+        }
+    }
+    (void)um;
+}
+
+// geoclaw_riemann_utils.f: riemann_aug_JCP (rarecorrectortest = .false.)
+void riemann_aug_JCP(int maxiter, double hL, double hR, double huL, double huR, double hvL, double hvR,
+                     double bL, double bR, double uL, double uR, double vL, double vR, double phiL,
+                     double phiR, double pL, double pR, double sE1, double sE2, double drytol, double g,
+                     double rho, double sw[3], double fw[3][3]) {
+    (void)hvL; (void)hvR;
+    double r[3][3], lambda[3], del[3], beta[3] = {0, 0, 0};
+    const double delh = hR - hL, delhu = huR - huL, delphi = phiR - phiL, delb = bR - bL, delP = pR - pL;
+    double delnorm = delh * delh + delphi * delphi;
+    double hm, s1m, s2m;
+    bool rare1, rare2;
+    riemanntype(hL, hR, uL, uR, hm, s1m, s2m, rare1, rare2, 1, drytol, g);
+    lambda[0] = std::min(sE1, s2m);
+    lambda[2] = std::max(sE2, s1m);
+    sE1 = lambda[0];
+    sE2 = lambda[2];
+    lambda[1] = 0.0;
+    const double hstarHLL = std::max((huL - huR + sE2 * hR - sE1 * hL) / (sE2 - sE1), 0.0);
+    const bool rarecorrector = false;
+    for (int mw = 0; mw < 3; ++mw) {
+        r[0][mw] = 1.0;
+        r[1][mw] = lambda[mw];
+        r[2][mw] = lambda[mw] * lambda[mw];
+    }
+    if (!rarecorrector) {
+        lambda[1] = 0.5 * (lambda[0] + lambda[2]);
+        r[0][1] = 0.0;
+        r[1][1] = 0.0;
+        r[2][1] = 1.0;
+    }
+    const double criticaltol = std::max(drytol * g, 1e-6);
+    const double criticaltol_2 = std::sqrt(criticaltol);
+    double deldelh = -delb;
+    double deldelphi = -0.5 * (hR + hL) * (g * delb + delP / rho);
+    double hLstar = hL, hRstar = hR, uLstar = uL, uRstar = uR;
+    double huLstar = uLstar * hLstar, huRstar = uRstar * hRstar;
+    const double convergencetol = 1e-6;
+    for (int iter = 1; iter <= maxiter; ++iter) {
+        const double hbar = std::max(0.5 * (hLstar + hRstar), 0.0);
+        const double s1s2bar = 0.25 * ((uLstar + uRstar) * (uLstar + uRstar)) - g * hbar;
+        const double s1s2tilde = std::max(0.0, uLstar * uRstar) - g * hbar;
+        bool sonic = false;
+        if (std::fabs(s1s2bar) <= criticaltol) sonic = true;
+        else if (s1s2bar * s1s2tilde <= criticaltol * criticaltol) sonic = true;
+        else if (s1s2bar * sE1 * sE2 <= criticaltol * criticaltol) sonic = true;
+        else if (std::min(std::fabs(sE1), std::fabs(sE2)) < criticaltol_2) sonic = true;
+        else if (sE1 < criticaltol_2 && s1m > -criticaltol_2) sonic = true;
+        else if (sE2 > -criticaltol_2 && s2m < criticaltol_2) sonic = true;
+        else if ((uL + std::sqrt(g * hL)) * (uR + std::sqrt(g * hR)) < 0.0) sonic = true;
+        else if ((uL - std::sqrt(g * hL)) * (uR - std::sqrt(g * hR)) < 0.0) sonic = true;
+        if (sonic) throw std::runtime_error("geoclaw_riemann_utils : sonic == true (the reference stops)");
+        deldelh = delb * g * hbar / s1s2bar;
+        if (sE1 < -criticaltol && sE2 > criticaltol) {
+            deldelh = std::min(deldelh, hstarHLL * (sE2 - sE1) / sE2);
+            deldelh = std::max(deldelh, hstarHLL * (sE2 - sE1) / sE1);
+        } else if (sE1 >= criticaltol) {
+            deldelh = std::min(deldelh, hstarHLL * (sE2 - sE1) / sE1);
+            deldelh = std::max(deldelh, -hL);
+        } else if (sE2 <= -criticaltol) {
+            deldelh = std::min(deldelh, hR);
+            deldelh = std::max(deldelh, hstarHLL * (sE2 - sE1) / sE2);
+        }
+        deldelh = deldelh - delP / (rho * g);
+        deldelphi = -(delb * g * hbar * s1s2tilde / s1s2bar);
+        deldelphi = std::min(deldelphi, g * std::max(-hLstar * delb, -hRstar * delb));
+        deldelphi = std::max(deldelphi, g * std::min(-hLstar * delb, -hRstar * delb));
+        deldelphi = deldelphi - hbar * delP / rho;
+        del[0] = delh - deldelh;
+        del[1] = delhu;
+        del[2] = delphi - deldelphi;
+        double det1 = r[0][0] * (r[1][1] * r[2][2] - r[1][2] * r[2][1]);
+        double det2 = r[0][1] * (r[1][0] * r[2][2] - r[1][2] * r[2][0]);
+        double det3 = r[0][2] * (r[1][0] * r[2][1] - r[1][1] * r[2][0]);
+        const double determinant = det1 - det2 + det3;
+        for (int k = 0; k < 3; ++k) {
+            double A[3][3];
+            for (int mw = 0; mw < 3; ++mw)
+                for (int m = 0; m < 3; ++m) A[m][mw] = r[m][mw];
+            A[0][k] = del[0];
+            A[1][k] = del[1];
+            A[2][k] = del[2];
+            det1 = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]);
+            det2 = A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]);
+            det3 = A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+            beta[k] = (det1 - det2 + det3) / determinant;
+        }
+        if (std::fabs(del[0] * del[0] + del[2] * del[2] - delnorm) < convergencetol) break;
+        delnorm = del[0] * del[0] + del[2] * del[2];
+        hLstar = hL; hRstar = hR; uLstar = uL; uRstar = uR;
+        huLstar = uLstar * hLstar;
+        huRstar = uRstar * hRstar;
+        for (int mw = 0; mw < 3; ++mw)
+            if (lambda[mw] < 0.0) {
+                hLstar = hLstar + beta[mw] * r[0][mw];
+                huLstar = huLstar + beta[mw] * r[1][mw];
+            }
+        for (int mw = 2; mw >= 0; --mw)
+            if (lambda[mw] > 0.0) {
+                hRstar = hRstar - beta[mw] * r[0][mw];
+                huRstar = huRstar - beta[mw] * r[1][mw];
+            }
+        if (hLstar > drytol) uLstar = huLstar / hLstar;
+        else { hLstar = std::max(hLstar, 0.0); uLstar = 0.0; }
+        if (hRstar > drytol) uRstar = huRstar / hRstar;
+        else { hRstar = std::max(hRstar, 0.0); uRstar = 0.0; }
+    }
+    for (int mw = 0; mw < 3; ++mw) {
+        sw[mw] = lambda[mw];
+        fw[0][mw] = beta[mw] * r[1][mw];
+        fw[1][mw] = beta[mw] * r[2][mw];
+        fw[2][mw] = beta[mw] * r[1][mw];
+    }
+    fw[2][0] = fw[2][0] * vL;
+    fw[2][2] = fw[2][2] * vR;
+    fw[2][1] = 0.0;
+    const double hustar_interface = huL + fw[0][0];
+    if (hustar_interface <= 0.0) fw[2][0] = fw[2][0] + (hR * uR * vR - hL * uL * vL - fw[2][0] - fw[2][2]);
+    else fw[2][2] = fw[2][2] + (hR * uR * vR - hL * uL * vL - fw[2][0] - fw[2][2]);
+}
+
+// rpn2_geoclaw.f90 (clawpack46 layout), use_simple = .false.
+void rpn2_geoclaw(const Slice& S, double grav, double drytol, int ixy, int meqn, int mwaves, int mx,
+                  const double* q, const double* aux2, double* wave, double* s, double* amdq, double* apdq) {
+    const int L = S.L, mbc = S.mbc;
+    const int mu = (ixy == 1) ? 1 : 2;
+    const int mv = (ixy == 1) ? 2 : 1;
+    auto Q = [&](int i, int m) { return q[m * L + S.at(i)]; };
+    auto FW = [&](int i, int m, int mw) -> double& { return wave[(mw * meqn + m) * L + S.at(i)]; };
+    const double g = grav, rho = -9999999.0, pL = 0, pR = 0;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        if (Q(i - 1, 0) < 0.0 || Q(i, 0) < 0.0) throw std::runtime_error("rpn2_geoclaw: negative input depth");
+        for (int mw = 0; mw < mwaves; ++mw) {
+            s[mw * L + S.at(i)] = 0.0;
+            FW(i, 0, mw) = 0.0; FW(i, 1, mw) = 0.0; FW(i, 2, mw) = 0;
+        }
+        if (Q(i - 1, 0) <= drytol && Q(i, 0) <= drytol) continue;
+        double hL = Q(i - 1, 0), hR = Q(i, 0), huL = Q(i - 1, mu), huR = Q(i, mu);
+        double bL = aux2[0 * L + S.at(i - 1)], bR = aux2[0 * L + S.at(i)];
+        double hvL = Q(i - 1, mv), hvR = Q(i, mv);
+        double uR, vR, phiR, uL, vL, phiL;
+        if (hR > drytol) {
+            uR = huR / hR; vR = hvR / hR;
+            phiR = 0.5 * grav * (hR * hR) + (huR * huR) / hR;
+        } else {
+            hR = 0.0; huR = 0.0; hvR = 0.0; uR = 0.0; vR = 0; phiR = 0.0;
+        }
+        if (hL > drytol) {
+            uL = huL / hL; vL = hvL / hL;
+            phiL = 0.5 * grav * (hL * hL) + (huL * huL) / hL;
+        } else {
+            hL = 0.0; huL = 0.0; hvL = 0.0; uL = 0.0; vL = 0.0; phiL = 0.0;
+        }
+        double wall[3] = {1.0, 1.0, 1.0};
+        double hstar, s1m, s2m;
+        bool rare1, rare2;
+        if (hR <= drytol) {
+            riemanntype(hL, hL, uL, -uL, hstar, s1m, s2m, rare1, rare2, 1, drytol, grav);
+            const double hstartest = std::max(hL, hstar);
+            if (hstartest + bL < bR) {
+                wall[1] = 0.0; wall[2] = 0.0;
+                hR = hL; huR = -huL; bR = bL; phiR = phiL; uR = -uL; vL = vR;
+            } else if (hL + bL < bR) {
+                bR = hL + bL;
+            }
+        } else if (hL <= drytol) {
+            riemanntype(hR, hR, -uR, uR, hstar, s1m, s2m, rare1, rare2, 1, drytol, grav);
+            const double hstartest = std::max(hR, hstar);
+            if (hstartest + bR < bL) {
+                wall[0] = 0.0; wall[1] = 0.0;
+                hL = hR; huL = -huR; bL = bR; phiL = phiR; uL = -uR; vR = vL;
+            } else if (hR + bR < bL) {
+                bL = hR + bR;
+            }
+        }
+        const double sL = uL - std::sqrt(grav * hL);
+        const double sR = uR + std::sqrt(grav * hR);
+        const double uhat = (std::sqrt(grav * hL) * uL + std::sqrt(grav * hR) * uR) /
+                            (std::sqrt(grav * hR) + std::sqrt(grav * hL));
+        const double chat = std::sqrt(grav * 0.5 * (hR + hL));
+        const double sRoe1 = uhat - chat, sRoe2 = uhat + chat;
+        const double sE1 = std::min(sL, sRoe1), sE2 = std::max(sR, sRoe2);
+        double sw[3], fw[3][3];
+        riemann_aug_JCP(1, hL, hR, huL, huR, hvL, hvR, bL, bR, uL, uR, vL, vR, phiL, phiR, pL, pR, sE1, sE2,
+                        drytol, g, rho, sw, fw);
+        for (int mw = 0; mw < mwaves; ++mw) {
+            sw[mw] = sw[mw] * wall[mw];
+            fw[0][mw] = fw[0][mw] * wall[mw];
+            fw[1][mw] = fw[1][mw] * wall[mw];
+            fw[2][mw] = fw[2][mw] * wall[mw];
+        }
+        for (int mw = 0; mw < mwaves; ++mw) {
+            s[mw * L + S.at(i)] = sw[mw];
+            FW(i, 0, mw) = fw[0][mw];
+            FW(i, mu, mw) = fw[1][mw];
+            FW(i, mv, mw) = fw[2][mw];
+        }
+    }
+    for (int i = 2 - mbc; i <= mx + mbc; ++i)
+        for (int m = 0; m < 3; ++m) {
+            amdq[m * L + S.at(i)] = 0.0;
+            apdq[m * L + S.at(i)] = 0.0;
+        }
+    for (int i = 2 - mbc; i <= mx + mbc; ++i)
+        for (int mw = 0; mw < 3; ++mw) {
+            const double sv = s[mw * L + S.at(i)];
+            for (int m = 0; m < 3; ++m) {
+                double& am = amdq[m * L + S.at(i)];
+                double& ap = apdq[m * L + S.at(i)];
+                if (sv < 0.0) am = am + FW(i, m, mw);
+                else if (sv > 0.0) ap = ap + FW(i, m, mw);
+                else {
+                    am = am + 0.5 * FW(i, m, mw);
+                    ap = ap + 0.5 * FW(i, m, mw);
+                }
+            }
+        }
+}
+
 // applications/clawpack/advection/2d/all/clawpack46_rpn2adv.f:1-61
 void rpn2_adv(const Slice& S, int ixy, int meqn, int mwaves, int mx, const double* q,
               const double* auxl, double* wave, double* s, double* amdq, double* apdq) {
@@ -400,6 +696,10 @@ void call_rpn2(const SolverParams& sp, Work& w, int ixy, int mx) {
             rpn2_euler4(w.S, w.R, sp.gamma, sp.gamma1, ixy, w.meqn, w.mwaves, mx, w.q1d.data(),
                         w.wave.data(), w.s.data(), w.amdq.data(), w.apdq.data());
             break;
+        case SOLVER_GEOCLAW_FWAVE:
+            rpn2_geoclaw(w.S, sp.grav, sp.drytol, ixy, w.meqn, w.mwaves, mx, w.q1d.data(), w.aux2.data(),
+                         w.wave.data(), w.s.data(), w.amdq.data(), w.apdq.data());
+            break;
         default: throw std::runtime_error("unknown solver kind");
     }
 }
@@ -428,8 +728,12 @@ double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, i
     const Slice& S = w.S;
     const int L = S.L, mbc = S.mbc, meqn = w.meqn, mwaves = w.mwaves;
     const bool v5 = mp.version == 5;
-    const int god_lo = v5 ? 1 : 2 - mbc, god_hi = v5 ? mx + 1 : mx + mbc - 1;  // Godunov, amdq += cqxx
-    const int cq_lo = v5 ? 1 : 2 - mbc, cq_hi = v5 ? mx + 1 : mx + mbc;          // cqxx, gadd updates
+    // f-waves: clawpack46_flux2fw.f (Godunov and cqxx over i = 1..mx+1, cqxx
+    // weighted by sign(s); the reference's rpt2_geoclaw stops, so no transverse part)
+    const bool fw = sp.kind == SOLVER_GEOCLAW_FWAVE;
+    if (fw && mp.order1 > 0) throw std::runtime_error("rpt2_geoclaw stops in the reference: use order (2, 0)");
+    const int god_lo = (v5 || fw) ? 1 : 2 - mbc, god_hi = (v5 || fw) ? mx + 1 : mx + mbc - 1;  // Godunov
+    const int cq_lo = (v5 || fw) ? 1 : 2 - mbc, cq_hi = (v5 || fw) ? mx + 1 : mx + mbc;          // cqxx
     bool limit = false;
     for (int mw = 0; mw < mwaves; ++mw)
         if (mp.mthlim[mw] > 0) limit = true;
@@ -462,8 +766,10 @@ double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, i
                 const int k = m * L + S.at(i);
                 w.cqxx[k] = 0.0;
                 for (int mw = 0; mw < mwaves; ++mw) {
-                    const double as = std::fabs(w.s[mw * L + S.at(i)]);
-                    w.cqxx[k] = w.cqxx[k] + as * (1.0 - as * dtdxave) *
+                    const double sv = w.s[mw * L + S.at(i)];
+                    const double as = std::fabs(sv);
+                    const double abs_sign = fw ? fsign(1.0, sv) : as;
+                    w.cqxx[k] = w.cqxx[k] + abs_sign * (1.0 - as * dtdxave) *
                                                 w.wave[(mw * meqn + m) * L + S.at(i)];
                 }
                 w.faddm[k] = w.faddm[k] + 0.5 * w.cqxx[k];
@@ -604,6 +910,31 @@ double step2(const SolverParams& sp, const MethodParams& mp, int mx, int my, int
                     q[P(i, j, m)] = q[P(i, j, m)] - (dtdx * df + dtdy * dg) / aux[P(i, j, mp.mcapa - 1)];
             }
     return cflgrid;
+}
+
+void setaux_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double* aux) {
+    const PatchIdx P(mx, my, mbc);
+    for (int j = 1 - mbc; j <= my + mbc; ++j)
+        for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+            const double xc = xlower + (i - 0.5) * dx, yc = ylower + (j - 0.5) * dy;
+            aux[P(i, j, 0)] = -1.0 + 0.8 * std::exp(-((xc - 0.5) * (xc - 0.5) + (yc - 0.5) * (yc - 0.5)) / 0.02);
+        }
+}
+
+void qinit_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, const double* p,
+                 double* q) {
+    const PatchIdx P(mx, my, mbc);
+    std::vector<double> b((size_t)P.size(1));
+    setaux_bathy(mx, my, mbc, xlower, ylower, dx, dy, b.data());
+    for (int j = 1 - mbc; j <= my + mbc; ++j)
+        for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+            const double xc = xlower + (i - 0.5) * dx, yc = ylower + (j - 0.5) * dy;
+            const double r2 = (xc - p[0]) * (xc - p[0]) + (yc - p[1]) * (yc - p[1]);
+            const double eta = p[2] * std::exp(-r2 / (p[3] * p[3]));
+            q[P(i, j, 0)] = std::max(0.0, eta - b[P(i, j, 0)]);
+            q[P(i, j, 1)] = 0.0;
+            q[P(i, j, 2)] = 0.0;
+        }
 }
 
 void b4step2_swirl(int mx, int my, int mbc, int maux, double xlower, double ylower, double dx,

@@ -19,6 +19,7 @@ enum SolverKind {
     SOLVER_ADVECTION = 0,   // clawpack46_rpn2adv / rpt2adv (swirl aux velocities)
     SOLVER_SWE_ROE = 1,     // shallow/2d/rp/clawpack46_rpn2.f / rpt2.f
     SOLVER_EULER4_ROE = 2,  // euler/2d/rp/clawpack46_rpn2_euler4.f / rpt2_euler4.f
+    SOLVER_GEOCLAW_FWAVE = 3,  // shallow/2d/rp/rpn2_geoclaw.f90 (f-waves, clawpack46_flux2fw.f)
 };
 
 struct SolverParams {
@@ -26,6 +27,7 @@ struct SolverParams {
     double grav = 1.0;      // /cparam/ grav (SWE)
     double gamma = 1.4;     // /cparam/ gamma (Euler)
     double gamma1 = 0.4;    // /cparam/ gamma1 = gamma - 1
+    double drytol = 1e-3;   // /common_swe/ dry_tolerance (GeoClaw)
 };
 
 struct MethodParams {
@@ -60,6 +62,14 @@ inline double dmin(double a, double b) { return a < b ? a : b; }
 double step2(const SolverParams& sp, const MethodParams& mp,
              int mx, int my, int mbc, int meqn, int maux,
              double* q, const double* aux, double dx, double dy, double dt);
+
+// Shallow water over bathymetry: b(x,y) = -1 + 0.8 exp(-((x-.5)^2 + (y-.5)^2)/0.02)
+// at cell centres (aux(i,j,1), ghost cells included), and a surface
+// eta = amp exp(-((x-x0)^2 + (y-y0)^2)/width^2) on a lake at rest: h = max(0, eta - b),
+// hu = hv = 0.  p = {x0, y0, amp, width}.
+void setaux_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double* aux);
+void qinit_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, const double* p,
+                 double* q);
 
 // swirl/user_4.6/b4step2.f (+ swirl/psi.f): time-dependent edge velocities.
 void b4step2_swirl(int mx, int my, int mbc, int maux, double xlower, double ylower,

@@ -23,6 +23,7 @@ def to_options(cfg: O.Config):
         tfinal=cfg.tfinal, initial_dt=cfg.initial_dt, max_cfl=cfg.max_cfl,
         desired_cfl=cfg.desired_cfl, solver_kind=cfg.solver, problem=cfg.problem,
         grav=cfg.grav, gamma=cfg.gamma, problem_params=cfg.pparams, claw_version=cfg.claw_version,
+        dry_tolerance=cfg.drytol,
     )
 
 
@@ -71,3 +72,22 @@ def radialdam_amr(seed=0, minlevel=3, maxlevel=6, mx=32, tfinal=0.5) -> O.Config
 
 def replace(cfg, **kw):
     return dataclasses.replace(cfg, **kw)
+
+
+def bathy_lake(level=3, mx=16, seed=0, amp=1e-3, width=0.05, minlevel=None, maxlevel=None) -> O.Config:
+    """Shallow water over a Gaussian bump, b = -1 + 0.8 exp(-r^2/0.02) about
+    (0.5, 0.5): a lake at rest (eta = 0, h = -b >= 0.2) plus a surface pulse of
+    amplitude `amp` and width `width` at a seeded place.  GeoClaw f-wave solver
+    (rpn2_geoclaw + clawpack46_flux2fw), order (2, 0) since the reference's
+    rpt2_geoclaw stops; g = 1, dry tolerance 1e-3, extrapolation boundaries."""
+    rng = np.random.default_rng(seed)
+    x0, y0 = rng.uniform(0.25, 0.75, size=2)
+    lo = level if minlevel is None else minlevel
+    hi = level if maxlevel is None else maxlevel
+    return O.Config(mx=mx, my=mx, mbc=2, meqn=3, maux=1, order=(2, 0), mwaves=3, mthlim=(4, 4, 4),
+                    mthbc=(1, 1, 1, 1), minlevel=lo, maxlevel=hi, subcycle=1,
+                    regrid_interval=0 if lo == hi else 1, smooth_refine=1, criteria=O.GRADIENT,
+                    refine_threshold=5e-3, coarsen_threshold=1e-3, use_fixed_dt=1,
+                    solver=O.GEOCLAW_FWAVE, problem=O.BATHY, grav=1.0,
+                    pparams=(float(x0), float(y0), amp, width))
+

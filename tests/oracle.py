@@ -18,9 +18,9 @@ ROOT = Path(__file__).resolve().parents[1]
 ORACLE_DIR = ROOT / "oracle"
 
 # Solver kinds (oracle/oracle_patch.hpp SolverKind)
-ADVECTION, SWE_ROE, EULER4_ROE = 0, 1, 2
+ADVECTION, SWE_ROE, EULER4_ROE, GEOCLAW_FWAVE = 0, 1, 2, 3
 # Problems (oracle/oracle_amr.hpp Problem)
-SWIRL, RADIALDAM, QUADRANTS = 0, 1, 2
+SWIRL, RADIALDAM, QUADRANTS, BATHY = 0, 1, 2, 3
 # Tagging criteria (oracle/oracle_clawpatch.hpp TagCriteria)
 VALUE, MINMAX, DIFFERENCE, GRADIENT = 0, 1, 2, 3
 
@@ -30,7 +30,7 @@ _I_FIELDS = (["mx", "my", "mbc", "meqn", "maux", "order0", "order1", "mcapa", "m
                 "smooth_level", "criteria", "ivar", "use_fixed_dt", "nout", "init_ghostcell",
                 "reduce_cfl", "solver", "problem", "claw_version"])
 _D_FIELDS = (["refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
-              "desired_cfl", "grav", "gamma", "gamma1"] + [f"p{k}" for k in range(32)])
+              "desired_cfl", "grav", "gamma", "gamma1", "drytol"] + [f"p{k}" for k in range(32)])
 
 
 @dataclass
@@ -70,6 +70,7 @@ class Config:
     gamma: float = 1.4
     pparams: tuple = field(default_factory=tuple)
     claw_version: int = 4   # 4: fc2d_clawpack46, 5: fc2d_clawpack5
+    drytol: float = 1e-3    # GeoClaw dry tolerance
 
     @property
     def gamma1(self) -> float:
@@ -95,7 +96,7 @@ class Config:
             "refine_threshold": self.refine_threshold, "coarsen_threshold": self.coarsen_threshold,
             "tfinal": self.tfinal, "initial_dt": self.initial_dt, "max_cfl": self.max_cfl,
             "desired_cfl": self.desired_cfl, "grav": self.grav, "gamma": self.gamma,
-            "gamma1": self.gamma1,
+            "gamma1": self.gamma1, "drytol": self.drytol,
         }
         for k in range(32):
             dv[f"p{k}"] = float(self.pparams[k]) if k < len(self.pparams) else 0.0

@@ -112,3 +112,28 @@ def test_claw5_interior_mass_conservation():
     for k in range(10):
         s.advance(k * 0.002, 0.002)
     assert abs(s.conservation()[0] - m0) <= 1e-13 * m0
+
+
+def test_geoclaw_lake_at_rest_oracle():
+    """rpn2_geoclaw's steady-state wave keeps a lake at rest over the bump to
+    round-off on patches the boundary extrapolation has not reached."""
+    cfg = cases.bathy_lake(level=3, mx=8, amp=0.0)
+    s = O.OracleSolver(cfg)
+    s.initialize()
+    q0 = s.all_q()
+    dt = 0.5 / (8 * 8)
+    for k in range(6):
+        s.advance(k * dt, dt)
+    central = [k for k, (lv, x, y) in enumerate(s.leaves())
+               if 2 <= x >> 25 <= 5 and 2 <= y >> 25 <= 5]
+    assert len(central) == 16
+    dq = np.abs(s.all_q() - q0)[central][:, :, 2:-2, 2:-2]
+    assert float(dq.max()) <= 1e-14
+
+
+def test_geoclaw_rejects_transverse_order():
+    cfg = cases.replace(cases.bathy_lake(level=1, mx=8), order=(2, 2))
+    s = O.OracleSolver(cfg)
+    with pytest.raises(Exception):
+        s.initialize()
+        s.advance(0.0, 0.001)
