@@ -40,6 +40,8 @@ EXPORTED_SYMBOLS = (
     "fcb_patch_neighbors", "fcb_patch_size", "fcb_physical_set_bc", "fcb_regrid", "fcb_run",
     "fcb_set_q", "fcb_single_step_update", "fcb_synchronize", "fcb_timeinterp",
     "fcb_update_single_step", "fcb_update_single_step_async", "fcb_conservation_sum_noalloc",
+    "fcb_server_create", "fcb_server_destroy", "fcb_server_submit", "fcb_server_round", "fcb_server_status",
+    "fcb_server_get_q", "fcb_server_release", "fcb_server_clock",
 )
 
 
@@ -67,6 +69,13 @@ class _Options(ctypes.Structure):
         ("claw_version", ctypes.c_int),
         ("dry_tolerance", ctypes.c_double),
     ]
+
+
+class RequestStatus(ctypes.Structure):
+    """Mirror of fcb_request_status_t."""
+    _fields_ = [("state", ctypes.c_int), ("num_patches", ctypes.c_int), ("t", ctypes.c_double),
+                ("submit_s", ctypes.c_double), ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double),
+                ("cell_updates", ctypes.c_longlong), ("count_amr_advance", ctypes.c_longlong)]
 
 
 class _Counters(ctypes.Structure):
@@ -201,6 +210,15 @@ def lib():
     L.fcb_curr_time.argtypes = [vp, dp]
     L.fcb_conservation_sum_noalloc.argtypes = [vp, sz, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, vp, vp, vp]
+    ll = ctypes.POINTER(ctypes.c_longlong)
+    L.fcb_server_create.argtypes = [sz, vp, ctypes.POINTER(vp)]
+    L.fcb_server_destroy.argtypes = [vp]
+    L.fcb_server_submit.argtypes = [vp, ctypes.POINTER(_Options), ip]
+    L.fcb_server_round.argtypes = [vp, ip, ip]
+    L.fcb_server_status.argtypes = [vp, ctypes.c_int, ctypes.POINTER(RequestStatus)]
+    L.fcb_server_get_q.argtypes = [vp, ctypes.c_int, dp, sz]
+    L.fcb_server_release.argtypes = [vp, ctypes.c_int]
+    L.fcb_server_clock.argtypes = [vp, dp, ll, ll]
     _lib = L
     return L
 

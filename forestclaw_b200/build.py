@@ -34,10 +34,11 @@ SOURCES = {
     "fcb_ghost.cu": ["-fmad=false"],
     "fcb_amr.cu": ["-fmad=false"],
     "fcb_runtime.cu": [],
+    "fcb_serve.cu": [],
     "fcb_capi.cu": ["-Xcompiler", "-fvisibility=default"],
     "fcb_noalloc.cu": ["-fmad=false"],
 }
-HEADERS = ["fcb_device.h", "fcb_solvers.cuh", "fcb_step_pipe.cuh", "fcb_forest.hpp", "fcb_runtime.hpp"]
+HEADERS = ["fcb_device.h", "fcb_solvers.cuh", "fcb_step_pipe.cuh", "fcb_forest.hpp", "fcb_runtime.hpp", "fcb_serve.hpp"]
 
 
 def _stale(target: Path, deps) -> bool:

@@ -6,6 +6,11 @@
 #include <string>
 
 #include "fcb_runtime.hpp"
+#include "fcb_serve.hpp"
+
+struct fcb_server {
+    fcb::Server* impl;
+};
 
 struct fcb_context {
     fcb::Context* impl;
@@ -204,5 +209,81 @@ int fcb_curr_time(fcb_context_t* ctx, double* t) {
 }
 
 int fcb_synchronize(fcb_context_t* ctx) { return guard([&] { CTX(); C.synchronize(); }); }
+
+// ---- serving ----
+int fcb_server_create(size_t budget_bytes, void* cuda_stream, fcb_server_t** out) {
+    return guard([&] {
+        need(out, "out");
+        *out = nullptr;
+        auto* sv = new fcb_server{nullptr};
+        try {
+            sv->impl = new fcb::Server(budget_bytes, (cudaStream_t)cuda_stream);
+        } catch (...) {
+            delete sv;
+            throw;
+        }
+        *out = sv;
+    });
+}
+int fcb_server_destroy(fcb_server_t* s) {
+    return guard([&] {
+        if (!s) return;
+        delete s->impl;
+        delete s;
+    });
+}
+int fcb_server_submit(fcb_server_t* s, const fcb_options_t* opt, int* id) {
+    return guard([&] {
+        need(s, "server");
+        need(opt, "opt");
+        need(id, "id");
+        *id = s->impl->submit(*opt);
+    });
+}
+int fcb_server_round(fcb_server_t* s, int* active, int* queued) {
+    return guard([&] {
+        need(s, "server");
+        const int a = s->impl->round();
+        if (active) *active = a;
+        if (queued) *queued = s->impl->queued();
+    });
+}
+int fcb_server_status(fcb_server_t* s, int id, fcb_request_status_t* out) {
+    return guard([&] {
+        need(s, "server");
+        need(out, "out");
+        const fcb::Request& r = s->impl->request(id);
+        out->state = r.state;
+        out->num_patches = r.ctx ? r.ctx->num_patches() : 0;
+        out->t = r.t;
+        out->submit_s = r.t_submit;
+        out->start_s = r.t_start;
+        out->finish_s = r.t_finish;
+        out->cell_updates = r.cell_updates;
+        out->count_amr_advance = r.ctx ? r.ctx->counters().count_amr_advance : 0;
+        if (r.state == FCB_REQ_FAILED) fcb::set_last_error(r.error);
+    });
+}
+int fcb_server_get_q(fcb_server_t* s, int id, double* host, size_t n) {
+    return guard([&] {
+        need(s, "server");
+        need(host, "host");
+        s->impl->get_q(id, host, n);
+    });
+}
+int fcb_server_release(fcb_server_t* s, int id) {
+    return guard([&] {
+        need(s, "server");
+        s->impl->release(id);
+    });
+}
+int fcb_server_clock(fcb_server_t* s, double* now, long long* rounds, long long* launches) {
+    return guard([&] {
+        need(s, "server");
+        if (now) *now = s->impl->now();
+        if (rounds) *rounds = s->impl->rounds();
+        if (launches) *launches = s->impl->launches();
+    });
+}
 
 }  // extern "C"

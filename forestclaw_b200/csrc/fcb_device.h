@@ -16,6 +16,18 @@ enum : int32_t { PATCH_SAVE_LAST = 1 };
 enum SolverKind : int32_t { SOLVER_ADVECTION = 0, SOLVER_SWE_ROE = 1, SOLVER_EULER4_ROE = 2, SOLVER_GEOCLAW_FWAVE = 3 };
 enum AuxKind : int32_t { AUX_NONE = 0, AUX_SWIRL = 1, AUX_STORED = 2 };
 
+// One patch of a launch that mixes patches of several solves (ensemble
+// serving): its arrays, geometry and time step travel with it.
+struct PatchDesc {
+    double* q;            // the patch's q (qlast at the same offset in its qlast arena)
+    double* qlast;
+    const double* aux;    // stored aux of the patch, or null
+    PatchMeta meta;
+    double dt, vt;        // step and swirl velocity scale of the patch's solve
+    int32_t req;          // CFL slot: cfl_out[req]
+    int32_t pad;
+};
+
 // Arguments of one batched step launch (all patches of one level).
 struct StepArgs {
     double* q;             // arena base
@@ -32,6 +44,7 @@ struct StepArgs {
     double dt;
     double vt;             // swirl: cos(2 pi (t + dt/2) / tperiod)
     const double* dyn;     // non-null: {dt, vt} read from device memory (one macro-step graph serves every step)
+    const PatchDesc* desc; // non-null: per-patch arrays, geometry and dt (slots, meta, q, dt unused)
     double grav, gamma, gamma1;
     double drytol;         // GeoClaw dry tolerance
     unsigned long long* cfl_out;  // atomicMax on the bits of a non-negative double

@@ -31,6 +31,9 @@ void DevBuf<T>::release() {
 }
 template struct DevBuf<int32_t>;
 template struct DevBuf<GhostOp>;
+template struct DevBuf<unsigned long long>;
+template struct DevBuf<PatchDesc>;
+template struct DevBuf<double>;
 
 void Context::check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw Error(FCB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -209,6 +212,7 @@ void Context::mesh_changed() {
         hm[slot_of_[p]] = m;
     }
     check(cudaMemcpy(d_meta_, hm.data(), (size_t)capacity_ * sizeof(PatchMeta), cudaMemcpyHostToDevice), "meta upload");
+    h_meta_ = hm;
     // level lists in Morton order
     const int L = QuadForest::kMaxLevel + 2;
     level_begin_.assign(L + 1, 0);
@@ -808,6 +812,79 @@ double Context::advance_all_levels(double t_curr, double dt) {
     use_dyn_ = false;
     ++cnt_.count_amr_advance;
     return read_cfl(d_cfl_);
+}
+
+// ---------------------------------------------------------------------------
+// Batched serving support
+// ---------------------------------------------------------------------------
+// Non-subcycled fclaw2d_advance_all_levels (src/fclaw2d_advance.c:300-324): each
+// of the 2^(maxlevel-minlevel) fine steps updates every level with the fine dt
+// and is followed by a ghost fill over all levels, so a fine step is one batch
+// of all leaves.
+void Context::step_descs(double t, double dt, int req, std::vector<PatchDesc>& out) {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "step before initialize");
+    double vt = 0.0;
+    if (aux_kind_ == AUX_SWIRL) {
+        const double pi = 4.0 * std::atan(1.0);
+        const double tperiod = opt_.problem_params[0];
+        vt = (tperiod == 0.0) ? 0.0 : std::cos(2.0 * pi * (t + dt / 2.0) / tperiod);
+    }
+    const int n = num_patches();
+    for (int p = 0; p < n; ++p) {
+        const int slot = slot_of_[p];
+        PatchDesc d{};
+        d.q = d_q_ + (int64_t)slot * stride_;
+        d.qlast = d_qlast_ + (int64_t)slot * stride_;
+        d.aux = aux_kind_ == AUX_STORED ? d_aux_ + (int64_t)slot * aux_stride_ : nullptr;
+        d.meta = h_meta_[slot];
+        d.dt = dt;
+        d.vt = vt;
+        d.req = req;
+        out.push_back(d);
+    }
+    cnt_.count_single_step += n;
+}
+
+void Context::after_fine_step(double t) { ghost_update(forest_.min_level(), forest_.max_level(), t, 0); }
+
+// fclaw2d_clawpatch_save_step / restore_step: the CFL-retry copy
+void Context::save_step() {
+    if (!d_qsave_) return;
+    check(cudaMemcpyAsync(d_qsave_, d_q_, (size_t)capacity_ * stride_ * sizeof(double), cudaMemcpyDeviceToDevice, st_),
+          "save_time_step");
+}
+void Context::restore_step() {
+    if (!d_qsave_) return;
+    check(cudaMemcpyAsync(d_q_, d_qsave_, (size_t)capacity_ * stride_ * sizeof(double), cudaMemcpyDeviceToDevice, st_),
+          "restore_time_step");
+}
+
+size_t Context::device_bytes() const {
+    const int arenas = 3 + (d_qsave_ ? 1 : 0);
+    return (size_t)capacity_ * ((size_t)stride_ * arenas + (size_t)aux_stride_) * sizeof(double) +
+           (size_t)capacity_ * sizeof(PatchMeta) + h_ops_.size() * sizeof(GhostOp);
+}
+
+cudaError_t launch_step_batch(const fcb_options_t& opt, int aux_kind, const PatchDesc* d_desc, int n,
+                              unsigned long long* d_cfl, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    StepArgs a{};
+    a.desc = d_desc;
+    a.npatches = n;
+    a.maux = aux_kind == AUX_STORED ? opt.maux : 0;
+    a.order0 = opt.order[0];
+    a.order1 = opt.order[1];
+    for (int k = 0; k < 8; ++k) a.mthlim[k] = opt.mthlim[k];
+    a.grav = opt.grav;
+    a.gamma = opt.gamma;
+    a.gamma1 = opt.gamma - 1.0;
+    a.drytol = opt.dry_tolerance;
+    a.cfl_out = d_cfl;
+    return opt.precision == 1
+               ? launch_step_pipe_mixed(opt.solver_kind, aux_kind, opt.mwaves, opt.mx, opt.my, opt.mbc,
+                                        opt.claw_version, a, st)
+               : launch_step_pipe(opt.solver_kind, aux_kind, opt.mwaves, opt.mx, opt.my, opt.mbc, opt.claw_version,
+                                  a, st);
 }
 
 // ---------------------------------------------------------------------------

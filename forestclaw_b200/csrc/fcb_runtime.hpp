@@ -21,6 +21,11 @@ struct Error : std::runtime_error {
     Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+// One step launch over patches of several solves (identical options apart from
+// the initial data, t_final and refinement depth): the pipelined form, FP64 or mixed.
+cudaError_t launch_step_batch(const fcb_options_t& opt, int aux_kind, const PatchDesc* d_desc, int n,
+                              unsigned long long* d_cfl, cudaStream_t st);
+
 // Kernel launchers (fcb_step.cu, fcb_ghost.cu, fcb_amr.cu)
 cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
                         cudaStream_t st);
@@ -92,6 +97,19 @@ class Context {
     void synchronize();
     fcb_counters_t counters() const { return cnt_; }
     double curr_time() const { return curr_time_; }
+    const fcb_options_t& options() const { return opt_; }
+    int aux_kind() const { return aux_kind_; }
+
+    // --- pieces of a non-subcycled macro step, for launches that batch several
+    // solves (serving): the patch descriptors of one fine step (every leaf, step
+    // dt), the ghost fill that follows it, and the CFL-retry copy of q ---
+    void step_descs(double t, double dt, int req, std::vector<PatchDesc>& out);
+    void after_fine_step(double t);
+    void save_step();
+    void restore_step();
+    void set_curr_time(double t) { curr_time_ = t; }
+    void count_advance() { ++cnt_.count_amr_advance; }
+    size_t device_bytes() const;
 
   private:
     // --- setup ---
@@ -136,6 +154,7 @@ class Context {
     double* d_aux_ = nullptr;         // stored aux (bathymetry), recomputed after every mesh change
     int64_t aux_stride_ = 0;
     PatchMeta* d_meta_ = nullptr;
+    std::vector<PatchMeta> h_meta_;  // host copy of the slot metadata
     // level lists (device), grouped by level
     DevBuf<int32_t> d_level_slots_;
     std::vector<int> level_begin_;    // size maxlevel+2

@@ -1,0 +1,251 @@
+// Ensemble serving loop (see fcb_serve.hpp).
+#include "fcb_serve.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <tuple>
+
+namespace fcb {
+
+namespace {
+
+// Options that must agree for two solves to share a step launch.
+auto launch_key(const fcb_options_t& o) {
+    return std::make_tuple(o.solver_kind, o.problem, o.mx, o.my, o.mbc, o.meqn, o.maux, o.mwaves, o.order[0],
+                           o.order[1], std::vector<int>(o.mthlim, o.mthlim + 8), o.precision, o.claw_version,
+                           o.grav, o.gamma, o.dry_tolerance);
+}
+
+}  // namespace
+
+Server::Server(size_t budget_bytes, cudaStream_t st) : budget_(budget_bytes), st_(st) {
+    t0_ = std::chrono::steady_clock::now();
+}
+
+Server::~Server() {
+    cudaStreamSynchronize(st_);
+    reqs_.clear();
+    cudaFreeHost(h_cfl_);
+    cudaFreeHost(h_desc_pinned_);
+}
+
+void Server::check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Error(FCB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+double Server::now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+}
+
+int Server::submit(const fcb_options_t& opt) {
+    if (opt.subcycle) throw Error(FCB_ERR_INVALID, "served solves use non-subcycled time stepping (subcycle = 0)");
+    if (opt.step_variant == 1 || opt.step_variant == 2)
+        throw Error(FCB_ERR_INVALID, "served solves use the pipelined step form");
+    if (opt.nout != 1) throw Error(FCB_ERR_INVALID, "served solves run to tfinal in one output interval (nout = 1)");
+    Request r;
+    r.id = next_id_++;
+    r.opt = opt;
+    r.t_submit = now();
+    reqs_.emplace(r.id, std::move(r));
+    queue_.push_back(r.id);
+    return r.id;
+}
+
+const Request& Server::request(int id) const {
+    auto it = reqs_.find(id);
+    if (it == reqs_.end()) throw Error(FCB_ERR_INVALID, "unknown request");
+    return it->second;
+}
+
+// Admit queued requests in arrival order while their device memory fits.
+void Server::admit() {
+    while (!queue_.empty()) {
+        Request& r = reqs_.at(queue_.front());
+        if (!active_.empty() && r.bytes > 0 && used_ + r.bytes > budget_) return;  // known size, no room yet
+        try {
+            r.ctx = std::make_unique<Context>(r.opt, st_);
+            r.ctx->initialize();
+        } catch (const Error& e) {
+            r.ctx.reset();
+            r.state = REQ_FAILED;
+            r.error = e.what();
+            r.t_finish = now();
+            queue_.pop_front();
+            continue;
+        }
+        r.bytes = r.ctx->device_bytes();
+        if (!active_.empty() && used_ + r.bytes > budget_) {  // first sight of its size: wait for room
+            r.ctx.reset();
+            return;
+        }
+        used_ += r.bytes;
+        r.state = REQ_ACTIVE;
+        r.t_start = now();
+        r.t = 0.0;
+        r.dt_min = r.opt.initial_dt;
+        r.n_inner = 0;
+        begin_macro(r);
+        active_.push_back(r.id);
+        queue_.pop_front();
+    }
+}
+
+// fclaw2d_run (src/fclaw2d_run.c, outstyle 1) up to the advance.
+void Server::begin_macro(Request& r) {
+    const fcb_options_t& o = r.opt;
+    if (!o.use_fixed_dt) r.ctx->save_step();
+    r.dt_step = r.dt_min;
+    r.took_small = 0;
+    if (!o.use_fixed_dt) {
+        const double tol = 1e-2 * r.dt_step;
+        const double small_step = o.tfinal - (r.t + r.dt_step);
+        if (small_step < tol) {
+            r.dt_step = o.tfinal - r.t;
+            if (small_step < 0) r.took_small = 1;
+        }
+    }
+    r.fine_total = r.fine_left = 1 << (o.maxlevel - o.minlevel);
+    r.macro_cfl = 0.0;
+}
+
+// fclaw2d_run after the advance: CFL retry, dt update, regrid, end of run.
+void Server::end_macro(Request& r) {
+    const fcb_options_t& o = r.opt;
+    r.ctx->count_advance();
+    if (r.macro_cfl > o.max_cfl && o.reduce_cfl && !o.use_fixed_dt) {
+        r.ctx->restore_step();
+        r.dt_min = r.dt_min * o.desired_cfl / r.macro_cfl;
+        begin_macro(r);
+        return;
+    }
+    ++r.n_inner;
+    r.t += r.dt_step;
+    if (!o.use_fixed_dt) {
+        const double dt_new = r.dt_min * o.desired_cfl / r.macro_cfl;
+        if (!r.took_small) r.dt_min = dt_new;
+    }
+    r.ctx->set_curr_time(r.t);
+    if (o.regrid_interval > 0 && r.n_inner % o.regrid_interval == 0) r.ctx->regrid();
+    if (r.t < o.tfinal) {
+        begin_macro(r);
+        return;
+    }
+    r.state = REQ_DONE;
+}
+
+int Server::round() {
+    admit();
+    if (active_.empty()) return 0;
+    // group the active requests by launch key, one launch per group
+    std::vector<std::vector<int>> groups;
+    {
+        std::vector<decltype(launch_key(fcb_options_t{}))> keys;
+        for (int id : active_) {
+            const auto k = launch_key(reqs_.at(id).opt);
+            size_t g = 0;
+            while (g < keys.size() && !(keys[g] == k)) ++g;
+            if (g == keys.size()) {
+                keys.push_back(k);
+                groups.emplace_back();
+            }
+            groups[g].push_back(id);
+        }
+    }
+    const int na = (int)active_.size();
+    std::map<int, int> cfl_slot;
+    for (int i = 0; i < na; ++i) cfl_slot[active_[i]] = i;
+    // descriptors of this fine step for every active request
+    h_desc_.clear();
+    std::vector<std::pair<size_t, size_t>> ranges;
+    for (const auto& g : groups) {
+        const size_t b = h_desc_.size();
+        for (int id : g) {
+            Request& r = reqs_.at(id);
+            const int k = r.fine_total - r.fine_left;
+            const double dt_fine = r.dt_step / r.fine_total;
+            // the reference advances the level time by repeated addition of the fine dt
+            double tf = r.t;
+            for (int j = 0; j < k; ++j) tf += dt_fine;
+            r.ctx->step_descs(tf, dt_fine, cfl_slot[id], h_desc_);
+        }
+        ranges.emplace_back(b, h_desc_.size() - b);
+    }
+    // upload, one launch per group
+    if (h_desc_.size() > h_desc_cap_) {
+        cudaFreeHost(h_desc_pinned_);
+        h_desc_cap_ = std::max(h_desc_.size(), 2 * h_desc_cap_);
+        check(cudaHostAlloc(&h_desc_pinned_, h_desc_cap_ * sizeof(PatchDesc), cudaHostAllocDefault), "host desc");
+    }
+    if ((size_t)na > h_cfl_cap_) {
+        cudaFreeHost(h_cfl_);
+        h_cfl_cap_ = std::max<size_t>(na, 2 * h_cfl_cap_);
+        check(cudaHostAlloc(&h_cfl_, h_cfl_cap_ * sizeof(unsigned long long), cudaHostAllocDefault), "host cfl");
+    }
+    std::memcpy(h_desc_pinned_, h_desc_.data(), h_desc_.size() * sizeof(PatchDesc));
+    d_desc_.reserve(std::max<size_t>(1, h_desc_.size()));
+    d_cfl_.reserve(std::max(1, na));
+    check(cudaMemcpyAsync(d_desc_.p, h_desc_pinned_, h_desc_.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, st_),
+          "descriptors");
+    check(cudaMemsetAsync(d_cfl_.p, 0, na * sizeof(unsigned long long), st_), "cfl");
+    for (size_t g = 0; g < groups.size(); ++g) {
+        const Request& r0 = reqs_.at(groups[g][0]);
+        check(launch_step_batch(r0.opt, r0.ctx->aux_kind(), d_desc_.p + ranges[g].first, (int)ranges[g].second,
+                                d_cfl_.p, st_),
+              "batched step");
+        ++launches_;
+    }
+    // each request's ghost fill after its fine step
+    for (int id : active_) {
+        Request& r = reqs_.at(id);
+        const int k = r.fine_total - r.fine_left;
+        const double dt_fine = r.dt_step / r.fine_total;
+        double tf = r.t;
+        for (int j = 0; j <= k; ++j) tf += dt_fine;
+        r.ctx->after_fine_step(tf);
+    }
+    check(cudaMemcpyAsync(h_cfl_, d_cfl_.p, na * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st_), "cfl");
+    check(cudaStreamSynchronize(st_), "round");
+    ++rounds_;
+    // per-request bookkeeping
+    std::vector<int> still;
+    for (int id : active_) {
+        Request& r = reqs_.at(id);
+        double c;
+        std::memcpy(&c, &h_cfl_[cfl_slot[id]], sizeof c);
+        try {
+            if (std::isnan(c)) throw Error(FCB_ERR_NUMERIC, "NaN CFL");
+            r.macro_cfl = std::max(r.macro_cfl, c);
+            r.cell_updates += (long long)r.ctx->num_patches() * r.opt.mx * r.opt.my;
+            if (--r.fine_left == 0) end_macro(r);
+        } catch (const Error& e) {
+            r.state = REQ_FAILED;
+            r.error = e.what();
+        }
+        if (r.state == REQ_ACTIVE) {
+            still.push_back(id);
+        } else {
+            r.t_finish = now();
+            used_ -= r.bytes;
+        }
+    }
+    active_.swap(still);
+    return (int)active_.size();
+}
+
+void Server::get_q(int id, double* host, size_t n) {
+    Request& r = reqs_.at(id);
+    if (!r.ctx) throw Error(FCB_ERR_STATE, "request has no state (queued, failed or released)");
+    r.ctx->get_q(host, n, false);
+}
+
+void Server::release(int id) {
+    auto it = reqs_.find(id);
+    if (it == reqs_.end()) return;
+    Request& r = it->second;
+    if (r.state == REQ_ACTIVE) throw Error(FCB_ERR_STATE, "request still running");
+    if (r.state == REQ_QUEUED) queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
+    reqs_.erase(it);
+}
+
+}  // namespace fcb

@@ -582,8 +582,10 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     const bool active = patch_ok && c < NX;
     const int pls = patch_ok ? pl : 0;  // threads without a patch read (never write) patch 0's rows
     const int cc = c < NX ? c : NX - 1;
-    const int slot = patch_ok ? a.slots[pg] : 0;
-    const PatchMeta meta = patch_ok ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0};
+    const PatchDesc* D = (a.desc && patch_ok) ? a.desc + pg : nullptr;  // mixed-solve launch
+    const int slot = (patch_ok && !a.desc) ? a.slots[pg] : 0;
+    const PatchMeta meta = D ? D->meta : (patch_ok ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0});
+    const int req = D ? D->req : -1;
     const SOL sol{R(a.grav), R(a.gamma), R(a.gamma1), R(a.drytol)};
 
     PipeThread<R> T;
@@ -592,15 +594,15 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     T.node = SWIRL && patch_ok;
     T.save_last = active && (meta.flags & PATCH_SAVE_LAST);
     T.ycol = active && c >= 1 && c <= NX - 2;
-    T.q = a.q + (int64_t)slot * a.q_stride + cc;
-    T.qlast = a.qlast + (int64_t)slot * a.q_stride + cc;
-    T.aux = (AUXK == AUX_STORED && active) ? a.aux + (int64_t)slot * a.aux_stride + cc : nullptr;
+    T.q = (D ? D->q : a.q + (int64_t)slot * a.q_stride) + cc;
+    T.qlast = (D ? D->qlast : a.qlast + (int64_t)slot * a.q_stride) + cc;
+    T.aux = (AUXK == AUX_STORED && active) ? (D ? D->aux : a.aux + (int64_t)slot * a.aux_stride) + cc : nullptr;
     T.rb = rsm + pls * NX + cc;
     T.db = dsm + pls * NX + cc;
     T.nb = dsm + L::ND + pls * (NX + 1) + c;
     T.ty = dsm + L::TY + pls * (NX + 1);
     // dtdx1d is uniform without capacity, so 0.5*(dtdx1d(i-1)+dtdx1d(i)) == dtdx exactly
-    const double dt = step_dt(a), vt = step_vt(a);
+    const double dt = D ? D->dt : step_dt(a), vt = D ? D->vt : step_vt(a);
     T.dtdx = dt / meta.dx;
     T.dtdy = dt / meta.dy;
     T.rdtdx = R(T.dtdx);
@@ -689,9 +691,20 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     // per direction gives the reference's value exactly.
     double cfl = (double)dmax(T.rdtdx * S.smax_x, T.rdtdy * S.smax_y);
     if (S.bad) cfl = __longlong_as_double(0x7ff8000000000000LL);  // NaN: wins the max, reported by the host
+    if (a.desc) {
+        // patches of different solves share warps: reduce over the lanes of each
+        // solve (max of the non-negative bit patterns, high word then low word)
+        const unsigned grp = __match_any_sync(0xffffffffu, req);
+        const unsigned long long b = (unsigned long long)__double_as_longlong(patch_ok ? cfl : 0.0);
+        const unsigned hi = __reduce_max_sync(grp, (unsigned)(b >> 32));
+        const unsigned lo = __reduce_max_sync(grp, ((unsigned)(b >> 32) == hi) ? (unsigned)b : 0u);
+        if (req >= 0 && (t & 31) == __ffs(grp) - 1 && a.cfl_out)
+            atomicMax(a.cfl_out + req, ((unsigned long long)hi << 32) | lo);
+    } else {
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
-    if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg_p(a.cfl_out, cfl);
+        for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+        if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg_p(a.cfl_out, cfl);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -217,6 +217,42 @@ int fcb_curr_time(fcb_context_t* ctx, double* t);
 /* Wait for all work of the context. */
 int fcb_synchronize(fcb_context_t* ctx);
 
+/* ---- ensemble serving -----------------------------------------------------
+ * No counterpart in the reference (ForestClaw runs one solve per process): a
+ * server admits independent solves as they arrive, keeps their arrays on the
+ * device, and advances them together.  Each served solve uses non-subcycled
+ * time stepping (subcycle = 0, nout = 1, pipelined step form); a round advances
+ * every active solve by one fine step, with the patches of all solves that
+ * share solver, patch shape, method and precision in ONE step launch, each
+ * patch carrying its own dt.  Queued solves are admitted in arrival order while
+ * their device arrays fit in budget_bytes (one solve is always admitted when
+ * none runs).  A served solve's result equals fcb_run on the same options bit
+ * for bit.  Work is enqueued on cuda_stream (NULL: the legacy default stream). */
+typedef struct fcb_server fcb_server_t;
+enum fcb_request_state { FCB_REQ_QUEUED = 0, FCB_REQ_ACTIVE = 1, FCB_REQ_DONE = 2, FCB_REQ_FAILED = 3 };
+typedef struct fcb_request_status {
+    int state;                /* enum fcb_request_state */
+    int num_patches;          /* current leaves (0 unless active or done) */
+    double t;                 /* simulated time reached */
+    double submit_s, start_s, finish_s;  /* server clock (seconds since creation) */
+    long long cell_updates;   /* interior cells advanced, summed over fine steps */
+    long long count_amr_advance;
+} fcb_request_status_t;
+int fcb_server_create(size_t budget_bytes, void* cuda_stream, fcb_server_t** out);
+int fcb_server_destroy(fcb_server_t* s);
+/* Queue a solve; *id receives its handle. */
+int fcb_server_submit(fcb_server_t* s, const fcb_options_t* opt, int* id);
+/* Admit what fits, advance every active solve by one fine step; reports the
+ * active and queued counts after the round. */
+int fcb_server_round(fcb_server_t* s, int* active, int* queued);
+int fcb_server_status(fcb_server_t* s, int id, fcb_request_status_t* out);
+/* Patch arrays of a finished (or running) solve, as fcb_get_q. */
+int fcb_server_get_q(fcb_server_t* s, int id, double* host, size_t n);
+/* Forget a finished, failed or queued solve and free its device arrays. */
+int fcb_server_release(fcb_server_t* s, int id);
+/* Seconds on the server clock; rounds and step launches so far. */
+int fcb_server_clock(fcb_server_t* s, double* now, long long* rounds, long long* launches);
+
 #ifdef __cplusplus
 }
 #endif

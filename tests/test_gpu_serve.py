@@ -1,0 +1,118 @@
+"""Ensemble serving: continuous batching of independent solves.
+
+A served solve must give the same result alone and in a mix of concurrent
+solves (batching only changes which launch a patch is in), and the same
+result as fcb_run on the same options with non-subcycled stepping.  Both are
+checked bit for bit, in FP64 and in the mixed FP32/FP64 form.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _dam(seed, maxlevel, mx=16, tfinal=0.03, precision=0):
+    import forestclaw_b200 as fcb
+
+    cfg = cases.radialdam_amr(seed=seed, minlevel=2, maxlevel=maxlevel, mx=mx, tfinal=tfinal)
+    o = cases.to_options(cfg)
+    o.subcycle = 0
+    o.precision = precision
+    return o
+
+
+def _serve(reqs, budget=1 << 40, stagger_rounds=0):
+    """Submit requests (staggered by `stagger_rounds` rounds), run to idle,
+    return the final states in submission order."""
+    from forestclaw_b200.serve import DONE, Server
+
+    sv = Server(budget)
+    ids, out = [], {}
+    pending = list(reqs)
+    while pending or any(sv.status(i).state < DONE for i in ids):
+        if pending:
+            ids.append(sv.submit(pending.pop(0)))
+            for _ in range(stagger_rounds):
+                sv.round()
+        else:
+            sv.round()
+    for k, i in enumerate(ids):
+        st = sv.status(i)
+        assert st.state == DONE, sv.error(i)
+        out[k] = sv.get_q(i)
+        sv.release(i)
+    sv.close()
+    return [out[k] for k in range(len(reqs))]
+
+
+def test_served_solve_equals_run(gpu_lib):
+    import forestclaw_b200 as fcb
+
+    o = _dam(seed=0, maxlevel=4)
+    d = fcb.Solver(dataclasses.replace(o))
+    d.initialize()
+    d.run()
+    (q_served,) = _serve([o])
+    assert np.array_equal(q_served, d.get_q())
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_alone_and_in_the_mix_are_identical(gpu_lib, precision):
+    reqs = [_dam(seed=s, maxlevel=ml, tfinal=tf, precision=precision)
+            for s, ml, tf in [(1, 3, 0.03), (2, 5, 0.02), (3, 4, 0.04), (4, 3, 0.01)]]
+    alone = [_serve([r])[0] for r in reqs]
+    mixed = _serve(reqs, stagger_rounds=3)
+    for k, (a, m) in enumerate(zip(alone, mixed)):
+        assert np.array_equal(a, m), f"request {k}"
+
+
+def test_two_patch_shapes_and_a_memory_budget(gpu_lib):
+    """Requests with mx 16 and 32 go to separate launches of the same round; a
+    budget that holds about one solve serialises admission but every request
+    completes with the same result as alone."""
+    from forestclaw_b200.serve import DONE, Server
+
+    reqs = [_dam(seed=5, maxlevel=3, mx=16), _dam(seed=6, maxlevel=3, mx=32), _dam(seed=7, maxlevel=3, mx=16)]
+    alone = [_serve([r])[0] for r in reqs]
+    sv = Server(1 << 40)
+    ids = [sv.submit(r) for r in reqs]
+    sv.round()
+    _, rounds0, launches0 = sv.clock()
+    sv.round()
+    _, rounds1, launches1 = sv.clock()
+    assert launches1 - launches0 == 2  # one launch per patch shape
+    sv.run_until_idle()
+    for k, i in enumerate(ids):
+        assert sv.status(i).state == DONE
+        assert np.array_equal(sv.get_q(i), alone[k])
+    sv.close()
+    # tiny budget: at most one solve on the device at a time
+    sv = Server(1)
+    ids = [sv.submit(r) for r in reqs]
+    spans = []
+    sv.run_until_idle()
+    for k, i in enumerate(ids):
+        st = sv.status(i)
+        assert st.state == DONE
+        spans.append((st.start_s, st.finish_s))
+        assert np.array_equal(sv.get_q(i), alone[k])
+    spans.sort()
+    for (s0, f0), (s1, f1) in zip(spans, spans[1:]):
+        assert s1 >= f0 - 1e-9  # admitted only after the previous one finished
+    sv.close()
+
+
+def test_poisson_stream_reports_latencies(gpu_lib):
+    from forestclaw_b200.serve import Server, poisson_stream
+
+    reqs = [_dam(seed=10 + k, maxlevel=3 + (k % 2), tfinal=0.01) for k in range(6)]
+    sv = Server(1 << 40)
+    res = poisson_stream(sv, reqs, rate=200.0, seed=1)
+    sv.close()
+    assert len(res.latencies) == 6 and res.failed == 0
+    assert res.pct(99) >= res.pct(50) > 0
+    assert res.cell_updates > 0 and res.launches >= res.rounds
