@@ -24,6 +24,8 @@ from __future__ import annotations
 
 import argparse
 import json
+
+import numpy as np
 import os
 import subprocess
 import sys
@@ -44,7 +46,9 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="uniform_swirl", choices=["uniform_swirl", "amr_radialdam"])
+    p.add_argument("--workload", default="uniform_swirl", choices=["uniform_swirl", "amr_radialdam", "serve"])
+    p.add_argument("--requests", type=int, default=24, help="serve: number of requests")
+    p.add_argument("--rates", default="5,20,80", help="serve: Poisson arrival rates (requests/s) to sweep")
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--mx", type=int, default=16)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
@@ -436,6 +440,75 @@ def amr_cpu_sample(budget_s):
                       f"of the reference, OpenMP over the patches of each level"}
 
 
+# ----------------------------------------------------------------------------
+# Ensemble serving: Poisson stream of shallow-water dam-break requests
+# ----------------------------------------------------------------------------
+def _serve_requests(n, seed, precision):
+    """Dam breaks with radius ~ U(0.1, 0.3), inner depth ~ U(1.5, 3), outer 1,
+    maxlevel ~ U{4, 5}, mx ~ {16, 32}, t_final ~ U(0.02, 0.05); levels from 2,
+    non-subcycled, regrid every macro step, adaptive dt (desired CFL 0.9)."""
+    import cases
+    import forestclaw_b200 as fcb
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        r0, hin = rng.uniform(0.1, 0.3), rng.uniform(1.5, 3.0)
+        maxlevel, mx = int(rng.integers(4, 6)), int(rng.choice([16, 32]))
+        cfg = cases.radialdam_amr(seed=0, minlevel=2, maxlevel=maxlevel, mx=mx, tfinal=float(rng.uniform(0.02, 0.05)))
+        cfg = cases.replace(cfg, pparams=(0.5, 0.5, r0, hin, 1.0), initial_dt=0.9 / (mx * 4) / (hin ** 0.5 + 1))
+        o = cases.to_options(cfg)
+        o.subcycle = 0
+        o.precision = fcb.PRECISION_MIXED if precision == "mixed" else fcb.PRECISION_FP64
+        out.append(o)
+    return out
+
+
+def run_serve(args, rank, world, local_rank):
+    import torch
+
+    from forestclaw_b200.serve import Server, poisson_stream
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.current_stream().cuda_stream
+    reqs = _serve_requests(args.requests, 7 + rank, args.precision)
+    budget = int(0.5 * torch.cuda.get_device_properties(local_rank).total_memory)
+    # isolated latency of each request (alone on the GPU)
+    iso = []
+    for o in reqs:
+        sv = Server(budget, stream)
+        r = poisson_stream(sv, [o], rate=0.0)
+        iso.append(r.latencies[0])
+        sv.close()
+    sweep = []
+    with ClockSampler(local_rank) as clk:
+        for lam in [float(x) for x in args.rates.split(",")]:
+            sv = Server(budget, stream)
+            r = poisson_stream(sv, reqs, rate=lam, seed=11)
+            sv.close()
+            sweep.append({"rate_per_s": lam, "p50_s": r.pct(50), "p99_s": r.pct(99),
+                          "cell_updates_per_s": r.cell_updates / r.wall, "wall_s": r.wall,
+                          "rounds": r.rounds, "launches": r.launches, "failed": r.failed,
+                          "p99_over_isolated_p99": r.pct(99) / float(np.percentile(iso, 99))})
+    if rank != 0:
+        return None
+    top = max(sweep, key=lambda d: d["cell_updates_per_s"])
+    return {
+        "metric": "cell-updates/s", "value": top["cell_updates_per_s"], "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.requests, "warmup": 0, "ms_per_step": top["wall_s"] * 1e3 / args.requests,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
+        "config": {"workload": "ensemble serving: Poisson stream of shallow-water dam-break solves "
+                               "(r ~ U(0.1,0.3), h_in ~ U(1.5,3), maxlevel ~ U{4,5}, mx ~ {16,32}, "
+                               "t_final ~ U(0.02,0.05)), continuous batching",
+                   "requests": args.requests, "isolated_p50_s": float(np.percentile(iso, 50)),
+                   "isolated_p99_s": float(np.percentile(iso, 99)), "sweep": sweep},
+        "p50_s": top["p50_s"], "p99_s": top["p99_s"],
+        "clocks": clk.summary(),
+        "gpu_launches": top["launches"],
+    }
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -457,7 +530,7 @@ def main():
                                              device_id=torch.device("cuda", local_rank))
     try:
         sys.path.insert(0, str(ROOT / "tests"))
-        run = run_amr if args.workload == "amr_radialdam" else run_ours
+        run = {"amr_radialdam": run_amr, "serve": run_serve}.get(args.workload, run_ours)
         line = run(args, rank, world, local_rank)
         if line:
             print(json.dumps(line), flush=True)
