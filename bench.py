@@ -107,6 +107,19 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+# DRAM bytes (read + write) per step-kernel launch from the ncu captures
+# summarised in profiles/ (same workload, same kernel build).
+_TRAFFIC = {("fp64", 8, 16): (357.29e6, "profiles/step_kernel_uniform_swirl_l8_mx16.md"),
+            ("mixed", 8, 16): (359.25e6, "profiles/step_kernel_mixed_uniform_swirl_l8_mx16.md")}
+
+
+def _profiled_traffic(args):
+    t = _TRAFFIC.get((args.precision, args.level, args.mx))
+    if t is None or args.step_variant not in (0, 3):
+        return None
+    return {"bytes_per_launch": t[0], "source": t[1]}
+
+
 def peaks():
     if PEAKS_FILE.exists():
         d = json.loads(PEAKS_FILE.read_text())
@@ -122,9 +135,11 @@ def native_oracle():
     so = ROOT / "oracle" / "liboracle_native.so"
     stamp = ROOT / "oracle" / "liboracle_native.host"
     host = open("/proc/cpuinfo").read().split("model name")[1].split("\n")[0] if Path("/proc/cpuinfo").exists() else "?"
-    if not so.exists() or not stamp.exists() or stamp.read_text() != host:
-        srcs = [str(ROOT / "oracle" / f) for f in
-                ("oracle_patch.cpp", "oracle_clawpatch.cpp", "oracle_amr.cpp", "oracle_capi.cpp")]
+    srcs = [str(ROOT / "oracle" / f) for f in
+            ("oracle_patch.cpp", "oracle_clawpatch.cpp", "oracle_amr.cpp", "oracle_capi.cpp")]
+    deps = srcs + [str(p) for p in (ROOT / "oracle").glob("*.hpp")]
+    stale = so.exists() and any(Path(d).stat().st_mtime > so.stat().st_mtime for d in deps)
+    if not so.exists() or stale or not stamp.exists() or stamp.read_text() != host:
         cxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
         subprocess.run([cxx, "-O3", "-march=native", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fopenmp",
                         "-DORC_OPENMP", "-shared", "-o", str(so), *srcs], check=True)
@@ -321,7 +336,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": state_bytes / args.steps + 8},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
+                     "frac": achieved / hbm, "traffic": _profiled_traffic(args),
                      "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback",
                      "bytes_per_cell": bytes_per_cell, "kernel": "step_kernel"},
     }
