@@ -222,7 +222,7 @@ def run_ours(args, rank, world, local_rank):
     import torch
 
     import forestclaw_b200 as fcb
-    from forestclaw_b200 import workloads
+    from forestclaw_b200 import replicas, workloads
 
     torch.cuda.set_device(local_rank)
     stream = torch.cuda.current_stream()
@@ -261,11 +261,7 @@ def run_ours(args, rank, world, local_rank):
     c1 = s.counters()
     launches = c1["count_kernel_launches"] - c0["count_kernel_launches"]
     cells = (c1["count_single_step"] - c0["count_single_step"]) * args.mx * args.mx
-    ms_t = torch.tensor([ms], device="cuda")
-    if dist:
-        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    total_cells = cells * world
+    ms_max, total_cells = replicas.aggregate(ms, cells, torch.distributed if dist else None)
 
     # --- step-kernel alone: K launches of the level update between events ---
     nk = max(5, args.steps)
@@ -305,11 +301,7 @@ def run_ours(args, rank, world, local_rank):
     s.get_q(out=hv)
     x1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = x0.elapsed_time(x1)
-    e2e_t = torch.tensor([e2e_ms], device="cuda")
-    if dist:
-        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-    e2e_ms = float(e2e_t.item())
+    e2e_ms, _ = replicas.aggregate(x0.elapsed_time(x1), 0, torch.distributed if dist else None)
     state_bytes = npatch * psize * 8
 
     if rank != 0:
