@@ -41,7 +41,7 @@ EXPORTED_SYMBOLS = (
     "fcb_set_q", "fcb_single_step_update", "fcb_synchronize", "fcb_timeinterp",
     "fcb_update_single_step", "fcb_update_single_step_async", "fcb_conservation_sum_noalloc",
     "fcb_server_create", "fcb_server_destroy", "fcb_server_submit", "fcb_server_round", "fcb_server_status",
-    "fcb_server_get_q", "fcb_server_release", "fcb_server_clock",
+    "fcb_server_get_q", "fcb_server_release", "fcb_server_clock", "fcb_autotune_info",
 )
 
 
@@ -208,6 +208,7 @@ def lib():
     L.fcb_counters.argtypes = [vp, ctypes.POINTER(_Counters)]
     L.fcb_conservation_check.argtypes = [vp, dp]
     L.fcb_curr_time.argtypes = [vp, dp]
+    L.fcb_autotune_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     L.fcb_conservation_sum_noalloc.argtypes = [vp, sz, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, vp, vp, vp]
     ll = ctypes.POINTER(ctypes.c_longlong)
@@ -347,6 +348,12 @@ class Solver:
         c = _Counters()
         _check(lib().fcb_counters(self._h, ctypes.byref(c)))
         return {n: getattr(c, n) for n, _ in _Counters._fields_}
+
+    def autotune_info(self) -> dict:
+        """Step form (1 CTA, 2 warp, 3 pipelined) and ghost unroll of the last launches."""
+        f, u = ctypes.c_int(), ctypes.c_int()
+        _check(lib().fcb_autotune_info(self._h, ctypes.byref(f), ctypes.byref(u)))
+        return {"step_form": f.value, "ghost_unroll": u.value}
 
     def conservation_check(self) -> np.ndarray:
         out = np.zeros(self.options.meqn)

@@ -210,6 +210,16 @@ int fcb_curr_time(fcb_context_t* ctx, double* t) {
 
 int fcb_synchronize(fcb_context_t* ctx) { return guard([&] { CTX(); C.synchronize(); }); }
 
+int fcb_autotune_info(fcb_context_t* ctx, int* step_form, int* ghost_unroll) {
+    return guard([&] {
+        CTX();
+        need(step_form, "step_form");
+        need(ghost_unroll, "ghost_unroll");
+        *step_form = C.step_form_used();
+        *ghost_unroll = C.ghost_unroll_used();
+    });
+}
+
 // ---- serving ----
 int fcb_server_create(size_t budget_bytes, void* cuda_stream, fcb_server_t** out) {
     return guard([&] {

@@ -336,8 +336,7 @@ __device__ __forceinline__ double* op_cell(const GhostArgs& a, const GhostOp& op
 // (prefix sum of op_cells over the lanes) and each lane takes items lane,
 // lane+32, ...  UNROLL items per lane issue their loads before any store.
 constexpr int GHOST_TPB = 256;
-constexpr int GHOST_UNROLL = 4;
-
+template <int GHOST_UNROLL>
 __global__ void __launch_bounds__(GHOST_TPB) ghost_wave_kernel(const GhostArgs a) {
     __shared__ GhostOp s_ops[GHOST_TPB / 32][32];
     __shared__ int s_end[GHOST_TPB / 32][32];
@@ -395,10 +394,16 @@ __global__ void __launch_bounds__(GHOST_TPB) ghost_wave_kernel(const GhostArgs a
     }
 }
 
-cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st) {
+// unroll: work items per lane whose loads are issued before the stores (2, 4
+// or 8; the autotuner picks one per patch shape)
+cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st, int unroll) {
     if (a.ngroups <= 0) return cudaSuccess;
     const int blocks = (int)(((int64_t)a.ngroups * 32 + GHOST_TPB - 1) / GHOST_TPB);
-    ghost_wave_kernel<<<blocks, GHOST_TPB, 0, st>>>(a);
+    switch (unroll) {
+        case 2: ghost_wave_kernel<2><<<blocks, GHOST_TPB, 0, st>>>(a); break;
+        case 8: ghost_wave_kernel<8><<<blocks, GHOST_TPB, 0, st>>>(a); break;
+        default: ghost_wave_kernel<4><<<blocks, GHOST_TPB, 0, st>>>(a); break;
+    }
     return cudaGetLastError();
 }
 

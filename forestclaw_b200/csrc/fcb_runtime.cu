@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <cstring>
 #include <functional>
 #include <unordered_map>
@@ -232,6 +233,8 @@ void Context::mesh_changed() {
     }
     level_begin_[L] = (int)h_level_slots_.size();
     ti_begin_[L] = (int)tis.size();
+    gmin_ = forest_.min_level();
+    gmax_ = forest_.max_level();
     d_level_slots_.reserve(std::max<size_t>(1, h_level_slots_.size()));
     d_ti_slots_.reserve(std::max<size_t>(1, tis.size()));
     d_all_slots_.reserve(std::max(1, n));
@@ -484,6 +487,7 @@ void Context::run_plan(const GhostPlan& g) {
                   "groups");
         ops_dirty_ = false;
     }
+    ghost_unroll_ = opt_.step_variant == 0 ? tune_ghost_unroll(g) : 4;
     const int nw = (int)g.wave_begin.size() - 1;
     for (int w = 0; w < nw; ++w) {
         GhostArgs a;
@@ -495,7 +499,7 @@ void Context::run_plan(const GhostPlan& g) {
         a.groups = d_groups_.p + g.first_group + g.group_begin[w];  // group starts, then an end marker
         a.ngroups = g.group_begin[w + 1] - g.group_begin[w] - 1;
         a.interp_fp32 = opt_.precision == 1;
-        check(launch_ghost_wave(a, st_), "ghost wave");
+        check(launch_ghost_wave(a, st_, ghost_unroll_), "ghost wave");
         ++cnt_.count_ghost_waves;
         ++cnt_.count_kernel_launches;
     }
@@ -594,7 +598,8 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     // reference's per-cell evaluations because the unit-square mesh with mx a
     // power of two is dyadic (xll + dx == next xll exactly); checked at creation.
     cudaError_t e = cudaErrorNotSupported;
-    const int v = opt_.step_variant;
+    const int v = opt_.step_variant == 0 ? tune_step_form(a, n) : opt_.step_variant;
+    step_form_used_ = v;
     if (opt_.precision == 1) {
         e = launch_step_pipe_mixed(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc,
                                    opt_.claw_version, a, st_);
@@ -602,8 +607,7 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     } else if (v == 2) {
         if (aux_kind_ == AUX_SWIRL) e = launch_step_warp_swirl(opt_.mx, opt_.mbc, a, st_);
         if (e == cudaErrorNotSupported) throw Error(FCB_ERR_INVALID, "no warp-synchronous step for this case");
-    } else if (v == 3 || (v == 0 && (opt_.solver_kind == SOLVER_ADVECTION || opt_.claw_version == 5 ||
-                                    opt_.solver_kind == SOLVER_GEOCLAW_FWAVE))) {
+    } else if (v == 3) {
         // default: the pipelined form for scalar advection; the Roe solvers keep
         // the four-barrier form, whose smaller register footprint suits them
         e = launch_step_pipe(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, opt_.claw_version,
@@ -662,7 +666,7 @@ void Context::timeinterp(int level, double alpha) {
 
 // fclaw2d_advance_all_levels (src/fclaw2d_advance.c:247-357)
 void Context::run_schedule(double t_curr, double dt) {
-    const int gmin = forest_.min_level(), gmax = forest_.max_level();
+    const int gmin = gmin_, gmax = gmax_;
     struct Counter { int last_step, step_inc, total_steps; double current_time, dt_step; };
     std::vector<Counter> ts(opt_.maxlevel + 1);
     for (int l = opt_.minlevel; l <= opt_.maxlevel; ++l) { ts[l].last_step = 0; ts[l].current_time = t_curr; }
@@ -719,7 +723,7 @@ std::vector<uintptr_t> Context::macro_fingerprint() const {
     return {(uintptr_t)d_q_, (uintptr_t)d_qlast_, (uintptr_t)d_qti_, (uintptr_t)d_meta_,
             (uintptr_t)d_level_slots_.p, (uintptr_t)d_ti_slots_.p, (uintptr_t)d_ops_.p, (uintptr_t)d_groups_.p,
             (uintptr_t)d_dyn_.p, (uintptr_t)d_cfl_, (uintptr_t)mesh_version_, (uintptr_t)plans_.size(),
-            (uintptr_t)dyn_n_, (uintptr_t)forest_.min_level(), (uintptr_t)forest_.max_level()};
+            (uintptr_t)dyn_n_, (uintptr_t)gmin_, (uintptr_t)gmax_};
 }
 
 void Context::drop_macro_graph() {
@@ -747,9 +751,9 @@ double Context::advance_all_levels(double t_curr, double dt) {
             throw;
         }
         dry_ = false;
-        // auto: a graph pays off once a macro step issues several level steps
-        // (subcycling); a single-level macro step is three launches
-        if (opt_.macro_graph == 2 && dyn_n_ < 3) use_dyn_ = false;
+        // auto: the graph, whenever the macro step has a level update (a replay
+        // beats host launches even for the three launches of one level)
+        if (opt_.macro_graph == 2 && dyn_n_ < 1) use_dyn_ = false;
     }
     if (use_dyn_) {
         d_dyn_.reserve(std::max<size_t>(2, 2 * (size_t)dyn_n_));
@@ -815,6 +819,153 @@ double Context::advance_all_levels(double t_curr, double dt) {
 }
 
 // ---------------------------------------------------------------------------
+// Autotuner.  For step_variant 0 the library times the step forms that exist
+// for a (solver, aux, waves, mx, clawpack version, precision, limiter, size)
+// key on the first level update of that key, and the ghost-fill unroll on the first
+// ghost update of a patch shape, both on scratch copies of the arrays (the
+// real state is not touched).  Choices are cached for the process.  Never runs while a
+// macro-step graph is captured (the first call on a mesh is eager).
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_tune_mu;
+std::map<std::vector<int>, int> g_step_form_cache, g_ghost_unroll_cache;
+
+int default_step_form(const fcb_options_t& o) {
+    return (o.solver_kind == SOLVER_ADVECTION || o.claw_version == 5 || o.solver_kind == SOLVER_GEOCLAW_FWAVE ||
+            o.precision == 1)
+               ? 3
+               : 1;
+}
+}  // namespace
+
+int Context::tune_step_form(const StepArgs& a, int n) {
+    const bool fixed_lim = opt_.order[0] == 2 && opt_.order[1] == 2;
+    int nb = 0;
+    while ((1 << (nb + 1)) <= n) ++nb;
+    const std::vector<int> key = {opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.claw_version, opt_.precision,
+                                  fixed_lim ? opt_.mthlim[0] : -1, nb};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_step_form_cache.find(key);
+        if (it != g_step_form_cache.end()) return it->second;
+    }
+    std::vector<int> cand;
+    if (opt_.precision == 1 || opt_.claw_version == 5 || opt_.solver_kind == SOLVER_GEOCLAW_FWAVE) cand = {3};
+    else if (aux_kind_ == AUX_SWIRL) cand = {1, 2, 3};
+    else cand = {1, 3};
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st_, &cs);
+    if (cand.size() == 1 || cs != cudaStreamCaptureStatusNone || dry_) return cand.size() == 1 ? cand[0] : default_step_form(opt_);
+    const size_t bytes = (size_t)capacity_ * stride_ * sizeof(double);
+    double *tq = nullptr, *tl = nullptr;
+    if (cudaMalloc(&tq, bytes) != cudaSuccess || cudaMalloc(&tl, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(tq);
+        cudaFree(tl);
+        return default_step_form(opt_);  // no room for scratch copies: no tuning
+    }
+    check(cudaMemcpyAsync(tq, d_q_, bytes, cudaMemcpyDeviceToDevice, st_), "tune copy");
+    StepArgs b = a;
+    b.q = tq;
+    b.qlast = tl;
+    b.dyn = nullptr;
+    b.cfl_out = d_cfl_ + 3;
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    int best = default_step_form(opt_);
+    float best_ms = 1e30f;
+    for (int v : cand) {
+        auto launch = [&]() -> cudaError_t {
+            if (v == 2) return launch_step_warp_swirl(opt_.mx, opt_.mbc, b, st_);
+            if (v == 3)
+                return launch_step_pipe(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc,
+                                        opt_.claw_version, b, st_);
+            return launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_);
+        };
+        if (launch() != cudaSuccess) {  // form not available for this case
+            cudaGetLastError();
+            continue;
+        }
+        check(cudaEventRecord(e0, st_), "event");
+        for (int r = 0; r < 3; ++r) check(launch(), "tune launch");
+        check(cudaEventRecord(e1, st_), "event");
+        check(cudaEventSynchronize(e1), "event");
+        float ms = 0;
+        check(cudaEventElapsedTime(&ms, e0, e1), "event");
+        if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check(cudaStreamSynchronize(st_), "sync");
+    cudaFree(tq);
+    cudaFree(tl);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_step_form_cache[key] = best;
+    return best;
+}
+
+int Context::tune_ghost_unroll(const GhostPlan& g) {
+    const std::vector<int> key = {opt_.mx, opt_.meqn, opt_.precision};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_ghost_unroll_cache.find(key);
+        if (it != g_ghost_unroll_cache.end()) return it->second;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st_, &cs);
+    if (cs != cudaStreamCaptureStatusNone || g.wave_begin.size() < 2) return 4;
+    // scratch copies of the arena and the time-interpolation arena, so the
+    // timed passes leave the real state untouched
+    const size_t bytes = (size_t)capacity_ * stride_ * sizeof(double);
+    double *tq = nullptr, *tt = nullptr;
+    if (cudaMalloc(&tq, bytes) != cudaSuccess || cudaMalloc(&tt, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(tq);
+        cudaFree(tt);
+        return 4;
+    }
+    check(cudaMemcpyAsync(tq, d_q_, bytes, cudaMemcpyDeviceToDevice, st_), "tune copy");
+    if (d_qti_) check(cudaMemcpyAsync(tt, d_qti_, bytes, cudaMemcpyDeviceToDevice, st_), "tune copy");
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    int best = 4;
+    float best_ms = 1e30f;
+    const int nw = (int)g.wave_begin.size() - 1;
+    for (int u : {2, 4, 8}) {
+        auto pass = [&]() {
+            for (int w = 0; w < nw; ++w) {
+                GhostArgs ga;
+                ga.q = tq; ga.qti = tt; ga.stride = stride_;
+                ga.mx = opt_.mx; ga.my = opt_.my; ga.mbc = opt_.mbc; ga.meqn = opt_.meqn;
+                ga.ops = d_ops_.p;
+                ga.groups = d_groups_.p + g.first_group + g.group_begin[w];
+                ga.ngroups = g.group_begin[w + 1] - g.group_begin[w] - 1;
+                ga.interp_fp32 = opt_.precision == 1;
+                check(launch_ghost_wave(ga, st_, u), "tune ghost");
+            }
+        };
+        pass();
+        check(cudaEventRecord(e0, st_), "event");
+        for (int r = 0; r < 3; ++r) pass();
+        check(cudaEventRecord(e1, st_), "event");
+        check(cudaEventSynchronize(e1), "event");
+        float ms = 0;
+        check(cudaEventElapsedTime(&ms, e0, e1), "event");
+        if (ms < best_ms) { best_ms = ms; best = u; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check(cudaStreamSynchronize(st_), "sync");
+    cudaFree(tq);
+    cudaFree(tt);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_ghost_unroll_cache[key] = best;
+    return best;
+}
+
+// ---------------------------------------------------------------------------
 // Batched serving support
 // ---------------------------------------------------------------------------
 // Non-subcycled fclaw2d_advance_all_levels (src/fclaw2d_advance.c:300-324): each
@@ -845,7 +996,7 @@ void Context::step_descs(double t, double dt, int req, std::vector<PatchDesc>& o
     cnt_.count_single_step += n;
 }
 
-void Context::after_fine_step(double t) { ghost_update(forest_.min_level(), forest_.max_level(), t, 0); }
+void Context::after_fine_step(double t) { ghost_update(gmin_, gmax_, t, 0); }
 
 // fclaw2d_clawpatch_save_step / restore_step: the CFL-retry copy
 void Context::save_step() {

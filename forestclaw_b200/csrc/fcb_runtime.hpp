@@ -35,7 +35,7 @@ cudaError_t launch_step_pipe(int solver, int aux_kind, int mwaves, int mx, int m
 cudaError_t launch_step_pipe_mixed(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
                                    int claw_version, const StepArgs& a, cudaStream_t st);
 struct GhostArgs;
-cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st);
+cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st, int unroll);
 cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64_t stride,
                               const int32_t* slots, int n, int mx, int my, int mbc, int meqn,
                               double alpha, cudaStream_t st);
@@ -110,6 +110,10 @@ class Context {
     void set_curr_time(double t) { curr_time_ = t; }
     void count_advance() { ++cnt_.count_amr_advance; }
     size_t device_bytes() const;
+    // autotuner: the step form (1 four-barrier CTA, 2 warp, 3 pipelined) and the
+    // ghost-fill unroll used by the last launches
+    int step_form_used() const { return step_form_used_; }
+    int ghost_unroll_used() const { return ghost_unroll_; }
 
   private:
     // --- setup ---
@@ -158,6 +162,7 @@ class Context {
     // level lists (device), grouped by level
     DevBuf<int32_t> d_level_slots_;
     std::vector<int> level_begin_;    // size maxlevel+2
+    int gmin_ = 0, gmax_ = 0;         // coarsest and finest leaf level (set with the level lists)
     std::vector<int32_t> h_level_slots_;
     DevBuf<int32_t> d_ti_slots_;      // per level: slots with fine-grid neighbours
     std::vector<int> ti_begin_;
@@ -192,6 +197,11 @@ class Context {
     uint64_t mesh_version_ = 0;
     cudaGraphExec_t macro_exec_ = nullptr;
     cudaStream_t cap_st_ = nullptr;  // capture stream (the caller's stream may be the legacy one)
+    // autotuner
+    int tune_step_form(const StepArgs& a, int n);
+    int tune_ghost_unroll(const GhostPlan& g);
+    int step_form_used_ = 0;
+    int ghost_unroll_ = 0;
     std::vector<uintptr_t> macro_key_, macro_seen_;
     fcb_counters_t macro_delta_{};
     // state

@@ -110,7 +110,7 @@ typedef struct fcb_options {
     /* 1: fcb_advance_all_levels replays the whole subcycled macro-step (level
      * updates, time interpolation, ghost fills) as one CUDA graph, captured on
      * the second call for a mesh; 0: every launch is issued from the host;
-     * 2: graph when a macro step updates three or more level batches */
+     * 2: automatic (the graph whenever a macro step updates a level) */
     int macro_graph;
     /* 4 (or 0): the fc2d_clawpack46 update; 5: the fc2d_clawpack5 update
      * (fluxes at interfaces 1..mx+1, interior cells updated, clawpack5 Riemann
@@ -214,6 +214,13 @@ int fcb_conservation_sum_noalloc(const double* d_q, size_t patch_stride, int npa
                                  int meqn, const double* d_area, double* d_sums, void* cuda_stream);
 /* Current time of the run loop. */
 int fcb_curr_time(fcb_context_t* ctx, double* t);
+/* Autotuner choices of the last launches (no counterpart in the reference):
+ * step_form 1 = one CTA per patch with four barriers per stage, 2 = one warp
+ * per patch, 3 = pipelined row sweep; ghost_unroll = ghost records per thread
+ * per pass (2, 4 or 8).  With step_variant 0 the library times the forms that
+ * exist for the case on its first level update, on scratch copies of the
+ * arrays, and keeps the fastest for the process; 0 before the first update. */
+int fcb_autotune_info(fcb_context_t* ctx, int* step_form, int* ghost_unroll);
 /* Wait for all work of the context. */
 int fcb_synchronize(fcb_context_t* ctx);
 

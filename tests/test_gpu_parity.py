@@ -202,3 +202,36 @@ def test_macro_step_graph_replays_bit_exact(gpu_lib):
     assert ce["count_graph_replays"] == 0
     for name in ("count_single_step", "count_ghost_waves", "count_kernel_launches"):
         assert cg[name] == ce[name], name
+
+
+@pytest.mark.parametrize("case", ["swirl", "radialdam"])
+def test_autotuned_form_is_bit_identical_to_forced_form(gpu_lib, case):
+    """step_variant 0 times the available step forms and ghost unrolls on
+    scratch copies; the run must equal the same run with the chosen form forced,
+    bit for bit (the tuner leaves the state alone and every form is exact)."""
+    import forestclaw_b200 as fcb
+
+    if case == "swirl":
+        cfg, dt = cases.swirl_uniform(level=4, mx=16), cases.swirl_dt(level=4, mx=16)
+    else:
+        cfg, dt = cases.radialdam_uniform(level=3, mx=16), 0.4 / (16 * 8) / 1.5
+    auto = fcb.Solver(cases.to_options(cfg))
+    auto.initialize()
+    assert auto.autotune_info()["step_form"] == 0
+    t = 0.0
+    for _ in range(4):
+        auto.advance_all_levels(t, dt)
+        t += dt
+    info = auto.autotune_info()
+    assert info["step_form"] in (1, 2, 3) and info["ghost_unroll"] in (2, 4, 8), info
+    opts = cases.to_options(cfg)
+    opts.step_variant = info["step_form"]
+    forced = fcb.Solver(opts)
+    forced.initialize()
+    t = 0.0
+    for _ in range(4):
+        forced.advance_all_levels(t, dt)
+        t += dt
+    assert np.array_equal(auto.get_q(), forced.get_q())
+    auto.close()
+    forced.close()
