@@ -331,12 +331,45 @@ def run_ours(args, rank, world, local_rank):
                      "frac": achieved / hbm, "traffic": _profiled_traffic(args),
                      "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback",
                      "bytes_per_cell": bytes_per_cell, "kernel": "step_kernel"},
+        "roofline_fp": fp_roofline("advection_swirl_order22", args.mx, cells_per_step / (step_ms * 1e-3),
+                                   args.precision, stream.cuda_stream),
     }
     if world == 1:
         sys.path.insert(0, str(ROOT / "tests"))
         line["cpu_baseline"] = cpu_sample(args, args.cpu_seconds)
     s.close()
     return line
+
+
+# FP64 operations per interior cell update of the reference's patch step
+# (adds, multiplies, divides, square roots, compare/selects; ghost-region work
+# included), counted by the instrumented build of the CPU restatement on dense
+# seeded inputs: `make -C oracle flopcount && oracle/flopcount`.  Keyed by
+# (case, mx); tests/test_flopcount.py checks them against that program.
+FP64_OPS_PER_CELL = {
+    ("advection_swirl_order22", 8): 244.5,
+    ("advection_swirl_order22", 16): 193.25,
+    ("advection_swirl_order22", 32): 169.875,
+    ("swe_roe_order22", 16): 1244.9609,
+    ("swe_roe_order22", 32): 1090.248,
+}
+
+
+def fp_roofline(case, mx, cells_per_s, precision, stream):
+    """Algorithmic FP64 operations per second of the step against this GPU's
+    measured add/multiply issue rate (FP64; FP32 for the mixed form, whose
+    solves run in FP32)."""
+    import forestclaw_b200 as fcb
+
+    ops = FP64_OPS_PER_CELL.get((case, mx))
+    if ops is None:
+        return None
+    fp64 = precision == "fp64"
+    peak = fcb.measure_fp_rate(fp64, stream) / 1e9
+    achieved = ops * cells_per_s / 1e9
+    return {"bound": "fp64 pipe" if fp64 else "fp32 pipe", "achieved": achieved, "peak": peak,
+            "unit": "Gop/s", "frac": achieved / peak, "ops_per_cell": ops,
+            "peak_source": "measured on this GPU (fcb_measure_fp_rate: lane add/multiply per second)"}
 
 
 # ----------------------------------------------------------------------------
@@ -416,6 +449,8 @@ def run_amr(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": None, "bytes_per_cell": bytes_per_cell, "kernel": "advance phase (all kernels)",
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback"},
+        "roofline_fp": fp_roofline("swe_roe_order22", cfg.mx, cells / (adv_ms * 1e-3), args.precision,
+                                   stream.cuda_stream),
     }
     if world == 1:
         line["cpu_baseline"] = amr_cpu_sample(args.cpu_seconds)

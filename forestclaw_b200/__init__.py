@@ -22,7 +22,7 @@ import numpy as np
 __all__ = ["Options", "Solver", "lib", "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
            "SOLVER_EULER4_ROE", "SOLVER_GEOCLAW_FWAVE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM",
            "PROBLEM_QUADRANTS", "PROBLEM_BATHY",
-           "PRECISION_FP64", "PRECISION_MIXED",
+           "PRECISION_FP64", "PRECISION_MIXED", "measure_fp_rate",
            "TAG_VALUE", "TAG_MINMAX", "TAG_DIFFERENCE", "TAG_GRADIENT", "EXPORTED_SYMBOLS"]
 
 PKG = Path(__file__).resolve().parent
@@ -42,6 +42,7 @@ EXPORTED_SYMBOLS = (
     "fcb_update_single_step", "fcb_update_single_step_async", "fcb_conservation_sum_noalloc",
     "fcb_server_create", "fcb_server_destroy", "fcb_server_submit", "fcb_server_round", "fcb_server_status",
     "fcb_server_get_q", "fcb_server_release", "fcb_server_clock", "fcb_autotune_info",
+    "fcb_measure_fp_rate",
 )
 
 
@@ -209,6 +210,7 @@ def lib():
     L.fcb_conservation_check.argtypes = [vp, dp]
     L.fcb_curr_time.argtypes = [vp, dp]
     L.fcb_autotune_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    L.fcb_measure_fp_rate.argtypes = [ctypes.c_int, vp, dp]
     L.fcb_conservation_sum_noalloc.argtypes = [vp, sz, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, vp, vp, vp]
     ll = ctypes.POINTER(ctypes.c_longlong)
@@ -227,6 +229,13 @@ def lib():
 def _check(rc: int):
     if rc != 0:
         raise FcbError(rc, lib().fcb_last_error().decode())
+
+
+def measure_fp_rate(fp64: bool = True, stream: int = 0) -> float:
+    """Lane add/multiply operations per second of the current GPU (FP64 or FP32)."""
+    r = ctypes.c_double()
+    _check(lib().fcb_measure_fp_rate(1 if fp64 else 0, ctypes.c_void_p(stream), ctypes.byref(r)))
+    return r.value
 
 
 def _dp(a: np.ndarray):

@@ -37,6 +37,7 @@ SOURCES = {
     "fcb_serve.cu": [],
     "fcb_capi.cu": ["-Xcompiler", "-fvisibility=default"],
     "fcb_noalloc.cu": ["-fmad=false"],
+    "fcb_probe.cu": ["-fmad=false"],
 }
 HEADERS = ["fcb_device.h", "fcb_solvers.cuh", "fcb_step_pipe.cuh", "fcb_forest.hpp", "fcb_runtime.hpp", "fcb_serve.hpp"]
 

@@ -210,6 +210,14 @@ int fcb_curr_time(fcb_context_t* ctx, double* t) {
 
 int fcb_synchronize(fcb_context_t* ctx) { return guard([&] { CTX(); C.synchronize(); }); }
 
+int fcb_measure_fp_rate(int fp64, void* cuda_stream, double* ops_per_second) {
+    return guard([&] {
+        need(ops_per_second, "ops_per_second");
+        const cudaError_t e = fcb::measure_fp_rate(fp64 != 0, (cudaStream_t)cuda_stream, ops_per_second);
+        if (e != cudaSuccess) throw fcb::Error(FCB_ERR_CUDA, std::string("fp rate probe: ") + cudaGetErrorString(e));
+    });
+}
+
 int fcb_autotune_info(fcb_context_t* ctx, int* step_form, int* ghost_unroll) {
     return guard([&] {
         CTX();

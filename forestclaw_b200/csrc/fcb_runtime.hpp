@@ -35,6 +35,9 @@ cudaError_t launch_step_pipe(int solver, int aux_kind, int mwaves, int mx, int m
 cudaError_t launch_step_pipe_mixed(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
                                    int claw_version, const StepArgs& a, cudaStream_t st);
 struct GhostArgs;
+// Lane add/multiply operations per second of this GPU in FP64 (fp64) or FP32
+// (fcb_probe.cu).
+cudaError_t measure_fp_rate(bool fp64, cudaStream_t st, double* ops_per_second);
 cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st, int unroll);
 cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64_t stride,
                               const int32_t* slots, int n, int mx, int my, int mbc, int meqn,

@@ -221,6 +221,12 @@ int fcb_curr_time(fcb_context_t* ctx, double* t);
  * exist for the case on its first level update, on scratch copies of the
  * arrays, and keeps the fastest for the process; 0 before the first update. */
 int fcb_autotune_info(fcb_context_t* ctx, int* step_form, int* ghost_unroll);
+/* Floating-point issue rate of the current GPU (no counterpart in the
+ * reference; for roofline reports): lane add/multiply operations per second in
+ * FP64 (fp64 != 0) or FP32, from independent multiply-then-add chains on one
+ * full wave of resident CTAs, best of five launches on cuda_stream.  Allocates
+ * and frees a small result array. */
+int fcb_measure_fp_rate(int fp64, void* cuda_stream, double* ops_per_second);
 /* Wait for all work of the context. */
 int fcb_synchronize(fcb_context_t* ctx);
 
