@@ -39,7 +39,6 @@ SOURCES = {
     "fcb_noalloc.cu": ["-fmad=false"],
     "fcb_probe.cu": ["-fmad=false"],
 }
-HEADERS = ["fcb_device.h", "fcb_solvers.cuh", "fcb_step_pipe.cuh", "fcb_forest.hpp", "fcb_runtime.hpp", "fcb_serve.hpp"]
 
 
 def _stale(target: Path, deps) -> bool:
@@ -49,15 +48,30 @@ def _stale(target: Path, deps) -> bool:
     return any(Path(d).stat().st_mtime > t for d in deps)
 
 
+def _includes(path: Path, seen=None) -> set:
+    """Project headers a source includes, directly or through other headers."""
+    seen = set() if seen is None else seen
+    for line in path.read_text().splitlines():
+        line = line.strip()
+        if line.startswith("#include \""):
+            name = line.split("\"")[1]
+            for d in (CSRC, PKG.parent / "include"):
+                h = d / name
+                if h.exists() and h not in seen:
+                    seen.add(h)
+                    _includes(h, seen)
+    return seen
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
-    hdrs = [CSRC / h for h in HEADERS] + [PKG.parent / "include" / "fclaw_b200.h", Path(__file__)]
     objs = []
     jobs = []
     for src, flags in SOURCES.items():
         obj = BUILD / (src + ".o")
         objs.append(obj)
-        if force or _stale(obj, [CSRC / src] + hdrs):
+        deps = [CSRC / src, Path(__file__), *sorted(_includes(CSRC / src))]
+        if force or _stale(obj, deps):
             cmd = [NVCC, *ARCH, *COMMON, *flags, "-c", str(CSRC / src), "-o", str(obj)]
             jobs.append(cmd)
 

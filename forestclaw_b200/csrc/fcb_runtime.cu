@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <thread>
+#include <exception>
 #include <cstring>
 #include <functional>
 #include <unordered_map>
@@ -117,7 +119,11 @@ double Context::read_cfl(const unsigned long long* d) {
 }
 
 Context::~Context() {
+    join_plans();
     cudaStreamSynchronize(st_);
+    if (upload_ev_) cudaEventDestroy(upload_ev_);
+    cudaFreeHost(h_ops_pinned_);
+    cudaFreeHost(h_groups_pinned_);
     drop_macro_graph();
     if (cap_st_) cudaStreamDestroy(cap_st_);
     cudaFreeHost(h_dyn_);
@@ -199,6 +205,7 @@ PatchMeta Context::meta_of(const Leaf& l) const {
 }
 
 void Context::mesh_changed() {
+    discard_plans();
     ++mesh_version_;
     drop_macro_graph();
     const int n = num_patches();
@@ -270,7 +277,7 @@ struct Touch {
 
 // fclaw2d_ghost_update_async (src/fclaw2d_ghost_fill.c:611-831) on one rank:
 // the records are emitted in the order the reference's callbacks run.
-void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>& ops) {
+void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>& ops) const {
     const int mx = opt_.mx, my = opt_.my;
     const int n = num_patches();
     std::vector<std::vector<int>> at((size_t)QuadForest::kMaxLevel + 1);
@@ -368,19 +375,21 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
     if (ti) setphysical(minlevel - 1, 1);
 }
 
-const GhostPlan& Context::plan(int minlevel, int maxlevel, int ti) {
-    auto key = std::make_tuple(minlevel, maxlevel, ti);
-    auto it = plans_.find(key);
-    if (it != plans_.end()) return it->second;
+// A plan's records in waves: each record goes one wave after the latest
+// earlier record it conflicts with (read-after-write, write-after-read,
+// write-after-write on overlapping cells of the same array), so the records of a
+// wave are independent and the waves keep the reference's order.
+Context::PlanBuild Context::build_plan(int minlevel, int maxlevel, int ti) const {
     std::vector<GhostOp> ops;
     build_ops(minlevel, maxlevel, ti, ops);
-    // Wave of each record: one more than the latest earlier record it
-    // conflicts with (read-after-write, write-after-read, write-after-write).
     const int mx = opt_.mx, my = opt_.my, mbc = opt_.mbc;
     const Rect whole{1 - mbc, mx + mbc, 1 - mbc, my + mbc};
     const Rect interior{1, mx, 1, my};
     std::vector<int> wave(ops.size(), 0);
-    std::unordered_map<int64_t, std::vector<std::pair<Touch, int>>> seen;
+    // writes and reads seen so far, per array (slot * 2 + time-interp flag):
+    // a read conflicts only with writes, a write with both
+    const size_t narr = (size_t)2 * std::max(1, capacity_);
+    std::vector<std::vector<std::pair<Rect, int>>> seen_w(narr), seen_r(narr);
     auto band = [&](int face) -> Rect {
         if (face == 0) return {1 - mbc, 0, 1, my};
         if (face == 1) return {mx + 1, mx + mbc, 1, my};
@@ -397,21 +406,21 @@ const GhostPlan& Context::plan(int minlevel, int maxlevel, int ti) {
     };
     for (size_t k = 0; k < ops.size(); ++k) {
         const GhostOp& o = ops[k];
-        std::vector<Touch> t;
+        Touch t[2];
         const int64_t kd = (int64_t)o.dst * 2 + o.dst_ti, ks = (int64_t)o.src * 2 + o.src_ti;
         switch (o.type) {
             case OP_COPY_FACE:
-                t.push_back({kd, band(o.face), true});
-                t.push_back({ks, shift(band(o.face), o.dx, o.dy), false});
+                t[0] = {kd, band(o.face), true};
+                t[1] = {ks, shift(band(o.face), o.dx, o.dy), false};
                 break;
             case OP_COPY_CORNER:
-                t.push_back({kd, corner(o.face), true});
-                t.push_back({ks, shift(corner(o.face), o.dx, o.dy), false});
+                t[0] = {kd, corner(o.face), true};
+                t[1] = {ks, shift(corner(o.face), o.dx, o.dy), false};
                 break;
             case OP_AVERAGE_FACE:
             case OP_AVERAGE_CORNER:
-                t.push_back({kd, o.type == OP_AVERAGE_FACE ? band(o.face) : corner(o.face), true});
-                t.push_back({ks, interior, false});
+                t[0] = {kd, o.type == OP_AVERAGE_FACE ? band(o.face) : corner(o.face), true};
+                t[1] = {ks, interior, false};
                 break;
             case OP_INTERP_FACE:
             case OP_INTERP_CORNER: {
@@ -426,67 +435,186 @@ const GhostPlan& Context::plan(int minlevel, int maxlevel, int ti) {
                     const int i0 = (o.face & 1) ? mx - mbc / 2 + 1 : 1, j0 = (o.face & 2) ? my - mbc / 2 + 1 : 1;
                     cb = {i0, i0 + mbc / 2 - 1, j0, j0 + mbc / 2 - 1};
                 }
-                t.push_back({ks, Rect{cb.i0 - 1, cb.i1 + 1, cb.j0 - 1, cb.j1 + 1}, false});
-                t.push_back({kd, clip(Rect{2 * cb.i0 + o.dx, 2 * cb.i1 + o.dx + 1, 2 * cb.j0 + o.dy, 2 * cb.j1 + o.dy + 1}), true});
+                t[0] = {ks, Rect{cb.i0 - 1, cb.i1 + 1, cb.j0 - 1, cb.j1 + 1}, false};
+                t[1] = {kd, clip(Rect{2 * cb.i0 + o.dx, 2 * cb.i1 + o.dx + 1, 2 * cb.j0 + o.dy, 2 * cb.j1 + o.dy + 1}), true};
                 break;
             }
-            case OP_PHYSBC:
-                t.push_back({kd, whole, true});
-                t.push_back({kd, whole, false});
+            default:  // OP_PHYSBC: reads and writes the whole array
+                t[0] = {kd, whole, true};
+                t[1] = {kd, whole, false};
                 break;
         }
         int w = 0;
         for (const Touch& a : t) {
-            auto f = seen.find(a.key);
-            if (f == seen.end()) continue;
-            for (const auto& pr : f->second) {
-                const Touch& b = pr.first;
-                if ((a.write || b.write) && a.r.hits(b.r)) w = std::max(w, pr.second + 1);
-            }
+            for (const auto& pr : seen_w[(size_t)a.key])
+                if (pr.second >= w && a.r.hits(pr.first)) w = pr.second + 1;
+            if (a.write)
+                for (const auto& pr : seen_r[(size_t)a.key])
+                    if (pr.second >= w && a.r.hits(pr.first)) w = pr.second + 1;
         }
         wave[k] = w;
-        for (const Touch& a : t) seen[a.key].push_back({a, w});
+        for (const Touch& a : t) (a.write ? seen_w : seen_r)[(size_t)a.key].push_back({a.r, w});
     }
     const int nw = ops.empty() ? 0 : *std::max_element(wave.begin(), wave.end()) + 1;
-    GhostPlan g;
-    g.first = h_ops_.size();
-    g.wave_begin.assign(nw + 1, 0);
+    PlanBuild b;
+    b.wave_begin.assign(nw + 1, 0);
     std::vector<int> count(nw, 0);
     for (int w : wave) ++count[w];
-    for (int w = 0; w < nw; ++w) g.wave_begin[w + 1] = g.wave_begin[w] + count[w];
-    std::vector<GhostOp> sorted(ops.size());
-    std::vector<int> pos(g.wave_begin.begin(), g.wave_begin.end() - (nw ? 1 : 0));
-    for (size_t k = 0; k < ops.size(); ++k) sorted[pos[wave[k]]++] = ops[k];
+    for (int w = 0; w < nw; ++w) b.wave_begin[w + 1] = b.wave_begin[w] + count[w];
+    b.ops.resize(ops.size());
+    std::vector<int> pos(b.wave_begin.begin(), b.wave_begin.end() - (nw ? 1 : 0));
+    for (size_t k = 0; k < ops.size(); ++k) b.ops[pos[wave[k]]++] = ops[k];
     // within a wave, records with the same destination patch form one group
-    g.first_group = h_groups_.size();
-    g.group_begin.assign(nw + 1, 0);
+    b.group_begin.assign(nw + 1, 0);
     for (int w = 0; w < nw; ++w) {
-        auto b = sorted.begin() + g.wave_begin[w], e = sorted.begin() + g.wave_begin[w + 1];
-        std::stable_sort(b, e, [](const GhostOp& x, const GhostOp& y) { return x.dst < y.dst; });
-        g.group_begin[w] = (int)(h_groups_.size() - g.first_group);
-        for (int k = g.wave_begin[w]; k < g.wave_begin[w + 1]; ++k)
-            if (k == g.wave_begin[w] || sorted[k].dst != sorted[k - 1].dst)
-                h_groups_.push_back((int32_t)(g.first + k));
-        h_groups_.push_back((int32_t)(g.first + g.wave_begin[w + 1]));  // end marker of the wave
+        auto first = b.ops.begin() + b.wave_begin[w], last = b.ops.begin() + b.wave_begin[w + 1];
+        std::stable_sort(first, last, [](const GhostOp& x, const GhostOp& y) { return x.dst < y.dst; });
+        b.group_begin[w] = (int)b.groups.size();
+        for (int k = b.wave_begin[w]; k < b.wave_begin[w + 1]; ++k)
+            if (k == b.wave_begin[w] || b.ops[k].dst != b.ops[k - 1].dst) b.groups.push_back(k);
+        b.groups.push_back(b.wave_begin[w + 1]);  // end marker of the wave
     }
-    g.group_begin[nw] = (int)(h_groups_.size() - g.first_group);
-    h_ops_.insert(h_ops_.end(), sorted.begin(), sorted.end());
+    b.group_begin[nw] = (int)b.groups.size();
+    return b;
+}
+
+const GhostPlan& Context::commit_plan(const std::tuple<int, int, int>& key, PlanBuild&& b) {
+    GhostPlan g;
+    g.first = h_ops_.size();
+    g.first_group = h_groups_.size();
+    g.wave_begin = std::move(b.wave_begin);
+    g.group_begin = std::move(b.group_begin);
+    for (int32_t k : b.groups) h_groups_.push_back((int32_t)(g.first + k));
+    h_ops_.insert(h_ops_.end(), b.ops.begin(), b.ops.end());
     ops_dirty_ = true;
     return plans_.emplace(key, std::move(g)).first->second;
 }
 
-void Context::run_plan(const GhostPlan& g) {
-    if (ops_dirty_) {
-        d_ops_.reserve(std::max<size_t>(1, h_ops_.size()));
-        d_groups_.reserve(std::max<size_t>(1, h_groups_.size()));
-        check(cudaStreamSynchronize(st_), "sync");
-        if (!h_ops_.empty())
-            check(cudaMemcpy(d_ops_.p, h_ops_.data(), h_ops_.size() * sizeof(GhostOp), cudaMemcpyHostToDevice), "ops");
-        if (!h_groups_.empty())
-            check(cudaMemcpy(d_groups_.p, h_groups_.data(), h_groups_.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
-                  "groups");
-        ops_dirty_ = false;
+const GhostPlan& Context::plan(int minlevel, int maxlevel, int ti) {
+    const auto key = std::make_tuple(minlevel, maxlevel, ti);
+    auto it = plans_.find(key);
+    if (it != plans_.end()) return it->second;
+    if (!plan_todo_.empty()) {
+        finish_plans();
+        it = plans_.find(key);
+        if (it != plans_.end()) return it->second;
     }
+    return commit_plan(key, build_plan(minlevel, maxlevel, ti));
+}
+
+void Context::start_plans(const std::vector<std::tuple<int, int, int>>& keys) {
+    finish_plans();
+    for (const auto& k : keys)
+        if (!plans_.count(k) && std::find(plan_todo_.begin(), plan_todo_.end(), k) == plan_todo_.end())
+            plan_todo_.push_back(k);
+    if (plan_todo_.empty()) return;
+    plan_built_.assign(plan_todo_.size(), PlanBuild{});
+    plan_err_.assign(plan_todo_.size(), nullptr);
+    // the builds only read the forest, neighbour tables, slot map and options
+    for (size_t k = 0; k < plan_todo_.size(); ++k)
+        plan_threads_.emplace_back([this, k] {
+            try {
+                const auto& t = plan_todo_[k];
+                plan_built_[k] = build_plan(std::get<0>(t), std::get<1>(t), std::get<2>(t));
+            } catch (...) {
+                plan_err_[k] = std::current_exception();
+            }
+        });
+}
+
+// Starts the builds of the ghost plans that one macro step uses on the current
+// mesh (the keys come from a dry run of the schedule, which launches nothing)
+// and of the full ghost update.  The next plan() that needs any of them waits
+// for all.
+void Context::prefetch_plans() {
+    const bool dyn0 = use_dyn_;
+    const int n0 = dyn_n_;
+    use_dyn_ = true;
+    dry_ = true;
+    dyn_n_ = 0;
+    dry_plan_keys_.clear();
+    try {
+        run_schedule(curr_time_, 1.0);
+    } catch (...) {
+        dry_ = false;
+        use_dyn_ = dyn0;
+        dyn_n_ = n0;
+        throw;
+    }
+    dry_ = false;
+    use_dyn_ = dyn0;
+    dyn_n_ = n0;
+    dry_plan_keys_.emplace_back(gmin_, gmax_, 0);
+    start_plans(dry_plan_keys_);
+}
+
+void Context::discard_plans() noexcept {
+    join_plans();
+    plan_todo_.clear();
+    plan_built_.clear();
+    plan_err_.clear();
+}
+
+void Context::join_plans() noexcept {
+    for (auto& t : plan_threads_)
+        if (t.joinable()) t.join();
+    plan_threads_.clear();
+}
+
+void Context::finish_plans() {
+    join_plans();
+    if (plan_todo_.empty()) return;
+    std::exception_ptr err;
+    for (size_t k = 0; k < plan_todo_.size(); ++k) {
+        if (plan_err_[k]) {
+            if (!err) err = plan_err_[k];
+            continue;
+        }
+        if (!plans_.count(plan_todo_[k])) commit_plan(plan_todo_[k], std::move(plan_built_[k]));
+    }
+    plan_todo_.clear();
+    plan_built_.clear();
+    plan_err_.clear();
+    if (err) std::rethrow_exception(err);
+}
+
+// Copies the op and group buffers to the device through pinned staging, in
+// stream order (ghost launches already queued read the old contents first).
+void Context::upload_ops() {
+    if (upload_ev_) check(cudaEventSynchronize(upload_ev_), "ops upload");  // staging free again
+    else check(cudaEventCreateWithFlags(&upload_ev_, cudaEventDisableTiming), "cudaEventCreate");
+    if (h_ops_.size() > h_ops_pinned_cap_) {
+        cudaFreeHost(h_ops_pinned_);
+        h_ops_pinned_ = nullptr;
+        h_ops_pinned_cap_ = std::max(h_ops_.size(), 2 * h_ops_pinned_cap_);
+        check(cudaHostAlloc(&h_ops_pinned_, h_ops_pinned_cap_ * sizeof(GhostOp), cudaHostAllocDefault), "host ops");
+    }
+    if (h_groups_.size() > h_groups_pinned_cap_) {
+        cudaFreeHost(h_groups_pinned_);
+        h_groups_pinned_ = nullptr;
+        h_groups_pinned_cap_ = std::max(h_groups_.size(), 2 * h_groups_pinned_cap_);
+        check(cudaHostAlloc(&h_groups_pinned_, h_groups_pinned_cap_ * sizeof(int32_t), cudaHostAllocDefault),
+              "host groups");
+    }
+    d_ops_.reserve(std::max<size_t>(1, h_ops_.size()));
+    d_groups_.reserve(std::max<size_t>(1, h_groups_.size()));
+    if (!h_ops_.empty()) {
+        std::memcpy(h_ops_pinned_, h_ops_.data(), h_ops_.size() * sizeof(GhostOp));
+        check(cudaMemcpyAsync(d_ops_.p, h_ops_pinned_, h_ops_.size() * sizeof(GhostOp), cudaMemcpyHostToDevice, st_),
+              "ops");
+    }
+    if (!h_groups_.empty()) {
+        std::memcpy(h_groups_pinned_, h_groups_.data(), h_groups_.size() * sizeof(int32_t));
+        check(cudaMemcpyAsync(d_groups_.p, h_groups_pinned_, h_groups_.size() * sizeof(int32_t),
+                              cudaMemcpyHostToDevice, st_),
+              "groups");
+    }
+    check(cudaEventRecord(upload_ev_, st_), "cudaEventRecord");
+    ops_dirty_ = false;
+}
+
+void Context::run_plan(const GhostPlan& g) {
+    if (ops_dirty_) upload_ops();
     ghost_unroll_ = opt_.step_variant == 0 ? tune_ghost_unroll(g) : 4;
     const int nw = (int)g.wave_begin.size() - 1;
     for (int w = 0; w < nw; ++w) {
@@ -507,7 +635,10 @@ void Context::run_plan(const GhostPlan& g) {
 
 void Context::ghost_update(int minlevel, int maxlevel, double, int time_interp) {
     if (!d_q_) throw Error(FCB_ERR_STATE, "ghost_update before initialize");
-    if (dry_) return;
+    if (dry_) {
+        dry_plan_keys_.emplace_back(minlevel, maxlevel, time_interp);
+        return;
+    }
     run_plan(plan(minlevel, maxlevel, time_interp));
 }
 
@@ -740,10 +871,19 @@ void Context::drop_macro_graph() {
 // to fill the {dt, vt} table that the step launches read.
 double Context::advance_all_levels(double t_curr, double dt) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "advance before initialize");
+    // on an error, plan builds still running are joined and dropped
+    struct PlanGuard {
+        Context* c;
+        bool armed = true;
+        ~PlanGuard() {
+            if (armed) c->discard_plans();
+        }
+    } plans_guard{this};
     use_dyn_ = opt_.macro_graph != 0;
     if (use_dyn_) {
         dyn_n_ = 0;
         dry_ = true;
+        dry_plan_keys_.clear();
         try {
             run_schedule(t_curr, dt);
         } catch (...) {
@@ -751,6 +891,10 @@ double Context::advance_all_levels(double t_curr, double dt) {
             throw;
         }
         dry_ = false;
+        // the ghost plans of this macro step that do not exist yet (after a
+        // regrid, none) are built on host threads while the first level
+        // updates run
+        start_plans(dry_plan_keys_);
         // auto: the graph, whenever the macro step has a level update (a replay
         // beats host launches even for the three launches of one level)
         if (opt_.macro_graph == 2 && dyn_n_ < 1) use_dyn_ = false;
@@ -814,6 +958,8 @@ double Context::advance_all_levels(double t_curr, double dt) {
         run_schedule(t_curr, dt);
     }
     use_dyn_ = false;
+    finish_plans();
+    plans_guard.armed = false;
     ++cnt_.count_amr_advance;
     return read_cfl(d_cfl_);
 }
@@ -1247,6 +1393,7 @@ bool Context::regrid() {
         forest_.leaves = nl;
         repopulate(old, old_slots, false);
         mesh_changed();
+        prefetch_plans();  // this update's plan and the next macro step's, built together
         ghost_update(forest_.min_level(), forest_.max_level(), curr_time_, 0);
         ++cnt_.count_amr_new_domain;
     }

@@ -9,6 +9,8 @@
 #include <string>
 #include <tuple>
 #include <vector>
+#include <thread>
+#include <exception>
 
 #include "../../include/fclaw_b200.h"
 #include "fcb_device.h"
@@ -127,7 +129,37 @@ class Context {
     PatchMeta meta_of(const Leaf& l) const;
     // --- ghost plans ---
     const GhostPlan& plan(int minlevel, int maxlevel, int time_interp);
-    void build_ops(int minlevel, int maxlevel, int time_interp, std::vector<GhostOp>& ops);
+    void build_ops(int minlevel, int maxlevel, int time_interp, std::vector<GhostOp>& ops) const;
+    // A ghost plan before it is appended to the context's op buffer: records in
+    // wave order, wave offsets, and the group starts of each wave (relative).
+    struct PlanBuild {
+        std::vector<GhostOp> ops;
+        std::vector<int> wave_begin, group_begin;
+        std::vector<int32_t> groups;
+    };
+    PlanBuild build_plan(int minlevel, int maxlevel, int time_interp) const;
+    const GhostPlan& commit_plan(const std::tuple<int, int, int>& key, PlanBuild&& b);
+    // Missing plans of a macro step are built on host threads while its first
+    // level updates run on the GPU; plan() waits for them.  Every build ends
+    // (finish_plans) before advance_all_levels returns, so no build outlives a
+    // call that may change the forest.
+    void start_plans(const std::vector<std::tuple<int, int, int>>& keys);
+    void finish_plans();
+    void join_plans() noexcept;
+    void discard_plans() noexcept;
+    void prefetch_plans();
+    void upload_ops();
+    std::vector<std::tuple<int, int, int>> dry_plan_keys_;  // plans the dry pass met
+    std::vector<std::tuple<int, int, int>> plan_todo_;
+    std::vector<PlanBuild> plan_built_;
+    std::vector<std::exception_ptr> plan_err_;
+    std::vector<std::thread> plan_threads_;
+    // pinned staging of the op and group buffers, and the event of its last upload
+    GhostOp* h_ops_pinned_ = nullptr;
+    size_t h_ops_pinned_cap_ = 0;
+    int32_t* h_groups_pinned_ = nullptr;
+    size_t h_groups_pinned_cap_ = 0;
+    cudaEvent_t upload_ev_ = nullptr;
     void run_plan(const GhostPlan& g);
     // --- regrid helpers ---
     void tag(bool domain_init, std::vector<int>& target);

@@ -502,14 +502,21 @@ cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// CTA size: the Roe systems run at the register limit (255 per thread), one
+// 256-thread CTA per SM, which packs 7 patches of mx = 32 (252 of 256 threads
+// busy) where 128 threads held 3 (108 busy) and left the last CTAs of a level
+// as a second wave; 1.4-1.65x faster on levels of 1,024 patches of mx = 32.
+// Scalar advection keeps 128 threads (its per-patch aux and stream-function
+// tables would not fit 256 threads' worth of patches of mx = 64 in shared memory).
 template <class SOL, int AUXK, int NAUX>
 cudaError_t launch_mx(int mx, int mbc, const StepArgs& a, cudaStream_t st) {
+    constexpr int TPB = SOL::M > 1 ? 256 : 128;
     if (mbc != 2) return cudaErrorInvalidValue;
     switch (mx) {
-        case 8: return launch_one<SOL, 8, 2, AUXK, NAUX, 128>(a, st);
-        case 16: return launch_one<SOL, 16, 2, AUXK, NAUX, 128>(a, st);
-        case 32: return launch_one<SOL, 32, 2, AUXK, NAUX, 128>(a, st);
-        case 64: return launch_one<SOL, 64, 2, AUXK, NAUX, 128>(a, st);
+        case 8: return launch_one<SOL, 8, 2, AUXK, NAUX, TPB>(a, st);
+        case 16: return launch_one<SOL, 16, 2, AUXK, NAUX, TPB>(a, st);
+        case 32: return launch_one<SOL, 32, 2, AUXK, NAUX, TPB>(a, st);
+        case 64: return launch_one<SOL, 64, 2, AUXK, NAUX, TPB>(a, st);
         default: return cudaErrorInvalidValue;
     }
 }
