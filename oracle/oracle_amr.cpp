@@ -148,17 +148,19 @@ Solver::Solver(const Options& o) : opt(o) {}
 
 double Solver::xlower(int p) const { return (double)forest.leaves[p].x / (double)Forest::kRoot; }
 double Solver::ylower(int p) const { return (double)forest.leaves[p].y / (double)Forest::kRoot; }
+// fclaw2d_clawpatch.cpp clawpatch_define (no mapping): physical corner
+// ax + (bx-ax)*x of the block coordinate, dx = (xupper - xlower)/mx.
+double Solver::xphys(int p) const { return opt.ax + (opt.bx - opt.ax) * xlower(p); }
+double Solver::yphys(int p) const { return opt.ay + (opt.by - opt.ay) * ylower(p); }
 double Solver::dx(int p) const {
     const double xl = xlower(p);
     const double xu = (double)(forest.leaves[p].x + Forest::h(forest.leaves[p].level)) / (double)Forest::kRoot;
-    const double ax = 0.0, bx = 1.0;
-    return ((ax + (bx - ax) * xu) - (ax + (bx - ax) * xl)) / opt.mx;
+    return ((opt.ax + (opt.bx - opt.ax) * xu) - (opt.ax + (opt.bx - opt.ax) * xl)) / opt.mx;
 }
 double Solver::dy(int p) const {
     const double yl = ylower(p);
     const double yu = (double)(forest.leaves[p].y + Forest::h(forest.leaves[p].level)) / (double)Forest::kRoot;
-    const double ay = 0.0, by = 1.0;
-    return ((ay + (by - ay) * yu) - (ay + (by - ay) * yl)) / opt.my;
+    return ((opt.ay + (opt.by - opt.ay) * yu) - (opt.ay + (opt.by - opt.ay) * yl)) / opt.my;
 }
 PatchGeom Solver::geom(int p) const { return PatchGeom{xlower(p), ylower(p), forest.leaves[p].level}; }
 
@@ -180,6 +182,16 @@ void Solver::build_patch(int p, bool) {
     d.qinterp.assign(patch_size(), 0.0);
     d.qsave.assign(patch_size(), 0.0);
     d.aux.assign(aux_size(), 0.0);
+    // fclaw2d_clawpatch_time_sync_new: zeroed registers on every new patch
+    const size_t ny = (size_t)opt.my * opt.meqn, nx = (size_t)opt.mx * opt.meqn;
+    for (int k = 0; k < 2; ++k) {
+        d.reg.fp[k].assign(ny, 0.0);
+        d.reg.fm[k].assign(ny, 0.0);
+        d.reg.gp[k].assign(nx, 0.0);
+        d.reg.gm[k].assign(nx, 0.0);
+        d.reg.ef[k].assign(2 * ny, 0.0);
+        d.reg.ef[k + 2].assign(2 * nx, 0.0);
+    }
 }
 
 void Solver::qinit_patch(int p) {
@@ -187,19 +199,24 @@ void Solver::qinit_patch(int p) {
     double* q = data[p].q.data();
     switch (opt.problem) {
         case PROB_SWIRL:
-            qinit_swirl(opt.mx, opt.my, opt.mbc, opt.meqn, xlower(p), ylower(p), dx(p), dy(p), q);
+            qinit_swirl(opt.mx, opt.my, opt.mbc, opt.meqn, xphys(p), yphys(p), dx(p), dy(p), q);
             break;
         case PROB_RADIALDAM:
-            qinit_radialdam(opt.mx, opt.my, opt.mbc, xlower(p), ylower(p), dx(p), dy(p), pp[0], pp[1],
+            qinit_radialdam(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), pp[0], pp[1],
                             pp[2], pp[3], pp[4], q);
+            break;
+        case PROB_RADIALDAM_CELLAVE:
+            // pparams: x0, y0, r0, hin, hout
+            qinit_radialdam_cellave(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), pp[0], pp[1],
+                                    pp[2], pp[3], pp[4], q);
             break;
         case PROB_QUADRANTS:
             // pparams: rho[4], u[4], v[4], p[4], xs, ys
-            qinit_quadrants(opt.mx, opt.my, opt.mbc, xlower(p), ylower(p), dx(p), dy(p),
+            qinit_quadrants(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p),
                             opt.solver.gamma1, pp + 0, pp + 4, pp + 8, pp + 12, pp[16], pp[17], q);
             break;
         case PROB_BATHY:
-            qinit_bathy(opt.mx, opt.my, opt.mbc, xlower(p), ylower(p), dx(p), dy(p), pp, q);
+            qinit_bathy(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), pp, q);
             break;
         default: throw std::runtime_error("unknown problem");
     }
@@ -209,18 +226,380 @@ void Solver::qinit_patch(int p) {
 // it from the formula (no transfer from its parent or children).
 void Solver::setaux_patch(int p) {
     if (opt.problem == PROB_BATHY)
-        setaux_bathy(opt.mx, opt.my, opt.mbc, xlower(p), ylower(p), dx(p), dy(p), data[p].aux.data());
+        setaux_bathy(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), data[p].aux.data());
 }
 
 // clawpack46_update (fc2d_clawpack46.cpp:403-444) for one patch.
 double Solver::single_step_patch(int p, double t, double dt) {
     PatchData& d = data[p];
     if (opt.problem == PROB_SWIRL)
-        b4step2_swirl(opt.mx, opt.my, opt.mbc, opt.maux, xlower(p), ylower(p), dx(p), dy(p), t, dt,
+        b4step2_swirl(opt.mx, opt.my, opt.mbc, opt.maux, xphys(p), yphys(p), dx(p), dy(p), t, dt,
                       opt.pparams[0], d.aux.data());
     d.qlast = d.q;  // fclaw2d_clawpatch_save_current_step
-    return step2(opt.solver, opt.method, opt.mx, opt.my, opt.mbc, opt.meqn, opt.maux, d.q.data(),
-                 opt.maux > 0 ? d.aux.data() : nullptr, dx(p), dy(p), dt);
+    if (!opt.time_sync)
+        return step2(opt.solver, opt.method, opt.mx, opt.my, opt.mbc, opt.meqn, opt.maux, d.q.data(),
+                     opt.maux > 0 ? d.aux.data() : nullptr, dx(p), dy(p), dt);
+    // clawpack46_step2 (fc2d_clawpack46.cpp:316-386): fluxes f(q) at the patch
+    // edges before the update, boundary fluctuations after it
+    time_sync_store_flux(p, dt);
+    StepFluxArrays f;
+    const double cfl = step2(opt.solver, opt.method, opt.mx, opt.my, opt.mbc, opt.meqn, opt.maux, d.q.data(),
+                             opt.maux > 0 ? d.aux.data() : nullptr, dx(p), dy(p), dt, &f);
+    time_sync_accumulate(p, dt, f);
+    return cfl;
+}
+
+// --------------------------------------------------------------------------
+// Conservative time synchronisation
+// --------------------------------------------------------------------------
+
+// clawpack46_time_sync.f:37-157 (clawpack46_time_sync_store_flux) with the
+// shallow-water rpn2_cons_update; edge lengths dy (x faces) and dx (y faces)
+// (clawpatch_time_sync_setup, fclaw2d_clawpatch_utils.f:259-310, no manifold).
+void Solver::time_sync_store_flux(int p, double dt) {
+    if (opt.solver.kind != SOLVER_SWE_ROE) throw std::runtime_error("time-sync: rpn2_cons for shallow water only");
+    if (opt.method.version != 4) throw std::runtime_error("time-sync: clawpack 4.6 registers only");
+    const int mx = opt.mx, my = opt.my, mbc = opt.mbc, meqn = opt.meqn;
+    const PatchIdx P(mx, my, mbc);
+    PatchData& d = data[p];
+    const double* q = d.q.data();
+    const double el_x = dy(p), el_y = dx(p);
+    double qv[8], fl[8];
+    auto cons = [&](int i, int j, int idir) {
+        for (int m = 0; m < meqn; ++m) qv[m] = q[P(i, j, m)];
+        rpn2_cons_update_swe(meqn, idir, qv, opt.solver.grav, fl);
+    };
+    for (int j = 1; j <= my; ++j) {
+        for (int k = 0; k <= 1; ++k) {
+            cons(1 - k, j, 0);
+            for (int m = 0; m < meqn; ++m) {
+                double& r = d.reg.ef[0][(j - 1) + my * (m + meqn * k)];
+                r = r + (dt * el_x) * fl[m];
+            }
+        }
+        for (int k = 0; k <= 1; ++k) {
+            cons(mx + k, j, 0);
+            for (int m = 0; m < meqn; ++m) {
+                double& r = d.reg.ef[1][(j - 1) + my * (m + meqn * k)];
+                r = r + (dt * el_x) * fl[m];
+            }
+        }
+    }
+    for (int i = 1; i <= mx; ++i) {
+        for (int k = 0; k <= 1; ++k) {
+            cons(i, 1 - k, 1);
+            for (int m = 0; m < meqn; ++m) {
+                double& r = d.reg.ef[2][(i - 1) + mx * (m + meqn * k)];
+                r = r + (dt * el_y) * fl[m];
+            }
+        }
+        for (int k = 0; k <= 1; ++k) {
+            cons(i, my + k, 1);
+            for (int m = 0; m < meqn; ++m) {
+                double& r = d.reg.ef[3][(i - 1) + mx * (m + meqn * k)];
+                r = r + (dt * el_y) * fl[m];
+            }
+        }
+    }
+}
+
+// clawpack46_time_sync.f:163-243 (clawpack46_time_sync_accumulate_waves)
+void Solver::time_sync_accumulate(int p, double dt, const StepFluxArrays& f) {
+    const int mx = opt.mx, my = opt.my, mbc = opt.mbc, meqn = opt.meqn;
+    const PatchIdx P(mx, my, mbc);
+    Registers& r = data[p].reg;
+    const double dtdy = dt * dy(p), dtdx = dt * dx(p);
+    for (int j = 1; j <= my; ++j)
+        for (int m = 0; m < meqn; ++m) {
+            const int k = (j - 1) + my * m;
+            r.fp[0][k] = r.fp[0][k] - dtdy * f.fp[P(1, j, m)];
+            r.fm[0][k] = r.fm[0][k] + dtdy * f.fm[P(1, j, m)];
+            r.fp[1][k] = r.fp[1][k] - dtdy * f.fp[P(mx + 1, j, m)];
+            r.fm[1][k] = r.fm[1][k] + dtdy * f.fm[P(mx + 1, j, m)];
+        }
+    for (int i = 1; i <= mx; ++i)
+        for (int m = 0; m < meqn; ++m) {
+            const int k = (i - 1) + mx * m;
+            r.gp[0][k] = r.gp[0][k] - dtdx * f.gp[P(i, 1, m)];
+            r.gm[0][k] = r.gm[0][k] + dtdx * f.gm[P(i, 1, m)];
+            r.gp[1][k] = r.gp[1][k] - dtdx * f.gp[P(i, my + 1, m)];
+            r.gm[1][k] = r.gm[1][k] + dtdx * f.gm[P(i, my + 1, m)];
+        }
+}
+
+namespace {
+// clawpack46_time_sync.f fc46_is_valid_correct / fc46_skip_this_grid
+bool skip_this_grid(const int i2[4], const int j2[4], int mx, int my) {
+    for (int m = 0; m < 4; ++m) {
+        const bool iv = 1 <= i2[m] && i2[m] <= mx, jv = 1 <= j2[m] && j2[m] <= my;
+        if (!(iv != jv)) return true;
+    }
+    return false;
+}
+}  // namespace
+
+// fclaw2d_clawpatch_time_sync_samesize (fclaw2d_clawpatch_conservation.c:410-470)
+// -> clawpack46_fort_time_sync_samesize (clawpack46_time_sync.f:528-700):
+// half of the mismatch between this patch's registers and its same-size
+// neighbour's goes into this patch's edge cells.
+void Solver::time_sync_samesize(int p, int iface) {
+    const int mx = opt.mx, my = opt.my, mbc = opt.mbc, meqn = opt.meqn;
+    const int n = nbrs[p].face_nbr[iface][0];
+    const PatchIdx P(mx, my, mbc);
+    const Transform t{geom(p), geom(n), mx, my};
+    int a[2][2], f[2];
+    build_transform_same(t, a, f);
+    const Registers& rt = data[p].reg;
+    const Registers& rn = data[n].reg;
+    std::vector<double> dum((size_t)P.size(meqn), 0.0);
+    for (int mq = 0; mq < meqn; ++mq) {
+        for (int j = 1; j <= my; ++j) {
+            const int k = (j - 1) + my * mq;
+            dum[P(0, j, mq)] = rn.fm[0][k];
+            dum[P(-1, j, mq)] = rn.ef[0][k + my * meqn];
+            dum[P(mx + 1, j, mq)] = rn.fp[1][k];
+            dum[P(mx + 2, j, mq)] = rn.ef[1][k + my * meqn];
+        }
+        for (int i = 1; i <= mx; ++i) {
+            const int k = (i - 1) + mx * mq;
+            dum[P(i, 0, mq)] = rn.gm[0][k];
+            dum[P(i, -1, mq)] = rn.ef[2][k + mx * meqn];
+            dum[P(i, my + 1, mq)] = rn.gp[1][k];
+            dum[P(i, my + 2, mq)] = rn.ef[3][k + mx * meqn];
+        }
+    }
+    double* q = data[p].q.data();
+    const double area = dx(p) * dy(p);
+    const int idir = iface / 2;
+    int i2, j2;
+    if (idir == 0) {
+        const int sc = a[0][0] + a[1][0];
+        for (int mq = 0; mq < meqn; ++mq)
+            for (int j = 1; j <= my; ++j) {
+                const int k = (j - 1) + my * mq;
+                int i1 = 1;
+                double delta;
+                if (iface == 0) {
+                    t.face(i1, j, i2, j2);
+                    const double fpv = dum[P(i2, j2, mq)];
+                    t.face(i1 + 1, j, i2, j2);
+                    const double ef = (double)sc * dum[P(i2, j2, mq)];
+                    delta = (ef - rt.ef[0][k]) - (fpv - rt.fp[0][k]);
+                } else {
+                    i1 = mx;
+                    t.face(i1, j, i2, j2);
+                    const double fmv = dum[P(i2, j2, mq)];
+                    t.face(i1 - 1, j, i2, j2);
+                    const double ef = (double)sc * dum[P(i2, j2, mq)];
+                    delta = (rt.ef[1][k] - ef) - (fmv - rt.fm[1][k]);
+                }
+                q[P(i1, j, mq)] = q[P(i1, j, mq)] + (0.5 * delta) / area;
+            }
+    } else {
+        const int sc = a[0][1] + a[1][1];
+        for (int mq = 0; mq < meqn; ++mq)
+            for (int i = 1; i <= mx; ++i) {
+                const int k = (i - 1) + mx * mq;
+                int j1 = 1;
+                double delta;
+                if (iface == 2) {
+                    t.face(i, j1, i2, j2);
+                    const double gpv = dum[P(i2, j2, mq)];
+                    t.face(i, j1 + 1, i2, j2);
+                    const double ef = (double)sc * dum[P(i2, j2, mq)];
+                    delta = (ef - rt.ef[2][k]) - (gpv - rt.gp[0][k]);
+                } else {
+                    j1 = my;
+                    t.face(i, j1, i2, j2);
+                    const double gmv = dum[P(i2, j2, mq)];
+                    t.face(i, j1 - 1, i2, j2);
+                    const double ef = (double)sc * dum[P(i2, j2, mq)];
+                    delta = (rt.ef[3][k] - ef) - (gmv - rt.gm[1][k]);
+                }
+                q[P(i, j1, mq)] = q[P(i, j1, mq)] + (0.5 * delta) / area;
+            }
+    }
+}
+
+// fclaw2d_clawpatch_time_sync_f2c (fclaw2d_clawpatch_conservation.c:344-405)
+// -> clawpack46_fort_time_sync_f2c (clawpack46_time_sync.f:254-520): the fine
+// patch's registers, summed over pairs of fine edge cells, replace the coarse
+// patch's along the shared face.
+void Solver::time_sync_f2c(int pc, int pf, int iface) {
+    const int mx = opt.mx, my = opt.my, mbc = opt.mbc, meqn = opt.meqn;
+    const PatchIdx P(mx, my, mbc);
+    const int nx2 = mx + 4 * mbc, ny2 = my + 4 * mbc;
+    // qfine_dummy(1-2mbc:mx+2mbc, 1-2mbc:my+2mbc, meqn)
+    std::vector<double> dum((size_t)nx2 * ny2 * meqn, 0.0);
+    auto D = [&](int i, int j, int m) -> double& {
+        return dum[((size_t)m * ny2 + (j + 2 * mbc - 1)) * nx2 + (i + 2 * mbc - 1)];
+    };
+    const Transform t{geom(pc), geom(pf), mx, my};
+    int a[2][2], f[2];
+    build_transform_half(t, a, f);
+    const Registers& rc = data[pc].reg;
+    const Registers& rf = data[pf].reg;
+    for (int mq = 0; mq < meqn; ++mq) {
+        for (int j = 1; j <= my / 2; ++j) {
+            const int jj1 = 2 * (j - 1) + 1, jj2 = 2 * (j - 1) + 2;
+            const int k1 = (jj1 - 1) + my * mq, k2 = (jj2 - 1) + my * mq;
+            double fm = rf.fm[0][k1] + rf.fm[0][k2];
+            double ef = rf.ef[0][k1 + my * meqn] + rf.ef[0][k2 + my * meqn];
+            for (int jj = jj1; jj <= jj2; ++jj)
+                for (int ii = -1; ii <= 0; ++ii) {
+                    D(ii, jj, mq) = fm;
+                    D(ii - 2, jj, mq) = ef;
+                }
+            const double fp = rf.fp[1][k1] + rf.fp[1][k2];
+            ef = rf.ef[1][k1 + my * meqn] + rf.ef[1][k2 + my * meqn];
+            for (int jj = jj1; jj <= jj2; ++jj)
+                for (int ii = 1; ii <= 2; ++ii) {
+                    D(mx + ii, jj, mq) = fp;
+                    D(mx + ii + 2, jj, mq) = ef;
+                }
+        }
+        for (int i = 1; i <= mx / 2; ++i) {
+            const int ii1 = 2 * (i - 1) + 1, ii2 = 2 * (i - 1) + 2;
+            const int k1 = (ii1 - 1) + mx * mq, k2 = (ii2 - 1) + mx * mq;
+            const double gm = rf.gm[0][k1] + rf.gm[0][k2];
+            double ef = rf.ef[2][k1 + mx * meqn] + rf.ef[2][k2 + mx * meqn];
+            for (int ii = ii1; ii <= ii2; ++ii)
+                for (int jj = -1; jj <= 0; ++jj) {
+                    D(ii, jj, mq) = gm;
+                    D(ii, jj - 2, mq) = ef;
+                }
+            const double gp = rf.gp[1][k1] + rf.gp[1][k2];
+            ef = rf.ef[3][k1 + mx * meqn] + rf.ef[3][k2 + mx * meqn];
+            for (int ii = ii1; ii <= ii2; ++ii)
+                for (int jj = 1; jj <= 2; ++jj) {
+                    D(ii, my + jj, mq) = gp;
+                    D(ii, my + jj + 2, mq) = ef;
+                }
+        }
+    }
+    double* q = data[pc].q.data();
+    const double areac_v = dx(pc) * dy(pc);
+    const int idir = iface / 2;
+    int i2[4], j2[4];
+    if (idir == 0) {
+        const int sc = (a[0][0] + a[1][0]) / 2;
+        for (int mq = 0; mq < meqn; ++mq)
+            for (int jc = 1; jc <= my; ++jc) {
+                const int k = (jc - 1) + my * mq;
+                int ic = 1;
+                double deltac = 0;
+                double areac = 1;
+                if (iface == 0) {
+                    ic = 1;
+                    t.face_half(ic, jc, i2, j2);
+                    deltac = 0;
+                    areac = areac_v;
+                    if (!skip_this_grid(i2, j2, mx, my)) {
+                        const double fp = D(i2[0], j2[0], mq);
+                        t.face_half(ic + 1, jc, i2, j2);
+                        const double ef = (double)sc * D(i2[0], j2[0], mq);
+                        deltac = (ef - rc.ef[0][k]) - (fp - rc.fp[0][k]);
+                    }
+                } else if (iface == 1) {
+                    ic = mx;
+                    t.face_half(ic, jc, i2, j2);
+                    deltac = 0;
+                    areac = areac_v;
+                    if (!skip_this_grid(i2, j2, mx, my)) {
+                        const double fm = D(i2[0], j2[0], mq);
+                        t.face_half(ic - 1, jc, i2, j2);
+                        const double ef = (double)sc * D(i2[0], j2[0], mq);
+                        deltac = (rc.ef[1][k] - ef) - (fm - rc.fm[1][k]);
+                    }
+                }
+                q[P(ic, jc, mq)] = q[P(ic, jc, mq)] + deltac / areac;
+            }
+    } else {
+        const int sc = (a[0][1] + a[1][1]) / 2;
+        for (int mq = 0; mq < meqn; ++mq)
+            for (int ic = 1; ic <= mx; ++ic) {
+                const int k = (ic - 1) + mx * mq;
+                int jc = 1;
+                double deltac = 0;
+                double areac = 1;
+                if (iface == 2) {
+                    jc = 1;
+                    t.face_half(ic, jc, i2, j2);
+                    deltac = 0;
+                    areac = areac_v;
+                    if (!skip_this_grid(i2, j2, mx, my)) {
+                        const double gp = D(i2[0], j2[0], mq);
+                        t.face_half(ic, jc + 1, i2, j2);
+                        const double ef = (double)sc * D(i2[0], j2[0], mq);
+                        deltac = (ef - rc.ef[2][k]) - (gp - rc.gp[0][k]);
+                    }
+                } else if (iface == 3) {
+                    jc = my;
+                    t.face_half(ic, jc, i2, j2);
+                    deltac = 0;
+                    areac = areac_v;
+                    if (!skip_this_grid(i2, j2, mx, my)) {
+                        const double gm = D(i2[0], j2[0], mq);
+                        t.face_half(ic, jc - 1, i2, j2);
+                        const double ef = (double)sc * D(i2[0], j2[0], mq);
+                        deltac = (rc.ef[3][k] - ef) - (gm - rc.gm[1][k]);
+                    }
+                }
+                q[P(ic, jc, mq)] = q[P(ic, jc, mq)] + deltac / areac;
+            }
+    }
+}
+
+// fclaw2d_clawpatch_time_sync_reset (fclaw2d_clawpatch_conservation.c:205-270)
+void Solver::time_sync_reset(int p, int coarse_level, int mode) {
+    const int fine_level = coarse_level + 1;
+    const int level = forest.leaves[p].level;
+    Registers& r = data[p].reg;
+    for (int k = 0; k < 4; ++k) {
+        const int rel = nbrs[p].face_rel[k];
+        bool reset = false;
+        if (mode == 1)  // FCLAW2D_TIME_SYNC_RESET_F2C
+            reset = (rel == REL_HALFSIZE && level == coarse_level) || (rel == REL_DOUBLESIZE && level == fine_level);
+        else if (mode == 2)  // FCLAW2D_TIME_SYNC_RESET_SAMESIZE
+            reset = rel == REL_SAMESIZE && level == coarse_level;
+        else  // FCLAW2D_TIME_SYNC_RESET_PHYS
+            reset = rel == REL_BOUNDARY;
+        if (!reset) continue;
+        if (k < 2) {
+            std::fill(r.fm[k].begin(), r.fm[k].end(), 0.0);
+            std::fill(r.fp[k].begin(), r.fp[k].end(), 0.0);
+        } else {
+            std::fill(r.gm[k - 2].begin(), r.gm[k - 2].end(), 0.0);
+            std::fill(r.gp[k - 2].begin(), r.gp[k - 2].end(), 0.0);
+        }
+        std::fill(r.ef[k].begin(), r.ef[k].end(), 0.0);
+    }
+}
+
+// fclaw2d_time_sync (src/fclaw2d_time_sync.c:157-205) -> correct_coarse_cells
+// (:115-155): per level from the finest option level down, same-size
+// corrections then their register reset, then fine-to-coarse corrections at
+// the level's coarse/fine faces and their reset; finally the physical-boundary
+// registers of every level are cleared.
+void Solver::time_sync(int minlevel, int maxlevel) {
+    (void)maxlevel;
+    for (int level = opt.maxlevel; level >= minlevel; --level) {
+        const std::vector<int> ps = patches_at_level(level);
+        for (int p : ps)
+            for (int f = 0; f < 4; ++f)
+                if (nbrs[p].face_rel[f] == REL_SAMESIZE) time_sync_samesize(p, f);
+        for (int p : ps) time_sync_reset(p, level, 2);
+        if (level < opt.maxlevel) {
+            for (int p : ps)
+                for (int f = 0; f < 4; ++f)
+                    if (nbrs[p].face_rel[f] == REL_HALFSIZE)
+                        for (int ig = 0; ig < 2; ++ig) time_sync_f2c(p, nbrs[p].face_nbr[f][ig], f);
+            for (int p : ps) time_sync_reset(p, level, 1);
+            for (int p : patches_at_level(level + 1)) time_sync_reset(p, level, 1);
+        }
+    }
+    for (int level = opt.maxlevel; level >= minlevel; --level)
+        for (int p : patches_at_level(level)) time_sync_reset(p, level, 3);
 }
 
 double Solver::update_single_step(int level, double t, double dt) {
@@ -467,12 +846,15 @@ double Solver::advance_all_levels(double t_curr, double dt) {
                 int ti_level = gmax - 1;
                 while (last_step % ts[ti_level].step_inc == 0) --ti_level;
                 ghost_update(ti_level + 1, gmax, sync_time, 1);
+                if (opt.time_sync) time_sync(ti_level + 1, gmax);
             } else {
                 ghost_update(gmin, gmax, sync_time, 0);
+                if (opt.time_sync) time_sync(gmin, gmax);
             }
         }
     }
     ghost_update(gmin, gmax, ts[gmax].current_time, 0);
+    if (opt.time_sync) time_sync(gmin, gmax);
     ++count_amr_advance;
     return maxcfl;
 }

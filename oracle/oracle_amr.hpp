@@ -16,7 +16,7 @@ namespace orc {
 
 enum Relation { REL_BOUNDARY = 0, REL_HALFSIZE = 1, REL_SAMESIZE = 2, REL_DOUBLESIZE = 3 };
 
-enum Problem { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2, PROB_BATHY = 3 };
+enum Problem { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2, PROB_BATHY = 3, PROB_RADIALDAM_CELLAVE = 4 };
 
 struct Options {
     // [clawpatch]
@@ -37,6 +37,10 @@ struct Options {
     int nout = 1;
     int init_ghostcell = 0;
     int reduce_cfl = 1;
+    // [Options] time-sync (flux-correction and fluctuation-correction on)
+    int time_sync = 0;
+    // [Options] ax, bx, ay, by: the physical extent of the (unmapped) unit square
+    double ax = 0.0, bx = 1.0, ay = 0.0, by = 1.0;
     // problem
     SolverParams solver;
     int problem = PROB_SWIRL;
@@ -86,8 +90,18 @@ class Forest {
     }
 };
 
+// Conservation registers of one patch (fclaw2d_clawpatch_conservation.h,
+// fclaw2d_clawpatch_time_sync_new): side k = 0 left, 1 right (fp, fm: my x
+// meqn) and k = 0 bottom, 1 top (gp, gm: mx x meqn); edge_fluxes on faces
+// 0..3 hold f(q) of the interior (0) and exterior (1) cell along the face
+// (len x meqn x 2).  Fortran index order: (j, m) and (j, m, k).
+struct Registers {
+    std::vector<double> fp[2], fm[2], gp[2], gm[2], ef[4];
+};
+
 struct PatchData {
     std::vector<double> q, qlast, qinterp, qsave, aux;
+    Registers reg;
 };
 
 class Solver {
@@ -113,8 +127,10 @@ class Solver {
     void conservation(std::vector<double>& sums) const;  // diagnostics (Kahan)
 
     // geometry of a leaf
-    double xlower(int p) const;
+    double xlower(int p) const;  // block coordinates
     double ylower(int p) const;
+    double xphys(int p) const;   // physical lower-left corner
+    double yphys(int p) const;
     double dx(int p) const;
     double dy(int p) const;
     PatchGeom geom(int p) const;
@@ -130,6 +146,8 @@ class Solver {
     double single_step_patch(int p, double t, double dt);
     void physical_bc(int p, int time_interp);
     bool domain_adapt(std::vector<Quad>& new_leaves);
+    // conservative time synchronisation (src/fclaw2d_time_sync.c)
+    void time_sync(int minlevel, int maxlevel);
 
   private:
     void copy2ghost(int level, int time_interp);
@@ -141,6 +159,11 @@ class Solver {
     void iterate_adapted(const std::vector<Quad>& old_leaves, std::vector<PatchData>& old_data,
                          bool domain_init);
     void tag_and_adapt(bool domain_init, bool* changed);
+    void time_sync_store_flux(int p, double dt);
+    void time_sync_accumulate(int p, double dt, const StepFluxArrays& f);
+    void time_sync_samesize(int p, int iface);
+    void time_sync_f2c(int pc, int pf, int iface);
+    void time_sync_reset(int p, int coarse_level, int mode);
 };
 
 }  // namespace orc

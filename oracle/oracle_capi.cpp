@@ -21,11 +21,11 @@ enum IOpt {
     I_MTHBC0, I_MTHBC3 = I_MTHBC0 + 3,
     I_MINLEVEL, I_MAXLEVEL, I_SUBCYCLE, I_REGRID_INTERVAL, I_SMOOTH_REFINE, I_SMOOTH_LEVEL,
     I_CRITERIA, I_IVAR, I_USE_FIXED_DT, I_NOUT, I_INIT_GHOSTCELL, I_REDUCE_CFL,
-    I_SOLVER, I_PROBLEM, I_CLAW_VERSION, I_COUNT
+    I_SOLVER, I_PROBLEM, I_CLAW_VERSION, I_TIME_SYNC, I_COUNT
 };
 enum DOpt {
     D_REFINE_TH, D_COARSEN_TH, D_TFINAL, D_INITIAL_DT, D_MAX_CFL, D_DESIRED_CFL,
-    D_GRAV, D_GAMMA, D_GAMMA1, D_DRYTOL, D_PPARAM0, D_COUNT = D_PPARAM0 + 32
+    D_GRAV, D_GAMMA, D_GAMMA1, D_DRYTOL, D_PPARAM0, D_AX = D_PPARAM0 + 32, D_BX, D_AY, D_BY, D_COUNT
 };
 
 Options unpack(const int* io, const double* d) {
@@ -42,6 +42,8 @@ Options unpack(const int* io, const double* d) {
     o.reduce_cfl = io[I_REDUCE_CFL];
     o.solver.kind = io[I_SOLVER]; o.problem = io[I_PROBLEM];
     o.method.version = io[I_CLAW_VERSION];
+    o.time_sync = io[I_TIME_SYNC];
+    o.ax = d[D_AX]; o.bx = d[D_BX]; o.ay = d[D_AY]; o.by = d[D_BY];
     o.refine_threshold = d[D_REFINE_TH]; o.coarsen_threshold = d[D_COARSEN_TH];
     o.tfinal = d[D_TFINAL]; o.initial_dt = d[D_INITIAL_DT]; o.max_cfl = d[D_MAX_CFL];
     o.desired_cfl = d[D_DESIRED_CFL];

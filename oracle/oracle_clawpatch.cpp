@@ -63,6 +63,8 @@ inline bool is_valid_average(int i, int j, int mx, int my) {
     return (1 <= i && i <= mx) && (1 <= j && j <= my);
 }
 
+}  // namespace
+
 // fclaw2d_clawpatch_utils.f:76-169: recover A, F of T(ic,jc) = A(ic,jc) + F.
 void build_transform_half(const Transform& t, int a[2][2], int f[2]) {
     int mi[4], mj[4];
@@ -83,7 +85,6 @@ void build_transform_same(const Transform& t, int a[2][2], int f[2]) {
     a[0][1] = mi - f[0]; a[1][1] = mj - f[1];
 }
 
-}  // namespace
 
 void copy_face(int mx, int my, int mbc, int meqn, double* qthis, const double* qnbr, int iface,
                const Transform& t) {

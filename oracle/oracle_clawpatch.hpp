@@ -30,6 +30,11 @@ struct Transform {
     void corner_half(int i1, int j1, int i2[4], int j2[4]) const;
 };
 
+// fclaw2d_clawpatch_utils.f:76-169: A and F of T(i,j) = A (i,j) + F for the
+// half-size (coarse to first fine index) and same-size transforms.
+void build_transform_half(const Transform& t, int a[2][2], int f[2]);
+void build_transform_same(const Transform& t, int a[2][2], int f[2]);
+
 // fort_4.6/fclaw2d_clawpatch46_copy.f:17-86
 void copy_face(int mx, int my, int mbc, int meqn, double* qthis, const double* qnbr, int iface,
                const Transform& t);

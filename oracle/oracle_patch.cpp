@@ -818,7 +818,7 @@ double flux2(const SolverParams& sp, const MethodParams& mp, Work& w, int ixy, i
 }  // namespace
 
 double step2(const SolverParams& sp, const MethodParams& mp, int mx, int my, int mbc, int meqn,
-             int maux, double* q, const double* aux, double dx, double dy, double dt) {
+             int maux, double* q, const double* aux, double dx, double dy, double dt, StepFluxArrays* keep) {
     const PatchIdx P(mx, my, mbc);
     const int maxm = std::max(mx, my);
     const int mwaves = mp.mwaves;
@@ -909,7 +909,165 @@ double step2(const SolverParams& sp, const MethodParams& mp, int mx, int my, int
                 else
                     q[P(i, j, m)] = q[P(i, j, m)] - (dtdx * df + dtdy * dg) / aux[P(i, j, mp.mcapa - 1)];
             }
+    if (keep) {
+        keep->fm = std::move(fm);
+        keep->fp = std::move(fp);
+        keep->gm = std::move(gm);
+        keep->gp = std::move(gp);
+    }
     return cflgrid;
+}
+
+void rpn2_cons_update_swe(int meqn, int idir, const double* q, double grav, double* flux) {
+    (void)meqn;
+    // mu, mv: normal and tangential momentum (1-based 2, 3 for idir 0)
+    const int mu = (idir == 0) ? 1 : 2;
+    const int mv = (idir == 0) ? 2 : 1;
+    const double hun = q[mu], hut = q[mv], h = q[0];
+    const double un = hun / h;
+    flux[0] = hun;
+    flux[mu] = (hun * hun) / h + (0.5 * grav) * (h * h);  // hun**2/h + 0.5*grav*h**2
+    flux[mv] = un * hut;
+}
+
+namespace {
+
+// radialdam/fdisc.f without a mapping: r^2 - r0^2
+struct Disc {
+    double x0, y0, r0;
+    double fdisc(double x, double y) const {
+        const double r2 = (x - x0) * (x - x0) + (y - y0) * (y - y0);
+        return r2 - r0 * r0;
+    }
+};
+
+// cellave2.f zeroin: Brent's root finder as the reference states it (netlib
+// zeroin), including its step "b = b - xm" where the published algorithm has
+// b - tol1, and eps found by halving until 1 + eps == 1.
+double zeroin(const Disc& dsc, double xc0, double yc0, double xc1, double yc1, double ax, double bx, double tol) {
+    auto f = [&](double sv) {  // fss
+        const double x = xc0 + sv * (xc1 - xc0);
+        const double y = yc0 + sv * (yc1 - yc0);
+        return dsc.fdisc(x, y);
+    };
+    double eps = 1.0, tol1;
+    do {
+        eps = eps / 2.0;
+        tol1 = 1.0 + eps;
+    } while (tol1 > 1.0);
+    double a = ax, b = bx, fa = f(a), fb = f(b);
+    double c, fc, d, e, xm, sv, p, qq, r;
+    goto L20;
+L20:
+    c = a;
+    fc = fa;
+    d = b - a;
+    e = d;
+L30:
+    if (std::fabs(fc) >= std::fabs(fb)) goto L40;
+    a = b;
+    b = c;
+    c = a;
+    fa = fb;
+    fb = fc;
+    fc = fa;
+L40:
+    tol1 = (2.0 * eps) * std::fabs(b) + 0.5 * tol;
+    xm = 0.5 * (c - b);
+    if (std::fabs(xm) <= tol1) goto L90;
+    if (fb == 0.0) goto L90;
+    if (std::fabs(e) < tol1) goto L70;
+    if (std::fabs(fa) <= std::fabs(fb)) goto L70;
+    if (a != c) goto L50;
+    sv = fb / fa;
+    p = (2.0 * xm) * sv;
+    qq = 1.0 - sv;
+    goto L60;
+L50:
+    qq = fa / fc;
+    r = fb / fc;
+    sv = fb / fa;
+    p = sv * (((2.0 * xm) * qq) * (qq - r) - (b - a) * (r - 1.0));
+    qq = ((qq - 1.0) * (r - 1.0)) * (sv - 1.0);
+L60:
+    if (p > 0.0) qq = -qq;
+    p = std::fabs(p);
+    if ((2.0 * p) >= ((3.0 * xm) * qq - std::fabs(tol1 * qq))) goto L70;
+    if (p >= std::fabs((0.5 * e) * qq)) goto L70;
+    e = d;
+    d = p / qq;
+    goto L80;
+L70:
+    d = xm;
+    e = d;
+L80:
+    a = b;
+    fa = fb;
+    if (std::fabs(d) > tol1) b = b + d;
+    if (std::fabs(d) <= tol1) {
+        if (xm >= 0) b = b + tol1;
+        else b = b - xm;
+    }
+    fb = f(b);
+    if ((fb * (fc / std::fabs(fc))) > 0.0) goto L20;
+    goto L30;
+L90:
+    return b;
+}
+
+// cellave2.f: fraction of the cell [xlow, xlow+dx] x [ylow, ylow+dy] where fdisc < 0
+double cellave2(const Disc& dsc, double xlow, double ylow, double dx, double dy) {
+    double xx[5], yy[5], x[10], y[10];
+    bool fl[5];
+    xx[0] = xlow; xx[1] = xlow; xx[2] = xlow + dx; xx[3] = xlow + dx; xx[4] = xx[0];
+    yy[0] = ylow; yy[1] = ylow + dy; yy[2] = ylow + dy; yy[3] = ylow; yy[4] = yy[0];
+    bool alll = true, allr = true;
+    for (int i = 0; i < 4; ++i) {
+        fl[i] = dsc.fdisc(xx[i], yy[i]) < 0.0;
+        alll = alll && fl[i];
+        allr = allr && !fl[i];
+    }
+    fl[4] = fl[0];
+    if (alll) return 1.0;
+    if (allr) return 0.0;
+    int iv = 0;
+    for (int i = 0; i < 4; ++i) {
+        if (fl[i]) {
+            x[iv] = xx[i];
+            y[iv] = yy[i];
+            ++iv;
+        }
+        if (fl[i] != fl[i + 1]) {
+            const double ss = zeroin(dsc, xx[i], yy[i], xx[i + 1], yy[i + 1], 0.0, 1.0, 1e-14);
+            x[iv] = xx[i] + ss * (xx[i + 1] - xx[i]);
+            y[iv] = yy[i] + ss * (yy[i + 1] - yy[i]);
+            ++iv;
+        }
+    }
+    if (iv == 0) return 0.0;
+    x[iv] = x[0];
+    y[iv] = y[0];
+    double area = 0.0;
+    for (int i = 0; i < iv; ++i) area = area + (0.5 * (y[i] + y[i + 1])) * (x[i + 1] - x[i]);
+    return area / (dx * dy);
+}
+
+}  // namespace
+
+void qinit_radialdam_cellave(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy,
+                             double x0, double y0, double r0, double hin, double hout, double* q) {
+    const PatchIdx P(mx, my, mbc);
+    const Disc dsc{x0, y0, r0};
+    for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+        const double xlow = xlower + (i - 1.0) * dx;
+        for (int j = 1 - mbc; j <= my + mbc; ++j) {
+            const double ylow = ylower + (j - 1.0) * dy;
+            const double win = cellave2(dsc, xlow, ylow, dx, dy);
+            q[P(i, j, 0)] = hin * win + hout * (1.0 - win);
+            q[P(i, j, 1)] = 0.0;
+            q[P(i, j, 2)] = 0.0;
+        }
+    }
 }
 
 void setaux_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double* aux) {

@@ -59,9 +59,25 @@ inline double dmin(double a, double b) { return a < b ? a : b; }
 // With mp.version == 5: clawpack5_step2_wrap.f:1-115 + clawpack5_step2.f90:1-172 +
 // clawpack5_flux2.f:4-235 (interfaces 1..mx+1 only, interior update i,j = 1..mx,
 // clawpack5_rpn2.f90 / clawpack5_rpt2.f90 arithmetic for the shallow-water solver).
+// The flux accumulators fm, fp, gm, gp of one step (46 layout), kept for the
+// time-sync registers (fc2d_clawpack46.cpp:369-386).
+struct StepFluxArrays {
+    std::vector<double> fm, fp, gm, gp;
+};
 double step2(const SolverParams& sp, const MethodParams& mp,
              int mx, int my, int mbc, int meqn, int maux,
-             double* q, const double* aux, double dx, double dy, double dt);
+             double* q, const double* aux, double dx, double dy, double dt,
+             StepFluxArrays* keep = nullptr);
+
+// shallow/2d/radialdam/rpn2cons_update.f: the physical flux f(q) (idir 0) or
+// g(q) (idir 1) of the shallow-water equations at one cell.
+void rpn2_cons_update_swe(int meqn, int idir, const double* q, double grav, double* flux);
+
+// radialdam/user_4.6/qinit.f with src/fortran_source2d/cellave2.f (cellave2,
+// fss, zeroin) and radialdam/fdisc.f (no mapping): h = hin*w + hout*(1-w),
+// w the fraction of the cell inside the circle of radius r0 about (x0, y0).
+void qinit_radialdam_cellave(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy,
+                             double x0, double y0, double r0, double hin, double hout, double* q);
 
 // Shallow water over bathymetry: b(x,y) = -1 + 0.8 exp(-((x-.5)^2 + (y-.5)^2)/0.02)
 // at cell centres (aux(i,j,1), ghost cells included), and a surface

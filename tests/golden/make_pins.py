@@ -4,7 +4,7 @@ The reference's regression tests pin three counters per run
 (src/fclaw2d_finalize.c:140-197): count_amr_advance, global_num_patches and
 count_amr_new_domain.  This script copies those numbers for the runs whose
 configuration lies on this path (swirl with clawpack 4.6 and 5, quadrants with
-clawpack 4.6), so the
+clawpack 4.6, radialdam example 0 with clawpack 4.6 and time-sync), so the
 tests can check the oracle and the CUDA path without the reference tree.
 
 Usage: python tests/golden/make_pins.py /path/to/reference
@@ -33,6 +33,10 @@ def main(ref: Path):
         "swirl_claw5": {
             "source": "applications/clawpack/advection/2d/swirl/regression_values_1.csv",
             "values": read_csv(ref / "applications/clawpack/advection/2d/swirl/regression_values_1.csv"),
+        },
+        "radialdam": {
+            "source": "applications/clawpack/shallow/2d/radialdam/regression_values_0.csv",
+            "values": read_csv(ref / "applications/clawpack/shallow/2d/radialdam/regression_values_0.csv"),
         },
         "quadrants": {
             "source": "applications/clawpack/euler/2d/quadrants/regression_values_0.csv",

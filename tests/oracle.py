@@ -20,7 +20,7 @@ ORACLE_DIR = ROOT / "oracle"
 # Solver kinds (oracle/oracle_patch.hpp SolverKind)
 ADVECTION, SWE_ROE, EULER4_ROE, GEOCLAW_FWAVE = 0, 1, 2, 3
 # Problems (oracle/oracle_amr.hpp Problem)
-SWIRL, RADIALDAM, QUADRANTS, BATHY = 0, 1, 2, 3
+SWIRL, RADIALDAM, QUADRANTS, BATHY, RADIALDAM_CELLAVE = 0, 1, 2, 3, 4
 # Tagging criteria (oracle/oracle_clawpatch.hpp TagCriteria)
 VALUE, MINMAX, DIFFERENCE, GRADIENT = 0, 1, 2, 3
 
@@ -28,9 +28,10 @@ _I_FIELDS = (["mx", "my", "mbc", "meqn", "maux", "order0", "order1", "mcapa", "m
              + [f"mthlim{k}" for k in range(8)] + [f"mthbc{k}" for k in range(4)]
              + ["minlevel", "maxlevel", "subcycle", "regrid_interval", "smooth_refine",
                 "smooth_level", "criteria", "ivar", "use_fixed_dt", "nout", "init_ghostcell",
-                "reduce_cfl", "solver", "problem", "claw_version"])
+                "reduce_cfl", "solver", "problem", "claw_version", "time_sync"])
 _D_FIELDS = (["refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
-              "desired_cfl", "grav", "gamma", "gamma1", "drytol"] + [f"p{k}" for k in range(32)])
+              "desired_cfl", "grav", "gamma", "gamma1", "drytol"] + [f"p{k}" for k in range(32)]
+             + ["ax", "bx", "ay", "by"])
 
 
 @dataclass
@@ -71,6 +72,8 @@ class Config:
     pparams: tuple = field(default_factory=tuple)
     claw_version: int = 4   # 4: fc2d_clawpack46, 5: fc2d_clawpack5
     drytol: float = 1e-3    # GeoClaw dry tolerance
+    time_sync: int = 0      # [Options] time-sync: conservative coarse/fine correction
+    extent: tuple = (0.0, 1.0, 0.0, 1.0)  # [Options] ax, bx, ay, by
 
     @property
     def gamma1(self) -> float:
@@ -86,7 +89,7 @@ class Config:
             "criteria": self.criteria, "ivar": self.ivar, "use_fixed_dt": self.use_fixed_dt,
             "nout": self.nout, "init_ghostcell": self.init_ghostcell,
             "reduce_cfl": self.reduce_cfl, "solver": self.solver, "problem": self.problem,
-            "claw_version": self.claw_version,
+            "claw_version": self.claw_version, "time_sync": self.time_sync,
         }
         for k in range(8):
             iv[f"mthlim{k}"] = self.mthlim[k] if k < len(self.mthlim) else 0
@@ -97,6 +100,7 @@ class Config:
             "tfinal": self.tfinal, "initial_dt": self.initial_dt, "max_cfl": self.max_cfl,
             "desired_cfl": self.desired_cfl, "grav": self.grav, "gamma": self.gamma,
             "gamma1": self.gamma1, "drytol": self.drytol,
+            "ax": self.extent[0], "bx": self.extent[1], "ay": self.extent[2], "by": self.extent[3],
         }
         for k in range(32):
             dv[f"p{k}"] = float(self.pparams[k]) if k < len(self.pparams) else 0.0
@@ -277,6 +281,20 @@ def swirl_regression(claw_version: int = 4) -> Config:
                   tfinal=0.1, initial_dt=0.005, max_cfl=1.0, desired_cfl=0.9, nout=1,
                   subcycle=1, solver=ADVECTION, problem=SWIRL, criteria=MINMAX,
                   pparams=(4.0,), claw_version=claw_version)
+
+
+def radialdam_regression(claw_version: int = 4) -> Config:
+    """applications/clawpack/shallow/2d/radialdam/regression.ini on top of that
+    directory's fclaw_options.ini (read first, fclaw_base.c:758-786), which sets
+    refinement-criteria = gradient; example 0: unmapped [-2.5, 2.5]^2, cellave2
+    initial depth, shallow-water Roe solver with time-sync = T."""
+    return Config(mx=16, my=16, mbc=2, meqn=3, maux=0, order=(2, 2), mwaves=3, mthlim=(4, 4, 4),
+                  mthbc=(1, 1, 1, 1), minlevel=1, maxlevel=5, regrid_interval=1,
+                  refine_threshold=0.5, coarsen_threshold=0.25, smooth_refine=1, smooth_level=4,
+                  tfinal=0.4, initial_dt=0.0625, max_cfl=1.0, desired_cfl=0.9, nout=1,
+                  subcycle=1, solver=SWE_ROE, problem=RADIALDAM_CELLAVE, criteria=GRADIENT, grav=1.0,
+                  pparams=(0.0, 0.0, 0.5, 2.0, 1.0), claw_version=claw_version, time_sync=1,
+                  extent=(-2.5, 2.5, -2.5, 2.5))
 
 
 QUADRANT_STATES = (

@@ -12,13 +12,14 @@ import oracle as O
 PINS = json.loads((Path(__file__).parent / "golden" / "regression_pins.json").read_text())
 
 
-@pytest.mark.parametrize("name", ["swirl", "swirl_claw5", "quadrants"])
+@pytest.mark.parametrize("name", ["swirl", "swirl_claw5", "quadrants", "radialdam"])
 def test_regression_pins(name):
     """applications/**/regression_values_{0,1}.csv: count_amr_advance,
-    global_num_patches and count_amr_new_domain of the clawpack 4.6 runs and of
-    the swirl run with --user:claw-version=5."""
+    global_num_patches and count_amr_new_domain of the clawpack 4.6 runs, of
+    the swirl run with --user:claw-version=5, and of the radialdam run
+    (time-sync, cellave2 initial depth, gradient tagging on [-2.5, 2.5]^2)."""
     cfg = {"swirl": O.swirl_regression, "swirl_claw5": lambda: O.swirl_regression(5),
-           "quadrants": O.quadrants_regression}[name]()
+           "quadrants": O.quadrants_regression, "radialdam": O.radialdam_regression}[name]()
     s = O.OracleSolver(cfg)
     s.initialize()
     s.run()
@@ -137,3 +138,58 @@ def test_geoclaw_rejects_transverse_order():
     with pytest.raises(Exception):
         s.initialize()
         s.advance(0.0, 0.001)
+
+
+def _fixed_mesh_dam(time_sync):
+    """The radialdam regression case on a mesh refined once at start and never
+    regridded, so the waves cross coarse/fine faces (levels 2-4, to t = 0.6)."""
+    import dataclasses
+
+    return dataclasses.replace(O.radialdam_regression(), time_sync=time_sync, tfinal=0.6,
+                               regrid_interval=0, minlevel=2, maxlevel=4)
+
+
+def test_time_sync_conserves_mass_exactly():
+    """fclaw2d_time_sync's corrections make subcycled AMR conservative: with
+    time-sync the Kahan mass sum is unchanged to the last bit while waves cross
+    the coarse/fine faces; without it the mass drifts."""
+    out = {}
+    for ts in (0, 1):
+        s = O.OracleSolver(_fixed_mesh_dam(ts))
+        s.initialize()
+        m0 = s.conservation()
+        s.run()
+        out[ts] = (m0, s.conservation())
+    m0, m1 = out[1]
+    assert m1[0] == m0[0]
+    m0, m1 = out[0]
+    assert abs(m1[0] - m0[0]) > 1e-6 * m0[0]
+
+
+def test_cellave_initial_depth():
+    """cellave2: a cell wholly inside the circle gets hin, wholly outside hout,
+    and the volume of the dam equals hin*pi*r0^2 + hout*(area - pi*r0^2) to the
+    accuracy of the polygonal cut of each boundary cell."""
+    import dataclasses
+
+    cfg = dataclasses.replace(O.radialdam_regression(), minlevel=3, maxlevel=3)
+    s = O.OracleSolver(cfg)
+    s.initialize()
+    q = s.all_q()
+    h = q[:, 0, 2:-2, 2:-2]
+    assert h.min() == 1.0 and h.max() == 2.0
+    assert ((h > 1.0) & (h < 2.0)).any()
+    mass = s.conservation()[0]
+    exact = 2.0 * np.pi * 0.25 + 1.0 * (25.0 - np.pi * 0.25)
+    assert abs(mass - exact) < 1e-3 * exact
+
+
+def test_time_sync_rejected_outside_its_scope():
+    import dataclasses
+
+    for kw in ({"claw_version": 5}, {"solver": O.EULER4_ROE, "meqn": 4, "mwaves": 4}):
+        cfg = dataclasses.replace(_fixed_mesh_dam(1), tfinal=0.01, **kw)
+        s = O.OracleSolver(cfg)
+        with pytest.raises(Exception):
+            s.initialize()
+            s.run()
