@@ -21,7 +21,7 @@ import numpy as np
 
 __all__ = ["Options", "Solver", "lib", "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
            "SOLVER_EULER4_ROE", "SOLVER_GEOCLAW_FWAVE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM",
-           "PROBLEM_QUADRANTS", "PROBLEM_BATHY",
+           "PROBLEM_QUADRANTS", "PROBLEM_BATHY", "PROBLEM_RADIALDAM_CELLAVE",
            "PRECISION_FP64", "PRECISION_MIXED", "measure_fp_rate",
            "TAG_VALUE", "TAG_MINMAX", "TAG_DIFFERENCE", "TAG_GRADIENT", "EXPORTED_SYMBOLS"]
 
@@ -29,7 +29,7 @@ PKG = Path(__file__).resolve().parent
 LIBPATH = PKG / "libfclaw_b200.so"
 
 SOLVER_ADVECTION, SOLVER_SWE_ROE, SOLVER_EULER4_ROE, SOLVER_GEOCLAW_FWAVE = 0, 1, 2, 3
-PROBLEM_SWIRL, PROBLEM_RADIALDAM, PROBLEM_QUADRANTS, PROBLEM_BATHY = 0, 1, 2, 3
+PROBLEM_SWIRL, PROBLEM_RADIALDAM, PROBLEM_QUADRANTS, PROBLEM_BATHY, PROBLEM_RADIALDAM_CELLAVE = 0, 1, 2, 3, 4
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 TAG_VALUE, TAG_MINMAX, TAG_DIFFERENCE, TAG_GRADIENT = 0, 1, 2, 3
 
@@ -69,6 +69,8 @@ class _Options(ctypes.Structure):
         ("macro_graph", ctypes.c_int),
         ("claw_version", ctypes.c_int),
         ("dry_tolerance", ctypes.c_double),
+        ("time_sync", ctypes.c_int),
+        ("ax", ctypes.c_double), ("bx", ctypes.c_double), ("ay", ctypes.c_double), ("by", ctypes.c_double),
     ]
 
 
@@ -130,23 +132,29 @@ class Options:
     # 0 = FP64 throughout, 1 = mixed FP32 solves / FP64 accumulation
     precision: int = PRECISION_FP64
     # 1: advance_all_levels replays the macro-step as one CUDA graph; 0: host
-    # launches; 2: graph once a macro step updates three or more level batches
+    # launches; 2: automatic (the graph whenever a macro step updates a level)
     macro_graph: int = 2
     # 4: fc2d_clawpack46 update, 5: fc2d_clawpack5 update (arrays in q(m,i,j) order)
     claw_version: int = 4
     # GeoClaw /common_swe/ dry_tolerance
     dry_tolerance: float = 1e-3
+    # [Options] time-sync: conservative coarse/fine and same-size corrections
+    time_sync: int = 0
+    # [Options] ax, bx, ay, by: physical extent of the block
+    extent: Sequence[float] = (0.0, 1.0, 0.0, 1.0)
 
     def to_c(self) -> _Options:
         o = _Options()
         for name in ("mx", "my", "mbc", "meqn", "maux", "refinement_criteria", "threshold_variable",
                      "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
                      "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
-                     "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph", "claw_version"):
+                     "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph", "claw_version",
+                     "time_sync"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
                      "desired_cfl", "grav", "gamma", "dry_tolerance"):
             setattr(o, name, float(getattr(self, name)))
+        o.ax, o.bx, o.ay, o.by = (float(v) for v in self.extent)
         o.order[0], o.order[1] = int(self.order[0]), int(self.order[1])
         for k in range(8):
             o.mthlim[k] = int(self.mthlim[k]) if k < len(self.mthlim) else 0

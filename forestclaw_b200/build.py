@@ -38,6 +38,7 @@ SOURCES = {
     "fcb_capi.cu": ["-Xcompiler", "-fvisibility=default"],
     "fcb_noalloc.cu": ["-fmad=false"],
     "fcb_probe.cu": ["-fmad=false"],
+    "fcb_timesync.cu": ["-fmad=false"],
 }
 
 

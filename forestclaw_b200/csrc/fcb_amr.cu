@@ -23,6 +23,123 @@ __device__ __forceinline__ double bathy_b(double xc, double yc) {
     return -1.0 + 0.8 * exp(-((xc - 0.5) * (xc - 0.5) + (yc - 0.5) * (yc - 0.5)) / 0.02);
 }
 
+// radialdam/fdisc.f (no mapping) and cellave2.f (cellave2, fss, zeroin): the
+// fraction of a cell inside the circle r < r0.  zeroin is Brent's method as the
+// reference states it (netlib zeroin, with its "b = b - xm" step); it converges
+// in a few tens of steps on [0, 1], and the loop stops after 1000 in any case.
+struct DiscD {
+    double x0, y0, r0;
+    __device__ double f(double x, double y) const {
+        const double r2 = (x - x0) * (x - x0) + (y - y0) * (y - y0);
+        return r2 - r0 * r0;
+    }
+};
+
+__device__ double zeroin_d(const DiscD& dsc, double xc0, double yc0, double xc1, double yc1, double tol) {
+    auto f = [&](double sv) { return dsc.f(xc0 + sv * (xc1 - xc0), yc0 + sv * (yc1 - yc0)); };
+    double eps = 1.0, tol1;
+    do {
+        eps = eps / 2.0;
+        tol1 = 1.0 + eps;
+    } while (tol1 > 1.0);
+    double a = 0.0, b = 1.0, fa = f(a), fb = f(b);
+    double c = a, fc = fa, d = b - a, e = d;
+    bool restart = false;  // label 20 (true) or 30 (false) at the top of the loop
+    for (int it = 0; it < 1000; ++it) {
+        if (restart) {
+            c = a;
+            fc = fa;
+            d = b - a;
+            e = d;
+        }
+        if (fabs(fc) < fabs(fb)) {
+            a = b;
+            b = c;
+            c = a;
+            fa = fb;
+            fb = fc;
+            fc = fa;
+        }
+        tol1 = (2.0 * eps) * fabs(b) + 0.5 * tol;
+        const double xm = 0.5 * (c - b);
+        if (fabs(xm) <= tol1) break;
+        if (fb == 0.0) break;
+        bool bisect = fabs(e) < tol1 || fabs(fa) <= fabs(fb);
+        if (!bisect) {
+            double p, qq;
+            if (a == c) {
+                const double sv = fb / fa;
+                p = (2.0 * xm) * sv;
+                qq = 1.0 - sv;
+            } else {
+                qq = fa / fc;
+                const double r = fb / fc;
+                const double sv = fb / fa;
+                p = sv * (((2.0 * xm) * qq) * (qq - r) - (b - a) * (r - 1.0));
+                qq = ((qq - 1.0) * (r - 1.0)) * (sv - 1.0);
+            }
+            if (p > 0.0) qq = -qq;
+            p = fabs(p);
+            if ((2.0 * p) >= ((3.0 * xm) * qq - fabs(tol1 * qq)) || p >= fabs((0.5 * e) * qq)) {
+                bisect = true;
+            } else {
+                e = d;
+                d = p / qq;
+            }
+        }
+        if (bisect) {
+            d = xm;
+            e = d;
+        }
+        a = b;
+        fa = fb;
+        if (fabs(d) > tol1) b = b + d;
+        if (fabs(d) <= tol1) {
+            if (xm >= 0) b = b + tol1;
+            else b = b - xm;
+        }
+        fb = f(b);
+        restart = (fb * (fc / fabs(fc))) > 0.0;
+    }
+    return b;
+}
+
+__device__ double cellave2_d(const DiscD& dsc, double xlow, double ylow, double dx, double dy) {
+    double xx[5], yy[5], x[10], y[10];
+    bool fl[5];
+    xx[0] = xlow; xx[1] = xlow; xx[2] = xlow + dx; xx[3] = xlow + dx; xx[4] = xx[0];
+    yy[0] = ylow; yy[1] = ylow + dy; yy[2] = ylow + dy; yy[3] = ylow; yy[4] = yy[0];
+    bool alll = true, allr = true;
+    for (int i = 0; i < 4; ++i) {
+        fl[i] = dsc.f(xx[i], yy[i]) < 0.0;
+        alll = alll && fl[i];
+        allr = allr && !fl[i];
+    }
+    fl[4] = fl[0];
+    if (alll) return 1.0;
+    if (allr) return 0.0;
+    int iv = 0;
+    for (int i = 0; i < 4; ++i) {
+        if (fl[i]) {
+            x[iv] = xx[i];
+            y[iv] = yy[i];
+            ++iv;
+        }
+        if (fl[i] != fl[i + 1]) {
+            const double ss = zeroin_d(dsc, xx[i], yy[i], xx[i + 1], yy[i + 1], 1e-14);
+            x[iv] = xx[i] + ss * (xx[i + 1] - xx[i]);
+            y[iv] = yy[i] + ss * (yy[i + 1] - yy[i]);
+            ++iv;
+        }
+    }
+    if (iv == 0) return 0.0;
+    x[iv] = x[0];
+    y[iv] = y[0];
+    double area = 0.0;
+    for (int i = 0; i < iv; ++i) area = area + (0.5 * (y[i] + y[i + 1])) * (x[i + 1] - x[i]);
+    return area / (dx * dy);
+}
+
 __global__ void qinit_kernel(const QinitArgs a) {
     const int pi = blockIdx.x;
     if (pi >= a.n) return;
@@ -55,6 +172,13 @@ __global__ void qinit_kernel(const QinitArgs a) {
             q[((int64_t)1 * ny + r) * nx + c] = rho * u;
             q[((int64_t)2 * ny + r) * nx + c] = rho * v;
             q[((int64_t)3 * ny + r) * nx + c] = pr / a.gamma1 + 0.5 * rho * (u * u + v * v);
+        } else if (a.problem == PROB_RADIALDAM_CELLAVE) {
+            const DiscD dsc{a.p[0], a.p[1], a.p[2]};
+            const double win = cellave2_d(dsc, mt.xlower + (i - 1.0) * mt.dx, mt.ylower + (j - 1.0) * mt.dy, mt.dx,
+                                          mt.dy);
+            q[((int64_t)0 * ny + r) * nx + c] = a.p[3] * win + a.p[4] * (1.0 - win);
+            q[((int64_t)1 * ny + r) * nx + c] = 0.0;
+            q[((int64_t)2 * ny + r) * nx + c] = 0.0;
         } else if (a.problem == PROB_BATHY) {
             const double r2 = (xc - a.p[0]) * (xc - a.p[0]) + (yc - a.p[1]) * (yc - a.p[1]);
             const double eta = a.p[2] * exp(-r2 / (a.p[3] * a.p[3]));

@@ -48,6 +48,50 @@ struct StepArgs {
     double grav, gamma, gamma1;
     double drytol;         // GeoClaw dry tolerance
     unsigned long long* cfl_out;  // atomicMax on the bits of a non-negative double
+    double* treg;          // time-sync: conservation-register arena (null: off)
+    int64_t treg_stride;   // doubles per slot in treg
+};
+
+// Conservation registers of one slot (fclaw2d_clawpatch_registers_t), doubles
+// at these offsets, Fortran index order (j, m) / (i, m) and (j|i, m, k):
+//   fp[k], fm[k]: k = 0 left, 1 right, my x meqn
+//   gp[k], gm[k]: k = 0 bottom, 1 top, mx x meqn
+//   ef[f]: f(q) accumulated at the interior (k = 0) and exterior (k = 1) cell
+//          along face f (len x meqn x 2)
+struct RegLayout {
+    int mx, my, meqn;
+    __host__ __device__ int ny() const { return my * meqn; }
+    __host__ __device__ int nx() const { return mx * meqn; }
+    __host__ __device__ int fp(int k) const { return k * ny(); }
+    __host__ __device__ int fm(int k) const { return 2 * ny() + k * ny(); }
+    __host__ __device__ int gp(int k) const { return 4 * ny() + k * nx(); }
+    __host__ __device__ int gm(int k) const { return 4 * ny() + 2 * nx() + k * nx(); }
+    __host__ __device__ int ef(int f) const {
+        const int b = 4 * ny() + 4 * nx();
+        return f < 2 ? b + f * 2 * ny() : b + 4 * ny() + (f - 2) * 2 * nx();
+    }
+    __host__ __device__ int size() const { return 8 * ny() + 8 * nx(); }
+};
+
+// Time-synchronisation records (fclaw2d_time_sync.c correct_coarse_cells).
+enum TsOpType : int32_t {
+    TS_SAMESIZE = 0,  // clawpack46_fort_time_sync_samesize on (slot, face) from neighbour nbr
+    TS_F2C = 1,       // clawpack46_fort_time_sync_f2c on coarse slot, face, from fine nbr
+    TS_RESET = 2,     // zero the registers of (slot, face)
+};
+struct TsOp {
+    int32_t type, slot, face, nbr;
+    int32_t dx, dy;  // same size: index shift to the neighbour; f2c: fine-index offset D
+};
+struct TsArgs {
+    double* q;
+    double* treg;
+    int64_t q_stride, treg_stride;
+    const PatchMeta* meta;
+    int mx, my, mbc, meqn;
+    const TsOp* ops;
+    const int32_t* groups;  // group k = records [groups[k], groups[k+1]), one patch each
+    int ngroups;
 };
 #ifdef __CUDACC__
 __device__ __forceinline__ double step_dt(const StepArgs& a) { return a.dyn ? a.dyn[0] : a.dt; }
@@ -87,7 +131,13 @@ struct GhostArgs {
     int interp_fp32;       // mixed precision: coarse-to-fine interpolation in FP32
 };
 
-enum Problem : int32_t { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2, PROB_BATHY = 3 };
+enum Problem : int32_t {
+    PROB_SWIRL = 0,
+    PROB_RADIALDAM = 1,
+    PROB_QUADRANTS = 2,
+    PROB_BATHY = 3,
+    PROB_RADIALDAM_CELLAVE = 4,  // radialdam/user_4.6/qinit.f with cellave2.f
+};
 
 struct QinitArgs {
     double* q;

@@ -37,6 +37,7 @@ template struct DevBuf<GhostOp>;
 template struct DevBuf<unsigned long long>;
 template struct DevBuf<PatchDesc>;
 template struct DevBuf<double>;
+template struct DevBuf<TsOp>;
 
 void Context::check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw Error(FCB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -68,7 +69,15 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
     if (opt_.problem == FCB_PROBLEM_SWIRL && opt_.solver_kind != FCB_SOLVER_ADVECTION) bad("swirl needs advection");
     if (opt_.solver_kind == FCB_SOLVER_ADVECTION && opt_.problem != FCB_PROBLEM_SWIRL)
         bad("the advection solver takes its velocities from the swirl stream function");
-    if (opt_.problem == FCB_PROBLEM_RADIALDAM && opt_.solver_kind != FCB_SOLVER_SWE_ROE) bad("radialdam needs SWE");
+    if ((opt_.problem == FCB_PROBLEM_RADIALDAM || opt_.problem == FCB_PROBLEM_RADIALDAM_CELLAVE) &&
+        opt_.solver_kind != FCB_SOLVER_SWE_ROE)
+        bad("radialdam needs SWE");
+    if (opt_.problem < FCB_PROBLEM_SWIRL || opt_.problem > FCB_PROBLEM_RADIALDAM_CELLAVE) bad("unknown problem");
+    if (opt_.ax == 0.0 && opt_.bx == 0.0 && opt_.ay == 0.0 && opt_.by == 0.0) {
+        opt_.bx = 1.0;  // all four unset: the unit square
+        opt_.by = 1.0;
+    }
+    if (!(opt_.bx > opt_.ax) || !(opt_.by > opt_.ay)) bad("the domain extent needs bx > ax and by > ay");
     if (opt_.problem == FCB_PROBLEM_QUADRANTS && opt_.solver_kind != FCB_SOLVER_EULER4_ROE) bad("quadrants needs Euler");
     if ((opt_.problem == FCB_PROBLEM_BATHY) != (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE))
         bad("the bathymetry problem and the GeoClaw f-wave solver go together");
@@ -93,11 +102,21 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
     if (opt_.claw_version != 4 && opt_.claw_version != 5) bad("claw_version must be 4 (clawpack 4.6) or 5");
     if (opt_.claw_version == 5 && (opt_.step_variant == 1 || opt_.step_variant == 2))
         bad("the clawpack 5 update exists in the pipelined step form only");
+    if (opt_.time_sync) {
+        if (opt_.solver_kind != FCB_SOLVER_SWE_ROE)
+            bad("time-sync needs the conservative flux rpn2_cons, given here for the shallow-water Roe solver");
+        if (opt_.claw_version == 5) bad("time-sync is on the clawpack 4.6 path");
+        if (opt_.precision != 0) bad("time-sync is FP64 only");
+        if (opt_.step_variant == 2 || opt_.step_variant == 3)
+            bad("time-sync accumulates its registers in the four-barrier step form (step_variant 0 or 1)");
+        time_sync_ = true;
+    }
     nx_ = opt_.mx + 2 * opt_.mbc;
     ny_ = opt_.my + 2 * opt_.mbc;
     const int64_t ps = (int64_t)opt_.meqn * nx_ * ny_;
     stride_ = (ps + 31) / 32 * 32;  // 256-byte aligned slots
     aux_stride_ = aux_kind_ == AUX_STORED ? ((int64_t)opt_.maux * nx_ * ny_ + 31) / 32 * 32 : 0;
+    treg_stride_ = time_sync_ ? ((int64_t)RegLayout{opt_.mx, opt_.my, opt_.meqn}.size() + 31) / 32 * 32 : 0;
     check(cudaMalloc(&d_cfl_, 4 * sizeof(unsigned long long)), "cudaMalloc cfl");
     check(cudaHostAlloc(&h_cfl_, sizeof(unsigned long long), cudaHostAllocDefault), "cudaHostAlloc cfl");
 }
@@ -137,6 +156,9 @@ Context::~Context() {
     cudaFreeHost(h_cfl_);
     cudaFree(d_scratch_);
     cudaFree(d_stage_);
+    cudaFree(d_treg_);
+    cudaFreeHost(h_ts_ops_pinned_);
+    cudaFreeHost(h_ts_groups_pinned_);
 }
 
 void Context::synchronize() { check(cudaStreamSynchronize(st_), "cudaStreamSynchronize"); }
@@ -160,6 +182,20 @@ void Context::ensure_capacity(int n) {
     grow(d_q_);
     grow(d_qlast_);
     grow(d_qti_);
+    if (time_sync_) {
+        const size_t rb = (size_t)nc * treg_stride_ * sizeof(double);
+        double* np = nullptr;
+        check(cudaMalloc(&np, rb), "cudaMalloc registers");
+        check(cudaMemsetAsync(np, 0, rb, st_), "cudaMemset registers");
+        if (d_treg_) {
+            check(cudaMemcpyAsync(np, d_treg_, (size_t)capacity_ * treg_stride_ * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, st_),
+                  "registers copy");
+            check(cudaStreamSynchronize(st_), "sync");
+            cudaFree(d_treg_);
+        }
+        d_treg_ = np;
+    }
     if (!opt_.use_fixed_dt) grow(d_qsave_);
     if (aux_kind_ == AUX_STORED) {  // recomputed for every patch by mesh_changed
         check(cudaStreamSynchronize(st_), "sync");
@@ -193,7 +229,7 @@ PatchMeta Context::meta_of(const Leaf& l) const {
     const double xl = (double)l.x / R, yl = (double)l.y / R;
     const double xu = (double)(l.x + QuadForest::width(l.level)) / R;
     const double yu = (double)(l.y + QuadForest::width(l.level)) / R;
-    const double ax = 0.0, bx = 1.0, ay = 0.0, by = 1.0;
+    const double ax = opt_.ax, bx = opt_.bx, ay = opt_.ay, by = opt_.by;
     PatchMeta m;
     m.xlower = ax + (bx - ax) * xl;
     m.ylower = ay + (by - ay) * yl;
@@ -255,6 +291,9 @@ void Context::mesh_changed() {
         ++cnt_.count_kernel_launches;
     }
     plans_.clear();
+    ts_plans_.clear();
+    h_ts_ops_.clear();
+    h_ts_groups_.clear();
     h_ops_.clear();
     h_groups_.clear();
     ops_dirty_ = true;
@@ -603,6 +642,32 @@ void Context::upload_ops() {
         check(cudaMemcpyAsync(d_ops_.p, h_ops_pinned_, h_ops_.size() * sizeof(GhostOp), cudaMemcpyHostToDevice, st_),
               "ops");
     }
+    if (!h_ts_ops_.empty()) {
+        if (h_ts_ops_.size() > h_ts_ops_pinned_cap_) {
+            cudaFreeHost(h_ts_ops_pinned_);
+            h_ts_ops_pinned_ = nullptr;
+            h_ts_ops_pinned_cap_ = std::max(h_ts_ops_.size(), 2 * h_ts_ops_pinned_cap_);
+            check(cudaHostAlloc(&h_ts_ops_pinned_, h_ts_ops_pinned_cap_ * sizeof(TsOp), cudaHostAllocDefault),
+                  "host ts ops");
+        }
+        if (h_ts_groups_.size() > h_ts_groups_pinned_cap_) {
+            cudaFreeHost(h_ts_groups_pinned_);
+            h_ts_groups_pinned_ = nullptr;
+            h_ts_groups_pinned_cap_ = std::max(h_ts_groups_.size(), 2 * h_ts_groups_pinned_cap_);
+            check(cudaHostAlloc(&h_ts_groups_pinned_, h_ts_groups_pinned_cap_ * sizeof(int32_t), cudaHostAllocDefault),
+                  "host ts groups");
+        }
+        d_ts_ops_.reserve(h_ts_ops_.size());
+        d_ts_groups_.reserve(h_ts_groups_.size());
+        std::memcpy(h_ts_ops_pinned_, h_ts_ops_.data(), h_ts_ops_.size() * sizeof(TsOp));
+        std::memcpy(h_ts_groups_pinned_, h_ts_groups_.data(), h_ts_groups_.size() * sizeof(int32_t));
+        check(cudaMemcpyAsync(d_ts_ops_.p, h_ts_ops_pinned_, h_ts_ops_.size() * sizeof(TsOp), cudaMemcpyHostToDevice,
+                              st_),
+              "ts ops");
+        check(cudaMemcpyAsync(d_ts_groups_.p, h_ts_groups_pinned_, h_ts_groups_.size() * sizeof(int32_t),
+                              cudaMemcpyHostToDevice, st_),
+              "ts groups");
+    }
     if (!h_groups_.empty()) {
         std::memcpy(h_groups_pinned_, h_groups_.data(), h_groups_.size() * sizeof(int32_t));
         check(cudaMemcpyAsync(d_groups_.p, h_groups_pinned_, h_groups_.size() * sizeof(int32_t),
@@ -611,6 +676,145 @@ void Context::upload_ops() {
     }
     check(cudaEventRecord(upload_ev_, st_), "cudaEventRecord");
     ops_dirty_ = false;
+}
+
+// ---------------------------------------------------------------------------
+// Time synchronisation (fclaw2d_time_sync.c:157-205, correct_coarse_cells
+// :115-155).  Per level L from the finest option level down to minlevel the
+// reference runs: A(L) same-size corrections of the level's patches, B(L) reset
+// of their same-size registers, and below the finest level C(L)
+// fine-to-coarse corrections at the level's coarse/fine faces and D(L) reset
+// of those registers on levels L and L+1; finally E, the reset of the
+// physical-boundary registers of every level.  Records are grouped per patch
+// (one CTA each, the records of a patch in order); launches merge steps that
+// touch disjoint data: B(L+1)+A(L) or D(L+1)+A(L) (registers of other levels
+// vs q and same-size registers of L), B(L)+C(L) (same-size vs coarse/fine
+// registers), and D(min)+E (different faces).
+// ---------------------------------------------------------------------------
+const Context::TsPlan& Context::ts_plan(int minlevel) {
+    auto it = ts_plans_.find(minlevel);
+    if (it != ts_plans_.end()) return it->second;
+    const int n = num_patches();
+    const int top = opt_.maxlevel;
+    std::vector<std::vector<int>> at((size_t)QuadForest::kMaxLevel + 2);
+    for (int p = 0; p < n; ++p) at[forest_.leaves[p].level].push_back(p);
+    auto level_list = [&](int l) -> const std::vector<int>& {
+        static const std::vector<int> empty;
+        return (l < 0 || l > QuadForest::kMaxLevel) ? empty : at[l];
+    };
+    auto xl = [&](int p) { return (double)forest_.leaves[p].x / (double)QuadForest::kRoot; };
+    auto yl = [&](int p) { return (double)forest_.leaves[p].y / (double)QuadForest::kRoot; };
+    using Step = std::vector<std::pair<int, TsOp>>;  // (patch, record) in reference order
+    auto same = [&](int L) {
+        Step st;
+        const double iw = (double)(1 << L);
+        for (int p : level_list(L))
+            for (int f = 0; f < 4; ++f) {
+                if (nbrs_[p].face_rel[f] != REL_SAMESIZE) continue;
+                const int q = nbrs_[p].face_nbr[f][0];
+                TsOp o{TS_SAMESIZE, slot_of_[p], f, slot_of_[q], 0, 0};
+                // fclaw2d_patch_transform_face, same block: i2 = i1 + shift
+                o.dx = (int)((xl(p) - xl(q)) * iw * (double)opt_.mx);
+                o.dy = (int)((yl(p) - yl(q)) * iw * (double)opt_.my);
+                st.push_back({p, o});
+            }
+        return st;
+    };
+    auto reset = [&](const std::vector<int>& ps, auto pred) {
+        Step st;
+        for (int p : ps)
+            for (int f = 0; f < 4; ++f)
+                if (pred(p, f)) st.push_back({p, TsOp{TS_RESET, slot_of_[p], f, 0, 0, 0}});
+        return st;
+    };
+    auto f2c = [&](int L) {
+        Step st;
+        for (int p : level_list(L))
+            for (int f = 0; f < 4; ++f) {
+                if (nbrs_[p].face_rel[f] != REL_HALFSIZE) continue;
+                for (int ig = 0; ig < 2; ++ig) {
+                    const int q = nbrs_[p].face_nbr[f][ig];
+                    TsOp o{TS_F2C, slot_of_[p], f, slot_of_[q], 0, 0};
+                    // fclaw2d_patch_transform_face2, same block: first fine index 1 + D + 2(c-1)
+                    const double ow = (double)(1 << forest_.leaves[q].level);
+                    o.dx = (int)((xl(p) - xl(q)) * ow * (double)opt_.mx);
+                    o.dy = (int)((yl(p) - yl(q)) * ow * (double)opt_.my);
+                    st.push_back({p, o});
+                }
+            }
+        return st;
+    };
+    auto rel = [&](int p, int f) { return nbrs_[p].face_rel[f]; };
+    auto lev = [&](int p) { return (int)forest_.leaves[p].level; };
+    std::vector<Step> launches;
+    auto cat = [](Step a, const Step& b) {
+        a.insert(a.end(), b.begin(), b.end());
+        return a;
+    };
+    Step pending;
+    for (int L = top; L >= minlevel; --L) {
+        const Step A = same(L);
+        launches.push_back(cat(pending, A));
+        const Step B = reset(level_list(L), [&](int p, int f) { return rel(p, f) == REL_SAMESIZE && lev(p) == L; });
+        if (L < top) {
+            launches.push_back(cat(B, f2c(L)));
+            Step D = reset(level_list(L), [&](int p, int f) { return rel(p, f) == REL_HALFSIZE && lev(p) == L; });
+            D = cat(D, reset(level_list(L + 1),
+                             [&](int p, int f) { return rel(p, f) == REL_DOUBLESIZE && lev(p) == L + 1; }));
+            pending = D;
+        } else {
+            pending = B;
+        }
+    }
+    Step E;
+    for (int L = top; L >= minlevel; --L)
+        E = cat(E, reset(level_list(L), [&](int p, int f) { return rel(p, f) == REL_BOUNDARY; }));
+    launches.push_back(cat(pending, E));
+    // group each launch's records per patch, patches in order of first appearance
+    TsPlan plan;
+    for (const Step& st : launches) {
+        std::vector<int> order;
+        std::unordered_map<int, std::vector<TsOp>> by;
+        for (const auto& pr : st) {
+            auto f = by.find(pr.first);
+            if (f == by.end()) {
+                order.push_back(pr.first);
+                by[pr.first] = {pr.second};
+            } else {
+                f->second.push_back(pr.second);
+            }
+        }
+        if (order.empty()) continue;
+        plan.first_group.push_back(h_ts_groups_.size());
+        plan.ngroups.push_back((int)order.size());
+        for (int p : order) {
+            h_ts_groups_.push_back((int32_t)h_ts_ops_.size());
+            for (const TsOp& o : by[p]) h_ts_ops_.push_back(o);
+        }
+        h_ts_groups_.push_back((int32_t)h_ts_ops_.size());  // end marker of the launch
+    }
+    ops_dirty_ = true;
+    return ts_plans_.emplace(minlevel, std::move(plan)).first->second;
+}
+
+void Context::time_sync(int minlevel) {
+    const TsPlan& plan = ts_plan(minlevel);
+    if (dry_) return;
+    if (ops_dirty_) upload_ops();
+    for (size_t k = 0; k < plan.ngroups.size(); ++k) {
+        TsArgs a;
+        a.q = d_q_;
+        a.treg = d_treg_;
+        a.q_stride = stride_;
+        a.treg_stride = treg_stride_;
+        a.meta = d_meta_;
+        a.mx = opt_.mx; a.my = opt_.my; a.mbc = opt_.mbc; a.meqn = opt_.meqn;
+        a.ops = d_ts_ops_.p;
+        a.groups = d_ts_groups_.p + plan.first_group[k];
+        a.ngroups = plan.ngroups[k];
+        check(launch_ts_apply(a, st_), "time sync");
+        ++cnt_.count_kernel_launches;
+    }
 }
 
 void Context::run_plan(const GhostPlan& g) {
@@ -700,6 +904,8 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     a.gamma1 = opt_.gamma - 1.0;
     a.drytol = opt_.dry_tolerance;
     a.cfl_out = cfl_slot;
+    a.treg = time_sync_ ? d_treg_ : nullptr;
+    a.treg_stride = treg_stride_;
     if (use_dyn_) {
         // {dt, vt} of launch dyn_n_ of the macro step: written to the table by
         // the dry pass, read from the device table by the launch itself
@@ -729,7 +935,12 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     // reference's per-cell evaluations because the unit-square mesh with mx a
     // power of two is dyadic (xll + dx == next xll exactly); checked at creation.
     cudaError_t e = cudaErrorNotSupported;
-    const int v = opt_.step_variant == 0 ? tune_step_form(a, n) : opt_.step_variant;
+    if (time_sync_) {
+        // clawpack46_time_sync_store_flux: f(q) at the patch faces before the update
+        check(launch_ts_store_flux(a, opt_.mx, opt_.my, opt_.mbc, opt_.meqn, st_), "time-sync store flux");
+        ++cnt_.count_kernel_launches;
+    }
+    const int v = time_sync_ ? 1 : opt_.step_variant == 0 ? tune_step_form(a, n) : opt_.step_variant;
     step_form_used_ = v;
     if (opt_.precision == 1) {
         e = launch_step_pipe_mixed(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc,
@@ -842,19 +1053,23 @@ void Context::run_schedule(double t_curr, double dt) {
                 int ti_level = gmax - 1;
                 while (last_step % ts[ti_level].step_inc == 0) --ti_level;
                 ghost_update(ti_level + 1, gmax, sync_time, 1);
+                if (time_sync_) time_sync(ti_level + 1);  // fclaw2d_advance.c:298-303
             } else {
                 ghost_update(gmin, gmax, sync_time, 0);
+                if (time_sync_) time_sync(gmin);
             }
         }
     }
     ghost_update(gmin, gmax, ts[gmax].current_time, 0);
+    if (time_sync_) time_sync(gmin);  // fclaw2d_advance.c:337-341
 }
 
 std::vector<uintptr_t> Context::macro_fingerprint() const {
     return {(uintptr_t)d_q_, (uintptr_t)d_qlast_, (uintptr_t)d_qti_, (uintptr_t)d_meta_,
             (uintptr_t)d_level_slots_.p, (uintptr_t)d_ti_slots_.p, (uintptr_t)d_ops_.p, (uintptr_t)d_groups_.p,
             (uintptr_t)d_dyn_.p, (uintptr_t)d_cfl_, (uintptr_t)mesh_version_, (uintptr_t)plans_.size(),
-            (uintptr_t)dyn_n_, (uintptr_t)gmin_, (uintptr_t)gmax_};
+            (uintptr_t)dyn_n_, (uintptr_t)gmin_, (uintptr_t)gmax_, (uintptr_t)d_treg_,
+            (uintptr_t)d_ts_ops_.p, (uintptr_t)d_ts_groups_.p, (uintptr_t)ts_plans_.size()};
 }
 
 void Context::drop_macro_graph() {
@@ -1158,7 +1373,7 @@ void Context::restore_step() {
 
 size_t Context::device_bytes() const {
     const int arenas = 3 + (d_qsave_ ? 1 : 0);
-    return (size_t)capacity_ * ((size_t)stride_ * arenas + (size_t)aux_stride_) * sizeof(double) +
+    return (size_t)capacity_ * ((size_t)stride_ * arenas + (size_t)aux_stride_ + (size_t)treg_stride_) * sizeof(double) +
            (size_t)capacity_ * sizeof(PatchMeta) + h_ops_.size() * sizeof(GhostOp);
 }
 
@@ -1361,6 +1576,14 @@ void Context::repopulate(const std::vector<Leaf>& old_leaves, const std::vector<
         }
     }
     slot_of_ = ns;
+    if (time_sync_ && !fresh.empty()) {
+        // fclaw2d_clawpatch_time_sync_new: every new patch starts with zero registers
+        DevBuf<int32_t> df;
+        df.reserve(fresh.size());
+        check(cudaMemcpy(df.p, fresh.data(), fresh.size() * 4, cudaMemcpyHostToDevice), "fresh slots");
+        check(launch_zero_registers(d_treg_, treg_stride_, df.p, (int)fresh.size(), st_), "zero registers");
+        check(cudaStreamSynchronize(st_), "sync");
+    }
     // metadata of the new mesh is needed by qinit; transfers only need slots
     if (domain_init) {
         mesh_changed();

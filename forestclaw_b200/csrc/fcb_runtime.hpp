@@ -40,6 +40,10 @@ struct GhostArgs;
 // Lane add/multiply operations per second of this GPU in FP64 (fp64) or FP32
 // (fcb_probe.cu).
 cudaError_t measure_fp_rate(bool fp64, cudaStream_t st, double* ops_per_second);
+// Time synchronisation (fcb_timesync.cu).
+cudaError_t launch_ts_store_flux(const StepArgs& a, int mx, int my, int mbc, int meqn, cudaStream_t st);
+cudaError_t launch_ts_apply(const TsArgs& a, cudaStream_t st);
+cudaError_t launch_zero_registers(double* treg, int64_t stride, const int32_t* slots, int n, cudaStream_t st);
 cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st, int unroll);
 cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64_t stride,
                               const int32_t* slots, int n, int mx, int my, int mbc, int meqn,
@@ -150,6 +154,26 @@ class Context {
     void prefetch_plans();
     void upload_ops();
     std::vector<std::tuple<int, int, int>> dry_plan_keys_;  // plans the dry pass met
+    // time synchronisation: registers, and per minlevel the launches of one
+    // fclaw2d_time_sync call (records grouped per patch, groups per launch)
+    struct TsPlan {
+        std::vector<size_t> first_group;  // per launch: first group in the group buffer
+        std::vector<int> ngroups;         // per launch
+    };
+    void time_sync(int minlevel);
+    const TsPlan& ts_plan(int minlevel);
+    bool time_sync_ = false;
+    double* d_treg_ = nullptr;
+    int64_t treg_stride_ = 0;
+    std::map<int, TsPlan> ts_plans_;
+    std::vector<TsOp> h_ts_ops_;
+    std::vector<int32_t> h_ts_groups_;
+    DevBuf<TsOp> d_ts_ops_;
+    DevBuf<int32_t> d_ts_groups_;
+    TsOp* h_ts_ops_pinned_ = nullptr;
+    size_t h_ts_ops_pinned_cap_ = 0;
+    int32_t* h_ts_groups_pinned_ = nullptr;
+    size_t h_ts_groups_pinned_cap_ = 0;
     std::vector<std::tuple<int, int, int>> plan_todo_;
     std::vector<PlanBuild> plan_built_;
     std::vector<std::exception_ptr> plan_err_;

@@ -14,7 +14,7 @@ namespace {
 auto launch_key(const fcb_options_t& o) {
     return std::make_tuple(o.solver_kind, o.problem, o.mx, o.my, o.mbc, o.meqn, o.maux, o.mwaves, o.order[0],
                            o.order[1], std::vector<int>(o.mthlim, o.mthlim + 8), o.precision, o.claw_version,
-                           o.grav, o.gamma, o.dry_tolerance);
+                           o.grav, o.gamma, o.dry_tolerance, o.ax, o.bx, o.ay, o.by);
 }
 
 }  // namespace
@@ -43,6 +43,7 @@ int Server::submit(const fcb_options_t& opt) {
     if (opt.step_variant == 1 || opt.step_variant == 2)
         throw Error(FCB_ERR_INVALID, "served solves use the pipelined step form");
     if (opt.nout != 1) throw Error(FCB_ERR_INVALID, "served solves run to tfinal in one output interval (nout = 1)");
+    if (opt.time_sync) throw Error(FCB_ERR_INVALID, "served solves do not run the time synchronisation");
     Request r;
     r.id = next_id_++;
     r.opt = opt;

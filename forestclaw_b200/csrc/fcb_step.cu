@@ -458,6 +458,29 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 const double gpv = GXs_m2[m] + FYp_prev[m];         // gp(i, j)
                 const double qv = q_m2[m] - dtdx * (fmv - fpv) - dtdy * (gmv - gpv);
                 q[((int64_t)m * NY + r) * NX + c] = qv;
+                if (a.treg) {
+                    // time-sync: boundary fluctuations scaled by dt and the edge
+                    // length (clawpack46_time_sync_accumulate_waves); each
+                    // register element has exactly one writer
+                    const RegLayout RL{MX, MX, M};
+                    double* R = a.treg + (int64_t)slot * a.treg_stride;
+                    const int i = c - MBC + 1, j = r - MBC + 1;
+                    const double dty = step_dt(a) * meta.dy, dtx = step_dt(a) * meta.dx;
+                    if (j >= 1 && j <= MX) {
+                        const int k = (j - 1) + MX * m;
+                        if (i == 1) R[RL.fp(0) + k] = R[RL.fp(0) + k] - dty * fpv;
+                        if (i == 0) R[RL.fm(0) + k] = R[RL.fm(0) + k] + dty * fmv;         // fm(1, j)
+                        if (i == MX) R[RL.fm(1) + k] = R[RL.fm(1) + k] + dty * fmv;        // fm(mx+1, j)
+                        if (i == MX + 1) R[RL.fp(1) + k] = R[RL.fp(1) + k] - dty * fpv;    // fp(mx+1, j)
+                    }
+                    if (i >= 1 && i <= MX) {
+                        const int k = (i - 1) + MX * m;
+                        if (j == 1) R[RL.gp(0) + k] = R[RL.gp(0) + k] - dtx * gpv;
+                        if (j == 0) R[RL.gm(0) + k] = R[RL.gm(0) + k] + dtx * gmv;         // gm(i, 1)
+                        if (j == MX) R[RL.gm(1) + k] = R[RL.gm(1) + k] + dtx * gmv;        // gm(i, my+1)
+                        if (j == MX + 1) R[RL.gp(1) + k] = R[RL.gp(1) + k] - dtx * gpv;    // gp(i, my+1)
+                    }
+                }
             }
         }
         // rotate per-row registers

@@ -57,8 +57,11 @@ enum fcb_problem {
     FCB_PROBLEM_SWIRL = 0,      /* advection/2d/swirl: qinit.f, b4step2.f velocities; p[0] = tperiod */
     FCB_PROBLEM_RADIALDAM = 1,  /* dam break: p = {x0, y0, r0, h_in, h_out} */
     FCB_PROBLEM_QUADRANTS = 2,  /* euler/2d/quadrants qinit.f: p = rho[4], u[4], v[4], p[4], xs, ys */
-    FCB_PROBLEM_BATHY = 3       /* lake at rest over b = -1 + 0.8 exp(-((x-.5)^2+(y-.5)^2)/0.02)
+    FCB_PROBLEM_BATHY = 3,      /* lake at rest over b = -1 + 0.8 exp(-((x-.5)^2+(y-.5)^2)/0.02)
                                  * with a surface pulse p[2] exp(-((x-p[0])^2+(y-p[1])^2)/p[3]^2) */
+    FCB_PROBLEM_RADIALDAM_CELLAVE = 4  /* the reference's radialdam qinit (radialdam/user_4.6/qinit.f):
+                                 * depth p[3]*w + p[4]*(1-w), w the fraction of the cell inside the
+                                 * circle about (p[0], p[1]) of radius p[2] (cellave2.f) */
 };
 
 /* Refinement criteria (fclaw2d_clawpatch_options "refinement-criteria"). */
@@ -67,7 +70,8 @@ enum fcb_criteria { FCB_TAG_VALUE = 0, FCB_TAG_MINMAX = 1, FCB_TAG_DIFFERENCE = 
 /*
  * The fields of fclaw_options_t, fclaw2d_clawpatch_options_t and
  * fc2d_clawpack46_options_t that the patch hot path reads (names as in the
- * reference's ini sections).  The domain is the unit square (ax=0,bx=1,ay=0,by=1).
+ * reference's ini sections).  One unmapped block: the unit square, or
+ * [ax, bx] x [ay, by] when those are set.
  */
 typedef struct fcb_options {
     /* [clawpatch] */
@@ -119,6 +123,15 @@ typedef struct fcb_options {
     int claw_version;
     /* GeoClaw /common_swe/ dry_tolerance */
     double dry_tolerance;
+    /* [Options] time-sync: conservative correction of coarse cells at
+     * coarse/fine faces and of edge cells at same-size faces after every
+     * synchronisation of levels (fclaw2d_time_sync.c; flux-correction and
+     * fluctuation-correction on).  Shallow-water Roe solver, clawpack 4.6, FP64,
+     * four-barrier step form (step_variant 0 or 1). */
+    int time_sync;
+    /* [Options] ax, bx, ay, by: physical extent of the block; all four zero
+     * means the unit square */
+    double ax, bx, ay, by;
 } fcb_options_t;
 
 typedef struct fcb_counters {
