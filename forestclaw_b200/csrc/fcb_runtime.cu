@@ -86,7 +86,6 @@ Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
     if (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE) {
         if (opt_.maux != 1) bad("the GeoClaw solver reads aux(1) = b: maux must be 1");
         if (opt_.order[1] != 0) bad("rpt2_geoclaw stops in the reference: the GeoClaw solver needs order (., 0)");
-        if (opt_.precision != 0) bad("the GeoClaw solver is FP64 only");
         if (opt_.claw_version == 5) bad("the GeoClaw solver is on the clawpack 4.6 path");
         if (opt_.step_variant == 1 || opt_.step_variant == 2)
             bad("the GeoClaw solver exists in the pipelined step form only");

@@ -315,129 +315,139 @@ using Euler4RoeSolver = Euler4RoeT<double>;
 // ---------------------------------------------------------------------------
 // GeoClaw f-wave solver: applications/clawpack/shallow/2d/rp/rpn2_geoclaw.f90
 // with geoclaw_riemann_utils.f (riemanntype, riemann_aug_JCP, maxiter = 1).
-// FP64 only.  The reference stops on a negative depth or a sonic state; here
-// such an interface sets `bad`, which the kernel reports as a NaN CFL.  The
+// The reference stops on a negative depth or a sonic state; here such an
+// interface sets `bad`, which the kernel reports as a NaN CFL.  The
 // reference's rpt2_geoclaw stops on entry, so no transverse solver exists.
+//
+// R = double is the reference's arithmetic.  R = float is the mixed form: the
+// speed estimates, the 3x3 f-wave solve and the waves in FP32, while the
+// hydrostatic part stays FP64 -- the states, dry-state and wall handling, the
+// bathymetry jump and the jumps del = (delh - deldelh, delhu, delphi -
+// deldelphi) the waves are solved for -- so that a lake at rest gives del = 0
+// and no waves.  Every R expression keeps the FP64 form's association, so
+// R = double compiles to the same arithmetic.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double fsignd(double a, double b) { return signbit(b) ? -fabs(a) : fabs(a); }
 
-__device__ __forceinline__ void geo_riemanntype(double hL, double hR, double uL, double uR, double& hm, double& s1m,
-                                                double& s2m, double drytol, double g) {
-    const double h_min = fmin(hR, hL), h_max = fmax(hR, hL);
-    const double delu = uR - uL;
+template <typename R>
+__device__ __forceinline__ void geo_riemanntype(R hL, R hR, R uL, R uR, R& hm, R& s1m, R& s2m, R drytol, R g) {
+    const R h_min = fmin(hR, hL), h_max = fmax(hR, hL);
+    const R delu = uR - uL;
     if (h_min <= drytol) {
-        hm = 0.0;
-        s1m = uR + uL - 2.0 * sqrt(g * hR) + 2.0 * sqrt(g * hL);
+        hm = R(0.0);
+        s1m = uR + uL - R(2.0) * sqrt(g * hR) + R(2.0) * sqrt(g * hL);
         s2m = s1m;
     } else {
-        const double F_min = delu + 2.0 * (sqrt(g * h_min) - sqrt(g * h_max));
-        const double F_max = delu + (h_max - h_min) * (sqrt(.5 * g * (h_max + h_min) / (h_max * h_min)));
-        if (F_min > 0.0) {
-            const double t = dmax(0.0, -delu + 2.0 * (sqrt(g * hL) + sqrt(g * hR)));
-            hm = (1.0 / (16.0 * g)) * (t * t);
-            s1m = uL + 2.0 * sqrt(g * hL) - 3.0 * sqrt(g * hm);
-            s2m = uR - 2.0 * sqrt(g * hR) + 3.0 * sqrt(g * hm);
-        } else if (F_max <= 0.0) {
-            double h0 = h_max;
+        const R F_min = delu + R(2.0) * (sqrt(g * h_min) - sqrt(g * h_max));
+        const R F_max = delu + (h_max - h_min) * (sqrt(R(.5) * g * (h_max + h_min) / (h_max * h_min)));
+        if (F_min > R(0.0)) {
+            const R t = dmax(R(0.0), -delu + R(2.0) * (sqrt(g * hL) + sqrt(g * hR)));
+            hm = (R(1.0) / (R(16.0) * g)) * (t * t);
+            s1m = uL + R(2.0) * sqrt(g * hL) - R(3.0) * sqrt(g * hm);
+            s2m = uR - R(2.0) * sqrt(g * hR) + R(3.0) * sqrt(g * hm);
+        } else if (F_max <= R(0.0)) {
+            R h0 = h_max;
             {
-                const double gL = sqrt(.5 * g * (1 / h0 + 1 / hL));
-                const double gR = sqrt(.5 * g * (1 / h0 + 1 / hR));
-                const double F0 = delu + (h0 - hL) * gL + (h0 - hR) * gR;
-                const double dfdh = gL - g * (h0 - hL) / (4.0 * (h0 * h0) * gL) + gR - g * (h0 - hR) / (4.0 * (h0 * h0) * gR);
-                const double slope = 2.0 * sqrt(h0) * dfdh;
-                const double t = sqrt(h0) - F0 / slope;
+                const R gL = sqrt(R(.5) * g * (R(1) / h0 + R(1) / hL));
+                const R gR = sqrt(R(.5) * g * (R(1) / h0 + R(1) / hR));
+                const R F0 = delu + (h0 - hL) * gL + (h0 - hR) * gR;
+                const R dfdh = gL - g * (h0 - hL) / (R(4.0) * (h0 * h0) * gL) + gR -
+                               g * (h0 - hR) / (R(4.0) * (h0 * h0) * gR);
+                const R slope = R(2.0) * sqrt(h0) * dfdh;
+                const R t = sqrt(h0) - F0 / slope;
                 h0 = t * t;
             }
             hm = h0;
-            const double u1m = uL - (hm - hL) * sqrt((.5 * g) * (1 / hm + 1 / hL));
-            const double u2m = uR + (hm - hR) * sqrt((.5 * g) * (1 / hm + 1 / hR));
+            const R u1m = uL - (hm - hL) * sqrt((R(.5) * g) * (R(1) / hm + R(1) / hL));
+            const R u2m = uR + (hm - hR) * sqrt((R(.5) * g) * (R(1) / hm + R(1) / hR));
             s1m = u1m - sqrt(g * hm);
             s2m = u2m + sqrt(g * hm);
         } else {
-            double h0 = h_min;
+            R h0 = h_min;
             {
-                const double F0 = delu + 2.0 * (sqrt(g * h0) - sqrt(g * h_max)) +
-                                  (h0 - h_min) * sqrt(.5 * g * (1 / h0 + 1 / h_min));
-                const double slope = (F_max - F0) / (h_max - h_min);
+                const R F0 = delu + R(2.0) * (sqrt(g * h0) - sqrt(g * h_max)) +
+                             (h0 - h_min) * sqrt(R(.5) * g * (R(1) / h0 + R(1) / h_min));
+                const R slope = (F_max - F0) / (h_max - h_min);
                 h0 = h0 - F0 / slope;
             }
             hm = h0;
             if (hL > hR) {
-                s1m = uL + 2.0 * sqrt(g * hL) - 3.0 * sqrt(g * hm);
-                s2m = uL + 2.0 * sqrt(g * hL) - sqrt(g * hm);
+                s1m = uL + R(2.0) * sqrt(g * hL) - R(3.0) * sqrt(g * hm);
+                s2m = uL + R(2.0) * sqrt(g * hL) - sqrt(g * hm);
             } else {
-                s2m = uR - 2.0 * sqrt(g * hR) + 3.0 * sqrt(g * hm);
-                s1m = uR - 2.0 * sqrt(g * hR) + sqrt(g * hm);
+                s2m = uR - R(2.0) * sqrt(g * hR) + R(3.0) * sqrt(g * hm);
+                s1m = uR - R(2.0) * sqrt(g * hR) + sqrt(g * hm);
             }
         }
     }
 }
 
 // riemann_aug_JCP with maxiter = 1 and rarecorrectortest = .false.; returns false on a sonic state
+template <typename R>
 __device__ __forceinline__ bool geo_riemann_aug(double hL, double hR, double huL, double huR, double bL, double bR,
                                                 double uL, double uR, double vL, double vR, double phiL, double phiR,
-                                                double sE1, double sE2, double drytol, double g, double sw[3],
-                                                double fw[3][3]) {
+                                                R sE1, R sE2, double drytol, double g, R sw[3], R fw[3][3]) {
     const double rho = -9999999.0, pL = 0.0, pR = 0.0;
     const double delh = hR - hL, delhu = huR - huL, delphi = phiR - phiL, delb = bR - bL, delP = pR - pL;
-    double hm, s1m, s2m;
-    geo_riemanntype(hL, hR, uL, uR, hm, s1m, s2m, drytol, g);
-    double lambda[3];
+    R hm, s1m, s2m;
+    geo_riemanntype<R>(R(hL), R(hR), R(uL), R(uR), hm, s1m, s2m, R(drytol), R(g));
+    R lambda[3];
     lambda[0] = dmin(sE1, s2m);
     lambda[2] = dmax(sE2, s1m);
     sE1 = lambda[0];
     sE2 = lambda[2];
-    const double hstarHLL = dmax((huL - huR + sE2 * hR - sE1 * hL) / (sE2 - sE1), 0.0);
-    double r[3][3];
+    const R hstarHLL = dmax((R(huL) - R(huR) + sE2 * R(hR) - sE1 * R(hL)) / (sE2 - sE1), R(0.0));
+    R r[3][3];
 #pragma unroll
     for (int mw = 0; mw < 3; ++mw) {
-        r[0][mw] = 1.0;
-        r[1][mw] = (mw == 1) ? 0.0 : lambda[mw];
-        r[2][mw] = (mw == 1) ? 0.0 : lambda[mw] * lambda[mw];
+        r[0][mw] = R(1.0);
+        r[1][mw] = (mw == 1) ? R(0.0) : lambda[mw];
+        r[2][mw] = (mw == 1) ? R(0.0) : lambda[mw] * lambda[mw];
     }
-    lambda[1] = 0.5 * (lambda[0] + lambda[2]);
-    r[0][1] = 0.0;
-    r[1][1] = 0.0;
-    r[2][1] = 1.0;
+    lambda[1] = R(0.5) * (lambda[0] + lambda[2]);
+    r[0][1] = R(0.0);
+    r[1][1] = R(0.0);
+    r[2][1] = R(1.0);
     const double criticaltol = dmax(drytol * g, 1e-6);
     const double criticaltol_2 = sqrt(criticaltol);
     const double hbar = dmax(0.5 * (hL + hR), 0.0);
     const double s1s2bar = 0.25 * ((uL + uR) * (uL + uR)) - g * hbar;
     const double s1s2tilde = dmax(0.0, uL * uR) - g * hbar;
+    const double dE1 = sE1, dE2 = sE2, ds1m = s1m, ds2m = s2m;
     bool sonic = false;
     if (fabs(s1s2bar) <= criticaltol) sonic = true;
     else if (s1s2bar * s1s2tilde <= criticaltol * criticaltol) sonic = true;
-    else if (s1s2bar * sE1 * sE2 <= criticaltol * criticaltol) sonic = true;
-    else if (dmin(fabs(sE1), fabs(sE2)) < criticaltol_2) sonic = true;
-    else if (sE1 < criticaltol_2 && s1m > -criticaltol_2) sonic = true;
-    else if (sE2 > -criticaltol_2 && s2m < criticaltol_2) sonic = true;
+    else if (s1s2bar * dE1 * dE2 <= criticaltol * criticaltol) sonic = true;
+    else if (dmin(fabs(dE1), fabs(dE2)) < criticaltol_2) sonic = true;
+    else if (dE1 < criticaltol_2 && ds1m > -criticaltol_2) sonic = true;
+    else if (dE2 > -criticaltol_2 && ds2m < criticaltol_2) sonic = true;
     else if ((uL + sqrt(g * hL)) * (uR + sqrt(g * hR)) < 0.0) sonic = true;
     else if ((uL - sqrt(g * hL)) * (uR - sqrt(g * hR)) < 0.0) sonic = true;
     double deldelh = delb * g * hbar / s1s2bar;
-    if (sE1 < -criticaltol && sE2 > criticaltol) {
-        deldelh = dmin(deldelh, hstarHLL * (sE2 - sE1) / sE2);
-        deldelh = dmax(deldelh, hstarHLL * (sE2 - sE1) / sE1);
-    } else if (sE1 >= criticaltol) {
-        deldelh = dmin(deldelh, hstarHLL * (sE2 - sE1) / sE1);
+    if (dE1 < -criticaltol && dE2 > criticaltol) {
+        deldelh = dmin(deldelh, (double)(hstarHLL * (sE2 - sE1) / sE2));
+        deldelh = dmax(deldelh, (double)(hstarHLL * (sE2 - sE1) / sE1));
+    } else if (dE1 >= criticaltol) {
+        deldelh = dmin(deldelh, (double)(hstarHLL * (sE2 - sE1) / sE1));
         deldelh = dmax(deldelh, -hL);
-    } else if (sE2 <= -criticaltol) {
+    } else if (dE2 <= -criticaltol) {
         deldelh = dmin(deldelh, hR);
-        deldelh = dmax(deldelh, hstarHLL * (sE2 - sE1) / sE2);
+        deldelh = dmax(deldelh, (double)(hstarHLL * (sE2 - sE1) / sE2));
     }
     deldelh = deldelh - delP / (rho * g);
     double deldelphi = -(delb * g * hbar * s1s2tilde / s1s2bar);
     deldelphi = dmin(deldelphi, g * dmax(-hL * delb, -hR * delb));
     deldelphi = dmax(deldelphi, g * dmin(-hL * delb, -hR * delb));
     deldelphi = deldelphi - hbar * delP / rho;
-    const double del[3] = {delh - deldelh, delhu, delphi - deldelphi};
-    double det1 = r[0][0] * (r[1][1] * r[2][2] - r[1][2] * r[2][1]);
-    double det2 = r[0][1] * (r[1][0] * r[2][2] - r[1][2] * r[2][0]);
-    double det3 = r[0][2] * (r[1][0] * r[2][1] - r[1][1] * r[2][0]);
-    const double determinant = det1 - det2 + det3;
-    double beta[3];
+    const R del[3] = {R(delh - deldelh), R(delhu), R(delphi - deldelphi)};
+    R det1 = r[0][0] * (r[1][1] * r[2][2] - r[1][2] * r[2][1]);
+    R det2 = r[0][1] * (r[1][0] * r[2][2] - r[1][2] * r[2][0]);
+    R det3 = r[0][2] * (r[1][0] * r[2][1] - r[1][1] * r[2][0]);
+    const R determinant = det1 - det2 + det3;
+    R beta[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        double A[3][3];
+        R A[3][3];
 #pragma unroll
         for (int mw = 0; mw < 3; ++mw)
 #pragma unroll
@@ -454,18 +464,18 @@ __device__ __forceinline__ bool geo_riemann_aug(double hL, double hR, double huL
         fw[1][mw] = beta[mw] * r[2][mw];
         fw[2][mw] = beta[mw] * r[1][mw];
     }
-    fw[2][0] = fw[2][0] * vL;
-    fw[2][2] = fw[2][2] * vR;
-    fw[2][1] = 0.0;
-    const double hustar_interface = huL + fw[0][0];
-    if (hustar_interface <= 0.0) fw[2][0] = fw[2][0] + (hR * uR * vR - hL * uL * vL - fw[2][0] - fw[2][2]);
-    else fw[2][2] = fw[2][2] + (hR * uR * vR - hL * uL * vL - fw[2][0] - fw[2][2]);
+    fw[2][0] = fw[2][0] * R(vL);
+    fw[2][2] = fw[2][2] * R(vR);
+    fw[2][1] = R(0.0);
+    const double hustar_interface = huL + (double)fw[0][0];
+    const R dvflux = R(hR * uR * vR - hL * uL * vL);
+    if (hustar_interface <= 0.0) fw[2][0] = fw[2][0] + (dvflux - fw[2][0] - fw[2][2]);
+    else fw[2][2] = fw[2][2] + (dvflux - fw[2][0] - fw[2][2]);
     return !sonic;
 }
 
 template <typename R, bool V5_ = false>
 struct GeoclawFwaveT {
-    static_assert(sizeof(R) == sizeof(double), "the GeoClaw solver is FP64 only");
     using Real = R;
     static constexpr bool V5 = V5_;
     static constexpr bool FWAVE = true;
@@ -473,62 +483,64 @@ struct GeoclawFwaveT {
     static constexpr int W = 3;
     struct Roe {};
     R grav, gamma, gamma1, drytol;
-    // one interface of rpn2_geoclaw.f90; bL, bR: aux(1) of the two cells
+    // one interface of rpn2_geoclaw.f90; the states and bL, bR (aux(1) of the
+    // two cells) in FP64
     __device__ __forceinline__ void rpn2b(int ixy, const double* qL, const double* qR, double bL, double bR,
-                                          double (*wave)[M], double* s, double* amdq, double* apdq,
-                                          bool& bad) const {
+                                          R (*wave)[M], R* s, R* amdq, R* apdq, bool& bad) const {
         const int mu = (ixy == 1) ? 1 : 2;
         const int mv = (ixy == 1) ? 2 : 1;
-        const double g = grav;
+        // the FP64 hydrostatic part reads gravity and the dry tolerance in FP64
+        const double g = gdbl, dtol = drytol_d;
 #pragma unroll
         for (int mw = 0; mw < 3; ++mw) {
-            s[mw] = 0.0;
-            wave[mw][0] = 0.0; wave[mw][1] = 0.0; wave[mw][2] = 0.0;
+            s[mw] = R(0.0);
+            wave[mw][0] = R(0.0); wave[mw][1] = R(0.0); wave[mw][2] = R(0.0);
         }
         if (qL[0] < 0.0 || qR[0] < 0.0) bad = true;
-        if (!(qL[0] <= drytol && qR[0] <= drytol)) {
+        if (!(qL[0] <= dtol && qR[0] <= dtol)) {
             double hL = qL[0], hR = qR[0], huL = qL[mu], huR = qR[mu], hvL = qL[mv], hvR = qR[mv];
             double uR, vR, phiR, uL, vL, phiL;
-            if (hR > drytol) {
+            if (hR > dtol) {
                 uR = huR / hR; vR = hvR / hR;
-                phiR = 0.5 * grav * (hR * hR) + (huR * huR) / hR;
+                phiR = 0.5 * g * (hR * hR) + (huR * huR) / hR;
             } else {
                 hR = 0.0; huR = 0.0; hvR = 0.0; uR = 0.0; vR = 0; phiR = 0.0;
             }
-            if (hL > drytol) {
+            if (hL > dtol) {
                 uL = huL / hL; vL = hvL / hL;
-                phiL = 0.5 * grav * (hL * hL) + (huL * huL) / hL;
+                phiL = 0.5 * g * (hL * hL) + (huL * huL) / hL;
             } else {
                 hL = 0.0; huL = 0.0; hvL = 0.0; uL = 0.0; vL = 0.0; phiL = 0.0;
             }
-            double wall[3] = {1.0, 1.0, 1.0};
+            R wall[3] = {R(1.0), R(1.0), R(1.0)};
             double hstar, s1m, s2m;
-            if (hR <= drytol) {
-                geo_riemanntype(hL, hL, uL, -uL, hstar, s1m, s2m, drytol, grav);
+            if (hR <= dtol) {
+                geo_riemanntype<double>(hL, hL, uL, -uL, hstar, s1m, s2m, dtol, g);
                 const double hstartest = dmax(hL, hstar);
                 if (hstartest + bL < bR) {
-                    wall[1] = 0.0; wall[2] = 0.0;
+                    wall[1] = R(0.0); wall[2] = R(0.0);
                     hR = hL; huR = -huL; bR = bL; phiR = phiL; uR = -uL; vL = vR;
                 } else if (hL + bL < bR) {
                     bR = hL + bL;
                 }
-            } else if (hL <= drytol) {
-                geo_riemanntype(hR, hR, -uR, uR, hstar, s1m, s2m, drytol, grav);
+            } else if (hL <= dtol) {
+                geo_riemanntype<double>(hR, hR, -uR, uR, hstar, s1m, s2m, dtol, g);
                 const double hstartest = dmax(hR, hstar);
                 if (hstartest + bR < bL) {
-                    wall[0] = 0.0; wall[1] = 0.0;
+                    wall[0] = R(0.0); wall[1] = R(0.0);
                     hL = hR; huL = -huR; bL = bR; phiL = phiR; uL = -uR; vR = vL;
                 } else if (hR + bR < bL) {
                     bL = hR + bR;
                 }
             }
-            const double sL = uL - sqrt(grav * hL);
-            const double sR = uR + sqrt(grav * hR);
-            const double uhat = (sqrt(grav * hL) * uL + sqrt(grav * hR) * uR) / (sqrt(grav * hR) + sqrt(grav * hL));
-            const double chat = sqrt(grav * 0.5 * (hR + hL));
-            const double sE1 = dmin(sL, uhat - chat), sE2 = dmax(sR, uhat + chat);
-            double sw[3], fw[3][3];
-            if (!geo_riemann_aug(hL, hR, huL, huR, bL, bR, uL, uR, vL, vR, phiL, phiR, sE1, sE2, drytol, g, sw, fw))
+            const R rg = R(g);
+            const R sL = R(uL) - sqrt(rg * R(hL));
+            const R sR = R(uR) + sqrt(rg * R(hR));
+            const R uhat = (sqrt(rg * R(hL)) * R(uL) + sqrt(rg * R(hR)) * R(uR)) / (sqrt(rg * R(hR)) + sqrt(rg * R(hL)));
+            const R chat = sqrt(rg * R(0.5) * (R(hR) + R(hL)));
+            const R sE1 = dmin(sL, uhat - chat), sE2 = dmax(sR, uhat + chat);
+            R sw[3], fw[3][3];
+            if (!geo_riemann_aug<R>(hL, hR, huL, huR, bL, bR, uL, uR, vL, vR, phiL, phiR, sE1, sE2, dtol, g, sw, fw))
                 bad = true;
 #pragma unroll
             for (int mw = 0; mw < 3; ++mw) {
@@ -540,20 +552,21 @@ struct GeoclawFwaveT {
         }
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            double am = 0.0, ap = 0.0;
+            R am = R(0.0), ap = R(0.0);
 #pragma unroll
             for (int mw = 0; mw < 3; ++mw) {
-                if (s[mw] < 0.0) am = am + wave[mw][m];
-                else if (s[mw] > 0.0) ap = ap + wave[mw][m];
+                if (s[mw] < R(0.0)) am = am + wave[mw][m];
+                else if (s[mw] > R(0.0)) ap = ap + wave[mw][m];
                 else {
-                    am = am + 0.5 * wave[mw][m];
-                    ap = ap + 0.5 * wave[mw][m];
+                    am = am + R(0.5) * wave[mw][m];
+                    ap = ap + R(0.5) * wave[mw][m];
                 }
             }
             amdq[m] = am;
             apdq[m] = ap;
         }
     }
+    double gdbl, drytol_d;  // gravity and dry tolerance in FP64, set by the step kernel
     // never called: order (2, 0) is enforced for this solver
     __device__ __forceinline__ void rpt2(int, const R* asdq, const Roe&, R, R, R* bm, R* bp) const {
 #pragma unroll

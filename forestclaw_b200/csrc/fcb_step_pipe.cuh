@@ -33,6 +33,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "fcb_device.h"
 #include "fcb_solvers.cuh"
 
@@ -65,25 +67,36 @@ __device__ __forceinline__ double psi_node(double tx, double ty) {
     else return (tx * ty) * (1.0 / pi);
 }
 
-template <int NX, int PPB, int M, int W, int NAUX, bool SWIRL, typename R>
+// Type of the state and aux rings: the compute type, except for the f-wave
+// solver, whose hydrostatic part reads FP64 states and bathymetry; in its mixed
+// form those two rings live in the FP64 region.
+template <class SOL>
+using ring_t = std::conditional_t<SOL::FWAVE, double, typename SOL::Real>;
+template <class SOL>
+constexpr bool ring_in_fp64 = SOL::FWAVE && !std::is_same_v<typename SOL::Real, double>;
+
+template <int NX, int PPB, int M, int W, int NAUX, bool SWIRL, typename R, bool QDBL = false>
 struct PipeSmem {
     // Rings are [slot][component][patch][column]: one thread's element of any
     // ring sits at (pl * NX + c) + a compile-time offset.
     static constexpr int PNX = PPB * NX;
-    // rings in the compute type R (offsets in R elements)
-    static constexpr int Q = 0;                       // 2 slots x M
-    static constexpr int XW = Q + 2 * M * PNX;        // 2 slots x W*M
+    // rings in the compute type R (offsets in R elements); with QDBL the state
+    // (Q) and aux (AX) rings are in the FP64 region instead
+    static constexpr int XW = QDBL ? 0 : 2 * M * PNX; // 2 slots x W*M (after Q: 2 slots x M)
     static constexpr int GL = XW + 2 * W * M * PNX;   // 2 slots x 2M
     static constexpr int FX = GL + 2 * 2 * M * PNX;   // 4 slots x 2M
-    static constexpr int AX = FX + 4 * 2 * M * PNX;   // 4 slots x NAUX
-    static constexpr int NR = AX + 4 * NAUX * PNX;
+    static constexpr int AXR = FX + 4 * 2 * M * PNX;  // 4 slots x NAUX
+    static constexpr int NR = QDBL ? AXR : AXR + 4 * NAUX * PNX;
     // FP64 region, from byte DBYTES on (offsets in doubles)
     static constexpr int DBYTES = ((NR * (int)sizeof(R) + 15) / 16) * 16;
     static constexpr int GY = 0;                      // 4 slots x 2M: y transverse sums
     static constexpr int NDS = PPB * (NX + 1);
     static constexpr int TY = GY + 4 * 2 * M * PNX;   // swirl: sin^2 of the node rows [patch][NX+1]
     static constexpr int ND = TY + (SWIRL ? NDS : 0); // swirl: psi node rows, 2 slots [patch][NX+1]
-    static constexpr int BYTES = DBYTES + (ND + (SWIRL ? 2 * NDS : 0)) * 8;
+    static constexpr int NDEND = ND + (SWIRL ? 2 * NDS : 0);
+    static constexpr int Q = QDBL ? NDEND : 0;
+    static constexpr int AX = QDBL ? NDEND + 2 * M * PNX : AXR;
+    static constexpr int BYTES = DBYTES + (QDBL ? NDEND + 2 * M * PNX + 4 * NAUX * PNX : NDEND) * 8;
 };
 
 // Values a thread carries from one row-iteration to the next.  R is the
@@ -134,12 +147,17 @@ template <class SOL, int MX, int MBC, int AUXK, int NAUX, int PPB, int LIM, int 
 __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                                           const PipeThread<typename SOL::Real>& T, PipeState<SOL>& S, int s) {
     using R = typename SOL::Real;
+    using QT = ring_t<SOL>;
     constexpr int M = SOL::M;
     constexpr int W = SOL::W;
     constexpr int NX = MX + 2 * MBC;
     constexpr int NY = NX;
     constexpr bool SWIRL = AUXK == AUX_SWIRL;
-    using L = PipeSmem<NX, PPB, M, W, NAUX, SWIRL, R>;
+    constexpr bool QDBL = ring_in_fp64<SOL>;
+    using L = PipeSmem<NX, PPB, M, W, NAUX, SWIRL, R, QDBL>;
+    QT* qb;  // this thread's element of the state and aux rings
+    if constexpr (QDBL) qb = T.db;
+    else qb = T.rb;
     const Method<LIM> meth{a};
     // clawpack 5 (clawpack5_flux2.f, clawpack5_step2.f90, clawpack5_step2_wrap.f):
     // fluxes at interfaces 1..mx+1 only, accumulated into cells 1..mx+1, and
@@ -157,9 +175,9 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
     auto s2 = [&](int d) -> int { return J >= 0 ? cslot(J, d, 2) : ((s - d) & 1); };
     auto s4 = [&](int d) -> int { return J >= 0 ? cslot(J, d, 4) : ((s - d) & 3); };
     // aux component k of row s-d, column c+dc
-    auto AUXV = [&](int k, int dc, int d) -> R {
-        if constexpr (NAUX > 0) return k < NAUX ? T.rb[L::AX + (s4(d) * NAUX + k) * L::PNX + dc] : R(0);
-        else return R(0);
+    auto AUXV = [&](int k, int dc, int d) -> QT {
+        if constexpr (NAUX > 0) return k < NAUX ? qb[L::AX + (s4(d) * NAUX + k) * L::PNX + dc] : QT(0);
+        else return QT(0);
     };
 
     // prefetch q(c, s+1); load q(c, s-4) for this iteration's update early
@@ -328,12 +346,12 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
     {
         const int k = s - 1;
         if (T.active && (STEADY || (k >= 1 && k <= NY - 2)) && c >= 1) {
-            const R* qr = T.rb + L::Q + s2(1) * (M * L::PNX);
-            R qL[M], qR[M];
+            const QT* qr = qb + L::Q + s2(1) * (M * L::PNX);
+            QT qL[M], qR[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 qL[m] = qr[m * L::PNX - 1];
-                qR[m] = R(S.q_m1[m]);
+                qR[m] = QT(S.q_m1[m]);
             }
             if constexpr (FWAVE) {
                 bool bad = false;
@@ -365,19 +383,19 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
 #pragma unroll
         for (int m = 0; m < M; ++m) yam_n[m] = yap_n[m] = R(0);
         if (T.active && (STEADY || s < NY)) {
-            R* qr = T.rb + L::Q + s2(0) * (M * L::PNX);
+            QT* qr = qb + L::Q + s2(0) * (M * L::PNX);
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 if (T.save_last) T.qlast[((int64_t)m * NY + s) * NX] = S.qcur[m];
-                qr[m * L::PNX] = R(S.qcur[m]);
+                qr[m * L::PNX] = QT(S.qcur[m]);
             }
             // raw y-interface s (between rows s-1 and s)
             if (T.ycol && (STEADY || s >= 1)) {
-                R qD[M], qU[M];
+                QT qD[M], qU[M];
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
-                    qD[m] = R(S.q_m1[m]);
-                    qU[m] = R(S.qcur[m]);
+                    qD[m] = QT(S.q_m1[m]);
+                    qU[m] = QT(S.qcur[m]);
                 }
                 if constexpr (FWAVE) {
                     bool bad = false;
@@ -534,16 +552,16 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 const double pn = psi_node<R>(T.tx, T.ty[s + 2]);
                 if (T.node) T.nb[s2(-2) * L::NDS] = pn;
                 if (T.active) {
-                    R* ax = T.rb + L::AX + s4(-1) * (NAUX * L::PNX);
-                    ax[0 * L::PNX] = R(T.vty * (pn - S.pcur));
-                    ax[1 * L::PNX] = R(-T.vtx * (T.nb[s2(-1) * L::NDS + 1] - S.pcur));
+                    QT* ax = qb + L::AX + s4(-1) * (NAUX * L::PNX);
+                    ax[0 * L::PNX] = QT(T.vty * (pn - S.pcur));
+                    ax[1 * L::PNX] = QT(-T.vtx * (T.nb[s2(-1) * L::NDS + 1] - S.pcur));
                 }
                 S.pcur = pn;
             } else if constexpr (AUXK == AUX_STORED) {
                 if (T.active) {
-                    R* ax = T.rb + L::AX + s4(-1) * (NAUX * L::PNX);
+                    QT* ax = qb + L::AX + s4(-1) * (NAUX * L::PNX);
 #pragma unroll
-                    for (int kk = 0; kk < NAUX; ++kk) ax[kk * L::PNX] = R(T.aux[(kk * NY + s + 1) * NX]);
+                    for (int kk = 0; kk < NAUX; ++kk) ax[kk * L::PNX] = QT(T.aux[(kk * NY + s + 1) * NX]);
                 }
             }
         }
@@ -566,7 +584,8 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     constexpr int TPP = pipe_threads_per_patch<NX, SWIRL>();
     constexpr int PPB = TPB / TPP;
     using R = typename SOL::Real;
-    using L = PipeSmem<NX, PPB, M, W, NAUX, SWIRL, R>;
+    using QT = ring_t<SOL>;
+    using L = PipeSmem<NX, PPB, M, W, NAUX, SWIRL, R, ring_in_fp64<SOL>>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* const rsm = reinterpret_cast<R*>(smem_raw);
     double* const dsm = reinterpret_cast<double*>(smem_raw + L::DBYTES);
@@ -586,7 +605,11 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     const int slot = (patch_ok && !a.desc) ? a.slots[pg] : 0;
     const PatchMeta meta = D ? D->meta : (patch_ok ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0});
     const int req = D ? D->req : -1;
-    const SOL sol{R(a.grav), R(a.gamma), R(a.gamma1), R(a.drytol)};
+    SOL sol{R(a.grav), R(a.gamma), R(a.gamma1), R(a.drytol)};
+    if constexpr (SOL::FWAVE) {
+        sol.gdbl = a.grav;
+        sol.drytol_d = a.drytol;
+    }
 
     PipeThread<R> T;
     T.c = cc;
@@ -661,14 +684,17 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
         }
         __syncthreads();
         if (active) {
-            T.rb[L::AX + 0 * L::PNX] = R(T.vty * (p1 - p0));
-            T.rb[L::AX + 1 * L::PNX] = R(-T.vtx * (T.nb[1] - p0));
+            T.rb[L::AX + 0 * L::PNX] = QT(T.vty * (p1 - p0));
+            T.rb[L::AX + 1 * L::PNX] = QT(-T.vtx * (T.nb[1] - p0));
         }
         S.pcur = p1;
     } else if constexpr (AUXK == AUX_STORED) {
         if (active) {
 #pragma unroll
-            for (int k = 0; k < NAUX; ++k) T.rb[L::AX + k * L::PNX] = R(T.aux[(k * NY + 0) * NX]);
+            for (int k = 0; k < NAUX; ++k) {
+                if constexpr (ring_in_fp64<SOL>) T.db[L::AX + k * L::PNX] = T.aux[(k * NY + 0) * NX];
+                else T.rb[L::AX + k * L::PNX] = QT(T.aux[(k * NY + 0) * NX]);
+            }
         }
     }
     __syncthreads();
@@ -717,7 +743,7 @@ cudaError_t launch_pipe_one(const StepArgs& a, cudaStream_t st) {
     constexpr int NX = MX + 2 * MBC;
     constexpr int PPB = TPB / pipe_threads_per_patch<NX, AUXK == AUX_SWIRL>();
     static_assert(PPB >= 1, "patch wider than the CTA");
-    using L = PipeSmem<NX, PPB, SOL::M, SOL::W, NAUX, AUXK == AUX_SWIRL, typename SOL::Real>;
+    using L = PipeSmem<NX, PPB, SOL::M, SOL::W, NAUX, AUXK == AUX_SWIRL, typename SOL::Real, ring_in_fp64<SOL>>;
     const size_t bytes = (size_t)L::BYTES;
     static bool configured = false;
     if (!configured) {
@@ -785,7 +811,7 @@ cudaError_t launch_step_pipe_v(int solver, int aux_kind, int mwaves, int mx, int
             if (mwaves != 4 || aux_kind != AUX_NONE) return cudaErrorNotSupported;
             return launch_pipe_mx<Euler4RoeT<R, V5>, AUX_NONE, 0>(mx, mbc, a, st);
         case SOLVER_GEOCLAW_FWAVE:
-            if constexpr (sizeof(R) == sizeof(double) && !V5) {
+            if constexpr (!V5) {
                 if (mwaves != 3 || aux_kind != AUX_STORED || a.maux != 1) return cudaErrorNotSupported;
                 return launch_pipe_mx<GeoclawFwaveT<R>, AUX_STORED, 1>(mx, mbc, a, st);
             }

@@ -91,12 +91,11 @@ def test_geoclaw_amr_macro_steps(gpu_lib):
         assert _rel_err(d.get_q(), o.all_q()) <= REL_TOL, f"after regrid {k}"
 
 
-def test_geoclaw_rejects_transverse_order_and_mixed(gpu_lib):
+def test_geoclaw_rejects_transverse_order(gpu_lib):
     import forestclaw_b200 as fcb
 
     base = cases.to_options(cases.bathy_lake(level=1, mx=8))
-    for kw in ({"order": (2, 2)}, {"precision": fcb.PRECISION_MIXED}, {"claw_version": 5},
-               {"maux": 0}, {"step_variant": 1}):
+    for kw in ({"order": (2, 2)}, {"claw_version": 5}, {"maux": 0}, {"step_variant": 1}):
         o = cases.to_options(cases.bathy_lake(level=1, mx=8))
         for k, v in kw.items():
             setattr(o, k, v)

@@ -109,3 +109,44 @@ def test_mixed_amr_subcycled_with_fp32_interpolation(gpu_lib):
     assert l1 <= L1_TOL, f"L1 {l1:.3e}"
     assert mx_err <= MAX_TOL, f"max {mx_err:.3e}"
     assert _mass_drift(d, o) <= MASS_TOL
+
+
+def _central(leaves, level):
+    n = 1 << level
+    return [k for k, (lv, x, y) in enumerate(leaves)
+            if 2 <= (x >> (28 - lv)) <= n - 3 and 2 <= (y >> (28 - lv)) <= n - 3]
+
+
+def test_mixed_geoclaw_pulse_amr(gpu_lib):
+    """GeoClaw f-waves over bathymetry, subcycled levels 2-4 with FP32 ghost
+    interpolation: the state against the FP64 oracle within the contract, and
+    the pulse itself (q - q0, amplitude 0.05) to 1e-3 of its own L1 norm."""
+    cfg = cases.bathy_lake(minlevel=2, maxlevel=4, mx=16, seed=2, amp=0.05)
+    o, d = _pair(cfg)
+    q0 = o.all_q()
+    t, dt = 0.0, 0.5 / (16 * 4)
+    for k in range(3):
+        o.advance(t, dt)
+        d.advance_all_levels(t, dt)
+        t += dt
+    qd, qo = d.get_q(), o.all_q()
+    l1, mx = _errors(qd, qo, cfg.mbc)
+    assert l1 <= L1_TOL and mx <= MAX_TOL, (l1, mx)
+    m = cfg.mbc
+    pert = np.abs(qo - q0)[..., m:-m, m:-m].sum()
+    assert np.abs(qd - qo)[..., m:-m, m:-m].sum() <= 1e-3 * pert
+    assert _mass_drift(d, o) <= MASS_TOL
+
+
+def test_mixed_geoclaw_lake_at_rest(gpu_lib):
+    """The hydrostatic part stays FP64, so a lake at rest stays at rest to
+    FP64 round-off in the mixed form too (uniform level, central patches)."""
+    cfg = cases.bathy_lake(level=3, mx=16, amp=0.0)
+    o, d = _pair(cfg)
+    q0 = d.get_q()
+    dt = 0.5 / (16 * 8)
+    for k in range(10):
+        d.advance_all_levels(k * dt, dt)
+    inner = _central(d.leaves(), 3)
+    dq = np.abs(d.get_q() - q0)[inner][:, :, 2:-2, 2:-2]
+    assert float(dq.max()) <= 1e-14, f"lake-at-rest residual {dq.max():.3e}"
