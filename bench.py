@@ -46,7 +46,8 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="uniform_swirl", choices=["uniform_swirl", "amr_radialdam", "serve"])
+    p.add_argument("--workload", default="uniform_swirl",
+                   choices=["uniform_swirl", "amr_radialdam", "bathy", "serve"])
     p.add_argument("--requests", type=int, default=24, help="serve: number of requests")
     p.add_argument("--rates", default="5,20,80", help="serve: Poisson arrival rates (requests/s) to sweep")
     p.add_argument("--level", type=int, default=8)
@@ -352,6 +353,7 @@ FP64_OPS_PER_CELL = {
     ("advection_swirl_order22", 32): 169.875,
     ("swe_roe_order22", 16): 1244.9609,
     ("swe_roe_order22", 32): 1090.248,
+    ("geoclaw_fwave_order20", 32): 1326.3662,
 }
 
 
@@ -483,6 +485,133 @@ def amr_cpu_sample(budget_s):
 
 
 # ----------------------------------------------------------------------------
+# Shallow water over bathymetry (GeoClaw f-waves): lake at rest over a Gaussian
+# bump plus a surface pulse, levels 4..7, mx = 32, subcycled, gradient tagging,
+# regrid every macro step, fixed dt.  --precision mixed also reports the error
+# against the same run in FP64, the mass drift and the lake-at-rest residual.
+# ----------------------------------------------------------------------------
+def _bathy_cfg(amp=1e-3):
+    import cases
+
+    return cases.bathy_lake(minlevel=4, maxlevel=7, mx=32, seed=0, amp=amp, width=0.05)
+
+
+def _bathy_dt():
+    return 0.5 / (32 * 16)  # CFL about 0.5 on level 4 (|u| + sqrt(g h) <= 1)
+
+
+def _bathy_run(opts, steps, t0=0.0, stream=None, timed=False):
+    """advance + regrid `steps` times; returns (solver, advance ms, cells, patch
+    counts); the solver's `bench_launches` holds the launches of the advances."""
+    import torch
+
+    import forestclaw_b200 as fcb
+
+    s = fcb.Solver(opts, stream=stream.cuda_stream if stream is not None else 0)
+    s.initialize()
+    t, dt, ms, cells, patches = t0, _bathy_dt(), 0.0, 0, []
+    s.bench_launches = 0
+    for _ in range(steps):
+        c = s.counters()
+        c0, l0 = c["count_single_step"], c["count_kernel_launches"]
+        if timed:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        s.advance_all_levels(t, dt)
+        if timed:
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        c = s.counters()
+        cells += (c["count_single_step"] - c0) * opts.mx * opts.my
+        s.bench_launches += c["count_kernel_launches"] - l0
+        t += dt
+        s.regrid()
+        patches.append(s.num_patches)
+    torch.cuda.synchronize()
+    return s, ms, cells, patches
+
+
+def run_bathy(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import cases
+    import forestclaw_b200 as fcb
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.current_stream()
+    cfg = _bathy_cfg()
+    opts = cases.to_options(cfg)
+    opts.precision = fcb.PRECISION_MIXED if args.precision == "mixed" else fcb.PRECISION_FP64
+    opts.macro_graph = args.macro_graph
+    # warm-up: the first macro steps of the same run (plans, autotuning, graph)
+    w, _, _, _ = _bathy_run(opts, args.warmup, stream=stream)
+    w.close()
+    with ClockSampler(local_rank) as clk:
+        s, ms, cells, patches = _bathy_run(opts, args.steps, stream=stream, timed=True)
+    from forestclaw_b200 import replicas
+
+    ms_max, total_cells = replicas.aggregate(ms, cells, torch.distributed if world > 1 else None)
+    accuracy = None
+    if args.precision == "mixed" and rank == 0:
+        o64 = cases.to_options(cfg)
+        o64.macro_graph = args.macro_graph
+        ref, _, _, _ = _bathy_run(o64, args.steps, stream=stream)
+        acc = {"against": "the same run in FP64 on the GPU", "same_mesh": ref.leaves() == s.leaves()}
+        q0s = None
+        if acc["same_mesh"]:
+            qm, qf = s.get_q(), ref.get_q()
+            m = cfg.mbc
+            a, b = qm[..., m:-m, m:-m], qf[..., m:-m, m:-m]
+            acc["l1_rel"] = float(np.abs(a - b).sum() / np.abs(b).sum())
+            acc["max_rel"] = float(np.abs(a - b).max() / max(1.0, np.abs(b).max()))
+            mm, mf = np.asarray(s.conservation_check()), np.asarray(ref.conservation_check())
+            acc["mass_drift_rel"] = float(np.max(np.abs(mm - mf)) / np.max(np.abs(mf)))
+        ref.close()
+        # lake at rest (no pulse): the largest change of any cell after the same steps
+        lake = cases.to_options(_bathy_cfg(amp=0.0))
+        lake.precision = fcb.PRECISION_MIXED
+        lake.macro_graph = args.macro_graph
+        ls = fcb.Solver(lake, stream=stream.cuda_stream)
+        ls.initialize()
+        q0s = ls.get_q()
+        t = 0.0
+        for _ in range(args.steps):
+            ls.advance_all_levels(t, _bathy_dt())
+            t += _bathy_dt()
+        m = cfg.mbc
+        acc["lake_at_rest_max_change"] = float(np.abs(ls.get_q() - q0s)[..., m:-m, m:-m].max())
+        ls.close()
+        accuracy = acc
+    if rank != 0:
+        s.close()
+        return None
+    hbm, src = peaks()
+    bytes_per_cell = 64.5  # meqn 3 + stored b, mx 32, mbc 2
+    achieved = total_cells * bytes_per_cell / (ms_max * 1e-3) / 1e9
+    line = {
+        "metric": "cell-updates/s", "value": total_cells / (ms_max * 1e-3), "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
+        "config": {"workload": "shallow water over bathymetry (GeoClaw f-waves), lake at rest + pulse 1e-3, "
+                               "levels 4-7, mx=my=32, subcycled, regrid every macro step (advance phase timed)",
+                   "patches_min": min(patches), "patches_max": max(patches), "macro_graph": args.macro_graph,
+                   "accuracy": accuracy},
+        "clocks": clk.summary(),
+        "gpu_launches": s.bench_launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "bytes_per_cell": bytes_per_cell, "kernel": "advance phase (all kernels)",
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback"},
+        "roofline_fp": fp_roofline("geoclaw_fwave_order20", cfg.mx, total_cells / (ms_max * 1e-3), args.precision,
+                                   stream.cuda_stream),
+    }
+    s.close()
+    return line
+
+
+# ----------------------------------------------------------------------------
 # Ensemble serving: Poisson stream of shallow-water dam-break requests
 # ----------------------------------------------------------------------------
 def _serve_requests(n, seed, precision):
@@ -572,7 +701,7 @@ def main():
                                              device_id=torch.device("cuda", local_rank))
     try:
         sys.path.insert(0, str(ROOT / "tests"))
-        run = {"amr_radialdam": run_amr, "serve": run_serve}.get(args.workload, run_ours)
+        run = {"amr_radialdam": run_amr, "bathy": run_bathy, "serve": run_serve}.get(args.workload, run_ours)
         line = run(args, rank, world, local_rank)
         if line:
             print(json.dumps(line), flush=True)
