@@ -47,7 +47,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="uniform_swirl",
-                   choices=["uniform_swirl", "amr_radialdam", "bathy", "serve"])
+                   choices=["uniform_swirl", "amr_radialdam", "amr_quadrants", "bathy", "serve"])
     p.add_argument("--requests", type=int, default=24, help="serve: number of requests")
     p.add_argument("--rates", default="5,20,80", help="serve: Poisson arrival rates (requests/s) to sweep")
     p.add_argument("--level", type=int, default=8)
@@ -354,6 +354,10 @@ FP64_OPS_PER_CELL = {
     ("swe_roe_order22", 16): 1244.9609,
     ("swe_roe_order22", 32): 1090.248,
     ("geoclaw_fwave_order20", 32): 1326.3662,
+    ("euler4_roe_order22", 8): 2549.3125,
+    ("euler4_roe_order22", 16): 2005.2109,
+    ("euler4_roe_order22", 32): 1756.8027,
+    ("euler4_roe_order22", 64): 1635.3647,
 }
 
 
@@ -378,10 +382,14 @@ def fp_roofline(case, mx, cells_per_s, precision, stream):
 # AMR shallow water: dam break, Roe solver, levels 3..6, mx = 32, subcycling,
 # gradient tagging, regrid after every macro step, adaptive dt
 # ----------------------------------------------------------------------------
-def _amr_cfg(seed=0):
+def _amr_cfg(seed=0, workload="amr_radialdam", mx=32):
+    """amr_radialdam: shallow water, levels 3-6, mx 32; amr_quadrants: Euler
+    quadrants, levels 2-7, mx from --mx (8, 16, 32 or 64)."""
     sys.path.insert(0, str(ROOT / "tests"))
     import cases
 
+    if workload == "amr_quadrants":
+        return cases.quadrants_amr(seed=seed, minlevel=2, maxlevel=7, mx=mx)
     return cases.radialdam_amr(seed=seed, minlevel=3, maxlevel=6, mx=32)
 
 
@@ -398,7 +406,7 @@ def run_amr(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     stream = torch.cuda.current_stream()
-    cfg = _amr_cfg()
+    cfg = _amr_cfg(workload=args.workload, mx=args.mx)
     opts = cases.to_options(cfg)
     opts.precision = fcb.PRECISION_MIXED if args.precision == "mixed" else fcb.PRECISION_FP64
     opts.macro_graph = args.macro_graph
@@ -433,14 +441,18 @@ def run_amr(args, rank, world, local_rank):
     if rank != 0:
         return None
     hbm, src = peaks()
-    bytes_per_cell = 54.4  # meqn 3, mx 32, mbc 2: 8*3*(1 + 36*36/(32*32))
+    # 8*meqn*(1 + (mx+4)^2/mx^2): ghosted read + interior write
+    bytes_per_cell = 8.0 * cfg.meqn * (1.0 + (cfg.mx + 4) ** 2 / cfg.mx ** 2)
+    euler = args.workload == "amr_quadrants"
     achieved = cells * bytes_per_cell / (adv_ms * 1e-3) / 1e9
     line = {
         "metric": "cell-updates/s", "value": cells / (adv_ms * 1e-3), "unit": "cell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": adv_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
-        "config": {"workload": "AMR shallow-water dam break, Roe, levels 3-6, mx=my=32, subcycled, "
+        "config": {"workload": (f"AMR Euler quadrants, Roe, levels 2-7, mx=my={cfg.mx}, subcycled, "
+                                if euler else "AMR shallow-water dam break, Roe, levels 3-6, mx=my=32, subcycled, ")
+                               + 
                                "regrid every macro step (advance phase timed; regrid reported apart)",
                    "patches_min": min(patches), "patches_max": max(patches),
                    "regrid_ms_per_step": reg_s * 1e3 / args.steps, "macro_graph": args.macro_graph,
@@ -451,21 +463,21 @@ def run_amr(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": None, "bytes_per_cell": bytes_per_cell, "kernel": "advance phase (all kernels)",
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback"},
-        "roofline_fp": fp_roofline("swe_roe_order22", cfg.mx, cells / (adv_ms * 1e-3), args.precision,
+        "roofline_fp": fp_roofline("euler4_roe_order22" if euler else "swe_roe_order22", cfg.mx,
+                                   cells / (adv_ms * 1e-3), args.precision,
                                    stream.cuda_stream),
     }
     if world == 1:
-        line["cpu_baseline"] = amr_cpu_sample(args.cpu_seconds)
+        line["cpu_baseline"] = amr_cpu_sample(args.cpu_seconds, cfg)
     s.close()
     return line
 
 
-def amr_cpu_sample(budget_s):
+def amr_cpu_sample(budget_s, cfg):
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle as O
 
     O.use_library(native_oracle())
-    cfg = _amr_cfg()
     o = O.OracleSolver(cfg)
     o.initialize()
     t, dt, el, cells, n = 0.0, cfg.initial_dt, 0.0, 0, 0
@@ -701,7 +713,8 @@ def main():
                                              device_id=torch.device("cuda", local_rank))
     try:
         sys.path.insert(0, str(ROOT / "tests"))
-        run = {"amr_radialdam": run_amr, "bathy": run_bathy, "serve": run_serve}.get(args.workload, run_ours)
+        run = {"amr_radialdam": run_amr, "amr_quadrants": run_amr, "bathy": run_bathy,
+               "serve": run_serve}.get(args.workload, run_ours)
         line = run(args, rank, world, local_rank)
         if line:
             print(json.dumps(line), flush=True)

@@ -70,6 +70,23 @@ def radialdam_amr(seed=0, minlevel=3, maxlevel=6, mx=32, tfinal=0.5) -> O.Config
                     pparams=(0.5, 0.5, r0, 2.0, 1.0))
 
 
+def quadrants_amr(seed=0, minlevel=2, maxlevel=7, mx=16, tfinal=0.25) -> O.Config:
+    """AMR Euler (Roe with entropy fix, gamma = 1.4), subcycled: four quadrant
+    states about (0.5, 0.5) drawn per seed, rho, p ~ U(0.1, 1.5) and
+    u, v ~ U(-0.8, 0.8); gradient tagging on rho (refine > 1.0, coarsen < 0.1),
+    regrid every step, adaptive dt."""
+    rng = np.random.default_rng(seed)
+    states = [(rng.uniform(0.1, 1.5), rng.uniform(-0.8, 0.8), rng.uniform(-0.8, 0.8), rng.uniform(0.1, 1.5))
+              for _ in range(4)]
+    return O.Config(mx=mx, my=mx, mbc=2, meqn=4, maux=0, order=(2, 2), mwaves=4, mthlim=(4, 4, 4, 4),
+                    mthbc=(1, 1, 1, 1), minlevel=minlevel, maxlevel=maxlevel, subcycle=1,
+                    regrid_interval=1, smooth_refine=1, criteria=O.GRADIENT,
+                    refine_threshold=1.0, coarsen_threshold=0.1, tfinal=tfinal,
+                    initial_dt=0.15 / (mx * (1 << minlevel)), max_cfl=1.0, desired_cfl=0.9,
+                    solver=O.EULER4_ROE, problem=O.QUADRANTS, gamma=1.4,
+                    pparams=O.quadrants_params(states, 0.5, 0.5))
+
+
 def replace(cfg, **kw):
     return dataclasses.replace(cfg, **kw)
 
