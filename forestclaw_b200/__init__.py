@@ -42,7 +42,7 @@ EXPORTED_SYMBOLS = (
     "fcb_update_single_step", "fcb_update_single_step_async", "fcb_conservation_sum_noalloc",
     "fcb_server_create", "fcb_server_destroy", "fcb_server_submit", "fcb_server_round", "fcb_server_status",
     "fcb_server_get_q", "fcb_server_release", "fcb_server_clock", "fcb_autotune_info",
-    "fcb_measure_fp_rate",
+    "fcb_measure_fp_rate", "fcb_output_ascii",
 )
 
 
@@ -219,6 +219,7 @@ def lib():
     L.fcb_curr_time.argtypes = [vp, dp]
     L.fcb_autotune_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     L.fcb_measure_fp_rate.argtypes = [ctypes.c_int, vp, dp]
+    L.fcb_output_ascii.argtypes = [vp, ctypes.c_int, ctypes.c_char_p]
     L.fcb_conservation_sum_noalloc.argtypes = [vp, sz, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, vp, vp, vp]
     ll = ctypes.POINTER(ctypes.c_longlong)
@@ -365,6 +366,10 @@ class Solver:
         c = _Counters()
         _check(lib().fcb_counters(self._h, ctypes.byref(c)))
         return {n: getattr(c, n) for n, _ in _Counters._fields_}
+
+    def output_ascii(self, iframe: int, directory: str = "."):
+        """Write fort.tNNNN and fort.qNNNN (the reference's ASCII frame) into `directory`."""
+        _check(lib().fcb_output_ascii(self._h, int(iframe), str(directory).encode()))
 
     def autotune_info(self) -> dict:
         """Step form (1 CTA, 2 warp, 3 pipelined) and ghost unroll of the last launches."""

@@ -39,6 +39,7 @@ SOURCES = {
     "fcb_noalloc.cu": ["-fmad=false"],
     "fcb_probe.cu": ["-fmad=false"],
     "fcb_timesync.cu": ["-fmad=false"],
+    "fcb_output.cpp": [],
 }
 
 

@@ -210,6 +210,13 @@ int fcb_curr_time(fcb_context_t* ctx, double* t) {
 
 int fcb_synchronize(fcb_context_t* ctx) { return guard([&] { CTX(); C.synchronize(); }); }
 
+int fcb_output_ascii(fcb_context_t* ctx, int iframe, const char* dir) {
+    return guard([&] {
+        CTX();
+        C.output_ascii(iframe, dir ? std::string(dir) : std::string("."));
+    });
+}
+
 int fcb_measure_fp_rate(int fp64, void* cuda_stream, double* ops_per_second) {
     return guard([&] {
         need(ops_per_second, "ops_per_second");

@@ -1,6 +1,7 @@
 // Host runtime: forest management, slot arena, ghost plans and the level
 // schedule of ForestClaw's time-stepping core on one GPU.
 #include "fcb_runtime.hpp"
+#include "fcb_output.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -1724,6 +1725,35 @@ void Context::get_q(double* host, size_t n, bool qinterp) {
     ++cnt_.count_kernel_launches;
     check(cudaMemcpyAsync(host, d_stage_, total * sizeof(double), cudaMemcpyDeviceToHost, st_), "get_q");
     synchronize();
+}
+
+void Context::output_ascii(int iframe, const std::string& dir) {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "output before initialize");
+    if (iframe < 0 || iframe > 9999) throw Error(FCB_ERR_INVALID, "frame number must be in 0..9999");
+    const size_t ps = patch_size();
+    const int n = num_patches();
+    std::vector<double> host(ps * (size_t)n);
+    if (ps * (size_t)n > stage_cap_) {
+        cudaFree(d_stage_);
+        check(cudaMalloc(&d_stage_, ps * (size_t)n * sizeof(double)), "cudaMalloc stage");
+        stage_cap_ = ps * (size_t)n;
+    }
+    // the clawpack 4.6 layout for both versions: the values per cell are the same
+    check(launch_gather(d_q_, stride_, d_all_slots_.p, n, (int64_t)ps, d_stage_, false, 0, st_), "gather");
+    ++cnt_.count_kernel_launches;
+    check(cudaMemcpyAsync(host.data(), d_stage_, host.size() * sizeof(double), cudaMemcpyDeviceToHost, st_), "output");
+    synchronize();
+    std::vector<OutputPatch> ps_out((size_t)n);
+    for (int p = 0; p < n; ++p) {
+        const PatchMeta m = meta_of(forest_.leaves[p]);
+        ps_out[p] = OutputPatch{p, (int)forest_.leaves[p].level, m.xlower, m.ylower, m.dx, m.dy};
+    }
+    try {
+        write_ascii_frame(dir, iframe, curr_time_, opt_.meqn, opt_.maux, opt_.mx, opt_.my, opt_.mbc, ps_out,
+                          host.data(), ps);
+    } catch (const std::runtime_error& e) {
+        throw Error(FCB_ERR_INVALID, e.what());
+    }
 }
 
 void Context::set_q(const double* host, size_t n) {

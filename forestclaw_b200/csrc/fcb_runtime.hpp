@@ -119,6 +119,8 @@ class Context {
     void set_curr_time(double t) { curr_time_ = t; }
     void count_advance() { ++cnt_.count_amr_advance; }
     size_t device_bytes() const;
+    // fclaw2d_clawpatch_output_ascii: frame iframe into dir/fort.tNNNN, fort.qNNNN
+    void output_ascii(int iframe, const std::string& dir);
     // autotuner: the step form (1 four-barrier CTA, 2 warp, 3 pipelined) and the
     // ghost-fill unroll used by the last launches
     int step_form_used() const { return step_form_used_; }

@@ -227,6 +227,13 @@ int fcb_conservation_sum_noalloc(const double* d_q, size_t patch_stride, int npa
                                  int meqn, const double* d_area, double* d_sums, void* cuda_stream);
 /* Current time of the run loop. */
 int fcb_curr_time(fcb_context_t* ctx, double* t);
+/* Output frame `iframe` (0..9999) of all leaves in the reference's ASCII
+ * format: dir/fort.tNNNN (time, meqn, ngrids, num_aux, num_dim) and
+ * dir/fort.qNNNN (per patch a grid header, then the interior cells row by row)
+ * (fclaw2d_clawpatch_output_ascii, src/patches/clawpatch/
+ * fclaw2d_clawpatch_output_ascii.c; fort_4.6/fclaw2d_clawpatch46_output_ascii.f).
+ * dir must exist; NULL means the working directory. */
+int fcb_output_ascii(fcb_context_t* ctx, int iframe, const char* dir);
 /* Autotuner choices of the last launches (no counterpart in the reference):
  * step_form 1 = one CTA per patch with four barriers per stage, 2 = one warp
  * per patch, 3 = pipelined row sweep; ghost_unroll = ghost records per thread
