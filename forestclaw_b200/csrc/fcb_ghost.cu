@@ -70,11 +70,21 @@ __device__ __forceinline__ void interp_cell(bool fp32, const PatchView& C, const
     else interp_cell_t<double>(C, F, m, ic, jc, i20, j20);
 }
 
+// Patch shape of a launch: MXC > 0 fixes mx = my = MXC and mbc = 2 at compile
+// time (index decoding by constant division), MXC == 0 reads the arguments.
+template <int MXC>
+__device__ __forceinline__ int gmx(const GhostArgs& a) { return MXC > 0 ? MXC : a.mx; }
+template <int MXC>
+__device__ __forceinline__ int gmy(const GhostArgs& a) { return MXC > 0 ? MXC : a.my; }
+template <int MXC>
+__device__ __forceinline__ int gmbc(const GhostArgs& a) { return MXC > 0 ? 2 : a.mbc; }
+
 }  // namespace
 
 // One record executed by the 32 lanes of a warp.
+template <int MXC>
 __device__ __forceinline__ void ghost_op(const GhostArgs& a, const GhostOp& op, int lane) {
-    const int mx = a.mx, my = a.my, mbc = a.mbc, meqn = a.meqn;
+    const int mx = gmx<MXC>(a), my = gmy<MXC>(a), mbc = gmbc<MXC>(a), meqn = a.meqn;
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
     PatchView D{(op.dst_ti ? a.qti : a.q) + (int64_t)op.dst * a.stride, mx, my, mbc, nx, ny};
     PatchView S{(op.src_ti ? a.qti : a.q) + (int64_t)op.src * a.stride, mx, my, mbc, nx, ny};
@@ -225,8 +235,9 @@ __device__ __forceinline__ void ghost_op(const GhostArgs& a, const GhostOp& op, 
 // Number of cells one lane-level work item of a record covers (0 for the
 // physical-boundary record, which keeps its whole-warp form: its sides read
 // cells that the previous side writes).
+template <int MXC>
 __device__ __forceinline__ int op_cells(const GhostArgs& a, const GhostOp& op) {
-    const int mx = a.mx, my = a.my, mbc = a.mbc, meqn = a.meqn;
+    const int mx = gmx<MXC>(a), my = gmy<MXC>(a), mbc = gmbc<MXC>(a), meqn = a.meqn;
     switch (op.type) {
         case OP_COPY_FACE: return (op.face < 2 ? mbc * my : mx * mbc) * meqn;
         case OP_COPY_CORNER:
@@ -242,8 +253,9 @@ __device__ __forceinline__ int op_cells(const GhostArgs& a, const GhostOp& op) {
 // and average items return their value and destination so the caller can
 // issue several loads before the stores; interpolation items store their four
 // fine cells themselves and return nullptr.
+template <int MXC>
 __device__ __forceinline__ double* op_cell(const GhostArgs& a, const GhostOp& op, int k, double& v) {
-    const int mx = a.mx, my = a.my, mbc = a.mbc;
+    const int mx = gmx<MXC>(a), my = gmy<MXC>(a), mbc = gmbc<MXC>(a);
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
     PatchView D{(op.dst_ti ? a.qti : a.q) + (int64_t)op.dst * a.stride, mx, my, mbc, nx, ny};
     PatchView S{(op.src_ti ? a.qti : a.q) + (int64_t)op.src * a.stride, mx, my, mbc, nx, ny};
@@ -336,7 +348,7 @@ __device__ __forceinline__ double* op_cell(const GhostArgs& a, const GhostOp& op
 // (prefix sum of op_cells over the lanes) and each lane takes items lane,
 // lane+32, ...  UNROLL items per lane issue their loads before any store.
 constexpr int GHOST_TPB = 256;
-template <int GHOST_UNROLL>
+template <int GHOST_UNROLL, int MXC>
 __global__ void __launch_bounds__(GHOST_TPB) ghost_wave_kernel(const GhostArgs a) {
     __shared__ GhostOp s_ops[GHOST_TPB / 32][32];
     __shared__ int s_end[GHOST_TPB / 32][32];
@@ -353,7 +365,7 @@ __global__ void __launch_bounds__(GHOST_TPB) ghost_wave_kernel(const GhostArgs a
             const GhostOp op = a.ops[base + lane];
             s_ops[wl][lane] = op;
             phys = op.type == OP_PHYSBC;
-            n = op_cells(a, op);
+            n = op_cells<MXC>(a, op);
         }
         int incl = n;
 #pragma unroll
@@ -376,7 +388,7 @@ __global__ void __launch_bounds__(GHOST_TPB) ghost_wave_kernel(const GhostArgs a
                 if (f < total) {
                     while (f >= s_end[wl][r]) ++r;
                     const int first = r > 0 ? s_end[wl][r - 1] : 0;
-                    dst[u] = op_cell(a, s_ops[wl][r], f - first, v[u]);
+                    dst[u] = op_cell<MXC>(a, s_ops[wl][r], f - first, v[u]);
                 }
             }
 #pragma unroll
@@ -388,7 +400,7 @@ __global__ void __launch_bounds__(GHOST_TPB) ghost_wave_kernel(const GhostArgs a
         while (pm) {
             const int l = __ffs(pm) - 1;
             pm &= pm - 1;
-            ghost_op(a, s_ops[wl][l], lane);
+            ghost_op<MXC>(a, s_ops[wl][l], lane);
         }
         __syncwarp();
     }
@@ -396,13 +408,27 @@ __global__ void __launch_bounds__(GHOST_TPB) ghost_wave_kernel(const GhostArgs a
 
 // unroll: work items per lane whose loads are issued before the stores (2, 4
 // or 8; the autotuner picks one per patch shape)
+namespace {
+template <int MXC>
+void launch_ghost_shape(const GhostArgs& a, cudaStream_t st, int unroll, int blocks) {
+    switch (unroll) {
+        case 2: ghost_wave_kernel<2, MXC><<<blocks, GHOST_TPB, 0, st>>>(a); break;
+        case 8: ghost_wave_kernel<8, MXC><<<blocks, GHOST_TPB, 0, st>>>(a); break;
+        default: ghost_wave_kernel<4, MXC><<<blocks, GHOST_TPB, 0, st>>>(a); break;
+    }
+}
+}  // namespace
+
 cudaError_t launch_ghost_wave(const GhostArgs& a, cudaStream_t st, int unroll) {
     if (a.ngroups <= 0) return cudaSuccess;
     const int blocks = (int)(((int64_t)a.ngroups * 32 + GHOST_TPB - 1) / GHOST_TPB);
-    switch (unroll) {
-        case 2: ghost_wave_kernel<2><<<blocks, GHOST_TPB, 0, st>>>(a); break;
-        case 8: ghost_wave_kernel<8><<<blocks, GHOST_TPB, 0, st>>>(a); break;
-        default: ghost_wave_kernel<4><<<blocks, GHOST_TPB, 0, st>>>(a); break;
+    const int shape = (a.mbc == 2 && a.mx == a.my) ? a.mx : 0;
+    switch (shape) {
+        case 8: launch_ghost_shape<8>(a, st, unroll, blocks); break;
+        case 16: launch_ghost_shape<16>(a, st, unroll, blocks); break;
+        case 32: launch_ghost_shape<32>(a, st, unroll, blocks); break;
+        case 64: launch_ghost_shape<64>(a, st, unroll, blocks); break;
+        default: launch_ghost_shape<0>(a, st, unroll, blocks); break;
     }
     return cudaGetLastError();
 }
