@@ -108,6 +108,10 @@ struct PipeState {
     static constexpr int M = SOL::M;
     static constexpr int W = SOL::W;
     double qcur[M], q_m1[M];                             // q(c, s), q(c, s-1)
+    // scalar case: q(c, s-2..s-4) kept from their loads, so the update of row
+    // s-4 reads its old value from registers instead of memory
+    static constexpr bool DELAY = M == 1;
+    double q_m2[M], q_m3[M], q_m4[M];
     R yw_f[W][M], ys_f[W], yam_f[M], yap_f[M], ydotl[W];  // raw y-interface s-1
     typename SOL::Roe yR_f;
     R gRm_prev[M], gRp_prev[M];                          // y transverse parts into row s-2
@@ -189,7 +193,8 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
 #pragma unroll
         for (int m = 0; m < M; ++m) {
             qnext[m] = on ? T.q[((int64_t)m * NY + s + 1) * NX] : 0.0;
-            qold[m] = upd ? T.q[((int64_t)m * NY + s - 4) * NX] : 0.0;
+            if constexpr (PipeState<SOL>::DELAY) qold[m] = S.q_m4[m];
+            else qold[m] = upd ? T.q[((int64_t)m * NY + s - 4) * NX] : 0.0;
         }
     }
 
@@ -540,6 +545,11 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
         for (int m = 0; m < M; ++m) {
             S.yam_f[m] = yam_n[m];
             S.yap_f[m] = yap_n[m];
+            if constexpr (PipeState<SOL>::DELAY) {
+                S.q_m4[m] = S.q_m3[m];
+                S.q_m3[m] = S.q_m2[m];
+                S.q_m2[m] = S.q_m1[m];
+            }
             S.q_m1[m] = S.qcur[m];
             S.qcur[m] = qnext[m];
         }
@@ -641,6 +651,7 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     for (int m = 0; m < M; ++m) {
         S.qcur[m] = active ? T.q[(int64_t)m * NY * NX] : 0.0;
         S.q_m1[m] = 0.0;
+        S.q_m2[m] = S.q_m3[m] = S.q_m4[m] = 0.0;
         S.yam_f[m] = S.yap_f[m] = R(0);
         S.gRm_prev[m] = S.gRp_prev[m] = R(0);
         S.xam[m] = S.xap[m] = R(0);
