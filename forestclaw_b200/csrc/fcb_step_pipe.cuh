@@ -18,7 +18,7 @@
 //   S2  x-row s-1: Riemann problem with the left neighbour's state (ring Q) -> ring XW
 //   S1  row s: y-interface s (raw) and y-interface s-1 (final, own column);
 //       y transverse parts -> ring GY; aux row s+1 -> ring AX
-// with q(c, s+1) prefetched at the top of iteration s.  Stages that carry
+// with q(c, s+2) prefetched at the top of iteration s.  Stages that carry
 // values to the next iteration run before their producers, so the carries
 // need no register copies.
 //
@@ -108,6 +108,7 @@ struct PipeState {
     static constexpr int M = SOL::M;
     static constexpr int W = SOL::W;
     double qcur[M], q_m1[M];                             // q(c, s), q(c, s-1)
+    double qpre[M];                                      // q(c, s+1), loaded one iteration ahead
     // scalar case: q(c, s-2..s-4) kept from their loads, so the update of row
     // s-4 reads its old value from registers instead of memory
     static constexpr bool DELAY = M == 1;
@@ -184,15 +185,18 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
         else return QT(0);
     };
 
-    // prefetch q(c, s+1); load q(c, s-4) for this iteration's update early
+    // prefetch q(c, s+2); the old value of q(c, s-4) for this iteration's update
     double qnext[M], qold[M];
     const bool upd = T.active && (V5 ? (s - 4 >= MBC && s - 4 <= MBC + MX - 1 && c >= MBC && c <= MBC + MX - 1)
                                      : ((STEADY || (s - 4 >= 0 && s - 4 <= NY - 2)) && c <= NX - 2));
     {
-        const bool on = T.active && (STEADY || s + 1 < NY);
+        // prefetch two rows ahead; the last steady iteration (s = 4 + 4*((NY-5)/4) - 1)
+        // still has row s+2 inside the patch for the patch sizes built here
+        constexpr bool STEADY_IN = 4 + 4 * ((NY - 5) / 4) + 1 < NY;
+        const bool on = T.active && ((STEADY && STEADY_IN) || s + 2 < NY);
 #pragma unroll
         for (int m = 0; m < M; ++m) {
-            qnext[m] = on ? T.q[((int64_t)m * NY + s + 1) * NX] : 0.0;
+            qnext[m] = on ? T.q[((int64_t)m * NY + s + 2) * NX] : 0.0;
             if constexpr (PipeState<SOL>::DELAY) qold[m] = S.q_m4[m];
             else qold[m] = upd ? T.q[((int64_t)m * NY + s - 4) * NX] : 0.0;
         }
@@ -551,7 +555,8 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 S.q_m2[m] = S.q_m1[m];
             }
             S.q_m1[m] = S.qcur[m];
-            S.qcur[m] = qnext[m];
+            S.qcur[m] = S.qpre[m];
+            S.qpre[m] = qnext[m];
         }
         S.yR_f = yR_n;
 
@@ -650,6 +655,7 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         S.qcur[m] = active ? T.q[(int64_t)m * NY * NX] : 0.0;
+        S.qpre[m] = active ? T.q[((int64_t)m * NY + 1) * NX] : 0.0;
         S.q_m1[m] = 0.0;
         S.q_m2[m] = S.q_m3[m] = S.q_m4[m] = 0.0;
         S.yam_f[m] = S.yap_f[m] = R(0);
