@@ -40,6 +40,40 @@ template struct DevBuf<PatchDesc>;
 template struct DevBuf<double>;
 template struct DevBuf<TsOp>;
 
+namespace {
+cudaMemPool_t arena_pool() {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) throw Error(FCB_ERR_CUDA, "cudaGetDevice failed");
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(dev);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) throw Error(FCB_ERR_CUDA, "cudaMemPoolCreate failed");
+    uint64_t keep = UINT64_MAX;  // freed blocks stay in the pool for the next allocation
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+        throw Error(FCB_ERR_CUDA, "cudaMemPoolSetAttribute failed");
+    pools[dev] = pool;
+    return pool;
+}
+}  // namespace
+
+template <class T>
+void Context::arena_alloc(T*& p, size_t bytes) {
+    void* q = nullptr;
+    check(cudaMallocFromPoolAsync(&q, std::max<size_t>(bytes, 256), arena_pool(), st_), "arena allocation");
+    p = static_cast<T*>(q);
+}
+
+void Context::arena_free(void* p) {
+    if (p) cudaFreeAsync(p, st_);
+}
+
 void Context::check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw Error(FCB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -146,17 +180,18 @@ Context::~Context() {
     drop_macro_graph();
     if (cap_st_) cudaStreamDestroy(cap_st_);
     cudaFreeHost(h_dyn_);
-    cudaFree(d_q_);
-    cudaFree(d_qlast_);
-    cudaFree(d_qti_);
-    cudaFree(d_qsave_);
-    cudaFree(d_aux_);
-    cudaFree(d_meta_);
+    arena_free(d_q_);
+    arena_free(d_qlast_);
+    arena_free(d_qti_);
+    arena_free(d_qsave_);
+    arena_free(d_aux_);
+    arena_free(d_meta_);
+    arena_free(d_treg_);
+    cudaStreamSynchronize(st_);
     cudaFree(d_cfl_);
     cudaFreeHost(h_cfl_);
     cudaFree(d_scratch_);
     cudaFree(d_stage_);
-    cudaFree(d_treg_);
     cudaFreeHost(h_ts_ops_pinned_);
     cudaFreeHost(h_ts_groups_pinned_);
 }
@@ -167,15 +202,16 @@ void Context::ensure_capacity(int n) {
     if (n <= capacity_) return;
     const int nc = std::max({n, capacity_ + capacity_ / 2, 64});
     const size_t bytes = (size_t)nc * stride_ * sizeof(double);
+    // stream-ordered: allocation, zeroing, copy of the old contents and the
+    // free of the old arena are all queued on the context's stream
     auto grow = [&](double*& p) {
         double* np = nullptr;
-        check(cudaMalloc(&np, bytes), "cudaMalloc arena");
+        arena_alloc(np, bytes);
         check(cudaMemsetAsync(np, 0, bytes, st_), "cudaMemset arena");
         if (p) {
             check(cudaMemcpyAsync(np, p, (size_t)capacity_ * stride_ * sizeof(double), cudaMemcpyDeviceToDevice, st_),
                   "arena copy");
-            check(cudaStreamSynchronize(st_), "sync");
-            cudaFree(p);
+            arena_free(p);
         }
         p = np;
     };
@@ -185,33 +221,32 @@ void Context::ensure_capacity(int n) {
     if (time_sync_) {
         const size_t rb = (size_t)nc * treg_stride_ * sizeof(double);
         double* np = nullptr;
-        check(cudaMalloc(&np, rb), "cudaMalloc registers");
+        arena_alloc(np, rb);
         check(cudaMemsetAsync(np, 0, rb, st_), "cudaMemset registers");
         if (d_treg_) {
             check(cudaMemcpyAsync(np, d_treg_, (size_t)capacity_ * treg_stride_ * sizeof(double),
                                   cudaMemcpyDeviceToDevice, st_),
                   "registers copy");
-            check(cudaStreamSynchronize(st_), "sync");
-            cudaFree(d_treg_);
+            arena_free(d_treg_);
         }
         d_treg_ = np;
     }
     if (!opt_.use_fixed_dt) grow(d_qsave_);
     if (aux_kind_ == AUX_STORED) {  // recomputed for every patch by mesh_changed
-        check(cudaStreamSynchronize(st_), "sync");
-        cudaFree(d_aux_);
+        arena_free(d_aux_);
         d_aux_ = nullptr;
-        check(cudaMalloc(&d_aux_, (size_t)nc * aux_stride_ * sizeof(double)), "cudaMalloc aux");
+        arena_alloc(d_aux_, (size_t)nc * aux_stride_ * sizeof(double));
     }
     PatchMeta* nm = nullptr;
-    check(cudaMalloc(&nm, (size_t)nc * sizeof(PatchMeta)), "cudaMalloc meta");
+    arena_alloc(nm, (size_t)nc * sizeof(PatchMeta));
     if (d_meta_) {
         check(cudaMemcpyAsync(nm, d_meta_, (size_t)capacity_ * sizeof(PatchMeta), cudaMemcpyDeviceToDevice, st_), "meta");
-        check(cudaStreamSynchronize(st_), "sync");
-        cudaFree(d_meta_);
+        arena_free(d_meta_);
     }
     d_meta_ = nm;
     capacity_ = nc;
+    // the arenas are used by synchronous copies on other streams too (uploads)
+    check(cudaStreamSynchronize(st_), "sync");
 }
 
 int Context::alloc_slot() {
@@ -622,16 +657,17 @@ void Context::finish_plans() {
 void Context::upload_ops() {
     if (upload_ev_) check(cudaEventSynchronize(upload_ev_), "ops upload");  // staging free again
     else check(cudaEventCreateWithFlags(&upload_ev_, cudaEventDisableTiming), "cudaEventCreate");
+    // staging grows geometrically from 64 Ki records (a pinned free synchronises the device)
     if (h_ops_.size() > h_ops_pinned_cap_) {
         cudaFreeHost(h_ops_pinned_);
         h_ops_pinned_ = nullptr;
-        h_ops_pinned_cap_ = std::max(h_ops_.size(), 2 * h_ops_pinned_cap_);
+        h_ops_pinned_cap_ = std::max({h_ops_.size(), 2 * h_ops_pinned_cap_, (size_t)1 << 16});
         check(cudaHostAlloc(&h_ops_pinned_, h_ops_pinned_cap_ * sizeof(GhostOp), cudaHostAllocDefault), "host ops");
     }
     if (h_groups_.size() > h_groups_pinned_cap_) {
         cudaFreeHost(h_groups_pinned_);
         h_groups_pinned_ = nullptr;
-        h_groups_pinned_cap_ = std::max(h_groups_.size(), 2 * h_groups_pinned_cap_);
+        h_groups_pinned_cap_ = std::max({h_groups_.size(), 2 * h_groups_pinned_cap_, (size_t)1 << 16});
         check(cudaHostAlloc(&h_groups_pinned_, h_groups_pinned_cap_ * sizeof(int32_t), cudaHostAllocDefault),
               "host groups");
     }
@@ -1219,10 +1255,13 @@ int Context::tune_step_form(const StepArgs& a, int n) {
     if (cand.size() == 1 || cs != cudaStreamCaptureStatusNone || dry_) return cand.size() == 1 ? cand[0] : default_step_form(opt_);
     const size_t bytes = (size_t)capacity_ * stride_ * sizeof(double);
     double *tq = nullptr, *tl = nullptr;
-    if (cudaMalloc(&tq, bytes) != cudaSuccess || cudaMalloc(&tl, bytes) != cudaSuccess) {
+    try {
+        arena_alloc(tq, bytes);
+        arena_alloc(tl, bytes);
+    } catch (const Error&) {
         cudaGetLastError();
-        cudaFree(tq);
-        cudaFree(tl);
+        arena_free(tq);
+        arena_free(tl);
         return default_step_form(opt_);  // no room for scratch copies: no tuning
     }
     check(cudaMemcpyAsync(tq, d_q_, bytes, cudaMemcpyDeviceToDevice, st_), "tune copy");
@@ -1258,9 +1297,9 @@ int Context::tune_step_form(const StepArgs& a, int n) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    arena_free(tq);
+    arena_free(tl);
     check(cudaStreamSynchronize(st_), "sync");
-    cudaFree(tq);
-    cudaFree(tl);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_step_form_cache[key] = best;
     return best;
@@ -1280,10 +1319,13 @@ int Context::tune_ghost_unroll(const GhostPlan& g) {
     // timed passes leave the real state untouched
     const size_t bytes = (size_t)capacity_ * stride_ * sizeof(double);
     double *tq = nullptr, *tt = nullptr;
-    if (cudaMalloc(&tq, bytes) != cudaSuccess || cudaMalloc(&tt, bytes) != cudaSuccess) {
+    try {
+        arena_alloc(tq, bytes);
+        arena_alloc(tt, bytes);
+    } catch (const Error&) {
         cudaGetLastError();
-        cudaFree(tq);
-        cudaFree(tt);
+        arena_free(tq);
+        arena_free(tt);
         return 4;
     }
     check(cudaMemcpyAsync(tq, d_q_, bytes, cudaMemcpyDeviceToDevice, st_), "tune copy");
@@ -1318,9 +1360,9 @@ int Context::tune_ghost_unroll(const GhostPlan& g) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    arena_free(tq);
+    arena_free(tt);
     check(cudaStreamSynchronize(st_), "sync");
-    cudaFree(tq);
-    cudaFree(tt);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_ghost_unroll_cache[key] = best;
     return best;
@@ -1616,7 +1658,10 @@ bool Context::regrid() {
         forest_.leaves = nl;
         repopulate(old, old_slots, false);
         mesh_changed();
-        prefetch_plans();  // this update's plan and the next macro step's, built together
+        // this update's plan and the next macro step's, built together, for a
+        // context that advances through fcb_advance_all_levels (a served solve
+        // steps level by level and builds its one plan on demand)
+        if (cnt_.count_amr_advance > 0) prefetch_plans();
         ghost_update(forest_.min_level(), forest_.max_level(), curr_time_, 0);
         ++cnt_.count_amr_new_domain;
     }

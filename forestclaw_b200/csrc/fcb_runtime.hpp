@@ -155,6 +155,12 @@ class Context {
     void discard_plans() noexcept;
     void prefetch_plans();
     void upload_ops();
+    // patch arenas and scratch come from a per-device stream-ordered pool that
+    // keeps freed memory (solves created and destroyed by a serving loop reuse
+    // each other's memory; a free never synchronises the device)
+    template <class T>
+    void arena_alloc(T*& p, size_t bytes);
+    void arena_free(void* p);
     std::vector<std::tuple<int, int, int>> dry_plan_keys_;  // plans the dry pass met
     // time synchronisation: registers, and per minlevel the launches of one
     // fclaw2d_time_sync call (records grouped per patch, groups per launch)
