@@ -111,7 +111,7 @@ class ClockSampler:
 # DRAM bytes (read + write) per step-kernel launch from the ncu captures
 # summarised in profiles/ (same workload, same kernel build).
 _TRAFFIC = {("fp64", 8, 16): (356.85e6, "profiles/step_kernel_uniform_swirl_l8_mx16.md"),
-            ("mixed", 8, 16): (359.25e6, "profiles/step_kernel_mixed_uniform_swirl_l8_mx16.md")}
+            ("mixed", 8, 16): (357.08e6, "profiles/step_kernel_mixed_uniform_swirl_l8_mx16.md")}
 
 
 def _profiled_traffic(args):
