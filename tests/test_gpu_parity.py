@@ -101,6 +101,24 @@ def test_uniform_quadrants_bit_exact(gpu_lib, mx, variant):
         assert c_d == c_o
 
 
+@pytest.mark.parametrize("solver", ["radialdam", "quadrants"])
+@pytest.mark.parametrize("mx", [8, 64])
+def test_cta_form_patch_sizes_and_partial_ctas(gpu_lib, solver, mx):
+    """The four-barrier form packs 256 // (mx + 4) patches per CTA for the Roe
+    systems (21 at mx = 8, 3 at mx = 64): 16 patches leave a partially filled
+    last CTA; every array bit-identical to the oracle."""
+    if solver == "radialdam":
+        cfg, dt = cases.radialdam_uniform(level=2, mx=mx), 0.4 / (mx * 4) / 1.5
+    else:
+        cfg, dt = cases.quadrants_uniform(level=2, mx=mx), 0.3 / (mx * 4) / 2.0
+    o, d = _pair_variant(cfg, 1)
+    t = 0.0
+    for step in range(4):
+        assert o.advance(t, dt) == d.advance_all_levels(t, dt)
+        t += dt
+        assert np.array_equal(d.get_q(), o.all_q()), f"step {step}"
+
+
 def test_single_step_update_protocol(gpu_lib):
     """patch_vt->single_step_update semantics: the batch runs on the last call."""
     cfg = cases.radialdam_uniform(level=2, mx=16)
