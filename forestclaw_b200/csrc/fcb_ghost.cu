@@ -81,154 +81,44 @@ __device__ __forceinline__ int gmbc(const GhostArgs& a) { return MXC > 0 ? 2 : a
 
 }  // namespace
 
-// One record executed by the 32 lanes of a warp.
+// A physical-boundary record (clawpack46_bc2_default.f) executed by the 32
+// lanes of a warp: its sides run in the reference's order, each reading cells
+// the previous side may have written.  Every other record type goes through
+// op_cell below.
 template <int MXC>
-__device__ __forceinline__ void ghost_op(const GhostArgs& a, const GhostOp& op, int lane) {
+__device__ __forceinline__ void physbc_op(const GhostArgs& a, const GhostOp& op, int lane) {
     const int mx = gmx<MXC>(a), my = gmy<MXC>(a), mbc = gmbc<MXC>(a), meqn = a.meqn;
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
     PatchView D{(op.dst_ti ? a.qti : a.q) + (int64_t)op.dst * a.stride, mx, my, mbc, nx, ny};
-    PatchView S{(op.src_ti ? a.qti : a.q) + (int64_t)op.src * a.stride, mx, my, mbc, nx, ny};
-
-    switch (op.type) {
-        case OP_COPY_FACE: {
-            int i0, i1, j0, j1;
-            if (op.face == 0) { i0 = 1 - mbc; i1 = 0; j0 = 1; j1 = my; }
-            else if (op.face == 1) { i0 = mx + 1; i1 = mx + mbc; j0 = 1; j1 = my; }
-            else if (op.face == 2) { i0 = 1; i1 = mx; j0 = 1 - mbc; j1 = 0; }
-            else { i0 = 1; i1 = mx; j0 = my + 1; j1 = my + mbc; }
-            const int w = i1 - i0 + 1, h = j1 - j0 + 1, n = w * h * meqn;
+    for (int side = 0; side < 4; ++side) {
+        const int mth = op.mthbc[side];
+        if (mth == 1 || mth == 3) {
+            const bool xside = side < 2;
+            const int len = xside ? ny : nx;
+            const int n = meqn * mbc * len;
             for (int k = lane; k < n; k += 32) {
-                const int m = k / (w * h), rem = k - m * w * h, jj = rem / w, ii = rem - jj * w;
-                const int i = i0 + ii, j = j0 + jj;
-                D.at(i, j, m) = S.at(i + op.dx, j + op.dy, m);
-            }
-            break;
-        }
-        case OP_COPY_CORNER: {
-            const int n = mbc * mbc * meqn;
-            for (int k = lane; k < n; k += 32) {
-                const int m = k / (mbc * mbc), rem = k - m * mbc * mbc;
-                const int ibc = rem / mbc + 1, jbc = rem % mbc + 1;
-                int i1, j1;
-                if (op.face == 0) { i1 = 1 - ibc; j1 = 1 - jbc; }
-                else if (op.face == 1) { i1 = mx + ibc; j1 = 1 - jbc; }
-                else if (op.face == 2) { i1 = 1 - ibc; j1 = my + jbc; }
-                else { i1 = mx + ibc; j1 = my + jbc; }
-                D.at(i1, j1, m) = S.at(i1 + op.dx, j1 + op.dy, m);
-            }
-            break;
-        }
-        case OP_AVERAGE_FACE: {
-            // dst = coarse patch, src = fine patch; face is the coarse face.
-            const int idir = op.face / 2;
-            const int along = idir == 0 ? my : mx;
-            const int n = along * mbc * meqn;
-            for (int k = lane; k < n; k += 32) {
-                const int m = k / (along * mbc), rem = k - m * along * mbc;
-                const int t = rem / mbc + 1, bc = rem % mbc + 1;
-                int ic, jc;
-                if (idir == 0) { jc = t; ic = (op.face == 0) ? 1 - bc : mx + bc; }
-                else { ic = t; jc = (op.face == 2) ? 1 - bc : my + bc; }
-                const int fi = 2 * ic + op.dx, fj = 2 * jc + op.dy;
-                if (fi < 1 || fi + 1 > mx || fj < 1 || fj + 1 > my) continue;  // is_valid_average
-                double sum = 0;
-                sum = sum + S.at(fi, fj, m);
-                sum = sum + S.at(fi + 1, fj, m);
-                sum = sum + S.at(fi, fj + 1, m);
-                sum = sum + S.at(fi + 1, fj + 1, m);
-                D.at(ic, jc, m) = sum / 4.0;
-            }
-            break;
-        }
-        case OP_AVERAGE_CORNER: {
-            const int n = mbc * mbc * meqn;
-            for (int k = lane; k < n; k += 32) {
-                const int m = k / (mbc * mbc), rem = k - m * mbc * mbc;
-                const int ibc = rem / mbc + 1, jbc = rem % mbc + 1;
-                int i1, j1;
-                if (op.face == 0) { i1 = 1 - ibc; j1 = 1 - jbc; }
-                else if (op.face == 1) { i1 = mx + ibc; j1 = 1 - jbc; }
-                else if (op.face == 2) { i1 = 1 - ibc; j1 = my + jbc; }
-                else { i1 = mx + ibc; j1 = my + jbc; }
-                const int fi = 2 * i1 + op.dx, fj = 2 * j1 + op.dy;
-                double sum = 0;
-                sum = sum + S.at(fi, fj, m);
-                sum = sum + S.at(fi + 1, fj, m);
-                sum = sum + S.at(fi, fj + 1, m);
-                sum = sum + S.at(fi + 1, fj + 1, m);
-                D.at(i1, j1, m) = sum / 4.0;
-            }
-            break;
-        }
-        case OP_INTERP_FACE: {
-            // src = coarse patch (q or time-interpolated), dst = fine patch (q).
-            const int idir = op.face / 2;
-            const int nb = mbc / 2;
-            const int along = idir == 0 ? mx : mx;  // the reference loops jc = 1..mx for idir = 0
-            const int n = along * nb * meqn;
-            for (int k = lane; k < n; k += 32) {
-                const int m = k / (along * nb), rem = k - m * along * nb;
-                const int t = rem / nb + 1, b = rem % nb + 1;
-                int ic, jc;
-                if (idir == 0) { jc = t; ic = (op.face == 0) ? b : mx - b + 1; }
-                else { ic = t; jc = (op.face == 2) ? b : my - b + 1; }
-                const int fi = 2 * ic + op.dx, fj = 2 * jc + op.dy;
-                if (fi < 1 - mbc || fi + 1 > mx + mbc || fj < 1 - mbc || fj + 1 > my + mbc) continue;
-                interp_cell(a.interp_fp32 != 0, S, D, m, ic, jc, fi, fj);
-            }
-            break;
-        }
-        case OP_INTERP_CORNER: {
-            const int nb = mbc / 2;
-            const int n = nb * nb * meqn;
-            for (int k = lane; k < n; k += 32) {
-                const int m = k / (nb * nb), rem = k - m * nb * nb;
-                const int ibc = rem / nb + 1, jbc = rem % nb + 1;
-                int ic, jc;
-                if (op.face == 0) { ic = ibc; jc = jbc; }
-                else if (op.face == 1) { ic = mx - ibc + 1; jc = jbc; }
-                else if (op.face == 2) { ic = ibc; jc = my - jbc + 1; }
-                else { ic = mx - ibc + 1; jc = my - jbc + 1; }
-                interp_cell(a.interp_fp32 != 0, S, D, m, ic, jc, 2 * ic + op.dx, 2 * jc + op.dy);
-            }
-            break;
-        }
-        case OP_PHYSBC: {
-            // Sides in the reference order; each side reads cells the previous side may write.
-            const int nyg = my + 2 * mbc, nxg = mx + 2 * mbc;
-            for (int side = 0; side < 4; ++side) {
-                const int mth = op.mthbc[side];
-                if (mth == 1 || mth == 3) {
-                    const bool xside = side < 2;
-                    const int len = xside ? nyg : nxg;
-                    const int n = meqn * mbc * len;
-                    for (int k = lane; k < n; k += 32) {
-                        const int m = k / (mbc * len), rem = k - m * mbc * len;
-                        const int bc = rem / len + 1, t = rem % len + (1 - mbc);
-                        if (side == 0) {
-                            double v = (mth == 1) ? D.at(1, t, m) : D.at(bc, t, m);
-                            if (mth == 3 && m == 1) v = -v;
-                            D.at(1 - bc, t, m) = v;
-                        } else if (side == 1) {
-                            double v = (mth == 1) ? D.at(mx, t, m) : D.at(mx + 1 - bc, t, m);
-                            if (mth == 3 && m == 1) v = -v;
-                            D.at(mx + bc, t, m) = v;
-                        } else if (side == 2) {
-                            double v = (mth == 1) ? D.at(t, 1, m) : D.at(t, bc, m);
-                            if (mth == 3 && m == 2) v = -v;
-                            D.at(t, 1 - bc, m) = v;
-                        } else {
-                            double v = (mth == 1) ? D.at(t, my, m) : D.at(t, my + 1 - bc, m);
-                            if (mth == 3 && m == 2) v = -v;
-                            D.at(t, my + bc, m) = v;
-                        }
-                    }
+                const int m = k / (mbc * len), rem = k - m * mbc * len;
+                const int bc = rem / len + 1, t = rem % len + (1 - mbc);
+                if (side == 0) {
+                    double v = (mth == 1) ? D.at(1, t, m) : D.at(bc, t, m);
+                    if (mth == 3 && m == 1) v = -v;
+                    D.at(1 - bc, t, m) = v;
+                } else if (side == 1) {
+                    double v = (mth == 1) ? D.at(mx, t, m) : D.at(mx + 1 - bc, t, m);
+                    if (mth == 3 && m == 1) v = -v;
+                    D.at(mx + bc, t, m) = v;
+                } else if (side == 2) {
+                    double v = (mth == 1) ? D.at(t, 1, m) : D.at(t, bc, m);
+                    if (mth == 3 && m == 2) v = -v;
+                    D.at(t, 1 - bc, m) = v;
+                } else {
+                    double v = (mth == 1) ? D.at(t, my, m) : D.at(t, my + 1 - bc, m);
+                    if (mth == 3 && m == 2) v = -v;
+                    D.at(t, my + bc, m) = v;
                 }
-                __syncwarp();
             }
-            break;
         }
-        default: break;
+        __syncwarp();
     }
 }
 
@@ -249,7 +139,7 @@ __device__ __forceinline__ int op_cells(const GhostArgs& a, const GhostOp& op) {
     }
 }
 
-// Work item k of a record (the same decomposition as ghost_op's loops).  Copy
+// Work item k of a record.  Copy
 // and average items return their value and destination so the caller can
 // issue several loads before the stores; interpolation items store their four
 // fine cells themselves and return nullptr.
@@ -400,7 +290,7 @@ __global__ void __launch_bounds__(GHOST_TPB) ghost_wave_kernel(const GhostArgs a
         while (pm) {
             const int l = __ffs(pm) - 1;
             pm &= pm - 1;
-            ghost_op<MXC>(a, s_ops[wl][l], lane);
+            physbc_op<MXC>(a, s_ops[wl][l], lane);
         }
         __syncwarp();
     }
