@@ -335,11 +335,45 @@ def run_ours(args, rank, world, local_rank):
         "roofline_fp": fp_roofline("advection_swirl_order22", args.mx, cells_per_step / (step_ms * 1e-3),
                                    args.precision, stream.cuda_stream),
     }
+    if args.precision == "mixed":
+        line["config"]["accuracy"] = _mixed_accuracy(args, opts, dt, stream)
     if world == 1:
         sys.path.insert(0, str(ROOT / "tests"))
         line["cpu_baseline"] = cpu_sample(args, args.cpu_seconds)
     s.close()
     return line
+
+
+def _mixed_accuracy(args, opts, dt, stream, steps=20):
+    """The mixed form against the FP64 form on the GPU after `steps` steps of
+    the same workload: relative L1 and max-norm error of the interior cells and
+    the relative difference of the mass sums."""
+    import dataclasses
+
+    import numpy as np
+
+    import forestclaw_b200 as fcb
+
+    q = {}
+    mass = {}
+    for prec in (fcb.PRECISION_MIXED, fcb.PRECISION_FP64):
+        o = dataclasses.replace(opts, precision=prec)
+        s = fcb.Solver(o, stream=stream.cuda_stream)
+        s.initialize()
+        t = 0.0
+        for _ in range(steps):
+            s.advance_all_levels(t, dt)
+            t += dt
+        q[prec] = s.get_q()
+        mass[prec] = np.asarray(s.conservation_check())
+        s.close()
+    m = opts.mbc
+    a, b = q[fcb.PRECISION_MIXED][..., m:-m, m:-m], q[fcb.PRECISION_FP64][..., m:-m, m:-m]
+    return {"against": f"the FP64 form on the GPU after {steps} steps",
+            "l1_rel": float(np.abs(a - b).sum() / np.abs(b).sum()),
+            "max_rel": float(np.abs(a - b).max() / max(1.0, np.abs(b).max())),
+            "mass_drift_rel": float(np.max(np.abs(mass[fcb.PRECISION_MIXED] - mass[fcb.PRECISION_FP64]))
+                                    / np.max(np.abs(mass[fcb.PRECISION_FP64])))}
 
 
 # FP64 operations per interior cell update of the reference's patch step
