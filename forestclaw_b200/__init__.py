@@ -19,7 +19,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-__all__ = ["Options", "Solver", "lib", "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
+__all__ = ["Options", "Solver", "Comm", "local_group", "nccl_unique_id", "nccl_comm", "lib", "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
            "SOLVER_EULER4_ROE", "SOLVER_GEOCLAW_FWAVE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM",
            "PROBLEM_QUADRANTS", "PROBLEM_BATHY", "PROBLEM_RADIALDAM_CELLAVE",
            "PRECISION_FP64", "PRECISION_MIXED", "measure_fp_rate",
@@ -42,7 +42,9 @@ EXPORTED_SYMBOLS = (
     "fcb_update_single_step", "fcb_update_single_step_async", "fcb_conservation_sum_noalloc",
     "fcb_server_create", "fcb_server_destroy", "fcb_server_submit", "fcb_server_round", "fcb_server_status",
     "fcb_server_get_q", "fcb_server_release", "fcb_server_clock", "fcb_autotune_info",
-    "fcb_measure_fp_rate", "fcb_output_ascii",
+    "fcb_measure_fp_rate", "fcb_output_ascii", "fcb_comm_create_local", "fcb_comm_nccl_unique_id",
+    "fcb_comm_create_nccl", "fcb_comm_destroy", "fcb_context_create_partitioned", "fcb_partition_info",
+    "fcb_global_maximum",
 )
 
 
@@ -71,6 +73,7 @@ class _Options(ctypes.Structure):
         ("dry_tolerance", ctypes.c_double),
         ("time_sync", ctypes.c_int),
         ("ax", ctypes.c_double), ("bx", ctypes.c_double), ("ay", ctypes.c_double), ("by", ctypes.c_double),
+        ("weighted_partition", ctypes.c_int),
     ]
 
 
@@ -142,6 +145,8 @@ class Options:
     time_sync: int = 0
     # [Options] ax, bx, ay, by: physical extent of the block
     extent: Sequence[float] = (0.0, 1.0, 0.0, 1.0)
+    # [Options] weighted-partition: partitioned solves weigh leaves by 2^level when subcycling
+    weighted_partition: int = 1
 
     def to_c(self) -> _Options:
         o = _Options()
@@ -149,7 +154,7 @@ class Options:
                      "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
                      "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
                      "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph", "claw_version",
-                     "time_sync"):
+                     "time_sync", "weighted_partition"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
                      "desired_cfl", "grav", "gamma", "dry_tolerance"):
@@ -231,6 +236,14 @@ def lib():
     L.fcb_server_get_q.argtypes = [vp, ctypes.c_int, dp, sz]
     L.fcb_server_release.argtypes = [vp, ctypes.c_int]
     L.fcb_server_clock.argtypes = [vp, dp, ll, ll]
+    L.fcb_comm_create_local.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(vp)]
+    L.fcb_comm_nccl_unique_id.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    L.fcb_comm_create_nccl.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, ctypes.POINTER(vp)]
+    L.fcb_comm_destroy.argtypes = [vp]
+    L.fcb_context_create_partitioned.argtypes = [ctypes.POINTER(_Options), vp, vp, ctypes.POINTER(vp)]
+    L.fcb_partition_info.argtypes = [vp, ip, ip, ip, ip]
+    L.fcb_global_maximum.argtypes = [vp, ctypes.c_double, dp]
     _lib = L
     return L
 
@@ -251,16 +264,95 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-class Solver:
-    """One solve on one GPU (a context of the C ABI)."""
+class Comm:
+    """One rank's communicator of a partitioned solve (fcb_comm_t)."""
 
-    def __init__(self, options: Options, stream: Optional[int] = None):
+    def __init__(self, handle: ctypes.c_void_p, rank: int, nranks: int):
+        self._h = handle
+        self.rank = rank
+        self.nranks = nranks
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().fcb_comm_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def local_group(nranks: int, timeout_s: float = 120.0) -> list:
+    """Communicators of an in-process group: rank r's Solver is driven by its
+    own host thread (ctypes releases the GIL during library calls)."""
+    arr = (ctypes.c_void_p * nranks)()
+    _check(lib().fcb_comm_create_local(int(nranks), float(timeout_s), arr))
+    return [Comm(ctypes.c_void_p(arr[r]), r, nranks) for r in range(nranks)]
+
+
+def nccl_library() -> str:
+    """libnccl.so.2 of the NCCL PyTorch ships (the one a torch process loads), else ''."""
+    try:
+        import nvidia.nccl as n  # noqa: PLC0415
+        for root in n.__path__:
+            f = Path(root) / "lib" / "libnccl.so.2"
+            if f.exists():
+                return str(f)
+    except ImportError:
+        pass
+    return ""
+
+
+def nccl_unique_id(library: Optional[str] = None) -> bytes:
+    """The 128-byte id of a new NCCL communicator (made on one rank, sent to the others)."""
+    buf = ctypes.create_string_buffer(128)
+    lp = (library if library is not None else nccl_library()).encode()
+    _check(lib().fcb_comm_nccl_unique_id(lp, buf))
+    return buf.raw
+
+
+def nccl_comm(unique_id: bytes, rank: int, nranks: int, timeout_s: float = 120.0,
+              library: Optional[str] = None) -> Comm:
+    """Rank `rank` of an NCCL communicator on the current CUDA device."""
+    if len(unique_id) != 128:
+        raise ValueError("an NCCL unique id has 128 bytes")
+    h = ctypes.c_void_p()
+    lp = (library if library is not None else nccl_library()).encode()
+    _check(lib().fcb_comm_create_nccl(lp, unique_id, int(rank), int(nranks), float(timeout_s), ctypes.byref(h)))
+    return Comm(h, rank, nranks)
+
+
+class Solver:
+    """One solve on one GPU (a context of the C ABI); with `comm`, one rank of
+    a partitioned solve."""
+
+    def __init__(self, options: Options, stream: Optional[int] = None, comm: Optional[Comm] = None):
         self.options = options
         self._copt = options.to_c()
+        self.comm = comm
         h = ctypes.c_void_p()
-        _check(lib().fcb_context_create(ctypes.byref(self._copt), ctypes.c_void_p(stream or 0),
-                                        ctypes.byref(h)))
+        if comm is None:
+            _check(lib().fcb_context_create(ctypes.byref(self._copt), ctypes.c_void_p(stream or 0),
+                                            ctypes.byref(h)))
+        else:
+            _check(lib().fcb_context_create_partitioned(ctypes.byref(self._copt), ctypes.c_void_p(stream or 0),
+                                                        comm._h, ctypes.byref(h)))
         self._h = h
+
+    def partition_info(self) -> dict:
+        """This rank, the number of ranks and the owned leaves [first, first + count)."""
+        r, n, f, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().fcb_partition_info(self._h, ctypes.byref(r), ctypes.byref(n), ctypes.byref(f),
+                                        ctypes.byref(c)))
+        return {"rank": r.value, "nranks": n.value, "first": f.value, "count": c.value}
+
+    def global_maximum(self, value: float) -> float:
+        """fclaw2d_domain_global_maximum over the ranks of a partitioned solve."""
+        out = ctypes.c_double()
+        _check(lib().fcb_global_maximum(self._h, float(value), ctypes.byref(out)))
+        return out.value
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

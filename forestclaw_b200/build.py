@@ -25,6 +25,20 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
           "-I", str(PKG.parent / "include")]
 
+
+
+def _nccl_include() -> str:
+    """nccl.h of the NCCL that PyTorch ships (the library the process loads), else the system one."""
+    try:
+        import nvidia.nccl as n  # noqa: PLC0415
+        for root in n.__path__:
+            if (Path(root) / "include" / "nccl.h").exists():
+                return str(Path(root) / "include")
+    except ImportError:
+        pass
+    return "/usr/include"
+
+
 # per-source extra flags
 SOURCES = {
     "fcb_step.cu": ["-fmad=false"],
@@ -40,6 +54,7 @@ SOURCES = {
     "fcb_probe.cu": ["-fmad=false"],
     "fcb_timesync.cu": ["-fmad=false"],
     "fcb_output.cpp": [],
+    "fcb_comm.cu": ["-I", _nccl_include()],
 }
 
 

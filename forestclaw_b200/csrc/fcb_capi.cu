@@ -2,6 +2,7 @@
 // catches exceptions and CUDA errors and turns them into status codes; the
 // library never terminates the process.
 #include <cmath>
+#include <memory>
 #include <new>
 #include <string>
 
@@ -14,6 +15,10 @@ struct fcb_server {
 
 struct fcb_context {
     fcb::Context* impl;
+};
+
+struct fcb_comm {
+    std::shared_ptr<fcb::Comm> impl;
 };
 
 namespace {
@@ -39,6 +44,17 @@ int guard(F&& f) {
 int need(const void* p, const char* what) {
     if (!p) throw fcb::Error(FCB_ERR_INVALID, std::string("null argument: ") + what);
     return 0;
+}
+
+// A collective call of a partitioned solve that fails on this rank marks the
+// communicator failed, so the other ranks' next collective returns
+// FCB_ERR_COMM instead of waiting out the time limit.
+template <class F>
+int collective(fcb_context_t* ctx, F&& f) {
+    const int rc = guard(std::forward<F>(f));
+    if (rc != FCB_OK && rc != FCB_ERR_COMM && ctx && ctx->impl && ctx->impl->partitioned())
+        ctx->impl->abort_comm(g_error);
+    return rc;
 }
 }  // namespace
 
@@ -79,11 +95,11 @@ int fcb_context_destroy(fcb_context_t* ctx) {
     need(ctx, "ctx");         \
     fcb::Context& C = *ctx->impl
 
-int fcb_initialize(fcb_context_t* ctx) { return guard([&] { CTX(); C.initialize(); }); }
-int fcb_run(fcb_context_t* ctx) { return guard([&] { CTX(); C.run(); }); }
+int fcb_initialize(fcb_context_t* ctx) { return collective(ctx, [&] { CTX(); C.initialize(); }); }
+int fcb_run(fcb_context_t* ctx) { return collective(ctx, [&] { CTX(); C.run(); }); }
 
 int fcb_advance_all_levels(fcb_context_t* ctx, double t, double dt, double* maxcfl) {
-    return guard([&] {
+    return collective(ctx, [&] {
         CTX();
         need(maxcfl, "maxcfl");
         *maxcfl = C.advance_all_levels(t, dt);
@@ -115,7 +131,7 @@ int fcb_single_step_update(fcb_context_t* ctx, int patchno, double t, double dt,
 }
 
 int fcb_ghost_update(fcb_context_t* ctx, int minlevel, int maxlevel, double sync_time, int time_interp) {
-    return guard([&] {
+    return collective(ctx, [&] {
         CTX();
         C.ghost_update(minlevel, maxlevel, sync_time, time_interp);
     });
@@ -126,7 +142,7 @@ int fcb_timeinterp(fcb_context_t* ctx, int level, double alpha) {
 }
 
 int fcb_regrid(fcb_context_t* ctx, int* changed) {
-    return guard([&] {
+    return collective(ctx, [&] {
         CTX();
         const bool ch = C.regrid();
         if (changed) *changed = ch ? 1 : 0;
@@ -201,7 +217,7 @@ int fcb_counters(fcb_context_t* ctx, fcb_counters_t* out) {
 }
 
 int fcb_conservation_check(fcb_context_t* ctx, double* sums) {
-    return guard([&] { CTX(); need(sums, "sums"); C.conservation(sums); });
+    return collective(ctx, [&] { CTX(); need(sums, "sums"); C.conservation(sums); });
 }
 
 int fcb_curr_time(fcb_context_t* ctx, double* t) {
@@ -209,6 +225,78 @@ int fcb_curr_time(fcb_context_t* ctx, double* t) {
 }
 
 int fcb_synchronize(fcb_context_t* ctx) { return guard([&] { CTX(); C.synchronize(); }); }
+
+// ---- partitioned solves ------------------------------------------------------
+int fcb_comm_create_local(int nranks, double timeout_s, fcb_comm_t** comms) {
+    return guard([&] {
+        need(comms, "comms");
+        auto g = fcb::make_local_group(nranks, timeout_s);
+        for (int r = 0; r < nranks; ++r) comms[r] = nullptr;
+        for (int r = 0; r < nranks; ++r) comms[r] = new fcb_comm{g[r]};
+    });
+}
+
+int fcb_comm_nccl_unique_id(const char* nccl_library, unsigned char id[128]) {
+    return guard([&] {
+        need(id, "id");
+        fcb::nccl_unique_id(nccl_library, id);
+    });
+}
+
+int fcb_comm_create_nccl(const char* nccl_library, const unsigned char id[128], int rank, int nranks,
+                         double timeout_s, fcb_comm_t** out) {
+    return guard([&] {
+        need(id, "id");
+        need(out, "out");
+        *out = nullptr;
+        auto c = fcb::make_nccl_comm(nccl_library, id, rank, nranks, timeout_s);
+        *out = new fcb_comm{std::move(c)};
+    });
+}
+
+int fcb_comm_destroy(fcb_comm_t* comm) {
+    return guard([&] { delete comm; });
+}
+
+int fcb_context_create_partitioned(const fcb_options_t* opt, void* cuda_stream, fcb_comm_t* comm,
+                                   fcb_context_t** out) {
+    return guard([&] {
+        need(opt, "opt");
+        need(comm, "comm");
+        need(out, "out");
+        *out = nullptr;
+        auto* c = new fcb_context{nullptr};
+        try {
+            c->impl = new fcb::Context(*opt, (cudaStream_t)cuda_stream, comm->impl);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int fcb_partition_info(fcb_context_t* ctx, int* rank, int* nranks, int* first, int* count) {
+    return guard([&] {
+        CTX();
+        need(rank, "rank");
+        need(nranks, "nranks");
+        need(first, "first");
+        need(count, "count");
+        *rank = C.rank();
+        *nranks = C.nranks();
+        *first = C.own_first();
+        *count = C.own_count();
+    });
+}
+
+int fcb_global_maximum(fcb_context_t* ctx, double value, double* out) {
+    return collective(ctx, [&] {
+        CTX();
+        need(out, "out");
+        *out = C.global_maximum(value);
+    });
+}
 
 int fcb_output_ascii(fcb_context_t* ctx, int iframe, const char* dir) {
     return guard([&] {

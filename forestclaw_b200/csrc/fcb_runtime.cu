@@ -88,8 +88,16 @@ static int solver_meqn(int kind) {
     }
 }
 
-Context::Context(const fcb_options_t& o, cudaStream_t st) : opt_(o), st_(st) {
+Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> comm)
+    : opt_(o), st_(st), comm_(std::move(comm)) {
     auto bad = [](const std::string& m) { throw Error(FCB_ERR_INVALID, m); };
+    if (comm_) {
+        rank_ = comm_->rank();
+        nranks_ = comm_->size();
+        if (opt_.time_sync) bad("time-sync is not available in a partitioned solve");
+        // the exchanges are host-driven collectives: every launch is issued from the host
+        opt_.macro_graph = 0;
+    }
     if (opt_.mx != opt_.my) bad("mx must equal my");
     if (opt_.mbc != 2) bad("mbc must be 2");
     if (opt_.mx != 8 && opt_.mx != 16 && opt_.mx != 32 && opt_.mx != 64) bad("mx must be 8, 16, 32 or 64");
@@ -283,9 +291,14 @@ void Context::mesh_changed() {
     nbrs_.resize(n);
     for (int p = 0; p < n; ++p) nbrs_[p] = forest_.neighbors(p);
     // slot metadata
+    if (!partitioned()) {
+        own_first_ = 0;
+        own_count_ = n;
+    }
     std::vector<PatchMeta> hm((size_t)capacity_);
     check(cudaStreamSynchronize(st_), "sync");
     for (int p = 0; p < n; ++p) {
+        if (slot_of_[p] < 0) continue;  // neither owned nor in the ghost layer
         PatchMeta m = meta_of(forest_.leaves[p]);
         if (nbrs_[p].has_fine) m.flags |= PATCH_SAVE_LAST;
         hm[slot_of_[p]] = m;
@@ -297,7 +310,7 @@ void Context::mesh_changed() {
     level_begin_.assign(L + 1, 0);
     ti_begin_.assign(L + 1, 0);
     std::vector<std::vector<int32_t>> by(L), tby(L);
-    for (int p = 0; p < n; ++p) {
+    for (int p = own_first_; p < own_first_ + own_count_; ++p) {
         by[forest_.leaves[p].level].push_back(slot_of_[p]);
         if (nbrs_[p].has_fine) tby[forest_.leaves[p].level].push_back(slot_of_[p]);
     }
@@ -315,13 +328,16 @@ void Context::mesh_changed() {
     gmax_ = forest_.max_level();
     d_level_slots_.reserve(std::max<size_t>(1, h_level_slots_.size()));
     d_ti_slots_.reserve(std::max<size_t>(1, tis.size()));
-    d_all_slots_.reserve(std::max(1, n));
-    check(cudaMemcpy(d_level_slots_.p, h_level_slots_.data(), h_level_slots_.size() * 4, cudaMemcpyHostToDevice), "levels");
+    d_all_slots_.reserve(std::max(1, own_count_));
+    if (!h_level_slots_.empty())
+        check(cudaMemcpy(d_level_slots_.p, h_level_slots_.data(), h_level_slots_.size() * 4, cudaMemcpyHostToDevice),
+              "levels");
     if (!tis.empty()) check(cudaMemcpy(d_ti_slots_.p, tis.data(), tis.size() * 4, cudaMemcpyHostToDevice), "ti");
-    std::vector<int32_t> all(slot_of_.begin(), slot_of_.end());
-    check(cudaMemcpy(d_all_slots_.p, all.data(), all.size() * 4, cudaMemcpyHostToDevice), "all slots");
-    if (opt_.problem == FCB_PROBLEM_BATHY) {
-        check(launch_setaux(d_aux_, aux_stride_, d_all_slots_.p, d_meta_, n, opt_.mx, opt_.my, opt_.mbc, st_),
+    // the owned leaves in Morton order (all leaves on one rank)
+    std::vector<int32_t> all(slot_of_.begin() + own_first_, slot_of_.begin() + own_first_ + own_count_);
+    if (!all.empty()) check(cudaMemcpy(d_all_slots_.p, all.data(), all.size() * 4, cudaMemcpyHostToDevice), "all slots");
+    if (opt_.problem == FCB_PROBLEM_BATHY && own_count_ > 0) {
+        check(launch_setaux(d_aux_, aux_stride_, d_all_slots_.p, d_meta_, own_count_, opt_.mx, opt_.my, opt_.mbc, st_),
               "setaux");
         ++cnt_.count_kernel_launches;
     }
@@ -331,6 +347,7 @@ void Context::mesh_changed() {
     h_ts_groups_.clear();
     h_ops_.clear();
     h_groups_.clear();
+    h_xitems_.clear();
     ops_dirty_ = true;
 }
 
@@ -351,7 +368,7 @@ struct Touch {
 
 // fclaw2d_ghost_update_async (src/fclaw2d_ghost_fill.c:611-831) on one rank:
 // the records are emitted in the order the reference's callbacks run.
-void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>& ops) const {
+void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>& ops, size_t* phase_b) const {
     const int mx = opt_.mx, my = opt_.my;
     const int n = num_patches();
     std::vector<std::vector<int>> at((size_t)QuadForest::kMaxLevel + 1);
@@ -375,7 +392,7 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
             for (int f = 0; f < 4; ++f) {
                 if (nbrs_[p].face_rel[f] != REL_SAMESIZE) continue;
                 const int q = nbrs_[p].face_nbr[f][0];
-                GhostOp o = base(OP_COPY_FACE, slot_of_[p], slot_of_[q], f, t, t);
+                GhostOp o = base(OP_COPY_FACE, p, q, f, t, t);
                 o.dx = (int)((xl(p) - xl(q)) * iw * (double)mx);
                 o.dy = (int)((yl(p) - yl(q)) * iw * (double)my);
                 ops.push_back(o);
@@ -384,7 +401,7 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
             for (int c = 0; c < 4; ++c) {
                 if (nbrs_[p].corner_rel[c] != REL_SAMESIZE) continue;
                 const int q = nbrs_[p].corner_nbr[c];
-                GhostOp o = base(OP_COPY_CORNER, slot_of_[p], slot_of_[q], c, t, t);
+                GhostOp o = base(OP_COPY_CORNER, p, q, c, t, t);
                 o.dx = (int)((xl(p) - xl(q) + 0.) * (iw * (double)mx));
                 o.dy = (int)((yl(p) - yl(q) + 0.) * (iw * (double)my));
                 ops.push_back(o);
@@ -404,8 +421,7 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
                 if (nbrs_[p].face_rel[f] != REL_HALFSIZE) continue;
                 for (int ig = 0; ig < 2; ++ig) {
                     const int q = nbrs_[p].face_nbr[f][ig];
-                    GhostOp o = average ? base(OP_AVERAGE_FACE, slot_of_[p], slot_of_[q], f, t, 0)
-                                        : base(OP_INTERP_FACE, slot_of_[q], slot_of_[p], f, 0, t);
+                    GhostOp o = average ? base(OP_AVERAGE_FACE, p, q, f, t, 0) : base(OP_INTERP_FACE, q, p, f, 0, t);
                     half(p, q, o.dx, o.dy);
                     ops.push_back(o);
                 }
@@ -416,8 +432,7 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
             for (int c = 0; c < 4; ++c) {
                 if (nbrs_[p].corner_rel[c] != REL_HALFSIZE) continue;
                 const int q = nbrs_[p].corner_nbr[c];
-                GhostOp o = average ? base(OP_AVERAGE_CORNER, slot_of_[p], slot_of_[q], c, t, 0)
-                                    : base(OP_INTERP_CORNER, slot_of_[q], slot_of_[p], c, 0, t);
+                GhostOp o = average ? base(OP_AVERAGE_CORNER, p, q, c, t, 0) : base(OP_INTERP_CORNER, q, p, c, 0, t);
                 half(p, q, o.dx, o.dy);
                 ops.push_back(o);
             }
@@ -426,7 +441,7 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
     // setphysical (fclaw2d_ghost_fill.c:290-308) -> clawpack46_bc2
     auto setphysical = [&](int level, int t) {
         for (int p : level_list(level)) {
-            GhostOp o = base(OP_PHYSBC, slot_of_[p], slot_of_[p], 0, t, t);
+            GhostOp o = base(OP_PHYSBC, p, p, 0, t, t);
             bool any = false;
             for (int f = 0; f < 4; ++f)
                 if (nbrs_[p].face_rel[f] == REL_BOUNDARY) { o.mthbc[f] = opt_.mthbc[f]; any = true; }
@@ -440,6 +455,7 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
     if (ti) copy2ghost(minlevel - 1, 1);
     for (int l = maxcoarse; l >= mincoarse; --l) setphysical(l, 0);
     if (ti) setphysical(mincoarse - 1, 1);
+    if (phase_b) *phase_b = ops.size();
     for (int l = maxcoarse; l >= mincoarse; --l) coarse_fine(l, 0, false);
     if (ti) coarse_fine(mincoarse - 1, 1, false);
     const int minfine = mincoarse + 1, maxfine = maxlevel;
@@ -449,13 +465,90 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
     if (ti) setphysical(minlevel - 1, 1);
 }
 
-// A plan's records in waves: each record goes one wave after the latest
-// earlier record it conflicts with (read-after-write, write-after-read,
-// write-after-write on overlapping cells of the same array), so the records of a
-// wave are independent and the waves keep the reference's order.
+// A ghost plan.  One rank: every record, in waves.  Partitioned: the records
+// whose destination this rank owns, in two wave sets (averages / copies /
+// coarse physical boundaries, then interpolations / remaining physical
+// boundaries), and the two exchanges before them.  No record writes a patch
+// interior, and the interpolations from level l read coarse ghost cells before
+// the interpolations into level l (which come later, l descending) write them,
+// so the first set reads only source interiors as they were before the update,
+// and the second reads sources as the first set left them: sending those two
+// states of the other ranks' patches reproduces the one-rank order exactly.
 Context::PlanBuild Context::build_plan(int minlevel, int maxlevel, int ti) const {
     std::vector<GhostOp> ops;
-    build_ops(minlevel, maxlevel, ti, ops);
+    size_t phase_b = 0;
+    build_ops(minlevel, maxlevel, ti, ops, &phase_b);
+    if (!partitioned()) {
+        for (GhostOp& o : ops) {
+            o.dst = slot_of_[o.dst];
+            o.src = slot_of_[o.src];
+        }
+        PlanBuild b = make_waves(ops);
+        b.nA = (int)b.wave_begin.size() - 1;
+        return b;
+    }
+    // exchange items (leaf * 2 + array) this rank receives from / sends to each rank
+    const int R = nranks_;
+    std::vector<std::vector<int64_t>> recv[2], send[2];
+    for (int x = 0; x < 2; ++x) {
+        recv[x].resize(R);
+        send[x].resize(R);
+    }
+    bool any[2] = {false, false};
+    std::vector<GhostOp> mine[2];
+    for (size_t k = 0; k < ops.size(); ++k) {
+        GhostOp o = ops[k];
+        const int x = k < phase_b ? 0 : 1;
+        const int od = owner_[o.dst], os = owner_[o.src];
+        if (od != os) {
+            any[x] = true;
+            const int64_t item = (int64_t)o.src * 2 + o.src_ti;
+            if (od == rank_) recv[x][os].push_back(item);
+            else if (os == rank_) send[x][od].push_back(item);
+        }
+        if (od != rank_) continue;
+        o.dst = slot_of_[o.dst];
+        o.src = slot_of_[o.src];
+        if (o.dst < 0 || o.src < 0) throw Error(FCB_ERR_INTERNAL, "ghost record outside the local patches");
+        mine[x].push_back(o);
+    }
+    PlanBuild b = make_waves(mine[0]);
+    b.nA = (int)b.wave_begin.size() - 1;
+    PlanBuild c = make_waves(mine[1]);
+    const int nops = (int)b.ops.size(), ngroups = (int)b.groups.size();
+    b.ops.insert(b.ops.end(), c.ops.begin(), c.ops.end());
+    for (size_t w = 1; w < c.wave_begin.size(); ++w) b.wave_begin.push_back(c.wave_begin[w] + nops);
+    b.group_begin.pop_back();
+    for (int g : c.group_begin) b.group_begin.push_back(g + ngroups);
+    for (int32_t g : c.groups) b.groups.push_back(g + nops);
+    for (int x = 0; x < 2; ++x) {
+        XList& xl = x == 0 ? b.x1 : b.x2;
+        xl.any = any[x];
+        xl.send_n.assign(R, 0);
+        xl.recv_n.assign(R, 0);
+        for (int r = 0; r < R; ++r) {
+            for (auto* v : {&recv[x][r], &send[x][r]}) {
+                std::sort(v->begin(), v->end());
+                v->erase(std::unique(v->begin(), v->end()), v->end());
+            }
+            for (int64_t it : send[x][r]) xl.send.push_back(slot_of_[it >> 1] * 2 + (int32_t)(it & 1));
+            for (int64_t it : recv[x][r]) {
+                const int sl = slot_of_[it >> 1];
+                if (sl < 0) throw Error(FCB_ERR_INTERNAL, "ghost-layer patch without a slot");
+                xl.recv.push_back(sl * 2 + (int32_t)(it & 1));
+            }
+            xl.send_n[r] = (int)send[x][r].size();
+            xl.recv_n[r] = (int)recv[x][r].size();
+        }
+    }
+    return b;
+}
+
+// Records in waves: each record goes one wave after the latest earlier record
+// it conflicts with (read-after-write, write-after-read, write-after-write on
+// overlapping cells of the same array), so the records of a wave are
+// independent and the waves keep the reference's order.
+Context::PlanBuild Context::make_waves(const std::vector<GhostOp>& ops) const {
     const int mx = opt_.mx, my = opt_.my, mbc = opt_.mbc;
     const Rect whole{1 - mbc, mx + mbc, 1 - mbc, my + mbc};
     const Rect interior{1, mx, 1, my};
@@ -560,6 +653,18 @@ const GhostPlan& Context::commit_plan(const std::tuple<int, int, int>& key, Plan
     g.group_begin = std::move(b.group_begin);
     for (int32_t k : b.groups) h_groups_.push_back((int32_t)(g.first + k));
     h_ops_.insert(h_ops_.end(), b.ops.begin(), b.ops.end());
+    g.nA = b.nA;
+    g.x1 = std::move(b.x1);
+    g.x2 = std::move(b.x2);
+    for (XList* x : {&g.x1, &g.x2}) {
+        for (const auto* v : {&x->send, &x->recv})
+            for (int32_t it : *v)
+                if (it < 0 || (it >> 1) >= capacity_) throw Error(FCB_ERR_INTERNAL, "exchange item outside the arena");
+        x->send_first = h_xitems_.size();
+        h_xitems_.insert(h_xitems_.end(), x->send.begin(), x->send.end());
+        x->recv_first = h_xitems_.size();
+        h_xitems_.insert(h_xitems_.end(), x->recv.begin(), x->recv.end());
+    }
     ops_dirty_ = true;
     return plans_.emplace(key, std::move(g)).first->second;
 }
@@ -710,6 +815,14 @@ void Context::upload_ops() {
                               cudaMemcpyHostToDevice, st_),
               "groups");
     }
+    if (!h_xitems_.empty()) {
+        // exchange items (partitioned solves): small, copied synchronously
+        d_xitems_.reserve(h_xitems_.size());
+        check(cudaMemcpyAsync(d_xitems_.p, h_xitems_.data(), h_xitems_.size() * sizeof(int32_t),
+                              cudaMemcpyHostToDevice, st_),
+              "exchange items");
+        check(cudaStreamSynchronize(st_), "sync");
+    }
     check(cudaEventRecord(upload_ev_, st_), "cudaEventRecord");
     ops_dirty_ = false;
 }
@@ -857,7 +970,9 @@ void Context::run_plan(const GhostPlan& g) {
     if (ops_dirty_) upload_ops();
     ghost_unroll_ = opt_.step_variant == 0 ? tune_ghost_unroll(g) : 4;
     const int nw = (int)g.wave_begin.size() - 1;
+    exchange(g.x1);
     for (int w = 0; w < nw; ++w) {
+        if (w == g.nA) exchange(g.x2);
         GhostArgs a;
         a.q = d_q_;
         a.qti = d_qti_;
@@ -871,6 +986,112 @@ void Context::run_plan(const GhostPlan& g) {
         ++cnt_.count_ghost_waves;
         ++cnt_.count_kernel_launches;
     }
+    if (g.nA >= nw) exchange(g.x2);
+}
+
+// The ghost-patch exchange (fclaw2d_exchange_ghost_patches_begin/_end,
+// fclaw2d_exchange.c:308-413): whole patch arrays packed by slot, one
+// alltoallv, unpacked into the ghost-layer slots.  Every rank calls it for
+// every exchange whose list is non-empty on some rank.
+void Context::exchange(const XList& x, const int32_t* d_items) {
+    if (!partitioned() || !x.any) return;
+    if (!d_items) d_items = d_xitems_.p;
+    const int64_t ps = (int64_t)patch_size();
+    const size_t ns = x.send.size(), nr = x.recv.size();
+    d_xsend_.reserve(std::max<size_t>(1, ns * ps));
+    d_xrecv_.reserve(std::max<size_t>(1, nr * ps));
+    check(launch_pack_patches(d_q_, d_qti_, stride_, d_items + x.send_first, (int)ns, ps, d_xsend_.p, true, st_),
+          "pack");
+    std::vector<size_t> so(nranks_), sb(nranks_), ro(nranks_), rb(nranks_);
+    size_t a = 0, b = 0;
+    for (int r = 0; r < nranks_; ++r) {
+        so[r] = a;
+        sb[r] = (size_t)x.send_n[r] * ps * sizeof(double);
+        a += sb[r];
+        ro[r] = b;
+        rb[r] = (size_t)x.recv_n[r] * ps * sizeof(double);
+        b += rb[r];
+    }
+    comm_->alltoallv(d_xsend_.p, so.data(), sb.data(), d_xrecv_.p, ro.data(), rb.data(), st_);
+    check(launch_pack_patches(d_q_, d_qti_, stride_, d_items + x.recv_first, (int)nr, ps, d_xrecv_.p, false, st_),
+          "unpack");
+    cnt_.count_kernel_launches += (ns ? 1 : 0) + (nr ? 1 : 0);
+}
+
+void Context::allgather_owned(const double* d_own, int per_leaf, double* d_all) {
+    std::vector<size_t> so(nranks_, 0), sb(nranks_, (size_t)own_count_ * per_leaf * sizeof(double)), ro(nranks_),
+        rb(nranks_);
+    for (int r = 0; r < nranks_; ++r) {
+        ro[r] = (size_t)cut_[r] * per_leaf * sizeof(double);
+        rb[r] = (size_t)(cut_[r + 1] - cut_[r]) * per_leaf * sizeof(double);
+    }
+    comm_->alltoallv(d_own, so.data(), sb.data(), d_all, ro.data(), rb.data(), st_);
+}
+
+double Context::global_maximum(double v) {
+    if (!partitioned()) return v;
+    unsigned long long bits;
+    std::memcpy(&bits, &v, sizeof bits);
+    if (std::signbit(v)) bits = 0;  // CFL numbers are >= 0
+    check(cudaMemcpyAsync(d_cfl_ + 2, &bits, sizeof bits, cudaMemcpyHostToDevice, st_), "global max");
+    comm_->allreduce_max_u64(d_cfl_ + 2, 1, st_);
+    check(cudaMemcpyAsync(h_cfl_, d_cfl_ + 2, sizeof bits, cudaMemcpyDeviceToHost, st_), "global max");
+    comm_->sync(st_);
+    return cfl_from_bits(*h_cfl_);
+}
+
+void Context::abort_comm(const std::string& why) noexcept {
+    if (comm_) comm_->abort(why);
+}
+
+// ---------------------------------------------------------------------------
+// Partition (fclaw2d_partition_domain, fclaw2d_partition.c:113-197, over
+// p4est_wrap_partition): rank r owns the Morton range [cut_[r], cut_[r+1]).
+// Cut r is the first leaf at which the running weight reaches r/R of the total
+// (weight 2^level with weighted_partition and subcycling, else 1), moved to the
+// nearer end of a complete family it would split (p4est's partition for
+// coarsening).  The solution never depends on the cuts: they only balance work.
+// ---------------------------------------------------------------------------
+void Context::partition_leaves() {
+    const int n = num_patches();
+    const int R = nranks_;
+    const int e = (opt_.subcycle && opt_.weighted_partition) ? 1 : 0;
+    std::vector<uint64_t> pre((size_t)n + 1, 0);
+    for (int p = 0; p < n; ++p) pre[p + 1] = pre[p] + ((uint64_t)1 << (e * forest_.leaves[p].level));
+    const unsigned __int128 W = pre[n];
+    cut_.assign(R + 1, 0);
+    cut_[R] = n;
+    for (int r = 1; r < R; ++r) {
+        const uint64_t target = (uint64_t)((W * (unsigned)r + (unsigned)R - 1) / (unsigned)R);
+        int k = (int)(std::lower_bound(pre.begin(), pre.end(), target) - pre.begin());
+        k = std::min(k, n);
+        for (int a = std::max(0, k - 3); a < k; ++a)
+            if (forest_.is_first_sibling(a) && a + 4 > k) {
+                k = (k - a <= a + 4 - k) ? a : a + 4;
+                break;
+            }
+        cut_[r] = std::min(n, std::max(k, cut_[r - 1]));
+    }
+    owner_.assign(n, 0);
+    for (int r = 0; r < R; ++r)
+        for (int p = cut_[r]; p < cut_[r + 1]; ++p) owner_[p] = r;
+    own_first_ = cut_[rank_];
+    own_count_ = cut_[rank_ + 1] - cut_[rank_];
+}
+
+std::vector<char> Context::local_set() const {
+    const int n = num_patches();
+    std::vector<char> loc(n, 0);
+    for (int p = own_first_; p < own_first_ + own_count_; ++p) {
+        loc[p] = 1;
+        const Neighbors& nb = nbrs_[p];
+        for (int f = 0; f < 4; ++f)
+            for (int k = 0; k < 2; ++k)
+                if (nb.face_nbr[f][k] >= 0) loc[nb.face_nbr[f][k]] = 1;
+        for (int c = 0; c < 4; ++c)
+            if (nb.corner_nbr[c] >= 0) loc[nb.corner_nbr[c]] = 1;
+    }
+    return loc;
 }
 
 void Context::ghost_update(int minlevel, int maxlevel, double, int time_interp) {
@@ -884,7 +1105,7 @@ void Context::ghost_update(int minlevel, int maxlevel, double, int time_interp) 
 
 void Context::physical_set_bc(int level, int time_interp) {
     std::vector<GhostOp> ops;
-    for (int p = 0; p < num_patches(); ++p) {
+    for (int p = own_first_; p < own_first_ + own_count_; ++p) {
         if (forest_.leaves[p].level != level) continue;
         GhostOp o{};
         o.type = OP_PHYSBC; o.dst = o.src = slot_of_[p]; o.dst_ti = o.src_ti = time_interp;
@@ -1021,6 +1242,7 @@ void Context::update_single_step_async(int level, double t, double dt) {
 double Context::single_step_update(int patchno, double t, double dt, int iter, int total) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "single_step_update before initialize");
     if (patchno < 0 || patchno >= num_patches()) throw Error(FCB_ERR_INVALID, "bad patch number");
+    if (!owned(patchno)) throw Error(FCB_ERR_INVALID, "patch not owned by this rank");
     if (iter == 0) pending_.clear();
     pending_.push_back(slot_of_[patchno]);
     if (iter + 1 < total) return 0.0;
@@ -1444,25 +1666,35 @@ cudaError_t launch_step_batch(const fcb_options_t& opt, int aux_kind, const Patc
 // ---------------------------------------------------------------------------
 // Regrid
 // ---------------------------------------------------------------------------
+// Partitioned solves tag their own leaves and gather every rank's values, so
+// that every rank adapts the whole forest identically.
 void Context::tag(bool domain_init, std::vector<int>& target) {
     const int n = num_patches();
-    const size_t need = (size_t)4 * n;
+    const size_t need = (size_t)4 * n + (partitioned() ? (size_t)4 * own_count_ : 0);
     if (need > scratch_cap_) {
-        cudaFree(d_scratch_);
+        if (d_scratch_) {
+            check(cudaStreamSynchronize(st_), "sync");
+            cudaFree(d_scratch_);
+        }
         check(cudaMalloc(&d_scratch_, need * sizeof(double)), "cudaMalloc scratch");
         scratch_cap_ = need;
     }
-    TagArgs a{};
-    a.q = d_q_; a.stride = stride_; a.slots = d_all_slots_.p; a.meta = d_meta_;
-    a.n = n; a.mx = opt_.mx; a.my = opt_.my; a.mbc = opt_.mbc; a.ivar = opt_.threshold_variable - 1;
-    a.criteria = opt_.refinement_criteria;
-    a.refine_th = opt_.refine_threshold; a.coarsen_th = opt_.coarsen_threshold;
-    a.out = d_scratch_;
-    check(launch_tag(a, st_), "tag");
-    ++cnt_.count_kernel_launches;
-    std::vector<double> h(need);
-    check(cudaMemcpyAsync(h.data(), d_scratch_, need * sizeof(double), cudaMemcpyDeviceToHost, st_), "tags");
-    synchronize();
+    double* own_out = partitioned() ? d_scratch_ + (size_t)4 * n : d_scratch_;
+    if (own_count_ > 0) {
+        TagArgs a{};
+        a.q = d_q_; a.stride = stride_; a.slots = d_all_slots_.p; a.meta = d_meta_;
+        a.n = own_count_; a.mx = opt_.mx; a.my = opt_.my; a.mbc = opt_.mbc; a.ivar = opt_.threshold_variable - 1;
+        a.criteria = opt_.refinement_criteria;
+        a.refine_th = opt_.refine_threshold; a.coarsen_th = opt_.coarsen_threshold;
+        a.out = own_out;
+        check(launch_tag(a, st_), "tag");
+        ++cnt_.count_kernel_launches;
+    }
+    if (partitioned()) allgather_owned(own_out, 4, d_scratch_);
+    std::vector<double> h((size_t)4 * n);
+    check(cudaMemcpyAsync(h.data(), d_scratch_, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st_), "tags");
+    if (partitioned()) comm_->sync(st_);
+    else synchronize();
     target.resize(n);
     for (int p = 0; p < n; ++p) target[p] = forest_.leaves[p].level;
     const bool minmax = opt_.refinement_criteria == FCB_TAG_MINMAX;
@@ -1600,8 +1832,8 @@ void Context::repopulate(const std::vector<Leaf>& old_leaves, const std::vector<
     int need = nslots_used_;
     for (auto& e : events) need += (std::get<0>(e) == 0) ? 4 : 1;
     ensure_capacity(need);
-    std::vector<int> saved_free = free_slots_;
-    free_slots_.clear();  // allocate only fresh slots in this pass
+    // new slots come from slots freed before this regrid or from the end of the
+    // arena, never from the slots this regrid frees (its transfer reads them)
     for (auto& e : events) {
         const int kind = std::get<0>(e), o = std::get<1>(e), w = std::get<2>(e);
         if (kind == 0) {
@@ -1642,8 +1874,197 @@ void Context::repopulate(const std::vector<Leaf>& old_leaves, const std::vector<
         ++cnt_.count_kernel_launches;
         synchronize();
     }
-    free_slots_ = saved_free;
     free_slots_.insert(free_slots_.end(), freed.begin(), freed.end());
+}
+
+// fclaw2d_domain_iterate_adapted + cb_fclaw2d_regrid_repopulate
+// (fclaw2d_regrid.c:114-230) followed by the patch transfer of
+// fclaw2d_partition_domain (fclaw2d_partition.c:113-197), with one exchange:
+// the owner of every new leaf receives the old patches its data comes from (the
+// leaf itself, its parent, or its four children, ghost cells included) from
+// their old owners, then runs the regrid transfer on its own slots.  Leaves of
+// the new ghost layer get slots and receive data at the next ghost update.
+void Context::repopulate_partitioned(const std::vector<Leaf>& old_leaves, const std::vector<int>& old_slots,
+                                     const std::vector<int>& old_owner, bool domain_init) {
+    const int nn = num_patches(), no = (int)old_leaves.size(), R = nranks_;
+    partition_leaves();
+    nbrs_.resize(nn);
+    for (int p = 0; p < nn; ++p) nbrs_[p] = forest_.neighbors(p);
+    const std::vector<char> loc = local_set();
+    // kind: 0 the same leaf, 1 a child of old leaf src, 2 the parent of old leaves src..src+3
+    std::vector<int> kind(nn, 0), src(nn, -1);
+    {
+        int oj = 0, nj = 0;
+        while (oj < no && nj < nn) {
+            const Leaf& o = old_leaves[oj];
+            const Leaf& w = forest_.leaves[nj];
+            if (o.level < w.level) {
+                for (int k = 0; k < 4; ++k) { kind[nj + k] = 1; src[nj + k] = oj; }
+                oj += 1; nj += 4;
+            } else if (o.level > w.level) {
+                kind[nj] = 2; src[nj] = oj;
+                oj += 4; nj += 1;
+            } else {
+                src[nj] = oj;
+                ++oj; ++nj;
+            }
+        }
+        if (nj != nn || oj != no) throw Error(FCB_ERR_INTERNAL, "iterate_adapted: leaf count mismatch");
+    }
+    // fresh leaves of the initial refinement are initialised, not transferred
+    auto fresh = [&](int w) { return domain_init && kind[w] != 0; };
+    std::vector<std::vector<int>> recv(R), send(R);
+    bool any = false;
+    for (int w = 0; w < nn; ++w) {
+        if (fresh(w)) continue;
+        const int ns = kind[w] == 2 ? 4 : 1;
+        for (int k = 0; k < ns; ++k) {
+            const int s = src[w] + k, os = old_owner[s], ow = owner_[w];
+            if (os == ow) continue;
+            any = true;
+            if (ow == rank_) recv[os].push_back(s);
+            else if (os == rank_) send[ow].push_back(s);
+        }
+    }
+    for (int r = 0; r < R; ++r)
+        for (auto* v : {&recv[r], &send[r]}) {
+            std::sort(v->begin(), v->end());
+            v->erase(std::unique(v->begin(), v->end()), v->end());
+        }
+    // slots: an upper bound of the new ones first (the arena may move)
+    int need = nslots_used_;
+    for (int r = 0; r < R; ++r) need += (int)recv[r].size();
+    for (int w = 0; w < nn; ++w) need += loc[w] ? 1 : 0;
+    for (int w = 0; w < nn; w += (kind[w] == 1 ? 4 : 1)) need += kind[w] == 1 ? 4 : 0;
+    ensure_capacity(need);
+    std::vector<int> ns(nn, -1), recv_slot(no, -1);
+    std::vector<char> adopted_old(no, 0);
+    std::vector<int32_t> temps;
+    // leaves that stay the same and stay local keep their slot
+    for (int w = 0; w < nn; ++w)
+        if (kind[w] == 0 && loc[w] && old_slots[src[w]] >= 0) {
+            ns[w] = old_slots[src[w]];
+            adopted_old[src[w]] = 1;
+        }
+    // received patches land in their old ghost-layer slot, or a new slot
+    for (int r = 0; r < R; ++r)
+        for (int s : recv[r]) {
+            if (old_slots[s] >= 0) {
+                recv_slot[s] = old_slots[s];
+            } else {
+                recv_slot[s] = alloc_slot();
+                temps.push_back(recv_slot[s]);
+            }
+        }
+    for (int w = 0; w < nn; ++w) {
+        if (!loc[w] || ns[w] >= 0) continue;
+        if (kind[w] == 0 && owner_[w] == rank_) {  // moved here from another rank
+            ns[w] = recv_slot[src[w]];
+        } else {
+            ns[w] = alloc_slot();
+        }
+    }
+    // regrid transfer records on this rank: refined families with an owned child
+    // (all four children are written), coarsened parents owned here
+    auto src_slot = [&](int s) { return old_owner[s] == rank_ ? old_slots[s] : recv_slot[s]; };
+    std::vector<int32_t> transfer, fine, fresh_slots;
+    for (int w = 0; w < nn;) {
+        if (kind[w] == 1) {
+            bool mine = false;
+            for (int k = 0; k < 4; ++k) mine = mine || owner_[w + k] == rank_;
+            if (mine && !domain_init) {
+                const int f0 = (int)fine.size();
+                for (int k = 0; k < 4; ++k) {
+                    int sl = ns[w + k];
+                    if (sl < 0) {
+                        sl = alloc_slot();
+                        temps.push_back(sl);
+                    }
+                    fine.push_back(sl);
+                }
+                transfer.insert(transfer.end(), {0, src_slot(src[w]), f0});
+            }
+            for (int k = 0; k < 4; ++k)
+                if (fresh(w + k) && owner_[w + k] == rank_) fresh_slots.push_back(ns[w + k]);
+            w += 4;
+            continue;
+        }
+        if (kind[w] == 2 && owner_[w] == rank_) {
+            if (domain_init) {
+                fresh_slots.push_back(ns[w]);
+            } else {
+                const int f0 = (int)fine.size();
+                for (int k = 0; k < 4; ++k) fine.push_back(src_slot(src[w] + k));
+                transfer.insert(transfer.end(), {1, ns[w], f0});
+            }
+        }
+        ++w;
+    }
+    for (int w = 0; w < nn; ++w)
+        if (owner_[w] == rank_ && ns[w] < 0) throw Error(FCB_ERR_INTERNAL, "owned leaf without a slot");
+    for (size_t k = 0; k < transfer.size(); k += 3)
+        if (transfer[k + 1] < 0 || transfer[k + 1] >= capacity_) throw Error(FCB_ERR_INTERNAL, "transfer slot");
+    for (int32_t sl : fine)
+        if (sl < 0 || sl >= capacity_) throw Error(FCB_ERR_INTERNAL, "transfer slot");
+    for (int r = 0; r < R; ++r) {
+        for (int s : send[r])
+            if (old_slots[s] < 0 || old_slots[s] >= capacity_) throw Error(FCB_ERR_INTERNAL, "sent patch without a slot");
+        for (int s : recv[r])
+            if (recv_slot[s] < 0 || recv_slot[s] >= capacity_) throw Error(FCB_ERR_INTERNAL, "received patch slot");
+    }
+    // the exchange: old owners' patches (whole arrays) to the new owners
+    if (any) {
+        XList x;
+        x.any = true;
+        x.send_n.assign(R, 0);
+        x.recv_n.assign(R, 0);
+        for (int r = 0; r < R; ++r) {
+            for (int s : send[r]) x.send.push_back(old_slots[s] * 2);
+            for (int s : recv[r]) x.recv.push_back(recv_slot[s] * 2);
+            x.send_n[r] = (int)send[r].size();
+            x.recv_n[r] = (int)recv[r].size();
+        }
+        std::vector<int32_t> items(x.send);
+        items.insert(items.end(), x.recv.begin(), x.recv.end());
+        x.send_first = 0;
+        x.recv_first = x.send.size();
+        DevBuf<int32_t> d;
+        d.reserve(std::max<size_t>(1, items.size()));
+        if (!items.empty())
+            check(cudaMemcpy(d.p, items.data(), items.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "items");
+        exchange(x, d.p);
+        comm_->sync(st_);
+    }
+    if (!transfer.empty()) {
+        DevBuf<int32_t> dt, df;
+        dt.reserve(transfer.size());
+        df.reserve(fine.size());
+        check(cudaMemcpy(dt.p, transfer.data(), transfer.size() * 4, cudaMemcpyHostToDevice), "transfer");
+        check(cudaMemcpy(df.p, fine.data(), fine.size() * 4, cudaMemcpyHostToDevice), "fine");
+        check(launch_regrid(d_q_, stride_, dt.p, df.p, (int)transfer.size() / 3, opt_.mx, opt_.my, opt_.mbc,
+                            opt_.meqn, st_),
+              "regrid transfer");
+        ++cnt_.count_kernel_launches;
+        synchronize();
+    }
+    // slots no longer referenced return to the free list
+    std::vector<char> live((size_t)capacity_, 0);
+    for (int w = 0; w < nn; ++w)
+        if (ns[w] >= 0) live[ns[w]] = 1;
+    std::vector<char> seen((size_t)capacity_, 0);
+    auto release = [&](int sl) {
+        if (sl >= 0 && !live[sl] && !seen[sl]) {
+            seen[sl] = 1;
+            free_slots_.push_back(sl);
+        }
+    };
+    for (int s = 0; s < no; ++s) release(old_slots[s]);
+    for (int32_t sl : temps) release(sl);
+    slot_of_ = ns;
+    if (!fresh_slots.empty()) {
+        mesh_changed();
+        qinit_slots(fresh_slots);
+    }
 }
 
 bool Context::regrid() {
@@ -1655,8 +2076,10 @@ bool Context::regrid() {
     if (changed) {
         const std::vector<Leaf> old = forest_.leaves;
         const std::vector<int> old_slots = slot_of_;
+        const std::vector<int> old_owner = owner_;
         forest_.leaves = nl;
-        repopulate(old, old_slots, false);
+        if (partitioned()) repopulate_partitioned(old, old_slots, old_owner, false);
+        else repopulate(old, old_slots, false);
         mesh_changed();
         // this update's plan and the next macro step's, built together, for a
         // context that advances through fcb_advance_all_levels (a served solve
@@ -1675,11 +2098,24 @@ void Context::initialize() {
     const int n = num_patches();
     free_slots_.clear();
     nslots_used_ = 0;
-    ensure_capacity(n);
-    slot_of_.resize(n);
-    for (int p = 0; p < n; ++p) slot_of_[p] = alloc_slot();
+    if (partitioned()) {
+        // fclaw2d_domain_new_unitsquare + the first partition: this rank's Morton
+        // range and its ghost layer get slots
+        partition_leaves();
+        nbrs_.resize(n);
+        for (int p = 0; p < n; ++p) nbrs_[p] = forest_.neighbors(p);
+        const std::vector<char> loc = local_set();
+        ensure_capacity(std::max(1, (int)std::count(loc.begin(), loc.end(), 1)));
+        slot_of_.assign(n, -1);
+        for (int p = 0; p < n; ++p)
+            if (loc[p]) slot_of_[p] = alloc_slot();
+    } else {
+        ensure_capacity(n);
+        slot_of_.resize(n);
+        for (int p = 0; p < n; ++p) slot_of_[p] = alloc_slot();
+    }
     mesh_changed();
-    qinit_slots(std::vector<int32_t>(slot_of_.begin(), slot_of_.end()));
+    qinit_slots(std::vector<int32_t>(slot_of_.begin() + own_first_, slot_of_.begin() + own_first_ + own_count_));
     initialized_ = true;
     if (opt_.init_ghostcell) ghost_update(forest_.min_level(), forest_.max_level(), 0.0, 0);
     if (opt_.minlevel < opt_.maxlevel) {
@@ -1690,8 +2126,10 @@ void Context::initialize() {
             if (!adapt(target, nl)) break;
             const std::vector<Leaf> old = forest_.leaves;
             const std::vector<int> old_slots = slot_of_;
+            const std::vector<int> old_owner = owner_;
             forest_.leaves = nl;
-            repopulate(old, old_slots, true);
+            if (partitioned()) repopulate_partitioned(old, old_slots, old_owner, true);
+            else repopulate(old, old_slots, true);
             mesh_changed();
         }
     }
@@ -1729,7 +2167,8 @@ void Context::run() {
                     if (small_step < 0) took_small_step = 1;
                 }
             }
-            const double maxcfl_step = advance_all_levels(t_curr, dt_step);
+            // fclaw2d_run.c:206: the CFL maximum over all ranks
+            const double maxcfl_step = global_maximum(advance_all_levels(t_curr, dt_step));
             if (std::isnan(maxcfl_step)) throw Error(FCB_ERR_NUMERIC, "NaN in the CFL number");
             if ((maxcfl_step > opt_.max_cfl) && opt_.reduce_cfl) {
                 if (!opt_.use_fixed_dt) {
@@ -1755,25 +2194,31 @@ void Context::run() {
 // ---------------------------------------------------------------------------
 // Data movement and diagnostics
 // ---------------------------------------------------------------------------
+// The owned patches (all patches on one rank) at their places in the
+// all-leaves layout; the other entries of the host buffer are not touched.
 void Context::get_q(double* host, size_t n, bool qinterp) {
     const size_t ps = patch_size();
     const size_t total = ps * num_patches();
     if (n < total) throw Error(FCB_ERR_INVALID, "host buffer too small");
-    if (total > stage_cap_) {
+    const size_t mine = ps * own_count_;
+    if (mine == 0) return;
+    if (mine > stage_cap_) {
         cudaFree(d_stage_);
-        check(cudaMalloc(&d_stage_, total * sizeof(double)), "cudaMalloc stage");
-        stage_cap_ = total;
+        check(cudaMalloc(&d_stage_, mine * sizeof(double)), "cudaMalloc stage");
+        stage_cap_ = mine;
     }
-    check(launch_gather(qinterp ? d_qti_ : d_q_, stride_, d_all_slots_.p, num_patches(), (int64_t)ps, d_stage_,
+    check(launch_gather(qinterp ? d_qti_ : d_q_, stride_, d_all_slots_.p, own_count_, (int64_t)ps, d_stage_,
                         false, opt_.claw_version == 5 ? opt_.meqn : 0, st_),
           "gather");
     ++cnt_.count_kernel_launches;
-    check(cudaMemcpyAsync(host, d_stage_, total * sizeof(double), cudaMemcpyDeviceToHost, st_), "get_q");
+    check(cudaMemcpyAsync(host + ps * own_first_, d_stage_, mine * sizeof(double), cudaMemcpyDeviceToHost, st_),
+          "get_q");
     synchronize();
 }
 
 void Context::output_ascii(int iframe, const std::string& dir) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "output before initialize");
+    if (partitioned()) throw Error(FCB_ERR_INVALID, "ASCII output of a partitioned solve is not available");
     if (iframe < 0 || iframe > 9999) throw Error(FCB_ERR_INVALID, "frame number must be in 0..9999");
     const size_t ps = patch_size();
     const int n = num_patches();
@@ -1805,33 +2250,47 @@ void Context::set_q(const double* host, size_t n) {
     const size_t ps = patch_size();
     const size_t total = ps * num_patches();
     if (n < total) throw Error(FCB_ERR_INVALID, "host buffer too small");
-    if (total > stage_cap_) {
+    const size_t mine = ps * own_count_;
+    if (mine == 0) return;
+    if (mine > stage_cap_) {
         cudaFree(d_stage_);
-        check(cudaMalloc(&d_stage_, total * sizeof(double)), "cudaMalloc stage");
-        stage_cap_ = total;
+        check(cudaMalloc(&d_stage_, mine * sizeof(double)), "cudaMalloc stage");
+        stage_cap_ = mine;
     }
-    check(cudaMemcpyAsync(d_stage_, host, total * sizeof(double), cudaMemcpyHostToDevice, st_), "set_q");
-    check(launch_gather(d_q_, stride_, d_all_slots_.p, num_patches(), (int64_t)ps, d_stage_, true,
+    check(cudaMemcpyAsync(d_stage_, host + ps * own_first_, mine * sizeof(double), cudaMemcpyHostToDevice, st_),
+          "set_q");
+    check(launch_gather(d_q_, stride_, d_all_slots_.p, own_count_, (int64_t)ps, d_stage_, true,
                         opt_.claw_version == 5 ? opt_.meqn : 0, st_),
           "scatter");
     ++cnt_.count_kernel_launches;
     synchronize();
 }
 
+// Per-patch sums on the owning ranks, gathered, then the same compensated sum
+// over all patches in Morton order on every rank (identical to one rank).
 void Context::conservation(double* sums) {
     const int n = num_patches();
-    const size_t need = (size_t)n * opt_.meqn;
+    const size_t need = (size_t)n * opt_.meqn + (partitioned() ? (size_t)own_count_ * opt_.meqn : 0);
     if (need > scratch_cap_) {
-        cudaFree(d_scratch_);
+        if (d_scratch_) {
+            check(cudaStreamSynchronize(st_), "sync");
+            cudaFree(d_scratch_);
+        }
         check(cudaMalloc(&d_scratch_, need * sizeof(double)), "cudaMalloc scratch");
         scratch_cap_ = need;
     }
-    check(launch_mass(d_q_, stride_, d_all_slots_.p, d_meta_, n, opt_.mx, opt_.my, opt_.mbc, opt_.meqn, d_scratch_, st_),
-          "mass");
-    ++cnt_.count_kernel_launches;
-    std::vector<double> h(need);
-    check(cudaMemcpyAsync(h.data(), d_scratch_, need * sizeof(double), cudaMemcpyDeviceToHost, st_), "mass");
-    synchronize();
+    double* own_out = partitioned() ? d_scratch_ + (size_t)n * opt_.meqn : d_scratch_;
+    if (own_count_ > 0) {
+        check(launch_mass(d_q_, stride_, d_all_slots_.p, d_meta_, own_count_, opt_.mx, opt_.my, opt_.mbc, opt_.meqn,
+                          own_out, st_),
+              "mass");
+        ++cnt_.count_kernel_launches;
+    }
+    if (partitioned()) allgather_owned(own_out, opt_.meqn, d_scratch_);
+    std::vector<double> h((size_t)n * opt_.meqn);
+    check(cudaMemcpyAsync(h.data(), d_scratch_, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st_), "mass");
+    if (partitioned()) comm_->sync(st_);
+    else synchronize();
     for (int m = 0; m < opt_.meqn; ++m) {
         double s = 0.0, c = 0.0;
         for (int p = 0; p < n; ++p) {

@@ -11,8 +11,10 @@
 #include <vector>
 #include <thread>
 #include <exception>
+#include <memory>
 
 #include "../../include/fclaw_b200.h"
+#include "fcb_comm.hpp"
 #include "fcb_device.h"
 #include "fcb_forest.hpp"
 
@@ -73,16 +75,35 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+// One exchange of whole patch arrays between the ranks of a partitioned solve
+// (the ghost-patch exchange of fclaw2d_exchange.c): items slot * 2 + array
+// (0 q, 1 the time-interpolated q), grouped by peer rank in rank order, in
+// increasing leaf order within a peer on both sides.
+struct XList {
+    std::vector<int32_t> send, recv;
+    std::vector<int> send_n, recv_n;        // items per peer rank
+    size_t send_first = 0, recv_first = 0;  // offsets in the context's device item buffer
+    bool any = false;                       // some rank sends something (the same on every rank)
+};
+
 struct GhostPlan {
     std::vector<int> wave_begin;   // op offsets of each wave, size nwaves+1
     size_t first = 0;              // first op of the plan in the context's op buffer
     std::vector<int> group_begin;  // per wave: first group, size nwaves+1
     size_t first_group = 0;        // first group of the plan in the context's group buffer
+    // partitioned solves: waves [0, nA) are the averages, copies and coarse
+    // physical boundaries, which read only the interiors of their sources (x1
+    // brings those of other ranks' patches first); x2 then brings the other
+    // ranks' coarse patches, ghost cells included, that the interpolations read
+    int nA = 0;
+    XList x1, x2;
 };
 
 class Context {
   public:
-    Context(const fcb_options_t& o, cudaStream_t st);
+    // comm: null for a solve on one rank; otherwise this context is rank
+    // comm->rank() of a partitioned solve (leaves in contiguous Morton ranges)
+    Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> comm = nullptr);
     ~Context();
 
     void initialize();
@@ -125,6 +146,16 @@ class Context {
     // ghost-fill unroll used by the last launches
     int step_form_used() const { return step_form_used_; }
     int ghost_unroll_used() const { return ghost_unroll_; }
+    // --- partitioned solves (fclaw2d_partition.c, fclaw2d_exchange.c) ---
+    bool partitioned() const { return comm_ != nullptr; }
+    int rank() const { return rank_; }
+    int nranks() const { return nranks_; }
+    int own_first() const { return own_first_; }
+    int own_count() const { return own_count_; }
+    // fclaw2d_domain_global_maximum (forestclaw2d.c:51)
+    double global_maximum(double v);
+    // marks the communicator failed, so that the other ranks stop at their next collective
+    void abort_comm(const std::string& why) noexcept;
 
   private:
     // --- setup ---
@@ -135,15 +166,20 @@ class Context {
     PatchMeta meta_of(const Leaf& l) const;
     // --- ghost plans ---
     const GhostPlan& plan(int minlevel, int maxlevel, int time_interp);
-    void build_ops(int minlevel, int maxlevel, int time_interp, std::vector<GhostOp>& ops) const;
+    // records in the reference's order with LEAF indices in dst / src; *phase_b:
+    // index of the first interpolation record
+    void build_ops(int minlevel, int maxlevel, int time_interp, std::vector<GhostOp>& ops, size_t* phase_b) const;
     // A ghost plan before it is appended to the context's op buffer: records in
     // wave order, wave offsets, and the group starts of each wave (relative).
     struct PlanBuild {
         std::vector<GhostOp> ops;
         std::vector<int> wave_begin, group_begin;
         std::vector<int32_t> groups;
+        int nA = 0;
+        XList x1, x2;
     };
     PlanBuild build_plan(int minlevel, int maxlevel, int time_interp) const;
+    PlanBuild make_waves(const std::vector<GhostOp>& ops) const;
     const GhostPlan& commit_plan(const std::tuple<int, int, int>& key, PlanBuild&& b);
     // Missing plans of a macro step are built on host threads while its first
     // level updates run on the GPU; plan() waits for them.  Every build ends
@@ -199,6 +235,24 @@ class Context {
     void repopulate(const std::vector<Leaf>& old_leaves, const std::vector<int>& old_slots,
                     bool domain_init);
     void qinit_slots(const std::vector<int32_t>& slots);
+    // --- partitioned solves ---
+    void partition_leaves();             // cut_, owner_, own range for forest_ (weighted Morton ranges)
+    std::vector<char> local_set() const;  // per leaf: owned, or a face/corner neighbour of an owned leaf
+    void exchange(const XList& x, const int32_t* d_items = nullptr);  // items: the plan item buffer
+    // every rank receives the owned ranges of all ranks: d_own holds this rank's
+    // own_count_ * per_leaf doubles, d_all receives num_patches() * per_leaf
+    void allgather_owned(const double* d_own, int per_leaf, double* d_all);
+    void repopulate_partitioned(const std::vector<Leaf>& old_leaves, const std::vector<int>& old_slots,
+                                const std::vector<int>& old_owner, bool domain_init);
+    bool owned(int p) const { return owner_.empty() || owner_[p] == rank_; }
+    std::shared_ptr<Comm> comm_;
+    int rank_ = 0, nranks_ = 1;
+    std::vector<int> owner_;  // per leaf (partitioned solves)
+    std::vector<int> cut_;    // rank r owns leaves [cut_[r], cut_[r+1])
+    int own_first_ = 0, own_count_ = 0;
+    std::vector<int32_t> h_xitems_;
+    DevBuf<int32_t> d_xitems_;
+    DevBuf<double> d_xsend_, d_xrecv_;
     double launch_level_step(int level, double t, double dt, unsigned long long* cfl_slot);
     // --- macro step ---
     void run_schedule(double t, double dt);  // the level schedule of one advance_all_levels

@@ -34,7 +34,9 @@ enum fcb_status {
     FCB_ERR_CUDA = 2,        /* a CUDA call failed */
     FCB_ERR_STATE = 3,       /* call out of order (e.g. step before initialize) */
     FCB_ERR_NUMERIC = 4,     /* NaN/Inf in the CFL number */
-    FCB_ERR_INTERNAL = 5
+    FCB_ERR_INTERNAL = 5,
+    FCB_ERR_COMM = 6         /* partitioned solve: a rank failed, sizes disagreed, or a
+                              * collective outlasted the communicator's time limit */
 };
 
 /* Riemann solver families (fc2d_clawpack46_vtable_t rpn2/rpt2 pairs). */
@@ -132,6 +134,10 @@ typedef struct fcb_options {
     /* [Options] ax, bx, ay, by: physical extent of the block; all four zero
      * means the unit square */
     double ax, bx, ay, by;
+    /* [Options] weighted-partition: with subcycling, a partitioned solve
+     * weighs a leaf of level l by 2^l (its updates per macro step) when it cuts
+     * the Morton order into ranges (fclaw2d_partition.c:142) */
+    int weighted_partition;
 } fcb_options_t;
 
 typedef struct fcb_counters {
@@ -249,6 +255,50 @@ int fcb_autotune_info(fcb_context_t* ctx, int* step_form, int* ghost_unroll);
 int fcb_measure_fp_rate(int fp64, void* cuda_stream, double* ops_per_second);
 /* Wait for all work of the context. */
 int fcb_synchronize(fcb_context_t* ctx);
+
+/* ---- partitioned solves ------------------------------------------------------
+ * Replaces the MPI layer under fclaw2d_domain_new_unitsquare(mpicomm, ...):
+ * every rank holds the whole forest (leaf metadata only) and the patch arrays
+ * of its Morton range of leaves (p4est_partition with weights 2^level when
+ * weighted_partition and subcycle are set, complete families never split)
+ * plus a ghost layer of the face and corner neighbours of those leaves.
+ * Ghost updates exchange the ghost layer (fclaw2d_exchange.c:308-413) in two
+ * steps: the sources' interiors before the averages and copies, and after
+ * them the coarse patches (ghost cells included) that the interpolations read.
+ * Refinement tags are gathered so every rank adapts the forest identically;
+ * after a regrid the leaves are repartitioned and the patch data moves to its
+ * new owners with the regrid transfer (fclaw2d_partition.c:113-197).  The
+ * state of every owned patch is bit-identical to a one-rank solve.
+ *
+ * Collective calls (all ranks, same order): fcb_initialize, fcb_run,
+ * fcb_advance_all_levels, fcb_ghost_update, fcb_regrid,
+ * fcb_conservation_check, fcb_global_maximum.  fcb_advance_all_levels returns
+ * this rank's CFL maximum, as fclaw2d_advance_all_levels does; fcb_run takes
+ * the global maximum itself (fclaw2d_run.c:206).  fcb_get_q / fcb_set_q /
+ * fcb_get_qinterp move only the owned patches, at their places in the
+ * all-leaves layout.  The macro-step graph is not used; fcb_output_ascii and
+ * time-sync are rejected.  A failed rank marks the communicator failed, and
+ * the others' next collective returns FCB_ERR_COMM. */
+typedef struct fcb_comm fcb_comm_t;
+/* nranks communicators of one in-process group: each rank's context is driven
+ * by its own host thread; every rendezvous waits at most timeout_s seconds */
+int fcb_comm_create_local(int nranks, double timeout_s, fcb_comm_t** comms);
+/* NCCL (nccl_library: path of libnccl.so.2, NULL for the default search):
+ * the 128-byte unique id made on one rank and sent to the others by the
+ * caller, and one rank's communicator (one process per GPU, the device current
+ * at the call); every wait is bounded by timeout_s, then the communicator is aborted */
+int fcb_comm_nccl_unique_id(const char* nccl_library, unsigned char id[128]);
+int fcb_comm_create_nccl(const char* nccl_library, const unsigned char id[128], int rank, int nranks,
+                         double timeout_s, fcb_comm_t** out);
+int fcb_comm_destroy(fcb_comm_t* comm);
+/* a context that is rank comm.rank of a partitioned solve (the context keeps
+ * its own reference to the communicator) */
+int fcb_context_create_partitioned(const fcb_options_t* opt, void* cuda_stream, fcb_comm_t* comm,
+                                   fcb_context_t** out);
+/* this rank, the number of ranks, and the owned leaves [first, first + count) */
+int fcb_partition_info(fcb_context_t* ctx, int* rank, int* nranks, int* first, int* count);
+/* fclaw2d_domain_global_maximum: the maximum of value over the ranks */
+int fcb_global_maximum(fcb_context_t* ctx, double value, double* out);
 
 /* ---- ensemble serving -----------------------------------------------------
  * No counterpart in the reference (ForestClaw runs one solve per process): a
