@@ -15,6 +15,9 @@ steps.
 Prints ONE JSON line.  With torchrun (N > 1) each rank advances its own
 replica (independent solves, weak scaling, no data-path collective); the time
 is the max over ranks and the value the cell updates of all ranks over it.
+With --partition the ranks share one solve instead (Morton ranges of leaves,
+ghost layers exchanged through NCCL, the CFL maximum reduced every step):
+strong scaling.
 
 --impl reference times the CPU restatement of the reference's Fortran/C
 (oracle/, compiled -O3 -march=native with OpenMP over the patches of a level)
@@ -58,6 +61,9 @@ def parse():
     p.add_argument("--macro-graph", type=int, default=2, choices=[0, 1, 2],
                    help="1: replay each macro step from a captured CUDA graph; 0: host launches; 2: automatic")
     p.add_argument("--step-variant", type=int, default=0, help="0 library's choice, 1 CTA rows, 2 warp, 3 pipelined CTA")
+    p.add_argument("--partition", action="store_true",
+                   help="uniform workload: one solve partitioned over the ranks (NCCL ghost exchange, "
+                        "strong scaling) instead of one replica per rank")
     return p.parse_args()
 
 
@@ -342,6 +348,95 @@ def run_ours(args, rank, world, local_rank):
         line["cpu_baseline"] = cpu_sample(args, args.cpu_seconds)
     s.close()
     return line
+
+
+def run_partitioned(args, rank, world, local_rank):
+    """One uniform swirl solve split over the ranks (Morton ranges, NCCL
+    ghost-layer exchange, global CFL maximum every step): strong scaling."""
+    import torch
+
+    import forestclaw_b200 as fcb
+    from forestclaw_b200 import replicas, workloads
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.current_stream()
+    uid = [fcb.nccl_unique_id() if rank == 0 else None]
+    if world > 1:
+        torch.distributed.broadcast_object_list(uid, src=0)
+    comm = fcb.nccl_comm(uid[0], rank, world, timeout_s=120.0)
+    opts = workloads.uniform_swirl(args.level, args.mx)
+    opts.step_variant = args.step_variant
+    opts.precision = fcb.PRECISION_MIXED if args.precision == "mixed" else fcb.PRECISION_FP64
+    dt = workloads.swirl_dt(args.level, args.mx)
+    s = fcb.Solver(opts, stream=stream.cuda_stream, comm=comm)
+    s.initialize()
+    info = s.partition_info()
+    t = 0.0
+
+    def step(t):
+        return s.global_maximum(s.advance_all_levels(t, dt))
+
+    for _ in range(args.warmup):
+        step(t)
+        t += dt
+    torch.cuda.synchronize()
+    c0 = s.counters()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(t)
+            t += dt
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+    c1 = s.counters()
+    cells = (c1["count_single_step"] - c0["count_single_step"]) * args.mx * args.mx
+    launches = c1["count_kernel_launches"] - c0["count_kernel_launches"]
+    d = torch.distributed if world > 1 else None
+    ms_max, total_cells = replicas.aggregate(e0.elapsed_time(e1), cells, d)
+    # end to end: this rank's patches from pinned host memory, K steps, back to the host
+    psize = opts.meqn * opts.nx * opts.ny
+    npatch = s.num_patches
+    host = torch.empty(npatch * psize, dtype=torch.float64, pin_memory=True)
+    hv = host.numpy().reshape(npatch, opts.meqn, opts.ny, opts.nx)
+    s.get_q(out=hv)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    s.set_q(hv)
+    for _ in range(args.steps):
+        step(t)
+        t += dt
+    s.get_q(out=hv)
+    x1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms, _ = replicas.aggregate(x0.elapsed_time(x1), 0, d)
+    own_bytes = info["count"] * psize * 8
+    s.close()
+    comm.close()
+    if rank != 0:
+        return None
+    return {
+        "metric": "cell-updates/s", "value": total_cells / (ms_max * 1e-3), "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
+        "config": {"workload": f"uniform swirl advection, level {args.level}, mx=my={args.mx}, one solve "
+                               f"partitioned over {world} rank(s)",
+                   "patches": npatch, "l2_flush": "inputs larger than L2",
+                   "parallelism": f"partitioned, {world} rank(s), NCCL ghost-layer exchange"},
+        "clocks": clk.summary(),
+        "e2e": {"value": total_cells / (e2e_ms * 1e-3), "unit": "cell-updates/s",
+                "h2d_bytes_per_step": own_bytes / args.steps + 16, "d2h_bytes_per_step": own_bytes / args.steps + 8},
+        "gpu_launches": launches,
+    }
 
 
 def _mixed_accuracy(args, opts, dt, stream, steps=20):
@@ -748,7 +843,7 @@ def main():
     try:
         sys.path.insert(0, str(ROOT / "tests"))
         run = {"amr_radialdam": run_amr, "amr_quadrants": run_amr, "bathy": run_bathy,
-               "serve": run_serve}.get(args.workload, run_ours)
+               "serve": run_serve}.get(args.workload, run_partitioned if args.partition else run_ours)
         line = run(args, rank, world, local_rank)
         if line:
             print(json.dumps(line), flush=True)

@@ -19,7 +19,8 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-__all__ = ["Options", "Solver", "Comm", "local_group", "nccl_unique_id", "nccl_comm", "lib", "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
+__all__ = ["Options", "Solver", "Comm", "local_group", "nccl_unique_id", "nccl_comm", "partition_plan", "lib",
+           "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
            "SOLVER_EULER4_ROE", "SOLVER_GEOCLAW_FWAVE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM",
            "PROBLEM_QUADRANTS", "PROBLEM_BATHY", "PROBLEM_RADIALDAM_CELLAVE",
            "PRECISION_FP64", "PRECISION_MIXED", "measure_fp_rate",
@@ -44,7 +45,7 @@ EXPORTED_SYMBOLS = (
     "fcb_server_get_q", "fcb_server_release", "fcb_server_clock", "fcb_autotune_info",
     "fcb_measure_fp_rate", "fcb_output_ascii", "fcb_comm_create_local", "fcb_comm_nccl_unique_id",
     "fcb_comm_create_nccl", "fcb_comm_destroy", "fcb_context_create_partitioned", "fcb_partition_info",
-    "fcb_global_maximum",
+    "fcb_global_maximum", "fcb_partition_plan",
 )
 
 
@@ -244,6 +245,8 @@ def lib():
     L.fcb_context_create_partitioned.argtypes = [ctypes.POINTER(_Options), vp, vp, ctypes.POINTER(vp)]
     L.fcb_partition_info.argtypes = [vp, ip, ip, ip, ip]
     L.fcb_global_maximum.argtypes = [vp, ctypes.c_double, dp]
+    L.fcb_partition_plan.argtypes = [ctypes.POINTER(_Options), ctypes.c_int, ctypes.c_int, ctypes.c_int, ip, ip, ip,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ip, ip, ip, ip, ip, ip, ip]
     _lib = L
     return L
 
@@ -322,6 +325,26 @@ def nccl_comm(unique_id: bytes, rank: int, nranks: int, timeout_s: float = 120.0
     lp = (library if library is not None else nccl_library()).encode()
     _check(lib().fcb_comm_create_nccl(lp, unique_id, int(rank), int(nranks), float(timeout_s), ctypes.byref(h)))
     return Comm(h, rank, nranks)
+
+
+def partition_plan(options: Options, leaves, rank: int, nranks: int, minlevel: int, maxlevel: int,
+                   time_interp: int = 0) -> dict:
+    """Host-only planning query (no GPU needed): how a partitioned solve over
+    `leaves` ((level, x, y) in Morton order) splits them, and the patches each
+    exchange of ghost update (minlevel, maxlevel, time_interp) sends to and
+    receives from every peer rank."""
+    n = len(leaves)
+    lv = (ctypes.c_int * n)(*[int(l[0]) for l in leaves])
+    xs = (ctypes.c_int * n)(*[int(l[1]) for l in leaves])
+    ys = (ctypes.c_int * n)(*[int(l[2]) for l in leaves])
+    first, count, ghosts = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    arrs = [(ctypes.c_int * nranks)() for _ in range(4)]
+    copt = options.to_c()
+    _check(lib().fcb_partition_plan(ctypes.byref(copt), int(nranks), int(rank), n, lv, xs, ys, int(minlevel),
+                                    int(maxlevel), int(time_interp), ctypes.byref(first), ctypes.byref(count),
+                                    ctypes.byref(ghosts), *arrs))
+    return {"first": first.value, "count": count.value, "ghosts": ghosts.value,
+            "x1_send": list(arrs[0]), "x1_recv": list(arrs[1]), "x2_send": list(arrs[2]), "x2_recv": list(arrs[3])}
 
 
 class Solver:

@@ -290,6 +290,41 @@ int fcb_partition_info(fcb_context_t* ctx, int* rank, int* nranks, int* first, i
     });
 }
 
+int fcb_partition_plan(const fcb_options_t* opt, int nranks, int rank, int nleaves, const int* level, const int* x,
+                       const int* y, int minlevel, int maxlevel, int time_interp, int* first, int* count,
+                       int* ghosts, int* x1_send, int* x1_recv, int* x2_send, int* x2_recv) {
+    return guard([&] {
+        need(opt, "opt");
+        for (const void* p : {(const void*)level, (const void*)x, (const void*)y, (const void*)first,
+                              (const void*)count, (const void*)ghosts, (const void*)x1_send, (const void*)x1_recv,
+                              (const void*)x2_send, (const void*)x2_recv})
+            need(p, "array");
+        if (nleaves < 1) throw fcb::Error(FCB_ERR_INVALID, "no leaves");
+        std::vector<fcb::Leaf> leaves;
+        leaves.reserve(nleaves);
+        for (int k = 0; k < nleaves; ++k) {
+            if (level[k] < 0 || level[k] > 20) throw fcb::Error(FCB_ERR_INVALID, "leaf level out of range");
+            const int32_t w = fcb::QuadForest::width(level[k]);
+            if (x[k] < 0 || y[k] < 0 || x[k] % w || y[k] % w || x[k] >= fcb::QuadForest::kRoot ||
+                y[k] >= fcb::QuadForest::kRoot)
+                throw fcb::Error(FCB_ERR_INVALID, "leaf corner not on its level's grid");
+            leaves.push_back(fcb::QuadForest::make(level[k], x[k], y[k]));
+            if (k && !(leaves[k - 1].key < leaves[k].key)) throw fcb::Error(FCB_ERR_INVALID, "leaves not in Morton order");
+        }
+        const fcb::PartitionPlan pp =
+            fcb::Context::partition_plan(*opt, leaves, rank, nranks, minlevel, maxlevel, time_interp);
+        *first = pp.first;
+        *count = pp.count;
+        *ghosts = pp.ghosts;
+        for (int r = 0; r < nranks; ++r) {
+            x1_send[r] = pp.x1_send[r];
+            x1_recv[r] = pp.x1_recv[r];
+            x2_send[r] = pp.x2_send[r];
+            x2_recv[r] = pp.x2_recv[r];
+        }
+    });
+}
+
 int fcb_global_maximum(fcb_context_t* ctx, double value, double* out) {
     return collective(ctx, [&] {
         CTX();

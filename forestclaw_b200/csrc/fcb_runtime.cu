@@ -159,8 +159,67 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
     stride_ = (ps + 31) / 32 * 32;  // 256-byte aligned slots
     aux_stride_ = aux_kind_ == AUX_STORED ? ((int64_t)opt_.maux * nx_ * ny_ + 31) / 32 * 32 : 0;
     treg_stride_ = time_sync_ ? ((int64_t)RegLayout{opt_.mx, opt_.my, opt_.meqn}.size() + 31) / 32 * 32 : 0;
+}
+
+// The CFL words (first device use of a context: creation itself touches no device).
+void Context::ensure_scalars() {
+    if (d_cfl_) return;
     check(cudaMalloc(&d_cfl_, 4 * sizeof(unsigned long long)), "cudaMalloc cfl");
     check(cudaHostAlloc(&h_cfl_, sizeof(unsigned long long), cudaHostAllocDefault), "cudaHostAlloc cfl");
+}
+
+namespace {
+// rank and size only: the host-only planning query makes no collective call
+class PlanOnlyComm final : public Comm {
+  public:
+    PlanOnlyComm(int r, int n) : r_(r), n_(n) {}
+    int rank() const override { return r_; }
+    int size() const override { return n_; }
+    void alltoallv(const void*, const size_t*, const size_t*, void*, const size_t*, const size_t*,
+                   cudaStream_t) override {
+        throw Error(FCB_ERR_INTERNAL, "planning query made a collective call");
+    }
+    void allreduce_max_u64(unsigned long long*, int, cudaStream_t) override {
+        throw Error(FCB_ERR_INTERNAL, "planning query made a collective call");
+    }
+    void sync(cudaStream_t) override {}
+    void abort(const std::string&) override {}
+
+  private:
+    int r_, n_;
+};
+}  // namespace
+
+PartitionPlan Context::partition_plan(const fcb_options_t& o, const std::vector<Leaf>& leaves, int rank,
+                                      int nranks, int minlevel, int maxlevel, int ti) {
+    if (nranks < 1 || rank < 0 || rank >= nranks) throw Error(FCB_ERR_INVALID, "bad rank / number of ranks");
+    Context c(o, nullptr, std::make_shared<PlanOnlyComm>(rank, nranks));
+    c.forest_.leaves = leaves;
+    const int n = (int)leaves.size();
+    try {
+        c.nbrs_.resize(n);
+        for (int p = 0; p < n; ++p) c.nbrs_[p] = c.forest_.neighbors(p);
+    } catch (const std::runtime_error& e) {
+        throw Error(FCB_ERR_INVALID, std::string("leaves: ") + e.what());
+    }
+    c.partition_leaves();
+    const std::vector<char> loc = c.local_set();
+    c.slot_of_.assign(n, -1);
+    int k = 0;
+    for (int p = 0; p < n; ++p)
+        if (loc[p]) c.slot_of_[p] = k++;
+    c.capacity_ = std::max(1, k);
+    PartitionPlan out;
+    out.first = c.own_first_;
+    out.count = c.own_count_;
+    out.ghosts = k - c.own_count_;
+    const PlanBuild b = c.build_plan(minlevel, maxlevel, ti);
+    out.x1_send = b.x1.send_n;
+    out.x1_recv = b.x1.recv_n;
+    out.x2_send = b.x2.send_n;
+    out.x2_recv = b.x2.recv_n;
+    out.records = (int)b.ops.size();
+    return out;
 }
 
 static double cfl_from_bits(unsigned long long b) {
@@ -1030,6 +1089,7 @@ void Context::allgather_owned(const double* d_own, int per_leaf, double* d_all) 
 
 double Context::global_maximum(double v) {
     if (!partitioned()) return v;
+    ensure_scalars();
     unsigned long long bits;
     std::memcpy(&bits, &v, sizeof bits);
     if (std::signbit(v)) bits = 0;  // CFL numbers are >= 0
@@ -2094,6 +2154,7 @@ bool Context::regrid() {
 
 // fclaw2d_initialize (src/fclaw2d_initialize.c:75-248)
 void Context::initialize() {
+    ensure_scalars();
     forest_.uniform(opt_.minlevel);
     const int n = num_patches();
     free_slots_.clear();

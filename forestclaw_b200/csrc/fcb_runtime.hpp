@@ -99,6 +99,12 @@ struct GhostPlan {
     XList x1, x2;
 };
 
+// Host-only planning query of a partitioned solve (fcb_partition_plan).
+struct PartitionPlan {
+    int first = 0, count = 0, ghosts = 0, records = 0;
+    std::vector<int> x1_send, x1_recv, x2_send, x2_recv;  // patches per peer rank
+};
+
 class Context {
   public:
     // comm: null for a solve on one rank; otherwise this context is rank
@@ -156,10 +162,15 @@ class Context {
     double global_maximum(double v);
     // marks the communicator failed, so that the other ranks stop at their next collective
     void abort_comm(const std::string& why) noexcept;
+    // rank `rank` of `nranks` over the given leaves (Morton order): owned range,
+    // ghost layer size and the exchange counts of one ghost update; no device call
+    static PartitionPlan partition_plan(const fcb_options_t& o, const std::vector<Leaf>& leaves, int rank,
+                                        int nranks, int minlevel, int maxlevel, int time_interp);
 
   private:
     // --- setup ---
     void check(cudaError_t e, const char* what);
+    void ensure_scalars();
     void ensure_capacity(int nslots);
     int alloc_slot();
     void mesh_changed();  // rebuild neighbour tables, level lists, metadata; drop ghost plans

@@ -299,6 +299,17 @@ int fcb_context_create_partitioned(const fcb_options_t* opt, void* cuda_stream, 
 int fcb_partition_info(fcb_context_t* ctx, int* rank, int* nranks, int* first, int* count);
 /* fclaw2d_domain_global_maximum: the maximum of value over the ranks */
 int fcb_global_maximum(fcb_context_t* ctx, double value, double* out);
+/* Planning query, host only (no device call, works without a GPU): rank `rank`
+ * of `nranks` over nleaves leaves in Morton order (level, and the lower-left
+ * corner x, y in units of 2^-28 of the block), partitioned as a partitioned
+ * solve does: the owned leaves [first, first + count), the size of the ghost
+ * layer, and per peer rank (arrays of nranks) the patches the ghost update
+ * (minlevel, maxlevel, time_interp) sends and receives in its first exchange
+ * (x1, before the averages and copies) and second (x2, before the
+ * interpolations).  Rank a's x?_send[b] equals rank b's x?_recv[a]. */
+int fcb_partition_plan(const fcb_options_t* opt, int nranks, int rank, int nleaves, const int* level, const int* x,
+                       const int* y, int minlevel, int maxlevel, int time_interp, int* first, int* count,
+                       int* ghosts, int* x1_send, int* x1_recv, int* x2_send, int* x2_recv);
 
 /* ---- ensemble serving -----------------------------------------------------
  * No counterpart in the reference (ForestClaw runs one solve per process): a

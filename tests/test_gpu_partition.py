@@ -260,3 +260,26 @@ def test_partitioned_option_checks(gpu_lib):
     with pytest.raises(fcb.FcbError) as e:
         fcb.Solver(opts, comm=comms[0])
     assert e.value.code == 1
+
+
+def test_nccl_communicator_one_rank(gpu_lib):
+    """The NCCL communicator (loaded at run time, non-blocking, bounded waits)
+    as a one-rank partitioned solve: initialisation, the global maximum, the
+    gathered tags and the rank's own exchange path; equal to the plain solve."""
+    import forestclaw_b200 as fcb
+
+    comm = fcb.nccl_comm(fcb.nccl_unique_id(), 0, 1, timeout_s=60.0)
+    opts = cases.to_options(cases.radialdam_amr(seed=1, minlevel=2, maxlevel=4, mx=16))
+    s = fcb.Solver(opts)
+    d = fcb.Solver(opts, comm=comm)
+    s.initialize()
+    d.initialize()
+    t, dt = 0.0, 0.002
+    for _ in range(4):
+        assert d.global_maximum(d.advance_all_levels(t, dt)) == s.advance_all_levels(t, dt)
+        t += dt
+        assert d.regrid() == s.regrid()
+    assert d.leaves() == s.leaves()
+    assert np.array_equal(d.get_q(), s.get_q())
+    assert np.array_equal(d.conservation_check(), s.conservation_check())
+    assert d.partition_info() == {"rank": 0, "nranks": 1, "first": 0, "count": s.num_patches}
