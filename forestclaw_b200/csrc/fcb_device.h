@@ -50,6 +50,10 @@ struct StepArgs {
     unsigned long long* cfl_out;  // atomicMax on the bits of a non-negative double
     double* treg;          // time-sync: conservation-register arena (null: off)
     int64_t treg_stride;   // doubles per slot in treg
+    // nlvl > 1: one launch over the level updates between two ghost updates;
+    // dyn holds {dt, vt} for levels lvl0 .. lvl0 + nlvl - 1 and each patch reads
+    // its own level's pair
+    int32_t lvl0, nlvl;
 };
 
 // Conservation registers of one slot (fclaw2d_clawpatch_registers_t), doubles
@@ -94,8 +98,14 @@ struct TsArgs {
     int ngroups;
 };
 #ifdef __CUDACC__
-__device__ __forceinline__ double step_dt(const StepArgs& a) { return a.dyn ? a.dyn[0] : a.dt; }
-__device__ __forceinline__ double step_vt(const StepArgs& a) { return a.dyn ? a.dyn[1] : a.vt; }
+// {dt, vt} of a patch of `level` (clamped: threads without a patch read a valid entry)
+__device__ __forceinline__ const double* step_dv(const StepArgs& a, int level) {
+    int k = level - a.lvl0;
+    k = a.nlvl > 1 ? (k < 0 ? 0 : (k >= a.nlvl ? a.nlvl - 1 : k)) : 0;
+    return a.dyn + 2 * k;
+}
+__device__ __forceinline__ double step_dt(const StepArgs& a, int level) { return a.dyn ? step_dv(a, level)[0] : a.dt; }
+__device__ __forceinline__ double step_vt(const StepArgs& a, int level) { return a.dyn ? step_dv(a, level)[1] : a.vt; }
 #endif
 
 // Ghost-cell operations, one record per reference kernel call.

@@ -1194,7 +1194,18 @@ void Context::physical_set_bc(int level, int time_interp) {
 // ---------------------------------------------------------------------------
 void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, double dt,
                                       unsigned long long* cfl_slot) {
+    const double tl[1] = {t}, dl[1] = {dt};
+    launch_levels_step_slots(d_slots, n, 0, 1, tl, dl, cfl_slot);
+}
+
+// One step launch over patches of levels lvl0 .. lvl0 + nlvl - 1 (their slots
+// contiguous in d_slots), level l at time t[l - lvl0] with step dt[l - lvl0].
+// nlvl > 1 needs the macro-step table (use_dyn_): each level's {dt, vt} pair.
+void Context::launch_levels_step_slots(const int32_t* d_slots, int n, int lvl0, int nlvl, const double* tl,
+                                       const double* dtl, unsigned long long* cfl_slot) {
     if (n <= 0) return;
+    if (nlvl > 1 && !use_dyn_) throw Error(FCB_ERR_INTERNAL, "merged level updates need the step-parameter table");
+    const double t = tl[0], dt = dtl[0];
     StepArgs a{};
     a.q = d_q_;
     a.qlast = d_qlast_;
@@ -1223,10 +1234,14 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     a.cfl_out = cfl_slot;
     a.treg = time_sync_ ? d_treg_ : nullptr;
     a.treg_stride = treg_stride_;
+    a.lvl0 = lvl0;
+    a.nlvl = nlvl;
     if (use_dyn_) {
-        // {dt, vt} of launch dyn_n_ of the macro step: written to the table by
-        // the dry pass, read from the device table by the launch itself
+        // {dt, vt} of launch dyn_n_ of the macro step (one pair per level of a
+        // merged launch): written to the table by the dry pass, read from the
+        // device table by the launch itself
         if (dry_) {
+            for (int k = 0; k < nlvl; ++k) {
             if (dyn_n_ >= (int)dyn_cap_) {
                 const size_t nc = std::max<size_t>(64, 2 * dyn_cap_);
                 double* np = nullptr;
@@ -1238,15 +1253,22 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
                 h_dyn_ = np;
                 dyn_cap_ = nc;
             }
-            h_dyn_[2 * dyn_n_] = a.dt;
-            h_dyn_[2 * dyn_n_ + 1] = a.vt;
+            double vk = 0.0;
+            if (aux_kind_ == AUX_SWIRL) {
+                const double pi2 = 2.0 * (4.0 * std::atan(1.0));
+                const double tperiod = opt_.problem_params[0];
+                vk = (tperiod == 0.0) ? 0.0 : std::cos(pi2 * (tl[k] + dtl[k] / 2.0) / tperiod);
+            }
+            h_dyn_[2 * dyn_n_] = dtl[k];
+            h_dyn_[2 * dyn_n_ + 1] = vk;
             ++dyn_n_;
+            }
             return;
         }
-        if (!d_dyn_.p || 2 * (size_t)dyn_n_ + 2 > d_dyn_.cap)
+        if (!d_dyn_.p || 2 * (size_t)(dyn_n_ + nlvl) > d_dyn_.cap)
             throw Error(FCB_ERR_STATE, "step-parameter table not sized by the dry pass");
         a.dyn = d_dyn_.p + 2 * dyn_n_;
-        ++dyn_n_;
+        dyn_n_ += nlvl;
     }
     // The warp form computes each swirl velocity node once, which equals the
     // reference's per-cell evaluations because the unit-square mesh with mx a
@@ -1345,8 +1367,34 @@ void Context::run_schedule(double t_curr, double dt) {
         }
     }
     if (!dry_) check(cudaMemsetAsync(d_cfl_, 0, sizeof(unsigned long long), st_), "memset");
+    // With the step-parameter table the level updates between two ghost
+    // updates (levels gmax down to some l, contiguous in the level-sorted slot
+    // list) go out as one launch: they touch disjoint patches, the CFL is a
+    // max, and each patch reads its own level's {dt, vt}.  Time interpolation,
+    // ghost updates and time-sync flush the queued levels first.
+    const bool merge = use_dyn_ && !time_sync_;
+    int q_lo = -1, q_hi = -1;
+    std::vector<double> q_t((size_t)QuadForest::kMaxLevel + 2), q_dt((size_t)QuadForest::kMaxLevel + 2);
+    auto flush = [&]() {
+        if (q_hi < 0) return;
+        const int b = level_begin_[q_lo], e = level_begin_[q_hi + 1];
+        launch_levels_step_slots(d_level_slots_.p + b, e - b, q_lo, q_hi - q_lo + 1, q_t.data() + q_lo,
+                                 q_dt.data() + q_lo, d_cfl_);
+        q_lo = q_hi = -1;
+    };
+    auto step_level = [&](int level, double t, double dts) {
+        if (!merge || level < 0 || level > QuadForest::kMaxLevel) {
+            launch_level_step(level, t, dts, d_cfl_);
+            return;
+        }
+        if (q_hi >= 0 && level != q_lo - 1) flush();  // keep the queued levels contiguous
+        if (q_hi < 0) q_hi = level;
+        q_lo = level;
+        q_t[level] = t;
+        q_dt[level] = dts;
+    };
     std::function<void(int, int)> advance_level = [&](int level, int curr_fine_step) {
-        launch_level_step(level, ts[level].current_time, ts[level].dt_step, d_cfl_);
+        step_level(level, ts[level].current_time, ts[level].dt_step);
         ts[level].last_step += ts[level].step_inc;
         ts[level].current_time += ts[level].dt_step;
         if (level > gmin) {
@@ -1356,6 +1404,7 @@ void Context::run_schedule(double t_curr, double dt) {
                 if (opt_.subcycle) {
                     const int coarse_inc = ts[level - 1].step_inc;
                     const double alpha = ((double)(ts[level].last_step % coarse_inc)) / coarse_inc;
+                    flush();
                     timeinterp(level - 1, alpha);
                 }
             }
@@ -1364,6 +1413,7 @@ void Context::run_schedule(double t_curr, double dt) {
     const int n_fine = ts[gmax].total_steps;
     for (int nf = 0; nf < n_fine; ++nf) {
         advance_level(gmax, nf);
+        flush();
         const int last_step = ts[gmax].last_step;
         if (last_step < ts[gmax].total_steps) {
             const double sync_time = ts[gmax].current_time;

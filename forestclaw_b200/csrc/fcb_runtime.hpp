@@ -270,6 +270,8 @@ class Context {
     std::vector<uintptr_t> macro_fingerprint() const;
     void drop_macro_graph();
     void launch_level_step_slots(const int32_t* d_slots, int n, double t, double dt, unsigned long long* cfl_slot);
+    void launch_levels_step_slots(const int32_t* d_slots, int n, int lvl0, int nlvl, const double* t,
+                                  const double* dt, unsigned long long* cfl_slot);
 
     fcb_options_t opt_;
     cudaStream_t st_;

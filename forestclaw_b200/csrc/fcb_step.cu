@@ -86,8 +86,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     double* __restrict__ q = a.q + (int64_t)slot * a.q_stride;
     double* __restrict__ qlast = a.qlast + (int64_t)slot * a.q_stride;
     const bool save_last = active && (meta.flags & PATCH_SAVE_LAST);
-    const double dtdx = step_dt(a) / meta.dx;
-    const double dtdy = step_dt(a) / meta.dy;
+    const double dtdx = step_dt(a, meta.level) / meta.dx;
+    const double dtdy = step_dt(a, meta.level) / meta.dy;
     const double dtdxave = 0.5 * (dtdx + dtdx);  // 0.5*(dtdx1d(i-1)+dtdx1d(i)), no capacity
     const double dtdyave = 0.5 * (dtdy + dtdy);
     SOL sol{a.grav, a.gamma, a.gamma1};
@@ -122,8 +122,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         }
         __syncthreads();
         if (active) {
-            const double vty = step_vt(a) / meta.dy;
-            const double vtx = step_vt(a) / meta.dx;
+            const double vty = step_vt(a, meta.level) / meta.dy;
+            const double vtx = step_vt(a, meta.level) / meta.dx;
             double* au = s_aux + (pl * NAUX + 0) * NY * NX;
             double* av = s_aux + (pl * NAUX + 1) * NY * NX;
             for (int r = 0; r < NY; ++r) {
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                     const RegLayout RL{MX, MX, M};
                     double* R = a.treg + (int64_t)slot * a.treg_stride;
                     const int i = c - MBC + 1, j = r - MBC + 1;
-                    const double dty = step_dt(a) * meta.dy, dtx = step_dt(a) * meta.dx;
+                    const double dty = step_dt(a, meta.level) * meta.dy, dtx = step_dt(a, meta.level) * meta.dx;
                     if (j >= 1 && j <= MX) {
                         const int k = (j - 1) + MX * m;
                         if (i == 1) R[RL.fp(0) + k] = R[RL.fp(0) + k] - dty * fpv;

@@ -640,7 +640,7 @@ __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
     T.nb = dsm + L::ND + pls * (NX + 1) + c;
     T.ty = dsm + L::TY + pls * (NX + 1);
     // dtdx1d is uniform without capacity, so 0.5*(dtdx1d(i-1)+dtdx1d(i)) == dtdx exactly
-    const double dt = D ? D->dt : step_dt(a), vt = D ? D->vt : step_vt(a);
+    const double dt = D ? D->dt : step_dt(a, meta.level), vt = D ? D->vt : step_vt(a, meta.level);
     T.dtdx = dt / meta.dx;
     T.dtdy = dt / meta.dy;
     T.rdtdx = R(T.dtdx);

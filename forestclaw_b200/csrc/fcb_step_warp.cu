@@ -66,9 +66,9 @@ __global__ void __launch_bounds__(128) step_kernel_warp(const StepArgs a) {
     double* __restrict__ q = a.q + (int64_t)slot * a.q_stride;
     double* __restrict__ qlast = a.qlast + (int64_t)slot * a.q_stride;
     const bool save_last = active && (meta.flags & PATCH_SAVE_LAST);
-    const double dtdx = step_dt(a) / meta.dx, dtdy = step_dt(a) / meta.dy;
+    const double dtdx = step_dt(a, meta.level) / meta.dx, dtdy = step_dt(a, meta.level) / meta.dy;
     const double dtdxave = 0.5 * (dtdx + dtdx), dtdyave = 0.5 * (dtdy + dtdy);
-    const double vty = step_vt(a) / meta.dy, vtx = step_vt(a) / meta.dx;
+    const double vty = step_vt(a, meta.level) / meta.dy, vtx = step_vt(a, meta.level) / meta.dx;
     const SOL sol{a.grav, a.gamma, a.gamma1};
     const int c0 = k * CPL;  // first own column
 

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(TS_TPB) store_flux_kernel(const StepArgs a, in
     const double* q = a.q + (int64_t)slot * a.q_stride;
     double* R = a.treg + (int64_t)slot * a.treg_stride;
     const RegLayout L{mx, my, meqn};
-    const double dt = step_dt(a);
+    const double dt = step_dt(a, mt.level);
     const int nitems = 2 * 2 * my + 2 * 2 * mx;  // faces 0, 1 (my cells) and 2, 3 (mx cells), two sides each
     for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
         int face, cell, k;
