@@ -253,3 +253,40 @@ def test_autotuned_form_is_bit_identical_to_forced_form(gpu_lib, case):
     assert np.array_equal(auto.get_q(), forced.get_q())
     auto.close()
     forced.close()
+
+
+def test_merged_level_launches_bit_exact(gpu_lib):
+    """Subcycled macro steps on a mesh of several levels: with the macro-step
+    table the level updates between two ghost updates go out as one launch
+    (each patch reads its level's dt); they must equal one launch per level
+    (macro_graph 0) and the oracle, through regrids."""
+    import forestclaw_b200 as fcb
+
+    cfg = cases.quadrants_amr(seed=1, minlevel=2, maxlevel=5, mx=8)
+    o = O.OracleSolver(cfg)
+    o.initialize()
+    solvers = []
+    for graph in (0, 2):
+        opts = cases.to_options(cfg)
+        opts.macro_graph = graph
+        d = fcb.Solver(opts)
+        d.initialize()
+        solvers.append(d)
+    per_level, merged = solvers
+    assert len({lv for lv, _, _ in o.leaves()}) >= 2
+    t, dt = 0.0, 0.9 / (8 * 32) / 1.5
+    for k in range(4):
+        c_o = o.advance(t, dt)
+        assert per_level.advance_all_levels(t, dt) == c_o
+        assert merged.advance_all_levels(t, dt) == c_o
+        t += dt
+        q = o.all_q()
+        assert np.array_equal(per_level.get_q(), q), f"macro step {k}"
+        assert np.array_equal(merged.get_q(), q), f"macro step {k}"
+        o.regrid()
+        per_level.regrid()
+        merged.regrid()
+        assert merged.leaves() == per_level.leaves() == o.leaves()
+    cp, cm = per_level.counters(), merged.counters()
+    assert cm["count_single_step"] == cp["count_single_step"]
+    assert cm["count_kernel_launches"] < cp["count_kernel_launches"]

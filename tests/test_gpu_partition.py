@@ -283,3 +283,14 @@ def test_nccl_communicator_one_rank(gpu_lib):
     assert np.array_equal(d.get_q(), s.get_q())
     assert np.array_equal(d.conservation_check(), s.conservation_check())
     assert d.partition_info() == {"rank": 0, "nranks": 1, "first": 0, "count": s.num_patches}
+
+
+@pytest.mark.parametrize("subcycle,weighted", [(0, 1), (1, 0)])
+def test_partitioned_schedule_variants(gpu_lib, subcycle, weighted):
+    """Non-subcycled steps (every level with the fine dt, ghost fills over all
+    levels) and an unweighted partition, on a mesh of several levels."""
+    cfg = dataclasses.replace(cases.quadrants_amr(seed=1, minlevel=2, maxlevel=5, mx=8), subcycle=subcycle)
+    opts = cases.to_options(cfg)
+    opts.weighted_partition = weighted
+    q_ref, q_all, _ = _stepped(opts, 3, steps=3, dt=0.9 / (8 * 32) / 1.5 / (1 if subcycle else 8), regrid=True)
+    assert np.array_equal(q_all, q_ref)
