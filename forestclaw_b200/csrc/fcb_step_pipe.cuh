@@ -589,8 +589,18 @@ __host__ __device__ constexpr int pipe_threads_per_patch() { return SWIRL ? NX +
 
 }  // namespace
 
+// Resident CTAs per SM the register budget is cut for: the mixed scalar form
+// fits six 128-thread CTAs at 80 registers (a 32-byte spill), 3 % faster on the
+// step than five at 93; seven (72 registers) and eight (64) spill more and
+// are slower (B200, uniform swirl mx = 16).  The FP64 and system forms keep the
+// compiler's choice.
+template <class SOL>
+constexpr int pipe_min_ctas() {
+    return (sizeof(typename SOL::Real) == 4 && SOL::M == 1) ? 6 : 1;
+}
+
 template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
-__global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
+__global__ void __launch_bounds__(TPB, pipe_min_ctas<SOL>()) step_kernel_pipe(const StepArgs a) {
     constexpr int M = SOL::M;
     constexpr int W = SOL::W;
     constexpr int NX = MX + 2 * MBC;
