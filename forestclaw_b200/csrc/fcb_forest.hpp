@@ -42,13 +42,20 @@ class QuadForest {
     std::vector<Leaf> leaves;
 
     static int32_t width(int level) { return (int32_t)1 << (kMaxLevel - level); }
-    static uint64_t morton(int32_t x, int32_t y) {
-        uint64_t k = 0;
-        for (int b = 0; b < kMaxLevel; ++b) {
-            k |= (uint64_t)((x >> b) & 1) << (2 * b);
-            k |= (uint64_t)((y >> b) & 1) << (2 * b + 1);
-        }
+    // bit b of v (b < 32) to bit 2b
+    static uint64_t spread(uint32_t v) {
+        uint64_t k = v;
+        k = (k | (k << 16)) & 0x0000FFFF0000FFFFull;
+        k = (k | (k << 8)) & 0x00FF00FF00FF00FFull;
+        k = (k | (k << 4)) & 0x0F0F0F0F0F0F0F0Full;
+        k = (k | (k << 2)) & 0x3333333333333333ull;
+        k = (k | (k << 1)) & 0x5555555555555555ull;
         return k;
+    }
+    // z-order key of the low kMaxLevel bits: x in the even bits, y in the odd
+    static uint64_t morton(int32_t x, int32_t y) {
+        constexpr uint32_t mask = ((uint32_t)1 << kMaxLevel) - 1;
+        return spread((uint32_t)x & mask) | (spread((uint32_t)y & mask) << 1);
     }
     static Leaf make(int level, int32_t x, int32_t y) { return Leaf{morton(x, y), x, y, level}; }
 

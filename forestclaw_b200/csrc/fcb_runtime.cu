@@ -342,13 +342,38 @@ PatchMeta Context::meta_of(const Leaf& l) const {
     return m;
 }
 
+// Neighbour relations of every leaf (point location in the Morton-sorted
+// leaves), split over host threads for large forests.
+void Context::compute_neighbors() {
+    const int n = num_patches();
+    nbrs_.resize(n);
+    const int nt = (int)std::min<unsigned>({8u, std::max(1u, std::thread::hardware_concurrency()), (unsigned)(n / 512 + 1)});
+    if (nt == 1) {
+        for (int p = 0; p < n; ++p) nbrs_[p] = forest_.neighbors(p);
+        return;
+    }
+    std::vector<std::thread> ts;
+    std::vector<std::exception_ptr> err(nt);
+    for (int k = 0; k < nt; ++k)
+        ts.emplace_back([&, k] {
+            try {
+                for (int p = (int)((int64_t)n * k / nt); p < (int)((int64_t)n * (k + 1) / nt); ++p)
+                    nbrs_[p] = forest_.neighbors(p);
+            } catch (...) {
+                err[k] = std::current_exception();
+            }
+        });
+    for (auto& t : ts) t.join();
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
+}
+
 void Context::mesh_changed() {
     discard_plans();
     ++mesh_version_;
     drop_macro_graph();
     const int n = num_patches();
-    nbrs_.resize(n);
-    for (int p = 0; p < n; ++p) nbrs_[p] = forest_.neighbors(p);
+    compute_neighbors();
     // slot metadata
     if (!partitioned()) {
         own_first_ = 0;
@@ -613,9 +638,18 @@ Context::PlanBuild Context::make_waves(const std::vector<GhostOp>& ops) const {
     const Rect interior{1, mx, 1, my};
     std::vector<int> wave(ops.size(), 0);
     // writes and reads seen so far, per array (slot * 2 + time-interp flag):
-    // a read conflicts only with writes, a write with both
+    // a read conflicts only with writes, a write with both.  Each array's
+    // touches form a list through flat arrays (newest first), no allocation
+    // per array.
     const size_t narr = (size_t)2 * std::max(1, capacity_);
-    std::vector<std::vector<std::pair<Rect, int>>> seen_w(narr), seen_r(narr);
+    struct Seen {
+        Rect r;
+        int wave;
+        int next;
+    };
+    std::vector<Seen> seen;
+    seen.reserve(2 * ops.size());
+    std::vector<int> head_w(narr, -1), head_r(narr, -1);
     auto band = [&](int face) -> Rect {
         if (face == 0) return {1 - mbc, 0, 1, my};
         if (face == 1) return {mx + 1, mx + mbc, 1, my};
@@ -672,14 +706,18 @@ Context::PlanBuild Context::make_waves(const std::vector<GhostOp>& ops) const {
         }
         int w = 0;
         for (const Touch& a : t) {
-            for (const auto& pr : seen_w[(size_t)a.key])
-                if (pr.second >= w && a.r.hits(pr.first)) w = pr.second + 1;
+            for (int i = head_w[(size_t)a.key]; i >= 0; i = seen[i].next)
+                if (seen[i].wave >= w && a.r.hits(seen[i].r)) w = seen[i].wave + 1;
             if (a.write)
-                for (const auto& pr : seen_r[(size_t)a.key])
-                    if (pr.second >= w && a.r.hits(pr.first)) w = pr.second + 1;
+                for (int i = head_r[(size_t)a.key]; i >= 0; i = seen[i].next)
+                    if (seen[i].wave >= w && a.r.hits(seen[i].r)) w = seen[i].wave + 1;
         }
         wave[k] = w;
-        for (const Touch& a : t) (a.write ? seen_w : seen_r)[(size_t)a.key].push_back({a.r, w});
+        for (const Touch& a : t) {
+            int& h = (a.write ? head_w : head_r)[(size_t)a.key];
+            seen.push_back({a.r, w, h});
+            h = (int)seen.size() - 1;
+        }
     }
     const int nw = ops.empty() ? 0 : *std::max_element(wave.begin(), wave.end()) + 1;
     PlanBuild b;
@@ -687,14 +725,26 @@ Context::PlanBuild Context::make_waves(const std::vector<GhostOp>& ops) const {
     std::vector<int> count(nw, 0);
     for (int w : wave) ++count[w];
     for (int w = 0; w < nw; ++w) b.wave_begin[w + 1] = b.wave_begin[w] + count[w];
-    b.ops.resize(ops.size());
+    // records ordered by (wave, destination), keeping the reference's order
+    // among equal keys: a stable counting sort by destination slot, then a
+    // stable counting sort by wave
+    const size_t n = ops.size();
+    std::vector<int> by_dst(n);
+    {
+        std::vector<int> start((size_t)std::max(1, capacity_) + 1, 0);
+        for (const GhostOp& o : ops) {
+            if (o.dst < 0 || o.dst >= std::max(1, capacity_)) throw Error(FCB_ERR_INTERNAL, "ghost record outside the arena");
+            ++start[(size_t)o.dst + 1];
+        }
+        for (size_t d = 1; d < start.size(); ++d) start[d] += start[d - 1];
+        for (size_t k = 0; k < n; ++k) by_dst[start[(size_t)ops[k].dst]++] = (int)k;
+    }
+    b.ops.resize(n);
     std::vector<int> pos(b.wave_begin.begin(), b.wave_begin.end() - (nw ? 1 : 0));
-    for (size_t k = 0; k < ops.size(); ++k) b.ops[pos[wave[k]]++] = ops[k];
+    for (int k : by_dst) b.ops[pos[wave[k]]++] = ops[k];
     // within a wave, records with the same destination patch form one group
     b.group_begin.assign(nw + 1, 0);
     for (int w = 0; w < nw; ++w) {
-        auto first = b.ops.begin() + b.wave_begin[w], last = b.ops.begin() + b.wave_begin[w + 1];
-        std::stable_sort(first, last, [](const GhostOp& x, const GhostOp& y) { return x.dst < y.dst; });
         b.group_begin[w] = (int)b.groups.size();
         for (int k = b.wave_begin[w]; k < b.wave_begin[w + 1]; ++k)
             if (k == b.wave_begin[w] || b.ops[k].dst != b.ops[k - 1].dst) b.groups.push_back(k);
@@ -1998,8 +2048,7 @@ void Context::repopulate_partitioned(const std::vector<Leaf>& old_leaves, const 
                                      const std::vector<int>& old_owner, bool domain_init) {
     const int nn = num_patches(), no = (int)old_leaves.size(), R = nranks_;
     partition_leaves();
-    nbrs_.resize(nn);
-    for (int p = 0; p < nn; ++p) nbrs_[p] = forest_.neighbors(p);
+    compute_neighbors();
     const std::vector<char> loc = local_set();
     // kind: 0 the same leaf, 1 a child of old leaf src, 2 the parent of old leaves src..src+3
     std::vector<int> kind(nn, 0), src(nn, -1);
@@ -2213,8 +2262,7 @@ void Context::initialize() {
         // fclaw2d_domain_new_unitsquare + the first partition: this rank's Morton
         // range and its ghost layer get slots
         partition_leaves();
-        nbrs_.resize(n);
-        for (int p = 0; p < n; ++p) nbrs_[p] = forest_.neighbors(p);
+        compute_neighbors();
         const std::vector<char> loc = local_set();
         ensure_capacity(std::max(1, (int)std::count(loc.begin(), loc.end(), 1)));
         slot_of_.assign(n, -1);

@@ -174,6 +174,7 @@ class Context {
     void ensure_capacity(int nslots);
     int alloc_slot();
     void mesh_changed();  // rebuild neighbour tables, level lists, metadata; drop ghost plans
+    void compute_neighbors();
     PatchMeta meta_of(const Leaf& l) const;
     // --- ghost plans ---
     const GhostPlan& plan(int minlevel, int maxlevel, int time_interp);

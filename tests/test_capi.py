@@ -89,3 +89,24 @@ def test_null_arguments_are_errors(built):
     lib = built.lib()
     assert lib.fcb_context_create(None, None, None) == 1
     assert b"null" in lib.fcb_last_error()
+
+
+def test_forest_morton_key_matches_bit_loop(tmp_path):
+    """The forest's z-order key (bit spreading) equals the key built bit by
+    bit (x in the even bits, y in the odd bits of the low 28 bits)."""
+    src = tmp_path / "mk.cpp"
+    src.write_text(
+        '#include <cstdio>\n#include <random>\n#include "fcb_forest.hpp"\n'
+        "static uint64_t loop(int32_t x, int32_t y) { uint64_t k = 0;\n"
+        "  for (int b = 0; b < 28; ++b) { k |= (uint64_t)((x >> b) & 1) << (2 * b);\n"
+        "    k |= (uint64_t)((y >> b) & 1) << (2 * b + 1); } return k; }\n"
+        "int main() { std::mt19937 g(7); int bad = 0;\n"
+        "  const int32_t edge[] = {0, 1, 2, 3, (1 << 27) - 1, 1 << 27, (1 << 28) - 1};\n"
+        "  for (int32_t a : edge) for (int32_t b : edge) bad += fcb::QuadForest::morton(a, b) != loop(a, b);\n"
+        "  for (int k = 0; k < 200000; ++k) { int32_t x = g() & ((1 << 28) - 1), y = g() & ((1 << 28) - 1);\n"
+        "    bad += fcb::QuadForest::morton(x, y) != loop(x, y); }\n"
+        '  std::printf("%d\\n", bad); return 0; }\n')
+    exe = tmp_path / "mk"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", str(ROOT / "forestclaw_b200" / "csrc"), str(src), "-o", str(exe)],
+                   check=True)
+    assert subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.strip() == "0"
