@@ -78,29 +78,46 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.samples = []
-        self._stop = threading.Event()
+        self._first = threading.Event()
+        self._p = None
         self._t = None
+        self._start = 0
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._p.stdout:
+            parts = [x.strip() for x in line.strip().split(",")]
+            if len(parts) > 2:
+                self.samples.append(parts)
+                self._first.set()
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        # one long-lived nvidia-smi (NVML initialised once), its first sample
+        # taken before the timed region starts
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self._p = None
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
+        self._first.wait(5.0)
+        self._start = len(self.samples)
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is None:
+            return
+        self._p.terminate()
+        try:
+            self._p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self._p.kill()
+            self._p.wait(timeout=5)
+        self._t.join(timeout=5)
+        if len(self.samples) > self._start:
+            self.samples = self.samples[self._start:]
 
     def summary(self):
         if not self.samples:

@@ -589,18 +589,19 @@ __host__ __device__ constexpr int pipe_threads_per_patch() { return SWIRL ? NX +
 
 }  // namespace
 
-// Resident CTAs per SM the register budget is cut for: the mixed scalar form
-// fits six 128-thread CTAs at 80 registers (a 32-byte spill), 3 % faster on the
-// step than five at 93; seven (72 registers) and eight (64) spill more and
-// are slower (B200, uniform swirl mx = 16).  The FP64 and system forms keep the
-// compiler's choice.
+// The mixed scalar form runs with the register budget cut for six resident
+// 128-thread CTAs per SM (80 registers, a 32-byte spill): 3 % faster on the step
+// than five at 93; seven (72 registers) and eight (64) spill more and are slower
+// (B200, uniform swirl mx = 16).  Every other form keeps the compiler's choice:
+// even an explicit minimum of one CTA changes its code (FP64 swirl step 18 %
+// slower), so the body is shared by two kernels that differ only in the bound.
 template <class SOL>
-constexpr int pipe_min_ctas() {
-    return (sizeof(typename SOL::Real) == 4 && SOL::M == 1) ? 6 : 1;
+constexpr bool pipe_six_ctas() {
+    return sizeof(typename SOL::Real) == 4 && SOL::M == 1;
 }
 
 template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
-__global__ void __launch_bounds__(TPB, pipe_min_ctas<SOL>()) step_kernel_pipe(const StepArgs a) {
+__device__ __forceinline__ void step_pipe_body(const StepArgs& a) {
     constexpr int M = SOL::M;
     constexpr int W = SOL::W;
     constexpr int NX = MX + 2 * MBC;
@@ -760,6 +761,23 @@ __global__ void __launch_bounds__(TPB, pipe_min_ctas<SOL>()) step_kernel_pipe(co
     }
 }
 
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
+__global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
+    step_pipe_body<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>(a);
+}
+
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
+__global__ void __launch_bounds__(TPB, 6) step_kernel_pipe_six(const StepArgs a) {
+    step_pipe_body<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>(a);
+}
+
+// the one kernel of the two that a form uses (only that one is instantiated)
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
+constexpr auto pipe_kernel() {
+    if constexpr (pipe_six_ctas<SOL>()) return step_kernel_pipe_six<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>;
+    else return step_kernel_pipe<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>;
+}
+
 // ---------------------------------------------------------------------------
 // Host-side launcher
 // ---------------------------------------------------------------------------
@@ -772,16 +790,16 @@ cudaError_t launch_pipe_one(const StepArgs& a, cudaStream_t st) {
     static_assert(PPB >= 1, "patch wider than the CTA");
     using L = PipeSmem<NX, PPB, SOL::M, SOL::W, NAUX, AUXK == AUX_SWIRL, typename SOL::Real, ring_in_fp64<SOL>>;
     const size_t bytes = (size_t)L::BYTES;
+    constexpr auto kernel = pipe_kernel<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>();
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(step_kernel_pipe<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e != cudaSuccess) return e;
         configured = true;
     }
     const int blocks = (a.npatches + PPB - 1) / PPB;
     if (blocks == 0) return cudaSuccess;
-    step_kernel_pipe<SOL, MX, MBC, AUXK, NAUX, TPB, LIM><<<blocks, TPB, bytes, st>>>(a);
+    kernel<<<blocks, TPB, bytes, st>>>(a);
     return cudaGetLastError();
 }
 
