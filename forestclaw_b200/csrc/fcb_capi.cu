@@ -334,7 +334,7 @@ int fcb_global_maximum(fcb_context_t* ctx, double value, double* out) {
 }
 
 int fcb_output_ascii(fcb_context_t* ctx, int iframe, const char* dir) {
-    return guard([&] {
+    return collective(ctx, [&] {
         CTX();
         C.output_ascii(iframe, dir ? std::string(dir) : std::string("."));
     });

@@ -62,21 +62,34 @@ FILE* open_or_throw(const std::string& path, const char* mode) {
 }
 }  // namespace
 
-void write_ascii_frame(const std::string& dir, int iframe, double time, int meqn, int maux, int mx, int my, int mbc,
-                       const std::vector<OutputPatch>& patches, const double* q, size_t patch_size) {
+void write_ascii_header(const std::string& dir, int iframe, double time, int meqn, int maux, long ngrids) {
     char name[32];
     const std::string base = dir.empty() ? std::string(".") : dir;
-    // fclaw2d_clawpatch46_fort_header_ascii
+    // fclaw2d_clawpatch46_fort_header_ascii: fort.t, and an empty fort.q
     std::snprintf(name, sizeof name, "fort.t%04d", iframe);
     FILE* ft = open_or_throw(base + "/" + name, "w");
     std::fprintf(ft, "%s    time\n", fortran_e(time, 30, 20).c_str());
     std::fprintf(ft, "%s                 meqn\n", fortran_i(meqn, 5).c_str());
-    std::fprintf(ft, "%s                 ngrids\n", fortran_i((long)patches.size(), 5).c_str());
+    std::fprintf(ft, "%s                 ngrids\n", fortran_i(ngrids, 5).c_str());
     std::fprintf(ft, "%s                 num_aux\n", fortran_i(maux, 5).c_str());
     std::fprintf(ft, "%s                 num_dim\n", fortran_i(2, 5).c_str());
     std::fclose(ft);
     std::snprintf(name, sizeof name, "fort.q%04d", iframe);
-    FILE* fq = open_or_throw(base + "/" + name, "w");
+    std::fclose(open_or_throw(base + "/" + name, "w"));
+}
+
+void write_ascii_frame(const std::string& dir, int iframe, double time, int meqn, int maux, int mx, int my, int mbc,
+                       const std::vector<OutputPatch>& patches, const double* q, size_t patch_size) {
+    write_ascii_header(dir, iframe, time, meqn, maux, (long)patches.size());
+    append_ascii_patches(dir, iframe, meqn, mx, my, mbc, patches, q, patch_size, 0);
+}
+
+void append_ascii_patches(const std::string& dir, int iframe, int meqn, int mx, int my, int mbc,
+                          const std::vector<OutputPatch>& patches, const double* q, size_t patch_size, int mpi_rank) {
+    char name[32];
+    const std::string base = dir.empty() ? std::string(".") : dir;
+    std::snprintf(name, sizeof name, "fort.q%04d", iframe);
+    FILE* fq = open_or_throw(base + "/" + name, "a");
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
     std::string line;
     for (size_t p = 0; p < patches.size(); ++p) {
@@ -85,7 +98,7 @@ void write_ascii_frame(const std::string& dir, int iframe, double time, int meqn
         std::fprintf(fq, "%s                 grid_number\n", fortran_i(P.global_num, 5).c_str());
         std::fprintf(fq, "%s                 AMR_level\n", fortran_i(P.level, 5).c_str());
         std::fprintf(fq, "%s                 block_number\n", fortran_i(0, 5).c_str());
-        std::fprintf(fq, "%s                 mpi_rank\n", fortran_i(0, 5).c_str());
+        std::fprintf(fq, "%s                 mpi_rank\n", fortran_i(mpi_rank, 5).c_str());
         std::fprintf(fq, "%s                 mx\n", fortran_i(mx, 5).c_str());
         std::fprintf(fq, "%s                 my\n", fortran_i(my, 5).c_str());
         std::fprintf(fq, "%s    xlow\n", fortran_e(P.xlower, 24, 16).c_str());

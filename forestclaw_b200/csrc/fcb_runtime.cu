@@ -2375,34 +2375,55 @@ void Context::get_q(double* host, size_t n, bool qinterp) {
     synchronize();
 }
 
+// fclaw2d_clawpatch_output_ascii: rank 0 writes the header, then the ranks
+// append their patches in rank order (fclaw2d_domain_serialization_enter/leave),
+// each turn separated by a collective barrier.  One rank writes the whole frame.
 void Context::output_ascii(int iframe, const std::string& dir) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "output before initialize");
-    if (partitioned()) throw Error(FCB_ERR_INVALID, "ASCII output of a partitioned solve is not available");
     if (iframe < 0 || iframe > 9999) throw Error(FCB_ERR_INVALID, "frame number must be in 0..9999");
     const size_t ps = patch_size();
-    const int n = num_patches();
+    const int n = own_count_;
     std::vector<double> host(ps * (size_t)n);
-    if (ps * (size_t)n > stage_cap_) {
-        cudaFree(d_stage_);
-        check(cudaMalloc(&d_stage_, ps * (size_t)n * sizeof(double)), "cudaMalloc stage");
-        stage_cap_ = ps * (size_t)n;
+    if (n > 0) {
+        if (ps * (size_t)n > stage_cap_) {
+            cudaFree(d_stage_);
+            check(cudaMalloc(&d_stage_, ps * (size_t)n * sizeof(double)), "cudaMalloc stage");
+            stage_cap_ = ps * (size_t)n;
+        }
+        // the clawpack 4.6 layout for both versions: the values per cell are the same
+        check(launch_gather(d_q_, stride_, d_all_slots_.p, n, (int64_t)ps, d_stage_, false, 0, st_), "gather");
+        ++cnt_.count_kernel_launches;
+        check(cudaMemcpyAsync(host.data(), d_stage_, host.size() * sizeof(double), cudaMemcpyDeviceToHost, st_),
+              "output");
+        synchronize();
     }
-    // the clawpack 4.6 layout for both versions: the values per cell are the same
-    check(launch_gather(d_q_, stride_, d_all_slots_.p, n, (int64_t)ps, d_stage_, false, 0, st_), "gather");
-    ++cnt_.count_kernel_launches;
-    check(cudaMemcpyAsync(host.data(), d_stage_, host.size() * sizeof(double), cudaMemcpyDeviceToHost, st_), "output");
-    synchronize();
     std::vector<OutputPatch> ps_out((size_t)n);
-    for (int p = 0; p < n; ++p) {
+    for (int k = 0; k < n; ++k) {
+        const int p = own_first_ + k;
         const PatchMeta m = meta_of(forest_.leaves[p]);
-        ps_out[p] = OutputPatch{p, (int)forest_.leaves[p].level, m.xlower, m.ylower, m.dx, m.dy};
+        ps_out[k] = OutputPatch{p, (int)forest_.leaves[p].level, m.xlower, m.ylower, m.dx, m.dy};
     }
-    try {
-        write_ascii_frame(dir, iframe, curr_time_, opt_.meqn, opt_.maux, opt_.mx, opt_.my, opt_.mbc, ps_out,
-                          host.data(), ps);
-    } catch (const std::runtime_error& e) {
-        throw Error(FCB_ERR_INVALID, e.what());
+    auto barrier = [&] {
+        if (!partitioned()) return;
+        check(cudaMemsetAsync(d_cfl_ + 2, 0, sizeof(unsigned long long), st_), "barrier");
+        comm_->allreduce_max_u64(d_cfl_ + 2, 1, st_);
+        comm_->sync(st_);
+    };
+    std::string err;
+    for (int r = 0; r < nranks_; ++r) {
+        if (r == rank_ && err.empty()) {
+            try {
+                if (r == 0)
+                    write_ascii_header(dir, iframe, curr_time_, opt_.meqn, opt_.maux, (long)num_patches());
+                append_ascii_patches(dir, iframe, opt_.meqn, opt_.mx, opt_.my, opt_.mbc, ps_out, host.data(), ps,
+                                     rank_);
+            } catch (const std::runtime_error& e) {
+                err = e.what();  // reported after the turns, so every rank takes every barrier
+            }
+        }
+        barrier();
     }
+    if (!err.empty()) throw Error(FCB_ERR_INVALID, err);
 }
 
 void Context::set_q(const double* host, size_t n) {

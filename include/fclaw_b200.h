@@ -272,12 +272,13 @@ int fcb_synchronize(fcb_context_t* ctx);
  *
  * Collective calls (all ranks, same order): fcb_initialize, fcb_run,
  * fcb_advance_all_levels, fcb_ghost_update, fcb_regrid,
- * fcb_conservation_check, fcb_global_maximum.  fcb_advance_all_levels returns
+ * fcb_conservation_check, fcb_global_maximum, fcb_output_ascii.  fcb_advance_all_levels returns
  * this rank's CFL maximum, as fclaw2d_advance_all_levels does; fcb_run takes
  * the global maximum itself (fclaw2d_run.c:206).  fcb_get_q / fcb_set_q /
  * fcb_get_qinterp move only the owned patches, at their places in the
- * all-leaves layout.  The macro-step graph is not used; fcb_output_ascii and
- * time-sync are rejected.  A failed rank marks the communicator failed, and
+ * all-leaves layout.  fcb_output_ascii is collective: rank 0 writes the
+ * header, then every rank appends its patches in rank order (mpi_rank in the
+ * grid headers).  The macro-step graph is not used; time-sync is rejected.  A failed rank marks the communicator failed, and
  * the others' next collective returns FCB_ERR_COMM. */
 typedef struct fcb_comm fcb_comm_t;
 /* nranks communicators of one in-process group: each rank's context is driven

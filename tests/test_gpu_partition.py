@@ -294,3 +294,46 @@ def test_partitioned_schedule_variants(gpu_lib, subcycle, weighted):
     opts.weighted_partition = weighted
     q_ref, q_all, _ = _stepped(opts, 3, steps=3, dt=0.9 / (8 * 32) / 1.5 / (1 if subcycle else 8), regrid=True)
     assert np.array_equal(q_all, q_ref)
+
+
+def test_partitioned_ascii_frame(gpu_lib, tmp_path):
+    """fcb_output_ascii of a 3-rank solve: the header from rank 0, then the
+    ranks' patches in rank order; equal to the one-rank frame apart from the
+    mpi_rank line of each grid header."""
+    import forestclaw_b200 as fcb
+
+    cfg = cases.radialdam_amr(seed=1, minlevel=2, maxlevel=4, mx=8)
+    opts = cases.to_options(cfg)
+    dt = 0.002
+    s = fcb.Solver(opts)
+    s.initialize()
+    s.advance_all_levels(0.0, dt)
+    (tmp_path / "one").mkdir()
+    (tmp_path / "three").mkdir()
+    s.output_ascii(7, str(tmp_path / "one"))
+
+    def rank(r, comm, stream):
+        d = fcb.Solver(opts, stream=stream, comm=comm)
+        d.initialize()
+        d.global_maximum(d.advance_all_levels(0.0, dt))
+        d.output_ascii(7, str(tmp_path / "three"))
+        return d.partition_info()
+
+    infos = _ranks(3, rank)
+    assert (tmp_path / "one" / "fort.t0007").read_text() == (tmp_path / "three" / "fort.t0007").read_text()
+    one = (tmp_path / "one" / "fort.q0007").read_text().split("\n")
+    three = (tmp_path / "three" / "fort.q0007").read_text().split("\n")
+    assert len(one) == len(three)
+    owner = {}
+    for i in infos:
+        for p in range(i["first"], i["first"] + i["count"]):
+            owner[p] = i["rank"]
+    grid = None
+    for a, b in zip(one, three):
+        if a.endswith("grid_number"):
+            grid = int(a.split()[0])
+        if a.endswith("mpi_rank"):
+            assert int(b.split()[0]) == owner[grid]
+        else:
+            assert a == b
+    assert len(set(owner.values())) == 3
