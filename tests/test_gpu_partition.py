@@ -337,3 +337,36 @@ def test_partitioned_ascii_frame(gpu_lib, tmp_path):
         else:
             assert a == b
     assert len(set(owner.values())) == 3
+
+
+def test_partitioned_state_io_and_patch_protocol(gpu_lib):
+    """set_q / get_q move only the owned patches at their places in the
+    all-leaves layout; the per-patch protocol (single_step_update) accepts a
+    rank's own patches and rejects the others'."""
+    import forestclaw_b200 as fcb
+
+    opts = cases.to_options(cases.swirl_uniform(level=3))
+    s = fcb.Solver(opts)
+    s.initialize()
+    q0 = s.get_q()
+    rng = np.random.default_rng(5)
+    q1 = q0 + rng.uniform(0.0, 1e-3, size=q0.shape)
+    out = np.full_like(q0, np.nan)
+
+    def rank(r, comm, stream):
+        d = fcb.Solver(opts, stream=stream, comm=comm)
+        d.initialize()
+        info = d.partition_info()
+        f, c = info["first"], info["count"]
+        d.set_q(q1)
+        d.get_q(out)
+        mine, other = f, (f + c) % d.num_patches
+        cfl = d.single_step_update(mine, 0.0, 0.001, 0, 1)
+        with pytest.raises(fcb.FcbError) as e:
+            d.single_step_update(other, 0.0, 0.001, 0, 1)
+        return cfl, e.value.code
+
+    res = _ranks(2, rank)
+    assert np.array_equal(out, q1)
+    for cfl, code in res:
+        assert cfl > 0.0 and code == 1
