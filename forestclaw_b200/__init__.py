@@ -22,7 +22,7 @@ import numpy as np
 __all__ = ["Options", "Solver", "Comm", "local_group", "nccl_unique_id", "nccl_comm", "partition_plan", "lib",
            "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
            "SOLVER_EULER4_ROE", "SOLVER_GEOCLAW_FWAVE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM",
-           "PROBLEM_QUADRANTS", "PROBLEM_BATHY", "PROBLEM_RADIALDAM_CELLAVE",
+           "PROBLEM_QUADRANTS", "PROBLEM_BATHY", "PROBLEM_RADIALDAM_CELLAVE", "PROBLEM_HUMP",
            "PRECISION_FP64", "PRECISION_MIXED", "measure_fp_rate",
            "TAG_VALUE", "TAG_MINMAX", "TAG_DIFFERENCE", "TAG_GRADIENT", "EXPORTED_SYMBOLS"]
 
@@ -31,6 +31,7 @@ LIBPATH = PKG / "libfclaw_b200.so"
 
 SOLVER_ADVECTION, SOLVER_SWE_ROE, SOLVER_EULER4_ROE, SOLVER_GEOCLAW_FWAVE = 0, 1, 2, 3
 PROBLEM_SWIRL, PROBLEM_RADIALDAM, PROBLEM_QUADRANTS, PROBLEM_BATHY, PROBLEM_RADIALDAM_CELLAVE = 0, 1, 2, 3, 4
+PROBLEM_HUMP = 5
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 TAG_VALUE, TAG_MINMAX, TAG_DIFFERENCE, TAG_GRADIENT = 0, 1, 2, 3
 

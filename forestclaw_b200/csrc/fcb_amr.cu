@@ -3,7 +3,8 @@
 // References:
 //   qinit:     applications/clawpack/advection/2d/swirl/user_4.6/qinit.f,
 //              applications/clawpack/euler/2d/quadrants/user_4.6/qinit.f,
-//              radial dam break (cell-centre test, as configured for this path)
+//              radial dam break (cell-centre test, as configured for this path),
+//              applications/clawpack/shallow/2d/bump/user_4.6/qinit.f (hump)
 //   tagging:   src/patches/clawpatch/fort_4.6/fclaw2d_clawpatch46_tag4refinement.f,
 //              fclaw2d_clawpatch46_tag4coarsening.f, fort_user/*_exceeds_th.f90.
 //              Every criterion's verdict is order independent (a running
@@ -177,6 +178,12 @@ __global__ void qinit_kernel(const QinitArgs a) {
             const double win = cellave2_d(dsc, mt.xlower + (i - 1.0) * mt.dx, mt.ylower + (j - 1.0) * mt.dy, mt.dx,
                                           mt.dy);
             q[((int64_t)0 * ny + r) * nx + c] = a.p[3] * win + a.p[4] * (1.0 - win);
+            q[((int64_t)1 * ny + r) * nx + c] = 0.0;
+            q[((int64_t)2 * ny + r) * nx + c] = 0.0;
+        } else if (a.problem == PROB_HUMP) {
+            // q(i,j,1) = 0.1d0 + exp(-200.d0*r2), r2 = (xc-x0)**2 + (yc-y0)**2
+            const double r2 = (xc - a.p[0]) * (xc - a.p[0]) + (yc - a.p[1]) * (yc - a.p[1]);
+            q[((int64_t)0 * ny + r) * nx + c] = a.p[2] + exp(-(a.p[3] * r2));
             q[((int64_t)1 * ny + r) * nx + c] = 0.0;
             q[((int64_t)2 * ny + r) * nx + c] = 0.0;
         } else if (a.problem == PROB_BATHY) {

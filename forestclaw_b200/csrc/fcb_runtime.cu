@@ -112,10 +112,11 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
     if (opt_.problem == FCB_PROBLEM_SWIRL && opt_.solver_kind != FCB_SOLVER_ADVECTION) bad("swirl needs advection");
     if (opt_.solver_kind == FCB_SOLVER_ADVECTION && opt_.problem != FCB_PROBLEM_SWIRL)
         bad("the advection solver takes its velocities from the swirl stream function");
-    if ((opt_.problem == FCB_PROBLEM_RADIALDAM || opt_.problem == FCB_PROBLEM_RADIALDAM_CELLAVE) &&
+    if ((opt_.problem == FCB_PROBLEM_RADIALDAM || opt_.problem == FCB_PROBLEM_RADIALDAM_CELLAVE ||
+         opt_.problem == FCB_PROBLEM_HUMP) &&
         opt_.solver_kind != FCB_SOLVER_SWE_ROE)
-        bad("radialdam needs SWE");
-    if (opt_.problem < FCB_PROBLEM_SWIRL || opt_.problem > FCB_PROBLEM_RADIALDAM_CELLAVE) bad("unknown problem");
+        bad("radialdam and hump need SWE");
+    if (opt_.problem < FCB_PROBLEM_SWIRL || opt_.problem > FCB_PROBLEM_HUMP) bad("unknown problem");
     if (opt_.ax == 0.0 && opt_.bx == 0.0 && opt_.ay == 0.0 && opt_.by == 0.0) {
         opt_.bx = 1.0;  // all four unset: the unit square
         opt_.by = 1.0;

@@ -61,9 +61,11 @@ enum fcb_problem {
     FCB_PROBLEM_QUADRANTS = 2,  /* euler/2d/quadrants qinit.f: p = rho[4], u[4], v[4], p[4], xs, ys */
     FCB_PROBLEM_BATHY = 3,      /* lake at rest over b = -1 + 0.8 exp(-((x-.5)^2+(y-.5)^2)/0.02)
                                  * with a surface pulse p[2] exp(-((x-p[0])^2+(y-p[1])^2)/p[3]^2) */
-    FCB_PROBLEM_RADIALDAM_CELLAVE = 4  /* the reference's radialdam qinit (radialdam/user_4.6/qinit.f):
+    FCB_PROBLEM_RADIALDAM_CELLAVE = 4, /* the reference's radialdam qinit (radialdam/user_4.6/qinit.f):
                                  * depth p[3]*w + p[4]*(1-w), w the fraction of the cell inside the
                                  * circle about (p[0], p[1]) of radius p[2] (cellave2.f) */
+    FCB_PROBLEM_HUMP = 5        /* shallow/2d/bump qinit (user_4.6/qinit.f, user_5.0/qinit.f90):
+                                 * depth p[2] + exp(-p[3]*r2), r2 = (xc-p[0])^2 + (yc-p[1])^2, at rest */
 };
 
 /* Refinement criteria (fclaw2d_clawpatch_options "refinement-criteria"). */

@@ -215,6 +215,10 @@ void Solver::qinit_patch(int p) {
             qinit_quadrants(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p),
                             opt.solver.gamma1, pp + 0, pp + 4, pp + 8, pp + 12, pp[16], pp[17], q);
             break;
+        case PROB_HUMP:
+            // pparams: x0, y0, base, coef
+            qinit_hump(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), pp[0], pp[1], pp[2], pp[3], q);
+            break;
         case PROB_BATHY:
             qinit_bathy(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), pp, q);
             break;

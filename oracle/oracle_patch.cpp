@@ -1147,6 +1147,21 @@ void qinit_radialdam(int mx, int my, int mbc, double xlower, double ylower, doub
     }
 }
 
+void qinit_hump(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double x0,
+                double y0, double base, double coef, double* q) {
+    const PatchIdx P(mx, my, mbc);
+    for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+        const double xc = xlower + (i - 0.5) * dx;
+        for (int j = 1 - mbc; j <= my + mbc; ++j) {
+            const double yc = ylower + (j - 0.5) * dy;
+            const double r2 = (xc - x0) * (xc - x0) + (yc - y0) * (yc - y0);
+            q[P(i, j, 0)] = base + std::exp(-(coef * r2));  // 0.1d0 + exp(-200.d0*r2)
+            q[P(i, j, 1)] = 0.0;
+            q[P(i, j, 2)] = 0.0;
+        }
+    }
+}
+
 void qinit_quadrants(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy,
                      double gamma1, const double* rpr, const double* rpu, const double* rpv,
                      const double* rpp, double xs, double ys, double* q) {

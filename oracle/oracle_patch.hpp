@@ -87,6 +87,13 @@ void setaux_bathy(int mx, int my, int mbc, double xlower, double ylower, double 
 void qinit_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, const double* p,
                  double* q);
 
+// shallow/2d/bump/user_4.6/qinit.f (user_5.0/qinit.f90 computes the same):
+// h = base + exp(-coef*r2), r2 = (xc-x0)**2 + (yc-y0)**2, hu = hv = 0 over the
+// whole patch, ghost cells included.  The reference has x0 = y0 = 0,
+// base = 0.1, coef = 200.
+void qinit_hump(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double x0,
+                double y0, double base, double coef, double* q);
+
 // swirl/user_4.6/b4step2.f (+ swirl/psi.f): time-dependent edge velocities.
 void b4step2_swirl(int mx, int my, int mbc, int maux, double xlower, double ylower,
                    double dx, double dy, double t, double dt, double tperiod, double* aux);

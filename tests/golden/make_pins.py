@@ -3,11 +3,12 @@
 The reference's regression tests pin three counters per run
 (src/fclaw2d_finalize.c:140-197): count_amr_advance, global_num_patches and
 count_amr_new_domain.  This script copies those numbers for the runs whose
-configuration lies on this path (swirl with clawpack 4.6 and 5, quadrants with
-clawpack 4.6, radialdam example 0 with clawpack 4.6 and time-sync), so the
-tests can check the oracle and the CUDA path without the reference tree.
+configuration lies on this path (swirl and quadrants with clawpack 4.6 and 5,
+bump with clawpack 4.6 and 5, radialdam example 0 with clawpack 4.6 and
+time-sync), so the tests can check the oracle and the CUDA path without the
+reference tree.
 
-Usage: python tests/golden/make_pins.py /path/to/reference
+Usage: python tests/golden/make_pins.py REFERENCE_ROOT
 """
 import csv
 import json
@@ -24,29 +25,25 @@ def read_csv(p: Path) -> dict:
     return out
 
 
+RUNS = {
+    "swirl": "applications/clawpack/advection/2d/swirl/regression_values_0.csv",
+    "swirl_claw5": "applications/clawpack/advection/2d/swirl/regression_values_1.csv",
+    "radialdam": "applications/clawpack/shallow/2d/radialdam/regression_values_0.csv",
+    "quadrants": "applications/clawpack/euler/2d/quadrants/regression_values_0.csv",
+    "quadrants_claw5": "applications/clawpack/euler/2d/quadrants/regression_values_1.csv",
+    "bump": "applications/clawpack/shallow/2d/bump/regression_values_0.csv",
+    "bump_claw5": "applications/clawpack/shallow/2d/bump/regression_values_1.csv",
+}
+
+
 def main(ref: Path):
-    pins = {
-        "swirl": {
-            "source": "applications/clawpack/advection/2d/swirl/regression_values_0.csv",
-            "values": read_csv(ref / "applications/clawpack/advection/2d/swirl/regression_values_0.csv"),
-        },
-        "swirl_claw5": {
-            "source": "applications/clawpack/advection/2d/swirl/regression_values_1.csv",
-            "values": read_csv(ref / "applications/clawpack/advection/2d/swirl/regression_values_1.csv"),
-        },
-        "radialdam": {
-            "source": "applications/clawpack/shallow/2d/radialdam/regression_values_0.csv",
-            "values": read_csv(ref / "applications/clawpack/shallow/2d/radialdam/regression_values_0.csv"),
-        },
-        "quadrants": {
-            "source": "applications/clawpack/euler/2d/quadrants/regression_values_0.csv",
-            "values": read_csv(ref / "applications/clawpack/euler/2d/quadrants/regression_values_0.csv"),
-        },
-    }
+    pins = {name: {"source": src, "values": read_csv(ref / src)} for name, src in RUNS.items()}
     out = Path(__file__).with_name("regression_pins.json")
     out.write_text(json.dumps(pins, indent=1) + "\n")
     print(out)
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    main(Path(sys.argv[1]))

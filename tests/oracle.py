@@ -20,7 +20,7 @@ ORACLE_DIR = ROOT / "oracle"
 # Solver kinds (oracle/oracle_patch.hpp SolverKind)
 ADVECTION, SWE_ROE, EULER4_ROE, GEOCLAW_FWAVE = 0, 1, 2, 3
 # Problems (oracle/oracle_amr.hpp Problem)
-SWIRL, RADIALDAM, QUADRANTS, BATHY, RADIALDAM_CELLAVE = 0, 1, 2, 3, 4
+SWIRL, RADIALDAM, QUADRANTS, BATHY, RADIALDAM_CELLAVE, HUMP = 0, 1, 2, 3, 4, 5
 # Tagging criteria (oracle/oracle_clawpatch.hpp TagCriteria)
 VALUE, MINMAX, DIFFERENCE, GRADIENT = 0, 1, 2, 3
 
@@ -117,29 +117,41 @@ class Config:
         return self.my + 2 * self.mbc
 
 
-_lib = None
+_libs = {}
 _lib_path = None
 
 
 def use_library(path):
     """Select another build of the oracle (e.g. the OpenMP timing build) before first use."""
-    global _lib_path, _lib
+    global _lib_path
     _lib_path = Path(path)
-    _lib = None
+    _libs.pop("plain", None)
 
 
-def lib():
-    """Load (building on first use if needed) the oracle shared library."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    if _lib_path is not None:
+def _build(target: str) -> Path:
+    so = ORACLE_DIR / target
+    srcs = list(ORACLE_DIR.glob("*.cpp")) + list(ORACLE_DIR.glob("*.hpp")) + [ORACLE_DIR / "Makefile"]
+    if not so.exists() or any(s.stat().st_mtime > so.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-s", target], cwd=ORACLE_DIR, check=True)
+    return so
+
+
+def lib(parallel: bool = False):
+    """Load (building on first use if needed) the oracle shared library.
+
+    parallel: the OpenMP build of the same arithmetic (liboracle_omp.so: same
+    compiler flags, the patches of a level updated by several threads), for
+    the checks at full configuration sizes; its results equal the plain
+    build's bit for bit."""
+    key = "omp" if parallel else "plain"
+    if key in _libs:
+        return _libs[key]
+    if parallel:
+        so = _build("liboracle_omp.so")
+    elif _lib_path is not None:
         so = _lib_path
     else:
-        so = ORACLE_DIR / "liboracle.so"
-        srcs = list(ORACLE_DIR.glob("*.cpp")) + list(ORACLE_DIR.glob("*.hpp"))
-        if not so.exists() or any(s.stat().st_mtime > so.stat().st_mtime for s in srcs):
-            subprocess.run(["make", "-s", "liboracle.so"], cwd=ORACLE_DIR, check=True)
+        so = _build("liboracle.so")
     L = ctypes.CDLL(str(so))
     assert L.orc_iopt_count() == len(_I_FIELDS), "oracle option layout changed"
     assert L.orc_dopt_count() == len(_D_FIELDS), "oracle option layout changed"
@@ -162,7 +174,7 @@ def lib():
     L.orc_conservation.argtypes = [ctypes.c_void_p, dp]
     L.orc_neighbors.argtypes = [ctypes.c_void_p, ctypes.c_int, ip]
     L.orc_step2.argtypes = [ip, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp]
-    _lib = L
+    _libs[key] = L
     return L
 
 
@@ -170,58 +182,60 @@ def _dptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-def _check(rc: int):
+def _check(rc: int, L=None):
     if rc != 0:
-        raise RuntimeError(lib().orc_last_error().decode())
+        raise RuntimeError((L or lib()).orc_last_error().decode())
 
 
 class OracleSolver:
-    """One CPU solve: forest + patch data + counters."""
+    """One CPU solve: forest + patch data + counters.  parallel=True runs the
+    OpenMP build of the same arithmetic (see lib())."""
 
-    def __init__(self, cfg: Config):
+    def __init__(self, cfg: Config, parallel: bool = False):
         self.cfg = cfg
+        self._L = lib(parallel)
         ia, da = cfg.arrays()
-        self._h = lib().orc_solver_new(ia, da)
+        self._h = self._L.orc_solver_new(ia, da)
         if not self._h:
-            raise RuntimeError(lib().orc_last_error().decode())
+            raise RuntimeError(self._L.orc_last_error().decode())
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().orc_solver_free(self._h)
+            self._L.orc_solver_free(self._h)
             self._h = None
 
     def initialize(self):
-        _check(lib().orc_initialize(self._h))
+        _check(self._L.orc_initialize(self._h), self._L)
 
     def run(self):
-        _check(lib().orc_run(self._h))
+        _check(self._L.orc_run(self._h))
 
     def advance(self, t: float, dt: float) -> float:
         c = ctypes.c_double()
-        _check(lib().orc_advance(self._h, t, dt, ctypes.byref(c)))
+        _check(self._L.orc_advance(self._h, t, dt, ctypes.byref(c)))
         return c.value
 
     def update_single_step(self, level: int, t: float, dt: float) -> float:
         c = ctypes.c_double()
-        _check(lib().orc_update_single_step(self._h, level, t, dt, ctypes.byref(c)))
+        _check(self._L.orc_update_single_step(self._h, level, t, dt, ctypes.byref(c)))
         return c.value
 
     def timeinterp(self, level: int, alpha: float):
-        _check(lib().orc_timeinterp_level(self._h, level, alpha))
+        _check(self._L.orc_timeinterp_level(self._h, level, alpha))
 
     def ghost_update(self, minlevel: int, maxlevel: int, t: float = 0.0, time_interp: int = 0):
-        _check(lib().orc_ghost_update(self._h, minlevel, maxlevel, t, time_interp))
+        _check(self._L.orc_ghost_update(self._h, minlevel, maxlevel, t, time_interp))
 
     def regrid(self):
-        _check(lib().orc_regrid(self._h))
+        _check(self._L.orc_regrid(self._h))
 
     @property
     def num_patches(self) -> int:
-        return lib().orc_num_patches(self._h)
+        return self._L.orc_num_patches(self._h)
 
     def patch_info(self, p: int):
         lv, x, y = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        lib().orc_patch_info(self._h, p, ctypes.byref(lv), ctypes.byref(x), ctypes.byref(y))
+        self._L.orc_patch_info(self._h, p, ctypes.byref(lv), ctypes.byref(x), ctypes.byref(y))
         return lv.value, x.value, y.value
 
     def leaves(self):
@@ -230,13 +244,13 @@ class OracleSolver:
     def q(self, p: int) -> np.ndarray:
         c = self.cfg
         out = np.empty((c.meqn, c.ny, c.nx), dtype=np.float64)
-        lib().orc_get_q(self._h, p, _dptr(out))
+        self._L.orc_get_q(self._h, p, _dptr(out))
         return out
 
     def qinterp(self, p: int) -> np.ndarray:
         c = self.cfg
         out = np.empty((c.meqn, c.ny, c.nx), dtype=np.float64)
-        lib().orc_get_qinterp(self._h, p, _dptr(out))
+        self._L.orc_get_qinterp(self._h, p, _dptr(out))
         return out
 
     def all_q(self) -> np.ndarray:
@@ -244,22 +258,22 @@ class OracleSolver:
 
     def set_q(self, p: int, q: np.ndarray):
         a = np.ascontiguousarray(q, dtype=np.float64)
-        lib().orc_set_q(self._h, p, _dptr(a))
+        self._L.orc_set_q(self._h, p, _dptr(a))
 
     def counters(self):
         a = (ctypes.c_longlong * 4)()
-        lib().orc_counters(self._h, a)
+        self._L.orc_counters(self._h, a)
         return {"count_amr_advance": a[0], "count_amr_new_domain": a[1],
                 "count_amr_regrid": a[2], "count_single_step": a[3]}
 
     def conservation(self) -> np.ndarray:
         out = np.zeros(self.cfg.meqn)
-        lib().orc_conservation(self._h, _dptr(out))
+        self._L.orc_conservation(self._h, _dptr(out))
         return out
 
     def neighbors(self, p: int):
         a = (ctypes.c_int * 22)()
-        lib().orc_neighbors(self._h, p, a)
+        self._L.orc_neighbors(self._h, p, a)
         return list(a)
 
 
@@ -297,6 +311,23 @@ def radialdam_regression(claw_version: int = 4) -> Config:
                   extent=(-2.5, 2.5, -2.5, 2.5))
 
 
+def bump_regression(claw_version: int = 4) -> Config:
+    """applications/clawpack/shallow/2d/bump/regression.ini on top of that
+    directory's fclaw_options.ini (read first), which sets refinement-criteria =
+    minmax: unmapped [-2.5, 2.5]^2, mx = 8, levels 4-6, smooth-level 4,
+    h = 0.1 + exp(-200 r^2) about the origin (user_4.6/qinit.f), shallow-water
+    Roe solver, g = 1.  The clawpack 4.6 run has extrapolation boundaries
+    ([clawpack46] mthbc = 1 1 1 1), the clawpack 5 run solid walls
+    ([clawpack5] mthbc = 3 3 3 3)."""
+    return Config(mx=8, my=8, mbc=2, meqn=3, maux=0, order=(2, 2), mwaves=3, mthlim=(4, 4, 4),
+                  mthbc=(1, 1, 1, 1) if claw_version == 4 else (3, 3, 3, 3), minlevel=4, maxlevel=6,
+                  regrid_interval=1, refine_threshold=0.05, coarsen_threshold=0.005, smooth_refine=1,
+                  smooth_level=4, tfinal=1.0, initial_dt=2.5e-2, max_cfl=1.0, desired_cfl=0.9, nout=1,
+                  subcycle=1, solver=SWE_ROE, problem=HUMP, criteria=MINMAX, grav=1.0,
+                  pparams=(0.0, 0.0, 0.1, 200.0), claw_version=claw_version,
+                  extent=(-2.5, 2.5, -2.5, 2.5))
+
+
 QUADRANT_STATES = (
     # rho, u, v, p for quadrants 1..4 (euler/2d/quadrants/user_4.6/qinit.f)
     (1.5, 0.0, 0.0, 1.5),
@@ -314,13 +345,14 @@ def quadrants_params(states=QUADRANT_STATES, xs=0.8, ys=0.8):
     return tuple(rho + u + v + p + [xs, ys])
 
 
-def quadrants_regression() -> Config:
+def quadrants_regression(claw_version: int = 4) -> Config:
     """applications/clawpack/euler/2d/quadrants/regression.ini on top of that directory's
     fclaw_options.ini, which the application reads first from its working directory
-    (fclaw_base.c:758-786); that file sets refinement-criteria = difference."""
+    (fclaw_base.c:758-786); that file sets refinement-criteria = difference.  The
+    [clawpack46] and [clawpack5] sections agree (extrapolation boundaries)."""
     return Config(mx=8, my=8, mbc=2, meqn=4, maux=0, order=(2, 2), mwaves=4, mthlim=(4, 4, 4, 4),
                   mthbc=(1, 1, 1, 1), minlevel=0, maxlevel=5, regrid_interval=1,
                   refine_threshold=0.25, coarsen_threshold=0.025, smooth_refine=1, smooth_level=5,
                   tfinal=0.1, initial_dt=0.05, max_cfl=1.0, desired_cfl=0.9, nout=1,
                   subcycle=1, solver=EULER4_ROE, problem=QUADRANTS, criteria=DIFFERENCE, gamma=1.4,
-                  pparams=quadrants_params())
+                  pparams=quadrants_params(), claw_version=claw_version)

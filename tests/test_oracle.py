@@ -12,14 +12,23 @@ import oracle as O
 PINS = json.loads((Path(__file__).parent / "golden" / "regression_pins.json").read_text())
 
 
-@pytest.mark.parametrize("name", ["swirl", "swirl_claw5", "quadrants", "radialdam"])
+PIN_CONFIGS = {
+    "swirl": O.swirl_regression, "swirl_claw5": lambda: O.swirl_regression(5),
+    "quadrants": O.quadrants_regression, "quadrants_claw5": lambda: O.quadrants_regression(5),
+    "radialdam": O.radialdam_regression,
+    "bump": O.bump_regression, "bump_claw5": lambda: O.bump_regression(5),
+}
+
+
+@pytest.mark.parametrize("name", sorted(PIN_CONFIGS))
 def test_regression_pins(name):
     """applications/**/regression_values_{0,1}.csv: count_amr_advance,
-    global_num_patches and count_amr_new_domain of the clawpack 4.6 runs, of
-    the swirl run with --user:claw-version=5, and of the radialdam run
-    (time-sync, cellave2 initial depth, gradient tagging on [-2.5, 2.5]^2)."""
-    cfg = {"swirl": O.swirl_regression, "swirl_claw5": lambda: O.swirl_regression(5),
-           "quadrants": O.quadrants_regression, "radialdam": O.radialdam_regression}[name]()
+    global_num_patches and count_amr_new_domain of the clawpack 4.6 runs and
+    the --user:claw-version=5 runs of swirl, quadrants and bump (bump's
+    clawpack 5 run has solid walls on all four sides, 14 new domains in 24
+    advances), and of the radialdam run (time-sync, cellave2 initial depth,
+    gradient tagging on [-2.5, 2.5]^2)."""
+    cfg = PIN_CONFIGS[name]()
     s = O.OracleSolver(cfg)
     s.initialize()
     s.run()
