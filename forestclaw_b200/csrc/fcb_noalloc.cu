@@ -37,7 +37,10 @@ static __device__ __align__(256) double g_patch_sums[kMaxPatchSums];
 
 // Host-side device address of g_patch_sums for each device, found once per
 // device with that device current.  The symbol's name in host code is only a
-// stand-in and must never be handed to a kernel.
+// stand-in and must never be handed to a kernel.  The address is kept for the
+// life of the process: a cudaDeviceReset tears down the context that owns it,
+// after which it would be stale, so a caller must not reset a device it has
+// used this entry point on.
 double* g_scratch_ptr[kMaxDevices] = {nullptr};
 std::mutex g_setup_mutex;
 

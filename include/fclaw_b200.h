@@ -228,9 +228,11 @@ int fcb_conservation_check(fcb_context_t* ctx, double* sums);
  * Per-patch partial sums live in a fixed array of 262,144 doubles (2 MiB)
  * inside the library, held by every GPU that loads it; npatches*meqn above
  * that is rejected with FCB_ERR_INVALID.  The first call on each device looks
- * up that array's address, so make it before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race and must be serialised
- * by the caller. */
+ * up that array's address, so make it before any stream capture; the address
+ * is kept for the life of the process, so a cudaDeviceReset of that device
+ * between calls leaves it stale (do not reset a device this entry point has
+ * used).  All calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller. */
 int fcb_conservation_sum_noalloc(const double* d_q, size_t patch_stride, int npatches, int mx, int my, int mbc,
                                  int meqn, const double* d_area, double* d_sums, void* cuda_stream);
 /* Current time of the run loop. */
