@@ -51,8 +51,13 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="uniform_swirl",
                    choices=["uniform_swirl", "amr_radialdam", "amr_quadrants", "bathy", "serve"])
-    p.add_argument("--requests", type=int, default=24, help="serve: number of requests")
-    p.add_argument("--rates", default="5,20,80", help="serve: Poisson arrival rates (requests/s) to sweep")
+    p.add_argument("--requests", type=int, default=200, help="serve: number of requests")
+    p.add_argument("--rates", default="2,5,10,20,40", help="serve: Poisson arrival rates (requests/s) to sweep")
+    p.add_argument("--serve-maxlevels", default="4,5,6,7", help="serve: maxlevel drawn uniformly from these")
+    p.add_argument("--serve-tfinal", default="0.2,1.0", help="serve: final time ~ U(a, b)")
+    p.add_argument("--extras", type=int, default=1,
+                   help="default workload: 1 also measures the other configurations (sub-objects of the line)")
+    p.add_argument("--extra-requests", type=int, default=48, help="requests of the serving sub-object (0: skip)")
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--mx", type=int, default=16)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
@@ -131,17 +136,18 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-# DRAM bytes (read + write) per step-kernel launch from the ncu captures
-# summarised in profiles/ (same workload, same kernel build).
-_TRAFFIC = {("fp64", 8, 16): (356.85e6, "profiles/step_kernel_uniform_swirl_l8_mx16.md"),
-            ("mixed", 8, 16): (357.08e6, "profiles/step_kernel_mixed_uniform_swirl_l8_mx16.md")}
+# DRAM bytes (read + write) per step-kernel launch, dram__bytes_read.sum +
+# dram__bytes_write.sum from an ncu capture of the same kernel on the same
+# workload (level 8, mx = 16), keyed by (precision, level, mx, fused step).
+_TRAFFIC = {("fp64", 8, 16, False): 356.85e6, ("mixed", 8, 16, False): 357.08e6}
 
 
-def _profiled_traffic(args):
-    t = _TRAFFIC.get((args.precision, args.level, args.mx))
+def _profiled_traffic(args, fused):
+    t = _TRAFFIC.get((args.precision, args.level, args.mx, bool(fused)))
     if t is None or args.step_variant not in (0, 3):
         return None
-    return {"bytes_per_launch": t[0], "source": t[1]}
+    return {"bytes_per_launch": t, "source": "ncu capture of this kernel on this workload "
+                                             "(dram__bytes_read.sum + dram__bytes_write.sum)"}
 
 
 def peaks():
@@ -178,6 +184,24 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
+def oracle_config(o):
+    """The oracle's configuration of a solve given by fcb Options (the CPU
+    restatement runs the same options)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle as O
+
+    return O.Config(mx=o.mx, my=o.my, mbc=o.mbc, meqn=o.meqn, maux=o.maux, order=tuple(o.order), mcapa=o.mcapa,
+                    mwaves=o.mwaves, mthlim=tuple(o.mthlim), mthbc=tuple(o.mthbc), minlevel=o.minlevel,
+                    maxlevel=o.maxlevel, subcycle=o.subcycle, regrid_interval=o.regrid_interval,
+                    smooth_refine=o.smooth_refine, smooth_level=o.smooth_level, criteria=o.refinement_criteria,
+                    ivar=o.threshold_variable - 1, use_fixed_dt=o.use_fixed_dt, nout=o.nout,
+                    init_ghostcell=o.init_ghostcell, reduce_cfl=o.reduce_cfl, solver=o.solver_kind,
+                    problem=o.problem, refine_threshold=o.refine_threshold, coarsen_threshold=o.coarsen_threshold,
+                    tfinal=o.tfinal, initial_dt=o.initial_dt, max_cfl=o.max_cfl, desired_cfl=o.desired_cfl,
+                    grav=o.grav, gamma=o.gamma, pparams=tuple(o.problem_params), claw_version=o.claw_version,
+                    drytol=o.dry_tolerance, time_sync=o.time_sync, extent=tuple(o.extent))
+
+
 def time_oracle(cfg, dt, steps, warmup):
     """Advance the oracle `warmup` + `steps` steps; returns (seconds for `steps`, cell updates)."""
     sys.path.insert(0, str(ROOT / "tests"))
@@ -201,10 +225,10 @@ def time_oracle(cfg, dt, steps, warmup):
 
 
 def cpu_sample(args, budget_s):
-    import cases
+    from forestclaw_b200 import workloads
 
-    cfg = cases.swirl_uniform(level=args.level, mx=args.mx)
-    dt = cases.swirl_dt(level=args.level, mx=args.mx)
+    cfg = oracle_config(workloads.uniform_swirl(args.level, args.mx))
+    dt = workloads.swirl_dt(args.level, args.mx)
     el1, _ = time_oracle(cfg, dt, 1, 0)
     steps = max(1, int(budget_s / max(el1, 1e-3)))
     el, cells = time_oracle(cfg, dt, steps, 1)
@@ -218,10 +242,10 @@ def cpu_sample(args, budget_s):
 def run_reference(args, rank, world):
     if rank != 0:
         return None
-    import cases
+    from forestclaw_b200 import workloads
 
-    cfg = cases.swirl_uniform(level=args.level, mx=args.mx)
-    dt = cases.swirl_dt(level=args.level, mx=args.mx)
+    cfg = oracle_config(workloads.uniform_swirl(args.level, args.mx))
+    dt = workloads.swirl_dt(args.level, args.mx)
     el, cells = time_oracle(cfg, dt, args.steps, args.warmup)
     v = cells / el
     line = {
@@ -287,23 +311,22 @@ def run_ours(args, rank, world, local_rank):
     cells = (c1["count_single_step"] - c0["count_single_step"]) * args.mx * args.mx
     ms_max, total_cells = replicas.aggregate(ms, cells, torch.distributed if dist else None)
 
-    # --- step-kernel alone: K launches of the level update between events ---
+    # --- the step kernel alone: the launch an advance makes (the ghost-exchange
+    # fused step when the tuner chose it), K launches on scratch copies of the
+    # arrays between CUDA events on the solve's stream; with the unfused form
+    # the ghost fill is timed apart ---
     nk = max(5, args.steps)
-    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    k0.record(stream)
-    for _ in range(nk):
-        s.update_single_step_async(args.level, t, dt)
-    k1.record(stream)
-    torch.cuda.synchronize()
-    step_ms = k0.elapsed_time(k1) / nk
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    for _ in range(nk):
-        s.ghost_update(args.level, args.level, t, 0)
-    g1.record(stream)
-    torch.cuda.synchronize()
-    ghost_ms = g0.elapsed_time(g1) / nk
+    step_ms, fused = s.step_kernel_time(t, dt, nk)
+    ghost_ms = None
+    if not fused:
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        g0.record(stream)
+        for _ in range(nk):
+            s.ghost_update(args.level, args.level, t, 0)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        ghost_ms = g0.elapsed_time(g1) / nk
 
     # --- end to end through the C ABI with host buffers: upload the state from
     # pinned host memory, advance K steps (host dt in, CFL out each step),
@@ -344,7 +367,11 @@ def run_ours(args, rank, world, local_rank):
                                + ("FP64 plain" if args.precision == "fp64" else "mixed FP32/FP64"),
                    "patches": npatch, "cells": cells_per_step, "l2_flush": "inputs larger than L2",
                    "parallelism": f"{world} independent replicas" if world > 1 else "single GPU",
-                   "step_kernel_ms": step_ms, "ghost_fill_ms": ghost_ms},
+                   "step_kernel_ms": step_ms, "ghost_fill_ms": ghost_ms,
+                   "ghost_fill": "fused into the step (neighbour reads)" if fused else "separate launch",
+                   "e2e_state_transfer": f"the whole state uploaded once and downloaded once per {args.steps} "
+                                         "steps (the arrays stay resident between steps), so e2e grows "
+                                         "with --steps"},
         "clocks": clk.summary(),
         "e2e": {"value": total_cells / (e2e_ms * 1e-3),
                 "unit": "cell-updates/s",
@@ -352,9 +379,10 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": state_bytes / args.steps + 8},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": _profiled_traffic(args),
+                     "frac": achieved / hbm, "traffic": _profiled_traffic(args, fused),
                      "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback",
-                     "bytes_per_cell": bytes_per_cell, "kernel": "step_kernel"},
+                     "bytes_per_cell": bytes_per_cell,
+                     "kernel": "step_kernel_pipe (ghost-exchange fused)" if fused else "step kernel"},
         "roofline_fp": fp_roofline("advection_swirl_order22", args.mx, cells_per_step / (step_ms * 1e-3),
                                    args.precision, stream.cuda_stream),
     }
@@ -525,50 +553,58 @@ def fp_roofline(case, mx, cells_per_s, precision, stream):
 
 
 # ----------------------------------------------------------------------------
-# AMR shallow water: dam break, Roe solver, levels 3..6, mx = 32, subcycling,
-# gradient tagging, regrid after every macro step, adaptive dt
+# AMR workloads: shallow water (levels 3-6, mx 32), Euler quadrants (levels
+# 2-7), shallow water over bathymetry (levels 4-7, mx 32).  One "step" is one
+# macro step (fcb_advance_all_levels) followed by a regrid; the advance phase
+# is timed with CUDA events on the solve's stream, the regrid on the host clock.
 # ----------------------------------------------------------------------------
-def _amr_cfg(seed=0, workload="amr_radialdam", mx=32):
-    """amr_radialdam: shallow water, levels 3-6, mx 32; amr_quadrants: Euler
-    quadrants, levels 2-7, mx from --mx (8, 16, 32 or 64)."""
-    sys.path.insert(0, str(ROOT / "tests"))
-    import cases
+def _amr_options(workload, mx, precision):
+    import forestclaw_b200 as fcb
+    from forestclaw_b200 import workloads
 
     if workload == "amr_quadrants":
-        return cases.quadrants_amr(seed=seed, minlevel=2, maxlevel=7, mx=mx)
-    return cases.radialdam_amr(seed=seed, minlevel=3, maxlevel=6, mx=32)
+        o = workloads.amr_euler(seed=0, mx=mx)
+    elif workload == "bathy":
+        o = workloads.bathymetry(seed=0)
+    else:
+        o = workloads.amr_shallow_water(seed=0)
+    o.precision = fcb.PRECISION_MIXED if precision == "mixed" else fcb.PRECISION_FP64
+    return o
 
 
-def _next_dt(dt, cfl, cfg):
-    # fclaw2d_run: dt_new = dt * desired_cfl / cfl
-    return dt * cfg.desired_cfl / cfl if cfl > 0 else dt
+def _next_dt(dt, cfl, o):
+    # fclaw2d_run: dt_new = dt * desired_cfl / cfl (fixed dt when use_fixed_dt)
+    if o.use_fixed_dt:
+        return dt
+    return dt * o.desired_cfl / cfl if cfl > 0 else dt
 
 
-def run_amr(args, rank, world, local_rank):
+def _first_dt(o):
+    from forestclaw_b200 import workloads
+
+    return workloads.bathymetry_dt(o.minlevel, o.mx) if o.problem == 3 else o.initial_dt
+
+
+def amr_measure(opts, steps, warmup, stream, local_rank, keep=False):
+    """Warm-up macro steps (plans, tuned forms, the macro-step graph), then
+    `steps` timed ones; every macro step is followed by a regrid."""
     import torch
 
-    import cases
     import forestclaw_b200 as fcb
 
-    torch.cuda.set_device(local_rank)
-    stream = torch.cuda.current_stream()
-    cfg = _amr_cfg(workload=args.workload, mx=args.mx)
-    opts = cases.to_options(cfg)
-    opts.precision = fcb.PRECISION_MIXED if args.precision == "mixed" else fcb.PRECISION_FP64
-    opts.macro_graph = args.macro_graph
     s = fcb.Solver(opts, stream=stream.cuda_stream)
     s.initialize()
-    t, dt = 0.0, cfg.initial_dt
-    for _ in range(args.warmup):
+    t, dt = 0.0, _first_dt(opts)
+    for _ in range(warmup):
         cfl = s.advance_all_levels(t, dt)
         t += dt
         s.regrid()
-        dt = _next_dt(dt, cfl, cfg)
+        dt = _next_dt(dt, cfl, opts)
     torch.cuda.synchronize()
     c0 = s.counters()
     adv_ms, reg_s, patches = 0.0, 0.0, []
     with ClockSampler(local_rank) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             cfl = s.advance_all_levels(t, dt)
@@ -581,52 +617,84 @@ def run_amr(args, rank, world, local_rank):
             torch.cuda.synchronize()
             reg_s += time.perf_counter() - r0
             patches.append(s.num_patches)
-            dt = _next_dt(dt, cfl, cfg)
+            dt = _next_dt(dt, cfl, opts)
     c1 = s.counters()
-    cells = (c1["count_single_step"] - c0["count_single_step"]) * cfg.mx * cfg.my
+    cells = (c1["count_single_step"] - c0["count_single_step"]) * opts.mx * opts.my
+    out = {"value": cells / (adv_ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": adv_ms / steps,
+           "steps": steps, "warmup": warmup, "cell_updates": cells,
+           "patches_min": min(patches), "patches_max": max(patches),
+           "regrid_ms_per_step": reg_s * 1e3 / steps,
+           "graph_replays": c1["count_graph_replays"] - c0["count_graph_replays"],
+           "gpu_launches": c1["count_kernel_launches"] - c0["count_kernel_launches"],
+           "clocks": clk.summary()}
+    if keep:
+        out["solver"] = s
+    else:
+        s.close()
+    return out
+
+
+def _fp_case(opts):
+    return {1: "swe_roe_order22", 2: "euler4_roe_order22", 3: "geoclaw_fwave_order20",
+            0: "advection_swirl_order22"}[opts.solver_kind]
+
+
+def _bytes_per_cell(opts):
+    # ghosted read + interior write of the state, plus the stored aux read
+    r = (opts.mx + 2 * opts.mbc) ** 2 / (opts.mx * opts.my)
+    aux = opts.maux if opts.solver_kind == 3 else 0
+    return 8.0 * (opts.meqn * (1.0 + r) + aux * r)
+
+
+def run_amr(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.current_stream()
+    opts = _amr_options(args.workload, args.mx, args.precision)
+    opts.macro_graph = args.macro_graph
+    m = amr_measure(opts, args.steps, args.warmup, stream, local_rank)
     if rank != 0:
         return None
     hbm, src = peaks()
-    # 8*meqn*(1 + (mx+4)^2/mx^2): ghosted read + interior write
-    bytes_per_cell = 8.0 * cfg.meqn * (1.0 + (cfg.mx + 4) ** 2 / cfg.mx ** 2)
-    euler = args.workload == "amr_quadrants"
-    achieved = cells * bytes_per_cell / (adv_ms * 1e-3) / 1e9
+    bpc = _bytes_per_cell(opts)
+    achieved = m["value"] * bpc / 1e9
+    name = {"amr_quadrants": f"AMR Euler quadrants, Roe, levels 2-7, mx=my={opts.mx}, subcycled",
+            "bathy": "shallow water over bathymetry (GeoClaw f-waves), lake at rest + pulse 1e-3, levels 4-7, "
+                     "mx=my=32, subcycled",
+            }.get(args.workload, "AMR shallow-water dam break, Roe, levels 3-6, mx=my=32, subcycled")
     line = {
-        "metric": "cell-updates/s", "value": cells / (adv_ms * 1e-3), "unit": "cell-updates/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": adv_ms / args.steps,
+        "metric": "cell-updates/s", "value": m["value"], "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
-        "config": {"workload": (f"AMR Euler quadrants, Roe, levels 2-7, mx=my={cfg.mx}, subcycled, "
-                                if euler else "AMR shallow-water dam break, Roe, levels 3-6, mx=my=32, subcycled, ")
-                               + 
-                               "regrid every macro step (advance phase timed; regrid reported apart)",
-                   "patches_min": min(patches), "patches_max": max(patches),
-                   "regrid_ms_per_step": reg_s * 1e3 / args.steps, "macro_graph": args.macro_graph,
-                   "graph_replays": c1["count_graph_replays"] - c0["count_graph_replays"],
-                   "launches_per_step": (c1["count_kernel_launches"] - c0["count_kernel_launches"]) / args.steps},
-        "clocks": clk.summary(),
-        "gpu_launches": c1["count_kernel_launches"] - c0["count_kernel_launches"],
+        "config": {"workload": name + ", regrid every macro step (advance phase timed; regrid reported apart)",
+                   "patches_min": m["patches_min"], "patches_max": m["patches_max"],
+                   "regrid_ms_per_step": m["regrid_ms_per_step"], "macro_graph": args.macro_graph,
+                   "graph_replays": m["graph_replays"]},
+        "clocks": m["clocks"],
+        "gpu_launches": m["gpu_launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "bytes_per_cell": bytes_per_cell, "kernel": "advance phase (all kernels)",
+                     "traffic": None, "bytes_per_cell": bpc, "kernel": "advance phase (all kernels)",
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback"},
-        "roofline_fp": fp_roofline("euler4_roe_order22" if euler else "swe_roe_order22", cfg.mx,
-                                   cells / (adv_ms * 1e-3), args.precision,
-                                   stream.cuda_stream),
+        "roofline_fp": fp_roofline(_fp_case(opts), opts.mx, m["value"], args.precision, stream.cuda_stream),
     }
+    if args.workload == "bathy" and args.precision == "mixed":
+        line["config"]["accuracy"] = bathy_accuracy(args.steps, args.macro_graph, stream)
     if world == 1:
-        line["cpu_baseline"] = amr_cpu_sample(args.cpu_seconds, cfg)
-    s.close()
+        line["cpu_baseline"] = amr_cpu_sample(args.cpu_seconds, opts)
     return line
 
 
-def amr_cpu_sample(budget_s, cfg):
+def amr_cpu_sample(budget_s, opts):
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle as O
 
     O.use_library(native_oracle())
+    cfg = oracle_config(opts)
     o = O.OracleSolver(cfg)
     o.initialize()
-    t, dt, el, cells, n = 0.0, cfg.initial_dt, 0.0, 0, 0
+    t, dt, el, cells, n = 0.0, _first_dt(opts), 0.0, 0, 0
     while el < budget_s and n < 50:
         c0 = o.counters()["count_single_step"]
         t0 = time.perf_counter()
@@ -635,207 +703,250 @@ def amr_cpu_sample(budget_s, cfg):
         cells += (o.counters()["count_single_step"] - c0) * cfg.mx * cfg.my
         t += dt
         o.regrid()
-        dt = _next_dt(dt, cfl, cfg)
+        dt = _next_dt(dt, cfl, opts)
         n += 1
     return {"value": cells / el, "unit": "cell-updates/s", "cores": cpu_threads(), "kind": "port",
             "sample": f"first {n} macro steps of the same AMR run (advance phase, {el:.2f} s), C++ restatement "
                       f"of the reference, OpenMP over the patches of each level"}
 
 
-# ----------------------------------------------------------------------------
-# Shallow water over bathymetry (GeoClaw f-waves): lake at rest over a Gaussian
-# bump plus a surface pulse, levels 4..7, mx = 32, subcycled, gradient tagging,
-# regrid every macro step, fixed dt.  --precision mixed also reports the error
-# against the same run in FP64, the mass drift and the lake-at-rest residual.
-# ----------------------------------------------------------------------------
-def _bathy_cfg(amp=1e-3):
-    import cases
-
-    return cases.bathy_lake(minlevel=4, maxlevel=7, mx=32, seed=0, amp=amp, width=0.05)
-
-
-def _bathy_dt():
-    return 0.5 / (32 * 16)  # CFL about 0.5 on level 4 (|u| + sqrt(g h) <= 1)
-
-
-def _bathy_run(opts, steps, t0=0.0, stream=None, timed=False):
-    """advance + regrid `steps` times; returns (solver, advance ms, cells, patch
-    counts); the solver's `bench_launches` holds the launches of the advances."""
-    import torch
-
+def bathy_accuracy(steps, macro_graph, stream):
+    """The mixed form of the bathymetry run against the same run in FP64 after
+    `steps` macro steps with regrids: relative L1 and max error of the interior
+    cells, mass drift, and the lake at rest (no pulse) after the same steps."""
     import forestclaw_b200 as fcb
+    from forestclaw_b200 import workloads
 
-    s = fcb.Solver(opts, stream=stream.cuda_stream if stream is not None else 0)
-    s.initialize()
-    t, dt, ms, cells, patches = t0, _bathy_dt(), 0.0, 0, []
-    s.bench_launches = 0
+    def run(o):
+        s = fcb.Solver(o, stream=stream.cuda_stream)
+        s.initialize()
+        t, dt = 0.0, workloads.bathymetry_dt(o.minlevel, o.mx)
+        for _ in range(steps):
+            s.advance_all_levels(t, dt)
+            t += dt
+            if o.regrid_interval:
+                s.regrid()
+        return s
+
+    res = {}
+    for prec in (fcb.PRECISION_MIXED, fcb.PRECISION_FP64):
+        o = workloads.bathymetry(seed=0)
+        o.precision, o.macro_graph = prec, macro_graph
+        res[prec] = run(o)
+    sm, sf = res[fcb.PRECISION_MIXED], res[fcb.PRECISION_FP64]
+    acc = {"against": f"the same run in FP64 on the GPU after {steps} macro steps with regrids",
+           "same_mesh": sm.leaves() == sf.leaves()}
+    if acc["same_mesh"]:
+        qm, qf = sm.get_q(), sf.get_q()
+        a, b = qm[..., 2:-2, 2:-2], qf[..., 2:-2, 2:-2]
+        acc["l1_rel"] = float(np.abs(a - b).sum() / np.abs(b).sum())
+        acc["max_rel"] = float(np.abs(a - b).max() / max(1.0, np.abs(b).max()))
+        mm, mf = np.asarray(sm.conservation_check()), np.asarray(sf.conservation_check())
+        acc["mass_drift_rel"] = float(np.max(np.abs(mm - mf)) / np.max(np.abs(mf)))
+    sm.close()
+    sf.close()
+    lake = workloads.bathymetry(seed=0, amp=0.0)
+    lake.precision, lake.macro_graph, lake.regrid_interval = fcb.PRECISION_MIXED, macro_graph, 0
+    ls = fcb.Solver(lake, stream=stream.cuda_stream)
+    ls.initialize()
+    q0 = ls.get_q()
+    t, dt = 0.0, workloads.bathymetry_dt(lake.minlevel, lake.mx)
     for _ in range(steps):
-        c = s.counters()
-        c0, l0 = c["count_single_step"], c["count_kernel_launches"]
-        if timed:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-        s.advance_all_levels(t, dt)
-        if timed:
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms += e0.elapsed_time(e1)
-        c = s.counters()
-        cells += (c["count_single_step"] - c0) * opts.mx * opts.my
-        s.bench_launches += c["count_kernel_launches"] - l0
+        ls.advance_all_levels(t, dt)
         t += dt
-        s.regrid()
-        patches.append(s.num_patches)
-    torch.cuda.synchronize()
-    return s, ms, cells, patches
-
-
-def run_bathy(args, rank, world, local_rank):
-    import numpy as np
-    import torch
-
-    import cases
-    import forestclaw_b200 as fcb
-
-    torch.cuda.set_device(local_rank)
-    stream = torch.cuda.current_stream()
-    cfg = _bathy_cfg()
-    opts = cases.to_options(cfg)
-    opts.precision = fcb.PRECISION_MIXED if args.precision == "mixed" else fcb.PRECISION_FP64
-    opts.macro_graph = args.macro_graph
-    # warm-up: the first macro steps of the same run (plans, autotuning, graph)
-    w, _, _, _ = _bathy_run(opts, args.warmup, stream=stream)
-    w.close()
-    with ClockSampler(local_rank) as clk:
-        s, ms, cells, patches = _bathy_run(opts, args.steps, stream=stream, timed=True)
-    from forestclaw_b200 import replicas
-
-    ms_max, total_cells = replicas.aggregate(ms, cells, torch.distributed if world > 1 else None)
-    accuracy = None
-    if args.precision == "mixed" and rank == 0:
-        o64 = cases.to_options(cfg)
-        o64.macro_graph = args.macro_graph
-        ref, _, _, _ = _bathy_run(o64, args.steps, stream=stream)
-        acc = {"against": "the same run in FP64 on the GPU", "same_mesh": ref.leaves() == s.leaves()}
-        q0s = None
-        if acc["same_mesh"]:
-            qm, qf = s.get_q(), ref.get_q()
-            m = cfg.mbc
-            a, b = qm[..., m:-m, m:-m], qf[..., m:-m, m:-m]
-            acc["l1_rel"] = float(np.abs(a - b).sum() / np.abs(b).sum())
-            acc["max_rel"] = float(np.abs(a - b).max() / max(1.0, np.abs(b).max()))
-            mm, mf = np.asarray(s.conservation_check()), np.asarray(ref.conservation_check())
-            acc["mass_drift_rel"] = float(np.max(np.abs(mm - mf)) / np.max(np.abs(mf)))
-        ref.close()
-        # lake at rest (no pulse): the largest change of any cell after the same steps
-        lake = cases.to_options(_bathy_cfg(amp=0.0))
-        lake.precision = fcb.PRECISION_MIXED
-        lake.macro_graph = args.macro_graph
-        ls = fcb.Solver(lake, stream=stream.cuda_stream)
-        ls.initialize()
-        q0s = ls.get_q()
-        t = 0.0
-        for _ in range(args.steps):
-            ls.advance_all_levels(t, _bathy_dt())
-            t += _bathy_dt()
-        m = cfg.mbc
-        acc["lake_at_rest_max_change"] = float(np.abs(ls.get_q() - q0s)[..., m:-m, m:-m].max())
-        ls.close()
-        accuracy = acc
-    if rank != 0:
-        s.close()
-        return None
-    hbm, src = peaks()
-    bytes_per_cell = 64.5  # meqn 3 + stored b, mx 32, mbc 2
-    achieved = total_cells * bytes_per_cell / (ms_max * 1e-3) / 1e9
-    line = {
-        "metric": "cell-updates/s", "value": total_cells / (ms_max * 1e-3), "unit": "cell-updates/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
-        "config": {"workload": "shallow water over bathymetry (GeoClaw f-waves), lake at rest + pulse 1e-3, "
-                               "levels 4-7, mx=my=32, subcycled, regrid every macro step (advance phase timed)",
-                   "patches_min": min(patches), "patches_max": max(patches), "macro_graph": args.macro_graph,
-                   "accuracy": accuracy},
-        "clocks": clk.summary(),
-        "gpu_launches": s.bench_launches,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "bytes_per_cell": bytes_per_cell, "kernel": "advance phase (all kernels)",
-                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback"},
-        "roofline_fp": fp_roofline("geoclaw_fwave_order20", cfg.mx, total_cells / (ms_max * 1e-3), args.precision,
-                                   stream.cuda_stream),
-    }
-    s.close()
-    return line
+    acc["lake_at_rest_max_change"] = float(np.abs(ls.get_q() - q0)[..., 2:-2, 2:-2].max())
+    ls.close()
+    return acc
 
 
 # ----------------------------------------------------------------------------
 # Ensemble serving: Poisson stream of shallow-water dam-break requests
 # ----------------------------------------------------------------------------
-def _serve_requests(n, seed, precision):
-    """Dam breaks with radius ~ U(0.1, 0.3), inner depth ~ U(1.5, 3), outer 1,
-    maxlevel ~ U{4, 5}, mx ~ {16, 32}, t_final ~ U(0.02, 0.05); levels from 2,
-    non-subcycled, regrid every macro step, adaptive dt (desired CFL 0.9)."""
-    import cases
-    import forestclaw_b200 as fcb
+def serve_measure(requests, rates, local_rank, stream, label):
+    """Isolated latency of every request (alone on the GPU), then the Poisson
+    stream at each rate: p50/p99 latency and aggregate cell-updates/s."""
+    import torch
 
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(n):
-        r0, hin = rng.uniform(0.1, 0.3), rng.uniform(1.5, 3.0)
-        maxlevel, mx = int(rng.integers(4, 6)), int(rng.choice([16, 32]))
-        cfg = cases.radialdam_amr(seed=0, minlevel=2, maxlevel=maxlevel, mx=mx, tfinal=float(rng.uniform(0.02, 0.05)))
-        cfg = cases.replace(cfg, pparams=(0.5, 0.5, r0, hin, 1.0), initial_dt=0.9 / (mx * 4) / (hin ** 0.5 + 1))
-        o = cases.to_options(cfg)
-        o.subcycle = 0
-        o.precision = fcb.PRECISION_MIXED if precision == "mixed" else fcb.PRECISION_FP64
-        out.append(o)
-    return out
+    from forestclaw_b200.serve import Server, poisson_stream
+
+    budget = int(0.5 * torch.cuda.get_device_properties(local_rank).total_memory)
+    iso = []
+    for o in requests:
+        sv = Server(budget, stream)
+        r = poisson_stream(sv, [o], rate=0.0)
+        iso.append(r.latencies[0])
+        sv.close()
+    iso_p99 = float(np.percentile(iso, 99))
+    sweep = []
+    with ClockSampler(local_rank) as clk:
+        for lam in rates:
+            sv = Server(budget, stream)
+            r = poisson_stream(sv, requests, rate=lam, seed=11)
+            sv.close()
+            sweep.append({"rate_per_s": lam, "p50_s": r.pct(50), "p99_s": r.pct(99),
+                          "cell_updates_per_s": r.cell_updates / r.wall, "wall_s": r.wall,
+                          "rounds": r.rounds, "launches": r.launches, "failed": r.failed,
+                          "p99_over_isolated_p99": r.pct(99) / iso_p99})
+    top = max(sweep, key=lambda d: d["cell_updates_per_s"])
+    # the highest rate whose throughput is within 5 % of the best one
+    knee = max((d for d in sweep if d["cell_updates_per_s"] >= 0.95 * top["cell_updates_per_s"]),
+               key=lambda d: d["rate_per_s"])
+    return {"workload": label, "requests": len(requests), "isolated_p50_s": float(np.percentile(iso, 50)),
+            "isolated_p99_s": iso_p99, "sweep": sweep, "best": top, "knee": knee, "clocks": clk.summary()}
 
 
 def run_serve(args, rank, world, local_rank):
     import torch
 
-    from forestclaw_b200.serve import Server, poisson_stream
+    import forestclaw_b200 as fcb
+    from forestclaw_b200 import workloads
 
     torch.cuda.set_device(local_rank)
     stream = torch.cuda.current_stream().cuda_stream
-    reqs = _serve_requests(args.requests, 7 + rank, args.precision)
-    budget = int(0.5 * torch.cuda.get_device_properties(local_rank).total_memory)
-    # isolated latency of each request (alone on the GPU)
-    iso = []
+    maxlevels = tuple(int(v) for v in args.serve_maxlevels.split(","))
+    tf = tuple(float(v) for v in args.serve_tfinal.split(","))
+    reqs = workloads.dam_break_requests(args.requests, 7 + rank, maxlevels=maxlevels, tfinal=tf)
     for o in reqs:
-        sv = Server(budget, stream)
-        r = poisson_stream(sv, [o], rate=0.0)
-        iso.append(r.latencies[0])
-        sv.close()
-    sweep = []
-    with ClockSampler(local_rank) as clk:
-        for lam in [float(x) for x in args.rates.split(",")]:
-            sv = Server(budget, stream)
-            r = poisson_stream(sv, reqs, rate=lam, seed=11)
-            sv.close()
-            sweep.append({"rate_per_s": lam, "p50_s": r.pct(50), "p99_s": r.pct(99),
-                          "cell_updates_per_s": r.cell_updates / r.wall, "wall_s": r.wall,
-                          "rounds": r.rounds, "launches": r.launches, "failed": r.failed,
-                          "p99_over_isolated_p99": r.pct(99) / float(np.percentile(iso, 99))})
+        o.precision = fcb.PRECISION_MIXED if args.precision == "mixed" else fcb.PRECISION_FP64
+    label = (f"ensemble serving: Poisson stream of shallow-water dam-break solves (r ~ U(0.1,0.3), h_in ~ "
+             f"U(1.5,3), maxlevel ~ U{{{','.join(map(str, maxlevels))}}}, mx ~ {{16,32}}, t_final ~ U({tf[0]},{tf[1]})), "
+             "continuous batching")
+    m = serve_measure(reqs, [float(x) for x in args.rates.split(",")], local_rank, stream, label)
     if rank != 0:
         return None
-    top = max(sweep, key=lambda d: d["cell_updates_per_s"])
+    top = m["best"]
     return {
         "metric": "cell-updates/s", "value": top["cell_updates_per_s"], "unit": "cell-updates/s",
         "n_gpus": world, "steps": args.requests, "warmup": 0, "ms_per_step": top["wall_s"] * 1e3 / args.requests,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
-        "config": {"workload": "ensemble serving: Poisson stream of shallow-water dam-break solves "
-                               "(r ~ U(0.1,0.3), h_in ~ U(1.5,3), maxlevel ~ U{4,5}, mx ~ {16,32}, "
-                               "t_final ~ U(0.02,0.05)), continuous batching",
-                   "requests": args.requests, "isolated_p50_s": float(np.percentile(iso, 50)),
-                   "isolated_p99_s": float(np.percentile(iso, 99)), "sweep": sweep},
+        "config": {"workload": label, "requests": args.requests, "isolated_p50_s": m["isolated_p50_s"],
+                   "isolated_p99_s": m["isolated_p99_s"], "sweep": m["sweep"], "knee": m["knee"]},
         "p50_s": top["p50_s"], "p99_s": top["p99_s"],
-        "clocks": clk.summary(),
+        "clocks": m["clocks"],
         "gpu_launches": top["launches"],
     }
+
+
+# ----------------------------------------------------------------------------
+# The other forms and configurations, measured in the default run and reported
+# as sub-objects of its line (each with its own clocks and CUDA-event times)
+# ----------------------------------------------------------------------------
+def _uniform_quick(level, mx, precision, steps, warmup, stream, local_rank):
+    import torch
+
+    import forestclaw_b200 as fcb
+    from forestclaw_b200 import workloads
+
+    o = workloads.uniform_swirl(level, mx)
+    o.precision = fcb.PRECISION_MIXED if precision == "mixed" else fcb.PRECISION_FP64
+    dt = workloads.swirl_dt(level, mx)
+    s = fcb.Solver(o, stream=stream.cuda_stream)
+    s.initialize()
+    t = 0.0
+    for _ in range(warmup):
+        s.advance_all_levels(t, dt)
+        t += dt
+    c0 = s.counters()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        for _ in range(steps):
+            s.advance_all_levels(t, dt)
+            t += dt
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    c1 = s.counters()
+    cells = (c1["count_single_step"] - c0["count_single_step"]) * mx * mx
+    kms, fused = s.step_kernel_time(t, dt, max(5, steps))
+    s.close()
+    return {"value": cells / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms / steps, "steps": steps,
+            "warmup": warmup, "step_kernel_ms": kms, "ghost_fill_fused": fused,
+            "gpu_launches": c1["count_kernel_launches"] - c0["count_kernel_launches"], "clocks": clk.summary()}
+
+
+def run_extras(args, local_rank, main_line):
+    """Sub-objects of the default line: the mixed form of the uniform case,
+    AMR shallow water (FP64, mixed), AMR Euler, bathymetry (FP64, mixed, with
+    the error of the mixed form) and a serving sweep."""
+    import torch
+
+    import forestclaw_b200 as fcb
+    from forestclaw_b200 import workloads
+
+    stream = torch.cuda.current_stream()
+    out = {}
+
+    def guarded(name, fn):
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as e:  # noqa: BLE001 - reported in the line, the main number stands
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = time.perf_counter() - t0
+
+    def mixed_uniform():
+        m = _uniform_quick(args.level, args.mx, "mixed", args.steps, args.warmup, stream, local_rank)
+        m["workload"] = f"uniform swirl advection, level {args.level}, mx=my={args.mx}, mixed FP32/FP64"
+        m["speedup_over_fp64"] = main_line["ms_per_step"] / m["ms_per_step"]
+        m["step_kernel_speedup_over_fp64"] = main_line["config"]["step_kernel_ms"] / m["step_kernel_ms"]
+        m["accuracy"] = _mixed_accuracy(args, workloads.uniform_swirl(args.level, args.mx),
+                                        workloads.swirl_dt(args.level, args.mx), stream)
+        m["roofline_fp"] = fp_roofline("advection_swirl_order22", args.mx, m["value"], "mixed", stream.cuda_stream)
+        return m
+
+    def amr(workload, precision, steps, mx=32):
+        o = _amr_options(workload, mx, precision)
+        m = amr_measure(o, steps, 2, stream, local_rank)
+        m["roofline_fp"] = fp_roofline(_fp_case(o), o.mx, m["value"], precision, stream.cuda_stream)
+        m["hbm_frac"] = m["value"] * _bytes_per_cell(o) / 1e9 / peaks()[0]
+        return m
+
+    def pair(workload, steps, mx=32):
+        f = amr(workload, "fp64", steps, mx)
+        mm = amr(workload, "mixed", steps, mx)
+        return {"fp64": f, "mixed": mm, "mixed_over_fp64": mm["value"] / f["value"]}
+
+    guarded("mixed_uniform", mixed_uniform)
+
+    def c2():
+        r = pair("amr_radialdam", 5)
+        r["workload"] = ("AMR shallow-water dam break (Roe), levels 3-6, mx=my=32, subcycled, regrid every macro "
+                         "step; advance phase timed, seed 0")
+        return r
+
+    guarded("amr_shallow_water", c2)
+
+    def c3():
+        r = amr("amr_quadrants", "fp64", 3, mx=16)
+        r["workload"] = ("AMR Euler quadrants (Roe), levels 2-7, mx=my=16, subcycled (32 fine steps per macro "
+                         "step), regrid every macro step; advance phase timed, seed 0")
+        return r
+
+    guarded("amr_euler", c3)
+
+    def c4():
+        r = pair("bathy", 3)
+        r["workload"] = ("shallow water over bathymetry (GeoClaw f-waves), lake at rest + pulse 1e-3, levels 4-7, "
+                         "mx=my=32, subcycled, regrid every macro step; advance phase timed")
+        r["mixed_accuracy"] = bathy_accuracy(3, 2, stream)
+        return r
+
+    guarded("bathymetry", c4)
+
+    def serving():
+        reqs = workloads.dam_break_requests(args.extra_requests, 7, maxlevels=(4, 5, 6, 7), tfinal=(0.02, 0.1))
+        label = ("ensemble serving, FP64: Poisson stream of shallow-water dam-break solves (r ~ U(0.1,0.3), "
+                 "h_in ~ U(1.5,3), maxlevel ~ U{4..7}, mx ~ {16,32}, t_final ~ U(0.02,0.1): the configured final "
+                 "times scaled by 1/10 so the sweep fits the default run), continuous batching")
+        return serve_measure(reqs, [float(x) for x in args.rates.split(",")], local_rank, stream.cuda_stream,
+                             label)
+
+    if args.extra_requests > 0:
+        guarded("serving", serving)
+    return out
 
 
 def main():
@@ -859,9 +970,11 @@ def main():
                                              device_id=torch.device("cuda", local_rank))
     try:
         sys.path.insert(0, str(ROOT / "tests"))
-        run = {"amr_radialdam": run_amr, "amr_quadrants": run_amr, "bathy": run_bathy,
+        run = {"amr_radialdam": run_amr, "amr_quadrants": run_amr, "bathy": run_amr,
                "serve": run_serve}.get(args.workload, run_partitioned if args.partition else run_ours)
         line = run(args, rank, world, local_rank)
+        if line and run is run_ours and args.extras and world == 1 and args.precision == "fp64":
+            line["extras"] = run_extras(args, local_rank, line)
         if line:
             print(json.dumps(line), flush=True)
     finally:

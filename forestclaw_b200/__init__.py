@@ -46,7 +46,7 @@ EXPORTED_SYMBOLS = (
     "fcb_server_get_q", "fcb_server_release", "fcb_server_clock", "fcb_autotune_info",
     "fcb_measure_fp_rate", "fcb_output_ascii", "fcb_comm_create_local", "fcb_comm_nccl_unique_id",
     "fcb_comm_create_nccl", "fcb_comm_destroy", "fcb_context_create_partitioned", "fcb_partition_info",
-    "fcb_global_maximum", "fcb_partition_plan",
+    "fcb_global_maximum", "fcb_partition_plan", "fcb_step_kernel_time",
 )
 
 
@@ -76,6 +76,7 @@ class _Options(ctypes.Structure):
         ("time_sync", ctypes.c_int),
         ("ax", ctypes.c_double), ("bx", ctypes.c_double), ("ay", ctypes.c_double), ("by", ctypes.c_double),
         ("weighted_partition", ctypes.c_int),
+        ("ghost_fusion", ctypes.c_int),
     ]
 
 
@@ -149,6 +150,8 @@ class Options:
     extent: Sequence[float] = (0.0, 1.0, 0.0, 1.0)
     # [Options] weighted-partition: partitioned solves weigh leaves by 2^level when subcycling
     weighted_partition: int = 1
+    # ghost-exchange fusion on a mesh of one level: 0 autotuned, 1 off, 2 on
+    ghost_fusion: int = 0
 
     def to_c(self) -> _Options:
         o = _Options()
@@ -156,7 +159,7 @@ class Options:
                      "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
                      "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
                      "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph", "claw_version",
-                     "time_sync", "weighted_partition"):
+                     "time_sync", "weighted_partition", "ghost_fusion"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
                      "desired_cfl", "grav", "gamma", "dry_tolerance"):
@@ -225,6 +228,7 @@ def lib():
     L.fcb_conservation_check.argtypes = [vp, dp]
     L.fcb_curr_time.argtypes = [vp, dp]
     L.fcb_autotune_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    L.fcb_step_kernel_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ip, dp]
     L.fcb_measure_fp_rate.argtypes = [ctypes.c_int, vp, dp]
     L.fcb_output_ascii.argtypes = [vp, ctypes.c_int, ctypes.c_char_p]
     L.fcb_conservation_sum_noalloc.argtypes = [vp, sz, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -492,6 +496,13 @@ class Solver:
         f, u = ctypes.c_int(), ctypes.c_int()
         _check(lib().fcb_autotune_info(self._h, ctypes.byref(f), ctypes.byref(u)))
         return {"step_form": f.value, "ghost_unroll": u.value}
+
+    def step_kernel_time(self, t: float, dt: float, launches: int = 10) -> tuple:
+        """(ms per launch, fused) of the step kernel an advance launches on the
+        current mesh, timed on scratch copies of the arrays."""
+        f, ms = ctypes.c_int(), ctypes.c_double()
+        _check(lib().fcb_step_kernel_time(self._h, t, dt, launches, ctypes.byref(f), ctypes.byref(ms)))
+        return ms.value, bool(f.value)
 
     def conservation_check(self) -> np.ndarray:
         out = np.zeros(self.options.meqn)

@@ -45,6 +45,8 @@ SOURCES = {
     "fcb_step_warp.cu": ["-fmad=false"],
     "fcb_step_pipe.cu": ["-fmad=false"],
     "fcb_step_mixed.cu": ["--use_fast_math"],
+    "fcb_step_fused.cu": ["-fmad=false"],
+    "fcb_step_fused_mixed.cu": ["--use_fast_math"],
     "fcb_ghost.cu": ["-fmad=false"],
     "fcb_amr.cu": ["-fmad=false"],
     "fcb_runtime.cu": [],

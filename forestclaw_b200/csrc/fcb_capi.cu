@@ -348,6 +348,17 @@ int fcb_measure_fp_rate(int fp64, void* cuda_stream, double* ops_per_second) {
     });
 }
 
+int fcb_step_kernel_time(fcb_context_t* ctx, double t, double dt, int launches, int* fused, double* ms_per_launch) {
+    return guard([&] {
+        CTX();
+        need(fused, "fused");
+        need(ms_per_launch, "ms_per_launch");
+        bool f = false;
+        *ms_per_launch = C.step_kernel_time(t, dt, launches, &f);
+        *fused = f ? 1 : 0;
+    });
+}
+
 int fcb_autotune_info(fcb_context_t* ctx, int* step_form, int* ghost_unroll) {
     return guard([&] {
         CTX();

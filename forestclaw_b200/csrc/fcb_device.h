@@ -28,6 +28,18 @@ struct PatchDesc {
     int32_t pad;
 };
 
+// Ghost-exchange fusion on a mesh of one level: per slot, the slots of its
+// same-size neighbours across faces 0-3 (left, right, bottom, top) and corners
+// 0-3 (bottom-left, bottom-right, top-left, top-right), -1 where there is none,
+// and the physical boundary condition of each face (mthbc 1 or 3, 0 where the
+// face has a neighbour).  A fused step reads its ghost cells from these
+// neighbours' interiors instead of from its own ghost cells.
+struct FuseNbr {
+    int32_t face[4];
+    int32_t corner[4];
+    int32_t bc[4];
+};
+
 // Arguments of one batched step launch (all patches of one level).
 struct StepArgs {
     double* q;             // arena base
@@ -54,6 +66,16 @@ struct StepArgs {
     // dyn holds {dt, vt} for levels lvl0 .. lvl0 + nlvl - 1 and each patch reads
     // its own level's pair
     int32_t lvl0, nlvl;
+    // ghost-exchange fusion (fuse non-null): the step reads the arena qsrc, its
+    // ghost cells resolved through fuse[slot] to the neighbours' interiors and
+    // the physical boundary conditions, and writes the updated interior cells to
+    // the arena q (qsrc != q)
+    const double* qsrc;
+    const FuseNbr* fuse;
+    // four-barrier form: nbands > 1 splits every patch's rows into that many
+    // bands, one CTA each, which read the copy qsrc of the arena (bands
+    // overlap in the rows they read) and update their own rows in q
+    int32_t nbands;
 };
 
 // Conservation registers of one slot (fclaw2d_clawpatch_registers_t), doubles

@@ -135,22 +135,25 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
             bad("the GeoClaw solver exists in the pipelined step form only");
         if (!(opt_.dry_tolerance >= 0.0)) bad("dry_tolerance must be >= 0");
     }
-    if (opt_.step_variant < 0 || opt_.step_variant > 3) bad("step_variant must be 0, 1, 2 or 3");
+    if (opt_.step_variant < 0 || opt_.step_variant > 5) bad("step_variant must be 0 to 5");
     if (opt_.precision != 0 && opt_.precision != 1) bad("precision must be 0 (FP64) or 1 (mixed)");
-    if (opt_.precision == 1 && (opt_.step_variant == 1 || opt_.step_variant == 2))
-        bad("the mixed-precision update exists in the pipelined step form only");
+    const bool not_pipe = opt_.step_variant == 1 || opt_.step_variant == 2 || opt_.step_variant >= 4;
+    if (opt_.precision == 1 && not_pipe) bad("the mixed-precision update exists in the pipelined step form only");
+    if (opt_.step_variant >= 4 && opt_.solver_kind != FCB_SOLVER_SWE_ROE && opt_.solver_kind != FCB_SOLVER_EULER4_ROE)
+        bad("row bands (step_variant 4, 5) are built for the Roe solvers' four-barrier form");
     if ((opt_.mx & (opt_.mx - 1)) != 0) bad("mx must be a power of two");
     if (opt_.macro_graph < 0 || opt_.macro_graph > 2) bad("macro_graph must be 0, 1 or 2");
+    if (opt_.ghost_fusion < 0 || opt_.ghost_fusion > 2) bad("ghost_fusion must be 0, 1 or 2");
+    if (comm_) opt_.ghost_fusion = 1;  // a partitioned ghost update exchanges between ranks
     if (opt_.claw_version == 0) opt_.claw_version = 4;
     if (opt_.claw_version != 4 && opt_.claw_version != 5) bad("claw_version must be 4 (clawpack 4.6) or 5");
-    if (opt_.claw_version == 5 && (opt_.step_variant == 1 || opt_.step_variant == 2))
-        bad("the clawpack 5 update exists in the pipelined step form only");
+    if (opt_.claw_version == 5 && not_pipe) bad("the clawpack 5 update exists in the pipelined step form only");
     if (opt_.time_sync) {
         if (opt_.solver_kind != FCB_SOLVER_SWE_ROE)
             bad("time-sync needs the conservative flux rpn2_cons, given here for the shallow-water Roe solver");
         if (opt_.claw_version == 5) bad("time-sync is on the clawpack 4.6 path");
         if (opt_.precision != 0) bad("time-sync is FP64 only");
-        if (opt_.step_variant == 2 || opt_.step_variant == 3)
+        if (opt_.step_variant != 0 && opt_.step_variant != 1)
             bad("time-sync accumulates its registers in the four-barrier step form (step_variant 0 or 1)");
         time_sync_ = true;
     }
@@ -252,6 +255,7 @@ Context::~Context() {
     arena_free(d_qlast_);
     arena_free(d_qti_);
     arena_free(d_qsave_);
+    arena_free(d_qalt_);
     arena_free(d_aux_);
     arena_free(d_meta_);
     arena_free(d_treg_);
@@ -300,6 +304,8 @@ void Context::ensure_capacity(int n) {
         d_treg_ = np;
     }
     if (!opt_.use_fixed_dt) grow(d_qsave_);
+    arena_free(d_qalt_);  // the second arena of fused steps: reallocated at its next use
+    d_qalt_ = nullptr;
     if (aux_kind_ == AUX_STORED) {  // recomputed for every patch by mesh_changed
         arena_free(d_aux_);
         d_aux_ = nullptr;
@@ -434,6 +440,7 @@ void Context::mesh_changed() {
     h_groups_.clear();
     h_xitems_.clear();
     ops_dirty_ = true;
+    build_fuse_table();
 }
 
 // ---------------------------------------------------------------------------
@@ -1207,14 +1214,17 @@ std::vector<char> Context::local_set() const {
 
 void Context::ghost_update(int minlevel, int maxlevel, double, int time_interp) {
     if (!d_q_) throw Error(FCB_ERR_STATE, "ghost_update before initialize");
+    ensure_ghosts();
     if (dry_) {
         dry_plan_keys_.emplace_back(minlevel, maxlevel, time_interp);
         return;
     }
     run_plan(plan(minlevel, maxlevel, time_interp));
+    if (minlevel <= gmin_ && maxlevel >= gmax_) ghosts_filled_ = true;
 }
 
 void Context::physical_set_bc(int level, int time_interp) {
+    ensure_ghosts();
     std::vector<GhostOp> ops;
     for (int p = own_first_; p < own_first_ + own_count_; ++p) {
         if (forest_.leaves[p].level != level) continue;
@@ -1249,23 +1259,15 @@ void Context::launch_level_step_slots(const int32_t* d_slots, int n, double t, d
     launch_levels_step_slots(d_slots, n, 0, 1, tl, dl, cfl_slot);
 }
 
-// One step launch over patches of levels lvl0 .. lvl0 + nlvl - 1 (their slots
-// contiguous in d_slots), level l at time t[l - lvl0] with step dt[l - lvl0].
-// nlvl > 1 needs the macro-step table (use_dyn_): each level's {dt, vt} pair.
-void Context::launch_levels_step_slots(const int32_t* d_slots, int n, int lvl0, int nlvl, const double* tl,
-                                       const double* dtl, unsigned long long* cfl_slot) {
-    if (n <= 0) return;
-    if (nlvl > 1 && !use_dyn_) throw Error(FCB_ERR_INTERNAL, "merged level updates need the step-parameter table");
-    const double t = tl[0], dt = dtl[0];
-    StepArgs a{};
+// The launch arguments every step form shares: arenas, method, time step,
+// swirl velocity scale, physical parameters, CFL slot.
+void Context::fill_step_args(StepArgs& a, double t, double dt, unsigned long long* cfl_slot) const {
     a.q = d_q_;
     a.qlast = d_qlast_;
     a.aux = aux_kind_ == AUX_STORED ? d_aux_ : nullptr;
-    a.slots = d_slots;
     a.meta = d_meta_;
     a.q_stride = stride_;
     a.aux_stride = aux_stride_;
-    a.npatches = n;
     a.maux = aux_kind_ == AUX_STORED ? opt_.maux : 0;
     a.order0 = opt_.order[0];
     a.order1 = opt_.order[1];
@@ -1285,6 +1287,22 @@ void Context::launch_levels_step_slots(const int32_t* d_slots, int n, int lvl0, 
     a.cfl_out = cfl_slot;
     a.treg = time_sync_ ? d_treg_ : nullptr;
     a.treg_stride = treg_stride_;
+    a.lvl0 = 0;
+    a.nlvl = 1;
+}
+
+// One step launch over patches of levels lvl0 .. lvl0 + nlvl - 1 (their slots
+// contiguous in d_slots), level l at time t[l - lvl0] with step dt[l - lvl0].
+// nlvl > 1 needs the macro-step table (use_dyn_): each level's {dt, vt} pair.
+void Context::launch_levels_step_slots(const int32_t* d_slots, int n, int lvl0, int nlvl, const double* tl,
+                                       const double* dtl, unsigned long long* cfl_slot) {
+    if (n <= 0) return;
+    if (nlvl > 1 && !use_dyn_) throw Error(FCB_ERR_INTERNAL, "merged level updates need the step-parameter table");
+    const double t = tl[0], dt = dtl[0];
+    StepArgs a{};
+    fill_step_args(a, t, dt, cfl_slot);
+    a.slots = d_slots;
+    a.npatches = n;
     a.lvl0 = lvl0;
     a.nlvl = nlvl;
     if (use_dyn_) {
@@ -1321,6 +1339,12 @@ void Context::launch_levels_step_slots(const int32_t* d_slots, int n, int lvl0, 
         a.dyn = d_dyn_.p + 2 * dyn_n_;
         dyn_n_ += nlvl;
     }
+    launch_step_form(a, n);
+}
+
+// The step launch of a level update in the form chosen for it (the autotuner's,
+// or step_variant), with the time-sync flux store before it when time-sync is on.
+void Context::launch_step_form(const StepArgs& a, int n) {
     // The warp form computes each swirl velocity node once, which equals the
     // reference's per-cell evaluations because the unit-square mesh with mx a
     // power of two is dyadic (xll + dx == next xll exactly); checked at creation.
@@ -1330,8 +1354,30 @@ void Context::launch_levels_step_slots(const int32_t* d_slots, int n, int lvl0, 
         check(launch_ts_store_flux(a, opt_.mx, opt_.my, opt_.mbc, opt_.meqn, st_), "time-sync store flux");
         ++cnt_.count_kernel_launches;
     }
-    const int v = time_sync_ ? 1 : opt_.step_variant == 0 ? tune_step_form(a, n) : opt_.step_variant;
+    // the tuner's choice is form + 8 * (row bands - 1): the four-barrier form
+    // may split every patch's rows into bands of separate CTAs
+    const int code = time_sync_                  ? 1
+                     : opt_.step_variant == 0      ? tune_step_form(a, n)
+                     : opt_.step_variant >= 4      ? 1 + 8 * (opt_.step_variant - 3)
+                                                   : opt_.step_variant;
+    const int v = code % 8, nb = code / 8 + 1;
     step_form_used_ = v;
+    bands_used_ = nb;
+    if (nb > 1) {
+        // the bands of a patch read rows beyond their own: they read a copy of
+        // the arena taken before the launch and update q in place
+        if (!d_qalt_) arena_alloc(d_qalt_, (size_t)capacity_ * stride_ * sizeof(double));
+        check(cudaMemcpyAsync(d_qalt_, a.q, (size_t)capacity_ * stride_ * sizeof(double), cudaMemcpyDeviceToDevice,
+                              st_),
+              "band source copy");
+        StepArgs b = a;
+        b.qsrc = d_qalt_;
+        b.nbands = nb;
+        check(launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_), "step");
+        cnt_.count_single_step += n;
+        ++cnt_.count_kernel_launches;
+        return;
+    }
     if (opt_.precision == 1) {
         e = launch_step_pipe_mixed(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc,
                                    opt_.claw_version, a, st_);
@@ -1362,6 +1408,8 @@ double Context::launch_level_step(int level, double t, double dt, unsigned long 
 
 double Context::update_single_step(int level, double t, double dt) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "update_single_step before initialize");
+    ensure_ghosts();
+    ghosts_filled_ = false;  // the step updates ghost cells; no ghost update follows
     check(cudaMemsetAsync(d_cfl_ + 1, 0, sizeof(unsigned long long), st_), "memset");
     launch_level_step(level, t, dt, d_cfl_ + 1);
     return read_cfl(d_cfl_ + 1);
@@ -1369,6 +1417,8 @@ double Context::update_single_step(int level, double t, double dt) {
 
 void Context::update_single_step_async(int level, double t, double dt) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "update_single_step before initialize");
+    ensure_ghosts();
+    ghosts_filled_ = false;
     launch_level_step(level, t, dt, d_cfl_);
 }
 
@@ -1376,6 +1426,8 @@ double Context::single_step_update(int patchno, double t, double dt, int iter, i
     if (!initialized_) throw Error(FCB_ERR_STATE, "single_step_update before initialize");
     if (patchno < 0 || patchno >= num_patches()) throw Error(FCB_ERR_INVALID, "bad patch number");
     if (!owned(patchno)) throw Error(FCB_ERR_INVALID, "patch not owned by this rank");
+    ensure_ghosts();
+    ghosts_filled_ = false;
     if (iter == 0) pending_.clear();
     pending_.push_back(slot_of_[patchno]);
     if (iter + 1 < total) return 0.0;
@@ -1389,6 +1441,7 @@ double Context::single_step_update(int patchno, double t, double dt, int iter, i
 
 void Context::timeinterp(int level, double alpha) {
     if (dry_ || level < 0 || level > QuadForest::kMaxLevel) return;
+    ensure_ghosts();
     const int b = ti_begin_[level], e = ti_begin_[level + 1];
     if (e == b) return;
     check(launch_timeinterp(d_q_, d_qlast_, d_qti_, stride_, d_ti_slots_.p + b, e - b, opt_.mx, opt_.my, opt_.mbc,
@@ -1488,7 +1541,7 @@ std::vector<uintptr_t> Context::macro_fingerprint() const {
             (uintptr_t)d_level_slots_.p, (uintptr_t)d_ti_slots_.p, (uintptr_t)d_ops_.p, (uintptr_t)d_groups_.p,
             (uintptr_t)d_dyn_.p, (uintptr_t)d_cfl_, (uintptr_t)mesh_version_, (uintptr_t)plans_.size(),
             (uintptr_t)dyn_n_, (uintptr_t)gmin_, (uintptr_t)gmax_, (uintptr_t)d_treg_,
-            (uintptr_t)d_ts_ops_.p, (uintptr_t)d_ts_groups_.p, (uintptr_t)ts_plans_.size()};
+            (uintptr_t)d_ts_ops_.p, (uintptr_t)d_ts_groups_.p, (uintptr_t)ts_plans_.size(), (uintptr_t)d_qalt_};
 }
 
 void Context::drop_macro_graph() {
@@ -1505,6 +1558,9 @@ void Context::drop_macro_graph() {
 // to fill the {dt, vt} table that the step launches read.
 double Context::advance_all_levels(double t_curr, double dt) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "advance before initialize");
+    fused_used_ = 0;
+    if (use_fusion(t_curr, dt)) return advance_fused(t_curr, dt);
+    ensure_ghosts();
     // on an error, plan builds still running are joined and dropped
     struct PlanGuard {
         Context* c;
@@ -1595,6 +1651,7 @@ double Context::advance_all_levels(double t_curr, double dt) {
     finish_plans();
     plans_guard.armed = false;
     ++cnt_.count_amr_advance;
+    ghosts_filled_ = true;  // the macro step ends with a ghost update of every level
     return read_cfl(d_cfl_);
 }
 
@@ -1629,22 +1686,27 @@ int Context::tune_step_form(const StepArgs& a, int n) {
         auto it = g_step_form_cache.find(key);
         if (it != g_step_form_cache.end()) return it->second;
     }
+    // codes: form + 8 * (row bands - 1); the Roe systems' four-barrier form
+    // also runs with each patch split into 2 or 3 row bands (shorter row
+    // sweeps, more CTAs: the level update is bound by one CTA's sweep)
     std::vector<int> cand;
     if (opt_.precision == 1 || opt_.claw_version == 5 || opt_.solver_kind == SOLVER_GEOCLAW_FWAVE) cand = {3};
     else if (aux_kind_ == AUX_SWIRL) cand = {1, 2, 3};
-    else cand = {1, 3};
+    else cand = {1, 3, 1 + 8, 1 + 16};
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st_, &cs);
     if (cand.size() == 1 || cs != cudaStreamCaptureStatusNone || dry_) return cand.size() == 1 ? cand[0] : default_step_form(opt_);
     const size_t bytes = (size_t)capacity_ * stride_ * sizeof(double);
-    double *tq = nullptr, *tl = nullptr;
+    double *tq = nullptr, *tl = nullptr, *ts = nullptr;
     try {
         arena_alloc(tq, bytes);
         arena_alloc(tl, bytes);
+        arena_alloc(ts, bytes);
     } catch (const Error&) {
         cudaGetLastError();
         arena_free(tq);
         arena_free(tl);
+        arena_free(ts);
         return default_step_form(opt_);  // no room for scratch copies: no tuning
     }
     check(cudaMemcpyAsync(tq, d_q_, bytes, cudaMemcpyDeviceToDevice, st_), "tune copy");
@@ -1658,12 +1720,21 @@ int Context::tune_step_form(const StepArgs& a, int n) {
     check(cudaEventCreate(&e1), "event");
     int best = default_step_form(opt_);
     float best_ms = 1e30f;
-    for (int v : cand) {
+    for (int code : cand) {
+        const int v = code % 8, nb = code / 8 + 1;
         auto launch = [&]() -> cudaError_t {
             if (v == 2) return launch_step_warp_swirl(opt_.mx, opt_.mbc, b, st_);
             if (v == 3)
                 return launch_step_pipe(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc,
                                         opt_.claw_version, b, st_);
+            if (nb > 1) {
+                cudaError_t ce = cudaMemcpyAsync(ts, tq, bytes, cudaMemcpyDeviceToDevice, st_);
+                if (ce != cudaSuccess) return ce;
+                StepArgs bb = b;
+                bb.qsrc = ts;
+                bb.nbands = nb;
+                return launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, bb, st_);
+            }
             return launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_);
         };
         if (launch() != cudaSuccess) {  // form not available for this case
@@ -1676,12 +1747,13 @@ int Context::tune_step_form(const StepArgs& a, int n) {
         check(cudaEventSynchronize(e1), "event");
         float ms = 0;
         check(cudaEventElapsedTime(&ms, e0, e1), "event");
-        if (ms < best_ms) { best_ms = ms; best = v; }
+        if (ms < best_ms) { best_ms = ms; best = code; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     arena_free(tq);
     arena_free(tl);
+    arena_free(ts);
     check(cudaStreamSynchronize(st_), "sync");
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_step_form_cache[key] = best;
@@ -1758,8 +1830,238 @@ int Context::tune_ghost_unroll(const GhostPlan& g) {
 // of the 2^(maxlevel-minlevel) fine steps updates every level with the fine dt
 // and is followed by a ghost fill over all levels, so a fine step is one batch
 // of all leaves.
+// ---------------------------------------------------------------------------
+// Ghost-exchange fusion on a mesh of one level.
+//
+// On such a mesh every macro step is n_fine level updates, each followed by a
+// ghost update whose records are same-size copies and physical boundary
+// conditions only (fclaw2d_advance.c:285-341 with one level).  The fused step
+// reads each patch's ghost cells from its neighbours' interiors through a
+// per-slot table (the values those records would write), reads from one arena
+// and writes the updated interiors into the other, so no patch reads a
+// neighbour that the same launch has already updated.  The ghost cells the
+// reference's step would also update are dead: the following ghost update
+// overwrites every one of them.  The last ghost update of the macro step is
+// recorded and run by ensure_ghosts() before anything reads ghost cells, so
+// every array a caller sees equals the unfused result bit for bit.
+// ---------------------------------------------------------------------------
+void Context::build_fuse_table() {
+    fuse_ok_ = false;
+    if (partitioned() || gmin_ != gmax_ || own_count_ <= 0 || capacity_ <= 0) return;
+    std::vector<FuseNbr> t((size_t)capacity_);
+    for (auto& f : t) {
+        for (int k = 0; k < 4; ++k) f.face[k] = f.corner[k] = -1;
+        for (int k = 0; k < 4; ++k) f.bc[k] = 0;
+    }
+    for (int p = 0; p < num_patches(); ++p) {
+        const Neighbors& nb = nbrs_[p];
+        FuseNbr f;
+        for (int k = 0; k < 4; ++k) {
+            f.bc[k] = 0;
+            f.face[k] = f.corner[k] = -1;
+            if (nb.face_rel[k] == REL_BOUNDARY) f.bc[k] = opt_.mthbc[k];
+            else if (nb.face_rel[k] == REL_SAMESIZE) f.face[k] = slot_of_[nb.face_nbr[k][0]];
+            else return;  // a coarse/fine face: not a mesh of one level
+            if (nb.corner_rel[k] == REL_SAMESIZE) f.corner[k] = slot_of_[nb.corner_nbr[k]];
+        }
+        // a corner block is copied from the corner neighbour unless one of its
+        // two faces is a physical boundary; that neighbour must exist
+        for (int c = 0; c < 4; ++c) {
+            const int fx = (c & 1) ? 1 : 0, fy = (c & 2) ? 3 : 2;
+            if (f.bc[fx] == 0 && f.bc[fy] == 0 && f.corner[c] < 0) return;
+        }
+        t[slot_of_[p]] = f;
+    }
+    d_fuse_.reserve((size_t)capacity_);
+    check(cudaMemcpy(d_fuse_.p, t.data(), t.size() * sizeof(FuseNbr), cudaMemcpyHostToDevice), "fuse table");
+    fuse_ok_ = true;
+}
+
+bool Context::fusion_possible() const {
+    // the fused step reads the neighbours' interiors where the unfused one
+    // reads its own ghost cells: equal only when those hold a ghost update's values
+    return opt_.ghost_fusion != 1 && fuse_ok_ && ghosts_filled_ && !partitioned() && !time_sync_ && !dry_ &&
+           gmin_ == gmax_ &&
+           own_count_ > 0 && (opt_.step_variant == 0 || opt_.step_variant == 3) && opt_.mbc == 2 &&
+           (opt_.mx == 8 || opt_.mx == 16 || opt_.mx == 32);
+}
+
+namespace {
+std::map<std::vector<int>, int> g_fusion_cache;
+}  // namespace
+
+bool Context::use_fusion(double t, double dt) {
+    if (!fusion_possible()) return false;
+    if (opt_.ghost_fusion == 2) return true;
+    // autotuner axis: the fused step against the best unfused form plus the
+    // ghost fill, on scratch copies, once per key for the process
+    const bool fixed_lim = opt_.order[0] == 2 && opt_.order[1] == 2;
+    int nb = 0;
+    while ((1 << (nb + 1)) <= own_count_) ++nb;
+    const std::vector<int> key = {opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.claw_version, opt_.precision,
+                                  fixed_lim ? opt_.mthlim[0] : -1, nb};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_fusion_cache.find(key);
+        if (it != g_fusion_cache.end()) return it->second != 0;
+    }
+    int choice = 1;
+    try {
+        const double tf = time_steps(true, false, 3, t, dt);
+        const double tu = time_steps(false, true, 3, t, dt);
+        choice = tf < tu ? 1 : 0;
+    } catch (const Error&) {
+        cudaGetLastError();
+        choice = 1;  // no room for the scratch copies: fuse (no extra arena beyond the second one)
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_fusion_cache[key] = choice;
+    return choice != 0;
+}
+
+void Context::launch_fused_step(double t, double dt, const double* src, double* dst, unsigned long long* cfl_slot) {
+    const int b = level_begin_[gmax_], e = level_begin_[gmax_ + 1];
+    StepArgs a{};
+    fill_step_args(a, t, dt, cfl_slot);
+    a.q = dst;
+    a.qsrc = src;
+    a.fuse = d_fuse_.p;
+    a.slots = d_level_slots_.p + b;
+    a.npatches = e - b;
+    cudaError_t r = opt_.precision == 1
+                        ? launch_step_pipe_fused_mixed(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my,
+                                                       opt_.mbc, opt_.claw_version, a, st_)
+                        : launch_step_pipe_fused(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my,
+                                                 opt_.mbc, opt_.claw_version, a, st_);
+    check(r, "fused step");
+    cnt_.count_single_step += e - b;
+    ++cnt_.count_kernel_launches;
+}
+
+// fclaw2d_advance_all_levels on a mesh of one level l: n_fine updates of l
+// (subcycled: 2^(l - minlevel) steps of dt halved per level; otherwise
+// 2^(maxlevel - minlevel) steps of dt/rf), each followed by a ghost update.
+double Context::advance_fused(double t_curr, double dt) {
+    int n_fine;
+    double dt_fine = dt;
+    if (opt_.subcycle) {
+        for (int l = opt_.minlevel; l < gmax_; ++l) dt_fine /= 2;
+        n_fine = 1 << (gmax_ - opt_.minlevel);
+    } else {
+        const int rf = 1 << (opt_.maxlevel - opt_.minlevel);
+        n_fine = rf;
+        dt_fine = dt / rf;
+    }
+    if (!d_qalt_) arena_alloc(d_qalt_, (size_t)capacity_ * stride_ * sizeof(double));
+    check(cudaMemsetAsync(d_cfl_, 0, sizeof(unsigned long long), st_), "memset");
+    double tk = t_curr;
+    for (int k = 0; k < n_fine; ++k) {
+        launch_fused_step(tk, dt_fine, d_q_, d_qalt_, d_cfl_);
+        std::swap(d_q_, d_qalt_);
+        tk += dt_fine;
+    }
+    ghosts_stale_ = true;
+    stale_min_ = gmin_;
+    stale_max_ = gmax_;
+    stale_t_ = tk;
+    fused_used_ = 1;
+    step_form_used_ = 3;
+    ++cnt_.count_amr_advance;
+    return read_cfl(d_cfl_);
+}
+
+void Context::ensure_ghosts() {
+    if (!ghosts_stale_ || dry_) return;
+    ghosts_stale_ = false;
+    run_plan(plan(stale_min_, stale_max_, 0));
+}
+
+double Context::time_steps(bool fused, bool with_fill, int launches, double t, double dt) {
+    const size_t bytes = (size_t)capacity_ * stride_ * sizeof(double);
+    double *s0 = nullptr, *s1 = nullptr;
+    try {
+        arena_alloc(s0, bytes);
+        arena_alloc(s1, bytes);
+    } catch (...) {
+        arena_free(s0);
+        arena_free(s1);
+        throw;
+    }
+    const fcb_counters_t cnt0 = cnt_;
+    const int form0 = step_form_used_;
+    double* const q_real = d_q_;
+    check(cudaMemcpyAsync(s0, d_q_, bytes, cudaMemcpyDeviceToDevice, st_), "timing copy");
+    check(cudaMemcpyAsync(s1, d_q_, bytes, cudaMemcpyDeviceToDevice, st_), "timing copy");
+    const int b = level_begin_[gmax_], e = level_begin_[gmax_ + 1];
+    int parity = 0;
+    auto one = [&]() {
+        if (fused) {
+            launch_fused_step(t, dt, parity ? s1 : s0, parity ? s0 : s1, d_cfl_ + 3);
+            parity ^= 1;
+        } else {
+            StepArgs a{};
+            fill_step_args(a, t, dt, d_cfl_ + 3);
+            a.q = s0;
+            a.qlast = s1;
+            a.slots = d_level_slots_.p + b;
+            a.npatches = e - b;
+            launch_step_form(a, e - b);
+            if (with_fill) {
+                d_q_ = s0;  // the ghost fill of the scratch copy (run_plan reads d_q_)
+                try {
+                    run_plan(plan(gmax_, gmax_, 0));
+                } catch (...) {
+                    d_q_ = q_real;
+                    throw;
+                }
+                d_q_ = q_real;
+            }
+        }
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    double ms_per = 0.0;
+    try {
+        one();  // warm-up: plans, tuned forms, first-launch setup
+        check(cudaEventCreate(&e0), "event");
+        check(cudaEventCreate(&e1), "event");
+        check(cudaEventRecord(e0, st_), "event");
+        for (int k = 0; k < launches; ++k) one();
+        check(cudaEventRecord(e1, st_), "event");
+        check(cudaEventSynchronize(e1), "event");
+        float ms = 0.0f;
+        check(cudaEventElapsedTime(&ms, e0, e1), "event");
+        ms_per = ms / launches;
+    } catch (...) {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        arena_free(s0);
+        arena_free(s1);
+        cnt_ = cnt0;
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    arena_free(s0);
+    arena_free(s1);
+    check(cudaStreamSynchronize(st_), "sync");
+    cnt_ = cnt0;  // timing launches are not the solve's
+    step_form_used_ = form0;
+    return ms_per;
+}
+
+double Context::step_kernel_time(double t, double dt, int launches, bool* fused) {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "step_kernel_time before initialize");
+    if (launches < 1) throw Error(FCB_ERR_INVALID, "launches must be >= 1");
+    ensure_ghosts();  // the unfused step reads the scratch copy's ghost cells
+    const bool f = use_fusion(t, dt);
+    *fused = f;
+    return time_steps(f, false, launches, t, dt);
+}
+
 void Context::step_descs(double t, double dt, int req, std::vector<PatchDesc>& out) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "step before initialize");
+    ensure_ghosts();
+    ghosts_filled_ = false;
     double vt = 0.0;
     if (aux_kind_ == AUX_SWIRL) {
         const double pi = 4.0 * std::atan(1.0);
@@ -1797,7 +2099,7 @@ void Context::restore_step() {
 }
 
 size_t Context::device_bytes() const {
-    const int arenas = 3 + (d_qsave_ ? 1 : 0);
+    const int arenas = 3 + (d_qsave_ ? 1 : 0) + (d_qalt_ ? 1 : 0);
     return (size_t)capacity_ * ((size_t)stride_ * arenas + (size_t)aux_stride_ + (size_t)treg_stride_) * sizeof(double) +
            (size_t)capacity_ * sizeof(PatchMeta) + h_ops_.size() * sizeof(GhostOp);
 }
@@ -2229,6 +2531,7 @@ void Context::repopulate_partitioned(const std::vector<Leaf>& old_leaves, const 
 
 bool Context::regrid() {
     if (!initialized_) throw Error(FCB_ERR_STATE, "regrid before initialize");
+    ensure_ghosts();  // tagging and the regrid transfer read ghost cells
     std::vector<int> target;
     tag(false, target);
     std::vector<Leaf> nl;
@@ -2255,6 +2558,8 @@ bool Context::regrid() {
 // fclaw2d_initialize (src/fclaw2d_initialize.c:75-248)
 void Context::initialize() {
     ensure_scalars();
+    ghosts_stale_ = false;
+    ghosts_filled_ = false;  // qinit sets the ghost cells itself (unless init_ghostcell)
     forest_.uniform(opt_.minlevel);
     const int n = num_patches();
     free_slots_.clear();
@@ -2315,8 +2620,11 @@ void Context::run() {
         while (t_curr < tend) {
             const size_t bytes = (size_t)capacity_ * stride_ * sizeof(double);
             (void)arena_bytes;
-            if (!opt_.use_fixed_dt)
+            if (!opt_.use_fixed_dt) {
                 check(cudaMemcpyAsync(d_qsave_, d_q_, bytes, cudaMemcpyDeviceToDevice, st_), "save_time_step");
+                saved_stale_ = ghosts_stale_;  // the copy holds the ghost cells as they are now
+                saved_filled_ = ghosts_filled_;
+            }
             double dt_step = dt_minlevel;
             const double tol = 1e-2 * dt_step;
             int took_small_step = 0;
@@ -2333,6 +2641,8 @@ void Context::run() {
             if ((maxcfl_step > opt_.max_cfl) && opt_.reduce_cfl) {
                 if (!opt_.use_fixed_dt) {
                     check(cudaMemcpyAsync(d_q_, d_qsave_, bytes, cudaMemcpyDeviceToDevice, st_), "restore_time_step");
+                    ghosts_stale_ = saved_stale_;
+                    ghosts_filled_ = saved_filled_;
                     dt_minlevel = dt_minlevel * opt_.desired_cfl / maxcfl_step;
                     continue;
                 }
@@ -2357,6 +2667,7 @@ void Context::run() {
 // The owned patches (all patches on one rank) at their places in the
 // all-leaves layout; the other entries of the host buffer are not touched.
 void Context::get_q(double* host, size_t n, bool qinterp) {
+    ensure_ghosts();
     const size_t ps = patch_size();
     const size_t total = ps * num_patches();
     if (n < total) throw Error(FCB_ERR_INVALID, "host buffer too small");
@@ -2382,6 +2693,7 @@ void Context::get_q(double* host, size_t n, bool qinterp) {
 void Context::output_ascii(int iframe, const std::string& dir) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "output before initialize");
     if (iframe < 0 || iframe > 9999) throw Error(FCB_ERR_INVALID, "frame number must be in 0..9999");
+    ensure_ghosts();
     const size_t ps = patch_size();
     const int n = own_count_;
     std::vector<double> host(ps * (size_t)n);
@@ -2444,6 +2756,8 @@ void Context::set_q(const double* host, size_t n) {
                         opt_.claw_version == 5 ? opt_.meqn : 0, st_),
           "scatter");
     ++cnt_.count_kernel_launches;
+    ghosts_stale_ = false;  // every cell of every patch was just written
+    ghosts_filled_ = false;
     synchronize();
 }
 

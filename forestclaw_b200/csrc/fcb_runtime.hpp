@@ -38,6 +38,11 @@ cudaError_t launch_step_pipe(int solver, int aux_kind, int mwaves, int mx, int m
                              const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_pipe_mixed(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
                                    int claw_version, const StepArgs& a, cudaStream_t st);
+// the ghost-exchange-fused pipelined forms (a.fuse, a.qsrc set; a mesh of one level)
+cudaError_t launch_step_pipe_fused(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, int claw_version,
+                                   const StepArgs& a, cudaStream_t st);
+cudaError_t launch_step_pipe_fused_mixed(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
+                                         int claw_version, const StepArgs& a, cudaStream_t st);
 struct GhostArgs;
 // Lane add/multiply operations per second of this GPU in FP64 (fp64) or FP32
 // (fcb_probe.cu).
@@ -148,10 +153,15 @@ class Context {
     size_t device_bytes() const;
     // fclaw2d_clawpatch_output_ascii: frame iframe into dir/fort.tNNNN, fort.qNNNN
     void output_ascii(int iframe, const std::string& dir);
+    // the step kernel an advance would launch on the current mesh, timed on
+    // scratch arrays (fused: the ghost-exchange-fused step); ms per launch
+    double step_kernel_time(double t, double dt, int launches, bool* fused);
     // autotuner: the step form (1 four-barrier CTA, 2 warp, 3 pipelined) and the
     // ghost-fill unroll used by the last launches
     int step_form_used() const { return step_form_used_; }
     int ghost_unroll_used() const { return ghost_unroll_; }
+    int fused_used() const { return fused_used_; }
+    int bands_used() const { return bands_used_; }
     // --- partitioned solves (fclaw2d_partition.c, fclaw2d_exchange.c) ---
     bool partitioned() const { return comm_ != nullptr; }
     int rank() const { return rank_; }
@@ -266,6 +276,38 @@ class Context {
     DevBuf<int32_t> d_xitems_;
     DevBuf<double> d_xsend_, d_xrecv_;
     double launch_level_step(int level, double t, double dt, unsigned long long* cfl_slot);
+    // --- ghost-exchange fusion on a mesh of one level ---
+    // The fused step reads arena d_q_ (ghost cells through the neighbour table
+    // d_fuse_) and writes the interiors into d_qalt_; the two are then swapped.
+    // The ghost update that would follow is recorded (ghosts_stale_) and run by
+    // ensure_ghosts() before anything reads ghost cells.
+    bool fusion_possible() const;             // mesh, options and step form allow it
+    bool use_fusion(double t, double dt);     // possible and chosen (tuner or forced)
+    double advance_fused(double t, double dt);
+    void launch_fused_step(double t, double dt, const double* src, double* dst, unsigned long long* cfl_slot);
+    // device time of `launches` step launches (fused: the fused step; with_fill:
+    // the unfused step followed by the ghost fill) on scratch copies of q
+    double time_steps(bool fused, bool with_fill, int launches, double t, double dt);
+    void build_fuse_table();
+    void fill_step_args(StepArgs& a, double t, double dt, unsigned long long* cfl_slot) const;
+    void launch_step_form(const StepArgs& a, int n);
+  public:
+    void ensure_ghosts();  // run the deferred ghost update, if one is pending
+  private:
+    double* d_qalt_ = nullptr;
+    DevBuf<FuseNbr> d_fuse_;
+    bool fuse_ok_ = false;        // the table of the current mesh is complete
+    bool ghosts_stale_ = false;
+    int stale_min_ = 0, stale_max_ = 0;
+    double stale_t_ = 0.0;
+    bool saved_stale_ = false;    // ghosts_stale_ of the CFL-retry copy
+    // the ghost cells are what a ghost update of every level gives (or such an
+    // update is pending): a fused step reads exactly these values from the
+    // neighbours.  False after initialize without init_ghostcell (qinit's own
+    // ghost values), set_q and level updates, until the next full ghost update.
+    bool ghosts_filled_ = false;
+    bool saved_filled_ = false;
+    int fused_used_ = 0;          // the last advance ran the fused step
     // --- macro step ---
     void run_schedule(double t, double dt);  // the level schedule of one advance_all_levels
     std::vector<uintptr_t> macro_fingerprint() const;
@@ -336,6 +378,7 @@ class Context {
     int tune_step_form(const StepArgs& a, int n);
     int tune_ghost_unroll(const GhostPlan& g);
     int step_form_used_ = 0;
+    int bands_used_ = 1;             // row bands of the last four-barrier launch
     int ghost_unroll_ = 0;
     std::vector<uintptr_t> macro_key_, macro_seen_;
     fcb_counters_t macro_delta_{};

@@ -40,7 +40,7 @@ double Server::now() const {
 
 int Server::submit(const fcb_options_t& opt) {
     if (opt.subcycle) throw Error(FCB_ERR_INVALID, "served solves use non-subcycled time stepping (subcycle = 0)");
-    if (opt.step_variant == 1 || opt.step_variant == 2)
+    if (opt.step_variant == 1 || opt.step_variant == 2 || opt.step_variant >= 4)
         throw Error(FCB_ERR_INVALID, "served solves use the pipelined step form");
     if (opt.nout != 1) throw Error(FCB_ERR_INVALID, "served solves run to tfinal in one output interval (nout = 1)");
     if (opt.time_sync) throw Error(FCB_ERR_INVALID, "served solves do not run the time synchronisation");

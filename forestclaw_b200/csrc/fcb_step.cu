@@ -79,11 +79,26 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     const int t = threadIdx.x;
     const int pl = t / NX;
     const int c = t - pl * NX;
-    const int pg = blockIdx.x * PPB + pl;
+    // Row bands: band `band` of the patch group updates cell rows [R0, R1) and
+    // streams rows s0..s1; it starts two rows early so that every carried
+    // value its first own row needs (the raw y-interface R0-1, the x-row R0-1)
+    // is computed inside the band.  Raw y-interfaces from before row s0+1 and
+    // finalized ones before s0+2 would see rows the band did not load and are
+    // skipped; the first band keeps the reference's boundary behaviour.
+    const int nb = a.nbands > 1 ? a.nbands : 1;
+    const int band = (int)(blockIdx.x % (unsigned)nb);
+    const int pg = (int)(blockIdx.x / (unsigned)nb) * PPB + pl;
+    const int R0 = band * (NY - 1) / nb, R1 = (band + 1) * (NY - 1) / nb;
+    const int s0 = band == 0 ? 0 : R0 - 2;
+    const int s1 = band == nb - 1 ? NY : R1 + 1;
+    const int ylo = band == 0 ? 1 : s0 + 1;
+    const int flo = band == 0 ? 1 : s0 + 2;
+    const int qlo = band == 0 ? 0 : R0, qhi = band == nb - 1 ? NY : R1;
     const bool active = (pl < PPB) && (pg < a.npatches);
     const int slot = active ? a.slots[pg] : 0;
     const PatchMeta meta = active ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0};
     double* __restrict__ q = a.q + (int64_t)slot * a.q_stride;
+    const double* __restrict__ qin = (nb > 1 ? a.qsrc : a.q) + (int64_t)slot * a.q_stride;
     double* __restrict__ qlast = a.qlast + (int64_t)slot * a.q_stride;
     const bool save_last = active && (meta.flags & PATCH_SAVE_LAST);
     const double dtdx = step_dt(a, meta.level) / meta.dx;
@@ -182,17 +197,17 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     double* gl = s_gl + pl * NX * 2 * M;
     double* gy = s_gy + pl * NX * 2 * M;
 
-    for (int s = 0; s <= NY; ++s) {
+    for (int s = s0; s <= s1; ++s) {
         // ---------------- phase 1: load row s; raw y-interface s ----------------
         if (s < NY && active) {
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 const int64_t k = ((int64_t)m * NY + s) * NX + c;
-                q_n[m] = q[k];
-                if (save_last) qlast[k] = q_n[m];
+                q_n[m] = qin[k];
+                if (save_last && s >= qlo && s < qhi) qlast[k] = q_n[m];
                 qrow[c * M + m] = q_n[m];
             }
-            if (ycol && s >= 1) {
+            if (ycol && s >= ylo) {
                 sol.rpn2(2, q_m1, q_n, AUXV(1, c, s), yw_n, ys_n, yam_n, yap_n, yR_n);
 #pragma unroll
                 for (int mw = 0; mw < W; ++mw) {
@@ -229,7 +244,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
 #pragma unroll
         for (int m = 0; m < M; ++m) { FYm_cur[m] = 0.0; GYd_r[m] = 0.0; GYu_r[m] = 0.0; }
         const int f = s - 1;
-        if (ycol && f >= 1) {
+        if (ycol && f >= flo) {
             double w[W][M];
 #pragma unroll
             for (int mw = 0; mw < W; ++mw)
@@ -325,7 +340,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         double FYp_cur[M];
 #pragma unroll
         for (int m = 0; m < M; ++m) {
-            FYp_cur[m] = (ycol && f >= 1) ? yap_f[m] : 0.0;
+            FYp_cur[m] = (ycol && f >= flo) ? yap_f[m] : 0.0;
             yam_f[m] = yam_n[m];
             yap_f[m] = yap_n[m];
         }
@@ -444,7 +459,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
 
         // ---------------- phase 5: update cell row r = s-2 ----------------
         const int r = s - 2;
-        if (active && r >= 0 && r <= NY - 2 && c <= NX - 2) {
+        if (active && r >= R0 && r < R1 && c <= NX - 2) {
             const double* fxr = s_fx + ((r % 3) * PPB + pl) * NX * 2 * M;
 #pragma unroll
             for (int m = 0; m < M; ++m) {
@@ -519,7 +534,9 @@ cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    const int blocks = (a.npatches + PPB - 1) / PPB;
+    const int nb = a.nbands > 1 ? a.nbands : 1;
+    if (nb > 1 && (!a.qsrc || a.qsrc == a.q || nb > 4)) return cudaErrorInvalidValue;
+    const int blocks = (a.npatches + PPB - 1) / PPB * nb;
     if (blocks == 0) return cudaSuccess;
     step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB><<<blocks, TPB, bytes, st>>>(a);
     return cudaGetLastError();

@@ -7,7 +7,7 @@ namespace fcb {
 
 cudaError_t launch_step_pipe_mixed(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
                                    int claw_version, const StepArgs& a, cudaStream_t st) {
-    return launch_step_pipe_t<float>(solver, aux_kind, mwaves, mx, my, mbc, claw_version, a, st);
+    return launch_step_pipe_t<float, false>(solver, aux_kind, mwaves, mx, my, mbc, claw_version, a, st);
 }
 
 }  // namespace fcb

@@ -129,8 +129,11 @@ struct PipeState {
 // Per-thread constants: column, flags and this thread's element of the rings.
 template <typename R>
 struct PipeThread {
-    double* q;        // q of the patch, offset to column c
+    double* q;        // q of the patch, offset to column c (fused: the patch in the arena written)
     double* qlast;    // qlast of the patch, offset to column c
+    const double* qs; // fused: where rows MBC..MBC+MX-1 of column c are read (neighbour or own patch)
+    unsigned negmid;  // fused: components negated on those rows (bit m: component m; solid walls)
+    int slot;         // fused: the patch's slot
     const double* aux;
     R* rb;            // this thread's element of the R rings
     double* db;       // this thread's element of the FP64 rings
@@ -145,10 +148,87 @@ struct PipeThread {
 // ring slot of row s - d when s == J (mod D) is known at compile time
 __host__ __device__ constexpr int cslot(int J, int d, int D) { return ((J - d) % D + D) % D; }
 
+// Ghost-exchange fusion: where cell (c, s) of the patch in `slot` gets its
+// value when the ghost update that precedes the step is folded into the step.
+// On a mesh of one level that update (fclaw2d_ghost_update_async, one rank)
+// first copies the same-size neighbours' interior cells into the face bands
+// and corner blocks (fclaw2d_clawpatch46_fort_copy_face/_corner, the
+// same-block transform a shift by mx), then applies the physical boundary
+// conditions (clawpack46_bc2_default.f) left, right, bottom, top, each over the
+// whole band including the corner cells.  The bottom/top conditions are
+// applied last, so they are resolved first: a cell of a physical bottom band
+// takes row 1 (extrapolation) or the mirrored row (wall, component 3 negated);
+// then a physical left/right band takes column 1 / mx or the mirrored column
+// (wall, component 2 negated); whatever still lies outside the interior is
+// the copy from the face or corner neighbour that owns it.  *p receives the
+// address of component 0 of the source cell in the arena qsrc; bit m of *neg
+// says that component m is negated.
+template <int MX, int MBC>
+__device__ __forceinline__ void fused_src(const StepArgs& a, int slot, int c, int s, const double*& p,
+                                          unsigned& neg) {
+    constexpr int NX = MX + 2 * MBC;
+    constexpr int HI = MBC + MX;  // first ghost row / column after the interior
+    const FuseNbr* F = a.fuse + slot;
+    int col = c, row = s, sl = slot;
+    neg = 0u;
+    if (row < MBC) {
+        const int bc = __ldg(&F->bc[2]);
+        if (bc == 3) { row = 2 * MBC - 1 - row; neg ^= 4u; }
+        else if (bc != 0) row = MBC;
+    } else if (row >= HI) {
+        const int bc = __ldg(&F->bc[3]);
+        if (bc == 3) { row = 2 * HI - 1 - row; neg ^= 4u; }
+        else if (bc != 0) row = HI - 1;
+    }
+    if (col < MBC) {
+        const int bc = __ldg(&F->bc[0]);
+        if (bc == 3) { col = 2 * MBC - 1 - col; neg ^= 2u; }
+        else if (bc != 0) col = MBC;
+    } else if (col >= HI) {
+        const int bc = __ldg(&F->bc[1]);
+        if (bc == 3) { col = 2 * HI - 1 - col; neg ^= 2u; }
+        else if (bc != 0) col = HI - 1;
+    }
+    const int h = col < MBC ? 0 : (col >= HI ? 2 : 1);
+    const int v = row < MBC ? 0 : (row >= HI ? 2 : 1);
+    if (h != 1 || v != 1) {
+        int n;
+        if (v == 1) n = __ldg(&F->face[h == 0 ? 0 : 1]);
+        else if (h == 1) n = __ldg(&F->face[v == 0 ? 2 : 3]);
+        else n = __ldg(&F->corner[(v == 0 ? 0 : 2) + (h == 0 ? 0 : 1)]);
+        if (n >= 0) {  // always on a complete table; otherwise the patch's own (stale) ghost cell
+            sl = n;
+            col += h == 0 ? MX : (h == 2 ? -MX : 0);
+            row += v == 0 ? MX : (v == 2 ? -MX : 0);
+        }
+    }
+    p = a.qsrc + (int64_t)sl * a.q_stride + (int64_t)row * NX + col;
+}
+
+// Component m of row `row` of this thread's column as the step sees it.
+template <int MX, int MBC, bool FUSED, typename R>
+__device__ __forceinline__ double load_q(const StepArgs& a, const PipeThread<R>& T, int m, int row) {
+    constexpr int NX = MX + 2 * MBC;
+    constexpr int NY = NX;
+    if constexpr (!FUSED) {
+        return T.q[((int64_t)m * NY + row) * NX];
+    } else {
+        if (row >= MBC && row < MBC + MX) {
+            const double v = T.qs[((int64_t)m * NY + row) * NX];
+            return ((T.negmid >> m) & 1u) ? -v : v;
+        }
+        const double* p;
+        unsigned neg;
+        fused_src<MX, MBC>(a, T.slot, T.c, row, p, neg);
+        const double v = p[(int64_t)m * NY * NX];
+        return ((neg >> m) & 1u) ? -v : v;
+    }
+}
+
 // One row-iteration.  J >= 0: s == J (mod 4) at compile time, so every ring
 // slot is a constant; STEADY: s in [4, NY-2], where every stage is active for
 // every row and the row-range tests vanish.
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int PPB, int LIM, int J, bool STEADY>
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int PPB, int LIM, int J, bool STEADY, bool FUSED>
 __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                                           const PipeThread<typename SOL::Real>& T, PipeState<SOL>& S, int s) {
     using R = typename SOL::Real;
@@ -187,8 +267,11 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
 
     // prefetch q(c, s+2); the old value of q(c, s-4) for this iteration's update
     double qnext[M], qold[M];
-    const bool upd = T.active && (V5 ? (s - 4 >= MBC && s - 4 <= MBC + MX - 1 && c >= MBC && c <= MBC + MX - 1)
-                                     : ((STEADY || (s - 4 >= 0 && s - 4 <= NY - 2)) && c <= NX - 2));
+    // a fused step writes the interior cells only: the ghost cells it would
+    // update are overwritten by the ghost update that follows every step on a
+    // mesh of one level, and that update is deferred until the ghost cells are read
+    const bool upd = T.active && ((V5 || FUSED) ? (s - 4 >= MBC && s - 4 <= MBC + MX - 1 && c >= MBC && c <= MBC + MX - 1)
+                                                : ((STEADY || (s - 4 >= 0 && s - 4 <= NY - 2)) && c <= NX - 2));
     {
         // prefetch two rows ahead; the last steady iteration (s = 4 + 4*((NY-5)/4) - 1)
         // still has row s+2 inside the patch for the patch sizes built here
@@ -196,9 +279,9 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
         const bool on = T.active && ((STEADY && STEADY_IN) || s + 2 < NY);
 #pragma unroll
         for (int m = 0; m < M; ++m) {
-            qnext[m] = on ? T.q[((int64_t)m * NY + s + 2) * NX] : 0.0;
+            qnext[m] = on ? load_q<MX, MBC, FUSED>(a, T, m, s + 2) : 0.0;
             if constexpr (PipeState<SOL>::DELAY) qold[m] = S.q_m4[m];
-            else qold[m] = upd ? T.q[((int64_t)m * NY + s - 4) * NX] : 0.0;
+            else qold[m] = upd ? load_q<MX, MBC, FUSED>(a, T, m, s - 4) : 0.0;
         }
     }
 
@@ -600,7 +683,7 @@ constexpr bool pipe_six_ctas() {
     return sizeof(typename SOL::Real) == 4 && SOL::M == 1;
 }
 
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM, bool FUSED>
 __device__ __forceinline__ void step_pipe_body(const StepArgs& a) {
     constexpr int M = SOL::M;
     constexpr int W = SOL::W;
@@ -645,6 +728,22 @@ __device__ __forceinline__ void step_pipe_body(const StepArgs& a) {
     T.ycol = active && c >= 1 && c <= NX - 2;
     T.q = (D ? D->q : a.q + (int64_t)slot * a.q_stride) + cc;
     T.qlast = (D ? D->qlast : a.qlast + (int64_t)slot * a.q_stride) + cc;
+    T.slot = slot;
+    T.qs = nullptr;
+    T.negmid = 0u;
+    if constexpr (FUSED) {
+        // rows MBC..MBC+MX-1 of this column come from one place (own patch,
+        // face neighbour, or the own patch's boundary column); rows outside are
+        // resolved row by row in load_q
+        T.save_last = false;  // a mesh of one level has no patch with finer neighbours
+        if (active) {
+            const double* p0;
+            unsigned neg;
+            fused_src<MX, MBC>(a, slot, cc, MBC, p0, neg);
+            T.qs = p0 - (int64_t)MBC * NX;
+            T.negmid = neg;
+        }
+    }
     T.aux = (AUXK == AUX_STORED && active) ? (D ? D->aux : a.aux + (int64_t)slot * a.aux_stride) + cc : nullptr;
     T.rb = rsm + pls * NX + cc;
     T.db = dsm + pls * NX + cc;
@@ -665,8 +764,8 @@ __device__ __forceinline__ void step_pipe_body(const StepArgs& a) {
     PipeState<SOL> S;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
-        S.qcur[m] = active ? T.q[(int64_t)m * NY * NX] : 0.0;
-        S.qpre[m] = active ? T.q[((int64_t)m * NY + 1) * NX] : 0.0;
+        S.qcur[m] = active ? load_q<MX, MBC, FUSED>(a, T, m, 0) : 0.0;
+        S.qpre[m] = active ? load_q<MX, MBC, FUSED>(a, T, m, 1) : 0.0;
         S.q_m1[m] = 0.0;
         S.q_m2[m] = S.q_m3[m] = S.q_m4[m] = 0.0;
         S.yam_f[m] = S.yap_f[m] = R(0);
@@ -729,15 +828,15 @@ __device__ __forceinline__ void step_pipe_body(const StepArgs& a) {
 
     // ---- rows: ramp-up, steady state (unrolled by the ring period 4), ramp-down ----
     int s = 0;
-    for (; s < 4; ++s) pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, -1, false>(a, sol, T, S, s);
+    for (; s < 4; ++s) pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, -1, false, FUSED>(a, sol, T, S, s);
     constexpr int NSTEADY = NY - 5;  // s = 4 .. NY-2
     for (int rnd = 0; rnd < NSTEADY / 4; ++rnd, s += 4) {
-        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 0, true>(a, sol, T, S, s);
-        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 1, true>(a, sol, T, S, s + 1);
-        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 2, true>(a, sol, T, S, s + 2);
-        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 3, true>(a, sol, T, S, s + 3);
+        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 0, true, FUSED>(a, sol, T, S, s);
+        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 1, true, FUSED>(a, sol, T, S, s + 1);
+        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 2, true, FUSED>(a, sol, T, S, s + 2);
+        pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, 3, true, FUSED>(a, sol, T, S, s + 3);
     }
-    for (; s <= NY + 2; ++s) pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, -1, false>(a, sol, T, S, s);
+    for (; s <= NY + 2; ++s) pipe_iter<SOL, MX, MBC, AUXK, NAUX, PPB, LIM, -1, false, FUSED>(a, sol, T, S, s);
 
     // ---- CFL: warp max, one atomic per warp ----
     // flux2: cfl = max(cfl, dtdx*s, -dtdx*s) over the interfaces.  Rounding is
@@ -761,21 +860,21 @@ __device__ __forceinline__ void step_pipe_body(const StepArgs& a) {
     }
 }
 
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM, bool FUSED>
 __global__ void __launch_bounds__(TPB) step_kernel_pipe(const StepArgs a) {
-    step_pipe_body<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>(a);
+    step_pipe_body<SOL, MX, MBC, AUXK, NAUX, TPB, LIM, FUSED>(a);
 }
 
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM, bool FUSED>
 __global__ void __launch_bounds__(TPB, 6) step_kernel_pipe_six(const StepArgs a) {
-    step_pipe_body<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>(a);
+    step_pipe_body<SOL, MX, MBC, AUXK, NAUX, TPB, LIM, FUSED>(a);
 }
 
 // the one kernel of the two that a form uses (only that one is instantiated)
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM, bool FUSED>
 constexpr auto pipe_kernel() {
-    if constexpr (pipe_six_ctas<SOL>()) return step_kernel_pipe_six<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>;
-    else return step_kernel_pipe<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>;
+    if constexpr (pipe_six_ctas<SOL>()) return step_kernel_pipe_six<SOL, MX, MBC, AUXK, NAUX, TPB, LIM, FUSED>;
+    else return step_kernel_pipe<SOL, MX, MBC, AUXK, NAUX, TPB, LIM, FUSED>;
 }
 
 // ---------------------------------------------------------------------------
@@ -783,14 +882,14 @@ constexpr auto pipe_kernel() {
 // ---------------------------------------------------------------------------
 namespace {
 
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM, bool FUSED>
 cudaError_t launch_pipe_one(const StepArgs& a, cudaStream_t st) {
     constexpr int NX = MX + 2 * MBC;
     constexpr int PPB = TPB / pipe_threads_per_patch<NX, AUXK == AUX_SWIRL>();
     static_assert(PPB >= 1, "patch wider than the CTA");
     using L = PipeSmem<NX, PPB, SOL::M, SOL::W, NAUX, AUXK == AUX_SWIRL, typename SOL::Real, ring_in_fp64<SOL>>;
     const size_t bytes = (size_t)L::BYTES;
-    constexpr auto kernel = pipe_kernel<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>();
+    constexpr auto kernel = pipe_kernel<SOL, MX, MBC, AUXK, NAUX, TPB, LIM, FUSED>();
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -813,22 +912,22 @@ int fixed_limiter(const StepArgs& a) {
     return (l == 3 || l == 4) ? l : 0;
 }
 
-template <class SOL, int MX, int AUXK, int NAUX>
+template <class SOL, int MX, int AUXK, int NAUX, bool FUSED>
 cudaError_t launch_pipe_lim(const StepArgs& a, cudaStream_t st) {
     switch (fixed_limiter<SOL>(a)) {
-        case 3: return launch_pipe_one<SOL, MX, 2, AUXK, NAUX, 128, 3>(a, st);
-        case 4: return launch_pipe_one<SOL, MX, 2, AUXK, NAUX, 128, 4>(a, st);
-        default: return launch_pipe_one<SOL, MX, 2, AUXK, NAUX, 128, 0>(a, st);
+        case 3: return launch_pipe_one<SOL, MX, 2, AUXK, NAUX, 128, 3, FUSED>(a, st);
+        case 4: return launch_pipe_one<SOL, MX, 2, AUXK, NAUX, 128, 4, FUSED>(a, st);
+        default: return launch_pipe_one<SOL, MX, 2, AUXK, NAUX, 128, 0, FUSED>(a, st);
     }
 }
 
-template <class SOL, int AUXK, int NAUX>
+template <class SOL, int AUXK, int NAUX, bool FUSED>
 cudaError_t launch_pipe_mx(int mx, int mbc, const StepArgs& a, cudaStream_t st) {
     if (mbc != 2) return cudaErrorNotSupported;
     switch (mx) {
-        case 8: return launch_pipe_lim<SOL, 8, AUXK, NAUX>(a, st);
-        case 16: return launch_pipe_lim<SOL, 16, AUXK, NAUX>(a, st);
-        case 32: return launch_pipe_lim<SOL, 32, AUXK, NAUX>(a, st);
+        case 8: return launch_pipe_lim<SOL, 8, AUXK, NAUX, FUSED>(a, st);
+        case 16: return launch_pipe_lim<SOL, 16, AUXK, NAUX, FUSED>(a, st);
+        case 32: return launch_pipe_lim<SOL, 32, AUXK, NAUX, FUSED>(a, st);
         default: return cudaErrorNotSupported;
     }
 }
@@ -838,38 +937,40 @@ cudaError_t launch_pipe_mx(int mx, int mbc, const StepArgs& a, cudaStream_t st) 
 // cudaErrorNotSupported: no pipelined form for this (solver, mx, mbc, aux).
 // R: compute type of the Riemann solves, limiters and transverse parts;
 // V5: the clawpack 5 update (fc2d_clawpack5) instead of clawpack 4.6.
-template <typename R, bool V5>
+template <typename R, bool V5, bool FUSED>
 cudaError_t launch_step_pipe_v(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
                                cudaStream_t st) {
     if (mx != my) return cudaErrorNotSupported;
     switch (solver) {
         case SOLVER_ADVECTION:
             if (mwaves != 1) return cudaErrorNotSupported;
-            if (aux_kind == AUX_SWIRL) return launch_pipe_mx<AdvectionSolver<1, R, V5>, AUX_SWIRL, 2>(mx, mbc, a, st);
+            if (aux_kind == AUX_SWIRL) return launch_pipe_mx<AdvectionSolver<1, R, V5>, AUX_SWIRL, 2, FUSED>(mx, mbc, a, st);
             if (aux_kind == AUX_STORED && a.maux == 2)
-                return launch_pipe_mx<AdvectionSolver<1, R, V5>, AUX_STORED, 2>(mx, mbc, a, st);
+                return launch_pipe_mx<AdvectionSolver<1, R, V5>, AUX_STORED, 2, FUSED>(mx, mbc, a, st);
             return cudaErrorNotSupported;
         case SOLVER_SWE_ROE:
             if (mwaves != 3 || aux_kind != AUX_NONE) return cudaErrorNotSupported;
-            return launch_pipe_mx<SweRoeT<R, V5>, AUX_NONE, 0>(mx, mbc, a, st);
+            return launch_pipe_mx<SweRoeT<R, V5>, AUX_NONE, 0, FUSED>(mx, mbc, a, st);
         case SOLVER_EULER4_ROE:
             if (mwaves != 4 || aux_kind != AUX_NONE) return cudaErrorNotSupported;
-            return launch_pipe_mx<Euler4RoeT<R, V5>, AUX_NONE, 0>(mx, mbc, a, st);
+            return launch_pipe_mx<Euler4RoeT<R, V5>, AUX_NONE, 0, FUSED>(mx, mbc, a, st);
         case SOLVER_GEOCLAW_FWAVE:
             if constexpr (!V5) {
                 if (mwaves != 3 || aux_kind != AUX_STORED || a.maux != 1) return cudaErrorNotSupported;
-                return launch_pipe_mx<GeoclawFwaveT<R>, AUX_STORED, 1>(mx, mbc, a, st);
+                return launch_pipe_mx<GeoclawFwaveT<R>, AUX_STORED, 1, FUSED>(mx, mbc, a, st);
             }
             return cudaErrorNotSupported;
         default: return cudaErrorNotSupported;
     }
 }
 
-template <typename R>
+// FUSED: the ghost-exchange-fused form (a.fuse and a.qsrc set; mesh of one level)
+template <typename R, bool FUSED>
 cudaError_t launch_step_pipe_t(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, int claw_version,
                                const StepArgs& a, cudaStream_t st) {
-    if (claw_version == 5) return launch_step_pipe_v<R, true>(solver, aux_kind, mwaves, mx, my, mbc, a, st);
-    return launch_step_pipe_v<R, false>(solver, aux_kind, mwaves, mx, my, mbc, a, st);
+    if (FUSED != (a.fuse != nullptr) || (FUSED && (a.desc || !a.qsrc || a.qsrc == a.q))) return cudaErrorInvalidValue;
+    if (claw_version == 5) return launch_step_pipe_v<R, true, FUSED>(solver, aux_kind, mwaves, mx, my, mbc, a, st);
+    return launch_step_pipe_v<R, false, FUSED>(solver, aux_kind, mwaves, mx, my, mbc, a, st);
 }
 
 }  // namespace fcb

@@ -108,7 +108,9 @@ typedef struct fcb_options {
     /* step kernel form: 0 = chosen by the library, 1 = one CTA per patch group
      * (rows through shared memory, four barriers per row), 2 = warp-synchronous
      * (swirl advection, mx = 8, 16, 32), 3 = software-pipelined CTA form (one
-     * barrier per row; mx = 8, 16, 32); all give identical results */
+     * barrier per row; mx = 8, 16, 32), 4 and 5 = form 1 with every patch's
+     * rows split into 2 or 3 bands of separate CTAs (Roe solvers; more, shorter
+     * row sweeps); all give identical results */
     int step_variant;
     /* arithmetic of the patch update: 0 = FP64 throughout (the reference's
      * arithmetic), 1 = mixed: Riemann solves, limiters, transverse parts and
@@ -140,6 +142,17 @@ typedef struct fcb_options {
      * weighs a leaf of level l by 2^l (its updates per macro step) when it cuts
      * the Morton order into ranges (fclaw2d_partition.c:142) */
     int weighted_partition;
+    /* Ghost-exchange fusion (no counterpart in the reference's options): on a
+     * mesh of one level, fcb_advance_all_levels may fold the ghost update that
+     * follows each step into the next step, which then reads its ghost cells
+     * from the neighbours' interiors (the same values the copy and physical
+     * boundary kernels would write).  The arrays move between two arenas, and
+     * the last ghost update of a macro step is deferred until a call reads
+     * ghost cells (fcb_get_q, fcb_regrid, a level update, ...), so every result
+     * equals the unfused one bit for bit.  0: chosen by the autotuner (the
+     * fused step against the best step form plus the ghost fill), 1: off,
+     * 2: on whenever the mesh has one level (pipelined step form). */
+    int ghost_fusion;
 } fcb_options_t;
 
 typedef struct fcb_counters {
@@ -251,6 +264,15 @@ int fcb_output_ascii(fcb_context_t* ctx, int iframe, const char* dir);
  * exist for the case on its first level update, on scratch copies of the
  * arrays, and keeps the fastest for the process; 0 before the first update. */
 int fcb_autotune_info(fcb_context_t* ctx, int* step_form, int* ghost_unroll);
+/* Device time of the step kernel that fcb_advance_all_levels launches for
+ * the current mesh (no counterpart in the reference; for roofline reports):
+ * `launches` launches over the finest level's patches at (t, dt), on scratch
+ * copies of the patch arrays (the solve's state is untouched), timed with
+ * CUDA events on the context's stream.  *fused = 1 when that is the
+ * ghost-exchange-fused step (ghost cells read from the neighbours), 0 for the
+ * step alone (the ghost fill is a separate launch).  *ms_per_launch receives
+ * the mean time of one launch.  Synchronises the stream. */
+int fcb_step_kernel_time(fcb_context_t* ctx, double t, double dt, int launches, int* fused, double* ms_per_launch);
 /* Floating-point issue rate of the current GPU (no counterpart in the
  * reference; for roofline reports): lane add/multiply operations per second in
  * FP64 (fp64 != 0) or FP32, from independent multiply-then-add chains on one

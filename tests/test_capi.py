@@ -46,7 +46,8 @@ def test_options_layout_matches_header(built, tmp_path):
         " offsetof(fcb_options_t, precision), offsetof(fcb_options_t, macro_graph));"
         " printf(\"%zu %zu %zu\\n\", offsetof(fcb_options_t, dry_tolerance),"
         " offsetof(fcb_options_t, time_sync), offsetof(fcb_options_t, by));"
-        " printf(\"%zu\\n\", offsetof(fcb_options_t, weighted_partition)); return 0;}\n")
+        " printf(\"%zu %zu\\n\", offsetof(fcb_options_t, weighted_partition),"
+        " offsetof(fcb_options_t, ghost_fusion)); return 0;}\n")
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
@@ -63,6 +64,7 @@ def test_options_layout_matches_header(built, tmp_path):
     assert int(out[8]) == _Options.time_sync.offset
     assert int(out[9]) == _Options.by.offset
     assert int(out[10]) == _Options.weighted_partition.offset
+    assert int(out[11]) == _Options.ghost_fusion.offset
 
 
 def test_invalid_options_rejected_before_any_device_call(built):

@@ -254,3 +254,40 @@ def test_cfl_rejection_and_retry(gpu_lib, claw_version):
     assert d.leaves() == o.leaves()
     assert np.array_equal(d.get_q(), _oracle_q(o))
     assert d.curr_time == pytest.approx(cfg.tfinal, rel=1e-12)
+
+
+@pytest.mark.parametrize("variant", [4, 5])
+@pytest.mark.parametrize("solver", ["radialdam", "quadrants"])
+@pytest.mark.parametrize("mx", [8, 32])
+def test_row_bands_uniform(gpu_lib, solver, mx, variant):
+    """The four-barrier form with every patch's rows split into 2 (variant 4)
+    or 3 (variant 5) bands of separate CTAs: each band starts two rows early,
+    reads a copy of the arena and updates its own rows; every array and the
+    CFL number bit for bit."""
+    if solver == "radialdam":
+        cfg, dt = cases.replace(cases.radialdam_uniform(level=2, mx=mx), mthbc=(3, 1, 1, 3),
+                                pparams=(0.3, 0.65, 0.2, 2.0, 1.0)), 0.4 / (mx * 4) / 1.5
+    else:
+        cfg, dt = cases.quadrants_uniform(level=2, mx=mx), 0.3 / (mx * 4) / 2.0
+    o, d = _pair(cfg, step_variant=variant)
+    _macro_steps(o, d, 6, dt, regrid=False)
+
+
+@pytest.mark.parametrize("variant", [4, 5])
+def test_row_bands_amr_time_interpolation(gpu_lib, variant):
+    """Row bands on an AMR shallow-water solve with subcycling: the bands write
+    the pre-step copy (qlast) of the patches with finer neighbours row by row,
+    which the time interpolation reads; mesh and fields bit for bit through
+    regrids."""
+    cfg = cases.radialdam_amr(seed=1, minlevel=2, maxlevel=4, mx=16)
+    o, d = _pair(cfg, step_variant=variant)
+    _macro_steps(o, d, 4, cfg.initial_dt)
+
+
+def test_row_bands_time_sync_rejected(gpu_lib):
+    import forestclaw_b200 as fcb
+
+    opts = cases.to_options(cases.replace(O.radialdam_regression(), time_sync=1))
+    opts.step_variant = 4
+    with pytest.raises(fcb.FcbError):
+        fcb.Solver(opts)

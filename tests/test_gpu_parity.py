@@ -217,6 +217,7 @@ def test_macro_step_graph_replays_bit_exact(gpu_lib):
     for graph in (0, 1):
         opts = cases.to_options(cfg)
         opts.macro_graph = graph
+        opts.ghost_fusion = 1  # this mesh has one level: keep the graph path (fused steps launch directly)
         d = fcb.Solver(opts)
         d.initialize()
         solvers.append(d)
