@@ -1686,13 +1686,15 @@ int Context::tune_step_form(const StepArgs& a, int n) {
         auto it = g_step_form_cache.find(key);
         if (it != g_step_form_cache.end()) return it->second;
     }
-    // codes: form + 8 * (row bands - 1); the Roe systems' four-barrier form
-    // also runs with each patch split into 2 or 3 row bands (shorter row
-    // sweeps, more CTAs: the level update is bound by one CTA's sweep)
+    // codes: form + 8 * (row bands - 1).  The four-barrier form with 2 or 3
+    // row bands (step_variant 4, 5) is not a candidate: on B200 it measured
+    // +1 % (shallow water) and -12 % (Euler) on the AMR configurations, whose
+    // level updates are bound by the SMs' throughput at one 255-register CTA
+    // each, not by the length of one CTA's row sweep.
     std::vector<int> cand;
     if (opt_.precision == 1 || opt_.claw_version == 5 || opt_.solver_kind == SOLVER_GEOCLAW_FWAVE) cand = {3};
     else if (aux_kind_ == AUX_SWIRL) cand = {1, 2, 3};
-    else cand = {1, 3, 1 + 8, 1 + 16};
+    else cand = {1, 3};
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st_, &cs);
     if (cand.size() == 1 || cs != cudaStreamCaptureStatusNone || dry_) return cand.size() == 1 ? cand[0] : default_step_form(opt_);
@@ -1720,7 +1722,14 @@ int Context::tune_step_form(const StepArgs& a, int n) {
     check(cudaEventCreate(&e1), "event");
     int best = default_step_form(opt_);
     float best_ms = 1e30f;
-    for (int code : cand) {
+    // two rounds over the candidates, each candidate's best round counts: a
+    // single timing per form was seen to pick a form ~7 % slower in steady state
+    std::vector<float> best_of(cand.size(), 1e30f);
+    std::vector<char> ok(cand.size(), 1);
+    for (int round = 0; round < 2; ++round)
+    for (size_t ci = 0; ci < cand.size(); ++ci) {
+        if (!ok[ci]) continue;
+        const int code = cand[ci];
         const int v = code % 8, nb = code / 8 + 1;
         auto launch = [&]() -> cudaError_t {
             if (v == 2) return launch_step_warp_swirl(opt_.mx, opt_.mbc, b, st_);
@@ -1739,6 +1748,7 @@ int Context::tune_step_form(const StepArgs& a, int n) {
         };
         if (launch() != cudaSuccess) {  // form not available for this case
             cudaGetLastError();
+            ok[ci] = 0;
             continue;
         }
         check(cudaEventRecord(e0, st_), "event");
@@ -1747,8 +1757,10 @@ int Context::tune_step_form(const StepArgs& a, int n) {
         check(cudaEventSynchronize(e1), "event");
         float ms = 0;
         check(cudaEventElapsedTime(&ms, e0, e1), "event");
-        if (ms < best_ms) { best_ms = ms; best = code; }
+        best_of[ci] = std::min(best_of[ci], ms);
     }
+    for (size_t ci = 0; ci < cand.size(); ++ci)
+        if (ok[ci] && best_of[ci] < best_ms) { best_ms = best_of[ci]; best = cand[ci]; }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     arena_free(tq);
