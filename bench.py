@@ -139,7 +139,8 @@ class ClockSampler:
 # DRAM bytes (read + write) per step-kernel launch, dram__bytes_read.sum +
 # dram__bytes_write.sum from an ncu capture of the same kernel on the same
 # workload (level 8, mx = 16), keyed by (precision, level, mx, fused step).
-_TRAFFIC = {("fp64", 8, 16, False): 356.85e6, ("mixed", 8, 16, False): 357.08e6}
+_TRAFFIC = {("fp64", 8, 16, False): 356.85e6, ("mixed", 8, 16, False): 357.08e6,
+            ("fp64", 8, 16, True): 374.58e6}
 
 
 def _profiled_traffic(args, fused):
