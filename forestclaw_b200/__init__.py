@@ -77,6 +77,7 @@ class _Options(ctypes.Structure):
         ("ax", ctypes.c_double), ("bx", ctypes.c_double), ("ay", ctypes.c_double), ("by", ctypes.c_double),
         ("weighted_partition", ctypes.c_int),
         ("ghost_fusion", ctypes.c_int),
+        ("src_term", ctypes.c_int),
     ]
 
 
@@ -152,6 +153,8 @@ class Options:
     weighted_partition: int = 1
     # ghost-exchange fusion on a mesh of one level: 0 autotuned, 1 off, 2 on
     ghost_fusion: int = 0
+    # [clawpack46] src_term: 1 = the axisymmetric Euler source (shockbubble src2)
+    src_term: int = 0
 
     def to_c(self) -> _Options:
         o = _Options()
@@ -159,7 +162,7 @@ class Options:
                      "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
                      "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
                      "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph", "claw_version",
-                     "time_sync", "weighted_partition", "ghost_fusion"):
+                     "time_sync", "weighted_partition", "ghost_fusion", "src_term"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
                      "desired_cfl", "grav", "gamma", "dry_tolerance"):

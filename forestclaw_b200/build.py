@@ -53,6 +53,7 @@ SOURCES = {
     "fcb_serve.cu": [],
     "fcb_capi.cu": ["-Xcompiler", "-fvisibility=default"],
     "fcb_noalloc.cu": ["-fmad=false"],
+    "fcb_src.cu": ["-fmad=false"],
     "fcb_probe.cu": ["-fmad=false"],
     "fcb_timesync.cu": ["-fmad=false"],
     "fcb_output.cpp": [],

@@ -144,6 +144,9 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
     if ((opt_.mx & (opt_.mx - 1)) != 0) bad("mx must be a power of two");
     if (opt_.macro_graph < 0 || opt_.macro_graph > 2) bad("macro_graph must be 0, 1 or 2");
     if (opt_.ghost_fusion < 0 || opt_.ghost_fusion > 2) bad("ghost_fusion must be 0, 1 or 2");
+    if (opt_.src_term < 0 || opt_.src_term > 1) bad("src_term must be 0 (none) or 1 (axisymmetric Euler source)");
+    if (opt_.src_term == 1 && opt_.solver_kind != FCB_SOLVER_EULER4_ROE)
+        bad("the axisymmetric source (src_term 1) is the Euler equations' (shockbubble src2)");
     if (comm_) opt_.ghost_fusion = 1;  // a partitioned ghost update exchanges between ranks
     if (opt_.claw_version == 0) opt_.claw_version = 4;
     if (opt_.claw_version != 4 && opt_.claw_version != 5) bad("claw_version must be 4 (clawpack 4.6) or 5");
@@ -1340,6 +1343,11 @@ void Context::launch_levels_step_slots(const int32_t* d_slots, int n, int lvl0, 
         dyn_n_ += nlvl;
     }
     launch_step_form(a, n);
+    if (opt_.src_term > 0) {
+        // clawpack46_update: src2 after step2 for every patch of the update
+        check(launch_src2(opt_.src_term, a, opt_.mx, opt_.my, opt_.mbc, opt_.meqn, st_), "src2");
+        ++cnt_.count_kernel_launches;
+    }
 }
 
 // The step launch of a level update in the form chosen for it (the autotuner's,
@@ -1893,6 +1901,7 @@ bool Context::fusion_possible() const {
     // the fused step reads the neighbours' interiors where the unfused one
     // reads its own ghost cells: equal only when those hold a ghost update's values
     return opt_.ghost_fusion != 1 && fuse_ok_ && ghosts_filled_ && !partitioned() && !time_sync_ && !dry_ &&
+           opt_.src_term == 0 &&
            gmin_ == gmax_ &&
            own_count_ > 0 && (opt_.step_variant == 0 || opt_.step_variant == 3) && opt_.mbc == 2 &&
            (opt_.mx == 8 || opt_.mx == 16 || opt_.mx == 32);

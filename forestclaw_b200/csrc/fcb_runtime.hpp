@@ -43,6 +43,8 @@ cudaError_t launch_step_pipe_fused(int solver, int aux_kind, int mwaves, int mx,
                                    const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_pipe_fused_mixed(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
                                          int claw_version, const StepArgs& a, cudaStream_t st);
+// src2 after the step (fcb_src.cu): kind 1 = the axisymmetric Euler source
+cudaError_t launch_src2(int kind, const StepArgs& a, int mx, int my, int mbc, int meqn, cudaStream_t st);
 struct GhostArgs;
 // Lane add/multiply operations per second of this GPU in FP64 (fp64) or FP32
 // (fcb_probe.cu).

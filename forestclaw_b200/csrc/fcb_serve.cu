@@ -44,6 +44,7 @@ int Server::submit(const fcb_options_t& opt) {
         throw Error(FCB_ERR_INVALID, "served solves use the pipelined step form");
     if (opt.nout != 1) throw Error(FCB_ERR_INVALID, "served solves run to tfinal in one output interval (nout = 1)");
     if (opt.time_sync) throw Error(FCB_ERR_INVALID, "served solves do not run the time synchronisation");
+    if (opt.src_term) throw Error(FCB_ERR_INVALID, "served solves have no source-term stage");
     Request r;
     r.id = next_id_++;
     r.opt = opt;

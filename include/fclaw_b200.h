@@ -68,6 +68,14 @@ enum fcb_problem {
                                  * depth p[2] + exp(-p[3]*r2), r2 = (xc-p[0])^2 + (yc-p[1])^2, at rest */
 };
 
+/* Source terms (fc2d_clawpack46_vtable_t / fc2d_clawpack5_vtable_t src2). */
+enum fcb_source {
+    FCB_SOURCE_NONE = 0,
+    FCB_SOURCE_AXISYMMETRIC_EULER = 1  /* euler/2d/shockbubble/user_4.6/src2.f: the axisymmetric Euler
+                                        * source, radius y at the cell centre (its setaux.f); Euler
+                                        * solver (meqn 4) */
+};
+
 /* Refinement criteria (fclaw2d_clawpatch_options "refinement-criteria"). */
 enum fcb_criteria { FCB_TAG_VALUE = 0, FCB_TAG_MINMAX = 1, FCB_TAG_DIFFERENCE = 2, FCB_TAG_GRADIENT = 3 };
 
@@ -153,6 +161,11 @@ typedef struct fcb_options {
      * fused step against the best step form plus the ghost fill), 1: off,
      * 2: on whenever the mesh has one level (pipelined step form). */
     int ghost_fusion;
+    /* [clawpack46] / [clawpack5] src_term: the src2 stage after every patch
+     * step (clawpack46_update, fc2d_clawpack46.cpp:436-440; clawpack5_update,
+     * fc2d_clawpack5.cpp:397-403), selected by enum fcb_source as the Riemann
+     * solvers are (the device cannot call the host's Fortran src2 pointer). */
+    int src_term;
 } fcb_options_t;
 
 typedef struct fcb_counters {

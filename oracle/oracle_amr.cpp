@@ -240,9 +240,14 @@ double Solver::single_step_patch(int p, double t, double dt) {
         b4step2_swirl(opt.mx, opt.my, opt.mbc, opt.maux, xphys(p), yphys(p), dx(p), dy(p), t, dt,
                       opt.pparams[0], d.aux.data());
     d.qlast = d.q;  // fclaw2d_clawpatch_save_current_step
-    if (!opt.time_sync)
-        return step2(opt.solver, opt.method, opt.mx, opt.my, opt.mbc, opt.meqn, opt.maux, d.q.data(),
-                     opt.maux > 0 ? d.aux.data() : nullptr, dx(p), dy(p), dt);
+    if (!opt.time_sync) {
+        const double cfl = step2(opt.solver, opt.method, opt.mx, opt.my, opt.mbc, opt.meqn, opt.maux, d.q.data(),
+                                 opt.maux > 0 ? d.aux.data() : nullptr, dx(p), dy(p), dt);
+        // clawpack46_update: src2 after the step when src_term > 0 (fc2d_clawpack46.cpp:436-440)
+        if (opt.src_term == 1)
+            src2_axisymmetric(opt.mx, opt.my, opt.mbc, opt.meqn, yphys(p), dy(p), opt.solver.gamma1, dt, d.q.data());
+        return cfl;
+    }
     // clawpack46_step2 (fc2d_clawpack46.cpp:316-386): fluxes f(q) at the patch
     // edges before the update, boundary fluctuations after it
     time_sync_store_flux(p, dt);
@@ -250,6 +255,8 @@ double Solver::single_step_patch(int p, double t, double dt) {
     const double cfl = step2(opt.solver, opt.method, opt.mx, opt.my, opt.mbc, opt.meqn, opt.maux, d.q.data(),
                              opt.maux > 0 ? d.aux.data() : nullptr, dx(p), dy(p), dt, &f);
     time_sync_accumulate(p, dt, f);
+    if (opt.src_term == 1)
+        src2_axisymmetric(opt.mx, opt.my, opt.mbc, opt.meqn, yphys(p), dy(p), opt.solver.gamma1, dt, d.q.data());
     return cfl;
 }
 

@@ -39,6 +39,9 @@ struct Options {
     int reduce_cfl = 1;
     // [Options] time-sync (flux-correction and fluctuation-correction on)
     int time_sync = 0;
+    // [clawpack46] src_term with the source of euler/2d/shockbubble/user_4.6/src2.f
+    // (1: axisymmetric Euler source, radius aux(i,j,1) = y at the cell centre)
+    int src_term = 0;
     // [Options] ax, bx, ay, by: the physical extent of the (unmapped) unit square
     double ax = 0.0, bx = 1.0, ay = 0.0, by = 1.0;
     // problem

@@ -21,7 +21,7 @@ enum IOpt {
     I_MTHBC0, I_MTHBC3 = I_MTHBC0 + 3,
     I_MINLEVEL, I_MAXLEVEL, I_SUBCYCLE, I_REGRID_INTERVAL, I_SMOOTH_REFINE, I_SMOOTH_LEVEL,
     I_CRITERIA, I_IVAR, I_USE_FIXED_DT, I_NOUT, I_INIT_GHOSTCELL, I_REDUCE_CFL,
-    I_SOLVER, I_PROBLEM, I_CLAW_VERSION, I_TIME_SYNC, I_COUNT
+    I_SOLVER, I_PROBLEM, I_CLAW_VERSION, I_TIME_SYNC, I_SRC_TERM, I_COUNT
 };
 enum DOpt {
     D_REFINE_TH, D_COARSEN_TH, D_TFINAL, D_INITIAL_DT, D_MAX_CFL, D_DESIRED_CFL,
@@ -43,6 +43,7 @@ Options unpack(const int* io, const double* d) {
     o.solver.kind = io[I_SOLVER]; o.problem = io[I_PROBLEM];
     o.method.version = io[I_CLAW_VERSION];
     o.time_sync = io[I_TIME_SYNC];
+    o.src_term = io[I_SRC_TERM];
     o.ax = d[D_AX]; o.bx = d[D_BX]; o.ay = d[D_AY]; o.by = d[D_BY];
     o.refine_threshold = d[D_REFINE_TH]; o.coarsen_threshold = d[D_COARSEN_TH];
     o.tfinal = d[D_TFINAL]; o.initial_dt = d[D_INITIAL_DT]; o.max_cfl = d[D_MAX_CFL];
@@ -69,6 +70,11 @@ extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
 int orc_iopt_count() { return I_COUNT; }
+// src2_axisymmetric on one patch (the source-term stage alone)
+int orc_src2_axisymmetric(int mx, int my, int mbc, int meqn, double ylower, double dy, double gamma1, double dt,
+                          double* q) {
+    return guard([&] { src2_axisymmetric(mx, my, mbc, meqn, ylower, dy, gamma1, dt, q); });
+}
 int orc_dopt_count() { return D_COUNT; }
 
 // ---- single-patch kernels --------------------------------------------------

@@ -1147,6 +1147,36 @@ void qinit_radialdam(int mx, int my, int mbc, double xlower, double ylower, doub
     }
 }
 
+void src2_axisymmetric(int mx, int my, int mbc, int meqn, double ylower, double dy, double gamma1, double dt,
+                       double* q) {
+    const PatchIdx P(mx, my, mbc);
+    const double dt2 = dt / 2.0;
+    const double ndim1 = 1.0;  // (ndim-1) with ndim = 2, converted to double
+    for (int i = 1; i <= mx; ++i) {
+        for (int j = 1; j <= my; ++j) {
+            const double rad = ylower + (j - 0.5) * dy;
+            double rho = q[P(i, j, 0)];
+            double u = q[P(i, j, 1)] / q[P(i, j, 0)];
+            double v = q[P(i, j, 2)] / q[P(i, j, 0)];
+            double press = gamma1 * (q[P(i, j, 3)] - 0.5 * rho * (u * u + v * v));
+            // Fortran a*b/c*d associates as ((a*b)/c)*d
+            const double qs1 = q[P(i, j, 0)] - dt2 * ndim1 / rad * q[P(i, j, 2)];
+            const double qs2 = q[P(i, j, 1)] - dt2 * ndim1 / rad * (rho * u * v);
+            const double qs3 = q[P(i, j, 2)] - dt2 * ndim1 / rad * (rho * v * v);
+            const double qs4 = q[P(i, j, 3)] - dt2 * ndim1 / rad * v * (q[P(i, j, 3)] + press);
+            rho = qs1;
+            u = qs2 / qs1;
+            v = qs3 / qs1;
+            press = gamma1 * (qs4 - 0.5 * rho * (u * u + v * v));
+            q[P(i, j, 0)] = q[P(i, j, 0)] - dt * ndim1 / rad * qs3;
+            q[P(i, j, 1)] = q[P(i, j, 1)] - dt * ndim1 / rad * (rho * u * v);
+            q[P(i, j, 2)] = q[P(i, j, 2)] - dt * ndim1 / rad * (rho * v * v);
+            q[P(i, j, 3)] = q[P(i, j, 3)] - dt * ndim1 / rad * v * (qs4 + press);
+        }
+    }
+    (void)meqn;
+}
+
 void qinit_hump(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double x0,
                 double y0, double base, double coef, double* q) {
     const PatchIdx P(mx, my, mbc);

@@ -94,6 +94,14 @@ void qinit_bathy(int mx, int my, int mbc, double xlower, double ylower, double d
 void qinit_hump(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double x0,
                 double y0, double base, double coef, double* q);
 
+// euler/2d/shockbubble/user_4.6/src2.f (clawpack5: user_5.0/src2.f90, the
+// same arithmetic): the axisymmetric source of the Euler equations over the
+// interior cells, a two-stage Runge-Kutta step with radius rad = y at the cell
+// centre (shockbubble setaux.f: aux(i,j,1) = ylower + (j-0.5)*dy); components
+// 1-4 change, a tracer (component 5) does not.
+void src2_axisymmetric(int mx, int my, int mbc, int meqn, double ylower, double dy, double gamma1, double dt,
+                       double* q);
+
 // swirl/user_4.6/b4step2.f (+ swirl/psi.f): time-dependent edge velocities.
 void b4step2_swirl(int mx, int my, int mbc, int maux, double xlower, double ylower,
                    double dx, double dy, double t, double dt, double tperiod, double* aux);

@@ -23,7 +23,7 @@ def to_options(cfg: O.Config):
         tfinal=cfg.tfinal, initial_dt=cfg.initial_dt, max_cfl=cfg.max_cfl,
         desired_cfl=cfg.desired_cfl, solver_kind=cfg.solver, problem=cfg.problem,
         grav=cfg.grav, gamma=cfg.gamma, problem_params=cfg.pparams, claw_version=cfg.claw_version,
-        dry_tolerance=cfg.drytol, time_sync=cfg.time_sync, extent=cfg.extent,
+        dry_tolerance=cfg.drytol, time_sync=cfg.time_sync, extent=cfg.extent, src_term=cfg.src_term,
     )
 
 

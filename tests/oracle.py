@@ -28,7 +28,7 @@ _I_FIELDS = (["mx", "my", "mbc", "meqn", "maux", "order0", "order1", "mcapa", "m
              + [f"mthlim{k}" for k in range(8)] + [f"mthbc{k}" for k in range(4)]
              + ["minlevel", "maxlevel", "subcycle", "regrid_interval", "smooth_refine",
                 "smooth_level", "criteria", "ivar", "use_fixed_dt", "nout", "init_ghostcell",
-                "reduce_cfl", "solver", "problem", "claw_version", "time_sync"])
+                "reduce_cfl", "solver", "problem", "claw_version", "time_sync", "src_term"])
 _D_FIELDS = (["refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
               "desired_cfl", "grav", "gamma", "gamma1", "drytol"] + [f"p{k}" for k in range(32)]
              + ["ax", "bx", "ay", "by"])
@@ -74,6 +74,7 @@ class Config:
     drytol: float = 1e-3    # GeoClaw dry tolerance
     time_sync: int = 0      # [Options] time-sync: conservative coarse/fine correction
     extent: tuple = (0.0, 1.0, 0.0, 1.0)  # [Options] ax, bx, ay, by
+    src_term: int = 0       # [clawpack46] src_term: 1 = the axisymmetric Euler source (shockbubble src2)
 
     @property
     def gamma1(self) -> float:
@@ -89,7 +90,7 @@ class Config:
             "criteria": self.criteria, "ivar": self.ivar, "use_fixed_dt": self.use_fixed_dt,
             "nout": self.nout, "init_ghostcell": self.init_ghostcell,
             "reduce_cfl": self.reduce_cfl, "solver": self.solver, "problem": self.problem,
-            "claw_version": self.claw_version, "time_sync": self.time_sync,
+            "claw_version": self.claw_version, "time_sync": self.time_sync, "src_term": self.src_term,
         }
         for k in range(8):
             iv[f"mthlim{k}"] = self.mthlim[k] if k < len(self.mthlim) else 0
@@ -174,6 +175,7 @@ def lib(parallel: bool = False):
     L.orc_conservation.argtypes = [ctypes.c_void_p, dp]
     L.orc_neighbors.argtypes = [ctypes.c_void_p, ctypes.c_int, ip]
     L.orc_step2.argtypes = [ip, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp]
+    L.orc_src2_axisymmetric.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 4 + [dp]
     _libs[key] = L
     return L
 
@@ -284,6 +286,15 @@ def step2(cfg: Config, q: np.ndarray, aux, dx: float, dy: float, dt: float) -> f
     auxp = _dptr(aux) if aux is not None else ctypes.POINTER(ctypes.c_double)()
     _check(lib().orc_step2(ia, da, _dptr(q), auxp, dx, dy, dt, ctypes.byref(c)))
     return c.value
+
+
+def src2_axisymmetric(q: np.ndarray, mbc: int, ylower: float, dy: float, gamma1: float, dt: float):
+    """The oracle's src2 (euler/2d/shockbubble/user_4.6/src2.f) on one patch
+    q[m, j, i] in place."""
+    meqn, ny, nx = q.shape
+    a = np.ascontiguousarray(q)
+    _check(lib().orc_src2_axisymmetric(nx - 2 * mbc, ny - 2 * mbc, mbc, meqn, ylower, dy, gamma1, dt, _dptr(a)))
+    q[...] = a
 
 
 # ---- configurations of the reference regression tests -----------------------

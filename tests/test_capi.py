@@ -47,7 +47,8 @@ def test_options_layout_matches_header(built, tmp_path):
         " printf(\"%zu %zu %zu\\n\", offsetof(fcb_options_t, dry_tolerance),"
         " offsetof(fcb_options_t, time_sync), offsetof(fcb_options_t, by));"
         " printf(\"%zu %zu\\n\", offsetof(fcb_options_t, weighted_partition),"
-        " offsetof(fcb_options_t, ghost_fusion)); return 0;}\n")
+        " offsetof(fcb_options_t, ghost_fusion)); printf(\"%zu\\n\", offsetof(fcb_options_t, src_term));"
+        " return 0;}\n")
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
@@ -65,6 +66,7 @@ def test_options_layout_matches_header(built, tmp_path):
     assert int(out[9]) == _Options.by.offset
     assert int(out[10]) == _Options.weighted_partition.offset
     assert int(out[11]) == _Options.ghost_fusion.offset
+    assert int(out[12]) == _Options.src_term.offset
 
 
 def test_invalid_options_rejected_before_any_device_call(built):

@@ -202,3 +202,46 @@ def test_time_sync_rejected_outside_its_scope():
         with pytest.raises(Exception):
             s.initialize()
             s.run()
+
+
+def test_src2_axisymmetric_restates_the_fortran():
+    """The oracle's src2 (shockbubble user_4.6/src2.f) against a NumPy
+    evaluation of the same formulas with the Fortran association
+    (a*b/c*d = ((a*b)/c)*d, rho*u*v = (rho*u)*v), bit for bit, on random
+    states; a state with v = 0 is left unchanged."""
+    rng = np.random.default_rng(3)
+    mbc, mx, gamma1, dt, ylower, dy = 2, 8, 0.4, 1e-3, 0.25, 1.0 / 64
+    q = np.empty((5, mx + 4, mx + 4))
+    q[0] = rng.uniform(0.5, 2.0, q[0].shape)
+    q[1] = rng.uniform(-1.0, 1.0, q[0].shape)
+    q[2] = rng.uniform(-1.0, 1.0, q[0].shape)
+    q[3] = rng.uniform(2.0, 5.0, q[0].shape)
+    q[4] = rng.uniform(0.0, 1.0, q[0].shape)
+    want = q.copy()
+    dt2 = dt / 2.0
+    for j in range(1, mx + 1):
+        for i in range(1, mx + 1):
+            jj, ii = j + mbc - 1, i + mbc - 1
+            rad = ylower + (j - 0.5) * dy
+            q1, q2, q3, q4 = (float(want[m, jj, ii]) for m in range(4))
+            rho, u, v = q1, q2 / q1, q3 / q1
+            press = gamma1 * (q4 - 0.5 * rho * (u * u + v * v))
+            qs1 = q1 - dt2 * 1.0 / rad * q3
+            qs2 = q2 - dt2 * 1.0 / rad * (rho * u * v)
+            qs3 = q3 - dt2 * 1.0 / rad * (rho * v * v)
+            qs4 = q4 - dt2 * 1.0 / rad * v * (q4 + press)
+            rho, u, v = qs1, qs2 / qs1, qs3 / qs1
+            press = gamma1 * (qs4 - 0.5 * rho * (u * u + v * v))
+            want[0, jj, ii] = q1 - dt * 1.0 / rad * qs3
+            want[1, jj, ii] = q2 - dt * 1.0 / rad * (rho * u * v)
+            want[2, jj, ii] = q3 - dt * 1.0 / rad * (rho * v * v)
+            want[3, jj, ii] = q4 - dt * 1.0 / rad * v * (qs4 + press)
+    got = q.copy()
+    O.src2_axisymmetric(got, mbc, ylower, dy, gamma1, dt)
+    assert np.array_equal(got, want)
+    assert np.array_equal(got[4], q[4])  # the tracer is not a source component
+    still = q.copy()
+    still[2] = 0.0
+    moved = still.copy()
+    O.src2_axisymmetric(moved, mbc, ylower, dy, gamma1, dt)
+    assert np.array_equal(moved, still)
