@@ -200,7 +200,8 @@ def oracle_config(o):
                     problem=o.problem, refine_threshold=o.refine_threshold, coarsen_threshold=o.coarsen_threshold,
                     tfinal=o.tfinal, initial_dt=o.initial_dt, max_cfl=o.max_cfl, desired_cfl=o.desired_cfl,
                     grav=o.grav, gamma=o.gamma, pparams=tuple(o.problem_params), claw_version=o.claw_version,
-                    drytol=o.dry_tolerance, time_sync=o.time_sync, extent=tuple(o.extent), src_term=o.src_term)
+                    drytol=o.dry_tolerance, time_sync=o.time_sync, extent=tuple(o.extent), src_term=o.src_term,
+                    brick=o.brick, periodic_x=o.periodic_x, periodic_y=o.periodic_y)
 
 
 def time_oracle(cfg, dt, steps, warmup):

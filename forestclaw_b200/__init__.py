@@ -22,7 +22,7 @@ import numpy as np
 __all__ = ["Options", "Solver", "Comm", "local_group", "nccl_unique_id", "nccl_comm", "partition_plan", "lib",
            "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
            "SOLVER_EULER4_ROE", "SOLVER_GEOCLAW_FWAVE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM",
-           "PROBLEM_QUADRANTS", "PROBLEM_BATHY", "PROBLEM_RADIALDAM_CELLAVE", "PROBLEM_HUMP",
+           "PROBLEM_QUADRANTS", "PROBLEM_BATHY", "PROBLEM_RADIALDAM_CELLAVE", "PROBLEM_HUMP", "PROBLEM_PERIODIC_DISC",
            "PRECISION_FP64", "PRECISION_MIXED", "measure_fp_rate",
            "TAG_VALUE", "TAG_MINMAX", "TAG_DIFFERENCE", "TAG_GRADIENT", "EXPORTED_SYMBOLS"]
 
@@ -32,6 +32,7 @@ LIBPATH = PKG / "libfclaw_b200.so"
 SOLVER_ADVECTION, SOLVER_SWE_ROE, SOLVER_EULER4_ROE, SOLVER_GEOCLAW_FWAVE = 0, 1, 2, 3
 PROBLEM_SWIRL, PROBLEM_RADIALDAM, PROBLEM_QUADRANTS, PROBLEM_BATHY, PROBLEM_RADIALDAM_CELLAVE = 0, 1, 2, 3, 4
 PROBLEM_HUMP = 5
+PROBLEM_PERIODIC_DISC = 6
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 TAG_VALUE, TAG_MINMAX, TAG_DIFFERENCE, TAG_GRADIENT = 0, 1, 2, 3
 
@@ -78,6 +79,7 @@ class _Options(ctypes.Structure):
         ("weighted_partition", ctypes.c_int),
         ("ghost_fusion", ctypes.c_int),
         ("src_term", ctypes.c_int),
+        ("brick", ctypes.c_int), ("periodic_x", ctypes.c_int), ("periodic_y", ctypes.c_int),
     ]
 
 
@@ -155,6 +157,10 @@ class Options:
     ghost_fusion: int = 0
     # [clawpack46] src_term: 1 = the axisymmetric Euler source (shockbubble src2)
     src_term: int = 0
+    # [Options] mi = mj (a power of two) and periodic_x / periodic_y
+    brick: int = 1
+    periodic_x: int = 0
+    periodic_y: int = 0
 
     def to_c(self) -> _Options:
         o = _Options()
@@ -162,7 +168,8 @@ class Options:
                      "mcapa", "mwaves", "minlevel", "maxlevel", "subcycle", "regrid_interval",
                      "smooth_refine", "smooth_level", "use_fixed_dt", "nout", "init_ghostcell",
                      "reduce_cfl", "solver_kind", "problem", "step_variant", "precision", "macro_graph", "claw_version",
-                     "time_sync", "weighted_partition", "ghost_fusion", "src_term"):
+                     "time_sync", "weighted_partition", "ghost_fusion", "src_term", "brick", "periodic_x",
+                     "periodic_y"):
             setattr(o, name, int(getattr(self, name)))
         for name in ("refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
                      "desired_cfl", "grav", "gamma", "dry_tolerance"):

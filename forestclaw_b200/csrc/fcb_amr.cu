@@ -4,7 +4,8 @@
 //   qinit:     applications/clawpack/advection/2d/swirl/user_4.6/qinit.f,
 //              applications/clawpack/euler/2d/quadrants/user_4.6/qinit.f,
 //              radial dam break (cell-centre test, as configured for this path),
-//              applications/clawpack/shallow/2d/bump/user_4.6/qinit.f (hump)
+//              applications/clawpack/shallow/2d/bump/user_4.6/qinit.f (hump),
+//              applications/clawpack/advection/2d/periodic/user_4.6/qinit.f with fdisc.f
 //   tagging:   src/patches/clawpatch/fort_4.6/fclaw2d_clawpatch46_tag4refinement.f,
 //              fclaw2d_clawpatch46_tag4coarsening.f, fort_user/*_exceeds_th.f90.
 //              Every criterion's verdict is order independent (a running
@@ -28,11 +29,14 @@ __device__ __forceinline__ double bathy_b(double xc, double yc) {
 // fraction of a cell inside the circle r < r0.  zeroin is Brent's method as the
 // reference states it (netlib zeroin, with its "b = b - xm" step); it converges
 // in a few tens of steps on [0, 1], and the loop stops after 1000 in any case.
+// kind 0: radialdam's r^2 - r0^2; kind 1: advection/2d/periodic/fdisc.f,
+// sqrt(x*x + y*y) - r0 (about (x0, y0); the application's disc is at the origin)
 struct DiscD {
     double x0, y0, r0;
+    int kind = 0;
     __device__ double f(double x, double y) const {
         const double r2 = (x - x0) * (x - x0) + (y - y0) * (y - y0);
-        return r2 - r0 * r0;
+        return kind == 0 ? r2 - r0 * r0 : sqrt(r2) - r0;
     }
 };
 
@@ -180,6 +184,11 @@ __global__ void qinit_kernel(const QinitArgs a) {
             q[((int64_t)0 * ny + r) * nx + c] = a.p[3] * win + a.p[4] * (1.0 - win);
             q[((int64_t)1 * ny + r) * nx + c] = 0.0;
             q[((int64_t)2 * ny + r) * nx + c] = 0.0;
+        } else if (a.problem == PROB_PERIODIC_DISC) {
+            // advection/2d/periodic/user_4.6/qinit.f: q(i,j,1) = the cell's fraction inside the disc
+            DiscD dsc{a.p[2], a.p[3], a.p[4]};
+            dsc.kind = 1;
+            q[r * nx + c] = cellave2_d(dsc, mt.xlower + (i - 1.0) * mt.dx, mt.ylower + (j - 1.0) * mt.dy, mt.dx, mt.dy);
         } else if (a.problem == PROB_HUMP) {
             // q(i,j,1) = 0.1d0 + exp(-200.d0*r2), r2 = (xc-x0)**2 + (yc-y0)**2
             const double r2 = (xc - a.p[0]) * (xc - a.p[0]) + (yc - a.p[1]) * (yc - a.p[1]);
@@ -197,10 +206,12 @@ __global__ void qinit_kernel(const QinitArgs a) {
     }
 }
 
-// setaux of the lake-at-rest problem: aux(i,j,1) = b at the cell centres,
-// ghost cells included, for every listed slot.
-__global__ void setaux_kernel(double* aux, int64_t stride, const int32_t* slots, const PatchMeta* meta, int n,
-                              int mx, int my, int mbc) {
+// setaux for every listed slot, ghost cells included: the lake-at-rest
+// problem's aux(i,j,1) = b at the cell centres; the periodic problem's
+// aux(i,j,1) = uvel, aux(i,j,2) = vvel (advection/2d/periodic/user_4.6/
+// clawpack46_setaux.f; further components 0, unused).
+__global__ void setaux_kernel(int problem, int maux, double uvel, double vvel, double* aux, int64_t stride,
+                              const int32_t* slots, const PatchMeta* meta, int n, int mx, int my, int mbc) {
     const int pi = blockIdx.x;
     if (pi >= n) return;
     const int slot = slots[pi];
@@ -209,16 +220,22 @@ __global__ void setaux_kernel(double* aux, int64_t stride, const int32_t* slots,
     double* a = aux + (int64_t)slot * stride;
     for (int k = threadIdx.x; k < nx * ny; k += blockDim.x) {
         const int r = k / nx, c = k - r * nx;
-        const double xc = mt.xlower + (c - mbc + 1 - 0.5) * mt.dx;
-        const double yc = mt.ylower + (r - mbc + 1 - 0.5) * mt.dy;
-        a[k] = bathy_b(xc, yc);
+        if (problem == PROB_BATHY) {
+            const double xc = mt.xlower + (c - mbc + 1 - 0.5) * mt.dx;
+            const double yc = mt.ylower + (r - mbc + 1 - 0.5) * mt.dy;
+            a[k] = bathy_b(xc, yc);
+        } else {
+            a[k] = uvel;
+            a[nx * ny + k] = vvel;
+            for (int m = 2; m < maux; ++m) a[(int64_t)m * nx * ny + k] = 0.0;
+        }
     }
 }
 
-cudaError_t launch_setaux(double* aux, int64_t stride, const int32_t* slots, const PatchMeta* meta, int n, int mx,
-                          int my, int mbc, cudaStream_t st) {
+cudaError_t launch_setaux(int problem, int maux, const double* params, double* aux, int64_t stride,
+                          const int32_t* slots, const PatchMeta* meta, int n, int mx, int my, int mbc, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    setaux_kernel<<<n, 256, 0, st>>>(aux, stride, slots, meta, n, mx, my, mbc);
+    setaux_kernel<<<n, 256, 0, st>>>(problem, maux, params[0], params[1], aux, stride, slots, meta, n, mx, my, mbc);
     return cudaGetLastError();
 }
 

@@ -170,6 +170,7 @@ enum Problem : int32_t {
     PROB_BATHY = 3,
     PROB_RADIALDAM_CELLAVE = 4,  // radialdam/user_4.6/qinit.f with cellave2.f
     PROB_HUMP = 5,               // shallow/2d/bump/user_4.6/qinit.f
+    PROB_PERIODIC_DISC = 6,      // advection/2d/periodic/user_4.6/qinit.f, fdisc.f
 };
 
 struct QinitArgs {

@@ -31,6 +31,10 @@ struct Neighbors {
     int face_pos[4];
     int corner_rel[4];  // 0 = no corner neighbour (boundary or hanging node)
     int corner_nbr[4];
+    // periodic domains: the neighbour adjacent to this leaf is the stored leaf
+    // moved by img * (block width) in x and y (0 unless a periodic side is crossed)
+    int face_img[4][2];
+    int corner_img[4][2];
     int has_fine;       // fclaw2d_patch_has_finegrid_neighbors
     int on_cf;          // fclaw2d_patch_on_coarsefine_interface
 };
@@ -40,6 +44,9 @@ class QuadForest {
     static constexpr int kMaxLevel = 28;
     static constexpr int32_t kRoot = (int32_t)1 << kMaxLevel;
     std::vector<Leaf> leaves;
+    // a periodic brick (p4est brick connectivity with periodic_i / periodic_j):
+    // points across a periodic side wrap to the opposite side
+    bool periodic_x = false, periodic_y = false;
 
     static int32_t width(int level) { return (int32_t)1 << (kMaxLevel - level); }
     // bit b of v (b < 32) to bit 2b
@@ -70,9 +77,27 @@ class QuadForest {
     void sort() {
         std::sort(leaves.begin(), leaves.end(), [](const Leaf& a, const Leaf& b) { return a.key < b.key; });
     }
-    // Leaf containing finest-resolution point (x, y), or -1 outside the block.
-    int locate(int32_t x, int32_t y) const {
-        if (x < 0 || y < 0 || x >= kRoot || y >= kRoot) return -1;
+    // Wrap a point across the periodic sides (img: -1 / +1 per direction it
+    // wrapped); false if it lies outside a non-periodic side.
+    bool wrap(int32_t& x, int32_t& y, int* img = nullptr) const {
+        int ix = 0, iy = 0;
+        if (x < 0 || x >= kRoot) {
+            if (!periodic_x) return false;
+            ix = x < 0 ? -1 : 1;
+            x -= ix * kRoot;
+        }
+        if (y < 0 || y >= kRoot) {
+            if (!periodic_y) return false;
+            iy = y < 0 ? -1 : 1;
+            y -= iy * kRoot;
+        }
+        if (img) { img[0] = ix; img[1] = iy; }
+        return true;
+    }
+    // Leaf containing finest-resolution point (x, y) (wrapped on periodic
+    // sides), or -1 outside the block.
+    int locate(int32_t x, int32_t y, int* img = nullptr) const {
+        if (!wrap(x, y, img)) return -1;
         const uint64_t k = morton(x, y);
         auto it = std::upper_bound(leaves.begin(), leaves.end(), k,
                                    [](uint64_t v, const Leaf& l) { return v < l.key; });
@@ -113,13 +138,14 @@ class QuadForest {
         for (int f = 0; f < 4; ++f) {
             n.face_nbr[f][0] = n.face_nbr[f][1] = -1;
             n.face_pos[f] = -1;
+            n.face_img[f][0] = n.face_img[f][1] = 0;
             // a point just across the face, at the face's low end
             int32_t px = l.x, py = l.y;
             if (f == 0) px = l.x - 1;
             else if (f == 1) px = l.x + h;
             else if (f == 2) py = l.y - 1;
             else py = l.y + h;
-            const int a = locate(px, py);
+            const int a = locate(px, py, n.face_img[f]);
             if (a < 0) { n.face_rel[f] = REL_BOUNDARY; continue; }
             const int la = leaves[a].level;
             if (la == l.level) { n.face_rel[f] = REL_SAMESIZE; n.face_nbr[f][0] = a; }
@@ -140,16 +166,19 @@ class QuadForest {
         for (int c = 0; c < 4; ++c) {
             n.corner_rel[c] = 0;
             n.corner_nbr[c] = -1;
+            n.corner_img[c][0] = n.corner_img[c][1] = 0;
             const int sx = (c & 1) ? 1 : -1, sy = (c & 2) ? 1 : -1;
             const int32_t X = l.x + ((c & 1) ? h : 0), Y = l.y + ((c & 2) ? h : 0);
-            const int a = locate(sx > 0 ? X : X - 1, sy > 0 ? Y : Y - 1);
+            const int a = locate(sx > 0 ? X : X - 1, sy > 0 ? Y : Y - 1, n.corner_img[c]);
             if (a < 0) continue;
             const Leaf& d = leaves[a];
             if (d.level == l.level) { n.corner_rel[c] = REL_SAMESIZE; n.corner_nbr[c] = a; }
             else if (d.level == l.level + 1) { n.corner_rel[c] = REL_HALFSIZE; n.corner_nbr[c] = a; }
             else if (d.level == l.level - 1) {
                 const int32_t hd = width(d.level);
-                const bool corner = (X == d.x || X == d.x + hd) && (Y == d.y || Y == d.y + hd);
+                // the neighbour's image adjacent to this leaf
+                const int32_t dx0 = d.x + n.corner_img[c][0] * kRoot, dy0 = d.y + n.corner_img[c][1] * kRoot;
+                const bool corner = (X == dx0 || X == dx0 + hd) && (Y == dy0 || Y == dy0 + hd);
                 if (corner) { n.corner_rel[c] = REL_DOUBLESIZE; n.corner_nbr[c] = a; }
                 // otherwise a hanging node: no corner neighbour
             } else {

@@ -97,7 +97,7 @@ void append_ascii_patches(const std::string& dir, int iframe, int meqn, int mx, 
         // fclaw2d_clawpatch46_fort_write_grid_header
         std::fprintf(fq, "%s                 grid_number\n", fortran_i(P.global_num, 5).c_str());
         std::fprintf(fq, "%s                 AMR_level\n", fortran_i(P.level, 5).c_str());
-        std::fprintf(fq, "%s                 block_number\n", fortran_i(0, 5).c_str());
+        std::fprintf(fq, "%s                 block_number\n", fortran_i(P.block, 5).c_str());
         std::fprintf(fq, "%s                 mpi_rank\n", fortran_i(mpi_rank, 5).c_str());
         std::fprintf(fq, "%s                 mx\n", fortran_i(mx, 5).c_str());
         std::fprintf(fq, "%s                 my\n", fortran_i(my, 5).c_str());

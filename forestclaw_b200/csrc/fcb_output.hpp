@@ -9,6 +9,7 @@ namespace fcb {
 struct OutputPatch {
     int global_num, level;
     double xlower, ylower, dx, dy;  // physical lower-left corner and spacing
+    int block = 0;  // block of a brick (fclaw2d's blockno), 0 on one block
 };
 
 // Fortran Ew.d edit descriptor (gfortran form: "0.d1..dd", exponent E+xx or +xxx)

@@ -110,13 +110,32 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
     if (opt_.minlevel < 0 || opt_.maxlevel < opt_.minlevel || opt_.maxlevel > 20) bad("bad minlevel/maxlevel");
     if (opt_.threshold_variable < 1 || opt_.threshold_variable > opt_.meqn) bad("bad threshold_variable");
     if (opt_.problem == FCB_PROBLEM_SWIRL && opt_.solver_kind != FCB_SOLVER_ADVECTION) bad("swirl needs advection");
-    if (opt_.solver_kind == FCB_SOLVER_ADVECTION && opt_.problem != FCB_PROBLEM_SWIRL)
-        bad("the advection solver takes its velocities from the swirl stream function");
+    if (opt_.solver_kind == FCB_SOLVER_ADVECTION && opt_.problem != FCB_PROBLEM_SWIRL &&
+        opt_.problem != FCB_PROBLEM_PERIODIC_DISC)
+        bad("the advection solver takes its velocities from the swirl stream function or from stored aux");
+    if (opt_.problem == FCB_PROBLEM_PERIODIC_DISC && (opt_.solver_kind != FCB_SOLVER_ADVECTION || opt_.maux < 2))
+        bad("the periodic disc problem is advection with velocities in aux(1:2) (maux >= 2)");
+    // a brick of b x b blocks is one tree with levels offset by log2(b)
+    // (fclaw2d_map_brick.c: the brick's patch corners are that tree's corners)
+    if (opt_.brick == 0) opt_.brick = 1;
+    if (opt_.brick < 1 || opt_.brick > 1024 || (opt_.brick & (opt_.brick - 1)) != 0)
+        bad("brick (mi = mj) must be a power of two");
+    {
+        int off = 0;
+        while ((1 << off) < opt_.brick) ++off;
+        opt_.minlevel += off;
+        opt_.maxlevel += off;
+        opt_.smooth_level += off;
+    }
+    if ((opt_.periodic_x || opt_.periodic_y) && (opt_.time_sync || comm_))
+        bad("periodic domains run on one rank without time-sync");
+    forest_.periodic_x = opt_.periodic_x != 0;
+    forest_.periodic_y = opt_.periodic_y != 0;
     if ((opt_.problem == FCB_PROBLEM_RADIALDAM || opt_.problem == FCB_PROBLEM_RADIALDAM_CELLAVE ||
          opt_.problem == FCB_PROBLEM_HUMP) &&
         opt_.solver_kind != FCB_SOLVER_SWE_ROE)
         bad("radialdam and hump need SWE");
-    if (opt_.problem < FCB_PROBLEM_SWIRL || opt_.problem > FCB_PROBLEM_HUMP) bad("unknown problem");
+    if (opt_.problem < FCB_PROBLEM_SWIRL || opt_.problem > FCB_PROBLEM_PERIODIC_DISC) bad("unknown problem");
     if (opt_.ax == 0.0 && opt_.bx == 0.0 && opt_.ay == 0.0 && opt_.by == 0.0) {
         opt_.bx = 1.0;  // all four unset: the unit square
         opt_.by = 1.0;
@@ -125,7 +144,7 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
     if (opt_.problem == FCB_PROBLEM_QUADRANTS && opt_.solver_kind != FCB_SOLVER_EULER4_ROE) bad("quadrants needs Euler");
     if ((opt_.problem == FCB_PROBLEM_BATHY) != (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE))
         bad("the bathymetry problem and the GeoClaw f-wave solver go together");
-    aux_kind_ = (opt_.solver_kind == FCB_SOLVER_ADVECTION) ? AUX_SWIRL
+    aux_kind_ = (opt_.solver_kind == FCB_SOLVER_ADVECTION) ? (opt_.problem == FCB_PROBLEM_SWIRL ? AUX_SWIRL : AUX_STORED)
               : (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE) ? AUX_STORED : AUX_NONE;
     if (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE) {
         if (opt_.maux != 1) bad("the GeoClaw solver reads aux(1) = b: maux must be 1");
@@ -430,8 +449,11 @@ void Context::mesh_changed() {
     // the owned leaves in Morton order (all leaves on one rank)
     std::vector<int32_t> all(slot_of_.begin() + own_first_, slot_of_.begin() + own_first_ + own_count_);
     if (!all.empty()) check(cudaMemcpy(d_all_slots_.p, all.data(), all.size() * 4, cudaMemcpyHostToDevice), "all slots");
-    if (opt_.problem == FCB_PROBLEM_BATHY && own_count_ > 0) {
-        check(launch_setaux(d_aux_, aux_stride_, d_all_slots_.p, d_meta_, own_count_, opt_.mx, opt_.my, opt_.mbc, st_),
+    if ((opt_.problem == FCB_PROBLEM_BATHY || opt_.problem == FCB_PROBLEM_PERIODIC_DISC) && own_count_ > 0) {
+        // the stored aux depends on the cell centres only (bathymetry) or is
+        // constant (the periodic problem's velocities): recomputed for every patch
+        check(launch_setaux(opt_.problem, opt_.maux, opt_.problem_params, d_aux_, aux_stride_, d_all_slots_.p, d_meta_,
+                            own_count_, opt_.mx, opt_.my, opt_.mbc, st_),
               "setaux");
         ++cnt_.count_kernel_launches;
     }
@@ -487,26 +509,28 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
             for (int f = 0; f < 4; ++f) {
                 if (nbrs_[p].face_rel[f] != REL_SAMESIZE) continue;
                 const int q = nbrs_[p].face_nbr[f][0];
+                const int* im = nbrs_[p].face_img[f];  // periodic image of q next to p
                 GhostOp o = base(OP_COPY_FACE, p, q, f, t, t);
-                o.dx = (int)((xl(p) - xl(q)) * iw * (double)mx);
-                o.dy = (int)((yl(p) - yl(q)) * iw * (double)my);
+                o.dx = (int)((xl(p) - (xl(q) + im[0])) * iw * (double)mx);
+                o.dy = (int)((yl(p) - (yl(q) + im[1])) * iw * (double)my);
                 ops.push_back(o);
             }
         for (int p : level_list(level))
             for (int c = 0; c < 4; ++c) {
                 if (nbrs_[p].corner_rel[c] != REL_SAMESIZE) continue;
                 const int q = nbrs_[p].corner_nbr[c];
+                const int* im = nbrs_[p].corner_img[c];
                 GhostOp o = base(OP_COPY_CORNER, p, q, c, t, t);
-                o.dx = (int)((xl(p) - xl(q) + 0.) * (iw * (double)mx));
-                o.dy = (int)((yl(p) - yl(q) + 0.) * (iw * (double)my));
+                o.dx = (int)((xl(p) - (xl(q) + im[0]) + 0.) * (iw * (double)mx));
+                o.dy = (int)((yl(p) - (yl(q) + im[1]) + 0.) * (iw * (double)my));
                 ops.push_back(o);
             }
     };
     // half-size transform offset D: fine index = 2*coarse + D
-    auto half = [&](int c, int f, int& Dx, int& Dy) {
+    auto half = [&](int c, int f, const int* im, int& Dx, int& Dy) {
         const double ow = (double)(1 << forest_.leaves[f].level);
-        Dx = (int)((xl(c) - xl(f)) * ow * (double)mx) - 1;
-        Dy = (int)((yl(c) - yl(f)) * ow * (double)my) - 1;
+        Dx = (int)((xl(c) - (xl(f) + im[0])) * ow * (double)mx) - 1;
+        Dy = (int)((yl(c) - (yl(f) + im[1])) * ow * (double)my) - 1;
     };
     // average2ghost (fclaw2d_ghost_fill.c:171-226), interpolate2ghost (:228-287)
     auto coarse_fine = [&](int level, int t, bool average) {
@@ -517,7 +541,7 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
                 for (int ig = 0; ig < 2; ++ig) {
                     const int q = nbrs_[p].face_nbr[f][ig];
                     GhostOp o = average ? base(OP_AVERAGE_FACE, p, q, f, t, 0) : base(OP_INTERP_FACE, q, p, f, 0, t);
-                    half(p, q, o.dx, o.dy);
+                    half(p, q, nbrs_[p].face_img[f], o.dx, o.dy);
                     ops.push_back(o);
                 }
             }
@@ -528,7 +552,7 @@ void Context::build_ops(int minlevel, int maxlevel, int ti, std::vector<GhostOp>
                 if (nbrs_[p].corner_rel[c] != REL_HALFSIZE) continue;
                 const int q = nbrs_[p].corner_nbr[c];
                 GhostOp o = average ? base(OP_AVERAGE_CORNER, p, q, c, t, 0) : base(OP_INTERP_CORNER, q, p, c, 0, t);
-                half(p, q, o.dx, o.dy);
+                half(p, q, nbrs_[p].corner_img[c], o.dx, o.dy);
                 ops.push_back(o);
             }
         }
@@ -2275,6 +2299,8 @@ bool Context::adapt(const std::vector<int>& target, std::vector<Leaf>& out) {
     }
     if (!changed) return false;
     QuadForest f;
+    f.periodic_x = forest_.periodic_x;  // balance wraps across the periodic sides too
+    f.periodic_y = forest_.periodic_y;
     f.leaves = c;
     f.balance();
     out = f.leaves;
@@ -2735,7 +2761,13 @@ void Context::output_ascii(int iframe, const std::string& dir) {
     for (int k = 0; k < n; ++k) {
         const int p = own_first_ + k;
         const PatchMeta m = meta_of(forest_.leaves[p]);
-        ps_out[k] = OutputPatch{p, (int)forest_.leaves[p].level, m.xlower, m.ylower, m.dx, m.dy};
+        // a brick's patches report the block's level and the block number
+        // (blocks in row-major order, block i + mi*j, as fclaw2d_map_brick)
+        int off = 0;
+        while ((1 << off) < opt_.brick) ++off;
+        ps_out[k] = OutputPatch{p, (int)forest_.leaves[p].level - off, m.xlower, m.ylower, m.dx, m.dy};
+        const int64_t bw = (int64_t)QuadForest::kRoot / opt_.brick;
+        ps_out[k].block = (int)(forest_.leaves[p].x / bw + opt_.brick * (forest_.leaves[p].y / bw));
     }
     auto barrier = [&] {
         if (!partitioned()) return;

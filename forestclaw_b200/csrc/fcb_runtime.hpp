@@ -59,8 +59,8 @@ cudaError_t launch_timeinterp(double* q, const double* qlast, double* qti, int64
                               double alpha, cudaStream_t st);
 struct QinitArgs;
 cudaError_t launch_qinit(const QinitArgs& a, cudaStream_t st);
-cudaError_t launch_setaux(double* aux, int64_t stride, const int32_t* slots, const PatchMeta* meta, int n, int mx,
-                          int my, int mbc, cudaStream_t st);
+cudaError_t launch_setaux(int problem, int maux, const double* params, double* aux, int64_t stride,
+                          const int32_t* slots, const PatchMeta* meta, int n, int mx, int my, int mbc, cudaStream_t st);
 struct TagArgs;
 cudaError_t launch_tag(const TagArgs& a, cudaStream_t st);
 cudaError_t launch_regrid(double* q, int64_t stride, const int32_t* ops, const int32_t* fine, int nops,

@@ -571,7 +571,7 @@ cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, in
         case SOLVER_ADVECTION:
             if (mwaves != 1) return cudaErrorInvalidValue;
             if (aux_kind == AUX_SWIRL) return launch_mx<AdvectionSolver<1>, AUX_SWIRL, 2>(mx, mbc, a, st);
-            if (aux_kind == AUX_STORED && a.maux == 2)
+            if (aux_kind == AUX_STORED && a.maux >= 2)
                 return launch_mx<AdvectionSolver<1>, AUX_STORED, 2>(mx, mbc, a, st);
             return cudaErrorInvalidValue;
         case SOLVER_SWE_ROE:

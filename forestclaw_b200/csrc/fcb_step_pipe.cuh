@@ -945,7 +945,7 @@ cudaError_t launch_step_pipe_v(int solver, int aux_kind, int mwaves, int mx, int
         case SOLVER_ADVECTION:
             if (mwaves != 1) return cudaErrorNotSupported;
             if (aux_kind == AUX_SWIRL) return launch_pipe_mx<AdvectionSolver<1, R, V5>, AUX_SWIRL, 2, FUSED>(mx, mbc, a, st);
-            if (aux_kind == AUX_STORED && a.maux == 2)
+            if (aux_kind == AUX_STORED && a.maux >= 2)
                 return launch_pipe_mx<AdvectionSolver<1, R, V5>, AUX_STORED, 2, FUSED>(mx, mbc, a, st);
             return cudaErrorNotSupported;
         case SOLVER_SWE_ROE:

@@ -64,8 +64,11 @@ enum fcb_problem {
     FCB_PROBLEM_RADIALDAM_CELLAVE = 4, /* the reference's radialdam qinit (radialdam/user_4.6/qinit.f):
                                  * depth p[3]*w + p[4]*(1-w), w the fraction of the cell inside the
                                  * circle about (p[0], p[1]) of radius p[2] (cellave2.f) */
-    FCB_PROBLEM_HUMP = 5        /* shallow/2d/bump qinit (user_4.6/qinit.f, user_5.0/qinit.f90):
+    FCB_PROBLEM_HUMP = 5,       /* shallow/2d/bump qinit (user_4.6/qinit.f, user_5.0/qinit.f90):
                                  * depth p[2] + exp(-p[3]*r2), r2 = (xc-p[0])^2 + (yc-p[1])^2, at rest */
+    FCB_PROBLEM_PERIODIC_DISC = 6 /* advection/2d/periodic (user_4.6/qinit.f, fdisc.f, clawpack46_setaux.f):
+                                 * q = the cell's fraction inside the disc of radius p[4] about (p[2], p[3])
+                                 * (cellave2.f), constant velocity (p[0], p[1]) in aux(1:2), maux >= 2 */
 };
 
 /* Source terms (fc2d_clawpack46_vtable_t / fc2d_clawpack5_vtable_t src2). */
@@ -166,6 +169,15 @@ typedef struct fcb_options {
      * fc2d_clawpack5.cpp:397-403), selected by enum fcb_source as the Riemann
      * solvers are (the device cannot call the host's Fortran src2 pointer). */
     int src_term;
+    /* [Options] mi = mj: a brick of brick x brick unmapped blocks (a power of
+     * two; 0 or 1: one block) on [ax, bx] x [ay, by] (fclaw2d_map_brick.c).
+     * It is kept as one quadtree whose levels count from the whole domain:
+     * minlevel/maxlevel/smooth_level are the brick's (per block), and
+     * fcb_patch_info reports block level + log2(brick). */
+    int brick;
+    /* [Options] periodic_x / periodic_y: faces on the domain boundary connect
+     * to the opposite side (one rank, no time-sync) */
+    int periodic_x, periodic_y;
 } fcb_options_t;
 
 typedef struct fcb_counters {

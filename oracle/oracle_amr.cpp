@@ -59,8 +59,26 @@ int Forest::max_level() const {
     return m;
 }
 
-// fclaw2d_patch_face_neighbors (src/forestclaw2d.c:443-541) on one tree.
-int Forest::face_neighbors(int p, int face, int nbr[2], int* pos) const {
+bool Forest::wrap(int32_t& x, int32_t& y, int img[2]) const {
+    int ix = 0, iy = 0;
+    if (x < 0 || x >= kRoot) {
+        if (!periodic_x) return false;
+        ix = x < 0 ? -1 : 1;
+        x -= ix * kRoot;
+    }
+    if (y < 0 || y >= kRoot) {
+        if (!periodic_y) return false;
+        iy = y < 0 ? -1 : 1;
+        y -= iy * kRoot;
+    }
+    if (img) { img[0] = ix; img[1] = iy; }
+    return true;
+}
+
+// fclaw2d_patch_face_neighbors (src/forestclaw2d.c:443-541) on one tree; on a
+// periodic brick the faces on the domain boundary connect to the opposite side
+// (p4est brick connectivity with periodic_i / periodic_j).
+int Forest::face_neighbors(int p, int face, int nbr[2], int* pos, int img[2]) const {
     const Quad& q = leaves[p];
     const int32_t hq = h(q.level);
     int32_t nx = q.x, ny = q.y;
@@ -70,7 +88,9 @@ int Forest::face_neighbors(int p, int face, int nbr[2], int* pos) const {
     else ny += hq;
     nbr[0] = nbr[1] = -1;
     *pos = -1;
-    if (nx < 0 || ny < 0 || nx >= kRoot || ny >= kRoot) return REL_BOUNDARY;
+    int im[2] = {0, 0};
+    if (!wrap(nx, ny, im)) return REL_BOUNDARY;
+    if (img) { img[0] = im[0]; img[1] = im[1]; }
     int k = find(q.level, nx, ny);
     if (k >= 0) { nbr[0] = k; return REL_SAMESIZE; }
     if (q.level > 0) {
@@ -98,13 +118,15 @@ int Forest::face_neighbors(int p, int face, int nbr[2], int* pos) const {
 // fclaw2d_patch_corner_neighbors (src/forestclaw2d.c:986-1112) on one tree:
 // hanging corners (the corner lies inside a larger neighbour's face) have no
 // corner neighbour, as in p4est_mesh's quad_to_corner.
-int Forest::corner_neighbor(int p, int corner, int* nbr) const {
+int Forest::corner_neighbor(int p, int corner, int* nbr, int img[2]) const {
     const Quad& q = leaves[p];
     const int32_t hq = h(q.level);
     const int sx = (corner & 1) ? 1 : -1, sy = (corner & 2) ? 1 : -1;
-    const int32_t cx = q.x + sx * hq, cy = q.y + sy * hq;
+    int32_t cx = q.x + sx * hq, cy = q.y + sy * hq;
     *nbr = -1;
-    if (cx < 0 || cy < 0 || cx >= kRoot || cy >= kRoot) return 0;
+    int im[2] = {0, 0};
+    if (!wrap(cx, cy, im)) return 0;
+    if (img) { img[0] = im[0]; img[1] = im[1]; }
     int k = find(q.level, cx, cy);
     if (k >= 0) { *nbr = k; return REL_SAMESIZE; }
     if (q.level > 0) {
@@ -113,7 +135,8 @@ int Forest::corner_neighbor(int p, int corner, int* nbr) const {
         k = find(q.level - 1, bx, by);
         if (k >= 0) {
             const int32_t X = q.x + (sx > 0 ? hq : 0), Y = q.y + (sy > 0 ? hq : 0);
-            const bool is_corner = (X == bx || X == bx + 2 * hq) && (Y == by || Y == by + 2 * hq);
+            const int32_t bxa = bx + im[0] * kRoot, bya = by + im[1] * kRoot;  // adjacent image
+            const bool is_corner = (X == bxa || X == bxa + 2 * hq) && (Y == bya || Y == bya + 2 * hq);
             if (!is_corner) return 0;  // hanging node
             *nbr = k;
             return REL_DOUBLESIZE;
@@ -144,7 +167,23 @@ int Forest::is_first_sibling(int p) const {
 // --------------------------------------------------------------------------
 // Solver
 // --------------------------------------------------------------------------
-Solver::Solver(const Options& o) : opt(o) {}
+// A brick of b x b blocks (b a power of two) is kept as one tree: block level
+// l is tree level l + log2(b), and the brick's patch corners
+// (xv[block] + xc)/mi (fclaw2d_map_brick.c:75) are the tree's dyadic corners
+// exactly; smooth-level and the level bounds move with the offset.
+Solver::Solver(const Options& o) : opt(o) {
+    int off = 0;
+    if (opt.brick < 1 || (opt.brick & (opt.brick - 1)) != 0)
+        throw std::runtime_error("brick must be a power of two (mi = mj)");
+    while ((1 << off) < opt.brick) ++off;
+    opt.minlevel += off;
+    opt.maxlevel += off;
+    opt.smooth_level += off;
+    forest.periodic_x = opt.periodic_x != 0;
+    forest.periodic_y = opt.periodic_y != 0;
+    if (opt.time_sync && (opt.periodic_x || opt.periodic_y))
+        throw std::runtime_error("time-sync is not built for periodic domains");
+}
 
 double Solver::xlower(int p) const { return (double)forest.leaves[p].x / (double)Forest::kRoot; }
 double Solver::ylower(int p) const { return (double)forest.leaves[p].y / (double)Forest::kRoot; }
@@ -163,6 +202,11 @@ double Solver::dy(int p) const {
     return ((opt.ay + (opt.by - opt.ay) * yu) - (opt.ay + (opt.by - opt.ay) * yl)) / opt.my;
 }
 PatchGeom Solver::geom(int p) const { return PatchGeom{xlower(p), ylower(p), forest.leaves[p].level}; }
+// the periodic image of leaf p adjacent to the patch that found it across a
+// face or corner (img from NeighborInfo; block-width shifts are exact)
+PatchGeom Solver::geom_img(int p, const int img[2]) const {
+    return PatchGeom{xlower(p) + img[0], ylower(p) + img[1], forest.leaves[p].level};
+}
 
 std::vector<int> Solver::patches_at_level(int level) const {
     std::vector<int> v;
@@ -215,6 +259,11 @@ void Solver::qinit_patch(int p) {
             qinit_quadrants(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p),
                             opt.solver.gamma1, pp + 0, pp + 4, pp + 8, pp + 12, pp[16], pp[17], q);
             break;
+        case PROB_PERIODIC_DISC:
+            // pparams: uvel, vvel, x0, y0, r0
+            qinit_disc_fraction(opt.mx, opt.my, opt.mbc, opt.meqn, xphys(p), yphys(p), dx(p), dy(p), pp[2], pp[3],
+                                pp[4], q);
+            break;
         case PROB_HUMP:
             // pparams: x0, y0, base, coef
             qinit_hump(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), pp[0], pp[1], pp[2], pp[3], q);
@@ -231,6 +280,8 @@ void Solver::qinit_patch(int p) {
 void Solver::setaux_patch(int p) {
     if (opt.problem == PROB_BATHY)
         setaux_bathy(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), data[p].aux.data());
+    if (opt.problem == PROB_PERIODIC_DISC)  // pparams: uvel, vvel
+        setaux_velocity(opt.mx, opt.my, opt.mbc, opt.maux, opt.pparams[0], opt.pparams[1], data[p].aux.data());
 }
 
 // clawpack46_update (fc2d_clawpack46.cpp:403-444) for one patch.
@@ -637,9 +688,13 @@ void Solver::set_neighbor_types() {
     nbrs.assign(forest.leaves.size(), NeighborInfo{});
     for (int p = 0; p < (int)forest.leaves.size(); ++p) {
         NeighborInfo& n = nbrs[p];
-        for (int f = 0; f < 4; ++f) n.face_rel[f] = forest.face_neighbors(p, f, n.face_nbr[f], &n.face_pos[f]);
+        for (int f = 0; f < 4; ++f) {
+            n.face_img[f][0] = n.face_img[f][1] = 0;
+            n.face_rel[f] = forest.face_neighbors(p, f, n.face_nbr[f], &n.face_pos[f], n.face_img[f]);
+        }
         for (int c = 0; c < 4; ++c) {
-            n.corner_rel[c] = forest.corner_neighbor(p, c, &n.corner_nbr[c]);
+            n.corner_img[c][0] = n.corner_img[c][1] = 0;
+            n.corner_rel[c] = forest.corner_neighbor(p, c, &n.corner_nbr[c], n.corner_img[c]);
             n.corner_exists[c] = n.corner_rel[c] != 0;
         }
         n.has_finegrid_neighbors = 0;
@@ -671,7 +726,7 @@ void Solver::copy2ghost(int level, int time_interp) {
         for (int f = 0; f < 4; ++f) {
             if (nbrs[p].face_rel[f] != REL_SAMESIZE) continue;
             const int n = nbrs[p].face_nbr[f][0];
-            Transform t{geom(p), geom(n), mx, my};
+            Transform t{geom(p), geom_img(n, nbrs[p].face_img[f]), mx, my};
             copy_face(mx, my, mbc, meqn, q_time_sync(p, time_interp), q_time_sync(n, time_interp), f, t);
         }
     }
@@ -679,7 +734,7 @@ void Solver::copy2ghost(int level, int time_interp) {
         for (int c = 0; c < 4; ++c) {
             if (!nbrs[p].corner_exists[c] || nbrs[p].corner_rel[c] != REL_SAMESIZE) continue;
             const int n = nbrs[p].corner_nbr[c];
-            Transform t{geom(p), geom(n), mx, my};
+            Transform t{geom(p), geom_img(n, nbrs[p].corner_img[c]), mx, my};
             copy_corner(mx, my, mbc, meqn, q_time_sync(p, time_interp), q_time_sync(n, time_interp), c, t);
         }
     }
@@ -694,7 +749,7 @@ void Solver::average2ghost(int coarse_level, int time_interp) {
             if (nbrs[p].face_rel[f] != REL_HALFSIZE) continue;
             for (int ig = 0; ig < 2; ++ig) {
                 const int n = nbrs[p].face_nbr[f][ig];
-                Transform t{geom(p), geom(n), mx, my};
+                Transform t{geom(p), geom_img(n, nbrs[p].face_img[f]), mx, my};
                 average_face(mx, my, mbc, meqn, q_time_sync(p, time_interp), data[n].q.data(), f / 2, f, t);
             }
         }
@@ -704,7 +759,7 @@ void Solver::average2ghost(int coarse_level, int time_interp) {
         for (int c = 0; c < 4; ++c) {
             if (!nbrs[p].corner_exists[c] || nbrs[p].corner_rel[c] != REL_HALFSIZE) continue;
             const int n = nbrs[p].corner_nbr[c];
-            Transform t{geom(p), geom(n), mx, my};
+            Transform t{geom(p), geom_img(n, nbrs[p].corner_img[c]), mx, my};
             average_corner(mx, my, mbc, meqn, q_time_sync(p, time_interp), data[n].q.data(), c, t);
         }
     }
@@ -719,7 +774,7 @@ void Solver::interpolate2ghost(int coarse_level, int time_interp) {
             if (nbrs[p].face_rel[f] != REL_HALFSIZE) continue;
             for (int ig = 0; ig < 2; ++ig) {
                 const int n = nbrs[p].face_nbr[f][ig];
-                Transform t{geom(p), geom(n), mx, my};
+                Transform t{geom(p), geom_img(n, nbrs[p].face_img[f]), mx, my};
                 interpolate_face(mx, my, mbc, meqn, q_time_sync(p, time_interp), data[n].q.data(), f / 2, f, t);
             }
         }
@@ -729,7 +784,7 @@ void Solver::interpolate2ghost(int coarse_level, int time_interp) {
         for (int c = 0; c < 4; ++c) {
             if (!nbrs[p].corner_exists[c] || nbrs[p].corner_rel[c] != REL_HALFSIZE) continue;
             const int n = nbrs[p].corner_nbr[c];
-            Transform t{geom(p), geom(n), mx, my};
+            Transform t{geom(p), geom_img(n, nbrs[p].corner_img[c]), mx, my};
             interpolate_corner(mx, my, mbc, meqn, q_time_sync(p, time_interp), data[n].q.data(), c, t);
         }
     }
@@ -956,6 +1011,8 @@ bool Solver::domain_adapt(std::vector<Quad>& new_leaves) {
     if (!changed) return false;
     // 2:1 balance across faces and corners (p4est_balance, P4EST_CONNECT_FULL)
     Forest f;
+    f.periodic_x = forest.periodic_x;
+    f.periodic_y = forest.periodic_y;
     f.leaves = after_coarsen;
     f.rebuild_index();
     for (;;) {
@@ -968,8 +1025,8 @@ bool Solver::domain_adapt(std::vector<Quad>& new_leaves) {
             for (int dyi = -1; dyi <= 1; ++dyi)
                 for (int dxi = -1; dxi <= 1; ++dxi) {
                     if (dxi == 0 && dyi == 0) continue;
-                    const int32_t cx = q.x + dxi * hq, cy = q.y + dyi * hq;
-                    if (cx < 0 || cy < 0 || cx >= Forest::kRoot || cy >= Forest::kRoot) continue;
+                    int32_t cx = q.x + dxi * hq, cy = q.y + dyi * hq;
+                    if (!forest.wrap(cx, cy, nullptr)) continue;
                     for (int lv = q.level - 2; lv >= 0; --lv) {
                         const int32_t m = ~(Forest::h(lv) - 1);
                         const int k = f.find(lv, cx & m, cy & m);

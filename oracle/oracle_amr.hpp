@@ -16,7 +16,7 @@ namespace orc {
 
 enum Relation { REL_BOUNDARY = 0, REL_HALFSIZE = 1, REL_SAMESIZE = 2, REL_DOUBLESIZE = 3 };
 
-enum Problem { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2, PROB_BATHY = 3, PROB_RADIALDAM_CELLAVE = 4, PROB_HUMP = 5 };
+enum Problem { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2, PROB_BATHY = 3, PROB_RADIALDAM_CELLAVE = 4, PROB_HUMP = 5, PROB_PERIODIC_DISC = 6 };
 
 struct Options {
     // [clawpatch]
@@ -39,6 +39,11 @@ struct Options {
     int reduce_cfl = 1;
     // [Options] time-sync (flux-correction and fluctuation-correction on)
     int time_sync = 0;
+    // [Options] mi = mj = brick (a power of two): a brick of brick x brick
+    // blocks (fclaw2d_map_brick.c) whose leaves are kept as one tree with
+    // levels offset by log2(brick); periodic_x / periodic_y wrap the domain
+    int brick = 1;
+    int periodic_x = 0, periodic_y = 0;
     // [clawpack46] src_term with the source of euler/2d/shockbubble/user_4.6/src2.f
     // (1: axisymmetric Euler source, radius aux(i,j,1) = y at the cell centre)
     int src_term = 0;
@@ -59,6 +64,11 @@ struct NeighborInfo {
     int face_rel[4];
     int face_nbr[4][2];
     int face_pos[4];  // DOUBLESIZE: which half of the big face this patch touches
+    // periodic domains: the neighbour's position adjacent to this patch is its
+    // stored position plus img * (block width) in x and y (0 unless the face or
+    // corner crosses a periodic boundary)
+    int face_img[4][2];
+    int corner_img[4][2];
     int corner_exists[4];
     int corner_rel[4];
     int corner_nbr[4];
@@ -77,8 +87,13 @@ class Forest {
     void rebuild_index();
     int find(int level, int32_t x, int32_t y) const;  // -1 if no leaf
     // Level of the leaf covering cell (level, x, y) searched at level-1..level+1 (-1 if none).
-    int face_neighbors(int p, int face, int nbr[2], int* pos) const;
-    int corner_neighbor(int p, int corner, int* nbr) const;  // returns relation, 0 if none
+    int face_neighbors(int p, int face, int nbr[2], int* pos, int img[2] = nullptr) const;
+    int corner_neighbor(int p, int corner, int* nbr, int img[2] = nullptr) const;  // relation, 0 if none
+    // periodic domains: a point outside the block wraps into it (img receives
+    // -1 / +1 per direction it wrapped); false if it lies outside a
+    // non-periodic side
+    bool wrap(int32_t& x, int32_t& y, int img[2]) const;
+    bool periodic_x = false, periodic_y = false;
     int is_first_sibling(int p) const;
     void sort_morton();
     static uint64_t morton(int32_t x, int32_t y);
@@ -137,6 +152,7 @@ class Solver {
     double dx(int p) const;
     double dy(int p) const;
     PatchGeom geom(int p) const;
+    PatchGeom geom_img(int p, const int img[2]) const;
 
     size_t patch_size() const { return (size_t)opt.meqn * (opt.mx + 2 * opt.mbc) * (opt.my + 2 * opt.mbc); }
     size_t aux_size() const { return (size_t)opt.maux * (opt.mx + 2 * opt.mbc) * (opt.my + 2 * opt.mbc); }

@@ -21,7 +21,8 @@ enum IOpt {
     I_MTHBC0, I_MTHBC3 = I_MTHBC0 + 3,
     I_MINLEVEL, I_MAXLEVEL, I_SUBCYCLE, I_REGRID_INTERVAL, I_SMOOTH_REFINE, I_SMOOTH_LEVEL,
     I_CRITERIA, I_IVAR, I_USE_FIXED_DT, I_NOUT, I_INIT_GHOSTCELL, I_REDUCE_CFL,
-    I_SOLVER, I_PROBLEM, I_CLAW_VERSION, I_TIME_SYNC, I_SRC_TERM, I_COUNT
+    I_SOLVER, I_PROBLEM, I_CLAW_VERSION, I_TIME_SYNC, I_SRC_TERM, I_BRICK, I_PERIODIC_X, I_PERIODIC_Y,
+    I_COUNT
 };
 enum DOpt {
     D_REFINE_TH, D_COARSEN_TH, D_TFINAL, D_INITIAL_DT, D_MAX_CFL, D_DESIRED_CFL,
@@ -44,6 +45,9 @@ Options unpack(const int* io, const double* d) {
     o.method.version = io[I_CLAW_VERSION];
     o.time_sync = io[I_TIME_SYNC];
     o.src_term = io[I_SRC_TERM];
+    o.brick = io[I_BRICK] > 0 ? io[I_BRICK] : 1;
+    o.periodic_x = io[I_PERIODIC_X];
+    o.periodic_y = io[I_PERIODIC_Y];
     o.ax = d[D_AX]; o.bx = d[D_BX]; o.ay = d[D_AY]; o.by = d[D_BY];
     o.refine_threshold = d[D_REFINE_TH]; o.coarsen_threshold = d[D_COARSEN_TH];
     o.tfinal = d[D_TFINAL]; o.initial_dt = d[D_INITIAL_DT]; o.max_cfl = d[D_MAX_CFL];

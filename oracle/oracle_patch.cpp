@@ -932,12 +932,14 @@ void rpn2_cons_update_swe(int meqn, int idir, const double* q, double grav, doub
 
 namespace {
 
-// radialdam/fdisc.f without a mapping: r^2 - r0^2
+// radialdam/fdisc.f without a mapping: r^2 - r0^2 (kind 0); periodic/fdisc.f:
+// sqrt(x*x + y*y) - r0 about (x0, y0) (kind 1)
 struct Disc {
     double x0, y0, r0;
+    int kind = 0;
     double fdisc(double x, double y) const {
         const double r2 = (x - x0) * (x - x0) + (y - y0) * (y - y0);
-        return r2 - r0 * r0;
+        return kind == 0 ? r2 - r0 * r0 : std::sqrt(r2) - r0;
     }
 };
 
@@ -1068,6 +1070,31 @@ void qinit_radialdam_cellave(int mx, int my, int mbc, double xlower, double ylow
             q[P(i, j, 2)] = 0.0;
         }
     }
+}
+
+void setaux_velocity(int mx, int my, int mbc, int maux, double uvel, double vvel, double* aux) {
+    const PatchIdx P(mx, my, mbc);
+    for (int i = 1 - mbc; i <= mx + mbc; ++i)
+        for (int j = 1 - mbc; j <= my + mbc; ++j) {
+            aux[P(i, j, 0)] = uvel;
+            aux[P(i, j, 1)] = vvel;
+            for (int k = 2; k < maux; ++k) aux[P(i, j, k)] = 0.0;  // not set by the reference (unused)
+        }
+}
+
+void qinit_disc_fraction(int mx, int my, int mbc, int meqn, double xlower, double ylower, double dx, double dy,
+                         double x0, double y0, double r0, double* q) {
+    const PatchIdx P(mx, my, mbc);
+    Disc dsc{x0, y0, r0};
+    dsc.kind = 1;
+    for (int m = 0; m < meqn; ++m)
+        for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+            const double xlow = xlower + (i - 1.0) * dx;
+            for (int j = 1 - mbc; j <= my + mbc; ++j) {
+                const double ylow = ylower + (j - 1.0) * dy;
+                q[P(i, j, 0)] = cellave2(dsc, xlow, ylow, dx, dy);  // qinit.f writes q(i,j,1) for every mq
+            }
+        }
 }
 
 void setaux_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double* aux) {

@@ -84,6 +84,14 @@ void qinit_radialdam_cellave(int mx, int my, int mbc, double xlower, double ylow
 // eta = amp exp(-((x-x0)^2 + (y-y0)^2)/width^2) on a lake at rest: h = max(0, eta - b),
 // hu = hv = 0.  p = {x0, y0, amp, width}.
 void setaux_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double* aux);
+
+// advection/2d/periodic: user_4.6/clawpack46_setaux.f (aux(i,j,1) = uvel,
+// aux(i,j,2) = vvel over the whole patch) and user_4.6/qinit.f with fdisc.f
+// (q = the fraction of each cell inside the disc sqrt((x-x0)^2+(y-y0)^2) < r0,
+// cellave2.f; the application's disc is r0 = 0.25 about the origin).
+void setaux_velocity(int mx, int my, int mbc, int maux, double uvel, double vvel, double* aux);
+void qinit_disc_fraction(int mx, int my, int mbc, int meqn, double xlower, double ylower, double dx, double dy,
+                         double x0, double y0, double r0, double* q);
 void qinit_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, const double* p,
                  double* q);
 

@@ -24,6 +24,7 @@ def to_options(cfg: O.Config):
         desired_cfl=cfg.desired_cfl, solver_kind=cfg.solver, problem=cfg.problem,
         grav=cfg.grav, gamma=cfg.gamma, problem_params=cfg.pparams, claw_version=cfg.claw_version,
         dry_tolerance=cfg.drytol, time_sync=cfg.time_sync, extent=cfg.extent, src_term=cfg.src_term,
+        brick=cfg.brick, periodic_x=cfg.periodic_x, periodic_y=cfg.periodic_y,
     )
 
 

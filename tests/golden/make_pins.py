@@ -3,10 +3,10 @@
 The reference's regression tests pin three counters per run
 (src/fclaw2d_finalize.c:140-197): count_amr_advance, global_num_patches and
 count_amr_new_domain.  This script copies those numbers for the runs whose
-configuration lies on this path (swirl and quadrants with clawpack 4.6 and 5,
-bump with clawpack 4.6 and 5, radialdam example 0 with clawpack 4.6 and
-time-sync), so the tests can check the oracle and the CUDA path without the
-reference tree.
+configuration lies on this path (swirl, quadrants, bump and the periodic
+2 x 2 brick with clawpack 4.6 and 5, radialdam example 0 with clawpack 4.6
+and time-sync), so the tests can check the oracle and the CUDA path without
+the reference tree.
 
 Usage: python tests/golden/make_pins.py REFERENCE_ROOT
 """
@@ -33,6 +33,8 @@ RUNS = {
     "quadrants_claw5": "applications/clawpack/euler/2d/quadrants/regression_values_1.csv",
     "bump": "applications/clawpack/shallow/2d/bump/regression_values_0.csv",
     "bump_claw5": "applications/clawpack/shallow/2d/bump/regression_values_1.csv",
+    "periodic": "applications/clawpack/advection/2d/periodic/regression_values_0.csv",
+    "periodic_claw5": "applications/clawpack/advection/2d/periodic/regression_values_1.csv",
 }
 
 

@@ -20,7 +20,7 @@ ORACLE_DIR = ROOT / "oracle"
 # Solver kinds (oracle/oracle_patch.hpp SolverKind)
 ADVECTION, SWE_ROE, EULER4_ROE, GEOCLAW_FWAVE = 0, 1, 2, 3
 # Problems (oracle/oracle_amr.hpp Problem)
-SWIRL, RADIALDAM, QUADRANTS, BATHY, RADIALDAM_CELLAVE, HUMP = 0, 1, 2, 3, 4, 5
+SWIRL, RADIALDAM, QUADRANTS, BATHY, RADIALDAM_CELLAVE, HUMP, PERIODIC_DISC = 0, 1, 2, 3, 4, 5, 6
 # Tagging criteria (oracle/oracle_clawpatch.hpp TagCriteria)
 VALUE, MINMAX, DIFFERENCE, GRADIENT = 0, 1, 2, 3
 
@@ -28,7 +28,8 @@ _I_FIELDS = (["mx", "my", "mbc", "meqn", "maux", "order0", "order1", "mcapa", "m
              + [f"mthlim{k}" for k in range(8)] + [f"mthbc{k}" for k in range(4)]
              + ["minlevel", "maxlevel", "subcycle", "regrid_interval", "smooth_refine",
                 "smooth_level", "criteria", "ivar", "use_fixed_dt", "nout", "init_ghostcell",
-                "reduce_cfl", "solver", "problem", "claw_version", "time_sync", "src_term"])
+                "reduce_cfl", "solver", "problem", "claw_version", "time_sync", "src_term", "brick",
+                "periodic_x", "periodic_y"])
 _D_FIELDS = (["refine_threshold", "coarsen_threshold", "tfinal", "initial_dt", "max_cfl",
               "desired_cfl", "grav", "gamma", "gamma1", "drytol"] + [f"p{k}" for k in range(32)]
              + ["ax", "bx", "ay", "by"])
@@ -75,6 +76,9 @@ class Config:
     time_sync: int = 0      # [Options] time-sync: conservative coarse/fine correction
     extent: tuple = (0.0, 1.0, 0.0, 1.0)  # [Options] ax, bx, ay, by
     src_term: int = 0       # [clawpack46] src_term: 1 = the axisymmetric Euler source (shockbubble src2)
+    brick: int = 1          # [Options] mi = mj: a brick of brick x brick blocks (a power of two)
+    periodic_x: int = 0     # [Options] periodic_x
+    periodic_y: int = 0     # [Options] periodic_y
 
     @property
     def gamma1(self) -> float:
@@ -91,6 +95,7 @@ class Config:
             "nout": self.nout, "init_ghostcell": self.init_ghostcell,
             "reduce_cfl": self.reduce_cfl, "solver": self.solver, "problem": self.problem,
             "claw_version": self.claw_version, "time_sync": self.time_sync, "src_term": self.src_term,
+            "brick": self.brick, "periodic_x": self.periodic_x, "periodic_y": self.periodic_y,
         }
         for k in range(8):
             iv[f"mthlim{k}"] = self.mthlim[k] if k < len(self.mthlim) else 0
@@ -337,6 +342,22 @@ def bump_regression(claw_version: int = 4) -> Config:
                   subcycle=1, solver=SWE_ROE, problem=HUMP, criteria=MINMAX, grav=1.0,
                   pparams=(0.0, 0.0, 0.1, 200.0), claw_version=claw_version,
                   extent=(-2.5, 2.5, -2.5, 2.5))
+
+
+def periodic_regression(claw_version: int = 4) -> Config:
+    """applications/clawpack/advection/2d/periodic/regression.ini on top of
+    that directory's fclaw_options.ini (minmax tagging): a 2 x 2 brick on
+    [-1, 1]^2, periodic in x and y, mx = 8, levels 2-5 of each block, constant
+    velocity (1, 1) in aux(1:2) (maux = 3), q = the fraction of each cell inside
+    the disc of radius 0.25 about the origin; rpn2adv/rpt2adv with the van Leer
+    limiter (mthlim = 3); smooth-level = 5 from fclaw_options.ini."""
+    return Config(mx=8, my=8, mbc=2, meqn=1, maux=3, order=(2, 2), mwaves=1, mthlim=(3,),
+                  mthbc=(1, 1, 1, 1), minlevel=2, maxlevel=5, regrid_interval=1,
+                  refine_threshold=0.25, coarsen_threshold=0.05, smooth_refine=1, smooth_level=5,
+                  tfinal=0.2, initial_dt=0.02, max_cfl=1.0, desired_cfl=0.9, nout=1,
+                  subcycle=1, solver=ADVECTION, problem=PERIODIC_DISC, criteria=MINMAX,
+                  pparams=(1.0, 1.0, 0.0, 0.0, 0.25), claw_version=claw_version,
+                  extent=(-1.0, 1.0, -1.0, 1.0), brick=2, periodic_x=1, periodic_y=1)
 
 
 QUADRANT_STATES = (

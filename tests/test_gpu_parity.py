@@ -143,6 +143,7 @@ PIN_CONFIGS = {
     "swirl": O.swirl_regression, "quadrants": O.quadrants_regression,
     "quadrants_claw5": lambda: O.quadrants_regression(5),
     "bump": O.bump_regression, "bump_claw5": lambda: O.bump_regression(5),
+    "periodic": O.periodic_regression, "periodic_claw5": lambda: O.periodic_regression(5),
 }
 
 
@@ -150,18 +151,21 @@ PIN_CONFIGS = {
 def test_regression_pins_on_gpu(gpu_lib, name):
     """The reference's own regression counters, reproduced by the CUDA path, with
     the final fields equal to the oracle's (bump: 24 advances and 14 new
-    domains; its clawpack 5 run has solid walls, mthbc = 3 on all four sides)."""
+    domains, its clawpack 5 run with solid walls, mthbc = 3 on all four sides;
+    periodic: a 2 x 2 brick periodic in x and y, 8 / 601 / 8)."""
     import json
     from pathlib import Path
 
     pins = json.loads((Path(__file__).parent / "golden" / "regression_pins.json").read_text())[name]["values"]
     cfg = PIN_CONFIGS[name]()
     # swirl velocities come from sin(), the bump's initial depth from exp(): CUDA
-    # and glibc may differ in the last bit there; the Euler runs are exact
-    tol = 0.0 if name.startswith("quadrants") else 1e-11
+    # and glibc may differ in the last bit there; the Euler runs and the
+    # periodic brick (sqrt and arithmetic only) are exact
+    exact = name.startswith("quadrants") or name.startswith("periodic")
+    tol = 0.0 if exact else 1e-11
     o, d = _pair(cfg)
     _assert_same_mesh(o, d)
-    assert _rel_err(d.get_q(), _oracle_q(o)) <= (0.0 if name.startswith("quadrants") else 1e-15)
+    assert _rel_err(d.get_q(), _oracle_q(o)) <= (0.0 if exact else 1e-15)
     o.run()
     d.run()
     c = d.counters()

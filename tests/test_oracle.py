@@ -17,6 +17,7 @@ PIN_CONFIGS = {
     "quadrants": O.quadrants_regression, "quadrants_claw5": lambda: O.quadrants_regression(5),
     "radialdam": O.radialdam_regression,
     "bump": O.bump_regression, "bump_claw5": lambda: O.bump_regression(5),
+    "periodic": O.periodic_regression, "periodic_claw5": lambda: O.periodic_regression(5),
 }
 
 
