@@ -173,10 +173,10 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
     if (opt_.time_sync) {
         if (opt_.solver_kind != FCB_SOLVER_SWE_ROE)
             bad("time-sync needs the conservative flux rpn2_cons, given here for the shallow-water Roe solver");
-        if (opt_.claw_version == 5) bad("time-sync is on the clawpack 4.6 path");
         if (opt_.precision != 0) bad("time-sync is FP64 only");
-        if (opt_.step_variant != 0 && opt_.step_variant != 1)
-            bad("time-sync accumulates its registers in the four-barrier step form (step_variant 0 or 1)");
+        if (opt_.step_variant != 0 && opt_.step_variant != 1 && opt_.step_variant != 3)
+            bad("time-sync accumulates its registers in the four-barrier and pipelined step forms (step_variant 0, 1 "
+                "or 3)");
         time_sync_ = true;
     }
     nx_ = opt_.mx + 2 * opt_.mbc;
@@ -1388,8 +1388,7 @@ void Context::launch_step_form(const StepArgs& a, int n) {
     }
     // the tuner's choice is form + 8 * (row bands - 1): the four-barrier form
     // may split every patch's rows into bands of separate CTAs
-    const int code = time_sync_                  ? 1
-                     : opt_.step_variant == 0      ? tune_step_form(a, n)
+    const int code = opt_.step_variant == 0      ? tune_step_form(a, n)
                      : opt_.step_variant >= 4      ? 1 + 8 * (opt_.step_variant - 3)
                                                    : opt_.step_variant;
     const int v = code % 8, nb = code / 8 + 1;
@@ -1749,6 +1748,7 @@ int Context::tune_step_form(const StepArgs& a, int n) {
     b.qlast = tl;
     b.dyn = nullptr;
     b.cfl_out = d_cfl_ + 3;
+    b.treg = nullptr;  // the trial steps leave the time-sync registers alone
     cudaEvent_t e0, e1;
     check(cudaEventCreate(&e0), "event");
     check(cudaEventCreate(&e1), "event");

@@ -141,9 +141,19 @@ struct PipeThread {
     const double* ty; // swirl: sin^2 table of the patch's node rows
     double dtdx, dtdy, vty, vtx, tx;
     R rdtdx, rdtdy, rhdtdx, rhdtdy;
+    double* treg;     // time-sync: the patch's conservation registers (nullptr: off)
+    double tdy, tdx;  // time-sync: dt*dy and dt*dx
     int c;
     bool active, save_last, ycol, node;
 };
+
+// The pipelined form accumulates the time-sync registers for the
+// shallow-water Roe solver in FP64, the one whose conservative flux
+// (rpn2_cons_update) the flux store has.
+template <class SOL, bool FUSED>
+__host__ __device__ constexpr bool pipe_time_sync() {
+    return !FUSED && std::is_same_v<SOL, SweRoeT<double, SOL::V5>>;
+}
 
 // ring slot of row s - d when s == J (mod D) is known at compile time
 __host__ __device__ constexpr int cslot(int J, int d, int D) { return ((J - d) % D + D) % D; }
@@ -311,7 +321,20 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
     // ---------------- S5: update cell row r = s-4 ----------------
     {
         const int r = s - 4;
-        if (upd) {
+        // time-sync: the boundary fluctuations of the cells next to the patch
+        // edges, inside and outside (clawpack46_time_sync_accumulate_waves,
+        // clawpack5_time_sync_accumulate_waves), which the clawpack 5 update
+        // computes but does not apply to the ghost cells
+        constexpr bool TSYNC = pipe_time_sync<SOL, FUSED>();
+        const int i = c - MBC + 1, j = r - MBC + 1;
+        bool tsr = false;
+        if constexpr (TSYNC) {
+            const bool iin = i >= 1 && i <= MX, jin = j >= 1 && j <= MX;
+            const bool iedge = i == 0 || i == 1 || i == MX || i == MX + 1;
+            const bool jedge = j == 0 || j == 1 || j == MX || j == MX + 1;
+            tsr = T.treg != nullptr && T.active && ((iedge && jin) || (jedge && iin));
+        }
+        if (upd || tsr) {
             const R* fx = T.rb + L::FX + s4(4) * (2 * M * L::PNX);
             const double* gy = T.db + L::GY + s4(4) * (2 * M * L::PNX);
 #pragma unroll
@@ -327,7 +350,28 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 const double fpv = (fxp0 + gyu_l) + gyd;   // fp(i, j)
                 const double gmv = GXs_new[m] + (double)S.FYm2[m];    // gm(i, j+1)
                 const double gpv = S.GXs_prev[m] + (double)S.FYp3[m];  // gp(i, j)
-                *qp = qold[m] - T.dtdx * (fmv - fpv) - T.dtdy * (gmv - gpv);
+                if (upd) *qp = qold[m] - T.dtdx * (fmv - fpv) - T.dtdy * (gmv - gpv);
+                if constexpr (TSYNC) {
+                    if (tsr) {
+                        // each register element has exactly one writer
+                        const RegLayout RL{MX, MX, M};
+                        double* Rg = T.treg;
+                        if (j >= 1 && j <= MX) {
+                            const int k = (j - 1) + MX * m;
+                            if (i == 1) Rg[RL.fp(0) + k] = Rg[RL.fp(0) + k] - T.tdy * fpv;
+                            if (i == 0) Rg[RL.fm(0) + k] = Rg[RL.fm(0) + k] + T.tdy * fmv;       // fm(1, j)
+                            if (i == MX) Rg[RL.fm(1) + k] = Rg[RL.fm(1) + k] + T.tdy * fmv;      // fm(mx+1, j)
+                            if (i == MX + 1) Rg[RL.fp(1) + k] = Rg[RL.fp(1) + k] - T.tdy * fpv;  // fp(mx+1, j)
+                        }
+                        if (i >= 1 && i <= MX) {
+                            const int k = (i - 1) + MX * m;
+                            if (j == 1) Rg[RL.gp(0) + k] = Rg[RL.gp(0) + k] - T.tdx * gpv;
+                            if (j == 0) Rg[RL.gm(0) + k] = Rg[RL.gm(0) + k] + T.tdx * gmv;       // gm(i, 1)
+                            if (j == MX) Rg[RL.gm(1) + k] = Rg[RL.gm(1) + k] + T.tdx * gmv;      // gm(i, my+1)
+                            if (j == MX + 1) Rg[RL.gp(1) + k] = Rg[RL.gp(1) + k] - T.tdx * gpv;  // gp(i, my+1)
+                        }
+                    }
+                }
             }
         }
 #pragma unroll
@@ -760,6 +804,15 @@ __device__ __forceinline__ void step_pipe_body(const StepArgs& a) {
     T.vty = vt / meta.dy;
     T.vtx = vt / meta.dx;
     T.tx = 0.0;
+    T.treg = nullptr;
+    T.tdy = T.tdx = 0.0;
+    if constexpr (pipe_time_sync<SOL, FUSED>()) {
+        if (a.treg && patch_ok && !D) {
+            T.treg = a.treg + (int64_t)slot * a.treg_stride;
+            T.tdy = dt * meta.dy;
+            T.tdx = dt * meta.dx;
+        }
+    }
 
     PipeState<SOL> S;
 #pragma unroll

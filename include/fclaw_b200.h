@@ -143,8 +143,9 @@ typedef struct fcb_options {
     /* [Options] time-sync: conservative correction of coarse cells at
      * coarse/fine faces and of edge cells at same-size faces after every
      * synchronisation of levels (fclaw2d_time_sync.c; flux-correction and
-     * fluctuation-correction on).  Shallow-water Roe solver, clawpack 4.6, FP64,
-     * four-barrier step form (step_variant 0 or 1). */
+     * fluctuation-correction on).  Shallow-water Roe solver, clawpack 4.6 or 5,
+     * FP64, the four-barrier or pipelined step form (step_variant 0, 1 or 3;
+     * clawpack 5: 0 or 3). */
     int time_sync;
     /* [Options] ax, bx, ay, by: physical extent of the block; all four zero
      * means the unit square */

@@ -320,7 +320,8 @@ double Solver::single_step_patch(int p, double t, double dt) {
 // (clawpatch_time_sync_setup, fclaw2d_clawpatch_utils.f:259-310, no manifold).
 void Solver::time_sync_store_flux(int p, double dt) {
     if (opt.solver.kind != SOLVER_SWE_ROE) throw std::runtime_error("time-sync: rpn2_cons for shallow water only");
-    if (opt.method.version != 4) throw std::runtime_error("time-sync: clawpack 4.6 registers only");
+    // clawpack5_time_sync.f has clawpack46_time_sync.f's arithmetic in the q(m,i,j)
+    // layout; the registers take clawpack 5's flux arrays (fc2d_clawpack5.cpp:286-343)
     const int mx = opt.mx, my = opt.my, mbc = opt.mbc, meqn = opt.meqn;
     const PatchIdx P(mx, my, mbc);
     PatchData& d = data[p];

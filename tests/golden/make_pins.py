@@ -5,7 +5,7 @@ The reference's regression tests pin three counters per run
 count_amr_new_domain.  This script copies those numbers for the runs whose
 configuration lies on this path (swirl, quadrants, bump and the periodic
 2 x 2 brick with clawpack 4.6 and 5, radialdam example 0 with clawpack 4.6
-and time-sync), so the tests can check the oracle and the CUDA path without
+and 5 and time-sync), so the tests can check the oracle and the CUDA path without
 the reference tree.
 
 Usage: python tests/golden/make_pins.py REFERENCE_ROOT
@@ -29,6 +29,7 @@ RUNS = {
     "swirl": "applications/clawpack/advection/2d/swirl/regression_values_0.csv",
     "swirl_claw5": "applications/clawpack/advection/2d/swirl/regression_values_1.csv",
     "radialdam": "applications/clawpack/shallow/2d/radialdam/regression_values_0.csv",
+    "radialdam_claw5": "applications/clawpack/shallow/2d/radialdam/regression_values_1.csv",
     "quadrants": "applications/clawpack/euler/2d/quadrants/regression_values_0.csv",
     "quadrants_claw5": "applications/clawpack/euler/2d/quadrants/regression_values_1.csv",
     "bump": "applications/clawpack/shallow/2d/bump/regression_values_0.csv",

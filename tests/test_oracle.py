@@ -15,7 +15,7 @@ PINS = json.loads((Path(__file__).parent / "golden" / "regression_pins.json").re
 PIN_CONFIGS = {
     "swirl": O.swirl_regression, "swirl_claw5": lambda: O.swirl_regression(5),
     "quadrants": O.quadrants_regression, "quadrants_claw5": lambda: O.quadrants_regression(5),
-    "radialdam": O.radialdam_regression,
+    "radialdam": O.radialdam_regression, "radialdam_claw5": lambda: O.radialdam_regression(5),
     "bump": O.bump_regression, "bump_claw5": lambda: O.bump_regression(5),
     "periodic": O.periodic_regression, "periodic_claw5": lambda: O.periodic_regression(5),
 }
@@ -27,8 +27,8 @@ def test_regression_pins(name):
     global_num_patches and count_amr_new_domain of the clawpack 4.6 runs and
     the --user:claw-version=5 runs of swirl, quadrants and bump (bump's
     clawpack 5 run has solid walls on all four sides, 14 new domains in 24
-    advances), and of the radialdam run (time-sync, cellave2 initial depth,
-    gradient tagging on [-2.5, 2.5]^2)."""
+    advances), and of the radialdam runs with clawpack 4.6 and 5 (time-sync,
+    cellave2 initial depth, gradient tagging on [-2.5, 2.5]^2)."""
     cfg = PIN_CONFIGS[name]()
     s = O.OracleSolver(cfg)
     s.initialize()
