@@ -197,7 +197,7 @@ def test_cellave_initial_depth():
 def test_time_sync_rejected_outside_its_scope():
     import dataclasses
 
-    for kw in ({"claw_version": 5}, {"solver": O.EULER4_ROE, "meqn": 4, "mwaves": 4}):
+    for kw in ({"solver": O.EULER4_ROE, "meqn": 4, "mwaves": 4},):
         cfg = dataclasses.replace(_fixed_mesh_dam(1), tfinal=0.01, **kw)
         s = O.OracleSolver(cfg)
         with pytest.raises(Exception):
