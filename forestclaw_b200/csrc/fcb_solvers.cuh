@@ -31,7 +31,15 @@ struct AdvectionSolver {
     static constexpr int M = 1;
     static constexpr int W = W_;
     struct Roe {};
+    // no per-cell quantities to share between the interfaces of a cell
+    struct Cell {};
+    static constexpr int NC = 0;
     R grav, gamma, gamma1, drytol;  // unused
+    __device__ __forceinline__ void prep(const R*, Cell&) const {}
+    __device__ __forceinline__ void rpn2c(int ixy, const R* qL, const R* qR, const Cell&, const Cell&, R speed,
+                                          R (*wave)[M], R* s, R* amdq, R* apdq, Roe& rr) const {
+        rpn2(ixy, qL, qR, speed, wave, s, amdq, apdq, rr);
+    }
     __device__ __forceinline__ void rpn2(int /*ixy*/, const R* qL, const R* qR, R speed,
                                          R (*wave)[M], R* s, R* amdq, R* apdq,
                                          Roe&) const {
@@ -75,18 +83,38 @@ struct SweRoeT {
     static constexpr int M = 3;
     static constexpr int W = 3;
     struct Roe { R u, v, a; };
+    // Quantities of one cell that every Riemann problem it takes part in (two
+    // x- and two y-interfaces) evaluates with the same operations on the same
+    // operands: sqrt(h), hu/sqrt(h), hv/sqrt(h), hu/h, hv/h, sqrt(g h).  The
+    // step kernels compute them once per cell; the values are bit-identical.
+    struct Cell { R sq, rq[2], vel[2], c; };
+    static constexpr int NC = 6;
     R grav, gamma, gamma1, drytol;  // drytol: GeoClaw only
-    __device__ __forceinline__ void rpn2(int ixy, const R* qL, const R* qR, R /*speed*/,
+    __device__ __forceinline__ void prep(const R* q, Cell& k) const {
+        k.sq = sqrt(q[0]);
+        k.rq[0] = q[1] / k.sq;
+        k.rq[1] = q[2] / k.sq;
+        k.vel[0] = q[1] / q[0];
+        k.vel[1] = q[2] / q[0];
+        k.c = sqrt(grav * q[0]);
+    }
+    __device__ __forceinline__ void rpn2(int ixy, const R* qL, const R* qR, R speed,
                                          R (*wave)[M], R* s, R* amdq, R* apdq,
                                          Roe& rr) const {
+        Cell cl, cr;
+        prep(qL, cl);
+        prep(qR, cr);
+        rpn2c(ixy, qL, qR, cl, cr, speed, wave, s, amdq, apdq, rr);
+    }
+    __device__ __forceinline__ void rpn2c(int ixy, const R* qL, const R* qR, const Cell& cl, const Cell& cr,
+                                          R /*speed*/, R (*wave)[M], R* s, R* amdq, R* apdq,
+                                          Roe& rr) const {
         const int mu = (ixy == 1) ? 1 : 2;
         const int mv = (ixy == 1) ? 2 : 1;
         const R h = (qL[0] + qR[0]) / R(2.0);
-        const R hsqrtl = sqrt(qL[0]);
-        const R hsqrtr = sqrt(qR[0]);
-        const R hsq2 = hsqrtl + hsqrtr;
-        const R u = (qL[mu] / hsqrtl + qR[mu] / hsqrtr) / hsq2;
-        const R v = (qL[mv] / hsqrtl + qR[mv] / hsqrtr) / hsq2;
+        const R hsq2 = cl.sq + cr.sq;                       // sqrt(qL(1)) + sqrt(qR(1))
+        const R u = (cl.rq[mu - 1] + cr.rq[mu - 1]) / hsq2;  // (qL(mu)/hsqrtl + qR(mu)/hsqrtr)/hsq2
+        const R v = (cl.rq[mv - 1] + cr.rq[mv - 1]) / hsq2;
         const R a = sqrt(grav * h);
         rr.u = u; rr.v = v; rr.a = a;
         const R d1 = qR[0] - qL[0];
@@ -101,8 +129,7 @@ struct SweRoeT {
         // entropy fix
         R am[3];
         {
-            const R him1 = qL[0];
-            const R s0 = qL[mu] / him1 - sqrt(grav * him1);
+            const R s0 = cl.vel[mu - 1] - cl.c;  // qL(mu)/him1 - sqrt(g*him1)
             R sfract;
             if (s0 > R(0.0) && s[0] > R(0.0)) {
                 am[0] = am[1] = am[2] = R(0.0);
@@ -122,8 +149,7 @@ struct SweRoeT {
 #pragma unroll
             for (int m = 0; m < 3; ++m) am[m] = am[m] + s[1] * wave[1][m];
             {
-                const R hi = qR[0];
-                const R s03 = qR[mu] / hi + sqrt(grav * hi);
+                const R s03 = cr.vel[mu - 1] + cr.c;  // qR(mu)/hi + sqrt(g*hi)
                 const R h3 = qR[0] - wave[2][0];
                 const R hu3 = qR[mu] - wave[2][mu];
                 const R s3 = hu3 / h3 + sqrt(grav * h3);
@@ -184,20 +210,41 @@ struct Euler4RoeT {
     static constexpr int M = 4;
     static constexpr int W = 4;
     struct Roe { R u, v, a, enth, u2v2, g1a2, euv; };
+    // Quantities of one cell shared by the four Riemann problems it takes part
+    // in: sqrt(rho), rho u/sqrt(rho), rho v/sqrt(rho), (E + p)/sqrt(rho), u, v
+    // and the sound speed sqrt(gamma p/rho).  The entropy fix's pressure sums
+    // the squared momenta in the normal direction's order, which equals p
+    // (addition commutes exactly), so every value is bit-identical.
+    struct Cell { R sq, rq[2], rh, vel[2], c; };
+    static constexpr int NC = 7;
     R grav, gamma, gamma1, drytol;  // drytol: GeoClaw only
-    __device__ __forceinline__ void rpn2(int ixy, const R* qL, const R* qR, R,
+    __device__ __forceinline__ void prep(const R* q, Cell& k) const {
+        k.sq = sqrt(q[0]);
+        const R p = gamma1 * (q[3] - R(0.5) * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+        k.rq[0] = q[1] / k.sq;
+        k.rq[1] = q[2] / k.sq;
+        k.rh = (q[3] + p) / k.sq;
+        k.vel[0] = q[1] / q[0];
+        k.vel[1] = q[2] / q[0];
+        k.c = sqrt(gamma * p / q[0]);
+    }
+    __device__ __forceinline__ void rpn2(int ixy, const R* qL, const R* qR, R speed,
                                          R (*wave)[M], R* s, R* amdq, R* apdq,
                                          Roe& rr) const {
+        Cell cl, cr;
+        prep(qL, cl);
+        prep(qR, cr);
+        rpn2c(ixy, qL, qR, cl, cr, speed, wave, s, amdq, apdq, rr);
+    }
+    __device__ __forceinline__ void rpn2c(int ixy, const R* qL, const R* qR, const Cell& cl, const Cell& cr, R,
+                                          R (*wave)[M], R* s, R* amdq, R* apdq,
+                                          Roe& rr) const {
         const int mu = (ixy == 1) ? 1 : 2;
         const int mv = (ixy == 1) ? 2 : 1;
-        const R rhsqrtl = sqrt(qL[0]);
-        const R rhsqrtr = sqrt(qR[0]);
-        const R pl = gamma1 * (qL[3] - R(0.5) * (qL[1] * qL[1] + qL[2] * qL[2]) / qL[0]);
-        const R pr = gamma1 * (qR[3] - R(0.5) * (qR[1] * qR[1] + qR[2] * qR[2]) / qR[0]);
-        const R rhsq2 = rhsqrtl + rhsqrtr;
-        const R u = (qL[mu] / rhsqrtl + qR[mu] / rhsqrtr) / rhsq2;
-        const R v = (qL[mv] / rhsqrtl + qR[mv] / rhsqrtr) / rhsq2;
-        const R enth = (((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr)) / rhsq2;
+        const R rhsq2 = cl.sq + cr.sq;
+        const R u = (cl.rq[mu - 1] + cr.rq[mu - 1]) / rhsq2;  // (qL(mu)/rhsqrtl + qR(mu)/rhsqrtr)/rhsq2
+        const R v = (cl.rq[mv - 1] + cr.rq[mv - 1]) / rhsq2;
+        const R enth = (cl.rh + cr.rh) / rhsq2;               // ((qL(4)+pl)/rhsqrtl + (qR(4)+pr)/rhsqrtr)/rhsq2
         const R u2v2 = u * u + v * v;
         const R a2s = gamma1 * (enth - R(0.5) * u2v2);
         const R a = sqrt(a2s);
@@ -220,10 +267,7 @@ struct Euler4RoeT {
         s[3] = u + a;
         R am[4];
         {
-            const R rhoim1 = qL[0];
-            const R pim1 = gamma1 * (qL[3] - R(0.5) * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) / rhoim1);
-            const R cim1 = sqrt(gamma * pim1 / rhoim1);
-            const R s0 = qL[mu] / rhoim1 - cim1;
+            const R s0 = cl.vel[mu - 1] - cl.c;  // qL(mu)/rhoim1 - sqrt(gamma*pim1/rhoim1)
             R sfract;
             if (s0 >= R(0.0) && s[0] > R(0.0)) {
                 am[0] = am[1] = am[2] = am[3] = R(0.0);
@@ -250,10 +294,7 @@ struct Euler4RoeT {
                 am[m] = am[m] + s[2] * wave[2][m];
             }
             {
-                const R rhoi = qR[0];
-                const R pi = gamma1 * (qR[3] - R(0.5) * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) / rhoi);
-                const R ci = sqrt(gamma * pi / rhoi);
-                const R s3 = qR[mu] / rhoi + ci;
+                const R s3 = cr.vel[mu - 1] + cr.c;  // qR(mu)/rhoi + sqrt(gamma*pi/rhoi)
                 const R rho2 = qR[0] - wave[3][0];
                 const R rhou2 = qR[mu] - wave[3][mu];
                 const R rhov2 = qR[mv] - wave[3][mv];

@@ -39,7 +39,7 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double 
     atomicMax(p, (unsigned long long)__double_as_longlong(v));
 }
 
-template <int NX, int NY, int PPB, int M, int W, int NAUX, bool PSI>
+template <int NX, int NY, int PPB, int M, int W, int NAUX, bool PSI, int NC>
 struct StepSmem {
     static constexpr int QROW = 0;
     static constexpr int XW = QROW + PPB * NX * M;
@@ -47,24 +47,39 @@ struct StepSmem {
     static constexpr int GL = XS + PPB * NX * W;
     static constexpr int FX = GL + PPB * NX * 2 * M;
     static constexpr int GY = FX + 3 * PPB * NX * 2 * M;
-    static constexpr int AUX = GY + PPB * NX * 2 * M;
+    static constexpr int CROW = GY + PPB * NX * 2 * M;
+    static constexpr int AUX = CROW + 2 * PPB * NX * NC;
     static constexpr int TAB = AUX + PPB * NAUX * NY * NX;
     static constexpr int PSIT = TAB + (PSI ? PPB * 2 * (NX + 1) : 0);
     static constexpr int TOTAL = PSIT + (PSI ? PPB * (NY + 1) * (NX + 1) : 0);
+};
+
+// LIM > 0: order (2, 2) and limiter LIM on every wave, fixed at compile time;
+// LIM == 0: order and limiters read from the launch arguments.
+template <int LIM>
+struct MethodC {
+    const StepArgs& a;
+    __device__ __forceinline__ bool second_order() const { return LIM > 0 || a.order0 == 2; }
+    __device__ __forceinline__ bool transverse() const { return LIM > 0 || a.order1 > 0; }
+    __device__ __forceinline__ bool transverse2() const { return LIM > 0 || (a.order0 > 1 && a.order1 == 2); }
+    __device__ __forceinline__ int lim(int mw) const { return LIM > 0 ? LIM : a.mthlim[mw]; }
 };
 
 }  // namespace
 
 // AUXK: AUX_NONE, AUX_SWIRL (velocities computed from the swirl stream function),
 // AUX_STORED (aux arena, NAUX components).
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB>
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
 __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     constexpr int M = SOL::M;
     constexpr int W = SOL::W;
+    constexpr int NC = SOL::NC;
     constexpr int NX = MX + 2 * MBC;
     constexpr int NY = NX;
     constexpr int PPB = TPB / NX;
-    using L = StepSmem<NX, NY, PPB, M, W, NAUX, AUXK == AUX_SWIRL>;
+    using L = StepSmem<NX, NY, PPB, M, W, NAUX, AUXK == AUX_SWIRL, NC>;
+    using Cell = typename SOL::Cell;
+    const MethodC<LIM> meth{a};
     extern __shared__ double smem[];
     double* s_qrow = smem + L::QROW;  // [PPB][NX][M]
     double* s_xw = smem + L::XW;      // [PPB][NX][W][M]
@@ -72,6 +87,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     double* s_gl = smem + L::GL;      // [PPB][NX][2][M]
     double* s_fx = smem + L::FX;      // [3][PPB][NX][2][M]
     double* s_gy = smem + L::GY;      // [PPB][NX][2][M]
+    double* s_crow = smem + L::CROW;  // [2][PPB][NX][NC]: the cell quantities of rows s-1 and s
     double* s_aux = smem + L::AUX;    // [PPB][NAUX][NY][NX]
     double* s_tab = smem + L::TAB;    // [PPB][2][NX+1] (swirl)
     double* s_psi = smem + L::PSIT;   // [PPB][NY+1][NX+1] (swirl)
@@ -197,6 +213,11 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     double* gl = s_gl + pl * NX * 2 * M;
     double* gy = s_gy + pl * NX * 2 * M;
 
+    // cell quantities of (column cc, row rr), shared by the interfaces of the cell
+    auto CELL = [&](int rr, int cc) -> Cell* {
+        return reinterpret_cast<Cell*>(s_crow + (((rr & 1) * PPB + pl) * NX + cc) * NC);
+    };
+
     for (int s = s0; s <= s1; ++s) {
         // ---------------- phase 1: load row s; raw y-interface s ----------------
         if (s < NY && active) {
@@ -207,8 +228,11 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 if (save_last && s >= qlo && s < qhi) qlast[k] = q_n[m];
                 qrow[c * M + m] = q_n[m];
             }
+            Cell cn;
+            sol.prep(q_n, cn);
+            if constexpr (NC > 0) *CELL(s, c) = cn;
             if (ycol && s >= ylo) {
-                sol.rpn2(2, q_m1, q_n, AUXV(1, c, s), yw_n, ys_n, yam_n, yap_n, yR_n);
+                sol.rpn2c(2, q_m1, q_n, *CELL(s - 1, c), cn, AUXV(1, c, s), yw_n, ys_n, yam_n, yap_n, yR_n);
 #pragma unroll
                 for (int mw = 0; mw < W; ++mw) {
                     double d = yw_f[mw][0] * yw_n[mw][0];
@@ -229,7 +253,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             double qL[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) qL[m] = qrow[(c - 1) * M + m];
-            sol.rpn2(1, qL, q_n, AUXV(0, c, s), xwl, xsl, xam, xap, xR);
+            sol.rpn2c(1, qL, q_n, *CELL(s, c - 1), *CELL(s, c), AUXV(0, c, s), xwl, xsl, xam, xap, xR);
 #pragma unroll
             for (int mw = 0; mw < W; ++mw) {
                 xs[c * W + mw] = xsl[mw];
@@ -257,17 +281,17 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             double cq[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) cq[m] = 0.0;
-            if (a.order0 == 2) {
+            if (meth.second_order()) {
                 if (f >= MBC && f <= MBC + MX) {
 #pragma unroll
                     for (int mw = 0; mw < W; ++mw) {
-                        if (a.mthlim[mw] == 0) continue;
+                        if (meth.lim(mw) == 0) continue;
                         double wn2 = yw_f[mw][0] * yw_f[mw][0];
 #pragma unroll
                         for (int m = 1; m < M; ++m) wn2 = wn2 + yw_f[mw][m] * yw_f[mw][m];
                         if (wn2 == 0.0) continue;
                         const double r = (ys_f[mw] > 0.0) ? ydotl[mw] / wn2 : ydotr[mw] / wn2;
-                        const double phi = limiter_phi(a.mthlim[mw], r);
+                        const double phi = limiter_phi(meth.lim(mw), r);
 #pragma unroll
                         for (int m = 0; m < M; ++m) w[mw][m] = phi * w[mw][m];
                     }
@@ -292,14 +316,14 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             for (int m = 0; m < M; ++m) {
                 double fmv = (f <= NY - 2) ? yam_f[m] : 0.0;
                 double fpv = (f <= NY - 2) ? -yap_f[m] : 0.0;
-                if (a.order0 == 2) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
+                if (meth.second_order()) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
                 fm_[m] = fmv; fp_[m] = fpv;
                 am[m] = yam_f[m]; ap[m] = yap_f[m];
-                if (a.order0 > 1 && a.order1 == 2 && f <= NY - 2) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
+                if (meth.transverse2() && f <= NY - 2) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
                 FYm_cur[m] = fmv;
             }
             double gLm[M], gLp[M], gRm[M], gRp[M];
-            if (a.order1 > 0) {
+            if (meth.transverse()) {
                 double bm[M], bp[M];
                 // imp = 1: aux2(j-1, kv=1), aux3(j-1, kv=1) = u at columns c, c+1, row f-1
                 sol.rpt2(2, am, yR_f, AUXV(0, c, f - 1), AUXV(0, c + 1, f - 1), bm, bp);
@@ -356,11 +380,11 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             double cq[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) cq[m] = 0.0;
-            if (a.order0 == 2) {
+            if (meth.second_order()) {
                 if (c >= MBC && c <= MBC + MX) {
 #pragma unroll
                     for (int mw = 0; mw < W; ++mw) {
-                        if (a.mthlim[mw] == 0) continue;
+                        if (meth.lim(mw) == 0) continue;
                         double wn2 = xwl[mw][0] * xwl[mw][0];
                         double dl = xw[((c - 1) * W + mw) * M + 0] * xwl[mw][0];
                         double dr = xwl[mw][0] * xw[((c + 1) * W + mw) * M + 0];
@@ -373,7 +397,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                         }
                         if (wn2 == 0.0) continue;
                         const double r = (xsl[mw] > 0.0) ? dl / wn2 : dr / wn2;
-                        const double phi = limiter_phi(a.mthlim[mw], r);
+                        const double phi = limiter_phi(meth.lim(mw), r);
 #pragma unroll
                         for (int m = 0; m < M; ++m) xwl[mw][m] = phi * xwl[mw][m];
                     }
@@ -398,13 +422,13 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             for (int m = 0; m < M; ++m) {
                 double fmv = (c <= NX - 2) ? xam[m] : 0.0;
                 double fpv = (c <= NX - 2) ? -xap[m] : 0.0;
-                if (a.order0 == 2) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
+                if (meth.second_order()) { fmv = fmv + 0.5 * cq[m]; fpv = fpv + 0.5 * cq[m]; }
                 fxs[(c * 2 + 0) * M + m] = fmv;
                 fxs[(c * 2 + 1) * M + m] = fpv;
                 am[m] = xam[m]; ap[m] = xap[m];
-                if (a.order0 > 1 && a.order1 == 2 && c <= NX - 2) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
+                if (meth.transverse2() && c <= NX - 2) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
             }
-            if (a.order1 > 0) {
+            if (meth.transverse()) {
                 double bm[M], bp[M];
                 // imp = 1: aux2(i-1, kv=2), aux3(i-1, kv=2) = v at column c-1, rows s, s+1
                 sol.rpt2(1, am, xR, AUXV(1, c - 1, s), AUXV(1, c - 1, s + 1), bm, bp);
@@ -520,16 +544,16 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
 // ---------------------------------------------------------------------------
 namespace {
 
-template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB>
+template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
 cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
     constexpr int NX = MX + 2 * MBC;
     constexpr int PPB = TPB / NX;
     static_assert(PPB >= 1, "patch wider than the CTA");
-    using L = StepSmem<NX, NX, PPB, SOL::M, SOL::W, NAUX, AUXK == AUX_SWIRL>;
+    using L = StepSmem<NX, NX, PPB, SOL::M, SOL::W, NAUX, AUXK == AUX_SWIRL, SOL::NC>;
     const size_t bytes = (size_t)L::TOTAL * sizeof(double);
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB>,
+        cudaError_t e = cudaFuncSetAttribute(step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e != cudaSuccess) return e;
         configured = true;
@@ -538,7 +562,7 @@ cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
     if (nb > 1 && (!a.qsrc || a.qsrc == a.q || nb > 4)) return cudaErrorInvalidValue;
     const int blocks = (a.npatches + PPB - 1) / PPB * nb;
     if (blocks == 0) return cudaSuccess;
-    step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB><<<blocks, TPB, bytes, st>>>(a);
+    step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB, LIM><<<blocks, TPB, bytes, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -548,15 +572,27 @@ cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
 // as a second wave; 1.4-1.65x faster on levels of 1,024 patches of mx = 32.
 // Scalar advection keeps 128 threads (its per-patch aux and stream-function
 // tables would not fit 256 threads' worth of patches of mx = 64 in shared memory).
+// The Roe systems with order (2, 2) and the MC limiter on every wave (the
+// benchmarked configurations) get the method fixed at compile time.
+template <class SOL, int MX, int AUXK, int NAUX, int TPB>
+cudaError_t launch_lim(const StepArgs& a, cudaStream_t st) {
+    if constexpr (SOL::M > 1) {
+        bool mc = a.order0 == 2 && a.order1 == 2;
+        for (int mw = 0; mw < SOL::W; ++mw) mc = mc && a.mthlim[mw] == 4;
+        if (mc) return launch_one<SOL, MX, 2, AUXK, NAUX, TPB, 4>(a, st);
+    }
+    return launch_one<SOL, MX, 2, AUXK, NAUX, TPB, 0>(a, st);
+}
+
 template <class SOL, int AUXK, int NAUX>
 cudaError_t launch_mx(int mx, int mbc, const StepArgs& a, cudaStream_t st) {
     constexpr int TPB = SOL::M > 1 ? 256 : 128;
     if (mbc != 2) return cudaErrorInvalidValue;
     switch (mx) {
-        case 8: return launch_one<SOL, 8, 2, AUXK, NAUX, TPB>(a, st);
-        case 16: return launch_one<SOL, 16, 2, AUXK, NAUX, TPB>(a, st);
-        case 32: return launch_one<SOL, 32, 2, AUXK, NAUX, TPB>(a, st);
-        case 64: return launch_one<SOL, 64, 2, AUXK, NAUX, TPB>(a, st);
+        case 8: return launch_lim<SOL, 8, AUXK, NAUX, TPB>(a, st);
+        case 16: return launch_lim<SOL, 16, AUXK, NAUX, TPB>(a, st);
+        case 32: return launch_lim<SOL, 32, AUXK, NAUX, TPB>(a, st);
+        case 64: return launch_lim<SOL, 64, AUXK, NAUX, TPB>(a, st);
         default: return cudaErrorInvalidValue;
     }
 }
