@@ -42,13 +42,14 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double 
 template <int NX, int NY, int PPB, int M, int W, int NAUX, bool PSI, int NC>
 struct StepSmem {
     static constexpr int QROW = 0;
-    static constexpr int XW = QROW + PPB * NX * M;
+    static constexpr int XW = QROW + 3 * PPB * NX * M;
     static constexpr int XS = XW + PPB * NX * W * M;
     static constexpr int GL = XS + PPB * NX * W;
     static constexpr int FX = GL + PPB * NX * 2 * M;
     static constexpr int GY = FX + 3 * PPB * NX * 2 * M;
     static constexpr int CROW = GY + PPB * NX * 2 * M;
-    static constexpr int AUX = CROW + 2 * PPB * NX * NC;
+    static constexpr int GXR = CROW + 2 * PPB * NX * NC;
+    static constexpr int AUX = GXR + 3 * PPB * NX * M;
     static constexpr int TAB = AUX + PPB * NAUX * NY * NX;
     static constexpr int PSIT = TAB + (PSI ? PPB * 2 * (NX + 1) : 0);
     static constexpr int TOTAL = PSIT + (PSI ? PPB * (NY + 1) * (NX + 1) : 0);
@@ -81,13 +82,14 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     using Cell = typename SOL::Cell;
     const MethodC<LIM> meth{a};
     extern __shared__ double smem[];
-    double* s_qrow = smem + L::QROW;  // [PPB][NX][M]
+    double* s_qrow = smem + L::QROW;  // [3][PPB][NX][M]: rows s-2, s-1, s (slot row % 3)
     double* s_xw = smem + L::XW;      // [PPB][NX][W][M]
     double* s_xs = smem + L::XS;      // [PPB][NX][W]
     double* s_gl = smem + L::GL;      // [PPB][NX][2][M]
     double* s_fx = smem + L::FX;      // [3][PPB][NX][2][M]
     double* s_gy = smem + L::GY;      // [PPB][NX][2][M]
     double* s_crow = smem + L::CROW;  // [2][PPB][NX][NC]: the cell quantities of rows s-1 and s
+    double* s_gxr = smem + L::GXR;    // [3][PPB][NX][M]: GXu(row-1) + GXd(row) of rows s-2, s-1, s (own column)
     double* s_aux = smem + L::AUX;    // [PPB][NAUX][NY][NX]
     double* s_tab = smem + L::TAB;    // [PPB][2][NX+1] (swirl)
     double* s_psi = smem + L::PSIT;   // [PPB][NY+1][NX+1] (swirl)
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     double cfl = 0.0;
 
     // q rows s-2, s-1, s of this column
-    double q_m2[M], q_m1[M], q_n[M];
+    double q_n[M];
     // y window: finalizing interface f = s-1 uses its raw waves (yw_f) and the
     // dot products with interfaces f-1 (ydotl) and f+1 (ydotr).
     double yw_f[W][M], ys_f[W], yam_f[M], yap_f[M], ydotl[W];
@@ -191,14 +193,13 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     double gRm_prev[M], gRp_prev[M];  // y transverse parts from interface f-1 into cell f-1
     double FYp_prev[M];               // faddp of interface s-2
     double GXu_prev[M];               // x-row s-1 "up" transverse part
-    double GXs_m2[M], GXs_m1[M];      // GXu(row-1) + GXd(row) for rows s-2, s-1
     double GYd_r[M], GYu_r[M];        // y transverse parts for cell row s-2
 #pragma unroll
     for (int m = 0; m < M; ++m) {
-        q_m2[m] = q_m1[m] = q_n[m] = 0.0;
+        q_n[m] = 0.0;
         yam_f[m] = yap_f[m] = yam_n[m] = yap_n[m] = 0.0;
         gRm_prev[m] = gRp_prev[m] = FYp_prev[m] = GXu_prev[m] = 0.0;
-        GXs_m2[m] = GXs_m1[m] = GYd_r[m] = GYu_r[m] = 0.0;
+        GYd_r[m] = GYu_r[m] = 0.0;
     }
 #pragma unroll
     for (int mw = 0; mw < W; ++mw) {
@@ -207,7 +208,9 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         for (int m = 0; m < M; ++m) yw_f[mw][m] = yw_n[mw][m] = 0.0;
     }
 
-    double* qrow = s_qrow + pl * NX * M;
+    // q of (column cc, row rr) in the row ring
+    auto QR = [&](int rr, int cc) -> double* { return s_qrow + (((rr % 3) * PPB + pl) * NX + cc) * M; };
+    auto GXS = [&](int rr) -> double* { return s_gxr + (((rr % 3) * PPB + pl) * NX + c) * M; };
     double* xw = s_xw + pl * NX * W * M;
     double* xs = s_xs + pl * NX * W;
     double* gl = s_gl + pl * NX * 2 * M;
@@ -226,12 +229,15 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 const int64_t k = ((int64_t)m * NY + s) * NX + c;
                 q_n[m] = qin[k];
                 if (save_last && s >= qlo && s < qhi) qlast[k] = q_n[m];
-                qrow[c * M + m] = q_n[m];
+                QR(s, c)[m] = q_n[m];
             }
             Cell cn;
             sol.prep(q_n, cn);
             if constexpr (NC > 0) *CELL(s, c) = cn;
             if (ycol && s >= ylo) {
+                double q_m1[M];
+#pragma unroll
+                for (int m = 0; m < M; ++m) q_m1[m] = QR(s - 1, c)[m];
                 sol.rpn2c(2, q_m1, q_n, *CELL(s - 1, c), cn, AUXV(1, c, s), yw_n, ys_n, yam_n, yap_n, yR_n);
 #pragma unroll
                 for (int mw = 0; mw < W; ++mw) {
@@ -242,27 +248,6 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 }
             }
         }
-        __syncthreads();  // A
-
-        // ---------------- phase 2: raw x-interface (c, s) ----------------
-        const bool xrow = active && s >= 1 && s <= NY - 2;
-        const bool xint = xrow && c >= 1;
-        double xwl[W][M], xsl[W], xam[M], xap[M];
-        typename SOL::Roe xR{};
-        if (xint) {
-            double qL[M];
-#pragma unroll
-            for (int m = 0; m < M; ++m) qL[m] = qrow[(c - 1) * M + m];
-            sol.rpn2c(1, qL, q_n, *CELL(s, c - 1), *CELL(s, c), AUXV(0, c, s), xwl, xsl, xam, xap, xR);
-#pragma unroll
-            for (int mw = 0; mw < W; ++mw) {
-                xs[c * W + mw] = xsl[mw];
-#pragma unroll
-                for (int m = 0; m < M; ++m) xw[(c * W + mw) * M + m] = xwl[mw][m];
-                if (c >= MBC && c <= MBC + MX) cfl = dmax(dmax(cfl, dtdx * xsl[mw]), -dtdx * xsl[mw]);
-            }
-        }
-
         // ---------------- y: finalize interface f = s-1 (own column) ----------------
         double FYm_cur[M];
 #pragma unroll
@@ -369,6 +354,27 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             yap_f[m] = yap_n[m];
         }
         yR_f = yR_n;
+        __syncthreads();  // A
+
+        // ---------------- phase 2: raw x-interface (c, s) ----------------
+        const bool xrow = active && s >= 1 && s <= NY - 2;
+        const bool xint = xrow && c >= 1;
+        double xwl[W][M], xsl[W], xam[M], xap[M];
+        typename SOL::Roe xR{};
+        if (xint) {
+            double qL[M];
+#pragma unroll
+            for (int m = 0; m < M; ++m) qL[m] = QR(s, c - 1)[m];
+            sol.rpn2c(1, qL, q_n, *CELL(s, c - 1), *CELL(s, c), AUXV(0, c, s), xwl, xsl, xam, xap, xR);
+#pragma unroll
+            for (int mw = 0; mw < W; ++mw) {
+                xs[c * W + mw] = xsl[mw];
+#pragma unroll
+                for (int m = 0; m < M; ++m) xw[(c * W + mw) * M + m] = xwl[mw][m];
+                if (c >= MBC && c <= MBC + MX) cfl = dmax(dmax(cfl, dtdx * xsl[mw]), -dtdx * xsl[mw]);
+            }
+        }
+
         __syncthreads();  // B
 
         // ---------------- phase 3: x limiter, corrections, transverse ----------------
@@ -456,7 +462,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         __syncthreads();  // C
 
         // ---------------- phase 4: complete GX(c, s); publish GY(c, s-2) ----------------
-        double GXs_n[M];
+        // (idle threads of the CTA, pl == PPB, own no ring slot)
+        double* GXs_n = GXS(s);
 #pragma unroll
         for (int m = 0; m < M; ++m) {
             double gxd = 0.0, gxu = 0.0;
@@ -469,7 +476,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                     gxu = -gRpx[m];
                 }
             }
-            GXs_n[m] = GXu_prev[m] + gxd;
+            if (active) GXs_n[m] = GXu_prev[m] + gxd;
             GXu_prev[m] = gxu;
         }
         if (active) {
@@ -493,9 +500,9 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 const double gyd_r = gy[((c + 1) * 2 + 0) * M + m];
                 const double fmv = (fxm1 + GYu_r[m]) + gyd_r;       // fm(i+1, j)
                 const double fpv = (fxp0 + gyu_l) + GYd_r[m];       // fp(i, j)
-                const double gmv = GXs_m1[m] + FYm_cur[m];          // gm(i, j+1)
-                const double gpv = GXs_m2[m] + FYp_prev[m];         // gp(i, j)
-                const double qv = q_m2[m] - dtdx * (fmv - fpv) - dtdy * (gmv - gpv);
+                const double gmv = GXS(s - 1)[m] + FYm_cur[m];      // gm(i, j+1)
+                const double gpv = GXS(r)[m] + FYp_prev[m];         // gp(i, j)
+                const double qv = QR(r, c)[m] - dtdx * (fmv - fpv) - dtdy * (gmv - gpv);
                 q[((int64_t)m * NY + r) * NX + c] = qv;
                 if (a.treg) {
                     // time-sync: boundary fluctuations scaled by dt and the edge
@@ -525,10 +532,6 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         // rotate per-row registers
 #pragma unroll
         for (int m = 0; m < M; ++m) {
-            q_m2[m] = q_m1[m];
-            q_m1[m] = q_n[m];
-            GXs_m2[m] = GXs_m1[m];
-            GXs_m1[m] = GXs_n[m];
             FYp_prev[m] = FYp_cur[m];
         }
     }
