@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "fcb_server_get_q", "fcb_server_release", "fcb_server_clock", "fcb_autotune_info",
     "fcb_measure_fp_rate", "fcb_output_ascii", "fcb_comm_create_local", "fcb_comm_nccl_unique_id",
     "fcb_comm_create_nccl", "fcb_comm_destroy", "fcb_context_create_partitioned", "fcb_partition_info",
-    "fcb_global_maximum", "fcb_partition_plan", "fcb_step_kernel_time",
+    "fcb_global_maximum", "fcb_partition_plan", "fcb_step_kernel_time", "fcb_server_set_work_limit",
 )
 
 
@@ -252,6 +252,7 @@ def lib():
     L.fcb_server_get_q.argtypes = [vp, ctypes.c_int, dp, sz]
     L.fcb_server_release.argtypes = [vp, ctypes.c_int]
     L.fcb_server_clock.argtypes = [vp, dp, ll, ll]
+    L.fcb_server_set_work_limit.argtypes = [vp, ctypes.c_longlong]
     L.fcb_comm_create_local.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(vp)]
     L.fcb_comm_nccl_unique_id.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
     L.fcb_comm_create_nccl.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,

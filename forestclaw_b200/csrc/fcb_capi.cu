@@ -436,6 +436,14 @@ int fcb_server_release(fcb_server_t* s, int id) {
         s->impl->release(id);
     });
 }
+int fcb_server_set_work_limit(fcb_server_t* s, long long max_cells) {
+    return guard([&] {
+        need(s, "server");
+        if (max_cells < 0) throw fcb::Error(FCB_ERR_INVALID, "max_cells must be >= 0");
+        s->impl->set_work_limit(max_cells);
+    });
+}
+
 int fcb_server_clock(fcb_server_t* s, double* now, long long* rounds, long long* launches) {
     return guard([&] {
         need(s, "server");

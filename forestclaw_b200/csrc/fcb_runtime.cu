@@ -2103,33 +2103,102 @@ double Context::step_kernel_time(double t, double dt, int launches, bool* fused)
     return time_steps(f, false, launches, t, dt);
 }
 
-void Context::step_descs(double t, double dt, int req, std::vector<PatchDesc>& out) {
+// The schedule of run_schedule (fclaw2d_advance.c:247-346) one fine step at a
+// time: the same counters, the same recursion over coarser levels whose step
+// falls on this fine step, the same time interpolations and ghost updates.
+int Context::serve_begin(double t_curr, double dt) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "step before initialize");
-    ensure_ghosts();
-    ghosts_filled_ = false;
-    double vt = 0.0;
-    if (aux_kind_ == AUX_SWIRL) {
-        const double pi = 4.0 * std::atan(1.0);
-        const double tperiod = opt_.problem_params[0];
-        vt = (tperiod == 0.0) ? 0.0 : std::cos(2.0 * pi * (t + dt / 2.0) / tperiod);
+    if (partitioned()) throw Error(FCB_ERR_INVALID, "served solves are not partitioned");
+    sv_ts_.assign(opt_.maxlevel + 1, SchedCounter{});
+    for (int l = opt_.minlevel; l <= opt_.maxlevel; ++l) sv_ts_[l].current_time = t_curr;
+    if (opt_.subcycle) {
+        double dt_level = dt;
+        int steps_inc = 1 << (gmax_ - opt_.minlevel);
+        int total_steps = 1;
+        for (int l = opt_.minlevel; l <= opt_.maxlevel; ++l) {
+            sv_ts_[l].dt_step = dt_level; sv_ts_[l].total_steps = total_steps; sv_ts_[l].step_inc = steps_inc;
+            dt_level /= 2; steps_inc /= 2; total_steps *= 2;
+        }
+    } else {
+        const int rf = 1 << (opt_.maxlevel - opt_.minlevel);
+        for (int l = opt_.minlevel; l <= opt_.maxlevel; ++l) {
+            sv_ts_[l].step_inc = 1; sv_ts_[l].dt_step = dt / rf; sv_ts_[l].total_steps = rf;
+        }
     }
-    const int n = num_patches();
-    for (int p = 0; p < n; ++p) {
-        const int slot = slot_of_[p];
-        PatchDesc d{};
-        d.q = d_q_ + (int64_t)slot * stride_;
-        d.qlast = d_qlast_ + (int64_t)slot * stride_;
-        d.aux = aux_kind_ == AUX_STORED ? d_aux_ + (int64_t)slot * aux_stride_ : nullptr;
-        d.meta = h_meta_[slot];
-        d.dt = dt;
-        d.vt = vt;
-        d.req = req;
-        out.push_back(d);
-    }
-    cnt_.count_single_step += n;
+    sv_nf_ = 0;
+    sv_steps_.clear();
+    sv_ti_.clear();
+    return sv_ts_[gmax_].total_steps;
 }
 
-void Context::after_fine_step(double t) { ghost_update(gmin_, gmax_, t, 0); }
+long long Context::serve_step_descs(int req, std::vector<PatchDesc>& out) {
+    if (!initialized_) throw Error(FCB_ERR_STATE, "step before initialize");
+    if (sv_ts_.empty() || sv_nf_ >= sv_ts_[gmax_].total_steps) throw Error(FCB_ERR_STATE, "no fine step left");
+    ensure_ghosts();
+    ghosts_filled_ = false;
+    sv_steps_.clear();
+    sv_ti_.clear();
+    std::function<void(int, int)> advance_level = [&](int level, int curr_fine_step) {
+        SchedCounter& c = sv_ts_[level];
+        sv_steps_.push_back({level, c.current_time, c.dt_step});
+        c.last_step += c.step_inc;
+        c.current_time += c.dt_step;
+        if (level > gmin_) {
+            const int last_coarse_step = sv_ts_[level - 1].last_step;
+            if (last_coarse_step == curr_fine_step) {
+                advance_level(level - 1, last_coarse_step);
+                if (opt_.subcycle) {
+                    const int coarse_inc = sv_ts_[level - 1].step_inc;
+                    sv_ti_.emplace_back(level - 1, ((double)(c.last_step % coarse_inc)) / coarse_inc);
+                }
+            }
+        }
+    };
+    advance_level(gmax_, sv_nf_);
+    long long cells = 0;
+    const double pi = 4.0 * std::atan(1.0);
+    for (const SvStep& u : sv_steps_) {
+        double vt = 0.0;
+        if (aux_kind_ == AUX_SWIRL) {
+            const double tperiod = opt_.problem_params[0];
+            vt = (tperiod == 0.0) ? 0.0 : std::cos(2.0 * pi * (u.t + u.dt / 2.0) / tperiod);
+        }
+        const int b = level_begin_[u.level], e = level_begin_[u.level + 1];
+        for (int k = b; k < e; ++k) {
+            const int slot = h_level_slots_[k];
+            PatchDesc d{};
+            d.q = d_q_ + (int64_t)slot * stride_;
+            d.qlast = d_qlast_ + (int64_t)slot * stride_;
+            d.aux = aux_kind_ == AUX_STORED ? d_aux_ + (int64_t)slot * aux_stride_ : nullptr;
+            d.meta = h_meta_[slot];
+            d.dt = u.dt;
+            d.vt = vt;
+            d.req = req;
+            out.push_back(d);
+        }
+        cnt_.count_single_step += e - b;
+        cells += (long long)(e - b) * opt_.mx * opt_.my;
+    }
+    return cells;
+}
+
+void Context::serve_after_step() {
+    for (const auto& ti : sv_ti_) timeinterp(ti.first, ti.second);
+    sv_ti_.clear();
+    ++sv_nf_;
+    const SchedCounter& top = sv_ts_[gmax_];
+    if (top.last_step < top.total_steps) {
+        if (opt_.subcycle) {
+            int ti_level = gmax_ - 1;
+            while (top.last_step % sv_ts_[ti_level].step_inc == 0) --ti_level;
+            ghost_update(ti_level + 1, gmax_, top.current_time, 1);
+        } else {
+            ghost_update(gmin_, gmax_, top.current_time, 0);
+        }
+    } else {
+        ghost_update(gmin_, gmax_, top.current_time, 0);
+    }
+}
 
 // fclaw2d_clawpatch_save_step / restore_step: the CFL-retry copy
 void Context::save_step() {
@@ -2164,6 +2233,11 @@ cudaError_t launch_step_batch(const fcb_options_t& opt, int aux_kind, const Patc
     a.gamma1 = opt.gamma - 1.0;
     a.drytol = opt.dry_tolerance;
     a.cfl_out = d_cfl;
+    // the Roe systems of clawpack 4.6 in FP64 run the four-barrier CTA form (on
+    // B200 about twice the pipelined form's rate for shallow water at mx = 32)
+    if (opt.precision != 1 && opt.claw_version != 5 &&
+        (opt.solver_kind == FCB_SOLVER_SWE_ROE || opt.solver_kind == FCB_SOLVER_EULER4_ROE))
+        return launch_step(opt.solver_kind, aux_kind, opt.mwaves, opt.mx, opt.my, opt.mbc, a, st);
     return opt.precision == 1
                ? launch_step_pipe_mixed(opt.solver_kind, aux_kind, opt.mwaves, opt.mx, opt.my, opt.mbc,
                                         opt.claw_version, a, st)

@@ -143,11 +143,19 @@ class Context {
     const fcb_options_t& options() const { return opt_; }
     int aux_kind() const { return aux_kind_; }
 
-    // --- pieces of a non-subcycled macro step, for launches that batch several
-    // solves (serving): the patch descriptors of one fine step (every leaf, step
-    // dt), the ghost fill that follows it, and the CFL-retry copy of q ---
-    void step_descs(double t, double dt, int req, std::vector<PatchDesc>& out);
-    void after_fine_step(double t);
+    // --- one macro step of fclaw2d_advance_all_levels (subcycled or not), one
+    // fine step at a time, for launches that batch several solves (serving) ---
+    // serve_begin: start the macro step at t_curr with coarse step dt; returns
+    // its number of fine steps.
+    int serve_begin(double t_curr, double dt);
+    // the level updates of the next fine step (as run_schedule orders them):
+    // one descriptor per patch with its level's t and dt and CFL slot req;
+    // returns the cells it updates
+    long long serve_step_descs(int req, std::vector<PatchDesc>& out);
+    // after the batched step launch: that fine step's time interpolations and
+    // the ghost update that follows it (the final one after the last fine step)
+    void serve_after_step();
+    // the CFL-retry copy of q
     void save_step();
     void restore_step();
     void set_curr_time(double t) { curr_time_ = t; }
@@ -339,6 +347,14 @@ class Context {
     PatchMeta* d_meta_ = nullptr;
     std::vector<PatchMeta> h_meta_;  // host copy of the slot metadata
     // level lists (device), grouped by level
+    // serving: the schedule counters of the macro step in progress, and the
+    // level updates and time interpolations of its current fine step
+    struct SchedCounter { int last_step = 0, step_inc = 1, total_steps = 1; double current_time = 0.0, dt_step = 0.0; };
+    std::vector<SchedCounter> sv_ts_;
+    int sv_nf_ = 0;
+    struct SvStep { int level; double t, dt; };
+    std::vector<SvStep> sv_steps_;
+    std::vector<std::pair<int, double>> sv_ti_;
     DevBuf<int32_t> d_level_slots_;
     std::vector<int> level_begin_;    // size maxlevel+2
     int gmin_ = 0, gmax_ = 0;         // coarsest and finest leaf level (set with the level lists)

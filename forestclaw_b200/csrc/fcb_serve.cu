@@ -39,9 +39,8 @@ double Server::now() const {
 }
 
 int Server::submit(const fcb_options_t& opt) {
-    if (opt.subcycle) throw Error(FCB_ERR_INVALID, "served solves use non-subcycled time stepping (subcycle = 0)");
-    if (opt.step_variant == 1 || opt.step_variant == 2 || opt.step_variant >= 4)
-        throw Error(FCB_ERR_INVALID, "served solves use the pipelined step form");
+    if (opt.step_variant == 2 || opt.step_variant >= 4)
+        throw Error(FCB_ERR_INVALID, "served solves use the four-barrier or pipelined step form");
     if (opt.nout != 1) throw Error(FCB_ERR_INVALID, "served solves run to tfinal in one output interval (nout = 1)");
     if (opt.time_sync) throw Error(FCB_ERR_INVALID, "served solves do not run the time synchronisation");
     if (opt.src_term) throw Error(FCB_ERR_INVALID, "served solves have no source-term stage");
@@ -60,28 +59,47 @@ const Request& Server::request(int id) const {
     return it->second;
 }
 
-// Admit queued requests in arrival order while their device memory fits.
+long long Server::active_cells() const {
+    long long n = 0;
+    for (int id : active_) {
+        const Request& r = reqs_.at(id);
+        n += (long long)r.ctx->num_patches() * r.opt.mx * r.opt.my;
+    }
+    return n;
+}
+
+// Admit queued requests in arrival order while their device memory fits the
+// budget and their cells the work limit.  The head is initialised on first
+// sight (its size is known only then); if it does not fit, it keeps its state
+// and waits when only the work limit stops it, and is dropped and rebuilt
+// later when its memory does not fit.
 void Server::admit() {
+    long long cells_now = max_cells_ > 0 ? active_cells() : 0;
     while (!queue_.empty()) {
         Request& r = reqs_.at(queue_.front());
-        if (!active_.empty() && r.bytes > 0 && used_ + r.bytes > budget_) return;  // known size, no room yet
-        try {
-            r.ctx = std::make_unique<Context>(r.opt, st_);
-            r.ctx->initialize();
-        } catch (const Error& e) {
-            r.ctx.reset();
-            r.state = REQ_FAILED;
-            r.error = e.what();
-            r.t_finish = now();
-            queue_.pop_front();
-            continue;
+        if (!active_.empty() && r.bytes > 0 && !r.ctx && used_ + r.bytes > budget_) return;  // known size, no room
+        if (!active_.empty() && r.ctx && max_cells_ > 0 && cells_now + r.cells > max_cells_) return;
+        if (!r.ctx) {
+            try {
+                r.ctx = std::make_unique<Context>(r.opt, st_);
+                r.ctx->initialize();
+            } catch (const Error& e) {
+                r.ctx.reset();
+                r.state = REQ_FAILED;
+                r.error = e.what();
+                r.t_finish = now();
+                queue_.pop_front();
+                continue;
+            }
+            r.bytes = r.ctx->device_bytes();
+            r.cells = (long long)r.ctx->num_patches() * r.opt.mx * r.opt.my;
+            if (!active_.empty() && used_ + r.bytes > budget_) {  // first sight of its size: wait for room
+                r.ctx.reset();
+                return;
+            }
+            used_ += r.bytes;  // held from here on, also while it waits for the work limit
+            if (!active_.empty() && max_cells_ > 0 && cells_now + r.cells > max_cells_) return;
         }
-        r.bytes = r.ctx->device_bytes();
-        if (!active_.empty() && used_ + r.bytes > budget_) {  // first sight of its size: wait for room
-            r.ctx.reset();
-            return;
-        }
-        used_ += r.bytes;
         r.state = REQ_ACTIVE;
         r.t_start = now();
         r.t = 0.0;
@@ -90,6 +108,7 @@ void Server::admit() {
         begin_macro(r);
         active_.push_back(r.id);
         queue_.pop_front();
+        cells_now += r.cells;
     }
 }
 
@@ -107,7 +126,7 @@ void Server::begin_macro(Request& r) {
             if (small_step < 0) r.took_small = 1;
         }
     }
-    r.fine_total = r.fine_left = 1 << (o.maxlevel - o.minlevel);
+    r.fine_total = r.fine_left = r.ctx->serve_begin(r.t, r.dt_step);
     r.macro_cfl = 0.0;
 }
 
@@ -160,17 +179,10 @@ int Server::round() {
     // descriptors of this fine step for every active request
     h_desc_.clear();
     std::vector<std::pair<size_t, size_t>> ranges;
+    std::map<int, long long> cells;
     for (const auto& g : groups) {
         const size_t b = h_desc_.size();
-        for (int id : g) {
-            Request& r = reqs_.at(id);
-            const int k = r.fine_total - r.fine_left;
-            const double dt_fine = r.dt_step / r.fine_total;
-            // the reference advances the level time by repeated addition of the fine dt
-            double tf = r.t;
-            for (int j = 0; j < k; ++j) tf += dt_fine;
-            r.ctx->step_descs(tf, dt_fine, cfl_slot[id], h_desc_);
-        }
+        for (int id : g) cells[id] = reqs_.at(id).ctx->serve_step_descs(cfl_slot[id], h_desc_);
         ranges.emplace_back(b, h_desc_.size() - b);
     }
     // upload, one launch per group
@@ -197,15 +209,8 @@ int Server::round() {
               "batched step");
         ++launches_;
     }
-    // each request's ghost fill after its fine step
-    for (int id : active_) {
-        Request& r = reqs_.at(id);
-        const int k = r.fine_total - r.fine_left;
-        const double dt_fine = r.dt_step / r.fine_total;
-        double tf = r.t;
-        for (int j = 0; j <= k; ++j) tf += dt_fine;
-        r.ctx->after_fine_step(tf);
-    }
+    // each request's time interpolations and ghost update after its fine step
+    for (int id : active_) reqs_.at(id).ctx->serve_after_step();
     check(cudaMemcpyAsync(h_cfl_, d_cfl_.p, na * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st_), "cfl");
     check(cudaStreamSynchronize(st_), "round");
     ++rounds_;
@@ -218,7 +223,7 @@ int Server::round() {
         try {
             if (std::isnan(c)) throw Error(FCB_ERR_NUMERIC, "NaN CFL");
             r.macro_cfl = std::max(r.macro_cfl, c);
-            r.cell_updates += (long long)r.ctx->num_patches() * r.opt.mx * r.opt.my;
+            r.cell_updates += cells[id];
             if (--r.fine_left == 0) end_macro(r);
         } catch (const Error& e) {
             r.state = REQ_FAILED;
@@ -246,7 +251,10 @@ void Server::release(int id) {
     if (it == reqs_.end()) return;
     Request& r = it->second;
     if (r.state == REQ_ACTIVE) throw Error(FCB_ERR_STATE, "request still running");
-    if (r.state == REQ_QUEUED) queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
+    if (r.state == REQ_QUEUED) {
+        queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
+        if (r.ctx) used_ -= r.bytes;  // initialised while it waited for the work limit
+    }
     reqs_.erase(it);
 }
 

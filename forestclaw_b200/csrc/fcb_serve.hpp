@@ -2,18 +2,21 @@
 // device, advanced together with continuous batching.
 //
 // Each request is one solve (its own forest, arena and ghost plans, one
-// fcb::Context) with non-subcycled time stepping, so every fine step of a
-// macro step updates all of its leaves with one dt.  A round advances every
-// active request by one fine step: the patches of all requests that share a
-// launch key (solver, patch shape, method, precision) go into ONE step launch,
-// each patch carrying its own arrays, geometry and dt (PatchDesc); then each
-// request's ghost fill runs and the per-request CFL numbers come back in one
-// copy.  Between rounds the loop retires finished requests, admits queued ones
-// while their device memory fits the budget, and runs the per-request macro-
+// fcb::Context), subcycled or not as its options say.  A round advances every
+// active request by one fine step of its macro step (the level updates that
+// fclaw2d_advance_all_levels makes between two ghost updates: with subcycling
+// the finest level and the coarser levels whose step falls on it, each with
+// its own dt): the patches of all requests that share a launch key (solver,
+// patch shape, method, precision) go into ONE step launch, each patch carrying
+// its own arrays, geometry and dt (PatchDesc); then each request's time
+// interpolations and ghost update run and the per-request CFL numbers come
+// back in one copy.  Between rounds the loop retires finished requests, admits
+// queued ones in arrival order while their device memory fits the budget (and
+// their cells the work limit, if one is set), and runs the per-request macro-
 // step logic of fclaw2d_run (outstyle 1: small last step, CFL retry from the
 // saved copy, dt = dt * desired_cfl / cfl, regrid every regrid_interval).
-// Results are those of fcb_run on the same options with subcycle = 0, bit for
-// bit: batching changes which launch a patch is in, never its arithmetic.
+// Results are those of fcb_run on the same options, bit for bit: batching
+// changes which launch a patch is in, never its arithmetic.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -44,6 +47,7 @@ struct Request {
     double macro_cfl = 0.0;
     int n_inner = 0;
     size_t bytes = 0;
+    long long cells = 0;      // cells of its current mesh (patches x mx x my)
     double t_submit = 0.0, t_start = 0.0, t_finish = 0.0;  // seconds on the server clock
     long long cell_updates = 0;
     std::string error;
@@ -59,6 +63,10 @@ class Server {
     const Request& request(int id) const;
     void get_q(int id, double* host, size_t n);
     void release(int id);
+    // Cap on the cells of the admitted solves' meshes (0: none).  The queue head
+    // waits, initialised, until the active solves' cells plus its own fit;
+    // one solve is always admitted when none runs.
+    void set_work_limit(long long max_cells) { max_cells_ = max_cells; }
     int queued() const { return (int)queue_.size(); }
     int active() const { return (int)active_.size(); }
     size_t used_bytes() const { return used_; }
@@ -74,6 +82,8 @@ class Server {
 
     size_t budget_;
     size_t used_ = 0;
+    long long max_cells_ = 0;
+    long long active_cells() const;
     cudaStream_t st_;
     std::chrono::steady_clock::time_point t0_;
     int next_id_ = 0;

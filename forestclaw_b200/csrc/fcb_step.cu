@@ -113,14 +113,19 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     const int flo = band == 0 ? 1 : s0 + 2;
     const int qlo = band == 0 ? 0 : R0, qhi = band == nb - 1 ? NY : R1;
     const bool active = (pl < PPB) && (pg < a.npatches);
-    const int slot = active ? a.slots[pg] : 0;
-    const PatchMeta meta = active ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0};
-    double* __restrict__ q = a.q + (int64_t)slot * a.q_stride;
-    const double* __restrict__ qin = (nb > 1 ? a.qsrc : a.q) + (int64_t)slot * a.q_stride;
-    double* __restrict__ qlast = a.qlast + (int64_t)slot * a.q_stride;
+    // a launch over the patches of several solves (serving) describes every
+    // patch by its own arrays, geometry, dt and CFL slot
+    const PatchDesc* D = (a.desc && active) ? a.desc + pg : nullptr;
+    const int slot = (active && !a.desc) ? a.slots[pg] : 0;
+    const PatchMeta meta = D ? D->meta : (active ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0});
+    const int req = D ? D->req : -1;
+    double* __restrict__ q = D ? D->q : a.q + (int64_t)slot * a.q_stride;
+    const double* __restrict__ qin = D ? D->q : (nb > 1 ? a.qsrc : a.q) + (int64_t)slot * a.q_stride;
+    double* __restrict__ qlast = D ? D->qlast : a.qlast + (int64_t)slot * a.q_stride;
     const bool save_last = active && (meta.flags & PATCH_SAVE_LAST);
-    const double dtdx = step_dt(a, meta.level) / meta.dx;
-    const double dtdy = step_dt(a, meta.level) / meta.dy;
+    const double pdt = D ? D->dt : step_dt(a, meta.level);
+    const double dtdx = pdt / meta.dx;
+    const double dtdy = pdt / meta.dy;
     const double dtdxave = 0.5 * (dtdx + dtdx);  // 0.5*(dtdx1d(i-1)+dtdx1d(i)), no capacity
     const double dtdyave = 0.5 * (dtdy + dtdy);
     SOL sol{a.grav, a.gamma, a.gamma1};
@@ -155,8 +160,9 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         }
         __syncthreads();
         if (active) {
-            const double vty = step_vt(a, meta.level) / meta.dy;
-            const double vtx = step_vt(a, meta.level) / meta.dx;
+            const double pvt = D ? D->vt : step_vt(a, meta.level);
+            const double vty = pvt / meta.dy;
+            const double vtx = pvt / meta.dx;
             double* au = s_aux + (pl * NAUX + 0) * NY * NX;
             double* av = s_aux + (pl * NAUX + 1) * NY * NX;
             for (int r = 0; r < NY; ++r) {
@@ -167,7 +173,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         }
     } else if constexpr (AUXK == AUX_STORED) {
         if (active) {
-            const double* ag = a.aux + (int64_t)slot * a.aux_stride;
+            const double* ag = D ? D->aux : a.aux + (int64_t)slot * a.aux_stride;
             for (int k = 0; k < NAUX; ++k)
                 for (int r = 0; r < NY; ++r)
                     s_aux[((pl * NAUX + k) * NY + r) * NX + c] = ag[(k * NY + r) * NX + c];
@@ -511,7 +517,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                     const RegLayout RL{MX, MX, M};
                     double* R = a.treg + (int64_t)slot * a.treg_stride;
                     const int i = c - MBC + 1, j = r - MBC + 1;
-                    const double dty = step_dt(a, meta.level) * meta.dy, dtx = step_dt(a, meta.level) * meta.dx;
+                    const double dty = pdt * meta.dy, dtx = pdt * meta.dx;
                     if (j >= 1 && j <= MX) {
                         const int k = (j - 1) + MX * m;
                         if (i == 1) R[RL.fp(0) + k] = R[RL.fp(0) + k] - dty * fpv;
@@ -536,7 +542,18 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         }
     }
 
-    // ---- CFL: warp max, one atomic per warp ----
+    // ---- CFL: warp max, one atomic per warp (per solve of a serving launch) ----
+    if (a.desc) {
+        // patches of different solves share warps: reduce over the lanes of each
+        // solve (max of the non-negative bit patterns, high word then low word)
+        const unsigned grp = __match_any_sync(0xffffffffu, req);
+        const unsigned long long b = (unsigned long long)__double_as_longlong(active ? cfl : 0.0);
+        const unsigned hi = __reduce_max_sync(grp, (unsigned)(b >> 32));
+        const unsigned lo = __reduce_max_sync(grp, ((unsigned)(b >> 32) == hi) ? (unsigned)b : 0u);
+        if (req >= 0 && (t & 31) == __ffs(grp) - 1 && a.cfl_out)
+            atomicMax(a.cfl_out + req, ((unsigned long long)hi << 32) | lo);
+        return;
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
     if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg(a.cfl_out, cfl);
@@ -562,7 +579,8 @@ cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
         configured = true;
     }
     const int nb = a.nbands > 1 ? a.nbands : 1;
-    if (nb > 1 && (!a.qsrc || a.qsrc == a.q || nb > 4)) return cudaErrorInvalidValue;
+    if (nb > 1 && (!a.qsrc || a.qsrc == a.q || nb > 4 || a.desc)) return cudaErrorInvalidValue;
+    if (a.desc && a.treg) return cudaErrorInvalidValue;
     const int blocks = (a.npatches + PPB - 1) / PPB * nb;
     if (blocks == 0) return cudaSuccess;
     step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB, LIM><<<blocks, TPB, bytes, st>>>(a);

@@ -44,6 +44,11 @@ class Server:
         self._opts[rid.value] = opts
         return rid.value
 
+    def set_work_limit(self, max_cells: int):
+        """Admit a queued solve only while the admitted solves' cells plus its
+        own stay within max_cells (0: no limit)."""
+        _check(lib().fcb_server_set_work_limit(self._h, ctypes.c_longlong(int(max_cells))))
+
     def round(self):
         a, q = ctypes.c_int(), ctypes.c_int()
         _check(lib().fcb_server_round(self._h, ctypes.byref(a), ctypes.byref(q)))

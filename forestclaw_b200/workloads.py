@@ -78,12 +78,13 @@ def bathymetry_dt(minlevel: int = 4, mx: int = 32) -> float:
     return 0.5 / (mx * (1 << minlevel))
 
 
-def dam_break_requests(n: int, seed: int, maxlevels=(4, 5, 6, 7), tfinal=(0.2, 1.0), mxs=(16, 32)):
+def dam_break_requests(n: int, seed: int, maxlevels=(4, 5, 6, 7), tfinal=(0.2, 1.0), mxs=(16, 32),
+                       subcycle: int = 1):
     """Ensemble-serving requests: dam breaks about (0.5, 0.5) with radius
     ~ U(0.1, 0.3), inner depth ~ U(1.5, 3), outer depth 1, maxlevel uniform
     over `maxlevels`, mx uniform over `mxs`, final time ~ U(tfinal); levels
-    from 2, non-subcycled (the served form), regrid every macro step,
-    adaptive dt (desired CFL 0.9)."""
+    from 2, subcycled (the reference's default) unless subcycle = 0, regrid
+    every macro step, adaptive dt (desired CFL 0.9)."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
@@ -94,6 +95,6 @@ def dam_break_requests(n: int, seed: int, maxlevels=(4, 5, 6, 7), tfinal=(0.2, 1
         o = amr_shallow_water(seed=0, minlevel=2, maxlevel=maxlevel, mx=mx, tfinal=tf)
         o.problem_params = (0.5, 0.5, float(r0), float(hin), 1.0)
         o.initial_dt = 0.9 / (mx * 4) / (hin ** 0.5 + 1)
-        o.subcycle = 0
+        o.subcycle = subcycle
         out.append(o)
     return out

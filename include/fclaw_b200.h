@@ -367,11 +367,12 @@ int fcb_partition_plan(const fcb_options_t* opt, int nranks, int rank, int nleav
 /* ---- ensemble serving -----------------------------------------------------
  * No counterpart in the reference (ForestClaw runs one solve per process): a
  * server admits independent solves as they arrive, keeps their arrays on the
- * device, and advances them together.  Each served solve uses non-subcycled
- * time stepping (subcycle = 0, nout = 1, pipelined step form); a round advances
- * every active solve by one fine step, with the patches of all solves that
- * share solver, patch shape, method and precision in ONE step launch, each
- * patch carrying its own dt.  Queued solves are admitted in arrival order while
+ * device, and advances them together.  A served solve runs to tfinal in one
+ * output interval (nout = 1), subcycled or not (subcycle), with the four-barrier
+ * or pipelined step form; a round advances every active solve by one fine step
+ * of its macro step (the level updates between two of its ghost updates), with
+ * the patches of all solves that share solver, patch shape, method and
+ * precision in ONE step launch, each patch carrying its own dt.  Queued solves are admitted in arrival order while
  * their device arrays fit in budget_bytes (one solve is always admitted when
  * none runs).  A served solve's result equals fcb_run on the same options bit
  * for bit.  Work is enqueued on cuda_stream (NULL: the legacy default stream). */
@@ -397,6 +398,12 @@ int fcb_server_status(fcb_server_t* s, int id, fcb_request_status_t* out);
 int fcb_server_get_q(fcb_server_t* s, int id, double* host, size_t n);
 /* Forget a finished, failed or queued solve and free its device arrays. */
 int fcb_server_release(fcb_server_t* s, int id);
+/* Work limit (no counterpart in the reference): admit the next queued solve
+ * only while the cells of the admitted solves' meshes (patches x mx x my,
+ * re-counted after every regrid) plus its own stay within max_cells; 0 (the
+ * default) sets no limit.  Admission stays in arrival order; a solve that
+ * waits for the limit keeps its initialised state and device arrays. */
+int fcb_server_set_work_limit(fcb_server_t* s, long long max_cells);
 /* Seconds on the server clock; rounds and step launches so far. */
 int fcb_server_clock(fcb_server_t* s, double* now, long long* rounds, long long* launches);
 

@@ -2,8 +2,9 @@
 
 A served solve must give the same result alone and in a mix of concurrent
 solves (batching only changes which launch a patch is in), and the same
-result as fcb_run on the same options with non-subcycled stepping.  Both are
-checked bit for bit, in FP64 and in the mixed FP32/FP64 form.
+result as fcb_run on the same options, subcycled or not.  Both are checked bit
+for bit, in FP64 and in the mixed FP32/FP64 form; a subcycled served solve is
+also checked against the oracle's fclaw2d_run.
 """
 import dataclasses
 
@@ -15,12 +16,13 @@ import cases
 pytestmark = pytest.mark.gpu
 
 
-def _dam(seed, maxlevel, mx=16, tfinal=0.03, precision=0):
-    import forestclaw_b200 as fcb
+def _dam_cfg(seed, maxlevel, mx=16, tfinal=0.03, subcycle=0):
+    return cases.replace(cases.radialdam_amr(seed=seed, minlevel=2, maxlevel=maxlevel, mx=mx, tfinal=tfinal),
+                         subcycle=subcycle)
 
-    cfg = cases.radialdam_amr(seed=seed, minlevel=2, maxlevel=maxlevel, mx=mx, tfinal=tfinal)
-    o = cases.to_options(cfg)
-    o.subcycle = 0
+
+def _dam(seed, maxlevel, mx=16, tfinal=0.03, precision=0, subcycle=0):
+    o = cases.to_options(_dam_cfg(seed, maxlevel, mx, tfinal, subcycle))
     o.precision = precision
     return o
 
@@ -49,10 +51,11 @@ def _serve(reqs, budget=1 << 40, stagger_rounds=0):
     return [out[k] for k in range(len(reqs))]
 
 
-def test_served_solve_equals_run(gpu_lib):
+@pytest.mark.parametrize("subcycle", [0, 1])
+def test_served_solve_equals_run(gpu_lib, subcycle):
     import forestclaw_b200 as fcb
 
-    o = _dam(seed=0, maxlevel=4)
+    o = _dam(seed=0, maxlevel=4, subcycle=subcycle)
     d = fcb.Solver(dataclasses.replace(o))
     d.initialize()
     d.run()
@@ -60,9 +63,24 @@ def test_served_solve_equals_run(gpu_lib):
     assert np.array_equal(q_served, d.get_q())
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_alone_and_in_the_mix_are_identical(gpu_lib, precision):
-    reqs = [_dam(seed=s, maxlevel=ml, tfinal=tf, precision=precision)
+def test_subcycled_served_solve_equals_oracle(gpu_lib):
+    """fclaw2d_run of the oracle (subcycled levels 2-5, time interpolation,
+    adaptive dt, regrid every macro step) against the served solve, every
+    patch array bit for bit."""
+    import oracle as O
+
+    cfg = _dam_cfg(seed=3, maxlevel=5, mx=16, tfinal=0.02, subcycle=1)
+    o = O.OracleSolver(cfg)
+    o.initialize()
+    o.run()
+    (q_served,) = _serve([cases.to_options(cfg)])
+    assert q_served.shape == o.all_q().shape
+    assert np.array_equal(q_served, o.all_q())
+
+
+@pytest.mark.parametrize("precision,subcycle", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_alone_and_in_the_mix_are_identical(gpu_lib, precision, subcycle):
+    reqs = [_dam(seed=s, maxlevel=ml, tfinal=tf, precision=precision, subcycle=subcycle)
             for s, ml, tf in [(1, 3, 0.03), (2, 5, 0.02), (3, 4, 0.04), (4, 3, 0.01)]]
     alone = [_serve([r])[0] for r in reqs]
     mixed = _serve(reqs, stagger_rounds=3)
@@ -116,3 +134,27 @@ def test_poisson_stream_reports_latencies(gpu_lib):
     assert len(res.latencies) == 6 and res.failed == 0
     assert res.pct(99) >= res.pct(50) > 0
     assert res.cell_updates > 0 and res.launches >= res.rounds
+
+
+def test_work_limit_serialises_admission(gpu_lib):
+    """A work limit smaller than any solve's cells admits one solve at a time
+    (each starts after the previous one finished); the results equal the
+    solves run alone."""
+    from forestclaw_b200.serve import DONE, Server
+
+    reqs = [_dam(seed=20 + k, maxlevel=3 + (k % 2), subcycle=1) for k in range(3)]
+    alone = [_serve([r])[0] for r in reqs]
+    sv = Server(1 << 40)
+    sv.set_work_limit(1)
+    ids = [sv.submit(r) for r in reqs]
+    sv.run_until_idle()
+    spans = []
+    for k, i in enumerate(ids):
+        st = sv.status(i)
+        assert st.state == DONE
+        spans.append((st.start_s, st.finish_s))
+        assert np.array_equal(sv.get_q(i), alone[k])
+    spans.sort()
+    for (s0, f0), (s1, f1) in zip(spans, spans[1:]):
+        assert s1 >= f0 - 1e-9
+    sv.close()
