@@ -2447,13 +2447,15 @@ void Context::repopulate(const std::vector<Leaf>& old_leaves, const std::vector<
         mesh_changed();
         qinit_slots(fresh);
     } else if (!transfer.empty()) {
-        DevBuf<int32_t> dt, df;
-        dt.reserve(transfer.size());
-        df.reserve(fine.size());
-        check(cudaMemcpy(dt.p, transfer.data(), transfer.size() * 4, cudaMemcpyHostToDevice), "transfer");
-        check(cudaMemcpy(df.p, fine.data(), fine.size() * 4, cudaMemcpyHostToDevice), "fine");
-        check(launch_regrid(d_q_, stride_, dt.p, df.p, (int)transfer.size() / 3, opt_.mx, opt_.my, opt_.mbc,
-                            opt_.meqn, st_),
+        // the transfer lists live in buffers that only grow: a freed device
+        // buffer would synchronise the whole device (every stream of a server);
+        // the previous transfer finished before its regrid returned
+        d_xfer_.reserve(transfer.size());
+        d_xfer_fine_.reserve(fine.size());
+        check(cudaMemcpy(d_xfer_.p, transfer.data(), transfer.size() * 4, cudaMemcpyHostToDevice), "transfer");
+        check(cudaMemcpy(d_xfer_fine_.p, fine.data(), fine.size() * 4, cudaMemcpyHostToDevice), "fine");
+        check(launch_regrid(d_q_, stride_, d_xfer_.p, d_xfer_fine_.p, (int)transfer.size() / 3, opt_.mx, opt_.my,
+                            opt_.mbc, opt_.meqn, st_),
               "regrid transfer");
         ++cnt_.count_kernel_launches;
         synchronize();

@@ -355,6 +355,7 @@ class Context {
     struct SvStep { int level; double t, dt; };
     std::vector<SvStep> sv_steps_;
     std::vector<std::pair<int, double>> sv_ti_;
+    DevBuf<int32_t> d_xfer_, d_xfer_fine_;  // regrid transfer lists
     DevBuf<int32_t> d_level_slots_;
     std::vector<int> level_begin_;    // size maxlevel+2
     int gmin_ = 0, gmax_ = 0;         // coarsest and finest leaf level (set with the level lists)

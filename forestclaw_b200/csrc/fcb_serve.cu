@@ -21,17 +21,50 @@ auto launch_key(const fcb_options_t& o) {
 
 Server::Server(size_t budget_bytes, cudaStream_t st) : budget_(budget_bytes), st_(st) {
     t0_ = std::chrono::steady_clock::now();
+    try {
+        check(cudaMalloc(&d_cfl_, kSlots * sizeof(unsigned long long)), "cfl slots");
+        check(cudaHostAlloc(&h_cfl_, kSlots * sizeof(unsigned long long), cudaHostAllocDefault), "host cfl slots");
+        for (int k = 0; k < kRing; ++k)
+            check(cudaEventCreateWithFlags(&desc_ev_[k], cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaEventCreateWithFlags(&step_ev_, cudaEventDisableTiming), "cudaEventCreate");
+    } catch (...) {
+        cudaFree(d_cfl_);
+        cudaFreeHost(h_cfl_);
+        for (int k = 0; k < kRing; ++k)
+            if (desc_ev_[k]) cudaEventDestroy(desc_ev_[k]);
+        if (step_ev_) cudaEventDestroy(step_ev_);
+        throw;
+    }
+    for (int k = kSlots - 1; k >= 0; --k) free_slots_.push_back(k);
 }
 
 Server::~Server() {
     cudaStreamSynchronize(st_);
+    for (auto& kv : reqs_) {
+        if (kv.second.st) cudaStreamSynchronize(kv.second.st);
+        kv.second.ctx.reset();
+        free_stream(kv.second);
+    }
     reqs_.clear();
+    cudaFree(d_cfl_);
     cudaFreeHost(h_cfl_);
-    cudaFreeHost(h_desc_pinned_);
+    for (int k = 0; k < kRing; ++k) {
+        cudaFreeHost(h_desc_pinned_[k]);
+        cudaEventDestroy(desc_ev_[k]);
+    }
+    cudaEventDestroy(step_ev_);
 }
 
 void Server::check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw Error(FCB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void Server::free_stream(Request& r) noexcept {
+    if (r.ev_ready) cudaEventDestroy(r.ev_ready);
+    if (r.ev_done) cudaEventDestroy(r.ev_done);
+    if (r.st) cudaStreamDestroy(r.st);
+    r.ev_ready = r.ev_done = nullptr;
+    r.st = nullptr;
 }
 
 double Server::now() const {
@@ -79,12 +112,17 @@ void Server::admit() {
         Request& r = reqs_.at(queue_.front());
         if (!active_.empty() && r.bytes > 0 && !r.ctx && used_ + r.bytes > budget_) return;  // known size, no room
         if (!active_.empty() && r.ctx && max_cells_ > 0 && cells_now + r.cells > max_cells_) return;
+        if (free_slots_.empty()) return;  // kSlots requests admitted at once
         if (!r.ctx) {
             try {
-                r.ctx = std::make_unique<Context>(r.opt, st_);
+                check(cudaStreamCreateWithFlags(&r.st, cudaStreamNonBlocking), "request stream");
+                check(cudaEventCreateWithFlags(&r.ev_ready, cudaEventDisableTiming), "cudaEventCreate");
+                check(cudaEventCreateWithFlags(&r.ev_done, cudaEventDisableTiming), "cudaEventCreate");
+                r.ctx = std::make_unique<Context>(r.opt, r.st);
                 r.ctx->initialize();
             } catch (const Error& e) {
                 r.ctx.reset();
+                free_stream(r);
                 r.state = REQ_FAILED;
                 r.error = e.what();
                 r.t_finish = now();
@@ -95,12 +133,16 @@ void Server::admit() {
             r.cells = (long long)r.ctx->num_patches() * r.opt.mx * r.opt.my;
             if (!active_.empty() && used_ + r.bytes > budget_) {  // first sight of its size: wait for room
                 r.ctx.reset();
+                free_stream(r);
                 return;
             }
             used_ += r.bytes;  // held from here on, also while it waits for the work limit
             if (!active_.empty() && max_cells_ > 0 && cells_now + r.cells > max_cells_) return;
         }
+        r.cslot = free_slots_.back();
+        free_slots_.pop_back();
         r.state = REQ_ACTIVE;
+        r.ending = false;
         r.t_start = now();
         r.t = 0.0;
         r.dt_min = r.opt.initial_dt;
@@ -128,11 +170,15 @@ void Server::begin_macro(Request& r) {
     }
     r.fine_total = r.fine_left = r.ctx->serve_begin(r.t, r.dt_step);
     r.macro_cfl = 0.0;
+    // the macro step's CFL maximum accumulates in the request's slot
+    check(cudaMemsetAsync(d_cfl_ + r.cslot, 0, sizeof(unsigned long long), r.st), "cfl slot");
 }
 
-// fclaw2d_run after the advance: CFL retry, dt update, regrid, end of run.
+// fclaw2d_run after the advance: CFL retry, dt update, regrid, end of run.  A
+// NaN anywhere in the macro step wins the maximum (its bits are the largest).
 void Server::end_macro(Request& r) {
     const fcb_options_t& o = r.opt;
+    if (std::isnan(r.macro_cfl)) throw Error(FCB_ERR_NUMERIC, "NaN CFL");
     r.ctx->count_advance();
     if (r.macro_cfl > o.max_cfl && o.reduce_cfl && !o.use_fixed_dt) {
         r.ctx->restore_step();
@@ -155,14 +201,55 @@ void Server::end_macro(Request& r) {
     r.state = REQ_DONE;
 }
 
+void Server::retire(Request& r, bool slot_idle) {
+    r.t_finish = now();
+    used_ -= r.bytes;
+    // a slot that a queued launch may still write is not handed out again
+    if (r.cslot >= 0 && slot_idle) free_slots_.push_back(r.cslot);
+    r.cslot = -1;
+    r.ending = false;
+    active_.erase(std::remove(active_.begin(), active_.end(), r.id), active_.end());
+}
+
+void Server::finish_macros(bool wait) {
+    std::vector<int> ids;
+    for (int id : active_)
+        if (reqs_.at(id).ending) ids.push_back(id);
+    bool first = true;
+    for (int id : ids) {
+        Request& r = reqs_.at(id);
+        const cudaError_t q = (wait && first) ? cudaEventSynchronize(r.ev_done) : cudaEventQuery(r.ev_done);
+        first = false;
+        if (q == cudaErrorNotReady) continue;
+        try {
+            check(q, "macro step");
+            std::memcpy(&r.macro_cfl, &h_cfl_[r.cslot], sizeof(double));
+            r.ending = false;
+            end_macro(r);
+        } catch (const Error& e) {
+            r.state = REQ_FAILED;
+            r.error = e.what();
+        }
+        if (r.state != REQ_ACTIVE) retire(r, true);
+    }
+}
+
 int Server::round() {
     admit();
-    if (active_.empty()) return 0;
-    // group the active requests by launch key, one launch per group
+    finish_macros(false);
+    std::vector<int> run;
+    for (int id : active_)
+        if (!reqs_.at(id).ending) run.push_back(id);
+    if (run.empty()) {
+        // nothing to launch: wait for the oldest macro step in flight
+        if (!active_.empty()) finish_macros(true);
+        return (int)active_.size();
+    }
+    // group the running requests by launch key, one launch per group
     std::vector<std::vector<int>> groups;
     {
         std::vector<decltype(launch_key(fcb_options_t{}))> keys;
-        for (int id : active_) {
+        for (int id : run) {
             const auto k = launch_key(reqs_.at(id).opt);
             size_t g = 0;
             while (g < keys.size() && !(keys[g] == k)) ++g;
@@ -173,70 +260,70 @@ int Server::round() {
             groups[g].push_back(id);
         }
     }
-    const int na = (int)active_.size();
-    std::map<int, int> cfl_slot;
-    for (int i = 0; i < na; ++i) cfl_slot[active_[i]] = i;
-    // descriptors of this fine step for every active request
+    // descriptors of this fine step for every running request
     h_desc_.clear();
     std::vector<std::pair<size_t, size_t>> ranges;
-    std::map<int, long long> cells;
     for (const auto& g : groups) {
         const size_t b = h_desc_.size();
-        for (int id : g) cells[id] = reqs_.at(id).ctx->serve_step_descs(cfl_slot[id], h_desc_);
+        for (int id : g) {
+            Request& r = reqs_.at(id);
+            r.cell_updates += r.ctx->serve_step_descs(r.cslot, h_desc_);
+        }
         ranges.emplace_back(b, h_desc_.size() - b);
     }
-    // upload, one launch per group
-    if (h_desc_.size() > h_desc_cap_) {
-        cudaFreeHost(h_desc_pinned_);
-        h_desc_cap_ = std::max(h_desc_.size(), 2 * h_desc_cap_);
-        check(cudaHostAlloc(&h_desc_pinned_, h_desc_cap_ * sizeof(PatchDesc), cudaHostAllocDefault), "host desc");
+    // upload through the next pinned buffer of the ring, once the copy that
+    // last read it has run
+    const int k = ring_;
+    ring_ = (ring_ + 1) % kRing;
+    check(cudaEventSynchronize(desc_ev_[k]), "descriptor staging");
+    if (h_desc_.size() > h_desc_cap_[k]) {
+        cudaFreeHost(h_desc_pinned_[k]);
+        h_desc_pinned_[k] = nullptr;
+        h_desc_cap_[k] = std::max(h_desc_.size(), 2 * h_desc_cap_[k]);
+        check(cudaHostAlloc(&h_desc_pinned_[k], h_desc_cap_[k] * sizeof(PatchDesc), cudaHostAllocDefault),
+              "host desc");
     }
-    if ((size_t)na > h_cfl_cap_) {
-        cudaFreeHost(h_cfl_);
-        h_cfl_cap_ = std::max<size_t>(na, 2 * h_cfl_cap_);
-        check(cudaHostAlloc(&h_cfl_, h_cfl_cap_ * sizeof(unsigned long long), cudaHostAllocDefault), "host cfl");
-    }
-    std::memcpy(h_desc_pinned_, h_desc_.data(), h_desc_.size() * sizeof(PatchDesc));
+    std::memcpy(h_desc_pinned_[k], h_desc_.data(), h_desc_.size() * sizeof(PatchDesc));
     d_desc_.reserve(std::max<size_t>(1, h_desc_.size()));
-    d_cfl_.reserve(std::max(1, na));
-    check(cudaMemcpyAsync(d_desc_.p, h_desc_pinned_, h_desc_.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, st_),
+    // the step reads what each request's stream has written so far
+    for (int id : run) {
+        Request& r = reqs_.at(id);
+        check(cudaEventRecord(r.ev_ready, r.st), "cudaEventRecord");
+        check(cudaStreamWaitEvent(st_, r.ev_ready, 0), "cudaStreamWaitEvent");
+    }
+    check(cudaMemcpyAsync(d_desc_.p, h_desc_pinned_[k], h_desc_.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice,
+                          st_),
           "descriptors");
-    check(cudaMemsetAsync(d_cfl_.p, 0, na * sizeof(unsigned long long), st_), "cfl");
+    check(cudaEventRecord(desc_ev_[k], st_), "cudaEventRecord");
     for (size_t g = 0; g < groups.size(); ++g) {
         const Request& r0 = reqs_.at(groups[g][0]);
         check(launch_step_batch(r0.opt, r0.ctx->aux_kind(), d_desc_.p + ranges[g].first, (int)ranges[g].second,
-                                d_cfl_.p, st_),
+                                d_cfl_, st_),
               "batched step");
         ++launches_;
     }
-    // each request's time interpolations and ghost update after its fine step
-    for (int id : active_) reqs_.at(id).ctx->serve_after_step();
-    check(cudaMemcpyAsync(h_cfl_, d_cfl_.p, na * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st_), "cfl");
-    check(cudaStreamSynchronize(st_), "round");
-    ++rounds_;
-    // per-request bookkeeping
-    std::vector<int> still;
-    for (int id : active_) {
+    check(cudaEventRecord(step_ev_, st_), "cudaEventRecord");
+    // each request's time interpolations and ghost update after its fine step,
+    // on its own stream; at the end of its macro step, its CFL comes back
+    for (int id : run) {
         Request& r = reqs_.at(id);
-        double c;
-        std::memcpy(&c, &h_cfl_[cfl_slot[id]], sizeof c);
         try {
-            if (std::isnan(c)) throw Error(FCB_ERR_NUMERIC, "NaN CFL");
-            r.macro_cfl = std::max(r.macro_cfl, c);
-            r.cell_updates += cells[id];
-            if (--r.fine_left == 0) end_macro(r);
+            check(cudaStreamWaitEvent(r.st, step_ev_, 0), "cudaStreamWaitEvent");
+            r.ctx->serve_after_step();
+            if (--r.fine_left == 0) {
+                check(cudaMemcpyAsync(&h_cfl_[r.cslot], d_cfl_ + r.cslot, sizeof(unsigned long long),
+                                      cudaMemcpyDeviceToHost, r.st),
+                      "cfl");
+                check(cudaEventRecord(r.ev_done, r.st), "cudaEventRecord");
+                r.ending = true;
+            }
         } catch (const Error& e) {
             r.state = REQ_FAILED;
             r.error = e.what();
-        }
-        if (r.state == REQ_ACTIVE) {
-            still.push_back(id);
-        } else {
-            r.t_finish = now();
-            used_ -= r.bytes;
+            retire(r, false);
         }
     }
-    active_.swap(still);
+    ++rounds_;
     return (int)active_.size();
 }
 
@@ -255,6 +342,9 @@ void Server::release(int id) {
         queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
         if (r.ctx) used_ -= r.bytes;  // initialised while it waited for the work limit
     }
+    if (r.st) cudaStreamSynchronize(r.st);
+    r.ctx.reset();
+    free_stream(r);
     reqs_.erase(it);
 }
 

@@ -2,21 +2,27 @@
 // device, advanced together with continuous batching.
 //
 // Each request is one solve (its own forest, arena and ghost plans, one
-// fcb::Context), subcycled or not as its options say.  A round advances every
-// active request by one fine step of its macro step (the level updates that
-// fclaw2d_advance_all_levels makes between two ghost updates: with subcycling
-// the finest level and the coarser levels whose step falls on it, each with
-// its own dt): the patches of all requests that share a launch key (solver,
-// patch shape, method, precision) go into ONE step launch, each patch carrying
-// its own arrays, geometry and dt (PatchDesc); then each request's time
-// interpolations and ghost update run and the per-request CFL numbers come
-// back in one copy.  Between rounds the loop retires finished requests, admits
-// queued ones in arrival order while their device memory fits the budget (and
-// their cells the work limit, if one is set), and runs the per-request macro-
-// step logic of fclaw2d_run (outstyle 1: small last step, CFL retry from the
-// saved copy, dt = dt * desired_cfl / cfl, regrid every regrid_interval).
-// Results are those of fcb_run on the same options, bit for bit: batching
-// changes which launch a patch is in, never its arithmetic.
+// fcb::Context on its own CUDA stream), subcycled or not as its options say.
+// A round advances every running request by one fine step of its macro step
+// (the level updates that fclaw2d_advance_all_levels makes between two ghost
+// updates: with subcycling the finest level and the coarser levels whose step
+// falls on it, each with its own dt): the patches of all requests that share a
+// launch key (solver, patch shape, method, precision) go into ONE step launch
+// on the server's stream, each patch carrying its own arrays, geometry, dt and
+// CFL slot (PatchDesc); the launch waits for each request's stream, and each
+// request's stream waits for the launch before its time interpolations and
+// ghost update.  The CFL maximum of a macro step accumulates in the request's
+// device slot and is read back, on the request's stream, only when the macro
+// step ends; the round does not wait for the GPU.  A request whose macro step
+// has ended sits out until its stream reaches that point, then the per-request
+// macro-step logic of fclaw2d_run runs on the host (outstyle 1: small last
+// step, CFL retry from the saved copy, dt = dt * desired_cfl / cfl, regrid
+// every regrid_interval), synchronising only the request's own stream, while
+// the rounds already queued keep the GPU busy.  Queued requests are admitted in
+// arrival order while their device memory fits the budget (and their cells the
+// work limit, if one is set).  Results are those of fcb_run on the same
+// options, bit for bit: batching changes which launch a patch is in, never its
+// arithmetic.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -35,8 +41,13 @@ enum RequestState : int { REQ_QUEUED = 0, REQ_ACTIVE = 1, REQ_DONE = 2, REQ_FAIL
 struct Request {
     int id = 0;
     fcb_options_t opt{};
-    std::unique_ptr<Context> ctx;
+    cudaStream_t st = nullptr;        // the request's own stream (non-blocking)
+    cudaEvent_t ev_ready = nullptr;   // its stream's work before a step launch
+    cudaEvent_t ev_done = nullptr;    // its stream's work up to the end of a macro step
+    std::unique_ptr<Context> ctx;     // destroyed before st
     int state = REQ_QUEUED;
+    bool ending = false;              // macro step enqueued to its end, CFL not yet read
+    int cslot = -1;                   // its CFL slot on the device and in pinned memory
     // time stepping (fclaw2d_run, outstyle 1, nout = 1)
     double t = 0.0;           // start of the current macro step
     double dt_min = 0.0;      // dt of the minimum level (adapted)
@@ -78,6 +89,13 @@ class Server {
     void admit();
     void begin_macro(Request& r);
     void end_macro(Request& r);
+    // ending requests whose stream has reached the end of their macro step:
+    // read the CFL and run end_macro; with wait, block for the oldest one first
+    void finish_macros(bool wait);
+    // a finished or failed request leaves the active set; slot_idle: no launch
+    // still in flight writes its CFL slot, which may then serve a new request
+    void retire(Request& r, bool slot_idle);
+    void free_stream(Request& r) noexcept;
     void check(cudaError_t e, const char* what);
 
     size_t budget_;
@@ -90,14 +108,21 @@ class Server {
     std::map<int, Request> reqs_;
     std::deque<int> queue_;
     std::vector<int> active_;
-    // round buffers
+    // round buffers: the descriptors of a round go through one of kRing pinned
+    // buffers (reused once the copy that read it has run), so the host runs at
+    // most kRing rounds ahead of the GPU
+    static constexpr int kRing = 3;
+    static constexpr int kSlots = 4096;  // CFL slots: requests admitted at once
     std::vector<PatchDesc> h_desc_;
     DevBuf<PatchDesc> d_desc_;
-    DevBuf<unsigned long long> d_cfl_;
-    unsigned long long* h_cfl_ = nullptr;  // pinned
-    size_t h_cfl_cap_ = 0;
-    PatchDesc* h_desc_pinned_ = nullptr;
-    size_t h_desc_cap_ = 0;
+    unsigned long long* d_cfl_ = nullptr;  // kSlots, device
+    unsigned long long* h_cfl_ = nullptr;  // kSlots, pinned
+    std::vector<int> free_slots_;
+    PatchDesc* h_desc_pinned_[kRing] = {};
+    size_t h_desc_cap_[kRing] = {};
+    cudaEvent_t desc_ev_[kRing] = {};
+    int ring_ = 0;
+    cudaEvent_t step_ev_ = nullptr;
     long long rounds_ = 0, launches_ = 0;
 };
 
