@@ -390,8 +390,11 @@ int fcb_server_create(size_t budget_bytes, void* cuda_stream, fcb_server_t** out
 int fcb_server_destroy(fcb_server_t* s);
 /* Queue a solve; *id receives its handle. */
 int fcb_server_submit(fcb_server_t* s, const fcb_options_t* opt, int* id);
-/* Admit what fits, advance every active solve by one fine step; reports the
- * active and queued counts after the round. */
+/* Admit what fits, enqueue one fine step of every running solve; reports the
+ * active and queued counts after the round.  The call does not wait for the
+ * GPU (each admitted solve runs on its own stream; the step launch goes to
+ * cuda_stream); it blocks only when every active solve waits for the end of
+ * its macro step to reach the host. */
 int fcb_server_round(fcb_server_t* s, int* active, int* queued);
 int fcb_server_status(fcb_server_t* s, int id, fcb_request_status_t* out);
 /* Patch arrays of a finished (or running) solve, as fcb_get_q. */
