@@ -52,11 +52,14 @@ def parse():
     p.add_argument("--workload", default="uniform_swirl",
                    choices=["uniform_swirl", "amr_radialdam", "amr_quadrants", "bathy", "serve"])
     p.add_argument("--requests", type=int, default=200, help="serve: number of requests")
-    p.add_argument("--rates", default="5,10,20,40", help="serve: Poisson arrival rates (requests/s) to sweep")
+    p.add_argument("--rates", default="auto",
+                   help="serve: Poisson arrival rates (requests/s) to sweep, or auto: 0.6, 0.8 and 0.95 of the "
+                        "capacity measured with every request submitted at once")
     p.add_argument("--serve-maxlevels", default="4,5,6,7", help="serve: maxlevel drawn uniformly from these")
     p.add_argument("--serve-tfinal", default="0.2,1.0", help="serve: final time ~ U(a, b)")
-    p.add_argument("--serve-work-limit", type=float, default=0,
-                   help="serve: cap on the cells of the admitted solves (0: none)")
+    p.add_argument("--serve-work-limit", type=float, default=3e6,
+                   help="serve: cap on the cells of the admitted solves' meshes (0: none); without one, "
+                        "concurrency and the per-solve host work of a round grow under load")
     p.add_argument("--extras", type=int, default=1,
                    help="default workload: 1 also measures the other configurations (sub-objects of the line)")
     p.add_argument("--extra-requests", type=int, default=200, help="requests of the serving sub-object (0: skip)")
@@ -766,11 +769,16 @@ def bathy_accuracy(steps, macro_graph, stream):
 # ----------------------------------------------------------------------------
 # Ensemble serving: Poisson stream of shallow-water dam-break requests
 # ----------------------------------------------------------------------------
-def serve_measure(requests, rates, local_rank, stream, label, work_limit=0):
-    """Isolated latency of every request (alone on the GPU, after one untimed
-    solve that loads the kernels and fills the autotuner's and the memory
-    pool's caches), then the Poisson stream at each rate: p50/p99 latency and
-    aggregate cell-updates/s."""
+def serve_measure(requests, rates, local_rank, stream, label, work_limit=0, loads=(0.6, 0.8, 0.95)):
+    """Isolated latency and cell updates of every request (alone on the GPU,
+    after one untimed solve that loads the kernels and fills the autotuner's
+    and the memory pool's caches); the saturation throughput (every request
+    submitted at once); then Poisson streams: at the given rates, or, with
+    rates None, at the given fractions of the capacity the saturation run
+    implies (requests/s = saturation cell-updates/s over the mean cell updates
+    of a request).  Each point reports p50/p99 latency and the aggregate
+    cell-updates/s; the knee is the lowest rate whose throughput is within 5 %
+    of the best point's."""
     import torch
 
     from forestclaw_b200.serve import Server, poisson_stream
@@ -779,33 +787,44 @@ def serve_measure(requests, rates, local_rank, stream, label, work_limit=0):
     sv = Server(budget, stream)
     poisson_stream(sv, requests[:1], rate=0.0)
     sv.close()
-    iso = []
+    iso, work = [], 0
     for o in requests:
         sv = Server(budget, stream)
         r = poisson_stream(sv, [o], rate=0.0)
         iso.append(r.latencies[0])
+        work += r.cell_updates
         sv.close()
     iso_p99 = float(np.percentile(iso, 99))
     sweep = []
     with ClockSampler(local_rank) as clk:
-        for lam in rates:
+        sv = Server(budget, stream)
+        sv.set_work_limit(work_limit)
+        r = poisson_stream(sv, requests, rate=0.0)
+        sv.close()
+        sat = r.cell_updates / r.wall
+        capacity = len(requests) * sat / work
+        points = [(lam, None) for lam in rates] if rates else [(f * capacity, f) for f in loads]
+        for lam, f in points:
             sv = Server(budget, stream)
             sv.set_work_limit(work_limit)
             r = poisson_stream(sv, requests, rate=lam, seed=11)
             sv.close()
-            sweep.append({"rate_per_s": lam, "p50_s": r.pct(50), "p99_s": r.pct(99),
-                          "cell_updates_per_s": r.cell_updates / r.wall, "wall_s": r.wall,
+            sweep.append({"rate_per_s": lam, "load": f, "p50_s": r.pct(50), "p99_s": r.pct(99),
+                          "cell_updates_per_s": r.cell_updates / r.wall,
+                          "throughput_over_saturation": r.cell_updates / r.wall / sat, "wall_s": r.wall,
                           "rounds": r.rounds, "launches": r.launches, "failed": r.failed,
                           "p99_over_isolated_p99": r.pct(99) / iso_p99})
     top = max(sweep, key=lambda d: d["cell_updates_per_s"])
-    full = [d for d in sweep if d["cell_updates_per_s"] >= 0.95 * top["cell_updates_per_s"]]
-    # knee: the lowest rate whose throughput is within 5 % of the best one (the
-    # onset of saturation); knee_highest: the highest such rate
-    knee = min(full, key=lambda d: d["rate_per_s"])
-    knee_hi = max(full, key=lambda d: d["rate_per_s"])
+    knee = min((d for d in sweep if d["cell_updates_per_s"] >= 0.95 * top["cell_updates_per_s"]),
+               key=lambda d: d["rate_per_s"])
     return {"workload": label, "requests": len(requests), "work_limit_cells": work_limit,
-            "isolated_p50_s": float(np.percentile(iso, 50)), "isolated_p99_s": iso_p99, "sweep": sweep,
-            "best": top, "knee": knee, "knee_highest": knee_hi, "clocks": clk.summary()}
+            "isolated_p50_s": float(np.percentile(iso, 50)), "isolated_p99_s": iso_p99,
+            "saturation_cell_updates_per_s": sat, "capacity_requests_per_s": capacity, "sweep": sweep,
+            "best": top, "knee": knee, "clocks": clk.summary()}
+
+
+def _rates(args):
+    return None if args.rates == "auto" else [float(x) for x in args.rates.split(",")]
 
 
 def run_serve(args, rank, world, local_rank):
@@ -824,8 +843,7 @@ def run_serve(args, rank, world, local_rank):
     label = (f"ensemble serving: Poisson stream of shallow-water dam-break solves (r ~ U(0.1,0.3), h_in ~ "
              f"U(1.5,3), maxlevel ~ U{{{','.join(map(str, maxlevels))}}}, mx ~ {{16,32}}, levels from 2, subcycled, "
              f"t_final ~ U({tf[0]},{tf[1]})), continuous batching")
-    m = serve_measure(reqs, [float(x) for x in args.rates.split(",")], local_rank, stream, label,
-                      int(args.serve_work_limit))
+    m = serve_measure(reqs, _rates(args), local_rank, stream, label, int(args.serve_work_limit))
     if rank != 0:
         return None
     top = m["best"]
@@ -836,7 +854,8 @@ def run_serve(args, rank, world, local_rank):
         "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
         "config": {"workload": label, "requests": args.requests, "work_limit_cells": m["work_limit_cells"],
                    "isolated_p50_s": m["isolated_p50_s"], "isolated_p99_s": m["isolated_p99_s"],
-                   "sweep": m["sweep"], "knee": m["knee"], "knee_highest": m["knee_highest"]},
+                   "saturation_cell_updates_per_s": m["saturation_cell_updates_per_s"],
+                   "capacity_requests_per_s": m["capacity_requests_per_s"], "sweep": m["sweep"], "knee": m["knee"]},
         "p50_s": top["p50_s"], "p99_s": top["p99_s"],
         "clocks": m["clocks"],
         "gpu_launches": top["launches"],
@@ -957,8 +976,8 @@ def run_extras(args, local_rank, main_line):
                  "h_in ~ U(1.5,3), maxlevel ~ U{4..7}, mx ~ {16,32}, levels from 2, subcycled, t_final ~ "
                  "U(0.02,0.1): the configured final times scaled by 1/10 so the sweep fits the default run), "
                  "continuous batching")
-        return serve_measure(reqs, [float(x) for x in args.rates.split(",")], local_rank, stream.cuda_stream,
-                             label)
+        return serve_measure(reqs, _rates(args), local_rank, stream.cuda_stream, label,
+                             int(args.serve_work_limit))
 
     if args.extra_requests > 0:
         guarded("serving", serving)
