@@ -158,3 +158,46 @@ def test_work_limit_serialises_admission(gpu_lib):
     for (s0, f0), (s1, f1) in zip(spans, spans[1:]):
         assert s1 >= f0 - 1e-9
     sv.close()
+
+
+def _retry_cfg(scale):
+    base = cases.radialdam_amr(seed=0, minlevel=2, maxlevel=4, mx=16, tfinal=0.05)
+    return cases.replace(base, initial_dt=scale * base.initial_dt)
+
+
+def test_served_cfl_retry_equals_run(gpu_lib):
+    """A served subcycled solve whose first macro step exceeds max_cfl (initial
+    dt 1.5 times too large): the saved state is restored and the step retaken
+    with the smaller dt, as fcb_run does; the result is bit for bit fcb_run's."""
+    import forestclaw_b200 as fcb
+
+    o = cases.to_options(_retry_cfg(1.5))
+    d = fcb.Solver(dataclasses.replace(o))
+    d.initialize()
+    d.run()
+    c = d.counters()
+    assert c["count_amr_advance"] > c["count_amr_regrid"]  # a step was retaken
+    (q_served,) = _serve([o])
+    assert np.array_equal(q_served, d.get_q())
+
+
+def test_failed_solve_leaves_the_mix_intact(gpu_lib):
+    """A solve with a negative depth outside the dam (every speed there a NaN,
+    so its CFL maximum is a NaN) fails with FCB_ERR_NUMERIC when its first
+    macro step ends; the solves batched with it finish with the same bits as
+    alone."""
+    from forestclaw_b200.serve import DONE, FAILED, Server
+
+    good = [_dam(seed=30 + k, maxlevel=3 + k, subcycle=1) for k in range(2)]
+    alone = [_serve([r])[0] for r in good]
+    bad_cfg = _dam_cfg(seed=32, maxlevel=3, subcycle=1)
+    bad = cases.to_options(cases.replace(bad_cfg, pparams=tuple(bad_cfg.pparams[:4]) + (-1.0,)))
+    sv = Server(1 << 40)
+    ids = [sv.submit(good[0]), sv.submit(bad), sv.submit(good[1])]
+    sv.run_until_idle()
+    assert sv.status(ids[1]).state == FAILED
+    assert "NaN" in sv.error(ids[1])
+    for k, i in ((0, ids[0]), (1, ids[2])):
+        assert sv.status(i).state == DONE
+        assert np.array_equal(sv.get_q(i), alone[k])
+    sv.close()
