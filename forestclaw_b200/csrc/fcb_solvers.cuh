@@ -16,6 +16,23 @@ template <typename T>
 __device__ __forceinline__ T dmax(T a, T b) { return a > b ? a : b; }
 template <typename T>
 __device__ __forceinline__ T dmin(T a, T b) { return a < b ? a : b; }
+// Maximum for the CFL number that keeps a NaN: a NaN wave speed (a negative
+// depth, say) must reach the host as a NaN CFL, which the library reports as
+// FCB_ERR_NUMERIC.  For numbers it equals dmax.
+template <typename T>
+__device__ __forceinline__ T nanmax(T a, T b) { return (b > a || b != b) ? b : a; }
+// max(m, |s|) for m >= 0 as the unsigned maximum of the bit patterns: for
+// non-negative numbers the same value as dmax, and a NaN (its magnitude's bits
+// are the largest) is kept, at the cost of one integer compare-select.
+__device__ __forceinline__ double absmax(double m, double s) {
+    const unsigned long long a = (unsigned long long)__double_as_longlong(m);
+    const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(s));
+    return __longlong_as_double((long long)(a > b ? a : b));
+}
+__device__ __forceinline__ float absmax(float m, float s) {
+    const unsigned a = __float_as_uint(m), b = __float_as_uint(fabsf(s));
+    return __uint_as_float(a > b ? a : b);
+}
 
 // ---------------------------------------------------------------------------
 // Scalar advection: applications/clawpack/advection/2d/all/clawpack46_rpn2adv.f,

@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 for (int m = 0; m < M; ++m) w[mw][m] = yw_f[mw][m];
             if (f >= MBC && f <= MBC + MX) {
 #pragma unroll
-                for (int mw = 0; mw < W; ++mw) cfl = dmax(dmax(cfl, dtdy * ys_f[mw]), -dtdy * ys_f[mw]);
+                for (int mw = 0; mw < W; ++mw) cfl = nanmax(nanmax(cfl, dtdy * ys_f[mw]), -dtdy * ys_f[mw]);
             }
             double cq[M];
 #pragma unroll
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 xs[c * W + mw] = xsl[mw];
 #pragma unroll
                 for (int m = 0; m < M; ++m) xw[(c * W + mw) * M + m] = xwl[mw][m];
-                if (c >= MBC && c <= MBC + MX) cfl = dmax(dmax(cfl, dtdx * xsl[mw]), -dtdx * xsl[mw]);
+                if (c >= MBC && c <= MBC + MX) cfl = nanmax(nanmax(cfl, dtdx * xsl[mw]), -dtdx * xsl[mw]);
             }
         }
 
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         return;
     }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+    for (int off = 16; off > 0; off >>= 1) cfl = nanmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
     if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg(a.cfl_out, cfl);
 }
 

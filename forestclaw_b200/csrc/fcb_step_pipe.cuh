@@ -501,7 +501,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
             for (int mw = 0; mw < W; ++mw) {
 #pragma unroll
                 for (int m = 0; m < M; ++m) xw[(mw * M + m) * L::PNX] = S.xwl[mw][m];
-                if (c >= MBC && c <= MBC + MX) S.smax_x = dmax(S.smax_x, fabs(S.xsl[mw]));
+                if (c >= MBC && c <= MBC + MX) S.smax_x = absmax(S.smax_x, S.xsl[mw]);
             }
         }
     }
@@ -573,7 +573,7 @@ __device__ __forceinline__ void pipe_iter(const StepArgs& a, const SOL& sol,
                 for (int m = 0; m < M; ++m) w[mw][m] = S.yw_f[mw][m];
             if (inner) {
 #pragma unroll
-                for (int mw = 0; mw < W; ++mw) S.smax_y = dmax(S.smax_y, fabs(S.ys_f[mw]));
+                for (int mw = 0; mw < W; ++mw) S.smax_y = absmax(S.smax_y, S.ys_f[mw]);
             }
             R cq[M];
 #pragma unroll
@@ -895,7 +895,7 @@ __device__ __forceinline__ void step_pipe_body(const StepArgs& a) {
     // flux2: cfl = max(cfl, dtdx*s, -dtdx*s) over the interfaces.  Rounding is
     // monotone, so max_i fl(dtdx*|s_i|) == fl(dtdx * max_i |s_i|): one product
     // per direction gives the reference's value exactly.
-    double cfl = (double)dmax(T.rdtdx * S.smax_x, T.rdtdy * S.smax_y);
+    double cfl = (double)nanmax(T.rdtdx * S.smax_x, T.rdtdy * S.smax_y);
     if (S.bad) cfl = __longlong_as_double(0x7ff8000000000000LL);  // NaN: wins the max, reported by the host
     if (a.desc) {
         // patches of different solves share warps: reduce over the lanes of each
@@ -908,7 +908,7 @@ __device__ __forceinline__ void step_pipe_body(const StepArgs& a) {
             atomicMax(a.cfl_out + req, ((unsigned long long)hi << 32) | lo);
     } else {
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+        for (int off = 16; off > 0; off >>= 1) cfl = nanmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
         if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg_p(a.cfl_out, cfl);
     }
 }

@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(128) step_kernel_warp(const StepArgs a) {
                 sol.rpn2(1, qL, q_n[j], u_s[j], xw[j], xs[j], xam[j], xap[j], xR[j]);
                 if (c >= MBC && c <= MBC + MX) {
 #pragma unroll
-                    for (int mw = 0; mw < W; ++mw) cfl = dmax(dmax(cfl, dtdx * xs[j][mw]), -dtdx * xs[j][mw]);
+                    for (int mw = 0; mw < W; ++mw) cfl = nanmax(nanmax(cfl, dtdx * xs[j][mw]), -dtdx * xs[j][mw]);
                 }
             }
         }
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(128) step_kernel_warp(const StepArgs a) {
                 for (int m = 0; m < M; ++m) wv[mw][m] = yw_f[j][mw][m];
             if (f >= MBC && f <= MBC + MX) {
 #pragma unroll
-                for (int mw = 0; mw < W; ++mw) cfl = dmax(dmax(cfl, dtdy * ys_f[j][mw]), -dtdy * ys_f[j][mw]);
+                for (int mw = 0; mw < W; ++mw) cfl = nanmax(nanmax(cfl, dtdy * ys_f[j][mw]), -dtdy * ys_f[j][mw]);
             }
             double cq[M];
 #pragma unroll
@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(128) step_kernel_warp(const StepArgs a) {
     }
 
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) cfl = dmax(cfl, __shfl_xor_sync(FULL, cfl, off));
+    for (int off = 16; off > 0; off >>= 1) cfl = nanmax(cfl, __shfl_xor_sync(FULL, cfl, off));
     if (lane == 0 && a.cfl_out) atomic_max_nonneg_w(a.cfl_out, cfl);
 }
 
