@@ -236,7 +236,6 @@ void Server::finish_macros(bool wait) {
 
 int Server::round() {
     admit();
-    finish_macros(false);
     std::vector<int> run;
     for (int id : active_)
         if (!reqs_.at(id).ending) run.push_back(id);
@@ -324,6 +323,9 @@ int Server::round() {
         }
     }
     ++rounds_;
+    // the macro-step ends (host logic, regrids) run while this round's work is
+    // queued on the GPU
+    finish_macros(false);
     return (int)active_.size();
 }
 
