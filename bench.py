@@ -371,7 +371,7 @@ def run_ours(args, rank, world, local_rank):
         "dtype": "f64" if args.precision == "fp64" else "f32/f64",
         "data": "synthetic",
         "config": {"workload": f"uniform swirl advection, level {args.level}, mx=my={args.mx}, "
-                               + ("FP64 plain" if args.precision == "fp64" else "mixed FP32/FP64"),
+                               + ("FP64" if args.precision == "fp64" else "mixed FP32/FP64"),
                    "patches": npatch, "cells": cells_per_step, "l2_flush": "inputs larger than L2",
                    "parallelism": f"{world} independent replicas" if world > 1 else "single GPU",
                    "step_kernel_ms": step_ms, "ghost_fill_ms": ghost_ms,
