@@ -76,6 +76,14 @@ struct StepArgs {
     // bands, one CTA each, which read the copy qsrc of the arena (bands
     // overlap in the rows they read) and update their own rows in q
     int32_t nbands;
+    // with nbands > 1: the first band_first CTAs update whole patches in place
+    // (from q) and only the patches after them are split into bands (the tail
+    // of a launch that would otherwise leave a nearly empty last wave)
+    int32_t band_first;
+    // four-barrier form, nbands <= 1: a scratch arena (q's layout) that lets
+    // the launcher split the last, partial wave of CTAs into row bands (the
+    // patches of that tail are copied there and read from it); null: off
+    double* qtail;
 };
 
 // Conservation registers of one slot (fclaw2d_clawpatch_registers_t), doubles

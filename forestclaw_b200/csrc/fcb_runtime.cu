@@ -1423,8 +1423,17 @@ void Context::launch_step_form(const StepArgs& a, int n) {
                              a, st_);
         if (e == cudaErrorNotSupported && v == 3) throw Error(FCB_ERR_INVALID, "no pipelined step for this case");
     }
-    if (e == cudaErrorNotSupported)
-        e = launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, a, st_);
+    if (e == cudaErrorNotSupported) {
+        StepArgs b = a;
+        if ((opt_.solver_kind == FCB_SOLVER_SWE_ROE || opt_.solver_kind == FCB_SOLVER_EULER4_ROE) && !a.treg &&
+            !a.desc) {
+            // the launcher may split the last, partial wave into row bands,
+            // reading those patches from a copy in the scratch arena
+            if (!d_qalt_) arena_alloc(d_qalt_, (size_t)capacity_ * stride_ * sizeof(double));
+            b.qtail = d_qalt_;
+        }
+        e = launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_);
+    }
     check(e, "step");
     cnt_.count_single_step += n;
     ++cnt_.count_kernel_launches;

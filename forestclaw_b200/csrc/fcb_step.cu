@@ -24,6 +24,7 @@
 // exactly as the reference's, operation by operation.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 
 #include "fcb_device.h"
@@ -103,9 +104,14 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     // is computed inside the band.  Raw y-interfaces from before row s0+1 and
     // finalized ones before s0+2 would see rows the band did not load and are
     // skipped; the first band keeps the reference's boundary behaviour.
-    const int nb = a.nbands > 1 ? a.nbands : 1;
-    const int band = (int)(blockIdx.x % (unsigned)nb);
-    const int pg = (int)(blockIdx.x / (unsigned)nb) * PPB + pl;
+    // With band_first, the CTAs before it update whole patches in place and
+    // the ones after it are the bands of the remaining patches.
+    const int B0 = a.nbands > 1 ? a.band_first : 0;
+    const bool banded = a.nbands > 1 && (int)blockIdx.x >= B0;
+    const int nb = banded ? a.nbands : 1;
+    const int rel = (int)blockIdx.x - B0;
+    const int band = banded ? rel % nb : 0;
+    const int pg = (banded ? B0 + rel / nb : (int)blockIdx.x) * PPB + pl;
     const int R0 = band * (NY - 1) / nb, R1 = (band + 1) * (NY - 1) / nb;
     const int s0 = band == 0 ? 0 : R0 - 2;
     const int s1 = band == nb - 1 ? NY : R1 + 1;
@@ -120,7 +126,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     const PatchMeta meta = D ? D->meta : (active ? a.meta[slot] : PatchMeta{0, 0, 1, 1, 0, 0});
     const int req = D ? D->req : -1;
     double* __restrict__ q = D ? D->q : a.q + (int64_t)slot * a.q_stride;
-    const double* __restrict__ qin = D ? D->q : (nb > 1 ? a.qsrc : a.q) + (int64_t)slot * a.q_stride;
+    const double* __restrict__ qin = D ? D->q : (banded ? a.qsrc : a.q) + (int64_t)slot * a.q_stride;
     double* __restrict__ qlast = D ? D->qlast : a.qlast + (int64_t)slot * a.q_stride;
     const bool save_last = active && (meta.flags & PATCH_SAVE_LAST);
     const double pdt = D ? D->dt : step_dt(a, meta.level);
@@ -559,10 +565,40 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     if ((t & 31) == 0 && a.cfl_out) atomic_max_nonneg(a.cfl_out, cfl);
 }
 
+// Copy the patches slots[0..n) of arena src into the same slots of dst
+// (two-double vectors; the slot stride is a multiple of 256 bytes).
+__global__ void copy_slots_kernel(const int32_t* __restrict__ slots, int n, const double* __restrict__ src,
+                                  double* __restrict__ dst, int64_t stride) {
+    const int64_t half = stride / 2;
+    const int64_t total = (int64_t)n * half;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int p = (int)(k / half);
+        const int64_t off = (int64_t)slots[p] * half + (k - (int64_t)p * half);
+        reinterpret_cast<double2*>(dst)[off] = reinterpret_cast<const double2*>(src)[off];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Host-side launcher: dispatch on (solver, mx, aux kind).
 // ---------------------------------------------------------------------------
 namespace {
+
+// A launch of G CTAs on an SM array that holds W at once ends with a wave of
+// G mod W CTAs that lasts a whole patch sweep.  When that tail is small, its
+// patches are split into nb row bands (nb CTAs of about 1/nb of a sweep each,
+// nb * tail <= W, at most 4), so the last wave is shorter; the full waves run
+// as before.  Returns the number of leading unbanded CTAs and sets nb, or
+// returns -1 when banding the tail does not pay.
+int tail_plan(int groups, int per_wave, int* nb) {
+    if (per_wave <= 0 || groups <= per_wave) return -1;
+    const int tail = groups % per_wave;
+    if (tail == 0) return -1;
+    const int k = std::min(4, per_wave / tail);
+    if (k < 2) return -1;
+    *nb = k;
+    return groups - tail;
+}
 
 template <class SOL, int MX, int MBC, int AUXK, int NAUX, int TPB, int LIM>
 cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
@@ -578,10 +614,40 @@ cudaError_t launch_one(const StepArgs& a, cudaStream_t st) {
         if (e != cudaSuccess) return e;
         configured = true;
     }
+    if (a.nbands <= 1 && a.qtail && !a.desc && !a.treg && a.npatches > 0) {
+        // CTAs one SM array holds at once (the Roe forms: one per SM)
+        static int per_wave = -1;
+        if (per_wave < 0) {
+            int dev = 0, sms = 0, occ = 0;
+            if (cudaGetDevice(&dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>,
+                                                              TPB, bytes) != cudaSuccess)
+                return cudaErrorInvalidValue;
+            per_wave = sms * occ;
+        }
+        int tb = 1;
+        const int b0 = tail_plan((a.npatches + PPB - 1) / PPB, per_wave, &tb);
+        if (b0 >= 0) {
+            const int first = b0 * PPB, ntail = a.npatches - first;
+            const int64_t vecs = (int64_t)ntail * (a.q_stride / 2);
+            const int cb = (int)std::min<int64_t>((vecs + 255) / 256, 4096);
+            copy_slots_kernel<<<cb, 256, 0, st>>>(a.slots + first, ntail, a.q, a.qtail, a.q_stride);
+            StepArgs t = a;
+            t.qsrc = a.qtail;
+            t.nbands = tb;
+            t.band_first = b0;
+            t.qtail = nullptr;
+            return launch_one<SOL, MX, MBC, AUXK, NAUX, TPB, LIM>(t, st);
+        }
+    }
     const int nb = a.nbands > 1 ? a.nbands : 1;
     if (nb > 1 && (!a.qsrc || a.qsrc == a.q || nb > 4 || a.desc)) return cudaErrorInvalidValue;
     if (a.desc && a.treg) return cudaErrorInvalidValue;
-    const int blocks = (a.npatches + PPB - 1) / PPB * nb;
+    const int groups = (a.npatches + PPB - 1) / PPB;
+    const int b0 = nb > 1 ? a.band_first : 0;
+    if (b0 < 0 || b0 > groups) return cudaErrorInvalidValue;
+    const int blocks = b0 + (groups - b0) * nb;
     if (blocks == 0) return cudaSuccess;
     step_kernel<SOL, MX, MBC, AUXK, NAUX, TPB, LIM><<<blocks, TPB, bytes, st>>>(a);
     return cudaGetLastError();

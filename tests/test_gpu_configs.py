@@ -291,3 +291,19 @@ def test_row_bands_time_sync_rejected(gpu_lib):
     opts.step_variant = 4
     with pytest.raises(fcb.FcbError):
         fcb.Solver(opts)
+
+
+@pytest.mark.parametrize("solver", ["radialdam", "quadrants"])
+def test_banded_last_wave(gpu_lib, solver):
+    """A level update whose CTAs end with a small last wave: on B200 (148 SMs,
+    one four-barrier Roe CTA of 12 patches of mx = 16 per SM) a level of 4,096
+    patches is 342 CTAs, two full waves and a tail of 46, which the launcher
+    splits into 3 row bands read from a copy of those patches.  Every array
+    and the CFL number equal the oracle's bit for bit, through three macro
+    steps (ghost updates between them, no regrid)."""
+    if solver == "radialdam":
+        cfg, dt = cases.replace(cases.radialdam_uniform(level=6, mx=16), mthbc=(3, 1, 1, 3)), 0.4 / (16 * 64) / 1.5
+    else:
+        cfg, dt = cases.quadrants_uniform(level=6, mx=16), 0.3 / (16 * 64) / 2.0
+    o, d = _pair(cfg, parallel=True, step_variant=1)
+    _macro_steps(o, d, 3, dt, regrid=False)
