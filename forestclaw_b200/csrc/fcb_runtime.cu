@@ -1731,9 +1731,17 @@ int Context::tune_step_form(const StepArgs& a, int n) {
     // +1 % (shallow water) and -12 % (Euler) on the AMR configurations, whose
     // level updates are bound by the SMs' throughput at one 255-register CTA
     // each, not by the length of one CTA's row sweep.
+    // The Roe systems of clawpack 4.6 in FP64 run the four-barrier form: since
+    // it shares the per-cell quantities of the Riemann problems it measured
+    // faster than the pipelined form at every size on B200 (shallow water
+    // mx = 32 about 2x, Euler 1.01-1.9x), and a choice between the two made
+    // per octave of the patch count could flip on a close race at one size and
+    // cost 2x at another (a one-wave four-barrier launch against a two-wave
+    // pipelined one), so the pipelined form is not tried for them.
     std::vector<int> cand;
     if (opt_.precision == 1 || opt_.claw_version == 5 || opt_.solver_kind == SOLVER_GEOCLAW_FWAVE) cand = {3};
     else if (aux_kind_ == AUX_SWIRL) cand = {1, 2, 3};
+    else if (opt_.solver_kind == SOLVER_SWE_ROE || opt_.solver_kind == SOLVER_EULER4_ROE) cand = {1};
     else cand = {1, 3};
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st_, &cs);

@@ -588,10 +588,11 @@ namespace {
 // G mod W CTAs that lasts a whole patch sweep.  When that tail is small, its
 // patches are split into nb row bands (nb CTAs of about 1/nb of a sweep each,
 // nb * tail <= W, at most 4), so the last wave is shorter; the full waves run
-// as before.  Returns the number of leading unbanded CTAs and sets nb, or
-// returns -1 when banding the tail does not pay.
+// as before.  A launch of at most W / 2 CTAs is all tail.  Returns the number
+// of leading unbanded CTAs and sets nb, or returns -1 when banding the tail
+// does not pay.
 int tail_plan(int groups, int per_wave, int* nb) {
-    if (per_wave <= 0 || groups <= per_wave) return -1;
+    if (per_wave <= 0 || groups <= 0 || (groups <= per_wave && 2 * groups > per_wave)) return -1;
     const int tail = groups % per_wave;
     if (tail == 0) return -1;
     const int k = std::min(4, per_wave / tail);
