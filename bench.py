@@ -305,14 +305,19 @@ def run_ours(args, rank, world, local_rank):
             torch.distributed.barrier()
         torch.cuda.synchronize()
         e0.record(stream)
+        # every step's CFL number goes into a running maximum on the device,
+        # read back once after the last step (fixed dt needs no per-step read)
         for _ in range(args.steps):
-            s.advance_all_levels(t, dt)
+            s.advance_all_levels_async(t, dt)
             t += dt
+        max_cfl = s.read_max_cfl()
         e1.record(stream)
         torch.cuda.synchronize()
         if dist:
             torch.distributed.barrier()
     ms = e0.elapsed_time(e1)
+    if not 0.0 < max_cfl <= opts.max_cfl:
+        raise RuntimeError(f"CFL number {max_cfl} outside (0, max_cfl]")
     c1 = s.counters()
     launches = c1["count_kernel_launches"] - c0["count_kernel_launches"]
     cells = (c1["count_single_step"] - c0["count_single_step"]) * args.mx * args.mx
@@ -378,7 +383,11 @@ def run_ours(args, rank, world, local_rank):
                    "ghost_fill": "fused into the step (neighbour reads)" if fused else "separate launch",
                    "e2e_state_transfer": f"the whole state uploaded once and downloaded once per {args.steps} "
                                          "steps (the arrays stay resident between steps), so e2e grows "
-                                         "with --steps"},
+                                         "with --steps; every e2e step reads its CFL number back",
+                   "timed_steps": "fcb_advance_all_levels_async: every step's CFL number folded into a "
+                                  "device maximum, read back once after the last step, inside the timed "
+                                  "region",
+                   "max_cfl": max_cfl},
         "clocks": clk.summary(),
         "e2e": {"value": total_cells / (e2e_ms * 1e-3),
                 "unit": "cell-updates/s",
@@ -887,8 +896,9 @@ def _uniform_quick(level, mx, precision, steps, warmup, stream, local_rank):
     with ClockSampler(local_rank) as clk:
         e0.record(stream)
         for _ in range(steps):
-            s.advance_all_levels(t, dt)
+            s.advance_all_levels_async(t, dt)
             t += dt
+        s.read_max_cfl()
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)

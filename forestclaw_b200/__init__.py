@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = (
     "fcb_measure_fp_rate", "fcb_output_ascii", "fcb_comm_create_local", "fcb_comm_nccl_unique_id",
     "fcb_comm_create_nccl", "fcb_comm_destroy", "fcb_context_create_partitioned", "fcb_partition_info",
     "fcb_global_maximum", "fcb_partition_plan", "fcb_step_kernel_time", "fcb_server_set_work_limit",
+    "fcb_advance_all_levels_async", "fcb_read_max_cfl",
 )
 
 
@@ -219,6 +220,8 @@ def lib():
     for n in ("fcb_initialize", "fcb_run", "fcb_synchronize"):
         getattr(L, n).argtypes = [vp]
     L.fcb_advance_all_levels.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp]
+    L.fcb_advance_all_levels_async.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+    L.fcb_read_max_cfl.argtypes = [vp, dp]
     L.fcb_update_single_step.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp]
     L.fcb_update_single_step_async.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
     L.fcb_single_step_update.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
@@ -414,6 +417,16 @@ class Solver:
     def advance_all_levels(self, t: float, dt: float) -> float:
         c = ctypes.c_double()
         _check(lib().fcb_advance_all_levels(self._h, t, dt, ctypes.byref(c)))
+        return c.value
+
+    def advance_all_levels_async(self, t: float, dt: float):
+        """The macro step without waiting for its CFL number (see read_max_cfl)."""
+        _check(lib().fcb_advance_all_levels_async(self._h, t, dt))
+
+    def read_max_cfl(self) -> float:
+        """Largest CFL number of the asynchronous macro steps since the last read."""
+        c = ctypes.c_double()
+        _check(lib().fcb_read_max_cfl(self._h, ctypes.byref(c)))
         return c.value
 
     def update_single_step(self, level: int, t: float, dt: float) -> float:

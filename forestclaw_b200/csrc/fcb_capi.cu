@@ -107,6 +107,21 @@ int fcb_advance_all_levels(fcb_context_t* ctx, double t, double dt, double* maxc
     });
 }
 
+int fcb_advance_all_levels_async(fcb_context_t* ctx, double t, double dt) {
+    return collective(ctx, [&] {
+        CTX();
+        C.advance_all_levels_async(t, dt);
+    });
+}
+
+int fcb_read_max_cfl(fcb_context_t* ctx, double* maxcfl) {
+    return guard([&] {
+        CTX();
+        need(maxcfl, "maxcfl");
+        *maxcfl = C.read_max_cfl();
+    });
+}
+
 int fcb_update_single_step(fcb_context_t* ctx, int level, double t, double dt, double* maxcfl) {
     return guard([&] {
         CTX();

@@ -190,7 +190,10 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
 // The CFL words (first device use of a context: creation itself touches no device).
 void Context::ensure_scalars() {
     if (d_cfl_) return;
-    check(cudaMalloc(&d_cfl_, 4 * sizeof(unsigned long long)), "cudaMalloc cfl");
+    // [0] macro step, [1] level / batch, [2] global maximum, [3] autotuner,
+    // [4] running maximum of the asynchronous macro steps
+    check(cudaMalloc(&d_cfl_, 5 * sizeof(unsigned long long)), "cudaMalloc cfl");
+    check(cudaMemsetAsync(d_cfl_, 0, 5 * sizeof(unsigned long long), st_), "memset cfl");
     check(cudaHostAlloc(&h_cfl_, sizeof(unsigned long long), cudaHostAllocDefault), "cudaHostAlloc cfl");
 }
 
@@ -1597,9 +1600,41 @@ void Context::drop_macro_graph() {
 // later calls replay it; every call first runs the schedule "dry" on the host
 // to fill the {dt, vt} table that the step launches read.
 double Context::advance_all_levels(double t_curr, double dt) {
+    advance_enqueue(t_curr, dt);
+    return read_cfl(d_cfl_);
+}
+
+namespace {
+// acc = max(acc, v) on the bits of non-negative doubles (a NaN wins)
+__global__ void cfl_merge_kernel(unsigned long long* acc, const unsigned long long* v) { atomicMax(acc, *v); }
+}  // namespace
+
+// The macro step without the wait for its CFL number: the number is folded
+// into a running maximum on the device, which read_max_cfl returns.
+void Context::advance_all_levels_async(double t_curr, double dt) {
+    advance_enqueue(t_curr, dt);
+    cfl_merge_kernel<<<1, 1, 0, st_>>>(d_cfl_ + 4, d_cfl_);
+    check(cudaGetLastError(), "cfl merge");
+    ++cnt_.count_kernel_launches;
+}
+
+double Context::read_max_cfl() {
+    if (!d_cfl_) throw Error(FCB_ERR_STATE, "read_max_cfl before initialize");
+    check(cudaMemcpyAsync(h_cfl_, d_cfl_ + 4, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st_), "cfl");
+    check(cudaMemsetAsync(d_cfl_ + 4, 0, sizeof(unsigned long long), st_), "memset");
+    synchronize();
+    const double c = cfl_from_bits(*h_cfl_);
+    if (std::isnan(c)) throw Error(FCB_ERR_NUMERIC, "NaN CFL in an asynchronous macro step");
+    return c;
+}
+
+void Context::advance_enqueue(double t_curr, double dt) {
     if (!initialized_) throw Error(FCB_ERR_STATE, "advance before initialize");
     fused_used_ = 0;
-    if (use_fusion(t_curr, dt)) return advance_fused(t_curr, dt);
+    if (use_fusion(t_curr, dt)) {
+        advance_fused(t_curr, dt);
+        return;
+    }
     ensure_ghosts();
     // on an error, plan builds still running are joined and dropped
     struct PlanGuard {
@@ -1692,7 +1727,6 @@ double Context::advance_all_levels(double t_curr, double dt) {
     plans_guard.armed = false;
     ++cnt_.count_amr_advance;
     ghosts_filled_ = true;  // the macro step ends with a ghost update of every level
-    return read_cfl(d_cfl_);
 }
 
 // ---------------------------------------------------------------------------
@@ -2003,7 +2037,7 @@ void Context::launch_fused_step(double t, double dt, const double* src, double* 
 // fclaw2d_advance_all_levels on a mesh of one level l: n_fine updates of l
 // (subcycled: 2^(l - minlevel) steps of dt halved per level; otherwise
 // 2^(maxlevel - minlevel) steps of dt/rf), each followed by a ghost update.
-double Context::advance_fused(double t_curr, double dt) {
+void Context::advance_fused(double t_curr, double dt) {
     int n_fine;
     double dt_fine = dt;
     if (opt_.subcycle) {
@@ -2029,7 +2063,6 @@ double Context::advance_fused(double t_curr, double dt) {
     fused_used_ = 1;
     step_form_used_ = 3;
     ++cnt_.count_amr_advance;
-    return read_cfl(d_cfl_);
 }
 
 void Context::ensure_ghosts() {

@@ -122,6 +122,10 @@ class Context {
     void initialize();
     void run();
     double advance_all_levels(double t, double dt);
+    // the same macro step without waiting for its CFL number, which goes into a
+    // running maximum on the device; read_max_cfl waits, returns and resets it
+    void advance_all_levels_async(double t, double dt);
+    double read_max_cfl();
     double update_single_step(int level, double t, double dt);
     void update_single_step_async(int level, double t, double dt);
     double single_step_update(int patchno, double t, double dt, int iter, int total);
@@ -293,7 +297,8 @@ class Context {
     // ensure_ghosts() before anything reads ghost cells.
     bool fusion_possible() const;             // mesh, options and step form allow it
     bool use_fusion(double t, double dt);     // possible and chosen (tuner or forced)
-    double advance_fused(double t, double dt);
+    void advance_fused(double t, double dt);
+    void advance_enqueue(double t, double dt);  // a macro step, its CFL left in d_cfl_[0]
     void launch_fused_step(double t, double dt, const double* src, double* dst, unsigned long long* cfl_slot);
     // device time of `launches` step launches (fused: the fused step; with_fill:
     // the unfused step followed by the ghost fill) on scratch copies of q

@@ -212,6 +212,15 @@ int fcb_run(fcb_context_t* ctx);
 /* fclaw2d_advance_all_levels (src/fclaw2d_advance.c:247): one subcycled
  * macro-step from t with coarse step dt; returns the max CFL over all updates. */
 int fcb_advance_all_levels(fcb_context_t* ctx, double t, double dt, double* maxcfl);
+/* The same macro step (fclaw2d_advance_all_levels, src/fclaw2d_advance.c:247)
+ * without waiting for its CFL number: the call returns once the work is
+ * enqueued on the context's stream, and the number goes into a running maximum
+ * on the device.  fcb_read_max_cfl waits for the work enqueued so far, returns
+ * the largest CFL number of the asynchronous macro steps since the last read
+ * (0 if none) and resets it; a NaN there is FCB_ERR_NUMERIC.  For run loops
+ * that need the CFL number only every few steps (fixed dt). */
+int fcb_advance_all_levels_async(fcb_context_t* ctx, double t, double dt);
+int fcb_read_max_cfl(fcb_context_t* ctx, double* maxcfl);
 /* fclaw2d_update_single_step (src/fclaw2d_update_single_step.c:73): every patch
  * of `level` advanced by dt in one batched launch; returns the level max CFL. */
 int fcb_update_single_step(fcb_context_t* ctx, int level, double t, double dt, double* maxcfl);

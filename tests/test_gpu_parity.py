@@ -312,3 +312,32 @@ def test_merged_level_launches_bit_exact(gpu_lib):
     cp, cm = per_level.counters(), merged.counters()
     assert cm["count_single_step"] == cp["count_single_step"]
     assert cm["count_kernel_launches"] < cp["count_kernel_launches"]
+
+
+@pytest.mark.parametrize("case", ["swirl_fused", "amr_swe"])
+def test_async_macro_steps_equal_sync(gpu_lib, case):
+    """fcb_advance_all_levels_async enqueues the same macro steps as
+    fcb_advance_all_levels without waiting for each CFL number; the running
+    maximum that fcb_read_max_cfl returns equals the largest of the
+    synchronous CFL numbers, bit for bit, and so do the fields (a mesh of one
+    level with the ghost exchange fused into the step, and a subcycled AMR
+    mesh with time interpolation, both with the macro-step graph)."""
+    import forestclaw_b200 as fcb
+
+    if case == "swirl_fused":
+        cfg, dt = cases.swirl_uniform(level=4, mx=16), cases.swirl_dt(level=4, mx=16)
+    else:
+        cfg, dt = cases.radialdam_amr(seed=0, minlevel=2, maxlevel=4, mx=16), 0.004
+    sync = fcb.Solver(cases.to_options(cfg))
+    asyn = fcb.Solver(cases.to_options(cfg))
+    sync.initialize()
+    asyn.initialize()
+    assert asyn.read_max_cfl() == 0.0
+    cfls = [sync.advance_all_levels(k * dt, dt) for k in range(4)]
+    for k in range(4):
+        asyn.advance_all_levels_async(k * dt, dt)
+    assert asyn.read_max_cfl() == max(cfls)
+    assert asyn.read_max_cfl() == 0.0  # reset by the read
+    assert np.array_equal(asyn.get_q(), sync.get_q())
+    sync.close()
+    asyn.close()
