@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <tuple>
 
 namespace fcb {
@@ -215,22 +216,50 @@ void Server::finish_macros(bool wait) {
     std::vector<int> ids;
     for (int id : active_)
         if (reqs_.at(id).ending) ids.push_back(id);
+    // the requests whose stream has reached the end of their macro step
+    std::vector<Request*> ready;
     bool first = true;
     for (int id : ids) {
         Request& r = reqs_.at(id);
         const cudaError_t q = (wait && first) ? cudaEventSynchronize(r.ev_done) : cudaEventQuery(r.ev_done);
         first = false;
         if (q == cudaErrorNotReady) continue;
-        try {
-            check(q, "macro step");
-            std::memcpy(&r.macro_cfl, &h_cfl_[r.cslot], sizeof(double));
-            r.ending = false;
-            end_macro(r);
-        } catch (const Error& e) {
+        r.ending = false;
+        if (q != cudaSuccess) {
+            cudaGetLastError();
             r.state = REQ_FAILED;
-            r.error = e.what();
+            r.error = std::string("macro step: ") + cudaGetErrorString(q);
+            continue;
         }
-        if (r.state != REQ_ACTIVE) retire(r, true);
+        std::memcpy(&r.macro_cfl, &h_cfl_[r.cslot], sizeof(double));
+        ready.push_back(&r);
+    }
+    // fclaw2d_run's logic of each (CFL retry, dt, regrid) touches only that
+    // request's context, stream and CFL slot, so the requests run it on
+    // separate host threads (a regrid costs the host milliseconds)
+    auto finish = [this](Request* r) {
+        try {
+            end_macro(*r);
+        } catch (const Error& e) {
+            r->state = REQ_FAILED;
+            r->error = e.what();
+        } catch (const std::exception& e) {
+            r->state = REQ_FAILED;
+            r->error = e.what();
+        }
+    };
+    if (ready.size() == 1) {
+        finish(ready[0]);
+    } else if (ready.size() > 1) {
+        std::vector<std::thread> th;
+        th.reserve(ready.size() - 1);
+        for (size_t k = 1; k < ready.size(); ++k) th.emplace_back(finish, ready[k]);
+        finish(ready[0]);
+        for (auto& t : th) t.join();
+    }
+    for (int id : ids) {
+        Request& r = reqs_.at(id);
+        if (!r.ending && r.state != REQ_ACTIVE) retire(r, true);
     }
 }
 
