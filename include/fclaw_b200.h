@@ -218,7 +218,9 @@ int fcb_advance_all_levels(fcb_context_t* ctx, double t, double dt, double* maxc
  * on the device.  fcb_read_max_cfl waits for the work enqueued so far, returns
  * the largest CFL number of the asynchronous macro steps since the last read
  * (0 if none) and resets it; a NaN there is FCB_ERR_NUMERIC.  For run loops
- * that need the CFL number only every few steps (fixed dt). */
+ * that need the CFL number only every few steps (fixed dt).  In a partitioned
+ * solve both calls are per rank, as fcb_advance_all_levels is: the number is
+ * the rank's maximum (fcb_global_maximum reduces it). */
 int fcb_advance_all_levels_async(fcb_context_t* ctx, double t, double dt);
 int fcb_read_max_cfl(fcb_context_t* ctx, double* maxcfl);
 /* fclaw2d_update_single_step (src/fclaw2d_update_single_step.c:73): every patch
