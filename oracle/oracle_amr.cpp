@@ -260,7 +260,8 @@ void Solver::qinit_patch(int p) {
                             opt.solver.gamma1, pp + 0, pp + 4, pp + 8, pp + 12, pp[16], pp[17], q);
             break;
         case PROB_PERIODIC_DISC:
-            // pparams: uvel, vvel, x0, y0, r0
+        case PROB_FILAMENT:
+            // pparams: uvel, vvel (periodic only), x0, y0, r0 (filament/fdisc.f: (0.5, 1), 0.25)
             qinit_disc_fraction(opt.mx, opt.my, opt.mbc, opt.meqn, xphys(p), yphys(p), dx(p), dy(p), pp[2], pp[3],
                                 pp[4], q);
             break;
@@ -282,6 +283,8 @@ void Solver::setaux_patch(int p) {
         setaux_bathy(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), data[p].aux.data());
     if (opt.problem == PROB_PERIODIC_DISC)  // pparams: uvel, vvel
         setaux_velocity(opt.mx, opt.my, opt.mbc, opt.maux, opt.pparams[0], opt.pparams[1], data[p].aux.data());
+    if (opt.problem == PROB_FILAMENT)
+        setaux_filament(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), data[p].aux.data());
 }
 
 // clawpack46_update (fc2d_clawpack46.cpp:403-444) for one patch.

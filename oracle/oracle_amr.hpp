@@ -16,7 +16,7 @@ namespace orc {
 
 enum Relation { REL_BOUNDARY = 0, REL_HALFSIZE = 1, REL_SAMESIZE = 2, REL_DOUBLESIZE = 3 };
 
-enum Problem { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2, PROB_BATHY = 3, PROB_RADIALDAM_CELLAVE = 4, PROB_HUMP = 5, PROB_PERIODIC_DISC = 6 };
+enum Problem { PROB_SWIRL = 0, PROB_RADIALDAM = 1, PROB_QUADRANTS = 2, PROB_BATHY = 3, PROB_RADIALDAM_CELLAVE = 4, PROB_HUMP = 5, PROB_PERIODIC_DISC = 6, PROB_FILAMENT = 7 };
 
 struct Options {
     // [clawpatch]

@@ -329,11 +329,14 @@ void rpn2_geoclaw(const Slice& S, double grav, double drytol, int ixy, int meqn,
         }
 }
 
-// applications/clawpack/advection/2d/all/clawpack46_rpn2adv.f:1-61
+// applications/clawpack/advection/2d/all/clawpack46_rpn2adv.f:1-61; with
+// shift = 1, clawpack46_rpn2adv_manifold.f:1-42 (s = auxl(i, 1+ixy): the edge
+// velocities follow the capacity in aux(1)); clawpack5_rpn2adv(_manifold).f90
+// have the same arithmetic
 void rpn2_adv(const Slice& S, int ixy, int meqn, int mwaves, int mx, const double* q,
-              const double* auxl, double* wave, double* s, double* amdq, double* apdq) {
+              const double* auxl, double* wave, double* s, double* amdq, double* apdq, int shift) {
     const int L = S.L, mbc = S.mbc;
-    const int iface = ixy;  // aux component 1 = x velocity, 2 = y velocity
+    const int iface = ixy + shift;  // aux component 1 (+shift) = x velocity, 2 (+shift) = y velocity
     double delta[10];
     for (int i = 2 - mbc; i <= mx + mbc; ++i) {
         const int ii = S.at(i);
@@ -357,11 +360,12 @@ void rpn2_adv(const Slice& S, int ixy, int meqn, int mwaves, int mx, const doubl
     }
 }
 
-// applications/clawpack/advection/2d/all/clawpack46_rpt2adv.f:62-89
+// applications/clawpack/advection/2d/all/clawpack46_rpt2adv.f:62-89; with
+// shift = 1, clawpack46_rpt2adv_manifold.f:1-44 (aux(i1, iface+1))
 void rpt2_adv(const Slice& S, int ixy, int meqn, int mx, const double* aux2, const double* aux3,
-              int imp, const double* asdq, double* bmasdq, double* bpasdq) {
+              int imp, const double* asdq, double* bmasdq, double* bpasdq, int shift) {
     const int L = S.L, mbc = S.mbc;
-    const int kv = 3 - ixy;
+    const int kv = 3 - ixy + shift;
     for (int i = 2 - mbc; i <= mx + mbc; ++i) {
         const int ii = S.at(i);
         const int i1 = S.at(i - 2 + imp);
@@ -685,8 +689,9 @@ struct Work {
 void call_rpn2(const SolverParams& sp, Work& w, int ixy, int mx) {
     switch (sp.kind) {
         case SOLVER_ADVECTION:
+        case SOLVER_ADVECTION_MANIFOLD:
             rpn2_adv(w.S, ixy, w.meqn, w.mwaves, mx, w.q1d.data(), w.aux2.data(), w.wave.data(),
-                     w.s.data(), w.amdq.data(), w.apdq.data());
+                     w.s.data(), w.amdq.data(), w.apdq.data(), sp.kind == SOLVER_ADVECTION_MANIFOLD);
             break;
         case SOLVER_SWE_ROE:
             rpn2_swe(w.S, w.R, sp.grav, ixy, w.meqn, w.mwaves, mx, w.q1d.data(), w.wave.data(),
@@ -707,8 +712,9 @@ void call_rpn2(const SolverParams& sp, Work& w, int ixy, int mx) {
 void call_rpt2(const SolverParams& sp, Work& w, int ixy, int mx, int imp, const double* asdq) {
     switch (sp.kind) {
         case SOLVER_ADVECTION:
+        case SOLVER_ADVECTION_MANIFOLD:
             rpt2_adv(w.S, ixy, w.meqn, mx, w.aux2.data(), w.aux3.data(), imp, asdq,
-                     w.bmasdq.data(), w.bpasdq.data());
+                     w.bmasdq.data(), w.bpasdq.data(), sp.kind == SOLVER_ADVECTION_MANIFOLD);
             break;
         case SOLVER_SWE_ROE:
             rpt2_swe(w.S, w.R, ixy, w.meqn, w.mwaves, mx, asdq, w.bmasdq.data(), w.bpasdq.data(), w.v5);
@@ -1079,6 +1085,59 @@ void setaux_velocity(int mx, int my, int mbc, int maux, double uvel, double vvel
             aux[P(i, j, 0)] = uvel;
             aux[P(i, j, 1)] = vvel;
             for (int k = 2; k < maux; ++k) aux[P(i, j, k)] = 0.0;  // not set by the reference (unused)
+        }
+}
+
+namespace {
+
+// filament/psi.f: psi = (4/3) r**3 (r**3 as r*r*r), r = sqrt((x-1)**2 + (y-1)**2)
+double psi_filament(double x, double y) {
+    const double r = std::sqrt((x - 1.0) * (x - 1.0) + (y - 1.0) * (y - 1.0));
+    return (4.0 / 3.0) * (r * r * r);
+}
+
+// fclaw2d_metric_default_fort.f90 get_area_approx: |T_xi x T_eta| of the
+// bilinear cell at its centre; corners q[icell][jcell] = (x, y), z = 0
+double area_approx(const double q[2][2][2]) {
+    double a01[3], a10[3], a11[3], txi[3], teta[3];
+    for (int m = 0; m < 3; ++m) {
+        const double c00 = m < 2 ? q[0][0][m] : 0.0, c10 = m < 2 ? q[1][0][m] : 0.0;
+        const double c01 = m < 2 ? q[0][1][m] : 0.0, c11 = m < 2 ? q[1][1][m] : 0.0;
+        a01[m] = c10 - c00;
+        a10[m] = c01 - c00;
+        a11[m] = c11 - c10 - c01 + c00;
+    }
+    for (int m = 0; m < 3; ++m) {
+        txi[m] = a01[m] + a11[m] * 0.5;
+        teta[m] = a10[m] + a11[m] * 0.5;
+    }
+    const double w1 = txi[1] * teta[2] - txi[2] * teta[1];
+    const double w2 = -txi[0] * teta[2] + txi[2] * teta[0];
+    const double w3 = txi[0] * teta[1] - txi[1] * teta[0];
+    return std::sqrt(w1 * w1 + w2 * w2 + w3 * w3);
+}
+
+}  // namespace
+
+void setaux_filament(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double* aux) {
+    const PatchIdx P(mx, my, mbc);
+    const double dxdy = dx * dy;
+    auto nx = [&](int i) { return xlower + (i - 1) * dx; };
+    auto ny = [&](int j) { return ylower + (j - 1) * dy; };
+    for (int i = 1 - mbc; i <= mx + mbc; ++i)
+        for (int j = 1 - mbc; j <= my + mbc; ++j) {
+            double q[2][2][2];
+            for (int ic = 0; ic < 2; ++ic)
+                for (int jc = 0; jc < 2; ++jc) {
+                    q[ic][jc][0] = nx(i) + ic * dx;  // xe + icell*dx
+                    q[ic][jc][1] = ny(j) + jc * dy;
+                }
+            aux[P(i, j, 0)] = area_approx(q) / dxdy;
+        }
+    for (int i = 1 - mbc; i <= mx + mbc; ++i)
+        for (int j = 1 - mbc; j <= my + mbc; ++j) {
+            aux[P(i, j, 1)] = (psi_filament(nx(i), ny(j + 1)) - psi_filament(nx(i), ny(j))) / dy;
+            aux[P(i, j, 2)] = -((psi_filament(nx(i + 1), ny(j)) - psi_filament(nx(i), ny(j))) / dx);
         }
 }
 

@@ -20,6 +20,8 @@ enum SolverKind {
     SOLVER_SWE_ROE = 1,     // shallow/2d/rp/clawpack46_rpn2.f / rpt2.f
     SOLVER_EULER4_ROE = 2,  // euler/2d/rp/clawpack46_rpn2_euler4.f / rpt2_euler4.f
     SOLVER_GEOCLAW_FWAVE = 3,  // shallow/2d/rp/rpn2_geoclaw.f90 (f-waves, clawpack46_flux2fw.f)
+    SOLVER_ADVECTION_MANIFOLD = 4,  // advection/2d/all/clawpack46_rpn2adv_manifold.f / rpt2adv_manifold.f
+                                    // (aux(1) capacity, aux(2:3) edge velocities)
 };
 
 struct SolverParams {
@@ -90,6 +92,18 @@ void setaux_bathy(int mx, int my, int mbc, double xlower, double ylower, double 
 // (q = the fraction of each cell inside the disc sqrt((x-x0)^2+(y-y0)^2) < r0,
 // cellave2.f; the application's disc is r0 = 0.25 about the origin).
 void setaux_velocity(int mx, int my, int mbc, int maux, double uvel, double vvel, double* aux);
+
+// advection/2d/filament, example 1 (a 2 x 2 brick under the cart mapping,
+// manifold = T): all/user46_setaux_manifold.f with the metric's affine area
+// (src/patches/metric/fortran_source2d/fclaw2d_metric_default_fort.f90:
+// compute_area_affine, get_area_approx, norm_cross) and filament/psi.f:
+//   aux(i,j,1) = area(i,j)/(dx*dy),
+//   aux(i,j,2) = (psi(node(i,j+1)) - psi(node(i,j)))/dy,
+//   aux(i,j,3) = -(psi(node(i+1,j)) - psi(node(i,j)))/dx,
+// psi = (4/3) r^3, r = |(x,y) - (1,1)|, node(i,j) = (xlower+(i-1)dx, ylower+(j-1)dy).
+// The brick and cart maps send every node of this dyadic mesh to the same
+// point of [0,2]^2 exactly, so the nodes are the physical coordinates.
+void setaux_filament(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double* aux);
 void qinit_disc_fraction(int mx, int my, int mbc, int meqn, double xlower, double ylower, double dx, double dy,
                          double x0, double y0, double r0, double* q);
 void qinit_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, const double* p,

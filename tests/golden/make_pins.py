@@ -5,7 +5,8 @@ The reference's regression tests pin three counters per run
 count_amr_new_domain.  This script copies those numbers for the runs whose
 configuration lies on this path (swirl, quadrants, bump and the periodic
 2 x 2 brick with clawpack 4.6 and 5, radialdam example 0 with clawpack 4.6
-and 5 and time-sync), so the tests can check the oracle and the CUDA path without
+and 5 and time-sync, filament example 1 (the cart-mapped 2 x 2 brick with
+capacity) with clawpack 4.6 and 5), so the tests can check the oracle and the CUDA path without
 the reference tree.
 
 Usage: python tests/golden/make_pins.py REFERENCE_ROOT
@@ -36,6 +37,8 @@ RUNS = {
     "bump_claw5": "applications/clawpack/shallow/2d/bump/regression_values_1.csv",
     "periodic": "applications/clawpack/advection/2d/periodic/regression_values_0.csv",
     "periodic_claw5": "applications/clawpack/advection/2d/periodic/regression_values_1.csv",
+    "filament": "applications/clawpack/advection/2d/filament/regression_values_0.csv",
+    "filament_claw5": "applications/clawpack/advection/2d/filament/regression_values_1.csv",
 }
 
 

@@ -18,9 +18,9 @@ ROOT = Path(__file__).resolve().parents[1]
 ORACLE_DIR = ROOT / "oracle"
 
 # Solver kinds (oracle/oracle_patch.hpp SolverKind)
-ADVECTION, SWE_ROE, EULER4_ROE, GEOCLAW_FWAVE = 0, 1, 2, 3
+ADVECTION, SWE_ROE, EULER4_ROE, GEOCLAW_FWAVE, ADVECTION_MANIFOLD = 0, 1, 2, 3, 4
 # Problems (oracle/oracle_amr.hpp Problem)
-SWIRL, RADIALDAM, QUADRANTS, BATHY, RADIALDAM_CELLAVE, HUMP, PERIODIC_DISC = 0, 1, 2, 3, 4, 5, 6
+SWIRL, RADIALDAM, QUADRANTS, BATHY, RADIALDAM_CELLAVE, HUMP, PERIODIC_DISC, FILAMENT = 0, 1, 2, 3, 4, 5, 6, 7
 # Tagging criteria (oracle/oracle_clawpatch.hpp TagCriteria)
 VALUE, MINMAX, DIFFERENCE, GRADIENT = 0, 1, 2, 3
 
@@ -358,6 +358,24 @@ def periodic_regression(claw_version: int = 4) -> Config:
                   subcycle=1, solver=ADVECTION, problem=PERIODIC_DISC, criteria=MINMAX,
                   pparams=(1.0, 1.0, 0.0, 0.0, 0.25), claw_version=claw_version,
                   extent=(-1.0, 1.0, -1.0, 1.0), brick=2, periodic_x=1, periodic_y=1)
+
+
+def filament_regression(claw_version: int = 4) -> Config:
+    """applications/clawpack/advection/2d/filament/regression_map.ini with
+    --user:example=1 on top of that directory's fclaw_options.ini (minmax
+    tagging): a 2 x 2 brick under the cart mapping shifted by (1, 1), i.e.
+    [0, 2]^2, manifold = T, capacity aux(1) (mcapa = 1), edge velocities from
+    psi = (4/3) r^3 about (1, 1) in aux(2:3) (user46_setaux_manifold.f), the
+    manifold advection solvers, q = the fraction of each cell inside the disc of
+    radius 0.25 about (0.5, 1) (fdisc.f, cellave2.f), mx = 16, levels 3-5 of
+    each block, van Leer limiter, t = 0 .. 0.025 from dt = 0.0025."""
+    return Config(mx=16, my=16, mbc=2, meqn=1, maux=3, order=(2, 2), mcapa=1, mwaves=1, mthlim=(3,),
+                  mthbc=(1, 1, 1, 1), minlevel=3, maxlevel=5, regrid_interval=1,
+                  refine_threshold=0.25, coarsen_threshold=0.05, smooth_refine=1, smooth_level=5,
+                  tfinal=0.025, initial_dt=0.0025, max_cfl=1.0, desired_cfl=0.9, nout=1,
+                  subcycle=1, solver=ADVECTION_MANIFOLD, problem=FILAMENT, criteria=MINMAX,
+                  pparams=(0.0, 0.0, 0.5, 1.0, 0.25), claw_version=claw_version,
+                  extent=(0.0, 2.0, 0.0, 2.0), brick=2)
 
 
 QUADRANT_STATES = (

@@ -18,6 +18,7 @@ PIN_CONFIGS = {
     "radialdam": O.radialdam_regression, "radialdam_claw5": lambda: O.radialdam_regression(5),
     "bump": O.bump_regression, "bump_claw5": lambda: O.bump_regression(5),
     "periodic": O.periodic_regression, "periodic_claw5": lambda: O.periodic_regression(5),
+    "filament": O.filament_regression, "filament_claw5": lambda: O.filament_regression(5),
 }
 
 
@@ -25,7 +26,8 @@ PIN_CONFIGS = {
 def test_regression_pins(name):
     """applications/**/regression_values_{0,1}.csv: count_amr_advance,
     global_num_patches and count_amr_new_domain of the clawpack 4.6 runs and
-    the --user:claw-version=5 runs of swirl, quadrants and bump (bump's
+    the --user:claw-version=5 runs of swirl, quadrants, bump, the periodic
+    brick and the cart-mapped filament brick with capacity (bump's
     clawpack 5 run has solid walls on all four sides, 14 new domains in 24
     advances), and of the radialdam runs with clawpack 4.6 and 5 (time-sync,
     cellave2 initial depth, gradient tagging on [-2.5, 2.5]^2)."""
