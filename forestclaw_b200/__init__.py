@@ -21,8 +21,9 @@ import numpy as np
 
 __all__ = ["Options", "Solver", "Comm", "local_group", "nccl_unique_id", "nccl_comm", "partition_plan", "lib",
            "FcbError", "SOLVER_ADVECTION", "SOLVER_SWE_ROE",
-           "SOLVER_EULER4_ROE", "SOLVER_GEOCLAW_FWAVE", "PROBLEM_SWIRL", "PROBLEM_RADIALDAM",
-           "PROBLEM_QUADRANTS", "PROBLEM_BATHY", "PROBLEM_RADIALDAM_CELLAVE", "PROBLEM_HUMP", "PROBLEM_PERIODIC_DISC",
+           "SOLVER_EULER4_ROE", "SOLVER_GEOCLAW_FWAVE", "SOLVER_ADVECTION_MANIFOLD", "PROBLEM_SWIRL",
+           "PROBLEM_RADIALDAM", "PROBLEM_QUADRANTS", "PROBLEM_BATHY", "PROBLEM_RADIALDAM_CELLAVE", "PROBLEM_HUMP",
+           "PROBLEM_PERIODIC_DISC", "PROBLEM_FILAMENT",
            "PRECISION_FP64", "PRECISION_MIXED", "measure_fp_rate",
            "TAG_VALUE", "TAG_MINMAX", "TAG_DIFFERENCE", "TAG_GRADIENT", "EXPORTED_SYMBOLS"]
 
@@ -30,9 +31,11 @@ PKG = Path(__file__).resolve().parent
 LIBPATH = PKG / "libfclaw_b200.so"
 
 SOLVER_ADVECTION, SOLVER_SWE_ROE, SOLVER_EULER4_ROE, SOLVER_GEOCLAW_FWAVE = 0, 1, 2, 3
+SOLVER_ADVECTION_MANIFOLD = 4
 PROBLEM_SWIRL, PROBLEM_RADIALDAM, PROBLEM_QUADRANTS, PROBLEM_BATHY, PROBLEM_RADIALDAM_CELLAVE = 0, 1, 2, 3, 4
 PROBLEM_HUMP = 5
 PROBLEM_PERIODIC_DISC = 6
+PROBLEM_FILAMENT = 7
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 TAG_VALUE, TAG_MINMAX, TAG_DIFFERENCE, TAG_GRADIENT = 0, 1, 2, 3
 

@@ -184,8 +184,9 @@ __global__ void qinit_kernel(const QinitArgs a) {
             q[((int64_t)0 * ny + r) * nx + c] = a.p[3] * win + a.p[4] * (1.0 - win);
             q[((int64_t)1 * ny + r) * nx + c] = 0.0;
             q[((int64_t)2 * ny + r) * nx + c] = 0.0;
-        } else if (a.problem == PROB_PERIODIC_DISC) {
+        } else if (a.problem == PROB_PERIODIC_DISC || a.problem == PROB_FILAMENT) {
             // advection/2d/periodic/user_4.6/qinit.f: q(i,j,1) = the cell's fraction inside the disc
+            // (filament/user_4.6/qinit.f with its fdisc.f: the disc of radius 0.25 about (0.5, 1))
             DiscD dsc{a.p[2], a.p[3], a.p[4]};
             dsc.kind = 1;
             q[r * nx + c] = cellave2_d(dsc, mt.xlower + (i - 1.0) * mt.dx, mt.ylower + (j - 1.0) * mt.dy, mt.dx, mt.dy);
@@ -206,10 +207,51 @@ __global__ void qinit_kernel(const QinitArgs a) {
     }
 }
 
+// filament/psi.f: psi = (4/3) r**3 (r**3 as r*r*r), r = sqrt((x-1)**2 + (y-1)**2)
+__device__ __forceinline__ double psi_filament(double x, double y) {
+    const double r = sqrt((x - 1.0) * (x - 1.0) + (y - 1.0) * (y - 1.0));
+    return (4.0 / 3.0) * (r * r * r);
+}
+
+// src/patches/metric/fortran_source2d/fclaw2d_metric_default_fort.f90
+// get_area_approx with norm_cross: |T_xi x T_eta| at the centre of the bilinear
+// cell with corners (x0 + ic*dx, y0 + jc*dy), z = 0 (compute_area_affine)
+__device__ double area_affine(double x0, double y0, double dx, double dy) {
+    double cx[2][2], cy[2][2];
+    for (int ic = 0; ic < 2; ++ic)
+        for (int jc = 0; jc < 2; ++jc) {
+            cx[ic][jc] = x0 + ic * dx;
+            cy[ic][jc] = y0 + jc * dy;
+        }
+    double a01[3], a10[3], a11[3], txi[3], teta[3];
+    for (int m = 0; m < 3; ++m) {
+        const double c00 = m == 0 ? cx[0][0] : (m == 1 ? cy[0][0] : 0.0);
+        const double c10 = m == 0 ? cx[1][0] : (m == 1 ? cy[1][0] : 0.0);
+        const double c01 = m == 0 ? cx[0][1] : (m == 1 ? cy[0][1] : 0.0);
+        const double c11 = m == 0 ? cx[1][1] : (m == 1 ? cy[1][1] : 0.0);
+        a01[m] = c10 - c00;
+        a10[m] = c01 - c00;
+        a11[m] = c11 - c10 - c01 + c00;
+    }
+    for (int m = 0; m < 3; ++m) {
+        txi[m] = a01[m] + a11[m] * 0.5;
+        teta[m] = a10[m] + a11[m] * 0.5;
+    }
+    const double w1 = txi[1] * teta[2] - txi[2] * teta[1];
+    const double w2 = -txi[0] * teta[2] + txi[2] * teta[0];
+    const double w3 = txi[0] * teta[1] - txi[1] * teta[0];
+    return sqrt(w1 * w1 + w2 * w2 + w3 * w3);
+}
+
 // setaux for every listed slot, ghost cells included: the lake-at-rest
 // problem's aux(i,j,1) = b at the cell centres; the periodic problem's
 // aux(i,j,1) = uvel, aux(i,j,2) = vvel (advection/2d/periodic/user_4.6/
-// clawpack46_setaux.f; further components 0, unused).
+// clawpack46_setaux.f; further components 0, unused); the filament's
+// (advection/2d/all/user46_setaux_manifold.f on the cart-mapped brick, whose
+// nodes map to themselves exactly on this dyadic mesh) aux(i,j,1) =
+// area/(dx*dy), aux(i,j,2) = (psi(node(i,j+1)) - psi(node(i,j)))/dy,
+// aux(i,j,3) = -(psi(node(i+1,j)) - psi(node(i,j)))/dx; p[0] != 0 multiplies the
+// capacity by 1 + p[0]*xc*yc (a test setting that makes dtdx1d vary by cell).
 __global__ void setaux_kernel(int problem, int maux, double uvel, double vvel, double* aux, int64_t stride,
                               const int32_t* slots, const PatchMeta* meta, int n, int mx, int my, int mbc) {
     const int pi = blockIdx.x;
@@ -224,6 +266,15 @@ __global__ void setaux_kernel(int problem, int maux, double uvel, double vvel, d
             const double xc = mt.xlower + (c - mbc + 1 - 0.5) * mt.dx;
             const double yc = mt.ylower + (r - mbc + 1 - 0.5) * mt.dy;
             a[k] = bathy_b(xc, yc);
+        } else if (problem == PROB_FILAMENT) {
+            const int i = c - mbc + 1, j = r - mbc + 1;
+            const double xn = mt.xlower + (i - 1) * mt.dx, yn = mt.ylower + (j - 1) * mt.dy;
+            a[k] = area_affine(xn, yn, mt.dx, mt.dy) / (mt.dx * mt.dy);
+            if (uvel != 0.0)  // p[0]: the capacity modulation of the tests (0 in the application)
+                a[k] = a[k] * (1.0 + uvel * ((mt.xlower + (i - 0.5) * mt.dx) * (mt.ylower + (j - 0.5) * mt.dy)));
+            const double p00 = psi_filament(xn, yn);
+            a[nx * ny + k] = (psi_filament(xn, mt.ylower + j * mt.dy) - p00) / mt.dy;
+            a[2 * nx * ny + k] = -((psi_filament(mt.xlower + i * mt.dx, yn) - p00) / mt.dx);
         } else {
             a[k] = uvel;
             a[nx * ny + k] = vvel;

@@ -13,7 +13,13 @@ struct PatchMeta {
 };
 enum : int32_t { PATCH_SAVE_LAST = 1 };
 
-enum SolverKind : int32_t { SOLVER_ADVECTION = 0, SOLVER_SWE_ROE = 1, SOLVER_EULER4_ROE = 2, SOLVER_GEOCLAW_FWAVE = 3 };
+enum SolverKind : int32_t {
+    SOLVER_ADVECTION = 0,
+    SOLVER_SWE_ROE = 1,
+    SOLVER_EULER4_ROE = 2,
+    SOLVER_GEOCLAW_FWAVE = 3,
+    SOLVER_ADVECTION_MANIFOLD = 4
+};
 enum AuxKind : int32_t { AUX_NONE = 0, AUX_SWIRL = 1, AUX_STORED = 2 };
 
 // One patch of a launch that mixes patches of several solves (ensemble
@@ -179,6 +185,7 @@ enum Problem : int32_t {
     PROB_RADIALDAM_CELLAVE = 4,  // radialdam/user_4.6/qinit.f with cellave2.f
     PROB_HUMP = 5,               // shallow/2d/bump/user_4.6/qinit.f
     PROB_PERIODIC_DISC = 6,      // advection/2d/periodic/user_4.6/qinit.f, fdisc.f
+    PROB_FILAMENT = 7,           // advection/2d/filament (example 1): qinit.f, fdisc.f, user46_setaux_manifold.f
 };
 
 struct QinitArgs {

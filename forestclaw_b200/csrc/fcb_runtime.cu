@@ -81,6 +81,7 @@ void Context::check(cudaError_t e, const char* what) {
 static int solver_meqn(int kind) {
     switch (kind) {
         case FCB_SOLVER_ADVECTION: return 1;
+        case FCB_SOLVER_ADVECTION_MANIFOLD: return 1;
         case FCB_SOLVER_SWE_ROE: return 3;
         case FCB_SOLVER_EULER4_ROE: return 4;
         case FCB_SOLVER_GEOCLAW_FWAVE: return 3;
@@ -101,7 +102,19 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
     if (opt_.mx != opt_.my) bad("mx must equal my");
     if (opt_.mbc != 2) bad("mbc must be 2");
     if (opt_.mx != 8 && opt_.mx != 16 && opt_.mx != 32 && opt_.mx != 64) bad("mx must be 8, 16, 32 or 64");
-    if (opt_.mcapa > 0) bad("capacity (mcapa > 0) is not supported on this path");
+    if (opt_.mcapa > 0 && opt_.solver_kind != FCB_SOLVER_ADVECTION_MANIFOLD)
+        bad("capacity (mcapa > 0) is built for the manifold advection solver, which reads it in aux(1)");
+    if (opt_.solver_kind == FCB_SOLVER_ADVECTION_MANIFOLD) {
+        if (opt_.mcapa != 1 || opt_.maux < 3)
+            bad("the manifold advection solver needs mcapa = 1 and maux >= 3 (capacity, then the edge velocities)");
+        if (opt_.problem != FCB_PROBLEM_FILAMENT) bad("the manifold advection solver runs the filament problem");
+        if (opt_.claw_version == 5 || opt_.precision != 0 || (opt_.step_variant != 0 && opt_.step_variant != 1))
+            bad("capacity is built in the four-barrier clawpack 4.6 FP64 step form (step_variant 0 or 1)");
+        if (opt_.time_sync) bad("time-sync is built for the shallow-water Roe solver");
+        opt_.ghost_fusion = 1;  // the fused step is a pipelined form
+    }
+    if (opt_.problem == FCB_PROBLEM_FILAMENT && opt_.solver_kind != FCB_SOLVER_ADVECTION_MANIFOLD)
+        bad("the filament problem stores capacity and edge velocities for the manifold advection solver");
     if (solver_meqn(opt_.solver_kind) < 0) bad("unknown solver kind");
     if (opt_.meqn != solver_meqn(opt_.solver_kind)) bad("meqn does not match the solver");
     if (opt_.mwaves != opt_.meqn) bad("mwaves must equal meqn for the configured solvers");
@@ -135,7 +148,7 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
          opt_.problem == FCB_PROBLEM_HUMP) &&
         opt_.solver_kind != FCB_SOLVER_SWE_ROE)
         bad("radialdam and hump need SWE");
-    if (opt_.problem < FCB_PROBLEM_SWIRL || opt_.problem > FCB_PROBLEM_PERIODIC_DISC) bad("unknown problem");
+    if (opt_.problem < FCB_PROBLEM_SWIRL || opt_.problem > FCB_PROBLEM_FILAMENT) bad("unknown problem");
     if (opt_.ax == 0.0 && opt_.bx == 0.0 && opt_.ay == 0.0 && opt_.by == 0.0) {
         opt_.bx = 1.0;  // all four unset: the unit square
         opt_.by = 1.0;
@@ -145,7 +158,9 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
     if ((opt_.problem == FCB_PROBLEM_BATHY) != (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE))
         bad("the bathymetry problem and the GeoClaw f-wave solver go together");
     aux_kind_ = (opt_.solver_kind == FCB_SOLVER_ADVECTION) ? (opt_.problem == FCB_PROBLEM_SWIRL ? AUX_SWIRL : AUX_STORED)
-              : (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE) ? AUX_STORED : AUX_NONE;
+              : (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE || opt_.solver_kind == FCB_SOLVER_ADVECTION_MANIFOLD)
+                  ? AUX_STORED
+                  : AUX_NONE;
     if (opt_.solver_kind == FCB_SOLVER_GEOCLAW_FWAVE) {
         if (opt_.maux != 1) bad("the GeoClaw solver reads aux(1) = b: maux must be 1");
         if (opt_.order[1] != 0) bad("rpt2_geoclaw stops in the reference: the GeoClaw solver needs order (., 0)");
@@ -452,7 +467,9 @@ void Context::mesh_changed() {
     // the owned leaves in Morton order (all leaves on one rank)
     std::vector<int32_t> all(slot_of_.begin() + own_first_, slot_of_.begin() + own_first_ + own_count_);
     if (!all.empty()) check(cudaMemcpy(d_all_slots_.p, all.data(), all.size() * 4, cudaMemcpyHostToDevice), "all slots");
-    if ((opt_.problem == FCB_PROBLEM_BATHY || opt_.problem == FCB_PROBLEM_PERIODIC_DISC) && own_count_ > 0) {
+    if ((opt_.problem == FCB_PROBLEM_BATHY || opt_.problem == FCB_PROBLEM_PERIODIC_DISC ||
+         opt_.problem == FCB_PROBLEM_FILAMENT) &&
+        own_count_ > 0) {
         // the stored aux depends on the cell centres only (bathymetry) or is
         // constant (the periodic problem's velocities): recomputed for every patch
         check(launch_setaux(opt_.problem, opt_.maux, opt_.problem_params, d_aux_, aux_stride_, d_all_slots_.p, d_meta_,
@@ -1742,6 +1759,7 @@ std::mutex g_tune_mu;
 std::map<std::vector<int>, int> g_step_form_cache, g_ghost_unroll_cache;
 
 int default_step_form(const fcb_options_t& o) {
+    if (o.solver_kind == SOLVER_ADVECTION_MANIFOLD) return 1;  // capacity: four-barrier form only
     return (o.solver_kind == SOLVER_ADVECTION || o.claw_version == 5 || o.solver_kind == SOLVER_GEOCLAW_FWAVE ||
             o.precision == 1)
                ? 3
@@ -1775,7 +1793,9 @@ int Context::tune_step_form(const StepArgs& a, int n) {
     std::vector<int> cand;
     if (opt_.precision == 1 || opt_.claw_version == 5 || opt_.solver_kind == SOLVER_GEOCLAW_FWAVE) cand = {3};
     else if (aux_kind_ == AUX_SWIRL) cand = {1, 2, 3};
-    else if (opt_.solver_kind == SOLVER_SWE_ROE || opt_.solver_kind == SOLVER_EULER4_ROE) cand = {1};
+    else if (opt_.solver_kind == SOLVER_SWE_ROE || opt_.solver_kind == SOLVER_EULER4_ROE ||
+             opt_.solver_kind == SOLVER_ADVECTION_MANIFOLD)
+        cand = {1};
     else cand = {1, 3};
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st_, &cs);
@@ -2285,8 +2305,10 @@ cudaError_t launch_step_batch(const fcb_options_t& opt, int aux_kind, const Patc
     a.cfl_out = d_cfl;
     // the Roe systems of clawpack 4.6 in FP64 run the four-barrier CTA form (on
     // B200 about twice the pipelined form's rate for shallow water at mx = 32)
+    // (capacity exists in that form only)
     if (opt.precision != 1 && opt.claw_version != 5 &&
-        (opt.solver_kind == FCB_SOLVER_SWE_ROE || opt.solver_kind == FCB_SOLVER_EULER4_ROE))
+        (opt.solver_kind == FCB_SOLVER_SWE_ROE || opt.solver_kind == FCB_SOLVER_EULER4_ROE ||
+         opt.solver_kind == FCB_SOLVER_ADVECTION_MANIFOLD))
         return launch_step(opt.solver_kind, aux_kind, opt.mwaves, opt.mx, opt.my, opt.mbc, a, st);
     return opt.precision == 1
                ? launch_step_pipe_mixed(opt.solver_kind, aux_kind, opt.mwaves, opt.mx, opt.my, opt.mbc,

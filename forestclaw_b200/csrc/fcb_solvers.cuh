@@ -86,6 +86,28 @@ struct AdvectionSolver {
     }
 };
 
+// Scalar advection on a mapped grid: applications/clawpack/advection/2d/all/
+// clawpack46_rpn2adv_manifold.f, clawpack46_rpt2adv_manifold.f.  The arithmetic
+// of rpn2adv / rpt2adv with the edge velocities in aux(2:3), after the
+// capacity kappa = area / (dx dy) in aux(1) (mcapa = 1), which the step then
+// applies (clawpack46_step2.f:122-126,191-195, clawpack46_flux2.f:134-220,
+// clawpack46_step2_wrap.f:118-121).
+template <int W_>
+struct AdvectionManifoldSolver : AdvectionSolver<W_> {};
+
+// Stored-aux layout of a solver: the first aux component its Riemann solvers
+// read, and whether aux(1) is the capacity.
+template <class SOL>
+struct AuxLayout {
+    static constexpr int SHIFT = 0;
+    static constexpr bool CAPA = false;
+};
+template <int W_>
+struct AuxLayout<AdvectionManifoldSolver<W_>> {
+    static constexpr int SHIFT = 1;
+    static constexpr bool CAPA = true;
+};
+
 // ---------------------------------------------------------------------------
 // Shallow water, Roe with entropy fix:
 // applications/clawpack/shallow/2d/rp/clawpack46_rpn2.f:1-247, clawpack46_rpt2.f:1-74

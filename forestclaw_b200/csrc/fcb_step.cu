@@ -81,6 +81,10 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     constexpr int PPB = TPB / NX;
     using L = StepSmem<NX, NY, PPB, M, W, NAUX, AUXK == AUX_SWIRL, NC>;
     using Cell = typename SOL::Cell;
+    // mapped grids: the Riemann solvers read aux from component KS on, and
+    // aux(1) is the capacity kappa (dtdx1d(i) = dtdx / kappa(i), clawpack46_step2.f:122-126)
+    constexpr int KS = AuxLayout<SOL>::SHIFT;
+    constexpr bool CAPA = AuxLayout<SOL>::CAPA;
     const MethodC<LIM> meth{a};
     extern __shared__ double smem[];
     double* s_qrow = smem + L::QROW;  // [3][PPB][NX][M]: rows s-2, s-1, s (slot row % 3)
@@ -190,6 +194,15 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         if constexpr (NAUX > 0) return s_aux[((pl * NAUX + k) * NY + rr) * NX + cc];
         else return 0.0;
     };
+    // dtdx1d / dtdy1d of cell (cc, rr)
+    auto DTDX = [&](int cc, int rr) -> double {
+        if constexpr (CAPA) return dtdx / AUXV(0, cc, rr);
+        else return dtdx;
+    };
+    auto DTDY = [&](int cc, int rr) -> double {
+        if constexpr (CAPA) return dtdy / AUXV(0, cc, rr);
+        else return dtdy;
+    };
 
     const bool ycol = active && c >= 1 && c <= NX - 2;
     double cfl = 0.0;
@@ -250,7 +263,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 double q_m1[M];
 #pragma unroll
                 for (int m = 0; m < M; ++m) q_m1[m] = QR(s - 1, c)[m];
-                sol.rpn2c(2, q_m1, q_n, *CELL(s - 1, c), cn, AUXV(1, c, s), yw_n, ys_n, yam_n, yap_n, yR_n);
+                sol.rpn2c(2, q_m1, q_n, *CELL(s - 1, c), cn, AUXV(1 + KS, c, s), yw_n, ys_n, yam_n, yap_n, yR_n);
 #pragma unroll
                 for (int mw = 0; mw < W; ++mw) {
                     double d = yw_f[mw][0] * yw_n[mw][0];
@@ -271,10 +284,13 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             for (int mw = 0; mw < W; ++mw)
 #pragma unroll
                 for (int m = 0; m < M; ++m) w[mw][m] = yw_f[mw][m];
+            // dtdy1d of the cells below (f-1) and above (f) the interface
+            const double dty_lo = DTDY(c, f - 1), dty_hi = DTDY(c, f);
             if (f >= MBC && f <= MBC + MX) {
 #pragma unroll
-                for (int mw = 0; mw < W; ++mw) cfl = nanmax(nanmax(cfl, dtdy * ys_f[mw]), -dtdy * ys_f[mw]);
+                for (int mw = 0; mw < W; ++mw) cfl = nanmax(nanmax(cfl, dty_hi * ys_f[mw]), -dty_lo * ys_f[mw]);
             }
+            const double dtyave = CAPA ? 0.5 * (dty_lo + dty_hi) : dtdyave;
             double cq[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) cq[m] = 0.0;
@@ -298,12 +314,12 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                     double acc;
                     {
                         const double as = fabs(ys_f[0]);
-                        acc = as * (1.0 - as * dtdyave) * w[0][m];
+                        acc = as * (1.0 - as * dtyave) * w[0][m];
                     }
 #pragma unroll
                     for (int mw = 1; mw < W; ++mw) {
                         const double as = fabs(ys_f[mw]);
-                        acc = acc + as * (1.0 - as * dtdyave) * w[mw][m];
+                        acc = acc + as * (1.0 - as * dtyave) * w[mw][m];
                     }
                     cq[m] = acc;
                 }
@@ -323,12 +339,12 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             if (meth.transverse()) {
                 double bm[M], bp[M];
                 // imp = 1: aux2(j-1, kv=1), aux3(j-1, kv=1) = u at columns c, c+1, row f-1
-                sol.rpt2(2, am, yR_f, AUXV(0, c, f - 1), AUXV(0, c + 1, f - 1), bm, bp);
+                sol.rpt2(2, am, yR_f, AUXV(KS, c, f - 1), AUXV(KS, c + 1, f - 1), bm, bp);
 #pragma unroll
-                for (int m = 0; m < M; ++m) { gLm[m] = 0.5 * dtdy * bm[m]; gLp[m] = 0.5 * dtdy * bp[m]; }
-                sol.rpt2(2, ap, yR_f, AUXV(0, c, f), AUXV(0, c + 1, f), bm, bp);
+                for (int m = 0; m < M; ++m) { gLm[m] = 0.5 * dty_lo * bm[m]; gLp[m] = 0.5 * dty_lo * bp[m]; }
+                sol.rpt2(2, ap, yR_f, AUXV(KS, c, f), AUXV(KS, c + 1, f), bm, bp);
 #pragma unroll
-                for (int m = 0; m < M; ++m) { gRm[m] = 0.5 * dtdy * bm[m]; gRp[m] = 0.5 * dtdy * bp[m]; }
+                for (int m = 0; m < M; ++m) { gRm[m] = 0.5 * dty_hi * bm[m]; gRp[m] = 0.5 * dty_hi * bp[m]; }
             } else {
 #pragma unroll
                 for (int m = 0; m < M; ++m) gLm[m] = gLp[m] = gRm[m] = gRp[m] = 0.0;
@@ -373,17 +389,21 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
         const bool xint = xrow && c >= 1;
         double xwl[W][M], xsl[W], xam[M], xap[M];
         typename SOL::Roe xR{};
+        // dtdx1d of the cells left (c-1) and right (c) of the interface
+        double dtx_lo = dtdx, dtx_hi = dtdx;
         if (xint) {
+            dtx_lo = DTDX(c - 1, s);
+            dtx_hi = DTDX(c, s);
             double qL[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) qL[m] = QR(s, c - 1)[m];
-            sol.rpn2c(1, qL, q_n, *CELL(s, c - 1), *CELL(s, c), AUXV(0, c, s), xwl, xsl, xam, xap, xR);
+            sol.rpn2c(1, qL, q_n, *CELL(s, c - 1), *CELL(s, c), AUXV(KS, c, s), xwl, xsl, xam, xap, xR);
 #pragma unroll
             for (int mw = 0; mw < W; ++mw) {
                 xs[c * W + mw] = xsl[mw];
 #pragma unroll
                 for (int m = 0; m < M; ++m) xw[(c * W + mw) * M + m] = xwl[mw][m];
-                if (c >= MBC && c <= MBC + MX) cfl = nanmax(nanmax(cfl, dtdx * xsl[mw]), -dtdx * xsl[mw]);
+                if (c >= MBC && c <= MBC + MX) cfl = nanmax(nanmax(cfl, dtx_hi * xsl[mw]), -dtx_lo * xsl[mw]);
             }
         }
 
@@ -395,6 +415,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
 #pragma unroll
         for (int m = 0; m < M; ++m) gRmx[m] = gRpx[m] = 0.0;
         if (xint) {
+            const double dtxave = CAPA ? 0.5 * (dtx_lo + dtx_hi) : dtdxave;
             double cq[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) cq[m] = 0.0;
@@ -425,12 +446,12 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                     double acc;
                     {
                         const double as = fabs(xsl[0]);
-                        acc = as * (1.0 - as * dtdxave) * xwl[0][m];
+                        acc = as * (1.0 - as * dtxave) * xwl[0][m];
                     }
 #pragma unroll
                     for (int mw = 1; mw < W; ++mw) {
                         const double as = fabs(xsl[mw]);
-                        acc = acc + as * (1.0 - as * dtdxave) * xwl[mw][m];
+                        acc = acc + as * (1.0 - as * dtxave) * xwl[mw][m];
                     }
                     cq[m] = acc;
                 }
@@ -449,15 +470,15 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
             if (meth.transverse()) {
                 double bm[M], bp[M];
                 // imp = 1: aux2(i-1, kv=2), aux3(i-1, kv=2) = v at column c-1, rows s, s+1
-                sol.rpt2(1, am, xR, AUXV(1, c - 1, s), AUXV(1, c - 1, s + 1), bm, bp);
+                sol.rpt2(1, am, xR, AUXV(1 + KS, c - 1, s), AUXV(1 + KS, c - 1, s + 1), bm, bp);
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
-                    gl[(c * 2 + 0) * M + m] = 0.5 * dtdx * bm[m];
-                    gl[(c * 2 + 1) * M + m] = 0.5 * dtdx * bp[m];
+                    gl[(c * 2 + 0) * M + m] = 0.5 * dtx_lo * bm[m];
+                    gl[(c * 2 + 1) * M + m] = 0.5 * dtx_lo * bp[m];
                 }
-                sol.rpt2(1, ap, xR, AUXV(1, c, s), AUXV(1, c, s + 1), bm, bp);
+                sol.rpt2(1, ap, xR, AUXV(1 + KS, c, s), AUXV(1 + KS, c, s + 1), bm, bp);
 #pragma unroll
-                for (int m = 0; m < M; ++m) { gRmx[m] = 0.5 * dtdx * bm[m]; gRpx[m] = 0.5 * dtdx * bp[m]; }
+                for (int m = 0; m < M; ++m) { gRmx[m] = 0.5 * dtx_hi * bm[m]; gRpx[m] = 0.5 * dtx_hi * bp[m]; }
             } else {
 #pragma unroll
                 for (int m = 0; m < M; ++m) { gl[(c * 2 + 0) * M + m] = 0.0; gl[(c * 2 + 1) * M + m] = 0.0; }
@@ -514,7 +535,11 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                 const double fpv = (fxp0 + gyu_l) + GYd_r[m];       // fp(i, j)
                 const double gmv = GXS(s - 1)[m] + FYm_cur[m];      // gm(i, j+1)
                 const double gpv = GXS(r)[m] + FYp_prev[m];         // gp(i, j)
-                const double qv = QR(r, c)[m] - dtdx * (fmv - fpv) - dtdy * (gmv - gpv);
+                double qv;
+                if constexpr (CAPA)  // clawpack46_step2_wrap.f:118-121
+                    qv = QR(r, c)[m] - (dtdx * (fmv - fpv) + dtdy * (gmv - gpv)) / AUXV(0, c, r);
+                else
+                    qv = QR(r, c)[m] - dtdx * (fmv - fpv) - dtdy * (gmv - gpv);
                 q[((int64_t)m * NY + r) * NX + c] = qv;
                 if (a.treg) {
                     // time-sync: boundary fluctuations scaled by dt and the edge
@@ -704,6 +729,10 @@ cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, in
         case SOLVER_EULER4_ROE:
             if (mwaves != 4 || aux_kind != AUX_NONE) return cudaErrorInvalidValue;
             return launch_mx<Euler4RoeSolver, AUX_NONE, 0>(mx, mbc, a, st);
+        case SOLVER_ADVECTION_MANIFOLD:
+            // capacity in aux(1), edge velocities in aux(2:3)
+            if (mwaves != 1 || aux_kind != AUX_STORED || a.maux < 3) return cudaErrorInvalidValue;
+            return launch_mx<AdvectionManifoldSolver<1>, AUX_STORED, 3>(mx, mbc, a, st);
         default: return cudaErrorInvalidValue;
     }
 }

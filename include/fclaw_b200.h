@@ -44,9 +44,12 @@ enum fcb_solver_kind {
     FCB_SOLVER_ADVECTION = 0,  /* clawpack46_rpn2adv / rpt2adv (edge velocities in aux) */
     FCB_SOLVER_SWE_ROE = 1,    /* shallow water Roe with entropy fix (clawpack46_rpn2/rpt2) */
     FCB_SOLVER_EULER4_ROE = 2, /* Euler Roe with entropy fix (clawpack46_rpn2_euler4/rpt2_euler4) */
-    FCB_SOLVER_GEOCLAW_FWAVE = 3 /* shallow water over bathymetry aux(1) = b: rpn2_geoclaw f-waves
-                                  * with clawpack46_flux2fw; order (2, 0) only, because the
-                                  * reference's rpt2_geoclaw stops; FP64 only */
+    FCB_SOLVER_GEOCLAW_FWAVE = 3, /* shallow water over bathymetry aux(1) = b: rpn2_geoclaw f-waves
+                                   * with clawpack46_flux2fw; order (2, 0) only, because the
+                                   * reference's rpt2_geoclaw stops; FP64 only */
+    FCB_SOLVER_ADVECTION_MANIFOLD = 4 /* clawpack46_rpn2adv_manifold / rpt2adv_manifold on a mapped grid:
+                                       * capacity aux(1) (mcapa = 1, clawpack46_step2.f / step2_wrap.f
+                                       * capacity form), edge velocities aux(2:3); clawpack 4.6, FP64 */
 };
 
 /* Initial conditions / b4step2 hooks of the configured applications. */
@@ -66,9 +69,16 @@ enum fcb_problem {
                                  * circle about (p[0], p[1]) of radius p[2] (cellave2.f) */
     FCB_PROBLEM_HUMP = 5,       /* shallow/2d/bump qinit (user_4.6/qinit.f, user_5.0/qinit.f90):
                                  * depth p[2] + exp(-p[3]*r2), r2 = (xc-p[0])^2 + (yc-p[1])^2, at rest */
-    FCB_PROBLEM_PERIODIC_DISC = 6 /* advection/2d/periodic (user_4.6/qinit.f, fdisc.f, clawpack46_setaux.f):
+    FCB_PROBLEM_PERIODIC_DISC = 6, /* advection/2d/periodic (user_4.6/qinit.f, fdisc.f, clawpack46_setaux.f):
                                  * q = the cell's fraction inside the disc of radius p[4] about (p[2], p[3])
                                  * (cellave2.f), constant velocity (p[0], p[1]) in aux(1:2), maux >= 2 */
+    FCB_PROBLEM_FILAMENT = 7    /* advection/2d/filament example 1 (cart-mapped 2 x 2 brick, extent [0, 2]^2):
+                                 * q as FCB_PROBLEM_PERIODIC_DISC with the disc (p[2], p[3]), radius p[4]
+                                 * (fdisc.f: (0.5, 1), 0.25); aux(1) = area/(dx dy) (the metric's affine
+                                 * area), aux(2:3) = edge velocities of psi = (4/3) r^3 about (1, 1)
+                                 * (user46_setaux_manifold.f, psi.f); manifold advection solver.
+                                 * p[0] != 0 (0 in the application) multiplies the capacity by
+                                 * 1 + p[0]*xc*yc at the cell centre (a test setting) */
 };
 
 /* Source terms (fc2d_clawpack46_vtable_t / fc2d_clawpack5_vtable_t src2). */

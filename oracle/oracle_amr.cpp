@@ -284,7 +284,8 @@ void Solver::setaux_patch(int p) {
     if (opt.problem == PROB_PERIODIC_DISC)  // pparams: uvel, vvel
         setaux_velocity(opt.mx, opt.my, opt.mbc, opt.maux, opt.pparams[0], opt.pparams[1], data[p].aux.data());
     if (opt.problem == PROB_FILAMENT)
-        setaux_filament(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), data[p].aux.data());
+        setaux_filament(opt.mx, opt.my, opt.mbc, xphys(p), yphys(p), dx(p), dy(p), opt.pparams[0],
+                        data[p].aux.data());
 }
 
 // clawpack46_update (fc2d_clawpack46.cpp:403-444) for one patch.

@@ -1119,7 +1119,8 @@ double area_approx(const double q[2][2][2]) {
 
 }  // namespace
 
-void setaux_filament(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double* aux) {
+void setaux_filament(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double kmod,
+                     double* aux) {
     const PatchIdx P(mx, my, mbc);
     const double dxdy = dx * dy;
     auto nx = [&](int i) { return xlower + (i - 1) * dx; };
@@ -1133,6 +1134,8 @@ void setaux_filament(int mx, int my, int mbc, double xlower, double ylower, doub
                     q[ic][jc][1] = ny(j) + jc * dy;
                 }
             aux[P(i, j, 0)] = area_approx(q) / dxdy;
+            if (kmod != 0.0)
+                aux[P(i, j, 0)] = aux[P(i, j, 0)] * (1.0 + kmod * ((xlower + (i - 0.5) * dx) * (ylower + (j - 0.5) * dy)));
         }
     for (int i = 1 - mbc; i <= mx + mbc; ++i)
         for (int j = 1 - mbc; j <= my + mbc; ++j) {

@@ -103,7 +103,10 @@ void setaux_velocity(int mx, int my, int mbc, int maux, double uvel, double vvel
 // psi = (4/3) r^3, r = |(x,y) - (1,1)|, node(i,j) = (xlower+(i-1)dx, ylower+(j-1)dy).
 // The brick and cart maps send every node of this dyadic mesh to the same
 // point of [0,2]^2 exactly, so the nodes are the physical coordinates.
-void setaux_filament(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double* aux);
+// kmod != 0 (a test setting; the application's is 0) multiplies the capacity
+// by 1 + kmod*xc*yc at the cell centre, so that dtdx1d varies from cell to cell.
+void setaux_filament(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, double kmod,
+                     double* aux);
 void qinit_disc_fraction(int mx, int my, int mbc, int meqn, double xlower, double ylower, double dx, double dy,
                          double x0, double y0, double r0, double* q);
 void qinit_bathy(int mx, int my, int mbc, double xlower, double ylower, double dx, double dy, const double* p,

@@ -114,3 +114,27 @@ def test_forest_morton_key_matches_bit_loop(tmp_path):
     subprocess.run(["g++", "-O2", "-std=c++17", "-I", str(ROOT / "forestclaw_b200" / "csrc"), str(src), "-o", str(exe)],
                    check=True)
     assert subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.strip() == "0"
+
+
+def test_capacity_options_are_checked():
+    """Capacity (mcapa > 0) belongs to the manifold advection solver, whose
+    update exists in the four-barrier clawpack 4.6 FP64 form; other
+    combinations fail at context creation (no device touched)."""
+    import cases
+    import forestclaw_b200 as fcb
+    import oracle as O
+
+    good = cases.to_options(O.filament_regression(4))
+    s = fcb.Solver(good)
+    del s
+    for change in (dict(mcapa=0), dict(claw_version=5), dict(precision=1), dict(maux=2), dict(step_variant=3),
+                   dict(problem=O.PERIODIC_DISC)):
+        opts = cases.to_options(O.filament_regression(4))
+        for k, v in change.items():
+            setattr(opts, k, v)
+        with pytest.raises(fcb.FcbError):
+            fcb.Solver(opts)
+    dam = cases.to_options(cases.radialdam_amr(seed=0, minlevel=2, maxlevel=3, mx=16))
+    dam.mcapa = 1
+    with pytest.raises(fcb.FcbError):
+        fcb.Solver(dam)

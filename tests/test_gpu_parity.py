@@ -144,6 +144,7 @@ PIN_CONFIGS = {
     "quadrants_claw5": lambda: O.quadrants_regression(5),
     "bump": O.bump_regression, "bump_claw5": lambda: O.bump_regression(5),
     "periodic": O.periodic_regression, "periodic_claw5": lambda: O.periodic_regression(5),
+    "filament": O.filament_regression,
 }
 
 
@@ -152,7 +153,8 @@ def test_regression_pins_on_gpu(gpu_lib, name):
     """The reference's own regression counters, reproduced by the CUDA path, with
     the final fields equal to the oracle's (bump: 24 advances and 14 new
     domains, its clawpack 5 run with solid walls, mthbc = 3 on all four sides;
-    periodic: a 2 x 2 brick periodic in x and y, 8 / 601 / 8)."""
+    periodic: a 2 x 2 brick periodic in x and y, 8 / 601 / 8; filament: the
+    cart-mapped 2 x 2 brick with capacity and the manifold solvers, 22 / 721 / 10)."""
     import json
     from pathlib import Path
 
@@ -160,8 +162,8 @@ def test_regression_pins_on_gpu(gpu_lib, name):
     cfg = PIN_CONFIGS[name]()
     # swirl velocities come from sin(), the bump's initial depth from exp(): CUDA
     # and glibc may differ in the last bit there; the Euler runs and the
-    # periodic brick (sqrt and arithmetic only) are exact
-    exact = name.startswith("quadrants") or name.startswith("periodic")
+    # periodic and filament bricks (sqrt and arithmetic only) are exact
+    exact = name.startswith("quadrants") or name.startswith("periodic") or name.startswith("filament")
     tol = 0.0 if exact else 1e-11
     o, d = _pair(cfg)
     _assert_same_mesh(o, d)
