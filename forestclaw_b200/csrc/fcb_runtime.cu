@@ -108,8 +108,8 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
         if (opt_.mcapa != 1 || opt_.maux < 3)
             bad("the manifold advection solver needs mcapa = 1 and maux >= 3 (capacity, then the edge velocities)");
         if (opt_.problem != FCB_PROBLEM_FILAMENT) bad("the manifold advection solver runs the filament problem");
-        if (opt_.claw_version == 5 || opt_.precision != 0 || (opt_.step_variant != 0 && opt_.step_variant != 1))
-            bad("capacity is built in the four-barrier clawpack 4.6 FP64 step form (step_variant 0 or 1)");
+        if (opt_.precision != 0 || (opt_.step_variant != 0 && opt_.step_variant != 1))
+            bad("capacity is built in the four-barrier FP64 step form (step_variant 0 or 1)");
         if (opt_.time_sync) bad("time-sync is built for the shallow-water Roe solver");
         opt_.ghost_fusion = 1;  // the fused step is a pipelined form
     }
@@ -184,7 +184,8 @@ Context::Context(const fcb_options_t& o, cudaStream_t st, std::shared_ptr<Comm> 
     if (comm_) opt_.ghost_fusion = 1;  // a partitioned ghost update exchanges between ranks
     if (opt_.claw_version == 0) opt_.claw_version = 4;
     if (opt_.claw_version != 4 && opt_.claw_version != 5) bad("claw_version must be 4 (clawpack 4.6) or 5");
-    if (opt_.claw_version == 5 && not_pipe) bad("the clawpack 5 update exists in the pipelined step form only");
+    if (opt_.claw_version == 5 && not_pipe && opt_.solver_kind != FCB_SOLVER_ADVECTION_MANIFOLD)
+        bad("the clawpack 5 update exists in the pipelined step form only (and the four-barrier form with capacity)");
     if (opt_.time_sync) {
         if (opt_.solver_kind != FCB_SOLVER_SWE_ROE)
             bad("time-sync needs the conservative flux rpn2_cons, given here for the shallow-water Roe solver");
@@ -1424,7 +1425,9 @@ void Context::launch_step_form(const StepArgs& a, int n) {
         StepArgs b = a;
         b.qsrc = d_qalt_;
         b.nbands = nb;
-        check(launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_), "step");
+        check(launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_,
+                          opt_.claw_version),
+              "step");
         cnt_.count_single_step += n;
         ++cnt_.count_kernel_launches;
         return;
@@ -1452,7 +1455,8 @@ void Context::launch_step_form(const StepArgs& a, int n) {
             if (!d_qalt_) arena_alloc(d_qalt_, (size_t)capacity_ * stride_ * sizeof(double));
             b.qtail = d_qalt_;
         }
-        e = launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_);
+        e = launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_,
+                        opt_.claw_version);
     }
     check(e, "step");
     cnt_.count_single_step += n;
@@ -1791,7 +1795,8 @@ int Context::tune_step_form(const StepArgs& a, int n) {
     // cost 2x at another (a one-wave four-barrier launch against a two-wave
     // pipelined one), so the pipelined form is not tried for them.
     std::vector<int> cand;
-    if (opt_.precision == 1 || opt_.claw_version == 5 || opt_.solver_kind == SOLVER_GEOCLAW_FWAVE) cand = {3};
+    if (opt_.solver_kind == SOLVER_ADVECTION_MANIFOLD) cand = {1};  // capacity: four-barrier form only
+    else if (opt_.precision == 1 || opt_.claw_version == 5 || opt_.solver_kind == SOLVER_GEOCLAW_FWAVE) cand = {3};
     else if (aux_kind_ == AUX_SWIRL) cand = {1, 2, 3};
     else if (opt_.solver_kind == SOLVER_SWE_ROE || opt_.solver_kind == SOLVER_EULER4_ROE ||
              opt_.solver_kind == SOLVER_ADVECTION_MANIFOLD)
@@ -1845,9 +1850,11 @@ int Context::tune_step_form(const StepArgs& a, int n) {
                 StepArgs bb = b;
                 bb.qsrc = ts;
                 bb.nbands = nb;
-                return launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, bb, st_);
+                return launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, bb, st_,
+                                   opt_.claw_version);
             }
-            return launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_);
+            return launch_step(opt_.solver_kind, aux_kind_, opt_.mwaves, opt_.mx, opt_.my, opt_.mbc, b, st_,
+                               opt_.claw_version);
         };
         if (launch() != cudaSuccess) {  // form not available for this case
             cudaGetLastError();
@@ -2305,10 +2312,11 @@ cudaError_t launch_step_batch(const fcb_options_t& opt, int aux_kind, const Patc
     a.cfl_out = d_cfl;
     // the Roe systems of clawpack 4.6 in FP64 run the four-barrier CTA form (on
     // B200 about twice the pipelined form's rate for shallow water at mx = 32)
-    // (capacity exists in that form only)
+    // (capacity exists in that form only, clawpack 4.6 and 5)
+    if (opt.solver_kind == FCB_SOLVER_ADVECTION_MANIFOLD)
+        return launch_step(opt.solver_kind, aux_kind, opt.mwaves, opt.mx, opt.my, opt.mbc, a, st, opt.claw_version);
     if (opt.precision != 1 && opt.claw_version != 5 &&
-        (opt.solver_kind == FCB_SOLVER_SWE_ROE || opt.solver_kind == FCB_SOLVER_EULER4_ROE ||
-         opt.solver_kind == FCB_SOLVER_ADVECTION_MANIFOLD))
+        (opt.solver_kind == FCB_SOLVER_SWE_ROE || opt.solver_kind == FCB_SOLVER_EULER4_ROE))
         return launch_step(opt.solver_kind, aux_kind, opt.mwaves, opt.mx, opt.my, opt.mbc, a, st);
     return opt.precision == 1
                ? launch_step_pipe_mixed(opt.solver_kind, aux_kind, opt.mwaves, opt.mx, opt.my, opt.mbc,

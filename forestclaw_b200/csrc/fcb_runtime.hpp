@@ -32,7 +32,7 @@ cudaError_t launch_step_batch(const fcb_options_t& opt, int aux_kind, const Patc
 
 // Kernel launchers (fcb_step.cu, fcb_ghost.cu, fcb_amr.cu)
 cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, const StepArgs& a,
-                        cudaStream_t st);
+                        cudaStream_t st, int claw_version = 4);
 cudaError_t launch_step_warp_swirl(int mx, int mbc, const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_pipe(int solver, int aux_kind, int mwaves, int mx, int my, int mbc, int claw_version,
                              const StepArgs& a, cudaStream_t st);

@@ -92,8 +92,9 @@ struct AdvectionSolver {
 // capacity kappa = area / (dx dy) in aux(1) (mcapa = 1), which the step then
 // applies (clawpack46_step2.f:122-126,191-195, clawpack46_flux2.f:134-220,
 // clawpack46_step2_wrap.f:118-121).
-template <int W_>
-struct AdvectionManifoldSolver : AdvectionSolver<W_> {};
+// V5: clawpack5_rpn2adv_manifold.f90 / rpt2adv_manifold.f90, the same arithmetic.
+template <int W_, bool V5_ = false>
+struct AdvectionManifoldSolver : AdvectionSolver<W_, double, V5_> {};
 
 // Stored-aux layout of a solver: the first aux component its Riemann solvers
 // read, and whether aux(1) is the capacity.
@@ -102,8 +103,8 @@ struct AuxLayout {
     static constexpr int SHIFT = 0;
     static constexpr bool CAPA = false;
 };
-template <int W_>
-struct AuxLayout<AdvectionManifoldSolver<W_>> {
+template <int W_, bool V5_>
+struct AuxLayout<AdvectionManifoldSolver<W_, V5_>> {
     static constexpr int SHIFT = 1;
     static constexpr bool CAPA = true;
 };

@@ -85,6 +85,12 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
     // aux(1) is the capacity kappa (dtdx1d(i) = dtdx / kappa(i), clawpack46_step2.f:122-126)
     constexpr int KS = AuxLayout<SOL>::SHIFT;
     constexpr bool CAPA = AuxLayout<SOL>::CAPA;
+    // clawpack 5 (scalar advection here): clawpack5_inlinelimiter.f's computed
+    // go to sends mthlim > 5 to its first branch (minmod), and
+    // clawpack5_step2_wrap.f updates the interior cells 1..mx, 1..my only;
+    // those read the interfaces 1..mx+1, whose fluxes are the same as 4.6's
+    constexpr bool V5 = SOL::V5;
+    auto LIMV = [](int l) { return (V5 && l > 5) ? 1 : l; };
     const MethodC<LIM> meth{a};
     extern __shared__ double smem[];
     double* s_qrow = smem + L::QROW;  // [3][PPB][NX][M]: rows s-2, s-1, s (slot row % 3)
@@ -304,7 +310,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                         for (int m = 1; m < M; ++m) wn2 = wn2 + yw_f[mw][m] * yw_f[mw][m];
                         if (wn2 == 0.0) continue;
                         const double r = (ys_f[mw] > 0.0) ? ydotl[mw] / wn2 : ydotr[mw] / wn2;
-                        const double phi = limiter_phi(meth.lim(mw), r);
+                        const double phi = limiter_phi(LIMV(meth.lim(mw)), r);
 #pragma unroll
                         for (int m = 0; m < M; ++m) w[mw][m] = phi * w[mw][m];
                     }
@@ -436,7 +442,7 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
                         }
                         if (wn2 == 0.0) continue;
                         const double r = (xsl[mw] > 0.0) ? dl / wn2 : dr / wn2;
-                        const double phi = limiter_phi(meth.lim(mw), r);
+                        const double phi = limiter_phi(LIMV(meth.lim(mw)), r);
 #pragma unroll
                         for (int m = 0; m < M; ++m) xwl[mw][m] = phi * xwl[mw][m];
                     }
@@ -523,7 +529,8 @@ __global__ void __launch_bounds__(TPB) step_kernel(const StepArgs a) {
 
         // ---------------- phase 5: update cell row r = s-2 ----------------
         const int r = s - 2;
-        if (active && r >= R0 && r < R1 && c <= NX - 2) {
+        const bool upd = V5 ? (c >= MBC && c < MBC + MX && r >= MBC && r < MBC + MX) : (c <= NX - 2);
+        if (active && r >= R0 && r < R1 && upd) {
             const double* fxr = s_fx + ((r % 3) * PPB + pl) * NX * 2 * M;
 #pragma unroll
             for (int m = 0; m < M; ++m) {
@@ -714,8 +721,10 @@ cudaError_t launch_mx(int mx, int mbc, const StepArgs& a, cudaStream_t st) {
 
 // Returns cudaErrorInvalidValue for an unsupported (solver, mx, mbc, aux) combination.
 cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, int mbc,
-                        const StepArgs& a, cudaStream_t st) {
+                        const StepArgs& a, cudaStream_t st, int claw_version) {
     if (mx != my) return cudaErrorInvalidValue;
+    // clawpack 5 exists in this form for the manifold advection solver only
+    if (claw_version == 5 && solver != SOLVER_ADVECTION_MANIFOLD) return cudaErrorInvalidValue;
     switch (solver) {
         case SOLVER_ADVECTION:
             if (mwaves != 1) return cudaErrorInvalidValue;
@@ -732,6 +741,7 @@ cudaError_t launch_step(int solver, int aux_kind, int mwaves, int mx, int my, in
         case SOLVER_ADVECTION_MANIFOLD:
             // capacity in aux(1), edge velocities in aux(2:3)
             if (mwaves != 1 || aux_kind != AUX_STORED || a.maux < 3) return cudaErrorInvalidValue;
+            if (claw_version == 5) return launch_mx<AdvectionManifoldSolver<1, true>, AUX_STORED, 3>(mx, mbc, a, st);
             return launch_mx<AdvectionManifoldSolver<1>, AUX_STORED, 3>(mx, mbc, a, st);
         default: return cudaErrorInvalidValue;
     }

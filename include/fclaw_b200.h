@@ -49,7 +49,8 @@ enum fcb_solver_kind {
                                    * reference's rpt2_geoclaw stops; FP64 only */
     FCB_SOLVER_ADVECTION_MANIFOLD = 4 /* clawpack46_rpn2adv_manifold / rpt2adv_manifold on a mapped grid:
                                        * capacity aux(1) (mcapa = 1, clawpack46_step2.f / step2_wrap.f
-                                       * capacity form), edge velocities aux(2:3); clawpack 4.6, FP64 */
+                                       * capacity form), edge velocities aux(2:3); clawpack 4.6 and 5
+                                       * (clawpack5_rpn2adv_manifold.f90, interior update), FP64 */
 };
 
 /* Initial conditions / b4step2 hooks of the configured applications. */

@@ -118,16 +118,17 @@ def test_forest_morton_key_matches_bit_loop(tmp_path):
 
 def test_capacity_options_are_checked():
     """Capacity (mcapa > 0) belongs to the manifold advection solver, whose
-    update exists in the four-barrier clawpack 4.6 FP64 form; other
+    update exists in the four-barrier FP64 form (clawpack 4.6 and 5); other
     combinations fail at context creation (no device touched)."""
     import cases
     import forestclaw_b200 as fcb
     import oracle as O
 
     good = cases.to_options(O.filament_regression(4))
-    s = fcb.Solver(good)
-    del s
-    for change in (dict(mcapa=0), dict(claw_version=5), dict(precision=1), dict(maux=2), dict(step_variant=3),
+    for ok in (good, cases.to_options(O.filament_regression(5))):
+        s = fcb.Solver(ok)
+        del s
+    for change in (dict(mcapa=0), dict(precision=1), dict(maux=2), dict(step_variant=3),
                    dict(problem=O.PERIODIC_DISC)):
         opts = cases.to_options(O.filament_regression(4))
         for k, v in change.items():

@@ -144,7 +144,7 @@ PIN_CONFIGS = {
     "quadrants_claw5": lambda: O.quadrants_regression(5),
     "bump": O.bump_regression, "bump_claw5": lambda: O.bump_regression(5),
     "periodic": O.periodic_regression, "periodic_claw5": lambda: O.periodic_regression(5),
-    "filament": O.filament_regression,
+    "filament": O.filament_regression, "filament_claw5": lambda: O.filament_regression(5),
 }
 
 
