@@ -657,8 +657,9 @@ def _fp_case(opts):
 
 def _bytes_per_cell(opts):
     # ghosted read + interior write of the state, plus the stored aux read
+    # (bathymetry; capacity and edge velocities of the manifold solver)
     r = (opts.mx + 2 * opts.mbc) ** 2 / (opts.mx * opts.my)
-    aux = opts.maux if opts.solver_kind == 3 else 0
+    aux = opts.maux if opts.solver_kind in (3, 4) else 0
     return 8.0 * (opts.meqn * (1.0 + r) + aux * r)
 
 
@@ -979,6 +980,18 @@ def run_extras(args, local_rank, main_line):
         return r
 
     guarded("bathymetry", c4)
+
+    def mapped():
+        o = workloads.filament()
+        m = amr_measure(o, 3, 2, stream, local_rank)
+        m["hbm_frac"] = m["value"] * _bytes_per_cell(o) / 1e9 / peaks()[0]
+        m["workload"] = ("filament (advection/2d/filament example 1 setup): cart-mapped 2 x 2 brick with capacity "
+                         "aux(1) and psi edge velocities aux(2:3), manifold advection solver (capacity form of the "
+                         "four-barrier step), levels 4-6 of each block, mx=my=32, subcycled, regrid every macro "
+                         "step; advance phase timed, FP64")
+        return m
+
+    guarded("filament", mapped)
 
     def serving():
         reqs = workloads.dam_break_requests(args.extra_requests, 7, maxlevels=(4, 5, 6, 7), tfinal=(0.02, 0.1))

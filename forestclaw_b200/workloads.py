@@ -3,8 +3,9 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import (PROBLEM_BATHY, PROBLEM_QUADRANTS, PROBLEM_RADIALDAM, PROBLEM_SWIRL, SOLVER_ADVECTION,
-               SOLVER_EULER4_ROE, SOLVER_GEOCLAW_FWAVE, SOLVER_SWE_ROE, TAG_GRADIENT, Options)
+from . import (PROBLEM_BATHY, PROBLEM_FILAMENT, PROBLEM_QUADRANTS, PROBLEM_RADIALDAM, PROBLEM_SWIRL,
+               SOLVER_ADVECTION, SOLVER_ADVECTION_MANIFOLD, SOLVER_EULER4_ROE, SOLVER_GEOCLAW_FWAVE, SOLVER_SWE_ROE,
+               TAG_GRADIENT, TAG_MINMAX, Options)
 
 
 def uniform_swirl(level: int = 8, mx: int = 16) -> Options:
@@ -98,3 +99,20 @@ def dam_break_requests(n: int, seed: int, maxlevels=(4, 5, 6, 7), tfinal=(0.2, 1
         o.subcycle = subcycle
         out.append(o)
     return out
+
+
+def filament(minlevel: int = 4, maxlevel: int = 6, mx: int = 32, claw_version: int = 4) -> Options:
+    """The filament application (advection/2d/filament, example 1) on a finer
+    mesh: a 2 x 2 brick under the cart mapping, [0, 2]^2, capacity in aux(1)
+    (mcapa = 1) and the edge velocities of psi = (4/3) r^3 about (1, 1) in
+    aux(2:3), manifold advection solvers, van Leer limiter, minmax tagging
+    (refine > 0.25, coarsen < 0.05), the disc of radius 0.25 about (0.5, 1) as
+    cell fractions; levels per block, subcycled, regrid every step, adaptive dt
+    (initial dt: CFL 0.9 at the largest edge speed, 8, on the coarsest level)."""
+    return Options(mx=mx, my=mx, mbc=2, meqn=1, maux=3, order=(2, 2), mcapa=1, mwaves=1, mthlim=(3,),
+                   mthbc=(1, 1, 1, 1), minlevel=minlevel, maxlevel=maxlevel, subcycle=1, regrid_interval=1,
+                   smooth_refine=1, smooth_level=maxlevel, refinement_criteria=TAG_MINMAX, refine_threshold=0.25,
+                   coarsen_threshold=0.05, tfinal=0.1, initial_dt=0.9 / (8.0 * mx * (1 << minlevel)),
+                   max_cfl=1.0, desired_cfl=0.9, solver_kind=SOLVER_ADVECTION_MANIFOLD, problem=PROBLEM_FILAMENT,
+                   problem_params=(0.0, 0.0, 0.5, 1.0, 0.25), claw_version=claw_version,
+                   extent=(0.0, 2.0, 0.0, 2.0), brick=2)
