@@ -106,7 +106,8 @@ typedef struct fcb_options {
     int threshold_variable;    /* 1-based component used for tagging */
     /* [clawpack46] */
     int order[2];              /* method(2:3) */
-    int mcapa;                 /* must be 0: capacity is not part of this path */
+    int mcapa;                 /* 0, or 1 with FCB_SOLVER_ADVECTION_MANIFOLD: capacity kappa in aux(1)
+                                * (the four-barrier FP64 step form, clawpack 4.6 or 5) */
     int mwaves;
     int mthlim[8];
     int mthbc[4];              /* left, right, bottom, top: 1 extrapolation, 3 wall */
